@@ -1,0 +1,445 @@
+/*
+ * mfcfd_capi.cpp - the extern "C" boundary declared in include/mfcfd.h.
+ *
+ * Owns the device copy of one point cloud and its iteration state, and maps
+ * each reference entry point (fpi_solver, the q_lskum loop, the setup
+ * routines) onto kernel launches on the handle's stream.
+ */
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "mfcfd_internal.h"
+
+using namespace mfcfd;
+
+struct mfcfd_handle {
+    mfcfd_params P;
+    Topology T;
+    DevCloud d;
+    cudaStream_t stream = nullptr;
+    double *U_buf[2] = {nullptr, nullptr};
+    double *q_buf[2] = {nullptr, nullptr};
+    int cur = 0;          // U/q buffer the next iteration reads
+    int last = 0;         // U/q buffer the last iteration read
+    std::vector<void *> allocs;
+    std::string err;
+    double res_old = 0.0, res_new = 0.0, residue = 0.0;
+    int res_cap = 1024;
+    int64_t bytes = 0;
+    bool have_state = false;
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev;          // (MFCFD_NPHASE+1) per iteration slot
+    double phase_ms[MFCFD_NPHASE] = {0};
+    int64_t prof_iters = 0;
+};
+
+namespace {
+
+const char *kStrerr[] = {"ok", "bad argument", "CUDA error", "stencil too wide",
+                         "singular least-squares system", "non-finite residual",
+                         "unsupported input", "out of device memory", "device wait timed out"};
+
+int fail(mfcfd_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(mfcfd_handle *h, cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(h, e == cudaErrorMemoryAllocation ? MFCFD_ERR_NOMEM : MFCFD_ERR_CUDA, m);
+}
+
+#define CK(call)                                                        \
+    do {                                                                \
+        cudaError_t e_ = (call);                                        \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);          \
+    } while (0)
+
+template <typename T>
+int dalloc(mfcfd_handle *h, T **p, size_t count) {
+    size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+    void *v = nullptr;
+    cudaError_t e = cudaMalloc(&v, bytes);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
+    h->allocs.push_back(v);
+    h->bytes += (int64_t)bytes;
+    *p = (T *)v;
+    return MFCFD_OK;
+}
+
+template <typename T>
+int upload(mfcfd_handle *h, const T **dst, const std::vector<T> &src) {
+    T *p = nullptr;
+    int rc = dalloc(h, &p, src.size());
+    if (rc) return rc;
+    if (!src.empty()) CK(cudaMemcpyAsync(p, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, h->stream));
+    *dst = p;
+    return MFCFD_OK;
+}
+
+void release(mfcfd_handle *h) {
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    h->ev.clear();
+    for (void *p : h->allocs) cudaFree(p);
+    h->allocs.clear();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    h->stream = nullptr;
+}
+
+int finish_step(mfcfd_handle *h, int32_t t, double res_new) {
+    h->res_new = res_new;
+    if (t <= 2) {                      // fpi_solver.f90:38-40
+        h->res_old = res_new;
+        h->residue = 0.0;
+    } else {
+        h->residue = std::log10(res_new / h->res_old);
+    }
+    if (!std::isfinite(res_new)) return fail(h, MFCFD_ERR_NONFINITE, "res_new is not finite");
+    return MFCFD_OK;
+}
+
+int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist) {
+    if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
+    std::vector<double> res(h->res_cap);
+    int status = MFCFD_OK;
+    for (int32_t done = 0; done < iters;) {
+        int chunk = std::min<int32_t>(iters - done, h->res_cap);
+        for (int j = 0; j < chunk; ++j) {
+            DevCloud dc = h->d;
+            dc.U = h->U_buf[h->cur];
+            dc.q = h->q_buf[h->cur];
+            cudaEvent_t *ev = h->profiling ? &h->ev[(size_t)j * (MFCFD_NPHASE + 1)] : nullptr;
+            cudaError_t e = launch_iteration(dc, j, h->stream, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], ev);
+            if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+            h->last = h->cur;
+            h->cur = 1 - h->cur;
+        }
+        CK(cudaMemcpyAsync(res.data(), h->d.res_dev, sizeof(double) * chunk, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->profiling) {
+            for (int j = 0; j < chunk; ++j) {
+                const cudaEvent_t *ev = &h->ev[(size_t)j * (MFCFD_NPHASE + 1)];
+                for (int ph = 0; ph < MFCFD_NPHASE; ++ph) {
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, ev[ph], ev[ph + 1]));
+                    h->phase_ms[ph] += ms;
+                }
+            }
+            h->prof_iters += chunk;
+        }
+        for (int j = 0; j < chunk; ++j) {
+            int32_t t = t0 + done + j;
+            int rc = finish_step(h, t, res[j]);
+            if (rc && status == MFCFD_OK) status = rc;
+            if (res_hist) {
+                res_hist[2 * (size_t)(done + j)] = h->res_new;
+                res_hist[2 * (size_t)(done + j) + 1] = h->residue;
+            }
+        }
+        done += chunk;
+    }
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    const double pi = 4.0 * std::atan(1.0);         // parameter.f90:19
+    const double theta = aoa_deg * pi / 180.0;      // parameter.f90:20
+    p->power = 0.0;                                 // parameter.f90:21
+    p->vl_const = 2.0;                              // parameter.f90:22
+    p->cfl = 5.0;                                   // parameter.f90:23
+    p->inner_iterations = 0;                        // parameter.f90:24
+    p->rho_inf = 1.0;                               // parameter.f90:29
+    p->u1_inf = mach * std::cos(theta);             // parameter.f90:30
+    p->u2_inf = mach * std::sin(theta);             // parameter.f90:31
+    p->u3_inf = 0.0;                                // parameter.f90:32
+    p->pr_inf = 1.0 / 1.4;                          // parameter.f90:33
+    p->split_capacity = 22;                         // data_structure.f90:83-88
+    p->precision = MFCFD_PRECISION_FP64;
+    p->device = 0;
+}
+
+int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, const double *x,
+                 const double *y, const double *z, const double *tan1, const double *tan2,
+                 const double *nor, const int32_t *nbhs, const int32_t *conn,
+                 const double *min_dist, mfcfd_handle **out) {
+    if (!out) return MFCFD_ERR_ARG;
+    *out = nullptr;
+    if (!params || n < 1 || !status || !x || !y || !z || !tan1 || !tan2 || !nor || !nbhs ||
+        !conn || !min_dist)
+        return MFCFD_ERR_ARG;
+    mfcfd_handle *h = new (std::nothrow) mfcfd_handle();
+    if (!h) return MFCFD_ERR_NOMEM;
+    h->P = *params;
+    const mfcfd_params &P = h->P;
+    if (P.power != 0.0 || P.inner_iterations != 0 || P.precision != MFCFD_PRECISION_FP64) {
+        h->err = "only power = 0, inner_iterations = 0 and FP64 are implemented";
+        *out = h;
+        return MFCFD_ERR_UNSUPPORTED;
+    }
+    if (P.split_capacity < 0 || P.split_capacity > 1000) {
+        h->err = "split_capacity out of range";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
+    int rc = build_topology(P, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, h->T, h->err);
+    *out = h;
+    if (rc) return rc;
+    const Topology &T = h->T;
+    if (P.device < 0) return MFCFD_OK;   // host-only handle: set-up results, no device state
+
+    if (cudaSetDevice(P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+
+    DevCloud &d = h->d;
+    std::memset(&d, 0, sizeof d);
+    d.n = n;
+    d.shared_frame = T.shared_frame;
+    std::memcpy(d.frame0, T.frame0, sizeof d.frame0);
+    d.power = P.power;
+    d.cfl = P.cfl;
+    d.rho_inf = P.rho_inf; d.u1_inf = P.u1_inf; d.u2_inf = P.u2_inf;
+    d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;
+
+    std::vector<double> vx(x, x + n), vy(y, y + n), vz(z, z + n);
+    std::vector<double> frame((size_t)n * 9);
+    for (int i = 0; i < n; ++i)
+        for (int r = 0; r < 3; ++r) {
+            frame[9 * (size_t)i + r] = tan1[3 * (size_t)i + r];
+            frame[9 * (size_t)i + 3 + r] = tan2[3 * (size_t)i + r];
+            frame[9 * (size_t)i + 6 + r] = nor[3 * (size_t)i + r];
+        }
+    std::vector<int32_t> vnb(nbhs, nbhs + n), vconn((size_t)n * MAX_CONN, 0);
+    for (size_t j = 0; j < vconn.size(); ++j) vconn[j] = conn[j] > 0 ? conn[j] - 1 : 0;
+    std::vector<int32_t> order;
+    order.insert(order.end(), T.wall_idx.begin(), T.wall_idx.end());
+    order.insert(order.end(), T.interior_idx.begin(), T.interior_idx.end());
+#define UP(field, vec) if ((rc = upload(h, &d.field, vec))) return rc
+    UP(x, vx); UP(y, vy); UP(z, vz); UP(frame, frame);
+    UP(cls, T.cls); UP(nbhs, vnb); UP(conn, vconn); UP(eps2, T.eps2);
+    UP(slot_nbr, T.slot_nbr); UP(nslot, T.nslot); UP(slot_mask, T.slot_mask);
+    UP(list_cnt, T.list_cnt); UP(list_ent, T.list_ent); UP(geo, T.geo);
+    UP(swept, T.swept); UP(consumer_shared, T.consumer_shared);
+    UP(fwd_lvl_ptr, T.fwd_lvl_ptr); UP(fwd_lvl_pts, T.fwd_lvl_pts);
+    UP(bwd_lvl_ptr, T.bwd_lvl_ptr); UP(bwd_lvl_pts, T.bwd_lvl_pts);
+    UP(fwd_off, T.fwd_off); UP(bwd_off, T.bwd_off);
+    UP(fwd_cnt, T.fwd_cnt); UP(bwd_cnt, T.bwd_cnt);
+    UP(fwd_ent, T.fwd_ent); UP(bwd_ent, T.bwd_ent);
+    UP(res_order, order);
+#undef UP
+    d.n_fwd_levels = (int)T.fwd_lvl_ptr.size() - 1;
+    d.n_bwd_levels = (int)T.bwd_lvl_ptr.size() - 1;
+    d.n_res = (int)order.size();
+    size_t n5 = (size_t)n * 5;
+#define AL(ptr, cnt) if ((rc = dalloc(h, &ptr, cnt))) return rc
+    AL(d.prim, n5); AL(h->U_buf[0], n5); AL(h->U_buf[1], n5); AL(h->q_buf[0], n5);
+    AL(h->q_buf[1], n5); AL(d.qm, (size_t)n * 10); AL(d.dq, (size_t)n * 15);
+    AL(d.delt, n); AL(d.flux_res, n5); AL(d.dUp, n5); AL(d.dUn, n5); AL(d.dinv, n);
+    AL(d.gold, (size_t)n * 30); AL(d.dgf, (size_t)n * 30); AL(d.dgb, (size_t)n * 30);
+    AL(d.res_sqr, n); AL(d.partial, 1024); AL(d.res_dev, h->res_cap);
+#undef AL
+    CK(cudaMemsetAsync(d.dUp, 0, n5 * 8, h->stream));
+    CK(cudaMemsetAsync(d.dUn, 0, n5 * 8, h->stream));
+    CK(cudaMemsetAsync(d.flux_res, 0, n5 * 8, h->stream));
+    CK(cudaMemsetAsync(d.dinv, 0, (size_t)n * 8, h->stream));
+    CK(cudaMemsetAsync(d.res_sqr, 0, (size_t)n * 8, h->stream));
+    d.U = h->U_buf[0];
+    d.q = h->q_buf[0];
+    CK(cudaStreamSynchronize(h->stream));
+    return MFCFD_OK;
+}
+
+int mfcfd_set_prim(mfcfd_handle *h, const double *prim) {
+    if (!h || !prim) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    size_t n5 = (size_t)h->d.n * 5;
+    CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->d.dUp, 0, n5 * 8, h->stream));
+    CK(cudaMemsetAsync(h->d.dUn, 0, n5 * 8, h->stream));
+    DevCloud dc = h->d;
+    dc.U = h->U_buf[h->cur];
+    dc.q = h->q_buf[h->cur];
+    CK(launch_conserved_q(dc, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->last = h->cur;
+    h->res_old = h->res_new = h->residue = 0.0;
+    h->have_state = true;
+    return MFCFD_OK;
+}
+
+int mfcfd_fpi_step(mfcfd_handle *h, int32_t t, double *res_new, double *residue) {
+    if (!h) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    double hist[2];
+    int rc = run_iterations(h, t, 1, hist);
+    if (res_new) *res_new = hist[0];
+    if (residue) *residue = hist[1];
+    return rc;
+}
+
+int mfcfd_run(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist) {
+    if (!h || iters < 0) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    return run_iterations(h, t0, iters, res_hist);
+}
+
+int mfcfd_get(mfcfd_handle *h, int32_t field, double *out) {
+    if (!h || !out) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    const DevCloud &d = h->d;
+    size_t n = (size_t)d.n;
+    const double *src = nullptr;
+    size_t w = 0;
+    switch (field) {
+    case MFCFD_FIELD_PRIM: src = d.prim; w = 5; break;
+    case MFCFD_FIELD_U: src = h->U_buf[h->last]; w = 5; break;
+    case MFCFD_FIELD_Q: src = h->q_buf[h->last]; w = 5; break;
+    case MFCFD_FIELD_QM: src = d.qm; w = 10; break;
+    case MFCFD_FIELD_DQ: src = d.dq; w = 15; break;
+    case MFCFD_FIELD_DELT: src = d.delt; w = 1; break;
+    case MFCFD_FIELD_FLUX_RES: src = d.flux_res; w = 5; break;
+    case MFCFD_FIELD_DELUP: src = d.dUp; w = 5; break;
+    case MFCFD_FIELD_DELUN: src = d.dUn; w = 5; break;
+    case MFCFD_FIELD_DINV: src = d.dinv; w = 1; break;
+    default: return fail(h, MFCFD_ERR_ARG, "unknown field");
+    }
+    CK(cudaMemcpyAsync(out, src, n * w * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MFCFD_OK;
+}
+
+int mfcfd_get_state(mfcfd_handle *h, double *prim, double *delu, double *res_old) {
+    if (!h || !prim || !delu) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    size_t n5 = (size_t)h->d.n * 5;
+    CK(cudaMemcpyAsync(prim, h->d.prim, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(delu, h->d.dUn, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (res_old) *res_old = h->res_old;
+    return MFCFD_OK;
+}
+
+int mfcfd_set_state(mfcfd_handle *h, const double *prim, const double *delu, double res_old) {
+    if (!h || !prim || !delu) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    size_t n5 = (size_t)h->d.n * 5;
+    CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d.dUn, delu, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d.dUp, delu, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+    DevCloud dc = h->d;
+    dc.U = h->U_buf[h->cur];
+    dc.q = h->q_buf[h->cur];
+    CK(launch_conserved_q(dc, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->last = h->cur;
+    h->res_old = res_old;
+    h->have_state = true;
+    return MFCFD_OK;
+}
+
+int mfcfd_get_stencils(mfcfd_handle *h, int32_t *counts, int32_t *lists, int32_t width) {
+    if (!h || !counts || !lists || width < 1) return MFCFD_ERR_ARG;
+    const Topology &T = h->T;
+    if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    for (int i = 0; i < T.n; ++i)
+        for (int dd = 0; dd < NDIR; ++dd) {
+            int c = T.split_cnt[dd][i];
+            counts[(size_t)i * NDIR + dd] = c;
+            for (int j = 0; j < width; ++j)
+                lists[((size_t)i * NDIR + dd) * width + j] =
+                    j < c ? T.split[dd][(size_t)i * T.cap + j] : 0;
+        }
+    return MFCFD_OK;
+}
+
+int mfcfd_get_alias(mfcfd_handle *h, int32_t *alias, int32_t *point_with_alias) {
+    if (!h || !alias || !point_with_alias) return MFCFD_ERR_ARG;
+    const Topology &T = h->T;
+    if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    std::memcpy(alias, T.alias.data(), sizeof(int32_t) * T.n);
+    std::memcpy(point_with_alias, T.point_with_alias.data(), sizeof(int32_t) * T.n);
+    return MFCFD_OK;
+}
+
+int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level) {
+    if (!h || !level || (dir != 0 && dir != 1)) return MFCFD_ERR_ARG;
+    const Topology &T = h->T;
+    if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    const std::vector<int32_t> &src = dir == 0 ? T.fwd_level : T.bwd_level;
+    std::memcpy(level, src.data(), sizeof(int32_t) * T.n);
+    return MFCFD_OK;
+}
+
+int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
+    if (!h || !info) return MFCFD_ERR_ARG;
+    const Topology &T = h->T;
+    std::memset(info, 0, sizeof *info);
+    info->n_points = T.n;
+    info->n_wall = (int32_t)T.wall_idx.size();
+    info->n_outer = (int32_t)T.outer_idx.size();
+    info->n_interior = (int32_t)T.interior_idx.size();
+    info->n_supersonic = 0;
+    info->n_levels_forward = T.fwd_lvl_ptr.empty() ? 0 : (int32_t)T.fwd_lvl_ptr.size() - 1;
+    info->n_levels_backward = T.bwd_lvl_ptr.empty() ? 0 : (int32_t)T.bwd_lvl_ptr.size() - 1;
+    info->max_level_width = T.max_level_width;
+    info->split_overflows = T.split_overflows;
+    info->shared_frame = T.shared_frame;
+    info->device_bytes = h->bytes;
+    return MFCFD_OK;
+}
+
+int mfcfd_get_stream(mfcfd_handle *h, void **stream) {
+    if (!h || !stream) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    *stream = (void *)h->stream;
+    return MFCFD_OK;
+}
+
+int mfcfd_set_profiling(mfcfd_handle *h, int32_t on) {
+    if (!h) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    if (on && h->ev.empty()) {
+        h->ev.resize((size_t)h->res_cap * (MFCFD_NPHASE + 1));
+        for (auto &e : h->ev) CK(cudaEventCreate(&e));
+    }
+    h->profiling = on != 0;
+    for (double &v : h->phase_ms) v = 0.0;
+    h->prof_iters = 0;
+    return MFCFD_OK;
+}
+
+int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters) {
+    if (!h || !ms) return MFCFD_ERR_ARG;
+    for (int p = 0; p < MFCFD_NPHASE; ++p) ms[p] = h->phase_ms[p];
+    if (iters) *iters = h->prof_iters;
+    return MFCFD_OK;
+}
+
+int mfcfd_destroy(mfcfd_handle *h) {
+    if (!h) return MFCFD_ERR_ARG;
+    release(h);
+    delete h;
+    return MFCFD_OK;
+}
+
+const char *mfcfd_last_error(const mfcfd_handle *h) {
+    if (!h) return "null handle";
+    return h->err.c_str();
+}
+
+const char *mfcfd_strerror(int code) {
+    if (code < 0 || code > MFCFD_ERR_TIMEOUT) return "unknown error";
+    return kStrerr[code];
+}
+
+}  // extern "C"

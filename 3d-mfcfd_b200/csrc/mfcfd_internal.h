@@ -1,0 +1,121 @@
+/*
+ * mfcfd_internal.h - data shared by the host set-up, the kernels and the C ABI.
+ */
+#pragma once
+
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/mfcfd.h"
+
+namespace mfcfd {
+
+constexpr int MAX_CONN = 27;      // conn(27, max_points), data_structure.f90:80
+constexpr int MAX_SLOTS = 32;     // distinct neighbours a point's lists may name
+constexpr int LIST_STRIDE = 28;   // bytes per (point, list) entry table: <= 27 entries
+constexpr int GEO_STRIDE = 48;    // doubles per point: 6 lists x 8
+constexpr int NDIR = 6;           // xpos, xneg, ypos, yneg, zpos, zneg
+
+enum PointClass : int8_t { CLS_INTERIOR = 0, CLS_WALL = 1, CLS_OUTER = 2, CLS_OTHER = 3 };
+
+// geo layout within one list's 8 doubles
+enum { G_XX = 0, G_YY, G_ZZ, G_XY, G_YZ, G_ZX, G_DET, G_DNUM };
+
+// One neighbour term of an LdelU / UdelU sum: neighbour and its weighted
+// offsets in the consumer's frame (dels*w, delt*w, deln*w).
+struct SweepEntry {
+    int32_t k;
+    int32_t pad;
+    double w[3];
+};
+
+// Everything the set-up derives from the cloud (host copy).
+struct Topology {
+    int n = 0;
+    int cap = 22;
+    std::vector<int8_t> cls;
+    // split lists exactly as stored by the reference (1-based ids, flat
+    // column-major with leading dimension cap, plus a tail pad)
+    std::vector<int32_t> split[NDIR];
+    std::vector<int32_t> split_cnt[NDIR];
+    int split_overflows = 0;
+    std::vector<int32_t> alias;             // 1-based values, 0 = none
+    std::vector<int32_t> point_with_alias;  // 1-based ids, 0 = none
+    // effective lists: the entries each flux / D_inv / sweep routine reads
+    std::vector<int32_t> slot_nbr;          // n*MAX_SLOTS, 0-based, -1 unused
+    std::vector<uint8_t> nslot;
+    std::vector<uint8_t> slot_mask;         // n*MAX_SLOTS, bit d: slot in list d
+    std::vector<uint8_t> list_cnt;          // n*6
+    std::vector<uint8_t> list_ent;          // n*6*LIST_STRIDE slot indices
+    std::vector<double> geo;                // n*GEO_STRIDE
+    std::vector<double> eps2;               // (VL*min_dist)^3 squared
+    // sweep schedules (0-based ids)
+    std::vector<int32_t> fwd_level, bwd_level;   // per point, -1 if not swept
+    std::vector<int32_t> fwd_lvl_ptr, fwd_lvl_pts, bwd_lvl_ptr, bwd_lvl_pts;
+    std::vector<int32_t> fwd_off, bwd_off;        // n+1 entry offsets
+    std::vector<uint8_t> fwd_cnt, bwd_cnt;        // n*6
+    std::vector<SweepEntry> fwd_ent, bwd_ent;
+    std::vector<uint8_t> swept;                   // 1 if the sweeps update the point
+    std::vector<uint8_t> consumer_shared;         // 1: reads published flux increments
+    int shared_frame = 0;
+    double frame0[9] = {0};
+    int max_level_width = 0;
+    std::vector<int32_t> wall_idx, outer_idx, interior_idx;   // 0-based, index order
+};
+
+// Build everything above.  Returns MFCFD_OK or an error code with a message.
+int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
+                   const double *y, const double *z, const double *tan1, const double *tan2,
+                   const double *nor, const int32_t *nbhs, const int32_t *conn,
+                   const double *min_dist, Topology &T, std::string &err);
+
+// Device-side views (plain pointers, passed to kernels by value).
+struct DevCloud {
+    int n;
+    int shared_frame;
+    double frame0[9];
+    double power, cfl;
+    double rho_inf, u1_inf, u2_inf, u3_inf, pr_inf;
+    // geometry
+    const double *x, *y, *z;
+    const double *frame;          // 9 per point: tan1, tan2, nor
+    const int8_t *cls;
+    const int32_t *nbhs;
+    const int32_t *conn;          // 27 per point, 0-based
+    const double *eps2;
+    const int32_t *slot_nbr;
+    const uint8_t *nslot;
+    const uint8_t *slot_mask;
+    const uint8_t *list_cnt;
+    const uint8_t *list_ent;
+    const double *geo;
+    const uint8_t *swept;
+    const uint8_t *consumer_shared;
+    // sweep schedules
+    const int32_t *fwd_lvl_ptr, *fwd_lvl_pts, *bwd_lvl_ptr, *bwd_lvl_pts;
+    int n_fwd_levels, n_bwd_levels;
+    const int32_t *fwd_off, *bwd_off;
+    const uint8_t *fwd_cnt, *bwd_cnt;
+    const SweepEntry *fwd_ent, *bwd_ent;
+    const int32_t *res_order;     // wall then interior ids, index order
+    int n_res;
+    // state (Fortran layout, point-major)
+    double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
+    double *gold;                 // 30 per point: fluxes of prim in frame0
+    double *dgf, *dgb;            // 30 per point: published flux increments
+    double *res_sqr;              // per point (residual sum terms)
+    double *partial;              // reduction scratch
+    double *res_dev;              // per-iteration res_new history
+};
+
+// kernel launchers (mfcfd_kernels.cu)
+// ev: null, or MFCFD_NPHASE+1 events recorded around the phases.
+cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
+                             double *U_next, double *q_next, cudaEvent_t *ev);
+cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
+int reduction_blocks(int n);
+
+}  // namespace mfcfd

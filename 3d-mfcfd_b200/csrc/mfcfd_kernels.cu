@@ -1,0 +1,568 @@
+/*
+ * mfcfd_kernels.cu - the FP64 q-LSKUM iteration on sm_100a.
+ *
+ * One iteration (fpi_solver.f90:27-36) is this launch sequence:
+ *   k_qderiv      q_derivatives + timestep_delt     thread per point
+ *   k_flux        eval_flux_residual                warp per point
+ *   k_dinv_gold   D_inv, fluxes of prim in the shared interior frame,
+ *                 flux increments of points the sweeps do not update
+ *   k_sweep x2    forward / backward LU-SGS sweep   one CTA, level by level
+ *   k_update      state_update_implicit + next iteration's U and q
+ *   k_reduce_*    res_new (deterministic two-pass sum)
+ * State stays resident in HBM in the reference's point-major layout.
+ *
+ * Built with -fmad=false: every multiply and add rounds separately, as in
+ * the reference's build; see mfcfd_physics.cuh for the expression order.
+ */
+#include <cuda_runtime.h>
+
+#include "mfcfd_internal.h"
+#include "mfcfd_physics.cuh"
+
+namespace mfcfd {
+
+constexpr int FLUX_WARPS = 4;            // warps per CTA in k_flux
+constexpr int FLUX_SMEM_PER_WARP = NDIR * MAX_SLOTS * 5 + MAX_SLOTS * 3;   // doubles
+constexpr int SWEEP_THREADS = 512;
+constexpr int SWEEP_WARPS = SWEEP_THREADS / 32;
+constexpr int SWEEP_SMEM_PER_WARP = 32 * 5 + 32 * 3;                      // doubles
+constexpr int RED_THREADS = 256;
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---------------------------------------------------------------- U and q
+
+// compute_conserved_vector + eval_q_variables for every point.
+__global__ void k_conserved_q(DevCloud d) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    Frame F;
+    load_frame(d.frame + 9 * (size_t)i, F);
+    double p[5], U[5], q[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) p[r] = d.prim[5 * (size_t)i + r];
+    primitive_to_rotated_conserved(p, F, U);
+    primitive_to_q(p, q);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        d.U[5 * (size_t)i + r] = U[r];
+        d.q[5 * (size_t)i + r] = q[r];
+    }
+}
+
+// ---------------------------------------------------------------- q-derivatives
+
+// eval_q_derivatives (q_derivatives.f90:25-110) and timestep_delt
+// (timestep_delt.f90:227-259), thread per point.  With power = 0 the weights
+// are exactly 1 and the products weights*delx*temp equal delx*temp.
+__global__ void __launch_bounds__(128) k_qderiv(DevCloud d) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const double xi = d.x[i], yi = d.y[i], zi = d.z[i];
+    double qi[5], qmax[5], qmin[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) { qi[r] = d.q[5 * (size_t)i + r]; qmax[r] = qi[r]; qmin[r] = qi[r]; }
+    double xx = 0, yy = 0, zz = 0, xy = 0, yz = 0, zx = 0;
+    double sx[5] = {0, 0, 0, 0, 0}, sy[5] = {0, 0, 0, 0, 0}, sz[5] = {0, 0, 0, 0, 0};
+    double min_delt = 1.0;
+    const int nb = d.nbhs[i];
+    const int32_t *cn = d.conn + (size_t)MAX_CONN * i;
+    for (int j = 0; j < nb; ++j) {
+        const int k = cn[j];
+        double qk[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            qk[r] = d.q[5 * (size_t)k + r];
+            if (qk[r] > qmax[r]) qmax[r] = qk[r];
+            if (qk[r] < qmin[r]) qmin[r] = qk[r];
+        }
+        const double delx = d.x[k] - xi, dely = d.y[k] - yi, delz = d.z[k] - zi;
+        const double dist = sqrt(delx * delx + dely * dely + delz * delz);
+        xx = xx + delx * delx;
+        yy = yy + dely * dely;
+        zz = zz + delz * delz;
+        xy = xy + delx * dely;
+        yz = yz + dely * delz;
+        zx = zx + delz * delx;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            const double t = qk[r] - qi[r];
+            sx[r] = sx[r] + delx * t;
+            sy[r] = sy[r] + dely * t;
+            sz[r] = sz[r] + delz * t;
+        }
+        // timestep_delt.f90:235-253
+        const double *pk = d.prim + 5 * (size_t)k;
+        const double rho = pk[0], u1 = pk[1], u2 = pk[2], u3 = pk[3], pr = pk[4];
+        const double mod_u = sqrt(u1 * u1 + u2 * u2 + u3 * u3);
+        const double delt = d.cfl * dist / (mod_u + 3.0 * sqrt(pr / rho));
+        if (delt < min_delt) min_delt = delt;
+    }
+    const double g[6] = {xx, yy, zz, xy, yz, zx};
+    const double det = xx * (yy * zz - yz * yz) - xy * (xy * zz - yz * zx) + zx * (xy * yz - yy * zx);
+    const double one_by_det = 1.0 / det;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        d.dq[15 * (size_t)i + 3 * r + 0] = cramer_num(0, g, sx[r], sy[r], sz[r]) * one_by_det;
+        d.dq[15 * (size_t)i + 3 * r + 1] = cramer_num(1, g, sx[r], sy[r], sz[r]) * one_by_det;
+        d.dq[15 * (size_t)i + 3 * r + 2] = cramer_num(2, g, sx[r], sy[r], sz[r]) * one_by_det;
+        d.qm[10 * (size_t)i + 2 * r + 0] = qmax[r];
+        d.qm[10 * (size_t)i + 2 * r + 1] = qmin[r];
+    }
+    d.delt[i] = min_delt;
+}
+
+// ---------------------------------------------------------------- flux residual
+
+// Limited midpoint reconstruction of point j's q toward the offset
+// (delx, dely, delz), then q -> primitive (interior_flux_dGxpos.f90:92-96,
+// limiters.f90:12-52, qvariables_to_primitive_variables.f90:9-31).
+__device__ __forceinline__ void reconstruct(const DevCloud &d, int j, double delx, double dely,
+                                            double delz, double prim[5]) {
+    const double *qj = d.q + 5 * (size_t)j;
+    const double *dqj = d.dq + 15 * (size_t)j;
+    const double *qmj = d.qm + 10 * (size_t)j;
+    const double eps2 = d.eps2[j];
+    double qt[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        const double q = qj[r];
+        const double temp = delx * dqj[3 * r] + dely * dqj[3 * r + 1] + delz * dqj[3 * r + 2];
+        const double del_neg = (q - 0.5 * temp) - q;
+        double phi = 1.0;
+        if (!(fabs(del_neg) <= MF_LIM_EPS)) {
+            const double del_pos = del_neg > 0.0 ? qmj[2 * r] - q : qmj[2 * r + 1] - q;
+            double num = (del_pos * del_pos) + eps2;
+            num = num * del_neg + 2.0 * del_neg * del_neg * del_pos;
+            double den = del_pos * del_pos + 2.0 * del_neg * del_neg;
+            den = den + del_neg * del_pos + eps2;
+            den = den * del_neg;
+            const double t = num / den;
+            phi = (t < 1.0) ? t : 1.0;
+        }
+        qt[r] = q - 0.5 * phi * temp;
+    }
+    qtilde_to_primitive(qt, prim);
+}
+
+// eval_flux_residual (flux_residual.f90:40-81): one warp per point.  Lanes
+// own the point's distinct neighbours: each reconstructs both ends of its
+// pair once and evaluates the flux of every list the neighbour belongs to;
+// then 30 lanes (list, component) sum the list terms in list order and solve
+// the 3x3 least-squares system with the precomputed moments.
+__global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *T = smem + warp * FLUX_SMEM_PER_WARP;     // T[(dir*32 + slot)*5 + c]
+    double *W = T + NDIR * MAX_SLOTS * 5;             // W[slot*3 + axis]
+    for (int p = blockIdx.x * FLUX_WARPS + warp; p < d.n; p += gridDim.x * FLUX_WARPS) {
+        const int cls = d.cls[p];
+        if (cls > 2) continue;
+        const int ns = d.nslot[p];
+        if (lane < ns) {
+            const int k = d.slot_nbr[(size_t)p * MAX_SLOTS + lane];
+            const int mask = d.slot_mask[(size_t)p * MAX_SLOTS + lane];
+            Frame F;
+            load_frame(d.frame + 9 * (size_t)p, F);
+            const double delx = d.x[k] - d.x[p], dely = d.y[k] - d.y[p], delz = d.z[k] - d.z[p];
+            W[lane * 3 + 0] = delx * F.t1[0] + dely * F.t1[1] + delz * F.t1[2];
+            W[lane * 3 + 1] = delx * F.t2[0] + dely * F.t2[1] + delz * F.t2[2];
+            W[lane * 3 + 2] = delx * F.n[0] + dely * F.n[1] + delz * F.n[2];
+            int axes = 0;
+#pragma unroll
+            for (int dd = 0; dd < NDIR; ++dd)
+                if (mask & (1 << dd)) axes |= kind_axes(flux_kind(cls, dd));
+            double prim[5];
+            FluxPre Pi, Pk;
+            AxisTerms Ai[3], Ak[3];
+            reconstruct(d, p, delx, dely, delz, prim);
+            flux_pre(prim, F, Pi);
+            reconstruct(d, k, delx, dely, delz, prim);
+            flux_pre(prim, F, Pk);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (axes & (1 << a)) {
+                    axis_terms(Pi, a, Ai[a]);
+                    axis_terms(Pk, a, Ak[a]);
+                }
+            }
+            for (int dd = 0; dd < NDIR; ++dd) {
+                if (!(mask & (1 << dd))) continue;
+                const int kind = flux_kind(cls, dd);
+#pragma unroll
+                for (int c = 0; c < 5; ++c) {
+                    const double gi = flux_component(kind, c, Pi, Ai);
+                    const double gk = flux_component(kind, c, Pk, Ak);
+                    T[(dd * MAX_SLOTS + lane) * 5 + c] = gk - gi;
+                }
+            }
+        }
+        __syncwarp();
+        double G = 0.0;
+        if (lane < 30) {
+            const int dd = lane / 5, c = lane - 5 * dd;
+            const int cnt = d.list_cnt[(size_t)p * NDIR + dd];
+            const uint8_t *ent = d.list_ent + ((size_t)p * NDIR + dd) * LIST_STRIDE;
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            for (int j = 0; j < cnt; ++j) {
+                const int s = ent[j];
+                const double t = T[(dd * MAX_SLOTS + s) * 5 + c];
+                sx = sx + t * W[s * 3 + 0];
+                sy = sy + t * W[s * 3 + 1];
+                sz = sz + t * W[s * 3 + 2];
+            }
+            const double *g = d.geo + (size_t)p * GEO_STRIDE + dd * 8;
+            const double num = cramer_num(dd >> 1, g, sx, sy, sz);
+            // outer_flux_dG*.f90:118-124 multiply by 1/det; the others divide
+            G = (cls == CLS_OUTER) ? num * (1.0 / g[G_DET]) : num / g[G_DET];
+        }
+        double gd[NDIR];
+#pragma unroll
+        for (int dd = 0; dd < NDIR; ++dd) gd[dd] = __shfl_sync(FULL, G, dd * 5 + (lane % 5));
+        if (lane < 5) {
+            double r;
+            if (cls == CLS_INTERIOR) r = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
+            else if (cls == CLS_WALL) r = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+            else r = gd[0] + gd[1] + gd[2] + gd[3] + gd[4];
+            d.flux_res[5 * (size_t)p + lane] = r;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- D_inv and sweep inputs
+
+// Fluxes of prim in the shared interior frame, all six directions.
+__device__ __forceinline__ void flux6_frame0(const DevCloud &d, const double prim[5], double out[30]) {
+    Frame F;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) { F.t1[r] = d.frame0[r]; F.t2[r] = d.frame0[3 + r]; F.n[r] = d.frame0[6 + r]; }
+    FluxPre P;
+    flux_pre(prim, F, P);
+    AxisTerms A[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) axis_terms(P, a, A[a]);
+#pragma unroll
+    for (int dd = 0; dd < NDIR; ++dd)
+#pragma unroll
+        for (int c = 0; c < 5; ++c) out[dd * 5 + c] = flux_component(dd, c, P, A);
+}
+
+// implicit_D_inv_interior.f90:46-417 / implicit_D_inv_wall.f90:45-356 with
+// the geometry-only sums precomputed; plus the sweep inputs that do not
+// depend on the sweep: G(prim_k) in the shared frame for every point and the
+// published increment G(prim(U_k + dU_k)) - G(prim_k) of points the sweeps
+// never update (outer points, point 1).
+__global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int cls = d.cls[i];
+    const double *p = d.prim + 5 * (size_t)i;
+    if (d.swept[i]) {
+        const double as = sqrt(1.40 * p[4] / p[0]);
+        const double *g = d.geo + (size_t)i * GEO_STRIDE;
+        double gd[NDIR];
+#pragma unroll
+        for (int dd = 0; dd < NDIR; ++dd) {
+            const double u = p[1 + (dd >> 1)];
+            const double temp = g[dd * 8 + G_DNUM], det = g[dd * 8 + G_DET];
+            if ((dd & 1) == 0) {
+                const double t1 = u + as;
+                gd[dd] = 0.50 * fabs(t1 + fabs(t1)) * temp / det;
+            } else {
+                const double t1 = u - as;
+                gd[dd] = -(0.50 * fabs(t1 - fabs(t1)) * temp / det);
+            }
+        }
+        double temp;
+        if (cls == CLS_WALL) temp = (1.0 / d.delt[i]) - 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+        else temp = (1.0 / d.delt[i]) - (gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5]);
+        d.dinv[i] = 1.0 / temp;
+    }
+    if (d.shared_frame) {
+        double prim[5], gold[30];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) prim[r] = p[r];
+        flux6_frame0(d, prim, gold);
+#pragma unroll
+        for (int c = 0; c < 30; ++c) d.gold[30 * (size_t)i + c] = gold[c];
+        if (!d.swept[i]) {
+            double U[5], pn[5], gnew[30];
+            Frame F;
+            load_frame(d.frame + 9 * (size_t)i, F);
+#pragma unroll
+            for (int r = 0; r < 5; ++r) U[r] = d.dUp[5 * (size_t)i + r] + d.U[5 * (size_t)i + r];
+            conserved_to_primitive(U, F, pn);
+            flux6_frame0(d, pn, gnew);
+#pragma unroll
+            for (int c = 0; c < 30; ++c) {
+                const double v = gnew[c] - gold[c];
+                d.dgf[30 * (size_t)i + c] = v;
+                d.dgb[30 * (size_t)i + c] = v;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- LU-SGS sweeps
+
+// One point of the forward (LdelU) or backward (UdelU) sweep, processed by
+// one warp (implicit_forward_and_reverse_sweeps.f90:30-37 / :61-68).
+__device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, double *sm) {
+    const int cls = d.cls[p];
+    const int off = forward ? d.fwd_off[p] : d.bwd_off[p];
+    const uint8_t *cnt = (forward ? d.fwd_cnt : d.bwd_cnt) + (size_t)p * NDIR;
+    const SweepEntry *ent = forward ? d.fwd_ent : d.bwd_ent;
+    const int dd = lane / 5, c = lane - 5 * (lane / 5);
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    if (d.consumer_shared[p]) {
+        // published increments of the neighbours in the shared frame
+        const double *src = forward ? d.dgf : d.dgb;
+        if (lane < 30) {
+            int base = off;
+            for (int e = 0; e < dd; ++e) base += cnt[e];
+            const int m = cnt[dd];
+            for (int j = 0; j < m; ++j) {
+                const SweepEntry &E = ent[base + j];
+                const double t = src[30 * (size_t)E.k + dd * 5 + c];
+                sx = sx + t * E.w[0];
+                sy = sy + t * E.w[1];
+                sz = sz + t * E.w[2];
+            }
+        }
+    } else {
+        // the point's own frame: evaluate G(prim(U_k + dU_k)) - G(prim_k)
+        const double *dsrc = forward ? d.dUp : d.dUn;
+        double *T = sm;               // T[j*5 + c]
+        double *Wm = sm + 32 * 5;     // W[j*3 + a]
+        int total = 0;
+#pragma unroll
+        for (int e = 0; e < NDIR; ++e) total += cnt[e];
+        Frame Fp;
+        load_frame(d.frame + 9 * (size_t)p, Fp);
+        for (int base = 0; base < total; base += 32) {
+            const int j = base + lane;
+            if (j < total) {
+                const SweepEntry &E = ent[off + j];
+                const int k = E.k;
+                const int kind = flux_kind(cls, E.pad);
+                Frame Fk;
+                load_frame(d.frame + 9 * (size_t)k, Fk);
+                double U[5], pn[5], po[5];
+#pragma unroll
+                for (int r = 0; r < 5; ++r) {
+                    U[r] = dsrc[5 * (size_t)k + r] + d.U[5 * (size_t)k + r];
+                    po[r] = d.prim[5 * (size_t)k + r];
+                }
+                conserved_to_primitive(U, Fk, pn);
+                FluxPre Pn, Po;
+                AxisTerms An[3], Ao[3];
+                flux_pre(pn, Fp, Pn);
+                flux_pre(po, Fp, Po);
+                const int axes = kind_axes(kind);
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    if (axes & (1 << a)) { axis_terms(Pn, a, An[a]); axis_terms(Po, a, Ao[a]); }
+#pragma unroll
+                for (int cc = 0; cc < 5; ++cc)
+                    T[(j - base) * 5 + cc] = flux_component(kind, cc, Pn, An) - flux_component(kind, cc, Po, Ao);
+                Wm[(j - base) * 3 + 0] = E.w[0];
+                Wm[(j - base) * 3 + 1] = E.w[1];
+                Wm[(j - base) * 3 + 2] = E.w[2];
+            }
+            __syncwarp();
+            if (lane < 30) {
+                int lo = 0;
+                for (int e = 0; e < dd; ++e) lo += cnt[e];
+                const int hi = lo + cnt[dd];
+                const int a0 = max(lo, base), a1 = min(hi, base + 32);
+                for (int jj = a0; jj < a1; ++jj) {
+                    const double t = T[(jj - base) * 5 + c];
+                    sx = sx + t * Wm[(jj - base) * 3 + 0];
+                    sy = sy + t * Wm[(jj - base) * 3 + 1];
+                    sz = sz + t * Wm[(jj - base) * 3 + 2];
+                }
+            }
+            __syncwarp();
+        }
+    }
+    double G = 0.0;
+    if (lane < 30) {
+        const double *g = d.geo + (size_t)p * GEO_STRIDE + dd * 8;
+        G = cramer_num(dd >> 1, g, sx, sy, sz) / g[G_DET];
+    }
+    double gd[NDIR];
+#pragma unroll
+    for (int e = 0; e < NDIR; ++e) gd[e] = __shfl_sync(FULL, G, e * 5 + (lane % 5));
+    double dnew = 0.0;
+    if (lane < 5) {
+        double lu;
+        if (cls == CLS_WALL) lu = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+        else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
+        const double dinv = d.dinv[p];
+        if (forward) {
+            dnew = -(dinv * (d.flux_res[5 * (size_t)p + lane] + lu));
+            d.dUp[5 * (size_t)p + lane] = dnew;
+        } else {
+            dnew = d.dUp[5 * (size_t)p + lane] - dinv * lu;
+            d.dUn[5 * (size_t)p + lane] = dnew;
+        }
+    }
+    if (d.shared_frame) {
+        // publish this point's increment for the consumers in the shared frame
+        double U[5], pn[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) U[r] = __shfl_sync(FULL, dnew, r) + d.U[5 * (size_t)p + r];
+        if (lane < 30) {
+            Frame Fp;
+            load_frame(d.frame + 9 * (size_t)p, Fp);
+            conserved_to_primitive(U, Fp, pn);
+            Frame F0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) { F0.t1[r] = d.frame0[r]; F0.t2[r] = d.frame0[3 + r]; F0.n[r] = d.frame0[6 + r]; }
+            FluxPre P;
+            flux_pre(pn, F0, P);
+            AxisTerms A[3];
+            const int a = dd >> 1;
+            axis_terms(P, a, A[a]);
+            const double gnew = flux_component(dd, c, P, A);
+            double *dst = forward ? d.dgf : d.dgb;
+            dst[30 * (size_t)p + lane] = gnew - d.gold[30 * (size_t)p + lane];
+        }
+    }
+}
+
+// Level-synchronous sweep in one CTA: the points of a level are independent
+// (none reads another's increment), so warps take them in parallel and a
+// block barrier separates levels.
+__global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(DevCloud d, int forward) {
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *sm = smem + warp * SWEEP_SMEM_PER_WARP;
+    const int nl = forward ? d.n_fwd_levels : d.n_bwd_levels;
+    const int32_t *lptr = forward ? d.fwd_lvl_ptr : d.bwd_lvl_ptr;
+    const int32_t *lpts = forward ? d.fwd_lvl_pts : d.bwd_lvl_pts;
+    for (int l = 0; l < nl; ++l) {
+        const int a = lptr[l], b = lptr[l + 1];
+        for (int idx = a + warp; idx < b; idx += SWEEP_WARPS) sweep_point(d, lpts[idx], forward != 0, lane, sm);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- state update
+
+// state_update_implicit.f90:119-152 + 189-191, then the next iteration's
+// compute_conserved_vector / eval_q_variables into the other U/q buffer.
+__global__ void k_update(DevCloud d, double *U_next, double *q_next) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const int cls = d.cls[i];
+    Frame F;
+    load_frame(d.frame + 9 * (size_t)i, F);
+    double U[5], dn[5], p[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) dn[r] = d.dUn[5 * (size_t)i + r];
+    double res = 0.0;
+    if (cls == CLS_WALL || cls == CLS_INTERIOR) {
+        const double temp = d.U[5 * (size_t)i];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) U[r] = d.U[5 * (size_t)i + r] + dn[r];
+        res = (U[0] - temp) * (U[0] - temp);
+        conserved_to_primitive(U, F, p);
+    } else if (cls == CLS_OUTER) {
+        double pc[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) pc[r] = d.prim[5 * (size_t)i + r];
+        conserved_vector_Ubar(pc, F, d.rho_inf, d.u1_inf, d.u2_inf, d.u3_inf, d.pr_inf, U);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) U[r] = U[r] + dn[r];
+        conserved_to_primitive(U, F, p);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 5; ++r) p[r] = d.prim[5 * (size_t)i + r];
+    }
+    d.res_sqr[i] = res;
+    double Un[5], qn[5];
+    primitive_to_rotated_conserved(p, F, Un);
+    primitive_to_q(p, qn);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        d.prim[5 * (size_t)i + r] = p[r];
+        d.dUp[5 * (size_t)i + r] = dn[r];
+        U_next[5 * (size_t)i + r] = Un[r];
+        q_next[5 * (size_t)i + r] = qn[r];
+    }
+}
+
+// res_new = sqrt(sum over wall, interior of (dU1)^2) / N
+// (state_update_implicit.f90:124-129, 187).  Fixed two-pass tree order, so
+// the value is deterministic; it differs from the reference's left-to-right
+// sum only by summation rounding.
+__global__ void k_reduce_partial(DevCloud d) {
+    __shared__ double s[RED_THREADS];
+    const int per = (d.n_res + gridDim.x - 1) / gridDim.x;
+    const int a = blockIdx.x * per, b = min(d.n_res, a + per);
+    double acc = 0.0;
+    for (int j = a + threadIdx.x; j < b; j += RED_THREADS) acc += d.res_sqr[d.res_order[j]];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) d.partial[blockIdx.x] = s[0];
+}
+
+__global__ void k_reduce_final(DevCloud d, int nblocks, int slot) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double acc = 0.0;
+    for (int b = 0; b < nblocks; ++b) acc += d.partial[b];
+    d.res_dev[slot] = sqrt(acc) / (double)d.n;
+}
+
+// ---------------------------------------------------------------- launchers
+
+int reduction_blocks(int n) {
+    int b = (n + 4095) / 4096;
+    return b < 1 ? 1 : (b > 1024 ? 1024 : b);
+}
+
+cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s) {
+    k_conserved_q<<<(d.n + 127) / 128, 128, 0, s>>>(d);
+    return cudaGetLastError();
+}
+
+static bool g_attr_set = false;
+
+cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
+                             double *U_next, double *q_next, cudaEvent_t *ev) {
+    const int n = d.n;
+    if (!g_attr_set) {
+        cudaFuncSetAttribute(k_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
+        cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SWEEP_WARPS * SWEEP_SMEM_PER_WARP * 8);
+        g_attr_set = true;
+    }
+    auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
+    mark(0);
+    k_qderiv<<<(n + 127) / 128, 128, 0, s>>>(d);
+    mark(1);
+    const int fblocks = (n + FLUX_WARPS - 1) / FLUX_WARPS;
+    k_flux<<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
+    mark(2);
+    k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);
+    mark(3);
+    k_sweep<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_PER_WARP * 8, s>>>(d, 1);
+    mark(4);
+    k_sweep<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_PER_WARP * 8, s>>>(d, 0);
+    mark(5);
+    k_update<<<(n + 127) / 128, 128, 0, s>>>(d, U_next, q_next);
+    mark(6);
+    const int rb = reduction_blocks(d.n_res);
+    k_reduce_partial<<<rb, RED_THREADS, 0, s>>>(d);
+    k_reduce_final<<<1, 32, 0, s>>>(d, rb, iter_slot);
+    mark(7);
+    return cudaGetLastError();
+}
+
+}  // namespace mfcfd

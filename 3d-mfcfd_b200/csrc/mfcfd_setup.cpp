@@ -1,0 +1,376 @@
+/*
+ * mfcfd_setup.cpp - one-time host set-up of a point cloud.
+ *
+ * Builds, from the reference's input arrays:
+ *   - the six split stencils of every point with the reference's storage
+ *     (generate_connectivity.f90:12-246), including its fixed capacity of 22
+ *     entries per list (data_structure.f90:83-88): a list that grows past the
+ *     capacity continues into the next point's column of the same
+ *     column-major array, as unchecked Fortran indexing does, and later reads
+ *     see whatever that column holds after all writes;
+ *   - the sweep order from the alias breadth-first search
+ *     (implicit_aliasing.f90:13-44) with its quirks (the first neighbour of
+ *     point 1 also receives alias 1; point_with_alias(N) stays 0);
+ *   - the "effective" neighbour lists each routine actually reads (the wall
+ *     z- terms use the full conn, wall_flux_dGzneg.f90:61-65,
+ *     implicit_D_inv_wall.f90:309-310), compacted into at most 32 distinct
+ *     neighbour slots per point for the warp-per-point flux kernel;
+ *   - the per-list least-squares moments, determinant and D_inv numerator,
+ *     which depend on geometry only (implicit_D_inv_interior.f90:63-105);
+ *   - the level schedules of the forward and backward LU-SGS sweeps: a point's
+ *     level is one more than the deepest level among the neighbours whose
+ *     increments it reads (lower alias forward, higher alias backward), so
+ *     every level can be processed in parallel and the result equals the
+ *     reference's sequential sweep bit for bit.
+ * All floating-point work here is compiled without contraction so the
+ * values equal those the reference computes inline.
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "mfcfd_internal.h"
+
+namespace mfcfd {
+
+namespace {
+
+struct Moments { double xx, yy, zz, xy, yz, zx; };
+
+inline double det_of(const Moments &m) {
+    return m.xx * (m.yy * m.zz - m.yz * m.yz)
+         - m.xy * (m.xy * m.zz - m.yz * m.zx)
+         + m.zx * (m.xy * m.yz - m.yy * m.zx);
+}
+
+// Cramer numerators, in the reference's operand order
+// (implicit_D_inv_interior.f90:103-105, :225-227, :347-349).
+inline double numerator(int axis, const Moments &m, double fx, double fy, double fz) {
+    if (axis == 0)
+        return fx * (m.yy * m.zz - m.yz * m.yz) - fy * (m.xy * m.zz - m.zx * m.yz)
+             + fz * (m.xy * m.yz - m.zx * m.yy);
+    if (axis == 1)
+        return m.xx * (fy * m.zz - m.yz * fz) - m.xy * (fx * m.zz - m.zx * fz)
+             + m.zx * (fx * m.yz - m.zx * fy);
+    return m.xx * (m.yy * fz - fy * m.yz) - m.xy * (m.xy * fz - fx * m.yz)
+         + m.zx * (m.xy * fy - fx * m.yy);
+}
+
+}  // namespace
+
+int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
+                   const double *y, const double *z, const double *tan1, const double *tan2,
+                   const double *nor, const int32_t *nbhs, const int32_t *conn,
+                   const double *min_dist, Topology &T, std::string &err) {
+    T.n = n;
+    T.cap = P.split_capacity > 0 ? P.split_capacity : MAX_CONN;
+    const int cap = T.cap;
+    T.cls.assign(n, CLS_OTHER);
+    for (int i = 0; i < n; ++i) {
+        if (nbhs[i] < 0 || nbhs[i] > MAX_CONN) {
+            err = "nbhs out of range [0,27] at point " + std::to_string(i + 1);
+            return MFCFD_ERR_ARG;
+        }
+        for (int r = 0; r < nbhs[i]; ++r) {
+            int k = conn[(size_t)i * MAX_CONN + r];
+            if (k < 1 || k > n) {
+                err = "conn entry out of range at point " + std::to_string(i + 1);
+                return MFCFD_ERR_ARG;
+            }
+        }
+        switch (status[i]) {
+        case 0: T.cls[i] = CLS_INTERIOR; T.interior_idx.push_back(i); break;
+        case 1: T.cls[i] = CLS_WALL; T.wall_idx.push_back(i); break;
+        case 2: T.cls[i] = CLS_OUTER; T.outer_idx.push_back(i); break;
+        case 5: case 6:
+            err = "supersonic inlet/outlet points (status 5/6) are not supported";
+            return MFCFD_ERR_UNSUPPORTED;
+        default:
+            err = "unknown point status " + std::to_string(status[i]);
+            return MFCFD_ERR_ARG;
+        }
+    }
+
+    // ---- split stencils with the reference's storage (generate_connectivity.f90)
+    const size_t flat = (size_t)n * cap + 64;
+    for (int d = 0; d < NDIR; ++d) {
+        T.split[d].assign(flat, 0);
+        T.split_cnt[d].assign(n, 0);
+    }
+    T.split_overflows = 0;
+    auto push = [&](int d, int i, int k) {   // i 0-based point, k 1-based id
+        int c = ++T.split_cnt[d][i];
+        if (c > cap) T.split_overflows++;
+        T.split[d][(size_t)i * cap + (c - 1)] = k;
+    };
+    auto classify = [&](int i, int cls) {
+        const double xi = x[i], yi = y[i], zi = z[i];
+        const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
+        // counts reset as the reference does (outer points leave zpos alone)
+        T.split_cnt[0][i] = 0; T.split_cnt[1][i] = 0; T.split_cnt[2][i] = 0;
+        T.split_cnt[3][i] = 0; T.split_cnt[5][i] = 0;
+        if (cls == CLS_INTERIOR) T.split_cnt[4][i] = 0;
+        for (int r = 0; r < nbhs[i]; ++r) {
+            int k = conn[(size_t)i * MAX_CONN + r];
+            double delx = x[k - 1] - xi, dely = y[k - 1] - yi, delz = z[k - 1] - zi;
+            double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+            double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+            if (cls == CLS_INTERIOR) {
+                double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                if (dels <= 0.0) push(0, i, k);
+                if (dels > 0.0) push(1, i, k);
+                if (delt <= 0.0) push(2, i, k);
+                if (delt > 0.0) push(3, i, k);
+                if (deln <= 0.0) push(4, i, k);
+                if (deln > 0.0) push(5, i, k);
+            } else {
+                if (dels <= 0.0) push(0, i, k);
+                if (dels >= 0.0) push(1, i, k);
+                if (delt <= 0.0) push(2, i, k);
+                if (delt >= 0.0) push(3, i, k);
+                push(cls == CLS_WALL ? 5 : 4, i, k);
+            }
+        }
+    };
+    for (int i : T.interior_idx) classify(i, CLS_INTERIOR);
+    for (int i : T.wall_idx) classify(i, CLS_WALL);
+    for (int i : T.outer_idx) classify(i, CLS_OUTER);
+
+    // ---- alias breadth-first search (implicit_aliasing.f90:21-42).
+    // Index 0 of the 1-based arrays is a zero guard: point_with_alias(i) = 0
+    // makes the inner loop run over nbhs(0) = 0 neighbours.
+    std::vector<int32_t> alias1(n + 1, 0), pwa1(n + 1, 0);
+    alias1[1] = 1;
+    pwa1[1] = 1;
+    int count = 0;
+    for (int i = 1; i <= n; ++i) {
+        int p = pwa1[i];
+        int nb = p > 0 ? nbhs[p - 1] : 0;
+        for (int j = 0; j < nb; ++j) {
+            int k = conn[(size_t)(p - 1) * MAX_CONN + j];
+            if (alias1[k] == 0) {
+                count = count + 1;
+                alias1[k] = count;
+                pwa1[count] = k;
+            }
+        }
+    }
+    T.alias.assign(alias1.begin() + 1, alias1.end());
+    T.point_with_alias.assign(pwa1.begin() + 1, pwa1.end());
+
+    // ---- effective lists and neighbour slots
+    T.slot_nbr.assign((size_t)n * MAX_SLOTS, -1);
+    T.nslot.assign(n, 0);
+    T.slot_mask.assign((size_t)n * MAX_SLOTS, 0);
+    T.list_cnt.assign((size_t)n * NDIR, 0);
+    T.list_ent.assign((size_t)n * NDIR * LIST_STRIDE, 0);
+    std::vector<int> eff[NDIR];
+    auto effective = [&](int i, int d, std::vector<int> &out) {   // 0-based ids
+        out.clear();
+        int cls = T.cls[i];
+        bool use_conn = (cls == CLS_WALL && d == 5);
+        bool unused = (cls == CLS_WALL && d == 4) || (cls == CLS_OUTER && d == 5) || cls == CLS_OTHER;
+        if (unused) return true;
+        if (use_conn) {
+            for (int r = 0; r < nbhs[i]; ++r) out.push_back(conn[(size_t)i * MAX_CONN + r] - 1);
+            return true;
+        }
+        int c = T.split_cnt[d][i];
+        for (int j = 0; j < c; ++j) {
+            int k = T.split[d][(size_t)i * cap + j];
+            if (k < 1 || k > n) return false;
+            out.push_back(k - 1);
+        }
+        return true;
+    };
+    for (int i = 0; i < n; ++i) {
+        int32_t *slots = &T.slot_nbr[(size_t)i * MAX_SLOTS];
+        int ns = 0;
+        auto slot_of = [&](int k) -> int {
+            for (int s = 0; s < ns; ++s) if (slots[s] == k) return s;
+            if (ns == MAX_SLOTS) return -1;
+            slots[ns] = k;
+            return ns++;
+        };
+        for (int r = 0; r < nbhs[i]; ++r) slot_of(conn[(size_t)i * MAX_CONN + r] - 1);
+        for (int d = 0; d < NDIR; ++d) {
+            if (!effective(i, d, eff[d])) {
+                err = "split list of point " + std::to_string(i + 1) + " names point 0";
+                return MFCFD_ERR_STENCIL;
+            }
+            if (eff[d].size() > (size_t)MAX_CONN) {
+                err = "split list longer than 27 at point " + std::to_string(i + 1);
+                return MFCFD_ERR_STENCIL;
+            }
+            T.list_cnt[(size_t)i * NDIR + d] = (uint8_t)eff[d].size();
+            for (size_t j = 0; j < eff[d].size(); ++j) {
+                int s = slot_of(eff[d][j]);
+                if (s < 0) {
+                    err = "more than 32 distinct stencil neighbours at point " + std::to_string(i + 1);
+                    return MFCFD_ERR_STENCIL;
+                }
+                T.list_ent[((size_t)i * NDIR + d) * LIST_STRIDE + j] = (uint8_t)s;
+                T.slot_mask[(size_t)i * MAX_SLOTS + s] |= (uint8_t)(1u << d);
+            }
+        }
+        T.nslot[i] = (uint8_t)ns;
+    }
+
+    // ---- geometry per (point, list): moments, determinant, D_inv numerator
+    T.geo.assign((size_t)n * GEO_STRIDE, 0.0);
+    auto weights_of = [&](double dist) { return 1.0 / std::pow(dist, P.power); };
+    for (int i = 0; i < n; ++i) {
+        const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
+        for (int d = 0; d < NDIR; ++d) {
+            int c = T.list_cnt[(size_t)i * NDIR + d];
+            Moments m = {0, 0, 0, 0, 0, 0};
+            double sdx = 0, sdy = 0, sdz = 0;
+            for (int j = 0; j < c; ++j) {
+                int s = T.list_ent[((size_t)i * NDIR + d) * LIST_STRIDE + j];
+                int k = T.slot_nbr[(size_t)i * MAX_SLOTS + s];
+                double delx = x[k] - x[i], dely = y[k] - y[i], delz = z[k] - z[i];
+                double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+                double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+                double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                double dist = std::sqrt(dels * dels + delt * delt + deln * deln);
+                double w = weights_of(dist);
+                double ws = dels * w, wt = delt * w, wn = deln * w;
+                m.xx = m.xx + dels * ws;
+                m.yy = m.yy + delt * wt;
+                m.zz = m.zz + deln * wn;
+                m.xy = m.xy + dels * wt;
+                m.yz = m.yz + delt * wn;
+                m.zx = m.zx + deln * ws;
+                sdx = sdx + ws;
+                sdy = sdy + wt;
+                sdz = sdz + wn;
+            }
+            double *g = &T.geo[(size_t)i * GEO_STRIDE + d * 8];
+            g[G_XX] = m.xx; g[G_YY] = m.yy; g[G_ZZ] = m.zz;
+            g[G_XY] = m.xy; g[G_YZ] = m.yz; g[G_ZX] = m.zx;
+            g[G_DET] = det_of(m);
+            g[G_DNUM] = numerator(d / 2, m, sdx, sdy, sdz);
+        }
+    }
+
+    // limiter epsilon: (VL_CONST*min_dist)**3 squared (limiters.f90:251-253)
+    T.eps2.resize(n);
+    for (int i = 0; i < n; ++i) {
+        double e = P.vl_const * min_dist[i];
+        e = std::pow(e, 3.0);
+        T.eps2[i] = e * e;
+    }
+
+    // ---- sweep schedules (implicit_forward_and_reverse_sweeps.f90:26-84)
+    T.swept.assign(n, 0);
+    std::vector<int> order;   // swept points in forward order (0-based)
+    for (int i = 0; i < n; ++i) {
+        int p = T.point_with_alias[i];
+        if (p == 0) continue;   // the reference's out-of-range entry
+        int cls = T.cls[p - 1];
+        if (cls == CLS_WALL || cls == CLS_INTERIOR) {
+            T.swept[p - 1] = 1;
+            order.push_back(p - 1);
+        }
+    }
+    auto al = [&](int k) { return T.alias[k]; };
+    auto build = [&](bool forward, std::vector<int32_t> &level, std::vector<int32_t> &lptr,
+                     std::vector<int32_t> &lpts, std::vector<int32_t> &off,
+                     std::vector<uint8_t> &cnt, std::vector<SweepEntry> &ent) {
+        level.assign(n, -1);
+        off.assign(n + 1, 0);
+        cnt.assign((size_t)n * NDIR, 0);
+        ent.clear();
+        // entries first (in point index order of the offsets)
+        std::vector<std::vector<SweepEntry>> per(n);
+        for (int p : order) {
+            const double *t1 = tan1 + 3 * (size_t)p, *t2 = tan2 + 3 * (size_t)p, *nn = nor + 3 * (size_t)p;
+            for (int d = 0; d < NDIR; ++d) {
+                int c = T.list_cnt[(size_t)p * NDIR + d];
+                int taken = 0;
+                for (int j = 0; j < c; ++j) {
+                    int s = T.list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
+                    int k = T.slot_nbr[(size_t)p * MAX_SLOTS + s];
+                    bool take = forward ? (al(k) < al(p)) : (al(k) > al(p));
+                    if (!take) continue;
+                    double delx = x[k] - x[p], dely = y[k] - y[p], delz = z[k] - z[p];
+                    double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+                    double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+                    double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                    double dist = std::sqrt(dels * dels + delt * delt + deln * deln);
+                    double w = weights_of(dist);
+                    SweepEntry e;
+                    e.k = k;
+                    e.pad = d;
+                    e.w[0] = dels * w; e.w[1] = delt * w; e.w[2] = deln * w;
+                    per[p].push_back(e);
+                    ++taken;
+                }
+                cnt[(size_t)p * NDIR + d] = (uint8_t)taken;
+            }
+        }
+        for (int p = 0; p < n; ++p) {
+            off[p] = (int32_t)ent.size();
+            ent.insert(ent.end(), per[p].begin(), per[p].end());
+        }
+        off[n] = (int32_t)ent.size();
+        // levels: longest path over swept dependencies
+        int maxl = -1;
+        auto visit = [&](int p) {
+            int lv = 0;
+            for (int e = off[p]; e < off[p + 1]; ++e) {
+                int k = ent[e].k;
+                if (T.swept[k] && level[k] + 1 > lv) lv = level[k] + 1;
+            }
+            level[p] = lv;
+            maxl = std::max(maxl, lv);
+        };
+        if (forward) for (int p : order) visit(p);
+        else for (auto it = order.rbegin(); it != order.rend(); ++it) visit(*it);
+        int nl = maxl + 1;
+        lptr.assign(nl + 1, 0);
+        for (int p : order) lptr[level[p] + 1]++;
+        for (int l = 0; l < nl; ++l) {
+            lptr[l + 1] += lptr[l];
+            T.max_level_width = std::max(T.max_level_width, lptr[l + 1] - lptr[l]);
+        }
+        lpts.assign(order.size(), 0);
+        std::vector<int32_t> fill(lptr.begin(), lptr.end() - 1);
+        if (forward) for (int p : order) lpts[fill[level[p]]++] = p;
+        else for (auto it = order.rbegin(); it != order.rend(); ++it) lpts[fill[level[*it]]++] = *it;
+    };
+    build(true, T.fwd_level, T.fwd_lvl_ptr, T.fwd_lvl_pts, T.fwd_off, T.fwd_cnt, T.fwd_ent);
+    build(false, T.bwd_level, T.bwd_lvl_ptr, T.bwd_lvl_pts, T.bwd_off, T.bwd_cnt, T.bwd_ent);
+
+    // ---- shared interior frame: lets producers publish flux increments
+    T.shared_frame = 0;
+    if (!T.interior_idx.empty()) {
+        int i0 = T.interior_idx[0];
+        double f0[9];
+        for (int r = 0; r < 3; ++r) {
+            f0[r] = tan1[3 * (size_t)i0 + r];
+            f0[3 + r] = tan2[3 * (size_t)i0 + r];
+            f0[6 + r] = nor[3 * (size_t)i0 + r];
+        }
+        bool same = true;
+        for (int i : T.interior_idx) {
+            for (int r = 0; r < 3 && same; ++r) {
+                if (std::memcmp(&tan1[3 * (size_t)i + r], &f0[r], 8) ||
+                    std::memcmp(&tan2[3 * (size_t)i + r], &f0[3 + r], 8) ||
+                    std::memcmp(&nor[3 * (size_t)i + r], &f0[6 + r], 8))
+                    same = false;
+            }
+            if (!same) break;
+        }
+        if (same) {
+            T.shared_frame = 1;
+            std::memcpy(T.frame0, f0, sizeof f0);
+        }
+    }
+    T.consumer_shared.assign(n, 0);
+    for (int i = 0; i < n; ++i)
+        T.consumer_shared[i] = (T.swept[i] && T.cls[i] == CLS_INTERIOR && T.shared_frame) ? 1 : 0;
+    return MFCFD_OK;
+}
+
+}  // namespace mfcfd

@@ -1,0 +1,100 @@
+"""ctypes binding of the C ABI in include/mfcfd.h (libmfcfd.so, built in-tree)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmfcfd.so")
+
+MFCFD_OK = 0
+ERRORS = {1: "bad argument", 2: "CUDA error", 3: "stencil too wide",
+          4: "singular least-squares system", 5: "non-finite residual",
+          6: "unsupported input", 7: "out of device memory", 8: "device wait timed out"}
+
+FIELD_PRIM, FIELD_U, FIELD_Q, FIELD_QM, FIELD_DQ, FIELD_DELT, FIELD_FLUX_RES, \
+    FIELD_DELUP, FIELD_DELUN, FIELD_DINV = range(10)
+FIELD_WIDTH = {FIELD_PRIM: 5, FIELD_U: 5, FIELD_Q: 5, FIELD_QM: 10, FIELD_DQ: 15,
+               FIELD_DELT: 1, FIELD_FLUX_RES: 5, FIELD_DELUP: 5, FIELD_DELUN: 5,
+               FIELD_DINV: 1}
+
+# Every symbol include/mfcfd.h declares.
+EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_step",
+           "mfcfd_run", "mfcfd_get", "mfcfd_get_state", "mfcfd_set_state",
+           "mfcfd_get_stencils", "mfcfd_get_alias", "mfcfd_get_levels", "mfcfd_get_info",
+           "mfcfd_get_stream", "mfcfd_set_profiling", "mfcfd_get_phase_times",
+           "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
+NPHASE = 7
+PHASES = ("qderiv", "flux", "dinv", "sweep_fwd", "sweep_bwd", "update", "residual")
+
+
+class Params(ctypes.Structure):
+    """mfcfd_params (include/mfcfd.h)."""
+    _fields_ = [("power", ctypes.c_double), ("vl_const", ctypes.c_double),
+                ("cfl", ctypes.c_double), ("rho_inf", ctypes.c_double),
+                ("u1_inf", ctypes.c_double), ("u2_inf", ctypes.c_double),
+                ("u3_inf", ctypes.c_double), ("pr_inf", ctypes.c_double),
+                ("inner_iterations", ctypes.c_int32), ("split_capacity", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 8)]
+
+
+class Info(ctypes.Structure):
+    """mfcfd_info (include/mfcfd.h)."""
+    _fields_ = [("n_points", ctypes.c_int32), ("n_wall", ctypes.c_int32),
+                ("n_outer", ctypes.c_int32), ("n_interior", ctypes.c_int32),
+                ("n_supersonic", ctypes.c_int32), ("n_levels_forward", ctypes.c_int32),
+                ("n_levels_backward", ctypes.c_int32), ("max_level_width", ctypes.c_int32),
+                ("split_overflows", ctypes.c_int32), ("shared_frame", ctypes.c_int32),
+                ("device_bytes", ctypes.c_int64)]
+
+
+class MfcfdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mfcfd error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libmfcfd.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C 3d-mfcfd_b200` "
+                          "or __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double
+    L.mfcfd_params_init.argtypes = [ctypes.POINTER(Params), dbl, dbl]
+    L.mfcfd_params_init.restype = None
+    L.mfcfd_create.argtypes = [ctypes.POINTER(Params), i32] + [vp] * 10 + [ctypes.POINTER(vp)]
+    L.mfcfd_set_prim.argtypes = [vp, vp]
+    L.mfcfd_fpi_step.argtypes = [vp, i32, vp, vp]
+    L.mfcfd_run.argtypes = [vp, i32, i32, vp]
+    L.mfcfd_get.argtypes = [vp, i32, vp]
+    L.mfcfd_get_state.argtypes = [vp, vp, vp, vp]
+    L.mfcfd_set_state.argtypes = [vp, vp, vp, dbl]
+    L.mfcfd_get_stencils.argtypes = [vp, vp, vp, i32]
+    L.mfcfd_get_alias.argtypes = [vp, vp, vp]
+    L.mfcfd_get_levels.argtypes = [vp, i32, vp]
+    L.mfcfd_get_info.argtypes = [vp, ctypes.POINTER(Info)]
+    L.mfcfd_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.mfcfd_set_profiling.argtypes = [vp, i32]
+    L.mfcfd_get_phase_times.argtypes = [vp, vp, vp]
+    L.mfcfd_destroy.argtypes = [vp]
+    L.mfcfd_last_error.argtypes = [vp]
+    L.mfcfd_last_error.restype = ctypes.c_char_p
+    L.mfcfd_strerror.argtypes = [ctypes.c_int]
+    L.mfcfd_strerror.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        if name not in ("mfcfd_params_init", "mfcfd_last_error", "mfcfd_strerror"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)

@@ -1,0 +1,309 @@
+"""Benchmark: FP64 point-iterations/s of the implicit q-LSKUM iteration.
+
+A step is one ``fpi_solver`` iteration (all seven phases) over one point
+cloud resident on the GPU.  The default workload is the 1.1M-point sphere
+(96 shells x 11,500 points, 1% jitter, M = 0.8, alpha = 2 deg, FP64); the
+cloud is seeded synthetic data from the package generator.  Its state
+(~1.5 GB) is larger than the 126 MB L2, so no flush is needed between steps.
+
+``value``    device-timed throughput with the state resident in HBM
+             (CUDA events on the library's stream, max over ranks).
+``e2e``      the same metric through the C ABI with host buffers: every step
+             copies prim and delU in from pinned host memory (mfcfd_set_state),
+             iterates (mfcfd_fpi_step) and copies them back (mfcfd_get_state).
+``roofline`` the dominant phase's algorithmic bytes (per point, from the
+             byte model of each phase) over its event-timed duration.
+Multi-GPU: independent replicas, one per rank (the LU-SGS sweep order is
+global, so one cloud does not shard); value sums the ranks' points.
+
+``--impl reference`` times the CPU oracle (the reference's algorithm restated
+in C++, glibc libm) instead: one independent solve per host core on a 62,400
+point sphere sample, one iteration per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "3d-mfcfd_b200")
+for _p in (PKG, REPO):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+# Algorithmic bytes per point-iteration of each phase (FP64 SoA model: own
+# point inputs read once, outputs written once, neighbour gathers counted as
+# cache hits; 26-neighbour interior point).
+PHASE_BYTES = {"qderiv": 372 + 180, "flux": 724, "dinv": 488, "sweep_fwd": 608,
+               "sweep_bwd": 608, "update": 196, "residual": 8}
+TOTAL_BYTES = 3368
+
+WORKLOADS = {
+    "sphere-1.1M": dict(shells=96, per_shell=11500, jitter=0.01, mach=0.8, aoa=2.0, seed=2001),
+    "sphere-62k": dict(shells=48, per_shell=1300, jitter=0.02, mach=0.4, aoa=0.0, seed=1001),
+}
+KERNELS_PER_ITER = 8
+
+
+def load_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+# ------------------------------------------------------------------ CPU side
+
+def _oracle_worker(args):
+    """One independent oracle solve (spawned process): time `steps` iterations."""
+    sys.path.insert(0, PKG)
+    sys.path.insert(0, REPO)
+    from mfcfd import cloud
+    from oracle import oracle
+    shells, per_shell, jitter, mach, aoa, seed, warm, steps = args
+    c = cloud.shell_cloud(shells, per_shell, jitter=jitter, seed=seed)
+    o = oracle.Oracle(c, mach, aoa, libm=oracle.LIBM_GLIBC)
+    o.set_prim(cloud.initial_state(c, mach, aoa))
+    for t in range(1, warm + 1):
+        o.step(t)
+    t0 = time.perf_counter()
+    for t in range(warm + 1, warm + steps + 1):
+        o.step(t)
+    return c.n, steps, time.perf_counter() - t0
+
+
+def cpu_reference(procs, warm, steps, mach, aoa):
+    """Throughput of the CPU oracle: `procs` independent 62,400-point solves."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    job = (48, 1300, 0.02, mach, aoa, 1001, warm, steps)
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_oracle_worker, [job] * procs)
+    n = res[0][0]
+    wall = max(r[2] for r in res)
+    return procs * n * steps / wall, wall / steps, n
+
+
+# ------------------------------------------------------------------ main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mfcfd", choices=["mfcfd", "reference"])
+    ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local_rank = dist_env()
+    wl = WORKLOADS[args.workload]
+    metric = "point-iters/s FP64"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        procs = max(1, min(os.cpu_count() or 1, 32))
+        value, sec_per_step, n = cpu_reference(procs, args.warmup, args.steps, wl["mach"], wl["aoa"])
+        sample = (f"CPU oracle (the reference's algorithm restated in C++, glibc libm, "
+                  f"-O2 -ffp-contract=off), {procs} independent solves of a {n}-point sphere "
+                  f"(M={wl['mach']}, alpha={wl['aoa']}), one iteration per step")
+        line = {"metric": metric, "value": value, "unit": "point-iters/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_step * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": args.workload, "sample_points": n},
+                "cpu_baseline": {"value": value, "unit": "point-iters/s", "cores": procs,
+                                 "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": "point-iters/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from mfcfd import cloud as cl
+    from mfcfd.solver import Solver
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    c = cl.shell_cloud(wl["shells"], wl["per_shell"], jitter=wl["jitter"], seed=wl["seed"] + rank)
+    s = Solver(c, wl["mach"], wl["aoa"], device=local_rank)
+    prim0 = cl.initial_state(c, wl["mach"], wl["aoa"])
+    s.initial_conditions(prim0)
+    info = s.info()
+    stream = torch.cuda.ExternalStream(s.stream())
+
+    # warm-up
+    t = 1
+    s.q_lskum(args.warmup, t0=t)
+    t += args.warmup
+    torch.cuda.synchronize()
+
+    # timed region: device events on the library's stream
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.q_lskum(args.steps, t0=t)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    t += args.steps
+    ms = e0.elapsed_time(e1)
+    ms_t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * c.n * args.steps / (ms_max / 1e3)
+
+    # phase timing (separate pass, same workload) for the roofline
+    s.set_profiling(True)
+    s.q_lskum(args.steps, t0=t)
+    t += args.steps
+    phases, piters = s.phase_times()
+    s.set_profiling(False)
+    dom = max(phases, key=lambda k: phases[k])
+    dom_ms = phases[dom] / max(piters, 1)
+    peak, peak_kind = load_peaks()
+    achieved = PHASE_BYTES[dom] * c.n / (dom_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "kernel": dom,
+                "peak_source": peak_kind,
+                "phase_ms_per_iter": {k: v / max(piters, 1) for k, v in phases.items()},
+                "iteration_bytes_model": TOTAL_BYTES}
+
+    # end to end through the C ABI with pinned host buffers
+    prim_h = torch.empty((c.n, 5), dtype=torch.float64, pin_memory=True).numpy()
+    delu_h = torch.empty((c.n, 5), dtype=torch.float64, pin_memory=True).numpy()
+    p_, d_, ro = s.get_state()
+    prim_h[:] = p_
+    delu_h[:] = d_
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for k in range(args.steps):
+        s.set_state(prim_h, delu_h, ro)
+        s.fpi_solver(t + k)
+        p_, d_, ro = None, None, None
+        prim_out, delu_out, ro = s.get_state()
+        prim_h[:] = prim_out
+        delu_h[:] = delu_out
+    torch.cuda.synchronize()
+    w1 = time.perf_counter()
+    e2e_s = w1 - w0
+    e2e_t = torch.tensor([e2e_s], device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * c.n * args.steps / float(e2e_t.item())
+    io_bytes = c.n * 5 * 8 * 2
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sps, n = cpu_reference(1, 0, 3, wl["mach"], wl["aoa"])
+        cpu_base = {"value": v, "unit": "point-iters/s", "cores": 1, "kind": "port",
+                    "sample": f"CPU oracle (C++ restatement, glibc libm), one solve of a {n}-point "
+                              f"sphere (M={wl['mach']}, alpha={wl['aoa']}), 3 iterations, 1 thread"}
+
+    if rank == 0:
+        line = {"metric": metric, "value": value, "unit": "point-iters/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded sphere-shell generator)",
+                "config": {"workload": args.workload, "points": c.n, "mach": wl["mach"],
+                           "alpha_deg": wl["aoa"], "precision": "fp64",
+                           "levels_forward": info["n_levels_forward"],
+                           "levels_backward": info["n_levels_backward"],
+                           "l2": "state larger than L2 (no flush)",
+                           "parallelism": f"replicas x{world}"},
+                "e2e": {"value": e2e_value, "unit": "point-iters/s",
+                        "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+                "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks,
+                "gpu_launches": KERNELS_PER_ITER * args.steps}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/*
+ * mfcfd.h - C ABI of the B200 q-LSKUM implicit iteration.
+ *
+ * The reference (a serial Fortran 90 meshfree Euler solver) keeps its point
+ * cloud in a module global (``type(points) :: point``, data_structure.f90:
+ * 7-59) and calls argument-less routines on it.  The solver loop is
+ *
+ *     call generate_split_stencils()          q_lskum.f90:25
+ *     call aliasing()                         q_lskum.f90:26
+ *     do t = 1, max_iters
+ *         call fpi_solver(t)                  q_lskum.f90:29
+ *     enddo
+ *
+ * This header is the drop-in boundary for that loop: the Fortran host keeps
+ * its arrays and passes them by pointer; the library copies them to the GPU
+ * once, keeps all iteration state resident there, and replaces each
+ * ``call fpi_solver(t)`` with ``mfcfd_fpi_step(h, t, &res_new, &residue)``.
+ *
+ * Conventions
+ *   - Arrays use the reference's Fortran layout: an array declared
+ *     ``A(m, N)`` is passed as m*N contiguous values with the m entries of a
+ *     point adjacent (column-major).  ``conn`` holds 1-based point indices.
+ *   - Every entry point returns an int status (MFCFD_OK = 0).  No exception,
+ *     exit, trap or abort crosses the boundary; ``mfcfd_last_error`` gives a
+ *     message for the last failure on a handle.
+ *   - A handle is not thread safe; separate handles may be used from
+ *     separate host threads.  Each handle owns one CUDA stream.
+ */
+#ifndef MFCFD_H
+#define MFCFD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MFCFD_OK               0
+#define MFCFD_ERR_ARG          1   /* bad argument (null pointer, size, index) */
+#define MFCFD_ERR_CUDA         2   /* CUDA runtime failure */
+#define MFCFD_ERR_STENCIL      3   /* a stencil exceeds the supported width */
+#define MFCFD_ERR_SINGULAR     4   /* a least-squares determinant is zero */
+#define MFCFD_ERR_NONFINITE    5   /* the density residual is not finite */
+#define MFCFD_ERR_UNSUPPORTED  6   /* input the library does not handle */
+#define MFCFD_ERR_NOMEM        7   /* device allocation failed */
+#define MFCFD_ERR_TIMEOUT      8   /* a bounded device wait ran out */
+
+/* fields for mfcfd_get / mfcfd_set_field (Fortran layout, width x N) */
+#define MFCFD_FIELD_PRIM      0    /* point%prim(5,N)        width 5  */
+#define MFCFD_FIELD_U         1    /* point%U(5,N)           width 5  */
+#define MFCFD_FIELD_Q         2    /* point%q(5,N)           width 5  */
+#define MFCFD_FIELD_QM        3    /* point%qm(2,5,N)        width 10 */
+#define MFCFD_FIELD_DQ        4    /* point%dq(3,5,N)        width 15 */
+#define MFCFD_FIELD_DELT      5    /* point%delt(N)          width 1  */
+#define MFCFD_FIELD_FLUX_RES  6    /* point%flux_res(5,N)    width 5  */
+#define MFCFD_FIELD_DELUP     7    /* point%delUp(5,N)       width 5  */
+#define MFCFD_FIELD_DELUN     8    /* point%delUn(5,N)       width 5  */
+#define MFCFD_FIELD_DINV      9    /* D_inv of the last sweep, width 1 */
+
+#define MFCFD_PRECISION_FP64  0    /* all FP64, bit-matched to the CPU oracle */
+
+/*
+ * Run-time form of the reference's compile-time constants (parameter.f90:
+ * 8-33).  mfcfd_params_init fills the reference's values for a given Mach
+ * number and angle of attack.
+ */
+typedef struct mfcfd_params {
+    double power;             /* least-squares weight exponent (parameter.f90:21) */
+    double vl_const;          /* Venkatakrishnan limiter K (parameter.f90:22) */
+    double cfl;               /* CFL number (parameter.f90:23) */
+    double rho_inf, u1_inf, u2_inf, u3_inf, pr_inf;   /* freestream (parameter.f90:29-33) */
+    int32_t inner_iterations; /* second-order q-derivative passes (parameter.f90:24) */
+    int32_t split_capacity;   /* split-list capacity: 22 reproduces the reference's
+                                 storage (data_structure.f90:83-88) including
+                                 overflow into the next point's column; 0 means
+                                 unlimited lists */
+    int32_t precision;        /* MFCFD_PRECISION_FP64 */
+    int32_t device;           /* CUDA device ordinal; -1 builds a host-only handle
+                                 (stencils, alias, schedule) without device state */
+    int32_t reserved[8];
+} mfcfd_params;
+
+typedef struct mfcfd_info {
+    int32_t n_points;
+    int32_t n_wall, n_outer, n_interior, n_supersonic;
+    int32_t n_levels_forward;     /* depth of the forward-sweep schedule */
+    int32_t n_levels_backward;
+    int32_t max_level_width;
+    int32_t split_overflows;      /* list entries written past split_capacity */
+    int32_t shared_frame;         /* 1 if interior points share one frame */
+    int64_t device_bytes;         /* device memory held by the handle */
+} mfcfd_info;
+
+typedef struct mfcfd_handle mfcfd_handle;
+
+/* Fill *p with parameter.f90's values: power 0, K 2, CFL 5, no inner
+ * iterations, rho 1, u = Mach (cos a, sin a, 0), p = 1/1.4, capacity 22. */
+void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg);
+
+/*
+ * Build the split stencils (generate_connectivity.f90:12-246) and the sweep
+ * order (implicit_aliasing.f90:13-44), validate them, and upload the cloud.
+ * Replaces allocate_size + read_input_point_data + generate_split_stencils +
+ * aliasing (data_structure.f90:63-104, point_preprocessor.f90:30-95,
+ * q_lskum.f90:25-26).  tan1/tan2/nor are (3,N); conn is (27,N), 1-based.
+ * On failure *out may still receive a handle that carries the message for
+ * mfcfd_last_error; destroy it with mfcfd_destroy.
+ */
+int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status,
+                 const double *x, const double *y, const double *z,
+                 const double *tan1, const double *tan2, const double *nor,
+                 const int32_t *nbhs, const int32_t *conn, const double *min_dist,
+                 mfcfd_handle **out);
+
+/* Set point%prim (5,N) and zero delUp/delUn: initial_conditions.f90:18-29. */
+int mfcfd_set_prim(mfcfd_handle *h, const double *prim);
+
+/* One call of fpi_solver(t) (fpi_solver.f90:20-45): the seven phases on the
+ * GPU; returns res_new (state_update_implicit.f90:187) and residue
+ * (fpi_solver.f90:38-43).  Either output pointer may be NULL. */
+int mfcfd_fpi_step(mfcfd_handle *h, int32_t t, double *res_new, double *residue);
+
+/* The q_lskum loop (q_lskum.f90:28-32) for t = t0 .. t0+iters-1 without host
+ * round trips; res_hist (2*iters, may be NULL) receives (res_new, residue)
+ * per iteration. */
+int mfcfd_run(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist);
+
+/* Copy a field to host memory (see MFCFD_FIELD_*). */
+int mfcfd_get(mfcfd_handle *h, int32_t field, double *out);
+
+/* Checkpoint / resume: the whole iteration state is prim (5,N) plus
+ * delUn (5,N) (delUp equals delUn between iterations) and the residual
+ * reference res_old.  set_state does not zero the increments. */
+int mfcfd_get_state(mfcfd_handle *h, double *prim, double *delu, double *res_old);
+int mfcfd_set_state(mfcfd_handle *h, const double *prim, const double *delu, double res_old);
+
+/* The six split lists as the flux routines read them (xpos, xneg, ypos,
+ * yneg, zpos, zneg): counts (6,N) and the first `width` entries of each
+ * list (width,6,N), 1-based, 0 past the count. */
+int mfcfd_get_stencils(mfcfd_handle *h, int32_t *counts, int32_t *lists, int32_t width);
+
+/* point%alias(N) and point%point_with_alias(N) (implicit_aliasing.f90). */
+int mfcfd_get_alias(mfcfd_handle *h, int32_t *alias, int32_t *point_with_alias);
+
+/* Level of every point in the forward (dir 0) or backward (dir 1) sweep
+ * schedule; -1 for points the sweeps skip. */
+int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level);
+
+int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info);
+
+/* The CUDA stream (cudaStream_t) all of the handle's work runs on, so a
+ * caller can order its own work or timing events after it. */
+int mfcfd_get_stream(mfcfd_handle *h, void **stream);
+
+/* Phase timing.  While enabled, every iteration records CUDA events between
+ * its phases; mfcfd_get_phase_times returns the summed device milliseconds
+ * per phase (MFCFD_NPHASE entries, order below) and the iteration count
+ * since profiling was enabled. */
+#define MFCFD_NPHASE 7   /* q-derivatives, flux residual, D_inv, forward sweep,
+                            backward sweep, state update, residual sum */
+int mfcfd_set_profiling(mfcfd_handle *h, int32_t on);
+int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters);
+
+int mfcfd_destroy(mfcfd_handle *h);
+
+const char *mfcfd_last_error(const mfcfd_handle *h);
+const char *mfcfd_strerror(int code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFCFD_H */
