@@ -35,6 +35,7 @@ struct mfcfd_handle {
     std::vector<cudaEvent_t> ev;          // (MFCFD_NPHASE+1) per iteration slot
     double phase_ms[MFCFD_NPHASE] = {0};
     int64_t prof_iters = 0;
+    int epoch = 1;        // ready-flag value of the next forward sweep (+1 backward)
 };
 
 namespace {
@@ -113,14 +114,27 @@ int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist)
             DevCloud dc = h->d;
             dc.U = h->U_buf[h->cur];
             dc.q = h->q_buf[h->cur];
+            dc.epoch = h->epoch;
+            h->epoch += 2;
+            if (h->epoch > (1 << 30)) h->epoch = 1;   // flags are reset below on wrap
             cudaEvent_t *ev = h->profiling ? &h->ev[(size_t)j * (MFCFD_NPHASE + 1)] : nullptr;
             cudaError_t e = launch_iteration(dc, j, h->stream, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], ev);
             if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
             h->last = h->cur;
             h->cur = 1 - h->cur;
         }
+        int err_flag = 0;
         CK(cudaMemcpyAsync(res.data(), h->d.res_dev, sizeof(double) * chunk, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(&err_flag, h->d.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
+        if (h->epoch == 1) CK(cudaMemsetAsync(h->d.flag, 0, sizeof(int) * (size_t)h->d.n, h->stream));
+        if (err_flag) {
+            CK(cudaMemsetAsync(h->d.err, 0, sizeof(int), h->stream));
+            CK(cudaMemsetAsync(h->d.flag, 0, sizeof(int) * (size_t)h->d.n, h->stream));
+            h->epoch = 1;
+            CK(cudaStreamSynchronize(h->stream));
+            return fail(h, MFCFD_ERR_TIMEOUT, "a sweep wait ran out; the iteration results are invalid");
+        }
         if (h->profiling) {
             for (int j = 0; j < chunk; ++j) {
                 const cudaEvent_t *ev = &h->ev[(size_t)j * (MFCFD_NPHASE + 1)];
@@ -187,6 +201,11 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         *out = h;
         return MFCFD_ERR_UNSUPPORTED;
     }
+    if (P.sweep_mode != MFCFD_SWEEP_DATAFLOW && P.sweep_mode != MFCFD_SWEEP_LEVELS) {
+        h->err = "unknown sweep_mode";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
     if (P.split_capacity < 0 || P.split_capacity > 1000) {
         h->err = "split_capacity out of range";
         *out = h;
@@ -235,11 +254,21 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     UP(fwd_off, T.fwd_off); UP(bwd_off, T.bwd_off);
     UP(fwd_cnt, T.fwd_cnt); UP(bwd_cnt, T.bwd_cnt);
     UP(fwd_ent, T.fwd_ent); UP(bwd_ent, T.bwd_ent);
+    UP(fwd_need, T.fwd_need); UP(bwd_need, T.bwd_need);
     UP(res_order, order);
 #undef UP
     d.n_fwd_levels = (int)T.fwd_lvl_ptr.size() - 1;
     d.n_bwd_levels = (int)T.bwd_lvl_ptr.size() - 1;
     d.n_res = (int)order.size();
+    d.n_swept = (int)T.fwd_lvl_pts.size();
+    d.max_width = T.max_level_width;
+    d.sweep_mode = P.sweep_mode;
+    if ((rc = dalloc(h, &d.flag, n))) return rc;
+    if ((rc = dalloc(h, &d.sweep_counter, 2))) return rc;
+    if ((rc = dalloc(h, &d.err, 1))) return rc;
+    CK(cudaMemsetAsync(d.flag, 0, sizeof(int) * (size_t)n, h->stream));
+    CK(cudaMemsetAsync(d.sweep_counter, 0, sizeof(int) * 2, h->stream));
+    CK(cudaMemsetAsync(d.err, 0, sizeof(int), h->stream));
     size_t n5 = (size_t)n * 5;
 #define AL(ptr, cnt) if ((rc = dalloc(h, &ptr, cnt))) return rc
     AL(d.prim, n5); AL(h->U_buf[0], n5); AL(h->U_buf[1], n5); AL(h->q_buf[0], n5);

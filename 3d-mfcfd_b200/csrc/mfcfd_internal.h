@@ -24,13 +24,16 @@ enum PointClass : int8_t { CLS_INTERIOR = 0, CLS_WALL = 1, CLS_OUTER = 2, CLS_OT
 // geo layout within one list's 8 doubles
 enum { G_XX = 0, G_YY, G_ZZ, G_XY, G_YZ, G_ZX, G_DET, G_DNUM };
 
-// One neighbour term of an LdelU / UdelU sum: neighbour and its weighted
-// offsets in the consumer's frame (dels*w, delt*w, deln*w).
+// One neighbour term of an LdelU / UdelU sum: neighbour, list (bits 0-7)
+// and neighbour slot (bits 8-15), and the weighted offsets in the
+// consumer's frame (dels*w, delt*w, deln*w).
 struct SweepEntry {
     int32_t k;
     int32_t pad;
     double w[3];
 };
+
+constexpr int SWEEP_MAX_ENTRIES = 96;   // per point and direction (checked at set-up)
 
 // Everything the set-up derives from the cloud (host copy).
 struct Topology {
@@ -58,6 +61,7 @@ struct Topology {
     std::vector<int32_t> fwd_off, bwd_off;        // n+1 entry offsets
     std::vector<uint8_t> fwd_cnt, bwd_cnt;        // n*6
     std::vector<SweepEntry> fwd_ent, bwd_ent;
+    std::vector<uint32_t> fwd_need, bwd_need;     // slots with terms in the sweep
     std::vector<uint8_t> swept;                   // 1 if the sweeps update the point
     std::vector<uint8_t> consumer_shared;         // 1: reads published flux increments
     int shared_frame = 0;
@@ -100,8 +104,16 @@ struct DevCloud {
     const int32_t *fwd_off, *bwd_off;
     const uint8_t *fwd_cnt, *bwd_cnt;
     const SweepEntry *fwd_ent, *bwd_ent;
+    const uint32_t *fwd_need, *bwd_need;
     const int32_t *res_order;     // wall then interior ids, index order
     int n_res;
+    int n_swept;                  // points in each sweep order
+    int max_width;                // widest sweep level
+    int sweep_mode;               // MFCFD_SWEEP_*
+    int epoch;                    // ready-flag value of this iteration's forward sweep
+    int *flag;                    // per point ready flag (dataflow sweeps)
+    int *sweep_counter;           // 2 work counters (forward, backward)
+    int *err;                     // set when a bounded wait gave up
     // state (Fortran layout, point-major)
     double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
     double *gold;                 // 30 per point: fluxes of prim in frame0

@@ -6,7 +6,8 @@
  *   k_flux        eval_flux_residual                warp per point
  *   k_dinv_gold   D_inv, fluxes of prim in the shared interior frame,
  *                 flux increments of points the sweeps do not update
- *   k_sweep x2    forward / backward LU-SGS sweep   one CTA, level by level
+ *   k_sweep_df x2 forward / backward LU-SGS sweep   dataflow over all SMs
+ *                 (k_sweep_levels: one CTA, level by level)
  *   k_update      state_update_implicit + next iteration's U and q
  *   k_reduce_*    res_new (deterministic two-pass sum)
  * State stays resident in HBM in the reference's point-major layout.
@@ -25,7 +26,6 @@ constexpr int FLUX_WARPS = 4;            // warps per CTA in k_flux
 constexpr int FLUX_SMEM_PER_WARP = NDIR * MAX_SLOTS * 5 + MAX_SLOTS * 3;   // doubles
 constexpr int SWEEP_THREADS = 512;
 constexpr int SWEEP_WARPS = SWEEP_THREADS / 32;
-constexpr int SWEEP_SMEM_PER_WARP = 32 * 5 + 32 * 3;                      // doubles
 constexpr int RED_THREADS = 256;
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -305,91 +305,198 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
 
 // ---------------------------------------------------------------- LU-SGS sweeps
 
+__device__ __forceinline__ int ld_relaxed_gpu(const int *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Acquire side of the flag handshake: after a relaxed read has seen the
+// producer's release store, this fence orders the reads that follow.
+__device__ __forceinline__ void fence_acquire_gpu() {
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
+__device__ __forceinline__ void st_release_gpu(int *p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait for a neighbour's ready flag.  Polls with relaxed loads (an
+// acquire load per poll would invalidate the SM's L1 every time); the caller
+// issues one fence_acquire_gpu() afterwards.  Gives up after SPIN_LIMIT polls
+// (seconds), or at once when another warp already gave up: it records the
+// failure in *err (the host reports MFCFD_ERR_TIMEOUT) and returns.
+constexpr int SPIN_LIMIT = 1 << 25;
+
+__device__ __forceinline__ void wait_ready(const int *flag, int epoch, int *err) {
+    int it = 0;
+    while (ld_relaxed_gpu(flag) != epoch) {
+        ++it;
+        if ((it & 4095) == 0) {
+            if (*(volatile int *)err) return;
+            __nanosleep(64);
+        }
+        if (it > SPIN_LIMIT) {
+            atomicExch(err, 1);
+            return;
+        }
+    }
+}
+
+// Per-warp shared memory of the sweep kernels.
+constexpr int SW_META_BYTES = SWEEP_MAX_ENTRIES * 8;                // int2 (k, list|slot<<8)
+constexpr int SW_W_BYTES = SWEEP_MAX_ENTRIES * 3 * 8;               // weights
+constexpr int SW_T_DOUBLES = NDIR * MAX_SLOTS * 5;                  // >= SWEEP_MAX_ENTRIES * 5
+constexpr int SWEEP_SMEM_BYTES = SW_META_BYTES + SW_W_BYTES + SW_T_DOUBLES * 8;
+static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
+
 // One point of the forward (LdelU) or backward (UdelU) sweep, processed by
 // one warp (implicit_forward_and_reverse_sweeps.f90:30-37 / :61-68).
-__device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, double *sm) {
+//
+// Phase A (no dependency on the sweep): stage the point's terms (neighbour,
+// list, weights) in shared memory and load everything else the point needs;
+// points outside the shared frame also evaluate G(prim_k) of their
+// neighbours here.  Phase B: wait for the ready flags of the neighbours whose
+// increments are read.  Phase C: read the published increments (or evaluate
+// G(prim(U_k + dU_k)) - G(prim_k)), sum each list in list order (30 lanes:
+// list x component), solve the 3x3 systems, update dU and publish this
+// point's own increment, then raise its flag.
+template <bool DATAFLOW>
+__device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, char *smb, int epoch) {
+    int2 *M = reinterpret_cast<int2 *>(smb);
+    double *Wt = reinterpret_cast<double *>(smb + SW_META_BYTES);
+    double *T = reinterpret_cast<double *>(smb + SW_META_BYTES + SW_W_BYTES);
     const int cls = d.cls[p];
     const int off = forward ? d.fwd_off[p] : d.bwd_off[p];
     const uint8_t *cnt = (forward ? d.fwd_cnt : d.bwd_cnt) + (size_t)p * NDIR;
     const SweepEntry *ent = forward ? d.fwd_ent : d.bwd_ent;
     const int dd = lane / 5, c = lane - 5 * (lane / 5);
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    if (d.consumer_shared[p]) {
-        // published increments of the neighbours in the shared frame
+    int total = 0, lo = 0, hi = 0;
+#pragma unroll
+    for (int e = 0; e < NDIR; ++e) {
+        const int ce = cnt[e];
+        if (e < dd) lo += ce;
+        if (e <= dd) hi += ce;
+        total += ce;
+    }
+    const bool shared = d.consumer_shared[p] != 0;
+
+    // ---- phase A
+    for (int j = lane; j < total; j += 32) {
+        const SweepEntry &E = ent[off + j];
+        M[j] = make_int2(E.k, E.pad);
+        Wt[3 * j + 0] = E.w[0];
+        Wt[3 * j + 1] = E.w[1];
+        Wt[3 * j + 2] = E.w[2];
+    }
+    double g[7] = {0, 0, 0, 0, 0, 0, 1.0};
+    double gold = 0.0;
+    if (lane < 30) {
+        const double *gp = d.geo + (size_t)p * GEO_STRIDE + dd * 8;
+#pragma unroll
+        for (int r = 0; r < 7; ++r) g[r] = gp[r];
+        gold = d.gold[30 * (size_t)p + lane];
+    }
+    double dinv = 0.0, base5 = 0.0;
+    if (lane < 5) {
+        dinv = d.dinv[p];
+        base5 = forward ? d.flux_res[5 * (size_t)p + lane] : d.dUp[5 * (size_t)p + lane];
+    }
+    double Up[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) Up[r] = d.U[5 * (size_t)p + r];
+    Frame Fp;
+    load_frame(d.frame + 9 * (size_t)p, Fp);
+    const uint32_t need = shared ? 0u : (forward ? d.fwd_need[p] : d.bwd_need[p]);
+    const bool mine = !shared && (need >> lane) & 1u;
+    int k_slot = 0, mask_slot = 0;
+    if (mine) {
+        k_slot = d.slot_nbr[(size_t)p * MAX_SLOTS + lane];
+        mask_slot = d.slot_mask[(size_t)p * MAX_SLOTS + lane];
+        double po[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) po[r] = d.prim[5 * (size_t)k_slot + r];
+        FluxPre Po;
+        flux_pre(po, Fp, Po);
+        int axes = 0;
+#pragma unroll
+        for (int e = 0; e < NDIR; ++e)
+            if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
+        AxisTerms Ao[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (axes & (1 << a)) axis_terms(Po, a, Ao[a]);
+        for (int e = 0; e < NDIR; ++e) {
+            if (!(mask_slot & (1 << e))) continue;
+            const int kind = flux_kind(cls, e);
+#pragma unroll
+            for (int cc = 0; cc < 5; ++cc) T[(e * MAX_SLOTS + lane) * 5 + cc] = flux_component(kind, cc, Po, Ao);
+        }
+    }
+    __syncwarp();
+
+    // ---- phase B
+    if (DATAFLOW) {
+        if (shared) {
+            for (int j = lane; j < total; j += 32) {
+                const int k = M[j].x;
+                if (d.swept[k]) wait_ready(d.flag + k, epoch, d.err);
+            }
+        } else if (mine && d.swept[k_slot]) {
+            wait_ready(d.flag + k_slot, epoch, d.err);
+        }
+        fence_acquire_gpu();
+        __syncwarp();
+    }
+
+    // ---- phase C
+    if (shared) {
         const double *src = forward ? d.dgf : d.dgb;
-        if (lane < 30) {
-            int base = off;
-            for (int e = 0; e < dd; ++e) base += cnt[e];
-            const int m = cnt[dd];
-            for (int j = 0; j < m; ++j) {
-                const SweepEntry &E = ent[base + j];
-                const double t = src[30 * (size_t)E.k + dd * 5 + c];
-                sx = sx + t * E.w[0];
-                sy = sy + t * E.w[1];
-                sz = sz + t * E.w[2];
+        for (int j = lane; j < total; j += 32) {
+            const double *gs = src + 30 * (size_t)M[j].x + 5 * (M[j].y & 255);
+#pragma unroll
+            for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __ldcg(gs + cc);
+        }
+    } else if (mine) {
+        const double *dsrc = forward ? d.dUp : d.dUn;
+        double U[5], pn[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) U[r] = __ldcg(dsrc + 5 * (size_t)k_slot + r) + d.U[5 * (size_t)k_slot + r];
+        Frame Fk;
+        load_frame(d.frame + 9 * (size_t)k_slot, Fk);
+        conserved_to_primitive(U, Fk, pn);
+        FluxPre Pn;
+        flux_pre(pn, Fp, Pn);
+        int axes = 0;
+#pragma unroll
+        for (int e = 0; e < NDIR; ++e)
+            if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
+        AxisTerms An[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (axes & (1 << a)) axis_terms(Pn, a, An[a]);
+        for (int e = 0; e < NDIR; ++e) {
+            if (!(mask_slot & (1 << e))) continue;
+            const int kind = flux_kind(cls, e);
+#pragma unroll
+            for (int cc = 0; cc < 5; ++cc) {
+                double *t = &T[(e * MAX_SLOTS + lane) * 5 + cc];
+                *t = flux_component(kind, cc, Pn, An) - *t;
             }
         }
-    } else {
-        // the point's own frame: evaluate G(prim(U_k + dU_k)) - G(prim_k)
-        const double *dsrc = forward ? d.dUp : d.dUn;
-        double *T = sm;               // T[j*5 + c]
-        double *Wm = sm + 32 * 5;     // W[j*3 + a]
-        int total = 0;
-#pragma unroll
-        for (int e = 0; e < NDIR; ++e) total += cnt[e];
-        Frame Fp;
-        load_frame(d.frame + 9 * (size_t)p, Fp);
-        for (int base = 0; base < total; base += 32) {
-            const int j = base + lane;
-            if (j < total) {
-                const SweepEntry &E = ent[off + j];
-                const int k = E.k;
-                const int kind = flux_kind(cls, E.pad);
-                Frame Fk;
-                load_frame(d.frame + 9 * (size_t)k, Fk);
-                double U[5], pn[5], po[5];
-#pragma unroll
-                for (int r = 0; r < 5; ++r) {
-                    U[r] = dsrc[5 * (size_t)k + r] + d.U[5 * (size_t)k + r];
-                    po[r] = d.prim[5 * (size_t)k + r];
-                }
-                conserved_to_primitive(U, Fk, pn);
-                FluxPre Pn, Po;
-                AxisTerms An[3], Ao[3];
-                flux_pre(pn, Fp, Pn);
-                flux_pre(po, Fp, Po);
-                const int axes = kind_axes(kind);
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-                    if (axes & (1 << a)) { axis_terms(Pn, a, An[a]); axis_terms(Po, a, Ao[a]); }
-#pragma unroll
-                for (int cc = 0; cc < 5; ++cc)
-                    T[(j - base) * 5 + cc] = flux_component(kind, cc, Pn, An) - flux_component(kind, cc, Po, Ao);
-                Wm[(j - base) * 3 + 0] = E.w[0];
-                Wm[(j - base) * 3 + 1] = E.w[1];
-                Wm[(j - base) * 3 + 2] = E.w[2];
-            }
-            __syncwarp();
-            if (lane < 30) {
-                int lo = 0;
-                for (int e = 0; e < dd; ++e) lo += cnt[e];
-                const int hi = lo + cnt[dd];
-                const int a0 = max(lo, base), a1 = min(hi, base + 32);
-                for (int jj = a0; jj < a1; ++jj) {
-                    const double t = T[(jj - base) * 5 + c];
-                    sx = sx + t * Wm[(jj - base) * 3 + 0];
-                    sy = sy + t * Wm[(jj - base) * 3 + 1];
-                    sz = sz + t * Wm[(jj - base) * 3 + 2];
-                }
-            }
-            __syncwarp();
+    }
+    __syncwarp();
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    if (lane < 30) {
+        for (int jj = lo; jj < hi; ++jj) {
+            const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + (M[jj].y >> 8)) * 5 + c];
+            sx = sx + t * Wt[3 * jj + 0];
+            sy = sy + t * Wt[3 * jj + 1];
+            sz = sz + t * Wt[3 * jj + 2];
         }
     }
     double G = 0.0;
-    if (lane < 30) {
-        const double *g = d.geo + (size_t)p * GEO_STRIDE + dd * 8;
-        G = cramer_num(dd >> 1, g, sx, sy, sz) / g[G_DET];
-    }
+    if (lane < 30) G = cramer_num(dd >> 1, g, sx, sy, sz) / g[6];
     double gd[NDIR];
 #pragma unroll
     for (int e = 0; e < NDIR; ++e) gd[e] = __shfl_sync(FULL, G, e * 5 + (lane % 5));
@@ -398,12 +505,11 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, do
         double lu;
         if (cls == CLS_WALL) lu = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
         else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
-        const double dinv = d.dinv[p];
         if (forward) {
-            dnew = -(dinv * (d.flux_res[5 * (size_t)p + lane] + lu));
+            dnew = -(dinv * (base5 + lu));
             d.dUp[5 * (size_t)p + lane] = dnew;
         } else {
-            dnew = d.dUp[5 * (size_t)p + lane] - dinv * lu;
+            dnew = base5 - dinv * lu;
             d.dUn[5 * (size_t)p + lane] = dnew;
         }
     }
@@ -411,40 +517,68 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, do
         // publish this point's increment for the consumers in the shared frame
         double U[5], pn[5];
 #pragma unroll
-        for (int r = 0; r < 5; ++r) U[r] = __shfl_sync(FULL, dnew, r) + d.U[5 * (size_t)p + r];
+        for (int r = 0; r < 5; ++r) U[r] = __shfl_sync(FULL, dnew, r) + Up[r];
         if (lane < 30) {
-            Frame Fp;
-            load_frame(d.frame + 9 * (size_t)p, Fp);
             conserved_to_primitive(U, Fp, pn);
             Frame F0;
 #pragma unroll
             for (int r = 0; r < 3; ++r) { F0.t1[r] = d.frame0[r]; F0.t2[r] = d.frame0[3 + r]; F0.n[r] = d.frame0[6 + r]; }
             FluxPre P;
             flux_pre(pn, F0, P);
-            AxisTerms A[3];
-            const int a = dd >> 1;
-            axis_terms(P, a, A[a]);
-            const double gnew = flux_component(dd, c, P, A);
+            AxisTerms At;
+            axis_terms(P, dd >> 1, At);
+            const double gnew = flux_component(dd, c, P, At, At, At);
             double *dst = forward ? d.dgf : d.dgb;
-            dst[30 * (size_t)p + lane] = gnew - d.gold[30 * (size_t)p + lane];
+            dst[30 * (size_t)p + lane] = gnew - gold;
         }
+    }
+    if (DATAFLOW) {
+        // the warp barrier orders the lanes' stores before lane 0's release
+        __syncwarp();
+        if (lane == 0) st_release_gpu(d.flag + p, epoch);
+    } else {
+        __syncwarp();
     }
 }
 
 // Level-synchronous sweep in one CTA: the points of a level are independent
 // (none reads another's increment), so warps take them in parallel and a
 // block barrier separates levels.
-__global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(DevCloud d, int forward) {
+__global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep_levels(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *sm = smem + warp * SWEEP_SMEM_PER_WARP;
+    char *smb = reinterpret_cast<char *>(smem) + warp * SWEEP_SMEM_BYTES;
     const int nl = forward ? d.n_fwd_levels : d.n_bwd_levels;
     const int32_t *lptr = forward ? d.fwd_lvl_ptr : d.bwd_lvl_ptr;
     const int32_t *lpts = forward ? d.fwd_lvl_pts : d.bwd_lvl_pts;
     for (int l = 0; l < nl; ++l) {
         const int a = lptr[l], b = lptr[l + 1];
-        for (int idx = a + warp; idx < b; idx += SWEEP_WARPS) sweep_point(d, lpts[idx], forward != 0, lane, sm);
+        for (int idx = a + warp; idx < b; idx += SWEEP_WARPS)
+            sweep_point<false>(d, lpts[idx], forward != 0, lane, smb, 0);
         __syncthreads();
+    }
+}
+
+// Dataflow sweep over many SMs: each warp takes the next point of the
+// level-major (topological) order from a global counter and waits for the
+// ready flags of the neighbours it reads.  A point's dependencies are always
+// taken before it by warps that are already running, so the waits end; each
+// is bounded anyway (wait_ready).
+constexpr int DF_WARPS = 4;
+
+__global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forward, int epoch) {
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    char *smb = reinterpret_cast<char *>(smem) + warp * SWEEP_SMEM_BYTES;
+    int *counter = d.sweep_counter + (forward ? 0 : 1);
+    const int32_t *order = forward ? d.fwd_lvl_pts : d.bwd_lvl_pts;
+    const int total = d.n_swept;
+    for (;;) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(counter, 1);
+        idx = __shfl_sync(FULL, idx, 0);
+        if (idx >= total) break;
+        sweep_point<true>(d, order[idx], forward != 0, lane, smb, epoch);
     }
 }
 
@@ -539,10 +673,26 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
     if (!g_attr_set) {
         cudaFuncSetAttribute(k_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
-        cudaFuncSetAttribute(k_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SWEEP_WARPS * SWEEP_SMEM_PER_WARP * 8);
+        cudaFuncSetAttribute(k_sweep_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SWEEP_WARPS * SWEEP_SMEM_BYTES);
+        cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             DF_WARPS * SWEEP_SMEM_BYTES);
         g_attr_set = true;
     }
+    // dataflow grid: about the widest level in warps (more warps only add
+    // pollers), within 8 per SM
+    int df_warps = d.max_width;
+    df_warps = df_warps < 64 ? 64 : (df_warps > 148 * 8 ? 148 * 8 : df_warps);
+    const int df_blocks = (df_warps + DF_WARPS - 1) / DF_WARPS;
+    auto sweep = [&](int forward) {
+        if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
+            k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
+        } else {
+            cudaMemsetAsync(d.sweep_counter + (forward ? 0 : 1), 0, sizeof(int), s);
+            k_sweep_df<<<df_blocks, DF_WARPS * 32, DF_WARPS * SWEEP_SMEM_BYTES, s>>>(
+                d, forward, forward ? d.epoch : d.epoch + 1);
+        }
+    };
     auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
     mark(0);
     k_qderiv<<<(n + 127) / 128, 128, 0, s>>>(d);
@@ -552,9 +702,9 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
     mark(2);
     k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);
     mark(3);
-    k_sweep<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_PER_WARP * 8, s>>>(d, 1);
+    sweep(1);
     mark(4);
-    k_sweep<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_PER_WARP * 8, s>>>(d, 0);
+    sweep(0);
     mark(5);
     k_update<<<(n + 127) / 128, 128, 0, s>>>(d, U_next, q_next);
     mark(6);

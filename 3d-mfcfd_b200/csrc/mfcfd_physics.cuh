@@ -34,33 +34,43 @@ __host__ __device__ __forceinline__ int flux_kind(int cls, int d) {
     return GNONE;
 }
 
+// Runtime choice among three register values.  Used instead of indexing a
+// small array with a runtime index, which would place it in local memory.
+__device__ __forceinline__ double sel3(int a, double v0, double v1, double v2) {
+    return a == 0 ? v0 : (a == 1 ? v1 : v2);
+}
+
 // Quantities every flux formula shares (split_fluxes.f90:24-40).
 struct FluxPre {
-    double rho, pr, ut[3], beta, sb, spb, usq;
+    double rho, pr, ut1, ut2, un, beta, sb, spb, usq;
+    __device__ __forceinline__ double ut(int a) const { return sel3(a, ut1, ut2, un); }
 };
 
 __device__ __forceinline__ void flux_pre(const double prim[5], const Frame &F, FluxPre &P) {
     const double rho = prim[0], u1 = prim[1], u2 = prim[2], u3 = prim[3], pr = prim[4];
     P.rho = rho;
     P.pr = pr;
-    P.ut[0] = F.t1[0] * u1 + F.t1[1] * u2 + F.t1[2] * u3;
-    P.ut[1] = F.t2[0] * u1 + F.t2[1] * u2 + F.t2[2] * u3;
-    P.ut[2] = F.n[0] * u1 + F.n[1] * u2 + F.n[2] * u3;
+    P.ut1 = F.t1[0] * u1 + F.t1[1] * u2 + F.t1[2] * u3;
+    P.ut2 = F.t2[0] * u1 + F.t2[1] * u2 + F.t2[2] * u3;
+    P.un = F.n[0] * u1 + F.n[1] * u2 + F.n[2] * u3;
     P.beta = 0.5 * rho / pr;
     P.sb = sqrt(P.beta);
     P.spb = sqrt(MF_PI * P.beta);
-    P.usq = P.ut[0] * P.ut[0] + P.ut[1] * P.ut[1] + P.ut[2] * P.ut[2];
+    P.usq = P.ut1 * P.ut1 + P.ut2 * P.ut2 + P.un * P.un;
 }
 
 // Half-range terms along one axis: B = 0.5 exp(-S^2)/sqrt(pi beta),
 // A+- = 0.5 (1 +- erf S) with S = u_axis sqrt(beta).
 struct AxisTerms { double B, Ap, An; };
 
+// The |S| < 1 erf polynomial does not need exp(-S^2), so it is evaluated
+// unconditionally and overlaps the exp; the result equals mf_erf(S).
 __device__ __forceinline__ void axis_terms(const FluxPre &P, int a, AxisTerms &T) {
-    const double S = P.ut[a] * P.sb;
+    const double S = P.ut(a) * P.sb;
     const double e = mf_exp(-(S * S));
+    const double small = mf_erf_small(S);
     T.B = 0.5 * e / P.spb;
-    const double er = mf_erf_given_exp(S, e);
+    const double er = fabs(S) < 1.0 ? small : mf_erf_large(S, e);
     T.Ap = 0.5 * (1.0 + er);
     T.An = 0.5 * (1.0 - er);
 }
@@ -77,16 +87,18 @@ __host__ __device__ __forceinline__ int kind_axes(int kind) {
     }
 }
 
-// One component c of flux `kind` given the shared terms and the axis terms.
-__device__ __forceinline__ double flux_component(int kind, int c, const FluxPre &P, const AxisTerms *AT) {
+// One component c of flux `kind` given the shared terms and the axis terms
+// of the three axes (only the axes the kind needs are read).
+__device__ __forceinline__ double flux_component(int kind, int c, const FluxPre &P, const AxisTerms &X,
+                                                 const AxisTerms &Y, const AxisTerms &Z) {
     const double rho = P.rho, pr = P.pr;
-    const double ut1 = P.ut[0], ut2 = P.ut[1], un = P.ut[2];
+    const double ut1 = P.ut1, ut2 = P.ut2, un = P.un;
     if (kind <= GZN) {
         const int a = kind >> 1;
         const bool pos = (kind & 1) == 0;
-        const double A = pos ? AT[a].Ap : AT[a].An;
-        const double B = AT[a].B;
-        const double ua = P.ut[a];
+        const double A = pos ? sel3(a, X.Ap, Y.Ap, Z.Ap) : sel3(a, X.An, Y.An, Z.An);
+        const double B = sel3(a, X.B, Y.B, Z.B);
+        const double ua = P.ut(a);
         const double temp1 = pos ? (ua * A + B) : (ua * A - B);
         if (c == 0) return rho * temp1;
         if (c == 4) {
@@ -95,7 +107,7 @@ __device__ __forceinline__ double flux_component(int kind, int c, const FluxPre 
                        : (t + pr) * ua * A - (t + 0.5 * pr) * B;
         }
         // c = 1..3: the axis component carries the pressure term
-        const double uc = P.ut[c - 1];
+        const double uc = P.ut(c - 1);
         if (c - 1 == a) return pr * A + rho * uc * temp1;
         return rho * uc * temp1;
     }
@@ -104,11 +116,11 @@ __device__ __forceinline__ double flux_component(int kind, int c, const FluxPre 
     const int k4 = wall ? kind - GWXP : kind - GOXP;        // 0 xp, 1 xn, 2 yp, 3 yn
     const int a = k4 >> 1;
     const bool pos = (k4 & 1) == 0;
-    const double A = pos ? AT[a].Ap : AT[a].An;
-    const double B = AT[a].B;
-    const double A3 = wall ? AT[2].An : AT[2].Ap;
-    const double B3 = AT[2].B;
-    const double ua = P.ut[a];
+    const double A = pos ? (a == 0 ? X.Ap : Y.Ap) : (a == 0 ? X.An : Y.An);
+    const double B = a == 0 ? X.B : Y.B;
+    const double A3 = wall ? Z.An : Z.Ap;
+    const double B3 = Z.B;
+    const double ua = a == 0 ? ut1 : ut2;
     const double temp1 = pos ? (ua * A + B) : (ua * A - B);
     switch (c) {
     case 0: return rho * temp1 * A3;
@@ -123,6 +135,10 @@ __device__ __forceinline__ double flux_component(int kind, int c, const FluxPre 
                     : temp3 * A3 + 0.5 * rho * un * B3 * temp1;
     }
     }
+}
+
+__device__ __forceinline__ double flux_component(int kind, int c, const FluxPre &P, const AxisTerms *AT) {
+    return flux_component(kind, c, P, AT[0], AT[1], AT[2]);
 }
 
 // qvariables_to_primitive_variables.f90:9-31

@@ -276,8 +276,10 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     auto al = [&](int k) { return T.alias[k]; };
     auto build = [&](bool forward, std::vector<int32_t> &level, std::vector<int32_t> &lptr,
                      std::vector<int32_t> &lpts, std::vector<int32_t> &off,
-                     std::vector<uint8_t> &cnt, std::vector<SweepEntry> &ent) {
+                     std::vector<uint8_t> &cnt, std::vector<SweepEntry> &ent,
+                     std::vector<uint32_t> &need) {
         level.assign(n, -1);
+        need.assign(n, 0u);
         off.assign(n + 1, 0);
         cnt.assign((size_t)n * NDIR, 0);
         ent.clear();
@@ -301,9 +303,10 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
                     double w = weights_of(dist);
                     SweepEntry e;
                     e.k = k;
-                    e.pad = d;
+                    e.pad = d | (s << 8);   // list and neighbour slot
                     e.w[0] = dels * w; e.w[1] = delt * w; e.w[2] = deln * w;
                     per[p].push_back(e);
+                    need[p] |= 1u << s;
                     ++taken;
                 }
                 cnt[(size_t)p * NDIR + d] = (uint8_t)taken;
@@ -314,6 +317,8 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             ent.insert(ent.end(), per[p].begin(), per[p].end());
         }
         off[n] = (int32_t)ent.size();
+        for (int p = 0; p < n; ++p)
+            if (off[p + 1] - off[p] > SWEEP_MAX_ENTRIES) return false;
         // levels: longest path over swept dependencies
         int maxl = -1;
         auto visit = [&](int p) {
@@ -338,9 +343,13 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         std::vector<int32_t> fill(lptr.begin(), lptr.end() - 1);
         if (forward) for (int p : order) lpts[fill[level[p]]++] = p;
         else for (auto it = order.rbegin(); it != order.rend(); ++it) lpts[fill[level[*it]]++] = *it;
+        return true;
     };
-    build(true, T.fwd_level, T.fwd_lvl_ptr, T.fwd_lvl_pts, T.fwd_off, T.fwd_cnt, T.fwd_ent);
-    build(false, T.bwd_level, T.bwd_lvl_ptr, T.bwd_lvl_pts, T.bwd_off, T.bwd_cnt, T.bwd_ent);
+    if (!build(true, T.fwd_level, T.fwd_lvl_ptr, T.fwd_lvl_pts, T.fwd_off, T.fwd_cnt, T.fwd_ent, T.fwd_need) ||
+        !build(false, T.bwd_level, T.bwd_lvl_ptr, T.bwd_lvl_pts, T.bwd_off, T.bwd_cnt, T.bwd_ent, T.bwd_need)) {
+        err = "a point reads more than " + std::to_string(SWEEP_MAX_ENTRIES) + " sweep terms";
+        return MFCFD_ERR_STENCIL;
+    }
 
     // ---- shared interior frame: lets producers publish flux increments
     T.shared_frame = 0;

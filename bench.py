@@ -164,6 +164,7 @@ def main():
     ap.add_argument("--impl", default="mfcfd", choices=["mfcfd", "reference"])
     ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep-mode", type=int, default=0, help="0 dataflow, 1 levels")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     wl = WORKLOADS[args.workload]
@@ -203,7 +204,7 @@ def main():
             dist.barrier()
 
     c = cl.shell_cloud(wl["shells"], wl["per_shell"], jitter=wl["jitter"], seed=wl["seed"] + rank)
-    s = Solver(c, wl["mach"], wl["aoa"], device=local_rank)
+    s = Solver(c, wl["mach"], wl["aoa"], device=local_rank, sweep_mode=args.sweep_mode)
     prim0 = cl.initial_state(c, wl["mach"], wl["aoa"])
     s.initial_conditions(prim0)
     info = s.info()

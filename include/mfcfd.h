@@ -78,8 +78,17 @@ typedef struct mfcfd_params {
     int32_t precision;        /* MFCFD_PRECISION_FP64 */
     int32_t device;           /* CUDA device ordinal; -1 builds a host-only handle
                                  (stencils, alias, schedule) without device state */
-    int32_t reserved[8];
+    int32_t sweep_mode;       /* MFCFD_SWEEP_DATAFLOW (default) or MFCFD_SWEEP_LEVELS */
+    int32_t reserved[7];
 } mfcfd_params;
+
+/* LU-SGS sweep schedules.  Both give the reference's sequential result bit
+ * for bit.  DATAFLOW: warps on all SMs take points in topological order and
+ * wait (bounded) on per-point ready flags of the neighbours they read.
+ * LEVELS: one CTA processes level after level with a block barrier between
+ * levels; no device-side waits at all. */
+#define MFCFD_SWEEP_DATAFLOW  0
+#define MFCFD_SWEEP_LEVELS    1
 
 typedef struct mfcfd_info {
     int32_t n_points;

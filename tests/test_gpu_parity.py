@@ -14,10 +14,10 @@ pytestmark = pytest.mark.gpu
 FIELDS = ["PRIM", "U", "Q", "QM", "DQ", "DELT", "FLUX_RES", "DELUP", "DELUN"]
 
 
-def _pair(cloud, mach, aoa, libm, oracle_lib):
+def _pair(cloud, mach, aoa, libm, oracle_lib, sweep_mode=0):
     from mfcfd.solver import Solver
     from mfcfd.cloud import initial_state
-    s = Solver(cloud, mach, aoa)
+    s = Solver(cloud, mach, aoa, sweep_mode=sweep_mode)
     o = oracle_lib.Oracle(cloud, mach, aoa, libm=libm)
     prim0 = initial_state(cloud, mach, aoa)
     s.initial_conditions(prim0)
@@ -31,9 +31,10 @@ def _field_ids(oracle_lib):
             for name in FIELDS]
 
 
+@pytest.mark.parametrize("sweep_mode", [0, 1])
 @pytest.mark.parametrize("mach,aoa", [(0.4, 0.0), (0.8, 2.0)])
-def test_one_iteration_bitexact(small_cloud, oracle_lib, mfcfd_lib, mach, aoa):
-    s, o = _pair(small_cloud, mach, aoa, oracle_lib.LIBM_MFMATH, oracle_lib)
+def test_one_iteration_bitexact(small_cloud, oracle_lib, mfcfd_lib, mach, aoa, sweep_mode):
+    s, o = _pair(small_cloud, mach, aoa, oracle_lib.LIBM_MFMATH, oracle_lib, sweep_mode)
     r_gpu = s.fpi_solver(1)
     r_cpu = o.step(1)
     for name, fg, fo in _field_ids(oracle_lib):
@@ -47,8 +48,9 @@ def test_one_iteration_bitexact(small_cloud, oracle_lib, mfcfd_lib, mach, aoa):
     assert abs(r_gpu[0] - r_cpu[0]) <= 1e-13 * abs(r_cpu[0])
 
 
-def test_twenty_iterations_bitexact(small_cloud, oracle_lib, mfcfd_lib):
-    s, o = _pair(small_cloud, 0.4, 0.0, oracle_lib.LIBM_MFMATH, oracle_lib)
+@pytest.mark.parametrize("sweep_mode", [0, 1])
+def test_twenty_iterations_bitexact(small_cloud, oracle_lib, mfcfd_lib, sweep_mode):
+    s, o = _pair(small_cloud, 0.4, 0.0, oracle_lib.LIBM_MFMATH, oracle_lib, sweep_mode)
     hist = s.q_lskum(20)
     for t in range(1, 21):
         rc = o.step(t)
