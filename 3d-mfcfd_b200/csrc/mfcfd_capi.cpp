@@ -454,6 +454,14 @@ int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters) {
     return MFCFD_OK;
 }
 
+int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new) {
+    if (!h || !res_new) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    cudaError_t e = cudaSetDevice(h->P.device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+    return residual_noalloc(h->d, h->stream, res_new, h->err);
+}
+
 int mfcfd_destroy(mfcfd_handle *h) {
     if (!h) return MFCFD_ERR_ARG;
     release(h);

@@ -129,5 +129,8 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
                              double *U_next, double *q_next, cudaEvent_t *ev);
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
 int reduction_blocks(int n);
+// Allocation-free residual (mfcfd_residual_noalloc); the current device must
+// be the handle's.
+int residual_noalloc(const DevCloud &d, cudaStream_t s, double *res_new, std::string &err);
 
 }  // namespace mfcfd

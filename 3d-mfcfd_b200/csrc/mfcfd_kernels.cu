@@ -17,6 +17,9 @@
  */
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <string>
+
 #include "mfcfd_internal.h"
 #include "mfcfd_physics.cuh"
 
@@ -658,6 +661,67 @@ __global__ void k_reduce_final(DevCloud d, int nblocks, int slot) {
 int reduction_blocks(int n) {
     int b = (n + 4095) / 4096;
     return b < 1 ? 1 : (b > 1024 ? 1024 : b);
+}
+
+// ---------------------------------------------------------------- allocation-free residual
+
+// Scratch of mfcfd_residual_noalloc: one partial sum per reduction block plus
+// the result slot.  A file-scope device array, so that entry point never
+// allocates; 8 KB that every GPU loading the library holds until exit.
+constexpr int NOALLOC_BLOCKS = MFCFD_NOALLOC_MAX_TERMS / 4096;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_BLOCKS + 1];
+
+// Device address of g_noalloc_scratch, looked up once per device.  In host
+// code the symbol names a host-side stand-in, not device memory, so kernels
+// must be given this address instead.
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[256] = {nullptr};
+
+int residual_noalloc(const DevCloud &d, cudaStream_t s, double *res_new, std::string &err) {
+    if (d.n_res > MFCFD_NOALLOC_MAX_TERMS) {
+        err = "mfcfd_residual_noalloc handles at most " + std::to_string(MFCFD_NOALLOC_MAX_TERMS) +
+              " residual terms; this cloud has " + std::to_string(d.n_res);
+        return MFCFD_ERR_UNSUPPORTED;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 256) {
+        err = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
+        return MFCFD_ERR_CUDA;
+    }
+    double *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                return MFCFD_ERR_CUDA;
+            }
+            g_noalloc_ptr[dev] = static_cast<double *>(p);
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    // Same partition as the iteration's own reduction (4096 terms a block),
+    // so the value is the one mfcfd_fpi_step returned.  Every partial that
+    // k_reduce_final reads is written first, so nothing needs clearing.
+    int blocks = (d.n_res + 4095) / 4096;
+    if (blocks < 1) blocks = 1;
+    DevCloud dc = d;
+    dc.partial = scratch;
+    dc.res_dev = scratch + NOALLOC_BLOCKS;
+    k_reduce_partial<<<blocks, RED_THREADS, 0, s>>>(dc);
+    k_reduce_final<<<1, 32, 0, s>>>(dc, blocks, 0);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(res_new, scratch + NOALLOC_BLOCKS, sizeof(double),
+                                              cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        err = std::string("residual_noalloc: ") + cudaGetErrorString(e);
+        return MFCFD_ERR_CUDA;
+    }
+    return MFCFD_OK;
 }
 
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s) {

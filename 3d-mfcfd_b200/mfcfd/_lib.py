@@ -23,7 +23,9 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_run", "mfcfd_get", "mfcfd_get_state", "mfcfd_set_state",
            "mfcfd_get_stencils", "mfcfd_get_alias", "mfcfd_get_levels", "mfcfd_get_info",
            "mfcfd_get_stream", "mfcfd_set_profiling", "mfcfd_get_phase_times",
+           "mfcfd_residual_noalloc",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
+NOALLOC_MAX_TERMS = 1024 * 4096
 NPHASE = 7
 PHASES = ("qderiv", "flux", "dinv", "sweep_fwd", "sweep_bwd", "update", "residual")
 
@@ -88,6 +90,7 @@ def lib():
     L.mfcfd_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.mfcfd_set_profiling.argtypes = [vp, i32]
     L.mfcfd_get_phase_times.argtypes = [vp, vp, vp]
+    L.mfcfd_residual_noalloc.argtypes = [vp, vp]
     L.mfcfd_destroy.argtypes = [vp]
     L.mfcfd_last_error.argtypes = [vp]
     L.mfcfd_last_error.restype = ctypes.c_char_p

@@ -136,6 +136,13 @@ class Solver:
         self._check(_lib.lib().mfcfd_get_phase_times(self.h, ptr(ms), ptr(it)))
         return dict(zip(_lib.PHASES, ms.tolist())), int(it[0])
 
+    def residual_noalloc(self) -> float:
+        """res_new of the last iteration, recomputed without any device
+        allocation (mfcfd_residual_noalloc)."""
+        out = np.zeros(1)
+        self._check(_lib.lib().mfcfd_residual_noalloc(self.h, ptr(out)))
+        return float(out[0])
+
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             _lib.lib().mfcfd_destroy(self.h)

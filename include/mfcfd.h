@@ -171,6 +171,30 @@ int mfcfd_get_stream(mfcfd_handle *h, void **stream);
 int mfcfd_set_profiling(mfcfd_handle *h, int32_t on);
 int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters);
 
+/*
+ * Allocation-free recomputation of the last iteration's density residual.
+ * (No counterpart in the reference; it exists for callers that must not
+ * allocate device memory.)
+ *
+ * Some callers cannot call cudaMalloc at the point where they need a result:
+ * a host whose device memory is owned by another allocator or memory pool,
+ * or code that runs while allocation is forbidden.  This entry point
+ * recomputes res_new of the most recent mfcfd_fpi_step / mfcfd_run
+ * iteration from the handle's per-point residual terms, with the same
+ * two-pass reduction, and allocates nothing: its scratch (one partial sum per
+ * reduction block) is a fixed device array inside the library that every GPU
+ * loading the library holds until the process exits.
+ *
+ * Limit: at most MFCFD_NOALLOC_MAX_TERMS residual terms (wall plus interior
+ * points); larger clouds get MFCFD_ERR_UNSUPPORTED.  The first call on a
+ * device looks up the scratch array's device address; make that first call
+ * before any stream capture.  All calls share the one array and it keeps the
+ * last call's contents (every call overwrites all of it that it reads), so
+ * calls that overlap on the GPU race: do not run two at once, on any stream.
+ */
+#define MFCFD_NOALLOC_MAX_TERMS (1024 * 4096)
+int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new);
+
 int mfcfd_destroy(mfcfd_handle *h);
 
 const char *mfcfd_last_error(const mfcfd_handle *h);
