@@ -191,19 +191,16 @@ def main():
         return
 
     import torch
-    import torch.distributed as dist
     from mfcfd import cloud as cl
+    from mfcfd import replicas
     from mfcfd.solver import Solver
 
     torch.cuda.set_device(local_rank)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    rank, world = replicas.init("nccl", timeout_s=600)
+    barrier = replicas.barrier
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    c = cl.shell_cloud(wl["shells"], wl["per_shell"], jitter=wl["jitter"], seed=wl["seed"] + rank)
+    c = cl.shell_cloud(wl["shells"], wl["per_shell"], jitter=wl["jitter"],
+                       seed=replicas.replica_seed(wl["seed"], rank))
     s = Solver(c, wl["mach"], wl["aoa"], device=local_rank, sweep_mode=args.sweep_mode)
     prim0 = cl.initial_state(c, wl["mach"], wl["aoa"])
     s.initial_conditions(prim0)
@@ -231,11 +228,8 @@ def main():
     clocks = sampler.stop()
     t += args.steps
     ms = e0.elapsed_time(e1)
-    ms_t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * c.n * args.steps / (ms_max / 1e3)
+    ms_max = replicas.max_over_ranks(ms, device="cuda")
+    value = replicas.throughput(c.n, args.steps, ms_max / 1e3, world)
 
     # phase timing (separate pass, same workload) for the roofline
     s.set_profiling(True)
@@ -271,11 +265,8 @@ def main():
         delu_h[:] = delu_out
     torch.cuda.synchronize()
     w1 = time.perf_counter()
-    e2e_s = w1 - w0
-    e2e_t = torch.tensor([e2e_s], device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * c.n * args.steps / float(e2e_t.item())
+    e2e_s = replicas.max_over_ranks(w1 - w0, device="cuda")
+    e2e_value = replicas.throughput(c.n, args.steps, e2e_s, world)
     io_bytes = c.n * 5 * 8 * 2
 
     cpu_base = None
@@ -302,8 +293,7 @@ def main():
                 "gpu_launches": KERNELS_PER_ITER * args.steps}
         print(json.dumps(line), flush=True)
     s.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finalize()
 
 
 if __name__ == "__main__":

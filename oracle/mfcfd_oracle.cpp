@@ -977,4 +977,15 @@ void oracle_get_alias(void *h, int *alias, int *point_with_alias) {
 
 void oracle_destroy(void *h) { delete (Oracle *)h; }
 
+// Evaluate one libm function over an array: fn 0 exp, 1 log, 2 erf;
+// mode 0 glibc, 1 mfmath.  For the accuracy tests of mfmath.h.
+void oracle_libm_eval(int fn, int mode, const double *x, double *y, int n) {
+    for (int i = 0; i < n; ++i) {
+        double v = x[i];
+        if (fn == 0) y[i] = mode ? mf_exp(v) : std::exp(v);
+        else if (fn == 1) y[i] = mode ? mf_log(v) : std::log(v);
+        else y[i] = mode ? mf_erf(v) : std::erf(v);
+    }
+}
+
 }  // extern "C"

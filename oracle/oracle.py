@@ -57,12 +57,21 @@ def lib():
         L.oracle_get_stencils.argtypes = [vp, vp, vp, ctypes.c_int]
         L.oracle_get_alias.argtypes = [vp, vp, vp]
         L.oracle_destroy.argtypes = [vp]
+        L.oracle_libm_eval.argtypes = [ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int]
         _lib = L
     return _lib
 
 
 def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def libm_eval(fn: str, mode: int, x) -> np.ndarray:
+    """exp / log / erf over x with glibc (mode 0) or mfmath.h (mode 1)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    lib().oracle_libm_eval({"exp": 0, "log": 1, "erf": 2}[fn], int(mode), _ptr(x), _ptr(y), x.size)
+    return y
 
 
 class Oracle:

@@ -1,0 +1,86 @@
+"""The C ABI library: loads without a GPU, exports every symbol the header
+declares, and reports errors as status codes."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(__file__)), "include", "mfcfd.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char \*)\s*(mfcfd_\w+)\s*\(", text, re.M)))
+
+
+def test_exports_every_declared_symbol(mfcfd_lib):
+    L = mfcfd_lib.lib()
+    declared = header_functions()
+    assert len(declared) >= 18
+    for name in declared:
+        assert hasattr(L, name), name
+    assert set(declared) == set(mfcfd_lib.EXPORTS)
+
+
+def test_params_init_matches_parameter_module(mfcfd_lib):
+    from mfcfd.solver import params_for
+    import math
+    p = params_for(0.8, 2.0)
+    theta = 2.0 * (4.0 * math.atan(1.0)) / 180.0
+    assert p.power == 0.0 and p.vl_const == 2.0 and p.cfl == 5.0 and p.inner_iterations == 0
+    assert p.rho_inf == 1.0 and p.pr_inf == 1.0 / 1.4 and p.u3_inf == 0.0
+    assert p.u1_inf == 0.8 * math.cos(theta) and p.u2_inf == 0.8 * math.sin(theta)
+    assert p.split_capacity == 22 and p.sweep_mode == 0
+
+
+def test_strerror(mfcfd_lib):
+    L = mfcfd_lib.lib()
+    assert L.mfcfd_strerror(0) == b"ok"
+    assert L.mfcfd_strerror(8) == b"device wait timed out"
+    assert L.mfcfd_strerror(99) == b"unknown error"
+
+
+def _create(mfcfd_lib, cloud, **over):
+    from mfcfd.solver import Solver
+    return Solver(cloud, 0.4, 0.0, device=-1, **over)
+
+
+def test_bad_inputs_are_status_codes(mfcfd_lib, small_cloud):
+    import copy
+    from mfcfd._lib import MfcfdError
+    c = copy.deepcopy(small_cloud)
+    c.status = c.status.copy()
+    c.status[5] = 7
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, c)
+    assert e.value.code == 1 and "status" in str(e.value)
+    c = copy.deepcopy(small_cloud)
+    c.conn = c.conn.copy()
+    c.conn[3, 0] = c.n + 5
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, c)
+    assert e.value.code == 1
+    c = copy.deepcopy(small_cloud)
+    c.status = c.status.copy()
+    c.status[10] = 5
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, c)
+    assert e.value.code == 6
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, small_cloud, power=1.0)
+    assert e.value.code == 6
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, small_cloud, sweep_mode=3)
+    assert e.value.code == 1
+
+
+def test_host_only_handle_refuses_device_calls(mfcfd_lib, small_cloud):
+    from mfcfd._lib import MfcfdError
+    s = _create(mfcfd_lib, small_cloud)
+    with pytest.raises(MfcfdError):
+        s.initial_conditions()
+    with pytest.raises(MfcfdError):
+        s.residual_noalloc()
+    assert s.info()["n_points"] == small_cloud.n

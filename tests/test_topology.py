@@ -1,0 +1,88 @@
+"""Host set-up of the library (split stencils, alias order, sweep schedule)
+against the oracle and the golden fixtures; needs no GPU (device = -1)."""
+import numpy as np
+import pytest
+
+
+def _solver(cloud, **over):
+    from mfcfd.solver import Solver
+    return Solver(cloud, 0.4, 0.0, device=-1, **over)
+
+
+def test_stencils_and_alias_match_reference(oracle_lib):
+    from tests.test_oracle_golden import GOLDEN, golden_cloud
+    with np.load(GOLDEN) as z:
+        g = {k: z[k] for k in z.files}
+    c = golden_cloud(g)
+    s = _solver(c)
+    counts, lists = s.stencils(27)
+    assert np.array_equal(counts, g["split_counts"])
+    assert np.array_equal(lists, g["split_lists"])
+    a, p = s.alias()
+    assert np.array_equal(a, g["case0_glibc_alias"])
+    assert np.array_equal(p, g["case0_glibc_point_with_alias"])
+    assert s.info()["split_overflows"] > 0
+
+
+@pytest.mark.parametrize("shells,per,r1", [(8, 150, 1.7), (5, 60, 1.4)])
+def test_against_oracle_small_clouds(oracle_lib, shells, per, r1):
+    from mfcfd import cloud
+    c = cloud.shell_cloud(shells, per, r1=r1, seed=shells * 100 + per)
+    s = _solver(c)
+    o = oracle_lib.Oracle(c, 0.4, 0.0)
+    cs, ls = s.stencils(27)
+    co, lo = o.stencils(27)
+    assert np.array_equal(cs, co) and np.array_equal(ls, lo)
+    assert all(np.array_equal(x, y) for x, y in zip(s.alias(), o.alias()))
+
+
+def test_unlimited_capacity_has_no_overflow(small_cloud):
+    s = _solver(small_cloud, split_capacity=0)
+    assert s.info()["split_overflows"] == 0
+    counts, lists = s.stencils(27)
+    # every list is a subsequence of conn in conn order
+    for i in range(0, small_cloud.n, 37):
+        conn = list(small_cloud.conn[i, :small_cloud.nbhs[i]])
+        for d in range(6):
+            ent = list(lists[i, d, :counts[i, d]])
+            it = iter(conn)
+            assert all(e in it for e in ent)
+
+
+def test_schedule_respects_every_dependency(small_cloud):
+    """A point's level exceeds the level of every swept neighbour it reads
+    (lower alias forward, higher alias backward): the level-parallel sweep
+    then equals the reference's sequential one."""
+    s = _solver(small_cloud)
+    counts, lists = s.stencils(27)
+    alias, pwa = s.alias()
+    st = small_cloud.status
+    swept = np.zeros(small_cloud.n, bool)
+    pw = pwa[pwa > 0] - 1
+    swept[pw[(st[pw] == 0) | (st[pw] == 1)]] = True
+    for direction in (0, 1):
+        lv = s.levels(direction)
+        assert np.all((lv >= 0) == swept)
+        for p in np.nonzero(swept)[0]:
+            if st[p] == 1:
+                nb = [k for d in range(4) for k in lists[p, d, :counts[p, d]]]
+                nb += list(small_cloud.conn[p, :small_cloud.nbhs[p]])
+            else:
+                nb = [k for d in range(6) for k in lists[p, d, :counts[p, d]]]
+            nb = np.array(nb) - 1
+            dep = nb[(alias[nb] < alias[p]) if direction == 0 else (alias[nb] > alias[p])]
+            dep = dep[swept[dep]]
+            assert np.all(lv[dep] < lv[p])
+
+
+def test_point_one_is_not_swept(small_cloud):
+    """implicit_aliasing.f90:276-288: point 1's first neighbour also gets alias 1
+    and takes its slot in point_with_alias, so point 1 is never swept."""
+    s = _solver(small_cloud)
+    alias, pwa = s.alias()
+    assert alias[0] == 1
+    first = small_cloud.conn[0, 0]
+    assert alias[first - 1] == 1 and pwa[0] == first
+    assert 1 not in set(pwa.tolist())
+    assert pwa[-1] == 0
+    assert s.levels(0)[0] == -1
