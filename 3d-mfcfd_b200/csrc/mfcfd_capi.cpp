@@ -201,7 +201,8 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         *out = h;
         return MFCFD_ERR_UNSUPPORTED;
     }
-    if (P.sweep_mode != MFCFD_SWEEP_DATAFLOW && P.sweep_mode != MFCFD_SWEEP_LEVELS) {
+    if (P.sweep_mode != MFCFD_SWEEP_DATAFLOW && P.sweep_mode != MFCFD_SWEEP_LEVELS &&
+        P.sweep_mode != MFCFD_SWEEP_CHAINS) {
         h->err = "unknown sweep_mode";
         *out = h;
         return MFCFD_ERR_ARG;
@@ -263,6 +264,23 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.n_swept = (int)T.fwd_lvl_pts.size();
     d.max_width = T.max_level_width;
     d.sweep_mode = P.sweep_mode;
+    if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+        // about twice the widest level in warps, all co-resident
+        const int per_block = chain_warps_per_block();
+        int maxw = chain_max_warps(P.device);
+        int w = 2 * T.max_level_width;
+        w = (w + per_block - 1) / per_block * per_block;
+        if (w > maxw) w = maxw / per_block * per_block;
+        if (w < per_block) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+        ChainSchedule S;
+        build_chain_schedule(T, w, S);
+        d.ch_warps = w;
+        for (int dir = 0; dir < 2; ++dir) {
+            if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;
+            if ((rc = upload(h, &d.ch_pts[dir], S.pts[dir]))) return rc;
+            if ((rc = upload(h, &d.ch_own[dir], S.owner[dir]))) return rc;
+        }
+    }
     if ((rc = dalloc(h, &d.flag, n))) return rc;
     if ((rc = dalloc(h, &d.sweep_counter, 2))) return rc;
     if ((rc = dalloc(h, &d.err, 1))) return rc;

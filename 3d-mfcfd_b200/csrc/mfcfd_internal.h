@@ -70,6 +70,17 @@ struct Topology {
     std::vector<int32_t> wall_idx, outer_idx, interior_idx;   // 0-based, index order
 };
 
+// Static warp assignment of the sweep points for the chain schedule: warp
+// lists (CSR, each in topological order) and the owner warp of every point,
+// per direction.  A point goes to the warp that just processed its deepest
+// dependency when that warp is free to continue, so critical chains stay
+// inside one warp; otherwise to the warp idle the longest.
+struct ChainSchedule {
+    int warps = 0;
+    std::vector<int32_t> ptr[2], pts[2], owner[2];
+};
+void build_chain_schedule(const Topology &T, int warps, ChainSchedule &S);
+
 // Build everything above.  Returns MFCFD_OK or an error code with a message.
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
                    const double *y, const double *z, const double *tan1, const double *tan2,
@@ -114,6 +125,9 @@ struct DevCloud {
     int *flag;                    // per point ready flag (dataflow sweeps)
     int *sweep_counter;           // 2 work counters (forward, backward)
     int *err;                     // set when a bounded wait gave up
+    // chain schedule (per direction: 0 forward, 1 backward)
+    int ch_warps;
+    const int32_t *ch_ptr[2], *ch_pts[2], *ch_own[2];
     // state (Fortran layout, point-major)
     double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
     double *gold;                 // 30 per point: fluxes of prim in frame0
@@ -129,6 +143,8 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
                              double *U_next, double *q_next, cudaEvent_t *ev);
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
 int reduction_blocks(int n);
+int chain_max_warps(int device);      // co-resident warps of the chain sweep kernel
+int chain_warps_per_block();
 // Allocation-free residual (mfcfd_residual_noalloc); the current device must
 // be the handle's.
 int residual_noalloc(const DevCloud &d, cudaStream_t s, double *res_new, std::string &err);

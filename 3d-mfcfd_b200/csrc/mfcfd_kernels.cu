@@ -350,7 +350,12 @@ __device__ __forceinline__ void wait_ready(const int *flag, int epoch, int *err)
 constexpr int SW_META_BYTES = SWEEP_MAX_ENTRIES * 8;                // int2 (k, list|slot<<8)
 constexpr int SW_W_BYTES = SWEEP_MAX_ENTRIES * 3 * 8;               // weights
 constexpr int SW_T_DOUBLES = NDIR * MAX_SLOTS * 5;                  // >= SWEEP_MAX_ENTRIES * 5
-constexpr int SWEEP_SMEM_BYTES = SW_META_BYTES + SW_W_BYTES + SW_T_DOUBLES * 8;
+// chain schedule: the increment the warp published last (30 doubles) and its
+// point index, so the next point of a chain reads it from shared memory
+constexpr int SW_LAST_BYTES = 30 * 8 + 8;
+constexpr int SWEEP_SMEM_BYTES = SW_META_BYTES + SW_W_BYTES + SW_T_DOUBLES * 8 + SW_LAST_BYTES;
+
+enum SweepMode { MODE_LEVELS = 0, MODE_DATAFLOW = 1, MODE_CHAINS = 2 };
 static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
 
 // One point of the forward (LdelU) or backward (UdelU) sweep, processed by
@@ -364,11 +369,16 @@ static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
 // G(prim(U_k + dU_k)) - G(prim_k)), sum each list in list order (30 lanes:
 // list x component), solve the 3x3 systems, update dU and publish this
 // point's own increment, then raise its flag.
-template <bool DATAFLOW>
-__device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, char *smb, int epoch) {
+template <int MODE>
+__device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, char *smb, int epoch,
+                            int me = -1) {
+    constexpr bool DATAFLOW = MODE != MODE_LEVELS;
     int2 *M = reinterpret_cast<int2 *>(smb);
     double *Wt = reinterpret_cast<double *>(smb + SW_META_BYTES);
     double *T = reinterpret_cast<double *>(smb + SW_META_BYTES + SW_W_BYTES);
+    double *last_dg = reinterpret_cast<double *>(smb + SW_META_BYTES + SW_W_BYTES + SW_T_DOUBLES * 8);
+    int *last_p = reinterpret_cast<int *>(last_dg + 30);
+    const int32_t *own = d.ch_own[forward ? 0 : 1];
     const int cls = d.cls[p];
     const int off = forward ? d.fwd_off[p] : d.bwd_off[p];
     const uint8_t *cnt = (forward ? d.fwd_cnt : d.bwd_cnt) + (size_t)p * NDIR;
@@ -440,25 +450,38 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, ch
 
     // ---- phase B
     if (DATAFLOW) {
+        // points produced earlier by this warp (chain schedule) need no wait
+        bool waited = false;
         if (shared) {
             for (int j = lane; j < total; j += 32) {
                 const int k = M[j].x;
-                if (d.swept[k]) wait_ready(d.flag + k, epoch, d.err);
+                if (d.swept[k] && (MODE != MODE_CHAINS || own[k] != me)) {
+                    wait_ready(d.flag + k, epoch, d.err);
+                    waited = true;
+                }
             }
-        } else if (mine && d.swept[k_slot]) {
+        } else if (mine && d.swept[k_slot] && (MODE != MODE_CHAINS || own[k_slot] != me)) {
             wait_ready(d.flag + k_slot, epoch, d.err);
+            waited = true;
         }
-        fence_acquire_gpu();
+        if (MODE != MODE_CHAINS || __any_sync(FULL, waited)) fence_acquire_gpu();
         __syncwarp();
     }
 
     // ---- phase C
     if (shared) {
         const double *src = forward ? d.dgf : d.dgb;
+        const int lp = MODE == MODE_CHAINS ? *last_p : -1;
         for (int j = lane; j < total; j += 32) {
-            const double *gs = src + 30 * (size_t)M[j].x + 5 * (M[j].y & 255);
+            const int k = M[j].x, li = M[j].y & 255;
+            if (MODE == MODE_CHAINS && k == lp) {
 #pragma unroll
-            for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __ldcg(gs + cc);
+                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = last_dg[5 * li + cc];
+            } else {
+                const double *gs = src + 30 * (size_t)k + 5 * li;
+#pragma unroll
+                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __ldcg(gs + cc);
+            }
         }
     } else if (mine) {
         const double *dsrc = forward ? d.dUp : d.dUn;
@@ -533,15 +556,18 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, ch
             const double gnew = flux_component(dd, c, P, At, At, At);
             double *dst = forward ? d.dgf : d.dgb;
             dst[30 * (size_t)p + lane] = gnew - gold;
+            if (MODE == MODE_CHAINS) last_dg[lane] = gnew - gold;
         }
     }
     if (DATAFLOW) {
         // the warp barrier orders the lanes' stores before lane 0's release
         __syncwarp();
-        if (lane == 0) st_release_gpu(d.flag + p, epoch);
-    } else {
-        __syncwarp();
+        if (lane == 0) {
+            st_release_gpu(d.flag + p, epoch);
+            if (MODE == MODE_CHAINS) *last_p = d.shared_frame ? p : -1;
+        }
     }
+    __syncwarp();
 }
 
 // Level-synchronous sweep in one CTA: the points of a level are independent
@@ -557,7 +583,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep_levels(DevCloud d, i
     for (int l = 0; l < nl; ++l) {
         const int a = lptr[l], b = lptr[l + 1];
         for (int idx = a + warp; idx < b; idx += SWEEP_WARPS)
-            sweep_point<false>(d, lpts[idx], forward != 0, lane, smb, 0);
+            sweep_point<MODE_LEVELS>(d, lpts[idx], forward != 0, lane, smb, 0);
         __syncthreads();
     }
 }
@@ -581,8 +607,30 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
         if (lane == 0) idx = atomicAdd(counter, 1);
         idx = __shfl_sync(FULL, idx, 0);
         if (idx >= total) break;
-        sweep_point<true>(d, order[idx], forward != 0, lane, smb, epoch);
+        sweep_point<MODE_DATAFLOW>(d, order[idx], forward != 0, lane, smb, epoch);
     }
+}
+
+// Chain sweep: each warp walks its own list (fixed at set-up, topological
+// order) and waits only for neighbours produced by other warps.  All warps
+// are resident (cooperative launch), so the earliest unfinished point always
+// belongs to a warp that is working on it and can finish: the waits end.
+constexpr int CH_WARPS = 4;
+
+__global__ void __launch_bounds__(CH_WARPS * 32) k_sweep_chain(DevCloud d, int forward, int epoch) {
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    char *smb = reinterpret_cast<char *>(smem) + warp * SWEEP_SMEM_BYTES;
+    const int me = blockIdx.x * CH_WARPS + warp;
+    if (me >= d.ch_warps) return;
+    int *last_p = reinterpret_cast<int *>(smb + SWEEP_SMEM_BYTES - 8);
+    if (lane == 0) *last_p = -1;
+    __syncwarp();
+    const int dir = forward ? 0 : 1;
+    const int a = d.ch_ptr[dir][me], b = d.ch_ptr[dir][me + 1];
+    const int32_t *pts = d.ch_pts[dir];
+    for (int idx = a; idx < b; ++idx)
+        sweep_point<MODE_CHAINS>(d, pts[idx], forward != 0, lane, smb, epoch, me);
 }
 
 // ---------------------------------------------------------------- state update
@@ -724,6 +772,18 @@ int residual_noalloc(const DevCloud &d, cudaStream_t s, double *res_new, std::st
     return MFCFD_OK;
 }
 
+int chain_max_warps(int device) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaFuncSetAttribute(k_sweep_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         CH_WARPS * SWEEP_SMEM_BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain, CH_WARPS * 32,
+                                                  CH_WARPS * SWEEP_SMEM_BYTES);
+    return sms * per_sm * CH_WARPS;
+}
+
+int chain_warps_per_block() { return CH_WARPS; }
+
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s) {
     k_conserved_q<<<(d.n + 127) / 128, 128, 0, s>>>(d);
     return cudaGetLastError();
@@ -741,6 +801,8 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
                              SWEEP_WARPS * SWEEP_SMEM_BYTES);
         cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              DF_WARPS * SWEEP_SMEM_BYTES);
+        cudaFuncSetAttribute(k_sweep_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             CH_WARPS * SWEEP_SMEM_BYTES);
         g_attr_set = true;
     }
     // dataflow grid: about the widest level in warps (more warps only add
@@ -749,7 +811,13 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
     df_warps = df_warps < 64 ? 64 : (df_warps > 148 * 8 ? 148 * 8 : df_warps);
     const int df_blocks = (df_warps + DF_WARPS - 1) / DF_WARPS;
     auto sweep = [&](int forward) {
-        if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
+        if (d.sweep_mode == MFCFD_SWEEP_CHAINS) {
+            int epoch = forward ? d.epoch : d.epoch + 1;
+            DevCloud dc = d;
+            void *args[] = {&dc, &forward, &epoch};
+            cudaLaunchCooperativeKernel((void *)k_sweep_chain, dim3(d.ch_warps / CH_WARPS),
+                                        dim3(CH_WARPS * 32), args, CH_WARPS * SWEEP_SMEM_BYTES, s);
+        } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
         } else {
             cudaMemsetAsync(d.sweep_counter + (forward ? 0 : 1), 0, sizeof(int), s);

@@ -382,4 +382,64 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     return MFCFD_OK;
 }
 
+void build_chain_schedule(const Topology &T, int warps, ChainSchedule &S) {
+    S.warps = warps;
+    const int n = T.n;
+    for (int dir = 0; dir < 2; ++dir) {
+        const bool fwd = dir == 0;
+        const std::vector<int32_t> &lpts = fwd ? T.fwd_lvl_pts : T.bwd_lvl_pts;
+        const std::vector<int32_t> &level = fwd ? T.fwd_level : T.bwd_level;
+        const std::vector<int32_t> &off = fwd ? T.fwd_off : T.bwd_off;
+        const std::vector<SweepEntry> &ent = fwd ? T.fwd_ent : T.bwd_ent;
+        std::vector<int32_t> &owner = S.owner[dir];
+        owner.assign(n, -1);
+        std::vector<int32_t> last_point(warps, -1), last_level(warps, -1);
+        std::vector<std::vector<int32_t>> lists(warps);
+        // warps ordered by the level of their last point (lazy min-heap)
+        std::vector<std::pair<int, int>> heap;
+        auto cmp = [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+            return a.first > b.first || (a.first == b.first && a.second > b.second);
+        };
+        for (int w = 0; w < warps; ++w) heap.push_back({-1, w});
+        std::make_heap(heap.begin(), heap.end(), cmp);
+        for (int p : lpts) {           // level-major, a topological order
+            int best = -1, best_level = -1;
+            for (int e = off[p]; e < off[p + 1]; ++e) {
+                const int k = ent[e].k;
+                if (!T.swept[k]) continue;
+                const int w = owner[k];
+                const bool cont = last_point[w] == k;
+                if (level[k] > best_level || (level[k] == best_level && cont)) {
+                    best_level = level[k];
+                    best = k;
+                }
+            }
+            int w = -1;
+            if (best >= 0 && last_point[owner[best]] == best) {
+                w = owner[best];
+            } else {
+                while (true) {     // pop stale heap entries
+                    std::pop_heap(heap.begin(), heap.end(), cmp);
+                    auto top = heap.back();
+                    heap.pop_back();
+                    if (top.first == last_level[top.second]) { w = top.second; break; }
+                }
+            }
+            owner[p] = w;
+            lists[w].push_back(p);
+            last_point[w] = p;
+            last_level[w] = level[p];
+            heap.push_back({level[p], w});
+            std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+        S.ptr[dir].assign(warps + 1, 0);
+        S.pts[dir].clear();
+        for (int w = 0; w < warps; ++w) {
+            S.ptr[dir][w] = (int32_t)S.pts[dir].size();
+            S.pts[dir].insert(S.pts[dir].end(), lists[w].begin(), lists[w].end());
+        }
+        S.ptr[dir][warps] = (int32_t)S.pts[dir].size();
+    }
+}
+
 }  // namespace mfcfd

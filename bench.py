@@ -124,34 +124,42 @@ def dist_env():
 
 # ------------------------------------------------------------------ CPU side
 
-def _oracle_worker(args):
-    """One independent oracle solve (spawned process): time `steps` iterations."""
+def _cpu_worker(args):
+    """One independent CPU solve (spawned process): time `steps` iterations.
+
+    Runs the reference itself (its Fortran routines translated to C,
+    oracle/_ref/libref.so, glibc libm) when that build is present, else the
+    C++ restatement of it."""
     sys.path.insert(0, PKG)
     sys.path.insert(0, REPO)
     from mfcfd import cloud
-    from oracle import oracle
+    from oracle import oracle, ref_translated
     shells, per_shell, jitter, mach, aoa, seed, warm, steps = args
     c = cloud.shell_cloud(shells, per_shell, jitter=jitter, seed=seed)
-    o = oracle.Oracle(c, mach, aoa, libm=oracle.LIBM_GLIBC)
-    o.set_prim(cloud.initial_state(c, mach, aoa))
+    prim0 = cloud.initial_state(c, mach, aoa)
+    if ref_translated.available("glibc"):
+        o, kind = ref_translated.TranslatedReference(c, prim0, mach, aoa), "reference"
+    else:
+        o, kind = oracle.Oracle(c, mach, aoa, libm=oracle.LIBM_GLIBC), "port"
+        o.set_prim(prim0)
     for t in range(1, warm + 1):
         o.step(t)
     t0 = time.perf_counter()
     for t in range(warm + 1, warm + steps + 1):
         o.step(t)
-    return c.n, steps, time.perf_counter() - t0
+    return c.n, steps, time.perf_counter() - t0, kind
 
 
 def cpu_reference(procs, warm, steps, mach, aoa):
-    """Throughput of the CPU oracle: `procs` independent 62,400-point solves."""
+    """CPU throughput: `procs` independent solves of the 62,400-point sphere."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     job = (48, 1300, 0.02, mach, aoa, 1001, warm, steps)
     with ctx.Pool(procs) as pool:
-        res = pool.map(_oracle_worker, [job] * procs)
+        res = pool.map(_cpu_worker, [job] * procs)
     n = res[0][0]
     wall = max(r[2] for r in res)
-    return procs * n * steps / wall, wall / steps, n
+    return procs * n * steps / wall, wall / steps, n, res[0][3]
 
 
 # ------------------------------------------------------------------ main
@@ -174,17 +182,18 @@ def main():
         if rank != 0:
             return
         procs = max(1, min(os.cpu_count() or 1, 32))
-        value, sec_per_step, n = cpu_reference(procs, args.warmup, args.steps, wl["mach"], wl["aoa"])
-        sample = (f"CPU oracle (the reference's algorithm restated in C++, glibc libm, "
-                  f"-O2 -ffp-contract=off), {procs} independent solves of a {n}-point sphere "
-                  f"(M={wl['mach']}, alpha={wl['aoa']}), one iteration per step")
+        value, sec_per_step, n, kind = cpu_reference(procs, args.warmup, args.steps, wl["mach"], wl["aoa"])
+        what = ("the reference's Fortran routines translated to C (oracle/_ref), glibc libm"
+                if kind == "reference" else "the C++ restatement of the reference, glibc libm")
+        sample = (f"{what}, -O2 -ffp-contract=off; {procs} independent solves of a {n}-point "
+                  f"sphere (M={wl['mach']}, alpha={wl['aoa']}), one iteration per step")
         line = {"metric": metric, "value": value, "unit": "point-iters/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_step * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "impl": "reference",
                 "config": {"workload": args.workload, "sample_points": n},
                 "cpu_baseline": {"value": value, "unit": "point-iters/s", "cores": procs,
-                                 "kind": "port", "sample": sample},
+                                 "kind": kind, "sample": sample},
                 "e2e": {"value": value, "unit": "point-iters/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -271,10 +280,12 @@ def main():
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, sps, n = cpu_reference(1, 0, 3, wl["mach"], wl["aoa"])
-        cpu_base = {"value": v, "unit": "point-iters/s", "cores": 1, "kind": "port",
-                    "sample": f"CPU oracle (C++ restatement, glibc libm), one solve of a {n}-point "
-                              f"sphere (M={wl['mach']}, alpha={wl['aoa']}), 3 iterations, 1 thread"}
+        v, sps, n, kind = cpu_reference(1, 0, 3, wl["mach"], wl["aoa"])
+        what = ("the reference's Fortran routines translated to C (oracle/_ref), glibc libm"
+                if kind == "reference" else "the C++ restatement of the reference, glibc libm")
+        cpu_base = {"value": v, "unit": "point-iters/s", "cores": 1, "kind": kind,
+                    "sample": f"{what}; one solve of a {n}-point sphere (M={wl['mach']}, "
+                              f"alpha={wl['aoa']}), 3 iterations, 1 thread"}
 
     if rank == 0:
         line = {"metric": metric, "value": value, "unit": "point-iters/s", "n_gpus": world,

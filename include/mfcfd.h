@@ -89,6 +89,10 @@ typedef struct mfcfd_params {
  * levels; no device-side waits at all. */
 #define MFCFD_SWEEP_DATAFLOW  0
 #define MFCFD_SWEEP_LEVELS    1
+/* CHAINS: points are assigned to warps ahead of time so that a point usually
+ * runs on the warp that processed its deepest dependency; waits are needed
+ * only across warps.  One cooperative launch keeps all warps resident. */
+#define MFCFD_SWEEP_CHAINS    2
 
 typedef struct mfcfd_info {
     int32_t n_points;

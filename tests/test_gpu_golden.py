@@ -22,7 +22,7 @@ def golden():
         return {k: z[k] for k in z.files}
 
 
-@pytest.mark.parametrize("sweep_mode", [0, 1])
+@pytest.mark.parametrize("sweep_mode", [0, 1, 2])
 @pytest.mark.parametrize("case", [0, 1])
 def test_gpu_matches_reference_bitwise(golden, mfcfd_lib, case, sweep_mode):
     from mfcfd.solver import Solver

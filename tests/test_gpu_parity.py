@@ -31,7 +31,7 @@ def _field_ids(oracle_lib):
             for name in FIELDS]
 
 
-@pytest.mark.parametrize("sweep_mode", [0, 1])
+@pytest.mark.parametrize("sweep_mode", [0, 1, 2])
 @pytest.mark.parametrize("mach,aoa", [(0.4, 0.0), (0.8, 2.0)])
 def test_one_iteration_bitexact(small_cloud, oracle_lib, mfcfd_lib, mach, aoa, sweep_mode):
     s, o = _pair(small_cloud, mach, aoa, oracle_lib.LIBM_MFMATH, oracle_lib, sweep_mode)
@@ -48,7 +48,7 @@ def test_one_iteration_bitexact(small_cloud, oracle_lib, mfcfd_lib, mach, aoa, s
     assert abs(r_gpu[0] - r_cpu[0]) <= 1e-13 * abs(r_cpu[0])
 
 
-@pytest.mark.parametrize("sweep_mode", [0, 1])
+@pytest.mark.parametrize("sweep_mode", [0, 1, 2])
 def test_twenty_iterations_bitexact(small_cloud, oracle_lib, mfcfd_lib, sweep_mode):
     s, o = _pair(small_cloud, 0.4, 0.0, oracle_lib.LIBM_MFMATH, oracle_lib, sweep_mode)
     hist = s.q_lskum(20)
