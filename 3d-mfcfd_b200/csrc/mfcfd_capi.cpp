@@ -36,6 +36,7 @@ struct mfcfd_handle {
     double phase_ms[MFCFD_NPHASE] = {0};
     int64_t prof_iters = 0;
     int epoch = 1;        // ready-flag value of the next forward sweep (+1 backward)
+    int64_t chain_terms[3] = {0, 0, 0};   // chain schedule: ring, same-warp, cross-warp terms
 };
 
 namespace {
@@ -181,6 +182,7 @@ void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg) {
     p->split_capacity = 22;                         // data_structure.f90:83-88
     p->precision = MFCFD_PRECISION_FP64;
     p->device = 0;
+    p->sweep_mode = MFCFD_SWEEP_CHAINS;
 }
 
 int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, const double *x,
@@ -241,6 +243,28 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         }
     std::vector<int32_t> vnb(nbhs, nbhs + n), vconn((size_t)n * MAX_CONN, 0);
     for (size_t j = 0; j < vconn.size(); ++j) vconn[j] = conn[j] > 0 ? conn[j] - 1 : 0;
+    // chain schedule first: it marks the entry lists before they are uploaded
+    if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+        // about twice the widest level in warps, all co-resident
+        const int per_block = chain_warps_per_block();
+        int maxw = chain_max_warps(P.device);
+        int w = 2 * T.max_level_width;
+        w = (w + per_block - 1) / per_block * per_block;
+        if (w > maxw) w = maxw / per_block * per_block;
+        if (w < per_block) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+        ChainSchedule S;
+        build_chain_schedule(h->T, w, S);
+        d.ch_warps = w;
+        for (int dir = 0; dir < 2; ++dir) {
+            if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;
+            if ((rc = upload(h, &d.ch_pts[dir], S.pts[dir]))) return rc;
+            if ((rc = upload(h, &d.ch_own[dir], S.owner[dir]))) return rc;
+            if ((rc = upload(h, &d.ch_items[dir], S.items[dir]))) return rc;
+        }
+        h->chain_terms[0] = S.terms_ring;
+        h->chain_terms[1] = S.terms_local;
+        h->chain_terms[2] = S.terms_cross;
+    }
     std::vector<int32_t> order;
     order.insert(order.end(), T.wall_idx.begin(), T.wall_idx.end());
     order.insert(order.end(), T.interior_idx.begin(), T.interior_idx.end());
@@ -264,23 +288,6 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.n_swept = (int)T.fwd_lvl_pts.size();
     d.max_width = T.max_level_width;
     d.sweep_mode = P.sweep_mode;
-    if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
-        // about twice the widest level in warps, all co-resident
-        const int per_block = chain_warps_per_block();
-        int maxw = chain_max_warps(P.device);
-        int w = 2 * T.max_level_width;
-        w = (w + per_block - 1) / per_block * per_block;
-        if (w > maxw) w = maxw / per_block * per_block;
-        if (w < per_block) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
-        ChainSchedule S;
-        build_chain_schedule(T, w, S);
-        d.ch_warps = w;
-        for (int dir = 0; dir < 2; ++dir) {
-            if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;
-            if ((rc = upload(h, &d.ch_pts[dir], S.pts[dir]))) return rc;
-            if ((rc = upload(h, &d.ch_own[dir], S.owner[dir]))) return rc;
-        }
-    }
     if ((rc = dalloc(h, &d.flag, n))) return rc;
     if ((rc = dalloc(h, &d.sweep_counter, 2))) return rc;
     if ((rc = dalloc(h, &d.err, 1))) return rc;
@@ -442,6 +449,11 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
     info->split_overflows = T.split_overflows;
     info->shared_frame = T.shared_frame;
     info->device_bytes = h->bytes;
+    info->sweep_mode = h->P.sweep_mode;
+    info->chain_warps = h->d.ch_warps;
+    info->chain_terms_ring = h->chain_terms[0];
+    info->chain_terms_local = h->chain_terms[1];
+    info->chain_terms_cross = h->chain_terms[2];
     return MFCFD_OK;
 }
 

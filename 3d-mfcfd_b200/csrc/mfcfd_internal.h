@@ -70,16 +70,41 @@ struct Topology {
     std::vector<int32_t> wall_idx, outer_idx, interior_idx;   // 0-based, index order
 };
 
+// One point of a sweep as a warp of the chain schedule reads it: the point,
+// the offset of its terms, the term count of each list (5 bits per list) and
+// CI_* bits.  All of a point's staged inputs are addressed from this record.
+struct ChainItem {
+    int32_t p;
+    int32_t off;
+    uint32_t cnt;
+    uint32_t info;
+};
+enum : uint32_t {
+    CI_WALL = 1,      // wall point (LdelU counts its lists twice, zpos skipped)
+    CI_SHARED = 2,    // consumer in the shared frame (reads published increments)
+    CI_PUBLISH = 4,   // some consumer reads this point's increment from global memory
+    CI_RELEASE = 8,   // some consumer runs on another warp (raise the ready flag)
+};
+// Bits the chain schedule adds to SweepEntry::pad (bits 0-15: list, slot).
+constexpr int32_t ENT_WAIT = 1 << 16;   // producer runs on another warp: wait for its flag
+constexpr int32_t ENT_RING = 1 << 17;   // producer's increment is in the warp's ring
+constexpr int ENT_RING_SHIFT = 18;      // ring slot (4 bits)
+constexpr int CHAIN_RING = 8;           // increments a warp keeps in shared memory
+
 // Static warp assignment of the sweep points for the chain schedule: warp
-// lists (CSR, each in topological order) and the owner warp of every point,
-// per direction.  A point goes to the warp that just processed its deepest
-// dependency when that warp is free to continue, so critical chains stay
-// inside one warp; otherwise to the warp idle the longest.
+// lists (CSR, each in topological order), the owner warp of every point and
+// the per-point records, per direction.  A point goes to the warp that just
+// processed its deepest dependency when that warp is free to continue, so
+// critical chains stay inside one warp; otherwise to the warp idle the
+// longest.  The builder also marks each term of T's entry lists with where
+// its producer's increment comes from (ENT_* bits).
 struct ChainSchedule {
     int warps = 0;
     std::vector<int32_t> ptr[2], pts[2], owner[2];
+    std::vector<ChainItem> items[2];
+    int64_t terms_ring = 0, terms_local = 0, terms_cross = 0;   // swept producers
 };
-void build_chain_schedule(const Topology &T, int warps, ChainSchedule &S);
+void build_chain_schedule(Topology &T, int warps, ChainSchedule &S);
 
 // Build everything above.  Returns MFCFD_OK or an error code with a message.
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
@@ -128,6 +153,7 @@ struct DevCloud {
     // chain schedule (per direction: 0 forward, 1 backward)
     int ch_warps;
     const int32_t *ch_ptr[2], *ch_pts[2], *ch_own[2];
+    const ChainItem *ch_items[2];
     // state (Fortran layout, point-major)
     double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
     double *gold;                 // 30 per point: fluxes of prim in frame0

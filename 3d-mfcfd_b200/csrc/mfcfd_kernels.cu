@@ -346,86 +346,154 @@ __device__ __forceinline__ void wait_ready(const int *flag, int epoch, int *err)
     }
 }
 
-// Per-warp shared memory of the sweep kernels.
-constexpr int SW_META_BYTES = SWEEP_MAX_ENTRIES * 8;                // int2 (k, list|slot<<8)
-constexpr int SW_W_BYTES = SWEEP_MAX_ENTRIES * 3 * 8;               // weights
-constexpr int SW_T_DOUBLES = NDIR * MAX_SLOTS * 5;                  // >= SWEEP_MAX_ENTRIES * 5
-// chain schedule: the increment the warp published last (30 doubles) and its
-// point index, so the next point of a chain reads it from shared memory
-constexpr int SW_LAST_BYTES = 30 * 8 + 8;
-constexpr int SWEEP_SMEM_BYTES = SW_META_BYTES + SW_W_BYTES + SW_T_DOUBLES * 8 + SW_LAST_BYTES;
+// Per-warp shared memory of the sweep kernels.  SweepStage holds everything a
+// point reads that the sweep itself does not change (its terms, geometry,
+// fluxes of prim in the shared frame, D_inv, U, frame, slot table); it is
+// filled with cp.async, so the chain kernel loads the next point's stage
+// while it works on the current one.
+struct __align__(16) SweepStage {
+    SweepEntry ent[SWEEP_MAX_ENTRIES];
+    double geo[GEO_STRIDE];
+    double gold[32];
+    double U[6];
+    double base[6];
+    double frame[10];
+    double dinv[2];
+    int32_t slot_nbr[MAX_SLOTS];
+    uint8_t slot_mask[MAX_SLOTS];
+    uint32_t need;
+    int32_t pad[3];
+};
+constexpr int SW_T_DOUBLES = NDIR * MAX_SLOTS * 5;                  // term fluxes, >= SWEEP_MAX_ENTRIES * 5
+constexpr int SW_RING_DOUBLES = CHAIN_RING * 30;                    // chain: last published increments
+constexpr int SWEEP_SMEM_BYTES = SW_T_DOUBLES * 8 + (int)sizeof(SweepStage);   // one stage
+constexpr int CHAIN_SMEM_BYTES = SW_T_DOUBLES * 8 + SW_RING_DOUBLES * 8 + 2 * (int)sizeof(SweepStage);
+static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
+static_assert(sizeof(SweepStage) % 16 == 0 && SWEEP_SMEM_BYTES % 16 == 0 && CHAIN_SMEM_BYTES % 16 == 0,
+              "stage alignment");
 
 enum SweepMode { MODE_LEVELS = 0, MODE_DATAFLOW = 1, MODE_CHAINS = 2 };
-static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
+
+__device__ __forceinline__ void cp_async16(void *s, const void *g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(s)),
+                 "l"(g)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *s, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(s)),
+                 "l"(g)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *s, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(s)),
+                 "l"(g)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ int item_count(uint32_t cnt, int e) { return (int)((cnt >> (5 * e)) & 31u); }
+
+// The record of point p for the level and dataflow schedules (the chain
+// schedule reads precomputed ones).
+__device__ __forceinline__ ChainItem make_item(const DevCloud &d, int p, bool forward) {
+    ChainItem it;
+    it.p = p;
+    it.off = forward ? d.fwd_off[p] : d.bwd_off[p];
+    const uint8_t *cnt = (forward ? d.fwd_cnt : d.bwd_cnt) + (size_t)p * NDIR;
+    it.cnt = 0;
+#pragma unroll
+    for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[e] << (5 * e);
+    it.info = (d.cls[p] == CLS_WALL ? CI_WALL : 0u) | (d.consumer_shared[p] ? CI_SHARED : 0u) | CI_PUBLISH |
+              CI_RELEASE;
+    return it;
+}
+
+// Issue the cp.async copies of one point's stage (all lanes; caller commits).
+// Every source is 16-byte aligned for the 16-byte copies: entries are 32-byte
+// records, geo rows 384 bytes, gold rows 240 bytes, slot rows 128 / 32 bytes.
+__device__ __forceinline__ void stage_issue(const DevCloud &d, const ChainItem &it, bool forward, int lane,
+                                            SweepStage *st) {
+    const size_t p = (size_t)it.p;
+    int total = 0;
+#pragma unroll
+    for (int e = 0; e < NDIR; ++e) total += item_count(it.cnt, e);
+    const char *es = reinterpret_cast<const char *>((forward ? d.fwd_ent : d.bwd_ent) + it.off);
+    char *ed = reinterpret_cast<char *>(st->ent);
+    for (int j = lane; j < 2 * total; j += 32) cp_async16(ed + 16 * j, es + 16 * j);
+    if (lane < GEO_STRIDE / 2) cp_async16(st->geo + 2 * lane, d.geo + p * GEO_STRIDE + 2 * lane);
+    if (lane < 15) cp_async16(st->gold + 2 * lane, d.gold + 30 * p + 2 * lane);
+    if (lane < 5) {
+        cp_async8(st->U + lane, d.U + 5 * p + lane);
+        cp_async8(st->base + lane, (forward ? d.flux_res : d.dUp) + 5 * p + lane);
+    } else if (lane < 14) {
+        cp_async8(st->frame + (lane - 5), d.frame + 9 * p + (lane - 5));
+    } else if (lane == 14) {
+        cp_async8(st->dinv, d.dinv + p);
+    } else if (!(it.info & CI_SHARED)) {
+        if (lane < 23) cp_async16(st->slot_nbr + 4 * (lane - 15), d.slot_nbr + p * MAX_SLOTS + 4 * (lane - 15));
+        else if (lane < 25) cp_async16(st->slot_mask + 16 * (lane - 23), d.slot_mask + p * MAX_SLOTS + 16 * (lane - 23));
+        else if (lane == 25) cp_async4(&st->need, (forward ? d.fwd_need : d.bwd_need) + p);
+    }
+}
 
 // One point of the forward (LdelU) or backward (UdelU) sweep, processed by
-// one warp (implicit_forward_and_reverse_sweeps.f90:30-37 / :61-68).
+// one warp (implicit_forward_and_reverse_sweeps.f90:30-37 / :61-68), from its
+// stage in shared memory.
 //
-// Phase A (no dependency on the sweep): stage the point's terms (neighbour,
-// list, weights) in shared memory and load everything else the point needs;
-// points outside the shared frame also evaluate G(prim_k) of their
-// neighbours here.  Phase B: wait for the ready flags of the neighbours whose
-// increments are read.  Phase C: read the published increments (or evaluate
-// G(prim(U_k + dU_k)) - G(prim_k)), sum each list in list order (30 lanes:
-// list x component), solve the 3x3 systems, update dU and publish this
-// point's own increment, then raise its flag.
+// Phase A (no dependency on the sweep): points outside the shared frame
+// evaluate G(prim_k) of their neighbours.  Phase B: wait for the ready flags
+// of the neighbours whose increments are read.  Phase C: read the published
+// increments (or evaluate G(prim(U_k + dU_k)) - G(prim_k)), sum each list in
+// list order (30 lanes: list x component), solve the 3x3 systems, update dU
+// and publish this point's own increment, then raise its flag.
+//
+// The chain schedule reads increments that this warp published recently from
+// `ring` (slot in the term's ENT_RING bits) and writes its own to ring slot
+// `ring_slot`; it waits only on terms marked ENT_WAIT.
 template <int MODE>
-__device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, char *smb, int epoch,
-                            int me = -1) {
+__device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepStage *st, bool forward, int lane,
+                            double *T, double *ring, int ring_slot, int epoch, int me) {
     constexpr bool DATAFLOW = MODE != MODE_LEVELS;
-    int2 *M = reinterpret_cast<int2 *>(smb);
-    double *Wt = reinterpret_cast<double *>(smb + SW_META_BYTES);
-    double *T = reinterpret_cast<double *>(smb + SW_META_BYTES + SW_W_BYTES);
-    double *last_dg = reinterpret_cast<double *>(smb + SW_META_BYTES + SW_W_BYTES + SW_T_DOUBLES * 8);
-    int *last_p = reinterpret_cast<int *>(last_dg + 30);
-    const int32_t *own = d.ch_own[forward ? 0 : 1];
-    const int cls = d.cls[p];
-    const int off = forward ? d.fwd_off[p] : d.bwd_off[p];
-    const uint8_t *cnt = (forward ? d.fwd_cnt : d.bwd_cnt) + (size_t)p * NDIR;
-    const SweepEntry *ent = forward ? d.fwd_ent : d.bwd_ent;
+    const int p = it.p;
+    const bool wall = (it.info & CI_WALL) != 0;
+    const bool shared = (it.info & CI_SHARED) != 0;
+    const int cls = wall ? CLS_WALL : CLS_INTERIOR;   // swept points are wall or interior
+    const SweepEntry *E = st->ent;
     const int dd = lane / 5, c = lane - 5 * (lane / 5);
     int total = 0, lo = 0, hi = 0;
 #pragma unroll
     for (int e = 0; e < NDIR; ++e) {
-        const int ce = cnt[e];
+        const int ce = item_count(it.cnt, e);
         if (e < dd) lo += ce;
         if (e <= dd) hi += ce;
         total += ce;
     }
-    const bool shared = d.consumer_shared[p] != 0;
 
     // ---- phase A
-    for (int j = lane; j < total; j += 32) {
-        const SweepEntry &E = ent[off + j];
-        M[j] = make_int2(E.k, E.pad);
-        Wt[3 * j + 0] = E.w[0];
-        Wt[3 * j + 1] = E.w[1];
-        Wt[3 * j + 2] = E.w[2];
-    }
     double g[7] = {0, 0, 0, 0, 0, 0, 1.0};
     double gold = 0.0;
     if (lane < 30) {
-        const double *gp = d.geo + (size_t)p * GEO_STRIDE + dd * 8;
 #pragma unroll
-        for (int r = 0; r < 7; ++r) g[r] = gp[r];
-        gold = d.gold[30 * (size_t)p + lane];
+        for (int r = 0; r < 7; ++r) g[r] = st->geo[dd * 8 + r];
+        gold = st->gold[lane];
     }
     double dinv = 0.0, base5 = 0.0;
     if (lane < 5) {
-        dinv = d.dinv[p];
-        base5 = forward ? d.flux_res[5 * (size_t)p + lane] : d.dUp[5 * (size_t)p + lane];
+        dinv = st->dinv[0];
+        base5 = st->base[lane];
     }
     double Up[5];
 #pragma unroll
-    for (int r = 0; r < 5; ++r) Up[r] = d.U[5 * (size_t)p + r];
+    for (int r = 0; r < 5; ++r) Up[r] = st->U[r];
     Frame Fp;
-    load_frame(d.frame + 9 * (size_t)p, Fp);
-    const uint32_t need = shared ? 0u : (forward ? d.fwd_need[p] : d.bwd_need[p]);
+    load_frame(st->frame, Fp);
+    const uint32_t need = shared ? 0u : st->need;
     const bool mine = !shared && (need >> lane) & 1u;
     int k_slot = 0, mask_slot = 0;
     if (mine) {
-        k_slot = d.slot_nbr[(size_t)p * MAX_SLOTS + lane];
-        mask_slot = d.slot_mask[(size_t)p * MAX_SLOTS + lane];
+        k_slot = st->slot_nbr[lane];
+        mask_slot = st->slot_mask[lane];
         double po[5];
 #pragma unroll
         for (int r = 0; r < 5; ++r) po[r] = d.prim[5 * (size_t)k_slot + r];
@@ -446,37 +514,37 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, ch
             for (int cc = 0; cc < 5; ++cc) T[(e * MAX_SLOTS + lane) * 5 + cc] = flux_component(kind, cc, Po, Ao);
         }
     }
-    __syncwarp();
 
     // ---- phase B
     if (DATAFLOW) {
-        // points produced earlier by this warp (chain schedule) need no wait
+        // chain schedule: points produced by this warp need no wait
         bool waited = false;
         if (shared) {
             for (int j = lane; j < total; j += 32) {
-                const int k = M[j].x;
-                if (d.swept[k] && (MODE != MODE_CHAINS || own[k] != me)) {
+                const int k = E[j].k;
+                const bool w = MODE == MODE_CHAINS ? (E[j].pad & ENT_WAIT) != 0 : d.swept[k] != 0;
+                if (w) {
                     wait_ready(d.flag + k, epoch, d.err);
                     waited = true;
                 }
             }
-        } else if (mine && d.swept[k_slot] && (MODE != MODE_CHAINS || own[k_slot] != me)) {
+        } else if (mine && d.swept[k_slot] && (MODE != MODE_CHAINS || d.ch_own[forward ? 0 : 1][k_slot] != me)) {
             wait_ready(d.flag + k_slot, epoch, d.err);
             waited = true;
         }
         if (MODE != MODE_CHAINS || __any_sync(FULL, waited)) fence_acquire_gpu();
-        __syncwarp();
     }
+    __syncwarp();
 
     // ---- phase C
     if (shared) {
         const double *src = forward ? d.dgf : d.dgb;
-        const int lp = MODE == MODE_CHAINS ? *last_p : -1;
         for (int j = lane; j < total; j += 32) {
-            const int k = M[j].x, li = M[j].y & 255;
-            if (MODE == MODE_CHAINS && k == lp) {
+            const int k = E[j].k, pad = E[j].pad, li = pad & 255;
+            if (MODE == MODE_CHAINS && (pad & ENT_RING)) {
+                const double *rs = ring + 30 * ((pad >> ENT_RING_SHIFT) & 15) + 5 * li;
 #pragma unroll
-                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = last_dg[5 * li + cc];
+                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = rs[cc];
             } else {
                 const double *gs = src + 30 * (size_t)k + 5 * li;
 #pragma unroll
@@ -515,10 +583,10 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, ch
     double sx = 0.0, sy = 0.0, sz = 0.0;
     if (lane < 30) {
         for (int jj = lo; jj < hi; ++jj) {
-            const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + (M[jj].y >> 8)) * 5 + c];
-            sx = sx + t * Wt[3 * jj + 0];
-            sy = sy + t * Wt[3 * jj + 1];
-            sz = sz + t * Wt[3 * jj + 2];
+            const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
+            sx = sx + t * E[jj].w[0];
+            sy = sy + t * E[jj].w[1];
+            sz = sz + t * E[jj].w[2];
         }
     }
     double G = 0.0;
@@ -529,7 +597,7 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, ch
     double dnew = 0.0;
     if (lane < 5) {
         double lu;
-        if (cls == CLS_WALL) lu = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+        if (wall) lu = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
         else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
         if (forward) {
             dnew = -(dinv * (base5 + lu));
@@ -553,21 +621,31 @@ __device__ void sweep_point(const DevCloud &d, int p, bool forward, int lane, ch
             flux_pre(pn, F0, P);
             AxisTerms At;
             axis_terms(P, dd >> 1, At);
-            const double gnew = flux_component(dd, c, P, At, At, At);
-            double *dst = forward ? d.dgf : d.dgb;
-            dst[30 * (size_t)p + lane] = gnew - gold;
-            if (MODE == MODE_CHAINS) last_dg[lane] = gnew - gold;
+            const double v = flux_component(dd, c, P, At, At, At) - gold;
+            if (it.info & CI_PUBLISH) (forward ? d.dgf : d.dgb)[30 * (size_t)p + lane] = v;
+            if (MODE == MODE_CHAINS) ring[30 * ring_slot + lane] = v;
         }
     }
-    if (DATAFLOW) {
+    if (DATAFLOW && (it.info & CI_RELEASE)) {
         // the warp barrier orders the lanes' stores before lane 0's release
         __syncwarp();
-        if (lane == 0) {
-            st_release_gpu(d.flag + p, epoch);
-            if (MODE == MODE_CHAINS) *last_p = d.shared_frame ? p : -1;
-        }
+        if (lane == 0) st_release_gpu(d.flag + p, epoch);
     }
     __syncwarp();
+}
+
+// Stage one point synchronously and sweep it (level and dataflow schedules).
+template <int MODE>
+__device__ __forceinline__ void sweep_point_sync(const DevCloud &d, int p, bool forward, int lane, char *smb,
+                                                 int epoch) {
+    double *T = reinterpret_cast<double *>(smb);
+    SweepStage *st = reinterpret_cast<SweepStage *>(smb + SW_T_DOUBLES * 8);
+    const ChainItem it = make_item(d, p, forward);
+    stage_issue(d, it, forward, lane, st);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncwarp();
+    sweep_point<MODE>(d, it, st, forward, lane, T, nullptr, 0, epoch, -1);
 }
 
 // Level-synchronous sweep in one CTA: the points of a level are independent
@@ -583,7 +661,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep_levels(DevCloud d, i
     for (int l = 0; l < nl; ++l) {
         const int a = lptr[l], b = lptr[l + 1];
         for (int idx = a + warp; idx < b; idx += SWEEP_WARPS)
-            sweep_point<MODE_LEVELS>(d, lpts[idx], forward != 0, lane, smb, 0);
+            sweep_point_sync<MODE_LEVELS>(d, lpts[idx], forward != 0, lane, smb, 0);
         __syncthreads();
     }
 }
@@ -607,30 +685,48 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
         if (lane == 0) idx = atomicAdd(counter, 1);
         idx = __shfl_sync(FULL, idx, 0);
         if (idx >= total) break;
-        sweep_point<MODE_DATAFLOW>(d, order[idx], forward != 0, lane, smb, epoch);
+        sweep_point_sync<MODE_DATAFLOW>(d, order[idx], forward != 0, lane, smb, epoch);
     }
 }
 
-// Chain sweep: each warp walks its own list (fixed at set-up, topological
-// order) and waits only for neighbours produced by other warps.  All warps
-// are resident (cooperative launch), so the earliest unfinished point always
-// belongs to a warp that is working on it and can finish: the waits end.
+// Chain sweep: each warp walks its own list of point records (fixed at
+// set-up, topological order) and waits only for neighbours produced by other
+// warps.  The stage of the next point is copied in while the current one is
+// processed (two stage buffers).  All warps are resident (cooperative
+// launch), so the earliest unfinished point always belongs to a warp that is
+// working on it and can finish: the waits end.
 constexpr int CH_WARPS = 4;
 
 __global__ void __launch_bounds__(CH_WARPS * 32) k_sweep_chain(DevCloud d, int forward, int epoch) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    char *smb = reinterpret_cast<char *>(smem) + warp * SWEEP_SMEM_BYTES;
+    char *smb = reinterpret_cast<char *>(smem) + warp * CHAIN_SMEM_BYTES;
+    double *T = reinterpret_cast<double *>(smb);
+    double *ring = T + SW_T_DOUBLES;
+    SweepStage *stg = reinterpret_cast<SweepStage *>(ring + SW_RING_DOUBLES);
     const int me = blockIdx.x * CH_WARPS + warp;
     if (me >= d.ch_warps) return;
-    int *last_p = reinterpret_cast<int *>(smb + SWEEP_SMEM_BYTES - 8);
-    if (lane == 0) *last_p = -1;
-    __syncwarp();
     const int dir = forward ? 0 : 1;
     const int a = d.ch_ptr[dir][me], b = d.ch_ptr[dir][me + 1];
-    const int32_t *pts = d.ch_pts[dir];
-    for (int idx = a; idx < b; ++idx)
-        sweep_point<MODE_CHAINS>(d, pts[idx], forward != 0, lane, smb, epoch, me);
+    if (a >= b) return;
+    const ChainItem *items = d.ch_items[dir];
+    ChainItem cur = items[a];
+    stage_issue(d, cur, forward != 0, lane, &stg[0]);
+    cp_async_commit();
+    ChainItem nxt = a + 1 < b ? items[a + 1] : cur;
+    for (int idx = a; idx < b; ++idx) {
+        const int s = (idx - a) & 1;
+        cp_async_wait_all();
+        __syncwarp();
+        if (idx + 1 < b) {
+            stage_issue(d, nxt, forward != 0, lane, &stg[s ^ 1]);
+            cp_async_commit();
+        }
+        const ChainItem after = idx + 2 < b ? items[idx + 2] : nxt;
+        sweep_point<MODE_CHAINS>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING, epoch, me);
+        cur = nxt;
+        nxt = after;
+    }
 }
 
 // ---------------------------------------------------------------- state update
@@ -776,9 +872,9 @@ int chain_max_warps(int device) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaFuncSetAttribute(k_sweep_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         CH_WARPS * SWEEP_SMEM_BYTES);
+                         CH_WARPS * CHAIN_SMEM_BYTES);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain, CH_WARPS * 32,
-                                                  CH_WARPS * SWEEP_SMEM_BYTES);
+                                                  CH_WARPS * CHAIN_SMEM_BYTES);
     return sms * per_sm * CH_WARPS;
 }
 
@@ -802,7 +898,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
         cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              DF_WARPS * SWEEP_SMEM_BYTES);
         cudaFuncSetAttribute(k_sweep_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             CH_WARPS * SWEEP_SMEM_BYTES);
+                             CH_WARPS * CHAIN_SMEM_BYTES);
         g_attr_set = true;
     }
     // dataflow grid: about the widest level in warps (more warps only add
@@ -816,7 +912,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
             DevCloud dc = d;
             void *args[] = {&dc, &forward, &epoch};
             cudaLaunchCooperativeKernel((void *)k_sweep_chain, dim3(d.ch_warps / CH_WARPS),
-                                        dim3(CH_WARPS * 32), args, CH_WARPS * SWEEP_SMEM_BYTES, s);
+                                        dim3(CH_WARPS * 32), args, CH_WARPS * CHAIN_SMEM_BYTES, s);
         } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
         } else {

@@ -382,7 +382,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     return MFCFD_OK;
 }
 
-void build_chain_schedule(const Topology &T, int warps, ChainSchedule &S) {
+void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
     S.warps = warps;
     const int n = T.n;
     for (int dir = 0; dir < 2; ++dir) {
@@ -439,6 +439,51 @@ void build_chain_schedule(const Topology &T, int warps, ChainSchedule &S) {
             S.pts[dir].insert(S.pts[dir].end(), lists[w].begin(), lists[w].end());
         }
         S.ptr[dir][warps] = (int32_t)S.pts[dir].size();
+
+        // where each term's producer increment comes from, and which points
+        // must publish to global memory / raise their ready flag
+        std::vector<int32_t> pos(n, -1);
+        for (int w = 0; w < warps; ++w)
+            for (int i = S.ptr[dir][w]; i < S.ptr[dir][w + 1]; ++i) pos[S.pts[dir][i]] = i - S.ptr[dir][w];
+        std::vector<SweepEntry> &went = fwd ? T.fwd_ent : T.bwd_ent;
+        std::vector<uint8_t> publish(n, 0), release(n, 0);
+        for (int p : lpts) {
+            const bool shared = T.consumer_shared[p] != 0;
+            for (int e = off[p]; e < off[p + 1]; ++e) {
+                SweepEntry &E = went[e];
+                E.pad &= 0xffff;
+                const int k = E.k;
+                if (!T.swept[k]) continue;   // fixed increment written before the sweep
+                const bool same = owner[k] == owner[p];
+                if (!same) release[k] = 1;
+                if (!shared) continue;       // reads dU of its slots directly
+                if (same && pos[p] - pos[k] <= CHAIN_RING) {
+                    E.pad |= ENT_RING | ((pos[k] % CHAIN_RING) << ENT_RING_SHIFT);
+                    ++S.terms_ring;
+                } else {
+                    publish[k] = 1;
+                    if (same) {
+                        ++S.terms_local;
+                    } else {
+                        E.pad |= ENT_WAIT;
+                        ++S.terms_cross;
+                    }
+                }
+            }
+        }
+        const std::vector<uint8_t> &cnt = fwd ? T.fwd_cnt : T.bwd_cnt;
+        std::vector<ChainItem> &items = S.items[dir];
+        items.resize(S.pts[dir].size());
+        for (size_t i = 0; i < items.size(); ++i) {
+            const int p = S.pts[dir][i];
+            ChainItem &it = items[i];
+            it.p = p;
+            it.off = off[p];
+            it.cnt = 0;
+            for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[(size_t)p * NDIR + e] << (5 * e);
+            it.info = (T.cls[p] == CLS_WALL ? CI_WALL : 0u) | (T.consumer_shared[p] ? CI_SHARED : 0u) |
+                      (publish[p] ? CI_PUBLISH : 0u) | (release[p] ? CI_RELEASE : 0u);
+        }
     }
 }
 

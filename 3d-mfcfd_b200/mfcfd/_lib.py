@@ -52,7 +52,9 @@ class Info(ctypes.Structure):
                 ("n_supersonic", ctypes.c_int32), ("n_levels_forward", ctypes.c_int32),
                 ("n_levels_backward", ctypes.c_int32), ("max_level_width", ctypes.c_int32),
                 ("split_overflows", ctypes.c_int32), ("shared_frame", ctypes.c_int32),
-                ("device_bytes", ctypes.c_int64)]
+                ("device_bytes", ctypes.c_int64), ("sweep_mode", ctypes.c_int32),
+                ("chain_warps", ctypes.c_int32), ("chain_terms_ring", ctypes.c_int64),
+                ("chain_terms_local", ctypes.c_int64), ("chain_terms_cross", ctypes.c_int64)]
 
 
 class MfcfdError(RuntimeError):

@@ -172,7 +172,7 @@ def main():
     ap.add_argument("--impl", default="mfcfd", choices=["mfcfd", "reference"])
     ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sweep-mode", type=int, default=0, help="0 dataflow, 1 levels")
+    ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     wl = WORKLOADS[args.workload]

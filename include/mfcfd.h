@@ -78,11 +78,11 @@ typedef struct mfcfd_params {
     int32_t precision;        /* MFCFD_PRECISION_FP64 */
     int32_t device;           /* CUDA device ordinal; -1 builds a host-only handle
                                  (stencils, alias, schedule) without device state */
-    int32_t sweep_mode;       /* MFCFD_SWEEP_DATAFLOW (default) or MFCFD_SWEEP_LEVELS */
+    int32_t sweep_mode;       /* MFCFD_SWEEP_CHAINS (default), _DATAFLOW or _LEVELS */
     int32_t reserved[7];
 } mfcfd_params;
 
-/* LU-SGS sweep schedules.  Both give the reference's sequential result bit
+/* LU-SGS sweep schedules.  All give the reference's sequential result bit
  * for bit.  DATAFLOW: warps on all SMs take points in topological order and
  * wait (bounded) on per-point ready flags of the neighbours they read.
  * LEVELS: one CTA processes level after level with a block barrier between
@@ -103,6 +103,13 @@ typedef struct mfcfd_info {
     int32_t split_overflows;      /* list entries written past split_capacity */
     int32_t shared_frame;         /* 1 if interior points share one frame */
     int64_t device_bytes;         /* device memory held by the handle */
+    int32_t sweep_mode;           /* MFCFD_SWEEP_* of the handle */
+    int32_t chain_warps;          /* CHAINS: warps of the schedule, else 0 */
+    /* CHAINS: sweep terms (both directions) of shared-frame consumers whose
+     * producer is a swept point, by where the increment is read: the warp's
+     * shared-memory ring, global memory written by the same warp, or global
+     * memory after a wait on another warp's flag */
+    int64_t chain_terms_ring, chain_terms_local, chain_terms_cross;
 } mfcfd_info;
 
 typedef struct mfcfd_handle mfcfd_handle;

@@ -32,7 +32,7 @@ def test_params_init_matches_parameter_module(mfcfd_lib):
     assert p.power == 0.0 and p.vl_const == 2.0 and p.cfl == 5.0 and p.inner_iterations == 0
     assert p.rho_inf == 1.0 and p.pr_inf == 1.0 / 1.4 and p.u3_inf == 0.0
     assert p.u1_inf == 0.8 * math.cos(theta) and p.u2_inf == 0.8 * math.sin(theta)
-    assert p.split_capacity == 22 and p.sweep_mode == 0
+    assert p.split_capacity == 22 and p.sweep_mode == 2   # MFCFD_SWEEP_CHAINS
 
 
 def test_strerror(mfcfd_lib):
