@@ -35,7 +35,6 @@ struct mfcfd_handle {
     std::vector<cudaEvent_t> ev;          // (MFCFD_NPHASE+1) per iteration slot
     double phase_ms[MFCFD_NPHASE] = {0};
     int64_t prof_iters = 0;
-    int epoch = 1;        // ready-flag value of the next forward sweep (+1 backward)
     int64_t chain_terms[3] = {0, 0, 0};   // chain schedule: ring, same-warp, cross-warp terms
 };
 
@@ -115,9 +114,6 @@ int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist)
             DevCloud dc = h->d;
             dc.U = h->U_buf[h->cur];
             dc.q = h->q_buf[h->cur];
-            dc.epoch = h->epoch;
-            h->epoch += 2;
-            if (h->epoch > (1 << 30)) h->epoch = 1;   // flags are reset below on wrap
             cudaEvent_t *ev = h->profiling ? &h->ev[(size_t)j * (MFCFD_NPHASE + 1)] : nullptr;
             cudaError_t e = launch_iteration(dc, j, h->stream, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], ev);
             if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
@@ -128,11 +124,8 @@ int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist)
         CK(cudaMemcpyAsync(res.data(), h->d.res_dev, sizeof(double) * chunk, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaMemcpyAsync(&err_flag, h->d.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        if (h->epoch == 1) CK(cudaMemsetAsync(h->d.flag, 0, sizeof(int) * (size_t)h->d.n, h->stream));
         if (err_flag) {
             CK(cudaMemsetAsync(h->d.err, 0, sizeof(int), h->stream));
-            CK(cudaMemsetAsync(h->d.flag, 0, sizeof(int) * (size_t)h->d.n, h->stream));
-            h->epoch = 1;
             CK(cudaStreamSynchronize(h->stream));
             return fail(h, MFCFD_ERR_TIMEOUT, "a sweep wait ran out; the iteration results are invalid");
         }
@@ -288,10 +281,8 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.n_swept = (int)T.fwd_lvl_pts.size();
     d.max_width = T.max_level_width;
     d.sweep_mode = P.sweep_mode;
-    if ((rc = dalloc(h, &d.flag, n))) return rc;
     if ((rc = dalloc(h, &d.sweep_counter, 2))) return rc;
     if ((rc = dalloc(h, &d.err, 1))) return rc;
-    CK(cudaMemsetAsync(d.flag, 0, sizeof(int) * (size_t)n, h->stream));
     CK(cudaMemsetAsync(d.sweep_counter, 0, sizeof(int) * 2, h->stream));
     CK(cudaMemsetAsync(d.err, 0, sizeof(int), h->stream));
     size_t n5 = (size_t)n * 5;
@@ -299,7 +290,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     AL(d.prim, n5); AL(h->U_buf[0], n5); AL(h->U_buf[1], n5); AL(h->q_buf[0], n5);
     AL(h->q_buf[1], n5); AL(d.qm, (size_t)n * 10); AL(d.dq, (size_t)n * 15);
     AL(d.delt, n); AL(d.flux_res, n5); AL(d.dUp, n5); AL(d.dUn, n5); AL(d.dinv, n);
-    AL(d.gold, (size_t)n * 30); AL(d.dgf, (size_t)n * 30); AL(d.dgb, (size_t)n * 30);
+    AL(d.gold, (size_t)n * 30); AL(d.dgf, (size_t)n * DG_STRIDE); AL(d.dgb, (size_t)n * DG_STRIDE);
     AL(d.res_sqr, n); AL(d.partial, 1024); AL(d.res_dev, h->res_cap);
 #undef AL
     CK(cudaMemsetAsync(d.dUp, 0, n5 * 8, h->stream));

@@ -83,13 +83,15 @@ enum : uint32_t {
     CI_WALL = 1,      // wall point (LdelU counts its lists twice, zpos skipped)
     CI_SHARED = 2,    // consumer in the shared frame (reads published increments)
     CI_PUBLISH = 4,   // some consumer reads this point's increment from global memory
-    CI_RELEASE = 8,   // some consumer runs on another warp (raise the ready flag)
 };
 // Bits the chain schedule adds to SweepEntry::pad (bits 0-15: list, slot).
-constexpr int32_t ENT_WAIT = 1 << 16;   // producer runs on another warp: wait for its flag
 constexpr int32_t ENT_RING = 1 << 17;   // producer's increment is in the warp's ring
 constexpr int ENT_RING_SHIFT = 18;      // ring slot (4 bits)
 constexpr int CHAIN_RING = 8;           // increments a warp keeps in shared memory
+// Published flux increments: per point 6 lists x (5 components + 1 pad), so
+// every list's record starts on a 16-byte boundary (cp.async.cg copies).
+constexpr int DG_STRIDE = 36;
+constexpr int DG_LIST = 6;
 
 // Static warp assignment of the sweep points for the chain schedule: warp
 // lists (CSR, each in topological order), the owner warp of every point and
@@ -146,10 +148,8 @@ struct DevCloud {
     int n_swept;                  // points in each sweep order
     int max_width;                // widest sweep level
     int sweep_mode;               // MFCFD_SWEEP_*
-    int epoch;                    // ready-flag value of this iteration's forward sweep
-    int *flag;                    // per point ready flag (dataflow sweeps)
     int *sweep_counter;           // 2 work counters (forward, backward)
-    int *err;                     // set when a bounded wait gave up
+    int *err;                     // set when a bounded poll gave up
     // chain schedule (per direction: 0 forward, 1 backward)
     int ch_warps;
     const int32_t *ch_ptr[2], *ch_pts[2], *ch_own[2];
@@ -157,7 +157,7 @@ struct DevCloud {
     // state (Fortran layout, point-major)
     double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
     double *gold;                 // 30 per point: fluxes of prim in frame0
-    double *dgf, *dgb;            // 30 per point: published flux increments
+    double *dgf, *dgb;            // DG_STRIDE per point: published flux increments
     double *res_sqr;              // per point (residual sum terms)
     double *partial;              // reduction scratch
     double *res_dev;              // per-iteration res_new history

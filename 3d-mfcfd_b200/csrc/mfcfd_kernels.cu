@@ -4,10 +4,12 @@
  * One iteration (fpi_solver.f90:27-36) is this launch sequence:
  *   k_qderiv      q_derivatives + timestep_delt     thread per point
  *   k_flux        eval_flux_residual                warp per point
+ *   k_pending     sweep hand-off words set to "not yet published"
  *   k_dinv_gold   D_inv, fluxes of prim in the shared interior frame,
  *                 flux increments of points the sweeps do not update
- *   k_sweep_df x2 forward / backward LU-SGS sweep   dataflow over all SMs
- *                 (k_sweep_levels: one CTA, level by level)
+ *   k_sweep_chain x2  forward / backward LU-SGS sweep: static warp chains
+ *                 on all SMs (k_sweep_df: dynamic topological order;
+ *                 k_sweep_levels: one CTA, level by level)
  *   k_update      state_update_implicit + next iteration's U and q
  *   k_reduce_*    res_new (deterministic two-pass sum)
  * State stays resident in HBM in the reference's point-major layout.
@@ -31,6 +33,9 @@ constexpr int SWEEP_THREADS = 512;
 constexpr int SWEEP_WARPS = SWEEP_THREADS / 32;
 constexpr int RED_THREADS = 256;
 constexpr unsigned FULL = 0xffffffffu;
+// "not yet published" value of the sweeps' hand-off words (see the LU-SGS
+// sweep section): a signalling-NaN bit pattern no arithmetic result has
+constexpr unsigned long long DU_PENDING = 0xFFF4DEADBEEF0001ull;
 
 // ---------------------------------------------------------------- U and q
 
@@ -250,11 +255,30 @@ __device__ __forceinline__ void flux6_frame0(const DevCloud &d, const double pri
         for (int c = 0; c < 5; ++c) out[dd * 5 + c] = flux_component(dd, c, P, A);
 }
 
+// Before the sweeps: every published-increment word, and dU of every swept
+// point, is set to DU_PENDING (coalesced grid-stride fill).
+__global__ void k_pending(DevCloud d) {
+    const double pend = __longlong_as_double((long long)DU_PENDING);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t ng = (size_t)d.n * DG_STRIDE, nu = (size_t)d.n * 5;
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < ng; w += stride) {
+        d.dgf[w] = pend;
+        d.dgb[w] = pend;
+    }
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < nu; w += stride) {
+        if (d.swept[w / 5]) {
+            d.dUp[w] = pend;
+            d.dUn[w] = pend;
+        }
+    }
+}
+
 // implicit_D_inv_interior.f90:46-417 / implicit_D_inv_wall.f90:45-356 with
 // the geometry-only sums precomputed; plus the sweep inputs that do not
 // depend on the sweep: G(prim_k) in the shared frame for every point and the
 // published increment G(prim(U_k + dU_k)) - G(prim_k) of points the sweeps
-// never update (outer points, point 1).
+// never update (outer points, point 1), over the DU_PENDING that k_pending
+// wrote there.
 __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
@@ -299,8 +323,9 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
 #pragma unroll
             for (int c = 0; c < 30; ++c) {
                 const double v = gnew[c] - gold[c];
-                d.dgf[30 * (size_t)i + c] = v;
-                d.dgb[30 * (size_t)i + c] = v;
+                const size_t o = DG_STRIDE * (size_t)i + DG_LIST * (c / 5) + c % 5;
+                d.dgf[o] = v;
+                d.dgb[o] = v;
             }
         }
     }
@@ -308,42 +333,47 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
 
 // ---------------------------------------------------------------- LU-SGS sweeps
 
-__device__ __forceinline__ int ld_relaxed_gpu(const int *p) {
-    int v;
-    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+// Hand-off of increments between warps.  Before the sweeps, k_dinv_gold sets
+// dUp, dUn, dgf and dgb of every swept point to DU_PENDING, a signalling-NaN
+// bit pattern that no arithmetic result has (arithmetic NaNs are quiet).  A
+// producer stores its values with strong (relaxed, gpu-scope) 8-byte stores;
+// a consumer polls the 8-byte words it needs with strong loads until none is
+// DU_PENDING.  Each word is single-copy atomic, so a value read that is not
+// DU_PENDING is the final one: no flags and no fences are needed.
+
+__device__ __forceinline__ unsigned long long ld_relaxed_b64(const double *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-
-// Acquire side of the flag handshake: after a relaxed read has seen the
-// producer's release store, this fence orders the reads that follow.
-__device__ __forceinline__ void fence_acquire_gpu() {
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+__device__ __forceinline__ void ld_relaxed_v2(const double *p, unsigned long long &a, unsigned long long &b) {
+    asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_f64(double *p, double v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
 
-__device__ __forceinline__ void st_release_gpu(int *p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
+// Polls give up after SPIN_LIMIT rounds (about a second), or soon after
+// another lane gave up: the failure goes to *err (the host reports
+// MFCFD_ERR_TIMEOUT and the iteration's results are invalid).
+constexpr int SPIN_LIMIT = 1 << 21;
 
-// Bounded wait for a neighbour's ready flag.  Polls with relaxed loads (an
-// acquire load per poll would invalidate the SM's L1 every time); the caller
-// issues one fence_acquire_gpu() afterwards.  Gives up after SPIN_LIMIT polls
-// (seconds), or at once when another warp already gave up: it records the
-// failure in *err (the host reports MFCFD_ERR_TIMEOUT) and returns.
-constexpr int SPIN_LIMIT = 1 << 25;
-
-__device__ __forceinline__ void wait_ready(const int *flag, int epoch, int *err) {
-    int it = 0;
-    while (ld_relaxed_gpu(flag) != epoch) {
-        ++it;
-        if ((it & 4095) == 0) {
-            if (*(volatile int *)err) return;
-            __nanosleep(64);
-        }
-        if (it > SPIN_LIMIT) {
-            atomicExch(err, 1);
-            return;
-        }
+__device__ __forceinline__ bool spin_continue(int &it, int *err) {
+    ++it;
+    if ((it & 1023) == 0) {
+        if (*(volatile int *)err) return false;
+        __nanosleep(64);
     }
+    if (it > SPIN_LIMIT) {
+        atomicExch(err, 1);
+        return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool ready5(const unsigned long long v[5]) {
+    return v[0] != DU_PENDING && v[1] != DU_PENDING && v[2] != DU_PENDING && v[3] != DU_PENDING &&
+           v[4] != DU_PENDING;
 }
 
 // Per-warp shared memory of the sweep kernels.  SweepStage holds everything a
@@ -367,8 +397,9 @@ struct __align__(16) SweepStage {
 constexpr int SW_T_DOUBLES = NDIR * MAX_SLOTS * 5;                  // term fluxes, >= SWEEP_MAX_ENTRIES * 5
 constexpr int SW_RING_DOUBLES = CHAIN_RING * 30;                    // chain: last published increments
 constexpr int SWEEP_SMEM_BYTES = SW_T_DOUBLES * 8 + (int)sizeof(SweepStage);   // one stage
-constexpr int CHAIN_SMEM_BYTES = SW_T_DOUBLES * 8 + SW_RING_DOUBLES * 8 + 2 * (int)sizeof(SweepStage);
+constexpr int CHAIN_SMEM_BYTES = (SW_T_DOUBLES + SW_RING_DOUBLES) * 8 + 2 * (int)sizeof(SweepStage);
 static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
+static_assert(SWEEP_MAX_ENTRIES <= 96, "entries are polled in three passes of 32");
 static_assert(sizeof(SweepStage) % 16 == 0 && SWEEP_SMEM_BYTES % 16 == 0 && CHAIN_SMEM_BYTES % 16 == 0,
               "stage alignment");
 
@@ -404,8 +435,7 @@ __device__ __forceinline__ ChainItem make_item(const DevCloud &d, int p, bool fo
     it.cnt = 0;
 #pragma unroll
     for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[e] << (5 * e);
-    it.info = (d.cls[p] == CLS_WALL ? CI_WALL : 0u) | (d.consumer_shared[p] ? CI_SHARED : 0u) | CI_PUBLISH |
-              CI_RELEASE;
+    it.info = (d.cls[p] == CLS_WALL ? CI_WALL : 0u) | (d.consumer_shared[p] ? CI_SHARED : 0u) | CI_PUBLISH;
     return it;
 }
 
@@ -442,19 +472,21 @@ __device__ __forceinline__ void stage_issue(const DevCloud &d, const ChainItem &
 // stage in shared memory.
 //
 // Phase A (no dependency on the sweep): points outside the shared frame
-// evaluate G(prim_k) of their neighbours.  Phase B: wait for the ready flags
-// of the neighbours whose increments are read.  Phase C: read the published
-// increments (or evaluate G(prim(U_k + dU_k)) - G(prim_k)), sum each list in
-// list order (30 lanes: list x component), solve the 3x3 systems, update dU
-// and publish this point's own increment, then raise its flag.
+// evaluate G(prim_k) of their neighbours.  Phase B: collect the neighbours'
+// increments as they are published (points in the shared frame: the
+// published flux increments; others: dU_k, then G(prim(U_k + dU_k)) -
+// G(prim_k)).  Phase C: sum each list in list order (30 lanes: list x
+// component), solve the 3x3 systems, update dU and publish this point's own
+// flux increment.
 //
-// The chain schedule reads increments that this warp published recently from
-// `ring` (slot in the term's ENT_RING bits) and writes its own to ring slot
-// `ring_slot`; it waits only on terms marked ENT_WAIT.
+// The chain schedule reads increments that this warp published within its
+// last CHAIN_RING points from `ring` (slot in the term's ENT_RING bits) and
+// writes its own to ring slot `ring_slot`; a point publishes to global memory
+// only if some consumer reads it there (CI_PUBLISH).
 template <int MODE>
 __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepStage *st, bool forward, int lane,
-                            double *T, double *ring, int ring_slot, int epoch, int me) {
-    constexpr bool DATAFLOW = MODE != MODE_LEVELS;
+                            double *T, double *ring, int ring_slot) {
+    constexpr bool CHAINS = MODE == MODE_CHAINS;
     const int p = it.p;
     const bool wall = (it.info & CI_WALL) != 0;
     const bool shared = (it.info & CI_SHARED) != 0;
@@ -516,46 +548,57 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     }
 
     // ---- phase B
-    if (DATAFLOW) {
-        // chain schedule: points produced by this warp need no wait
-        bool waited = false;
-        if (shared) {
-            for (int j = lane; j < total; j += 32) {
-                const int k = E[j].k;
-                const bool w = MODE == MODE_CHAINS ? (E[j].pad & ENT_WAIT) != 0 : d.swept[k] != 0;
-                if (w) {
-                    wait_ready(d.flag + k, epoch, d.err);
-                    waited = true;
-                }
-            }
-        } else if (mine && d.swept[k_slot] && (MODE != MODE_CHAINS || d.ch_own[forward ? 0 : 1][k_slot] != me)) {
-            wait_ready(d.flag + k_slot, epoch, d.err);
-            waited = true;
-        }
-        if (MODE != MODE_CHAINS || __any_sync(FULL, waited)) fence_acquire_gpu();
-    }
-    __syncwarp();
-
-    // ---- phase C
     if (shared) {
+        // lane owns entries lane, lane+32, lane+64; all their loads are in
+        // flight together, re-polling only the ones still pending
         const double *src = forward ? d.dgf : d.dgb;
-        for (int j = lane; j < total; j += 32) {
-            const int k = E[j].k, pad = E[j].pad, li = pad & 255;
-            if (MODE == MODE_CHAINS && (pad & ENT_RING)) {
-                const double *rs = ring + 30 * ((pad >> ENT_RING_SHIFT) & 15) + 5 * li;
+        uint32_t pend = 0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int j = lane + 32 * q;
+            if (j >= total) continue;
+            const int pad = E[j].pad;
+            if (CHAINS && (pad & ENT_RING)) {
+                const double *rs = ring + 30 * ((pad >> ENT_RING_SHIFT) & 15) + 5 * (pad & 255);
 #pragma unroll
                 for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = rs[cc];
             } else {
-                const double *gs = src + 30 * (size_t)k + 5 * li;
-#pragma unroll
-                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __ldcg(gs + cc);
+                pend |= 1u << q;
             }
         }
+        int spins = 0;
+        while (pend) {
+            unsigned long long v[3][5];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (!((pend >> q) & 1u)) continue;
+                const int j = lane + 32 * q;
+                const double *gs = src + DG_STRIDE * (size_t)E[j].k + DG_LIST * (E[j].pad & 255);
+                ld_relaxed_v2(gs, v[q][0], v[q][1]);
+                ld_relaxed_v2(gs + 2, v[q][2], v[q][3]);
+                v[q][4] = ld_relaxed_b64(gs + 4);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                if (!((pend >> q) & 1u) || !ready5(v[q])) continue;
+                const int j = lane + 32 * q;
+#pragma unroll
+                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __longlong_as_double(v[q][cc]);
+                pend &= ~(1u << q);
+            }
+            if (pend && !spin_continue(spins, d.err)) break;
+        }
     } else if (mine) {
-        const double *dsrc = forward ? d.dUp : d.dUn;
+        const double *dsrc = (forward ? d.dUp : d.dUn) + 5 * (size_t)k_slot;
+        unsigned long long v[5];
+        int spins = 0;
+        do {
+#pragma unroll
+            for (int r = 0; r < 5; ++r) v[r] = ld_relaxed_b64(dsrc + r);
+        } while (!ready5(v) && spin_continue(spins, d.err));
         double U[5], pn[5];
 #pragma unroll
-        for (int r = 0; r < 5; ++r) U[r] = __ldcg(dsrc + 5 * (size_t)k_slot + r) + d.U[5 * (size_t)k_slot + r];
+        for (int r = 0; r < 5; ++r) U[r] = __longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r];
         Frame Fk;
         load_frame(d.frame + 9 * (size_t)k_slot, Fk);
         conserved_to_primitive(U, Fk, pn);
@@ -580,6 +623,8 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         }
     }
     __syncwarp();
+
+    // ---- phase C
     double sx = 0.0, sy = 0.0, sz = 0.0;
     if (lane < 30) {
         for (int jj = lo; jj < hi; ++jj) {
@@ -601,10 +646,10 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
         if (forward) {
             dnew = -(dinv * (base5 + lu));
-            d.dUp[5 * (size_t)p + lane] = dnew;
+            st_relaxed_f64(d.dUp + 5 * (size_t)p + lane, dnew);
         } else {
             dnew = base5 - dinv * lu;
-            d.dUn[5 * (size_t)p + lane] = dnew;
+            st_relaxed_f64(d.dUn + 5 * (size_t)p + lane, dnew);
         }
     }
     if (d.shared_frame) {
@@ -622,22 +667,17 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
             AxisTerms At;
             axis_terms(P, dd >> 1, At);
             const double v = flux_component(dd, c, P, At, At, At) - gold;
-            if (it.info & CI_PUBLISH) (forward ? d.dgf : d.dgb)[30 * (size_t)p + lane] = v;
-            if (MODE == MODE_CHAINS) ring[30 * ring_slot + lane] = v;
+            if (it.info & CI_PUBLISH)
+                st_relaxed_f64((forward ? d.dgf : d.dgb) + DG_STRIDE * (size_t)p + DG_LIST * dd + c, v);
+            if (CHAINS) ring[30 * ring_slot + lane] = v;
         }
-    }
-    if (DATAFLOW && (it.info & CI_RELEASE)) {
-        // the warp barrier orders the lanes' stores before lane 0's release
-        __syncwarp();
-        if (lane == 0) st_release_gpu(d.flag + p, epoch);
     }
     __syncwarp();
 }
 
 // Stage one point synchronously and sweep it (level and dataflow schedules).
 template <int MODE>
-__device__ __forceinline__ void sweep_point_sync(const DevCloud &d, int p, bool forward, int lane, char *smb,
-                                                 int epoch) {
+__device__ __forceinline__ void sweep_point_sync(const DevCloud &d, int p, bool forward, int lane, char *smb) {
     double *T = reinterpret_cast<double *>(smb);
     SweepStage *st = reinterpret_cast<SweepStage *>(smb + SW_T_DOUBLES * 8);
     const ChainItem it = make_item(d, p, forward);
@@ -645,12 +685,12 @@ __device__ __forceinline__ void sweep_point_sync(const DevCloud &d, int p, bool 
     cp_async_commit();
     cp_async_wait_all();
     __syncwarp();
-    sweep_point<MODE>(d, it, st, forward, lane, T, nullptr, 0, epoch, -1);
+    sweep_point<MODE>(d, it, st, forward, lane, T, nullptr, 0);
 }
 
 // Level-synchronous sweep in one CTA: the points of a level are independent
 // (none reads another's increment), so warps take them in parallel and a
-// block barrier separates levels.
+// block barrier separates levels; every poll succeeds at once.
 __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep_levels(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -661,19 +701,18 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep_levels(DevCloud d, i
     for (int l = 0; l < nl; ++l) {
         const int a = lptr[l], b = lptr[l + 1];
         for (int idx = a + warp; idx < b; idx += SWEEP_WARPS)
-            sweep_point_sync<MODE_LEVELS>(d, lpts[idx], forward != 0, lane, smb, 0);
+            sweep_point_sync<MODE_LEVELS>(d, lpts[idx], forward != 0, lane, smb);
         __syncthreads();
     }
 }
 
 // Dataflow sweep over many SMs: each warp takes the next point of the
-// level-major (topological) order from a global counter and waits for the
-// ready flags of the neighbours it reads.  A point's dependencies are always
-// taken before it by warps that are already running, so the waits end; each
-// is bounded anyway (wait_ready).
+// level-major (topological) order from a global counter and polls for the
+// increments it reads.  A point's dependencies are always taken before it by
+// warps that are already running, so the polls end; each is bounded anyway.
 constexpr int DF_WARPS = 4;
 
-__global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forward, int epoch) {
+__global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char *smb = reinterpret_cast<char *>(smem) + warp * SWEEP_SMEM_BYTES;
@@ -685,19 +724,18 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
         if (lane == 0) idx = atomicAdd(counter, 1);
         idx = __shfl_sync(FULL, idx, 0);
         if (idx >= total) break;
-        sweep_point_sync<MODE_DATAFLOW>(d, order[idx], forward != 0, lane, smb, epoch);
+        sweep_point_sync<MODE_DATAFLOW>(d, order[idx], forward != 0, lane, smb);
     }
 }
 
 // Chain sweep: each warp walks its own list of point records (fixed at
-// set-up, topological order) and waits only for neighbours produced by other
-// warps.  The stage of the next point is copied in while the current one is
-// processed (two stage buffers).  All warps are resident (cooperative
-// launch), so the earliest unfinished point always belongs to a warp that is
-// working on it and can finish: the waits end.
+// set-up, topological order).  The stage of the next point is copied in
+// while the current one is processed (two stage buffers).  All warps are
+// resident (cooperative launch), so the earliest unfinished point always
+// belongs to a warp that is working on it and can finish: the polls end.
 constexpr int CH_WARPS = 4;
 
-__global__ void __launch_bounds__(CH_WARPS * 32) k_sweep_chain(DevCloud d, int forward, int epoch) {
+__global__ void __launch_bounds__(CH_WARPS * 32) k_sweep_chain(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char *smb = reinterpret_cast<char *>(smem) + warp * CHAIN_SMEM_BYTES;
@@ -723,7 +761,7 @@ __global__ void __launch_bounds__(CH_WARPS * 32) k_sweep_chain(DevCloud d, int f
             cp_async_commit();
         }
         const ChainItem after = idx + 2 < b ? items[idx + 2] : nxt;
-        sweep_point<MODE_CHAINS>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING, epoch, me);
+        sweep_point<MODE_CHAINS>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING);
         cur = nxt;
         nxt = after;
     }
@@ -908,17 +946,15 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
     const int df_blocks = (df_warps + DF_WARPS - 1) / DF_WARPS;
     auto sweep = [&](int forward) {
         if (d.sweep_mode == MFCFD_SWEEP_CHAINS) {
-            int epoch = forward ? d.epoch : d.epoch + 1;
             DevCloud dc = d;
-            void *args[] = {&dc, &forward, &epoch};
+            void *args[] = {&dc, &forward};
             cudaLaunchCooperativeKernel((void *)k_sweep_chain, dim3(d.ch_warps / CH_WARPS),
                                         dim3(CH_WARPS * 32), args, CH_WARPS * CHAIN_SMEM_BYTES, s);
         } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
         } else {
             cudaMemsetAsync(d.sweep_counter + (forward ? 0 : 1), 0, sizeof(int), s);
-            k_sweep_df<<<df_blocks, DF_WARPS * 32, DF_WARPS * SWEEP_SMEM_BYTES, s>>>(
-                d, forward, forward ? d.epoch : d.epoch + 1);
+            k_sweep_df<<<df_blocks, DF_WARPS * 32, DF_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
         }
     };
     auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
@@ -928,6 +964,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
     const int fblocks = (n + FLUX_WARPS - 1) / FLUX_WARPS;
     k_flux<<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
     mark(2);
+    k_pending<<<148 * 8, 256, 0, s>>>(d);
     k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);
     mark(3);
     sweep(1);

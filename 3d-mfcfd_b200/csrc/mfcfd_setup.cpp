@@ -441,12 +441,12 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
         S.ptr[dir][warps] = (int32_t)S.pts[dir].size();
 
         // where each term's producer increment comes from, and which points
-        // must publish to global memory / raise their ready flag
+        // must publish to global memory
         std::vector<int32_t> pos(n, -1);
         for (int w = 0; w < warps; ++w)
             for (int i = S.ptr[dir][w]; i < S.ptr[dir][w + 1]; ++i) pos[S.pts[dir][i]] = i - S.ptr[dir][w];
         std::vector<SweepEntry> &went = fwd ? T.fwd_ent : T.bwd_ent;
-        std::vector<uint8_t> publish(n, 0), release(n, 0);
+        std::vector<uint8_t> publish(n, 0);
         for (int p : lpts) {
             const bool shared = T.consumer_shared[p] != 0;
             for (int e = off[p]; e < off[p + 1]; ++e) {
@@ -455,19 +455,14 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
                 const int k = E.k;
                 if (!T.swept[k]) continue;   // fixed increment written before the sweep
                 const bool same = owner[k] == owner[p];
-                if (!same) release[k] = 1;
                 if (!shared) continue;       // reads dU of its slots directly
                 if (same && pos[p] - pos[k] <= CHAIN_RING) {
                     E.pad |= ENT_RING | ((pos[k] % CHAIN_RING) << ENT_RING_SHIFT);
                     ++S.terms_ring;
                 } else {
                     publish[k] = 1;
-                    if (same) {
-                        ++S.terms_local;
-                    } else {
-                        E.pad |= ENT_WAIT;
-                        ++S.terms_cross;
-                    }
+                    if (same) ++S.terms_local;
+                    else ++S.terms_cross;
                 }
             }
         }
@@ -482,7 +477,7 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
             it.cnt = 0;
             for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[(size_t)p * NDIR + e] << (5 * e);
             it.info = (T.cls[p] == CLS_WALL ? CI_WALL : 0u) | (T.consumer_shared[p] ? CI_SHARED : 0u) |
-                      (publish[p] ? CI_PUBLISH : 0u) | (release[p] ? CI_RELEASE : 0u);
+                      (publish[p] ? CI_PUBLISH : 0u);
         }
     }
 }

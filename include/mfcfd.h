@@ -84,14 +84,14 @@ typedef struct mfcfd_params {
 
 /* LU-SGS sweep schedules.  All give the reference's sequential result bit
  * for bit.  DATAFLOW: warps on all SMs take points in topological order and
- * wait (bounded) on per-point ready flags of the neighbours they read.
- * LEVELS: one CTA processes level after level with a block barrier between
- * levels; no device-side waits at all. */
+ * poll (bounded) for the increments of the neighbours they read.  LEVELS: one
+ * CTA processes level after level with a block barrier between levels. */
 #define MFCFD_SWEEP_DATAFLOW  0
 #define MFCFD_SWEEP_LEVELS    1
 /* CHAINS: points are assigned to warps ahead of time so that a point usually
- * runs on the warp that processed its deepest dependency; waits are needed
- * only across warps.  One cooperative launch keeps all warps resident. */
+ * runs on the warp that processed its deepest dependency, which hands its
+ * increment over in shared memory; other neighbours are polled for.  One
+ * cooperative launch keeps all warps resident. */
 #define MFCFD_SWEEP_CHAINS    2
 
 typedef struct mfcfd_info {
@@ -108,7 +108,7 @@ typedef struct mfcfd_info {
     /* CHAINS: sweep terms (both directions) of shared-frame consumers whose
      * producer is a swept point, by where the increment is read: the warp's
      * shared-memory ring, global memory written by the same warp, or global
-     * memory after a wait on another warp's flag */
+     * memory written by another warp */
     int64_t chain_terms_ring, chain_terms_local, chain_terms_cross;
 } mfcfd_info;
 
