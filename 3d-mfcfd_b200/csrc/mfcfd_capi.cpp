@@ -21,6 +21,8 @@ struct mfcfd_handle {
     Topology T;
     DevCloud d;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;          // flux residual beside the chain forward sweep
+    cudaEvent_t fork = nullptr, join = nullptr;
     double *U_buf[2] = {nullptr, nullptr};
     double *q_buf[2] = {nullptr, nullptr};
     int cur = 0;          // U/q buffer the next iteration reads
@@ -84,10 +86,16 @@ int upload(mfcfd_handle *h, const T **dst, const std::vector<T> &src) {
 
 void release(mfcfd_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->side) cudaStreamSynchronize(h->side);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
     for (void *p : h->allocs) cudaFree(p);
     h->allocs.clear();
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
+    h->fork = h->join = nullptr;
+    if (h->side) cudaStreamDestroy(h->side);
+    h->side = nullptr;
     if (h->stream) cudaStreamDestroy(h->stream);
     h->stream = nullptr;
 }
@@ -115,7 +123,8 @@ int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist)
             dc.U = h->U_buf[h->cur];
             dc.q = h->q_buf[h->cur];
             cudaEvent_t *ev = h->profiling ? &h->ev[(size_t)j * (MFCFD_NPHASE + 1)] : nullptr;
-            cudaError_t e = launch_iteration(dc, j, h->stream, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], ev);
+            const IterStreams st{h->stream, h->side, h->fork, h->join};
+            cudaError_t e = launch_iteration(dc, j, st, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], ev);
             if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
             h->last = h->cur;
             h->cur = 1 - h->cur;
@@ -132,9 +141,16 @@ int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist)
         if (h->profiling) {
             for (int j = 0; j < chunk; ++j) {
                 const cudaEvent_t *ev = &h->ev[(size_t)j * (MFCFD_NPHASE + 1)];
+                // event pairs per phase; under the chain schedule the flux
+                // residual (ended by event 2, side stream) starts at event 3
+                // and runs beside the forward sweep, after k_pending (1-3)
+                static const int kSeq[MFCFD_NPHASE][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}};
+                static const int kFused[MFCFD_NPHASE][2] = {{0, 1}, {3, 2}, {1, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}};
+                const bool fused = h->d.sweep_mode == MFCFD_SWEEP_CHAINS;
                 for (int ph = 0; ph < MFCFD_NPHASE; ++ph) {
                     float ms = 0.f;
-                    CK(cudaEventElapsedTime(&ms, ev[ph], ev[ph + 1]));
+                    const int *pr = fused ? kFused[ph] : kSeq[ph];
+                    CK(cudaEventElapsedTime(&ms, ev[pr[0]], ev[pr[1]]));
                     h->phase_ms[ph] += ms;
                 }
             }
@@ -214,7 +230,16 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     if (P.device < 0) return MFCFD_OK;   // host-only handle: set-up results, no device state
 
     if (cudaSetDevice(P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
-    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    {
+        // the main stream outranks the side stream, so the chain sweep's
+        // blocks are placed before the concurrent flux kernel's
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatest));
+        CK(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, least));
+        CK(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming));
+    }
 
     DevCloud &d = h->d;
     std::memset(&d, 0, sizeof d);
@@ -239,15 +264,16 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     // chain schedule first: it marks the entry lists before they are uploaded
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
         // about twice the widest level in warps, all co-resident
-        const int per_block = chain_warps_per_block();
-        int maxw = chain_max_warps(P.device);
-        int w = 2 * T.max_level_width;
-        w = (w + per_block - 1) / per_block * per_block;
-        if (w > maxw) w = maxw / per_block * per_block;
-        if (w < per_block) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+        int wpb = 0, blocks = 0;
+        const int w = chain_shape(P.device, 2 * T.max_level_width, &wpb, &blocks);
+        if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
         ChainSchedule S;
         build_chain_schedule(h->T, w, S);
         d.ch_warps = w;
+        d.ch_wpb = wpb;
+        std::vector<int32_t> pre;
+        build_pre_order(T, pre);
+        if ((rc = upload(h, &d.pre_order, pre))) return rc;
         for (int dir = 0; dir < 2; ++dir) {
             if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;
             if ((rc = upload(h, &d.ch_pts[dir], S.pts[dir]))) return rc;

@@ -107,6 +107,7 @@ struct ChainSchedule {
     int64_t terms_ring = 0, terms_local = 0, terms_cross = 0;   // swept producers
 };
 void build_chain_schedule(Topology &T, int warps, ChainSchedule &S);
+void build_pre_order(const Topology &T, std::vector<int32_t> &order);
 
 // Build everything above.  Returns MFCFD_OK or an error code with a message.
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
@@ -151,7 +152,8 @@ struct DevCloud {
     int *sweep_counter;           // 2 work counters (forward, backward)
     int *err;                     // set when a bounded poll gave up
     // chain schedule (per direction: 0 forward, 1 backward)
-    int ch_warps;
+    int ch_warps, ch_wpb;         // warps and warps per block
+    const int32_t *pre_order;     // all points, forward sweep order first (fused flux)
     const int32_t *ch_ptr[2], *ch_pts[2], *ch_own[2];
     const ChainItem *ch_items[2];
     // state (Fortran layout, point-major)
@@ -163,14 +165,25 @@ struct DevCloud {
     double *res_dev;              // per-iteration res_new history
 };
 
+// Streams of one handle: the main stream (high priority) and a side stream
+// that runs the flux residual beside the chain schedule's forward sweep,
+// with the events that fork and join them.
+struct IterStreams {
+    cudaStream_t main, side;
+    cudaEvent_t fork, join;
+};
+
 // kernel launchers (mfcfd_kernels.cu)
-// ev: null, or MFCFD_NPHASE+1 events recorded around the phases.
-cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
+// ev: null, or MFCFD_NPHASE+1 events recorded around the phases (ev[2] on
+// the side stream under the chain schedule).
+cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams &st,
                              double *U_next, double *q_next, cudaEvent_t *ev);
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
 int reduction_blocks(int n);
-int chain_max_warps(int device);      // co-resident warps of the chain sweep kernel
-int chain_warps_per_block();
+// Launch shape of the chain sweep for about `want` warps: warps per block
+// and blocks (one block per SM, some SMs left free); returns the warps, 0 if
+// the kernel cannot run on the device.
+int chain_shape(int device, int want, int *wpb, int *blocks);
 // Allocation-free residual (mfcfd_residual_noalloc); the current device must
 // be the handle's.
 int residual_noalloc(const DevCloud &d, cudaStream_t s, double *res_new, std::string &err);

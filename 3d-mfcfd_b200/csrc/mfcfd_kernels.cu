@@ -33,9 +33,6 @@ constexpr int SWEEP_THREADS = 512;
 constexpr int SWEEP_WARPS = SWEEP_THREADS / 32;
 constexpr int RED_THREADS = 256;
 constexpr unsigned FULL = 0xffffffffu;
-// "not yet published" value of the sweeps' hand-off words (see the LU-SGS
-// sweep section): a signalling-NaN bit pattern no arithmetic result has
-constexpr unsigned long long DU_PENDING = 0xFFF4DEADBEEF0001ull;
 
 // ---------------------------------------------------------------- U and q
 
@@ -119,6 +116,68 @@ __global__ void __launch_bounds__(128) k_qderiv(DevCloud d) {
     d.delt[i] = min_delt;
 }
 
+// ---------------------------------------------------------------- hand-off words
+
+// Hand-off of increments between warps.  Before the sweeps, k_dinv_gold sets
+// dUp, dUn, dgf and dgb of every swept point to DU_PENDING, a signalling-NaN
+// bit pattern that no arithmetic result has (arithmetic NaNs are quiet).  A
+// producer stores its values with strong (relaxed, gpu-scope) 8-byte stores;
+// a consumer polls the 8-byte words it needs with strong loads until none is
+// DU_PENDING.  Each word is single-copy atomic, so a value read that is not
+// DU_PENDING is the final one: no flags and no fences are needed.  The same
+// hand-off carries the sweep inputs (flux_res, D_inv, Gold) from k_flux<true>
+// to the forward sweep running beside it.
+constexpr unsigned long long DU_PENDING = 0xFFF4DEADBEEF0001ull;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_b64(const double *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void ld_relaxed_v2(const double *p, unsigned long long &a, unsigned long long &b) {
+    asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_f64(double *p, double v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
+// Polls give up after SPIN_LIMIT rounds (about a second), or soon after
+// another lane gave up: the failure goes to *err (the host reports
+// MFCFD_ERR_TIMEOUT and the iteration's results are invalid).
+constexpr int SPIN_LIMIT = 1 << 21;
+
+__device__ __forceinline__ bool spin_continue(int &it, int *err) {
+    ++it;
+    if ((it & 1023) == 0) {
+        if (*(volatile int *)err) return false;
+        __nanosleep(64);
+    }
+    if (it > SPIN_LIMIT) {
+        atomicExch(err, 1);
+        return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool is_pending(double v) {
+    return (unsigned long long)__double_as_longlong(v) == DU_PENDING;
+}
+
+// Poll one word until it is published.
+__device__ __forceinline__ double poll_word(const double *p, int *err) {
+    unsigned long long v;
+    int spins = 0;
+    do {
+        v = ld_relaxed_b64(p);
+    } while (v == DU_PENDING && spin_continue(spins, err));
+    return __longlong_as_double((long long)v);
+}
+
+__device__ __forceinline__ bool ready5(const unsigned long long v[5]) {
+    return v[0] != DU_PENDING && v[1] != DU_PENDING && v[2] != DU_PENDING && v[3] != DU_PENDING &&
+           v[4] != DU_PENDING;
+}
+
 // ---------------------------------------------------------------- flux residual
 
 // Limited midpoint reconstruction of point j's q toward the offset
@@ -152,87 +211,165 @@ __device__ __forceinline__ void reconstruct(const DevCloud &d, int j, double del
     qtilde_to_primitive(qt, prim);
 }
 
+// Per-list diagonal terms of D_inv (implicit_D_inv_interior.f90:46-417 /
+// implicit_D_inv_wall.f90:45-356 with the geometry-only sums precomputed).
+// u: the velocity component of list dd's axis; as: the speed of sound.
+__device__ __forceinline__ double dinv_term(const DevCloud &d, int i, int dd, double u, double as) {
+    const double *g = d.geo + (size_t)i * GEO_STRIDE;
+    const double temp = g[dd * 8 + G_DNUM], det = g[dd * 8 + G_DET];
+    if ((dd & 1) == 0) {
+        const double t1 = u + as;
+        return 0.50 * fabs(t1 + fabs(t1)) * temp / det;
+    }
+    const double t1 = u - as;
+    return -(0.50 * fabs(t1 - fabs(t1)) * temp / det);
+}
+
+__device__ __forceinline__ double dinv_combine(int cls, double delt, const double gd[NDIR]) {
+    double temp;
+    if (cls == CLS_WALL) temp = (1.0 / delt) - 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+    else temp = (1.0 / delt) - (gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5]);
+    return 1.0 / temp;
+}
+
+// The sweep inputs of point i computed by one warp (same arithmetic as
+// k_dinv_gold): lanes 0-5 the D_inv terms, lane (list, component) the flux
+// of prim and, for an unswept point, of prim(U + dU) in the shared frame.
+// Strong stores: the forward sweep polls for these words.
+__device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int lane) {
+    double p[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) p[r] = d.prim[5 * (size_t)i + r];
+    const bool swept = d.swept[i] != 0;
+    if (swept) {
+        const double as = sqrt(1.40 * p[4] / p[0]);
+        const double u = (lane >> 1) == 0 ? p[1] : ((lane >> 1) == 1 ? p[2] : p[3]);
+        const double t = lane < NDIR ? dinv_term(d, i, lane, u, as) : 0.0;
+        double gd[NDIR];
+#pragma unroll
+        for (int dd = 0; dd < NDIR; ++dd) gd[dd] = __shfl_sync(FULL, t, dd);
+        if (lane == 0) st_relaxed_f64(d.dinv + i, dinv_combine(d.cls[i], d.delt[i], gd));
+    }
+    if (d.shared_frame && lane < 30) {
+        const int dd = lane / 5, c = lane - 5 * dd;
+        Frame F0;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) { F0.t1[r] = d.frame0[r]; F0.t2[r] = d.frame0[3 + r]; F0.n[r] = d.frame0[6 + r]; }
+        FluxPre P;
+        flux_pre(p, F0, P);
+        AxisTerms At;
+        axis_terms(P, dd >> 1, At);
+        const double gold = flux_component(dd, c, P, At, At, At);
+        st_relaxed_f64(d.gold + 30 * (size_t)i + lane, gold);
+        if (!swept) {
+            double U[5], pn[5];
+            Frame F;
+            load_frame(d.frame + 9 * (size_t)i, F);
+#pragma unroll
+            for (int r = 0; r < 5; ++r) U[r] = d.dUp[5 * (size_t)i + r] + d.U[5 * (size_t)i + r];
+            conserved_to_primitive(U, F, pn);
+            flux_pre(pn, F0, P);
+            axis_terms(P, dd >> 1, At);
+            const double v = flux_component(dd, c, P, At, At, At) - gold;
+            const size_t o = DG_STRIDE * (size_t)i + DG_LIST * dd + c;
+            st_relaxed_f64(d.dgf + o, v);
+            st_relaxed_f64(d.dgb + o, v);
+        }
+    }
+}
+
 // eval_flux_residual (flux_residual.f90:40-81): one warp per point.  Lanes
 // own the point's distinct neighbours: each reconstructs both ends of its
 // pair once and evaluates the flux of every list the neighbour belongs to;
 // then 30 lanes (list, component) sum the list terms in list order and solve
 // the 3x3 least-squares system with the precomputed moments.
+//
+// FUSED (chain schedule): the warps take the points in the forward sweep's
+// order (d.pre_order) and also produce the point's sweep inputs (D_inv,
+// fluxes of prim in the shared frame, the fixed increment of an unswept
+// point) with strong stores, while the forward sweep runs concurrently and
+// polls for them (they start as DU_PENDING).
+template <bool FUSED>
 __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *T = smem + warp * FLUX_SMEM_PER_WARP;     // T[(dir*32 + slot)*5 + c]
     double *W = T + NDIR * MAX_SLOTS * 5;             // W[slot*3 + axis]
-    for (int p = blockIdx.x * FLUX_WARPS + warp; p < d.n; p += gridDim.x * FLUX_WARPS) {
+    for (int i = blockIdx.x * FLUX_WARPS + warp; i < d.n; i += gridDim.x * FLUX_WARPS) {
+        const int p = FUSED ? d.pre_order[i] : i;
         const int cls = d.cls[p];
-        if (cls > 2) continue;
-        const int ns = d.nslot[p];
-        if (lane < ns) {
-            const int k = d.slot_nbr[(size_t)p * MAX_SLOTS + lane];
-            const int mask = d.slot_mask[(size_t)p * MAX_SLOTS + lane];
-            Frame F;
-            load_frame(d.frame + 9 * (size_t)p, F);
-            const double delx = d.x[k] - d.x[p], dely = d.y[k] - d.y[p], delz = d.z[k] - d.z[p];
-            W[lane * 3 + 0] = delx * F.t1[0] + dely * F.t1[1] + delz * F.t1[2];
-            W[lane * 3 + 1] = delx * F.t2[0] + dely * F.t2[1] + delz * F.t2[2];
-            W[lane * 3 + 2] = delx * F.n[0] + dely * F.n[1] + delz * F.n[2];
-            int axes = 0;
+        if (cls <= 2) {
+            const int ns = d.nslot[p];
+            if (lane < ns) {
+                const int k = d.slot_nbr[(size_t)p * MAX_SLOTS + lane];
+                const int mask = d.slot_mask[(size_t)p * MAX_SLOTS + lane];
+                Frame F;
+                load_frame(d.frame + 9 * (size_t)p, F);
+                const double delx = d.x[k] - d.x[p], dely = d.y[k] - d.y[p], delz = d.z[k] - d.z[p];
+                W[lane * 3 + 0] = delx * F.t1[0] + dely * F.t1[1] + delz * F.t1[2];
+                W[lane * 3 + 1] = delx * F.t2[0] + dely * F.t2[1] + delz * F.t2[2];
+                W[lane * 3 + 2] = delx * F.n[0] + dely * F.n[1] + delz * F.n[2];
+                int axes = 0;
 #pragma unroll
-            for (int dd = 0; dd < NDIR; ++dd)
-                if (mask & (1 << dd)) axes |= kind_axes(flux_kind(cls, dd));
-            double prim[5];
-            FluxPre Pi, Pk;
-            AxisTerms Ai[3], Ak[3];
-            reconstruct(d, p, delx, dely, delz, prim);
-            flux_pre(prim, F, Pi);
-            reconstruct(d, k, delx, dely, delz, prim);
-            flux_pre(prim, F, Pk);
+                for (int dd = 0; dd < NDIR; ++dd)
+                    if (mask & (1 << dd)) axes |= kind_axes(flux_kind(cls, dd));
+                double prim[5];
+                FluxPre Pi, Pk;
+                AxisTerms Ai[3], Ak[3];
+                reconstruct(d, p, delx, dely, delz, prim);
+                flux_pre(prim, F, Pi);
+                reconstruct(d, k, delx, dely, delz, prim);
+                flux_pre(prim, F, Pk);
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (axes & (1 << a)) {
-                    axis_terms(Pi, a, Ai[a]);
-                    axis_terms(Pk, a, Ak[a]);
+                for (int a = 0; a < 3; ++a) {
+                    if (axes & (1 << a)) {
+                        axis_terms(Pi, a, Ai[a]);
+                        axis_terms(Pk, a, Ak[a]);
+                    }
+                }
+                for (int dd = 0; dd < NDIR; ++dd) {
+                    if (!(mask & (1 << dd))) continue;
+                    const int kind = flux_kind(cls, dd);
+#pragma unroll
+                    for (int c = 0; c < 5; ++c) {
+                        const double gi = flux_component(kind, c, Pi, Ai);
+                        const double gk = flux_component(kind, c, Pk, Ak);
+                        T[(dd * MAX_SLOTS + lane) * 5 + c] = gk - gi;
+                    }
                 }
             }
-            for (int dd = 0; dd < NDIR; ++dd) {
-                if (!(mask & (1 << dd))) continue;
-                const int kind = flux_kind(cls, dd);
-#pragma unroll
-                for (int c = 0; c < 5; ++c) {
-                    const double gi = flux_component(kind, c, Pi, Ai);
-                    const double gk = flux_component(kind, c, Pk, Ak);
-                    T[(dd * MAX_SLOTS + lane) * 5 + c] = gk - gi;
+            __syncwarp();
+            double G = 0.0;
+            if (lane < 30) {
+                const int dd = lane / 5, c = lane - 5 * dd;
+                const int cnt = d.list_cnt[(size_t)p * NDIR + dd];
+                const uint8_t *ent = d.list_ent + ((size_t)p * NDIR + dd) * LIST_STRIDE;
+                double sx = 0.0, sy = 0.0, sz = 0.0;
+                for (int j = 0; j < cnt; ++j) {
+                    const int s = ent[j];
+                    const double t = T[(dd * MAX_SLOTS + s) * 5 + c];
+                    sx = sx + t * W[s * 3 + 0];
+                    sy = sy + t * W[s * 3 + 1];
+                    sz = sz + t * W[s * 3 + 2];
                 }
+                const double *g = d.geo + (size_t)p * GEO_STRIDE + dd * 8;
+                const double num = cramer_num(dd >> 1, g, sx, sy, sz);
+                // outer_flux_dG*.f90:118-124 multiply by 1/det; the others divide
+                G = (cls == CLS_OUTER) ? num * (1.0 / g[G_DET]) : num / g[G_DET];
             }
-        }
-        __syncwarp();
-        double G = 0.0;
-        if (lane < 30) {
-            const int dd = lane / 5, c = lane - 5 * dd;
-            const int cnt = d.list_cnt[(size_t)p * NDIR + dd];
-            const uint8_t *ent = d.list_ent + ((size_t)p * NDIR + dd) * LIST_STRIDE;
-            double sx = 0.0, sy = 0.0, sz = 0.0;
-            for (int j = 0; j < cnt; ++j) {
-                const int s = ent[j];
-                const double t = T[(dd * MAX_SLOTS + s) * 5 + c];
-                sx = sx + t * W[s * 3 + 0];
-                sy = sy + t * W[s * 3 + 1];
-                sz = sz + t * W[s * 3 + 2];
-            }
-            const double *g = d.geo + (size_t)p * GEO_STRIDE + dd * 8;
-            const double num = cramer_num(dd >> 1, g, sx, sy, sz);
-            // outer_flux_dG*.f90:118-124 multiply by 1/det; the others divide
-            G = (cls == CLS_OUTER) ? num * (1.0 / g[G_DET]) : num / g[G_DET];
-        }
-        double gd[NDIR];
+            double gd[NDIR];
 #pragma unroll
-        for (int dd = 0; dd < NDIR; ++dd) gd[dd] = __shfl_sync(FULL, G, dd * 5 + (lane % 5));
-        if (lane < 5) {
-            double r;
-            if (cls == CLS_INTERIOR) r = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
-            else if (cls == CLS_WALL) r = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
-            else r = gd[0] + gd[1] + gd[2] + gd[3] + gd[4];
-            d.flux_res[5 * (size_t)p + lane] = r;
+            for (int dd = 0; dd < NDIR; ++dd) gd[dd] = __shfl_sync(FULL, G, dd * 5 + (lane % 5));
+            if (lane < 5) {
+                double r;
+                if (cls == CLS_INTERIOR) r = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
+                else if (cls == CLS_WALL) r = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+                else r = gd[0] + gd[1] + gd[2] + gd[3] + gd[4];
+                if (FUSED) st_relaxed_f64(d.flux_res + 5 * (size_t)p + lane, r);
+                else d.flux_res[5 * (size_t)p + lane] = r;
+            }
         }
+        if (FUSED) sweep_inputs_warp(d, p, lane);
         __syncwarp();
     }
 }
@@ -256,26 +393,36 @@ __device__ __forceinline__ void flux6_frame0(const DevCloud &d, const double pri
 }
 
 // Before the sweeps: every published-increment word, and dU of every swept
-// point, is set to DU_PENDING (coalesced grid-stride fill).
-__global__ void k_pending(DevCloud d) {
+// point, is set to DU_PENDING (coalesced grid-stride fill).  With inputs set,
+// also the swept points' flux_res, D_inv and Gold, which k_flux<true>
+// produces while the forward sweep runs.
+__global__ void k_pending(DevCloud d, int inputs) {
     const double pend = __longlong_as_double((long long)DU_PENDING);
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t ng = (size_t)d.n * DG_STRIDE, nu = (size_t)d.n * 5;
-    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < ng; w += stride) {
+    const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t ng = (size_t)d.n * DG_STRIDE, nu = (size_t)d.n * 5, n30 = (size_t)d.n * 30;
+    for (size_t w = t0; w < ng; w += stride) {
         d.dgf[w] = pend;
         d.dgb[w] = pend;
     }
-    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < nu; w += stride) {
+    for (size_t w = t0; w < nu; w += stride) {
         if (d.swept[w / 5]) {
             d.dUp[w] = pend;
             d.dUn[w] = pend;
+            if (inputs) d.flux_res[w] = pend;
         }
+    }
+    if (inputs) {
+        for (size_t w = t0; w < (size_t)d.n; w += stride)
+            if (d.swept[w]) d.dinv[w] = pend;
+        if (d.shared_frame)
+            for (size_t w = t0; w < n30; w += stride)
+                if (d.swept[w / 30]) d.gold[w] = pend;
     }
 }
 
-// implicit_D_inv_interior.f90:46-417 / implicit_D_inv_wall.f90:45-356 with
-// the geometry-only sums precomputed; plus the sweep inputs that do not
-// depend on the sweep: G(prim_k) in the shared frame for every point and the
+// implicit_D_inv_interior.f90:46-417 / implicit_D_inv_wall.f90:45-356 (see
+// dinv_term); plus the sweep inputs that do not depend on the sweep: G(prim_k) in the shared frame for every point and the
 // published increment G(prim(U_k + dU_k)) - G(prim_k) of points the sweeps
 // never update (outer points, point 1), over the DU_PENDING that k_pending
 // wrote there.
@@ -286,24 +433,10 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
     const double *p = d.prim + 5 * (size_t)i;
     if (d.swept[i]) {
         const double as = sqrt(1.40 * p[4] / p[0]);
-        const double *g = d.geo + (size_t)i * GEO_STRIDE;
         double gd[NDIR];
 #pragma unroll
-        for (int dd = 0; dd < NDIR; ++dd) {
-            const double u = p[1 + (dd >> 1)];
-            const double temp = g[dd * 8 + G_DNUM], det = g[dd * 8 + G_DET];
-            if ((dd & 1) == 0) {
-                const double t1 = u + as;
-                gd[dd] = 0.50 * fabs(t1 + fabs(t1)) * temp / det;
-            } else {
-                const double t1 = u - as;
-                gd[dd] = -(0.50 * fabs(t1 - fabs(t1)) * temp / det);
-            }
-        }
-        double temp;
-        if (cls == CLS_WALL) temp = (1.0 / d.delt[i]) - 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
-        else temp = (1.0 / d.delt[i]) - (gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5]);
-        d.dinv[i] = 1.0 / temp;
+        for (int dd = 0; dd < NDIR; ++dd) gd[dd] = dinv_term(d, i, dd, p[1 + (dd >> 1)], as);
+        d.dinv[i] = dinv_combine(cls, d.delt[i], gd);
     }
     if (d.shared_frame) {
         double prim[5], gold[30];
@@ -332,49 +465,6 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
 }
 
 // ---------------------------------------------------------------- LU-SGS sweeps
-
-// Hand-off of increments between warps.  Before the sweeps, k_dinv_gold sets
-// dUp, dUn, dgf and dgb of every swept point to DU_PENDING, a signalling-NaN
-// bit pattern that no arithmetic result has (arithmetic NaNs are quiet).  A
-// producer stores its values with strong (relaxed, gpu-scope) 8-byte stores;
-// a consumer polls the 8-byte words it needs with strong loads until none is
-// DU_PENDING.  Each word is single-copy atomic, so a value read that is not
-// DU_PENDING is the final one: no flags and no fences are needed.
-
-__device__ __forceinline__ unsigned long long ld_relaxed_b64(const double *p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void ld_relaxed_v2(const double *p, unsigned long long &a, unsigned long long &b) {
-    asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
-}
-__device__ __forceinline__ void st_relaxed_f64(double *p, double v) {
-    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
-}
-
-// Polls give up after SPIN_LIMIT rounds (about a second), or soon after
-// another lane gave up: the failure goes to *err (the host reports
-// MFCFD_ERR_TIMEOUT and the iteration's results are invalid).
-constexpr int SPIN_LIMIT = 1 << 21;
-
-__device__ __forceinline__ bool spin_continue(int &it, int *err) {
-    ++it;
-    if ((it & 1023) == 0) {
-        if (*(volatile int *)err) return false;
-        __nanosleep(64);
-    }
-    if (it > SPIN_LIMIT) {
-        atomicExch(err, 1);
-        return false;
-    }
-    return true;
-}
-
-__device__ __forceinline__ bool ready5(const unsigned long long v[5]) {
-    return v[0] != DU_PENDING && v[1] != DU_PENDING && v[2] != DU_PENDING && v[3] != DU_PENDING &&
-           v[4] != DU_PENDING;
-}
 
 // Per-warp shared memory of the sweep kernels.  SweepStage holds everything a
 // point reads that the sweep itself does not change (its terms, geometry,
@@ -514,6 +604,12 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     if (lane < 5) {
         dinv = st->dinv[0];
         base5 = st->base[lane];
+    }
+    // inputs the concurrent flux kernel had not produced when the stage was copied
+    if (lane < 30 && is_pending(gold)) gold = poll_word(d.gold + 30 * (size_t)p + lane, d.err);
+    if (lane < 5) {
+        if (is_pending(dinv)) dinv = poll_word(d.dinv + p, d.err);
+        if (is_pending(base5)) base5 = poll_word((forward ? d.flux_res : d.dUp) + 5 * (size_t)p + lane, d.err);
     }
     double Up[5];
 #pragma unroll
@@ -730,19 +826,22 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
 
 // Chain sweep: each warp walks its own list of point records (fixed at
 // set-up, topological order).  The stage of the next point is copied in
-// while the current one is processed (two stage buffers).  All warps are
-// resident (cooperative launch), so the earliest unfinished point always
-// belongs to a warp that is working on it and can finish: the polls end.
-constexpr int CH_WARPS = 4;
+// while the current one is processed (two stage buffers).  One block of WPB
+// warps per SM (the dynamic shared memory is sized for that), on at most
+// all SMs but CH_FREE_SMS, so all blocks are resident and the concurrent
+// flux kernel keeps SMs of its own: every poll ends.
+constexpr int CH_SMEM_MIN = 116 * 1024;   // over half an SM's shared memory
+constexpr int CH_FREE_SMS = 16;
 
-__global__ void __launch_bounds__(CH_WARPS * 32) k_sweep_chain(DevCloud d, int forward) {
+template <int WPB>
+__global__ void __launch_bounds__(WPB * 32, 1) k_sweep_chain(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char *smb = reinterpret_cast<char *>(smem) + warp * CHAIN_SMEM_BYTES;
     double *T = reinterpret_cast<double *>(smb);
     double *ring = T + SW_T_DOUBLES;
     SweepStage *stg = reinterpret_cast<SweepStage *>(ring + SW_RING_DOUBLES);
-    const int me = blockIdx.x * CH_WARPS + warp;
+    const int me = blockIdx.x * WPB + warp;
     if (me >= d.ch_warps) return;
     const int dir = forward ? 0 : 1;
     const int a = d.ch_ptr[dir][me], b = d.ch_ptr[dir][me + 1];
@@ -765,6 +864,11 @@ __global__ void __launch_bounds__(CH_WARPS * 32) k_sweep_chain(DevCloud d, int f
         cur = nxt;
         nxt = after;
     }
+}
+
+template <int WPB>
+static int chain_smem() {
+    return WPB * CHAIN_SMEM_BYTES > CH_SMEM_MIN ? WPB * CHAIN_SMEM_BYTES : CH_SMEM_MIN;
 }
 
 // ---------------------------------------------------------------- state update
@@ -906,50 +1010,70 @@ int residual_noalloc(const DevCloud &d, cudaStream_t s, double *res_new, std::st
     return MFCFD_OK;
 }
 
-int chain_max_warps(int device) {
-    int sms = 0, per_sm = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaFuncSetAttribute(k_sweep_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         CH_WARPS * CHAIN_SMEM_BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain, CH_WARPS * 32,
-                                                  CH_WARPS * CHAIN_SMEM_BYTES);
-    return sms * per_sm * CH_WARPS;
+// Sets the kernels' shared-memory limits once per device.
+static void set_attributes(int device) {
+    static std::mutex mu;
+    static bool done[256] = {false};
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0 || device >= 256 || done[device]) return;
+    cudaFuncSetAttribute(k_flux<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
+    cudaFuncSetAttribute(k_flux<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
+    cudaFuncSetAttribute(k_sweep_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         SWEEP_WARPS * SWEEP_SMEM_BYTES);
+    cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize, DF_WARPS * SWEEP_SMEM_BYTES);
+    cudaFuncSetAttribute(k_sweep_chain<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
+    cudaFuncSetAttribute(k_sweep_chain<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
+    done[device] = true;
 }
 
-int chain_warps_per_block() { return CH_WARPS; }
+int chain_shape(int device, int want, int *wpb, int *blocks) {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    set_attributes(device);
+    const int max_blocks = sms - CH_FREE_SMS;
+    if (max_blocks < 1) return 0;
+    *wpb = want <= 4 * max_blocks ? 4 : 8;
+    // with 8-warp blocks, three quarters of the warps: more SMs stay with the
+    // concurrent flux kernel, which then keeps ahead of the forward sweep
+    if (*wpb == 8) want = want * 3 / 4;
+    int per_sm = 0;
+    if (*wpb == 4)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4>, 4 * 32, chain_smem<4>());
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8>, 8 * 32, chain_smem<8>());
+    if (per_sm < 1) return 0;
+    int b = (want + *wpb - 1) / *wpb;
+    if (b > max_blocks) b = max_blocks;
+    if (b < 1) b = 1;
+    *blocks = b;
+    return b * *wpb;
+}
 
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s) {
     k_conserved_q<<<(d.n + 127) / 128, 128, 0, s>>>(d);
     return cudaGetLastError();
 }
 
-static bool g_attr_set = false;
-
-cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
-                             double *U_next, double *q_next, cudaEvent_t *ev) {
+cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams &st, double *U_next,
+                             double *q_next, cudaEvent_t *ev) {
     const int n = d.n;
-    if (!g_attr_set) {
-        cudaFuncSetAttribute(k_flux, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
-        cudaFuncSetAttribute(k_sweep_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SWEEP_WARPS * SWEEP_SMEM_BYTES);
-        cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             DF_WARPS * SWEEP_SMEM_BYTES);
-        cudaFuncSetAttribute(k_sweep_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             CH_WARPS * CHAIN_SMEM_BYTES);
-        g_attr_set = true;
-    }
+    cudaStream_t s = st.main;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    set_attributes(dev);
     // dataflow grid: about the widest level in warps (more warps only add
     // pollers), within 8 per SM
     int df_warps = d.max_width;
     df_warps = df_warps < 64 ? 64 : (df_warps > 148 * 8 ? 148 * 8 : df_warps);
     const int df_blocks = (df_warps + DF_WARPS - 1) / DF_WARPS;
+    const bool chains = d.sweep_mode == MFCFD_SWEEP_CHAINS;
     auto sweep = [&](int forward) {
-        if (d.sweep_mode == MFCFD_SWEEP_CHAINS) {
-            DevCloud dc = d;
-            void *args[] = {&dc, &forward};
-            cudaLaunchCooperativeKernel((void *)k_sweep_chain, dim3(d.ch_warps / CH_WARPS),
-                                        dim3(CH_WARPS * 32), args, CH_WARPS * CHAIN_SMEM_BYTES, s);
+        if (chains) {
+            const int blocks = d.ch_warps / d.ch_wpb;
+            if (d.ch_wpb == 4) k_sweep_chain<4><<<blocks, 4 * 32, chain_smem<4>(), s>>>(d, forward);
+            else k_sweep_chain<8><<<blocks, 8 * 32, chain_smem<8>(), s>>>(d, forward);
         } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
         } else {
@@ -957,26 +1081,46 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, cudaStream_t s,
             k_sweep_df<<<df_blocks, DF_WARPS * 32, DF_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
         }
     };
-    auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
-    mark(0);
-    k_qderiv<<<(n + 127) / 128, 128, 0, s>>>(d);
-    mark(1);
+    auto mark = [&](int i, cudaStream_t on) { if (ev) cudaEventRecord(ev[i], on); };
     const int fblocks = (n + FLUX_WARPS - 1) / FLUX_WARPS;
-    k_flux<<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
-    mark(2);
-    k_pending<<<148 * 8, 256, 0, s>>>(d);
-    k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);
-    mark(3);
-    sweep(1);
-    mark(4);
+    mark(0, s);
+    k_qderiv<<<(n + 127) / 128, 128, 0, s>>>(d);
+    mark(1, s);
+    if (chains) {
+        // the flux residual and the sweep inputs run on the side stream beside
+        // the forward sweep, in its order; the sweep polls for them.  The flux
+        // kernel is issued first: where kernels run one at a time (a profiler,
+        // blocking launches) it completes before the sweep starts, and it
+        // never waits on the sweep, so no order of execution can stall.  The
+        // main stream's higher priority places the sweep's blocks first when
+        // both run.
+        k_pending<<<148 * 8, 256, 0, s>>>(d, 1);
+        mark(3, s);
+        cudaEventRecord(st.fork, s);
+        cudaStreamWaitEvent(st.side, st.fork, 0);
+        k_flux<true><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, st.side>>>(d);
+        mark(2, st.side);
+        cudaEventRecord(st.join, st.side);
+        sweep(1);
+        mark(4, s);
+        cudaStreamWaitEvent(s, st.join, 0);
+    } else {
+        k_flux<false><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
+        mark(2, s);
+        k_pending<<<148 * 8, 256, 0, s>>>(d, 0);
+        k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);
+        mark(3, s);
+        sweep(1);
+        mark(4, s);
+    }
     sweep(0);
-    mark(5);
+    mark(5, s);
     k_update<<<(n + 127) / 128, 128, 0, s>>>(d, U_next, q_next);
-    mark(6);
+    mark(6, s);
     const int rb = reduction_blocks(d.n_res);
     k_reduce_partial<<<rb, RED_THREADS, 0, s>>>(d);
     k_reduce_final<<<1, 32, 0, s>>>(d, rb, iter_slot);
-    mark(7);
+    mark(7, s);
     return cudaGetLastError();
 }
 

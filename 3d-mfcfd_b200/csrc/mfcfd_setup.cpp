@@ -482,4 +482,25 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
     }
 }
 
+// Order in which the fused flux kernel visits the points: the forward
+// sweep's levels, each preceded by the unswept points whose fixed increments
+// that level reads first; points the forward sweep never reads come last.
+void build_pre_order(const Topology &T, std::vector<int32_t> &order) {
+    const int n = T.n;
+    const int64_t last = INT64_MAX;
+    std::vector<int64_t> key(n, last);
+    for (int p = 0; p < n; ++p)
+        if (T.swept[p]) key[p] = 2 * (int64_t)T.fwd_level[p] + 1;
+    for (int p = 0; p < n; ++p) {
+        if (!T.swept[p]) continue;
+        for (int e = T.fwd_off[p]; e < T.fwd_off[p + 1]; ++e) {
+            const int k = T.fwd_ent[e].k;
+            if (!T.swept[k]) key[k] = std::min(key[k], 2 * (int64_t)T.fwd_level[p]);
+        }
+    }
+    order.resize(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
+}
+
 }  // namespace mfcfd

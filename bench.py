@@ -45,12 +45,19 @@ import numpy as np  # noqa: E402
 PHASE_BYTES = {"qderiv": 372 + 180, "flux": 724, "dinv": 488, "sweep_fwd": 608,
                "sweep_bwd": 608, "update": 196, "residual": 8}
 TOTAL_BYTES = 3368
+# DRAM bytes (read + write) per swept point of one chain-sweep launch, from
+# the ncu capture of the 62,400-point sphere's forward sweep (161.96 MB per
+# launch, profiles/ncu_k_sweep_chain_sphere62k.txt); traffic grows with the
+# point count, so a launch of n points moves about n times this.
+SWEEP_TRAFFIC_PER_POINT = 161.96e6 / 62400
 
 WORKLOADS = {
     "sphere-1.1M": dict(shells=96, per_shell=11500, jitter=0.01, mach=0.8, aoa=2.0, seed=2001),
     "sphere-62k": dict(shells=48, per_shell=1300, jitter=0.02, mach=0.4, aoa=0.0, seed=1001),
 }
-KERNELS_PER_ITER = 8
+# kernels of one iteration per sweep mode (2 chains: k_qderiv, k_pending,
+# k_flux, two k_sweep_chain, k_update, two reductions; 0/1 add k_dinv_gold)
+KERNELS_PER_ITER = {2: 8, 0: 9, 1: 9}
 
 
 def load_peaks():
@@ -250,11 +257,16 @@ def main():
     dom_ms = phases[dom] / max(piters, 1)
     peak, peak_kind = load_peaks()
     achieved = PHASE_BYTES[dom] * c.n / (dom_ms / 1e3) / 1e9
+    traffic = SWEEP_TRAFFIC_PER_POINT * c.n if dom.startswith("sweep") and args.sweep_mode == 2 else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "kernel": dom,
+                "frac": achieved / peak, "traffic": traffic, "kernel": dom,
                 "peak_source": peak_kind,
                 "phase_ms_per_iter": {k: v / max(piters, 1) for k, v in phases.items()},
-                "iteration_bytes_model": TOTAL_BYTES}
+                "iteration_bytes_model": TOTAL_BYTES,
+                # the sweeps are bound by their dependency chain, not by HBM:
+                # levels of the schedule and device time per level
+                "sweep_us_per_level": dom_ms * 1e3 / max(1, info["n_levels_forward"]
+                                                        if dom == "sweep_fwd" else info["n_levels_backward"])}
 
     # end to end through the C ABI with pinned host buffers
     prim_h = torch.empty((c.n, 5), dtype=torch.float64, pin_memory=True).numpy()
@@ -297,11 +309,12 @@ def main():
                            "levels_forward": info["n_levels_forward"],
                            "levels_backward": info["n_levels_backward"],
                            "l2": "state larger than L2 (no flush)",
+                           "sweep_mode": args.sweep_mode,
                            "parallelism": f"replicas x{world}"},
                 "e2e": {"value": e2e_value, "unit": "point-iters/s",
                         "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                 "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks,
-                "gpu_launches": KERNELS_PER_ITER * args.steps}
+                "gpu_launches": KERNELS_PER_ITER[args.sweep_mode] * args.steps}
         print(json.dumps(line), flush=True)
     s.close()
     replicas.finalize()
