@@ -31,6 +31,9 @@ struct SweepEntry {
     int32_t k;
     int32_t pad;
     double w[3];
+    // leaves the fields unset, so sizing a large table does not zero it
+    // first: the set-up writes every entry
+    SweepEntry() {}
 };
 
 constexpr int SWEEP_MAX_ENTRIES = 96;   // per point and direction (checked at set-up)

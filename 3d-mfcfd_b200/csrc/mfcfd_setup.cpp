@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "mfcfd_internal.h"
 
@@ -36,6 +37,26 @@ namespace mfcfd {
 namespace {
 
 struct Moments { double xx, yy, zz, xy, yz, zx; };
+
+// f(i) for i in [0, n) on the host's cores; every i writes only its own
+// outputs, so the result does not depend on the thread count.
+template <class F>
+void parallel_for(int n, const F &f) {
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = nt < 1 ? 1 : (nt > 32 ? 32 : nt);
+    if (n < (1 << 16) || nt == 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    const int chunk = (n + (int)nt - 1) / (int)nt;
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) {
+        const int a = (int)t * chunk, b = std::min(n, a + chunk);
+        if (a >= b) break;
+        th.emplace_back([a, b, &f] { for (int i = a; i < b; ++i) f(i); });
+    }
+    for (auto &t : th) t.join();
+}
 
 inline double det_of(const Moments &m) {
     return m.xx * (m.yy * m.zz - m.yz * m.yz)
@@ -164,7 +185,6 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     T.slot_mask.assign((size_t)n * MAX_SLOTS, 0);
     T.list_cnt.assign((size_t)n * NDIR, 0);
     T.list_ent.assign((size_t)n * NDIR * LIST_STRIDE, 0);
-    std::vector<int> eff[NDIR];
     auto effective = [&](int i, int d, std::vector<int> &out) {   // 0-based ids
         out.clear();
         int cls = T.cls[i];
@@ -183,7 +203,12 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         }
         return true;
     };
-    for (int i = 0; i < n; ++i) {
+    // per point: 0 ok, else the first problem found (reported for the
+    // lowest such point, as a sequential pass would)
+    enum { SLOT_OK = 0, SLOT_ZERO, SLOT_LONG, SLOT_WIDE };
+    std::vector<uint8_t> slot_err(n, SLOT_OK);
+    parallel_for(n, [&](int i) {
+        std::vector<int> eff;
         int32_t *slots = &T.slot_nbr[(size_t)i * MAX_SLOTS];
         int ns = 0;
         auto slot_of = [&](int k) -> int {
@@ -194,32 +219,36 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         };
         for (int r = 0; r < nbhs[i]; ++r) slot_of(conn[(size_t)i * MAX_CONN + r] - 1);
         for (int d = 0; d < NDIR; ++d) {
-            if (!effective(i, d, eff[d])) {
-                err = "split list of point " + std::to_string(i + 1) + " names point 0";
-                return MFCFD_ERR_STENCIL;
-            }
-            if (eff[d].size() > (size_t)MAX_CONN) {
-                err = "split list longer than 27 at point " + std::to_string(i + 1);
-                return MFCFD_ERR_STENCIL;
-            }
-            T.list_cnt[(size_t)i * NDIR + d] = (uint8_t)eff[d].size();
-            for (size_t j = 0; j < eff[d].size(); ++j) {
-                int s = slot_of(eff[d][j]);
-                if (s < 0) {
-                    err = "more than 32 distinct stencil neighbours at point " + std::to_string(i + 1);
-                    return MFCFD_ERR_STENCIL;
-                }
+            if (!effective(i, d, eff)) { slot_err[i] = SLOT_ZERO; return; }
+            if (eff.size() > (size_t)MAX_CONN) { slot_err[i] = SLOT_LONG; return; }
+            T.list_cnt[(size_t)i * NDIR + d] = (uint8_t)eff.size();
+            for (size_t j = 0; j < eff.size(); ++j) {
+                int s = slot_of(eff[j]);
+                if (s < 0) { slot_err[i] = SLOT_WIDE; return; }
                 T.list_ent[((size_t)i * NDIR + d) * LIST_STRIDE + j] = (uint8_t)s;
                 T.slot_mask[(size_t)i * MAX_SLOTS + s] |= (uint8_t)(1u << d);
             }
         }
         T.nslot[i] = (uint8_t)ns;
+    });
+    for (int i = 0; i < n; ++i) {
+        if (slot_err[i] == SLOT_OK) continue;
+        const std::string at = std::to_string(i + 1);
+        if (slot_err[i] == SLOT_ZERO) err = "split list of point " + at + " names point 0";
+        else if (slot_err[i] == SLOT_LONG) err = "split list longer than 27 at point " + at;
+        else err = "more than 32 distinct stencil neighbours at point " + at;
+        return MFCFD_ERR_STENCIL;
     }
 
     // ---- geometry per (point, list): moments, determinant, D_inv numerator
     T.geo.assign((size_t)n * GEO_STRIDE, 0.0);
-    auto weights_of = [&](double dist) { return 1.0 / std::pow(dist, P.power); };
-    for (int i = 0; i < n; ++i) {
+    // least-squares weight 1/dist**power; dist**0 is exactly 1 for every dist
+    auto weight = [&](double dels, double delt, double deln) {
+        if (P.power == 0.0) return 1.0;
+        const double dist = std::sqrt(dels * dels + delt * delt + deln * deln);
+        return 1.0 / std::pow(dist, P.power);
+    };
+    parallel_for(n, [&](int i) {
         const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
         for (int d = 0; d < NDIR; ++d) {
             int c = T.list_cnt[(size_t)i * NDIR + d];
@@ -232,8 +261,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
                 double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
                 double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
                 double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
-                double dist = std::sqrt(dels * dels + delt * delt + deln * deln);
-                double w = weights_of(dist);
+                double w = weight(dels, delt, deln);
                 double ws = dels * w, wt = delt * w, wn = deln * w;
                 m.xx = m.xx + dels * ws;
                 m.yy = m.yy + delt * wt;
@@ -251,7 +279,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             g[G_DET] = det_of(m);
             g[G_DNUM] = numerator(d / 2, m, sdx, sdy, sdz);
         }
-    }
+    });
 
     // limiter epsilon: (VL_CONST*min_dist)**3 squared (limiters.f90:251-253)
     T.eps2.resize(n);
@@ -282,41 +310,47 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         need.assign(n, 0u);
         off.assign(n + 1, 0);
         cnt.assign((size_t)n * NDIR, 0);
-        ent.clear();
-        // entries first (in point index order of the offsets)
-        std::vector<std::vector<SweepEntry>> per(n);
-        for (int p : order) {
-            const double *t1 = tan1 + 3 * (size_t)p, *t2 = tan2 + 3 * (size_t)p, *nn = nor + 3 * (size_t)p;
+        // entries, in point index order of the offsets: count, then fill
+        auto takes = [&](int p, int k) { return forward ? (al(k) < al(p)) : (al(k) > al(p)); };
+        parallel_for((int)order.size(), [&](int oi) {
+            const int p = order[oi];
             for (int d = 0; d < NDIR; ++d) {
-                int c = T.list_cnt[(size_t)p * NDIR + d];
+                const int c = T.list_cnt[(size_t)p * NDIR + d];
                 int taken = 0;
                 for (int j = 0; j < c; ++j) {
-                    int s = T.list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
-                    int k = T.slot_nbr[(size_t)p * MAX_SLOTS + s];
-                    bool take = forward ? (al(k) < al(p)) : (al(k) > al(p));
-                    if (!take) continue;
+                    const int s = T.list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
+                    if (takes(p, T.slot_nbr[(size_t)p * MAX_SLOTS + s])) ++taken;
+                }
+                cnt[(size_t)p * NDIR + d] = (uint8_t)taken;
+                off[p + 1] += taken;
+            }
+        });
+        for (int p = 0; p < n; ++p) off[p + 1] += off[p];
+        ent.clear();
+        ent.resize((size_t)off[n]);
+        parallel_for((int)order.size(), [&](int oi) {
+            const int p = order[oi];
+            const double *t1 = tan1 + 3 * (size_t)p, *t2 = tan2 + 3 * (size_t)p, *nn = nor + 3 * (size_t)p;
+            size_t e_at = (size_t)off[p];
+            for (int d = 0; d < NDIR; ++d) {
+                const int c = T.list_cnt[(size_t)p * NDIR + d];
+                for (int j = 0; j < c; ++j) {
+                    const int s = T.list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
+                    const int k = T.slot_nbr[(size_t)p * MAX_SLOTS + s];
+                    if (!takes(p, k)) continue;
                     double delx = x[k] - x[p], dely = y[k] - y[p], delz = z[k] - z[p];
                     double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
                     double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
                     double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
-                    double dist = std::sqrt(dels * dels + delt * delt + deln * deln);
-                    double w = weights_of(dist);
-                    SweepEntry e;
+                    double w = weight(dels, delt, deln);
+                    SweepEntry &e = ent[e_at++];
                     e.k = k;
                     e.pad = d | (s << 8);   // list and neighbour slot
                     e.w[0] = dels * w; e.w[1] = delt * w; e.w[2] = deln * w;
-                    per[p].push_back(e);
                     need[p] |= 1u << s;
-                    ++taken;
                 }
-                cnt[(size_t)p * NDIR + d] = (uint8_t)taken;
             }
-        }
-        for (int p = 0; p < n; ++p) {
-            off[p] = (int32_t)ent.size();
-            ent.insert(ent.end(), per[p].begin(), per[p].end());
-        }
-        off[n] = (int32_t)ent.size();
+        });
         for (int p = 0; p < n; ++p)
             if (off[p + 1] - off[p] > SWEEP_MAX_ENTRIES) return false;
         // levels: longest path over swept dependencies

@@ -86,3 +86,50 @@ def test_point_one_is_not_swept(small_cloud):
     assert 1 not in set(pwa.tolist())
     assert pwa[-1] == 0
     assert s.levels(0)[0] == -1
+
+
+def _level_check(s, c, direction):
+    """Levels are exactly the longest-path depths over swept dependencies."""
+    counts, lists = s.stencils(27)
+    alias, pwa = s.alias()
+    st = c.status
+    swept = np.zeros(c.n, bool)
+    pw = pwa[pwa > 0] - 1
+    swept[pw[(st[pw] == 0) | (st[pw] == 1)]] = True
+    ps, ks = [], []
+    for d in range(6):
+        for j in range(27):
+            m = (counts[:, d] > j) & ((st == 0) | ((st == 1) & (d < 4)))
+            ps.append(np.nonzero(m)[0])
+            ks.append(lists[m, d, j] - 1)
+    wall = np.nonzero(st == 1)[0]
+    for j in range(27):
+        m = c.nbhs[wall] > j
+        ps.append(wall[m])
+        ks.append(c.conn[wall[m], j] - 1)
+    p, k = np.concatenate(ps), np.concatenate(ks)
+    keep = swept[p] & swept[k] & ((alias[k] < alias[p]) if direction == 0 else (alias[k] > alias[p]))
+    p, k = p[keep], k[keep]
+    lv = s.levels(direction)
+    assert np.array_equal(lv >= 0, swept)
+    assert np.all(lv[k] < lv[p])
+    deepest = np.full(c.n, -1)
+    np.maximum.at(deepest, p, lv[k])
+    assert np.array_equal(lv[swept], deepest[swept] + 1)
+
+
+def test_large_cloud_parallel_setup(oracle_lib):
+    """Above the size where the set-up runs its per-point loops on several
+    host threads: stencils and alias still equal the oracle's, and the sweep
+    levels are the exact longest-path depths."""
+    from mfcfd import cloud
+    c = cloud.shell_cloud(12, 6000, r1=3.0, seed=4242)
+    assert c.n >= 1 << 16
+    s = _solver(c)
+    o = oracle_lib.Oracle(c, 0.4, 0.0)
+    cs, ls = s.stencils(27)
+    co, lo = o.stencils(27)
+    assert np.array_equal(cs, co) and np.array_equal(ls, lo)
+    assert all(np.array_equal(x, y) for x, y in zip(s.alias(), o.alias()))
+    for direction in (0, 1):
+        _level_check(s, c, direction)
