@@ -44,7 +44,8 @@ namespace {
 
 const char *kStrerr[] = {"ok", "bad argument", "CUDA error", "stencil too wide",
                          "singular least-squares system", "non-finite residual",
-                         "unsupported input", "out of device memory", "device wait timed out"};
+                         "unsupported input", "out of device memory", "device wait timed out",
+                         "file input/output error"};
 
 int fail(mfcfd_handle *h, int code, const std::string &msg) {
     if (h) h->err = msg;
@@ -517,13 +518,56 @@ int mfcfd_destroy(mfcfd_handle *h) {
 }
 
 const char *mfcfd_last_error(const mfcfd_handle *h) {
-    if (!h) return "null handle";
+    if (!h) return g_io_err.c_str();
     return h->err.c_str();
 }
 
 const char *mfcfd_strerror(int code) {
-    if (code < 0 || code > MFCFD_ERR_TIMEOUT) return "unknown error";
+    if (code < 0 || code > MFCFD_ERR_IO) return "unknown error";
     return kStrerr[code];
+}
+
+int mfcfd_count_input_points(const char *path, int32_t *n) {
+    if (!path || !n) return MFCFD_ERR_ARG;
+    return io_count_input_points(path, n);
+}
+
+int mfcfd_read_input_point_data(const char *path, int32_t n, int32_t *status, double *x, double *y,
+                                double *z, double *tan1, double *tan2, double *nor, int32_t *nbhs,
+                                int32_t *conn, double *min_dist) {
+    if (!path || n < 1 || !status || !x || !y || !z || !tan1 || !tan2 || !nor || !nbhs || !conn || !min_dist)
+        return MFCFD_ERR_ARG;
+    return io_read_input_point_data(path, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist);
+}
+
+int mfcfd_read_stored_solution(const char *path, int32_t n, double *prim) {
+    if (!path || n < 1 || !prim) return MFCFD_ERR_ARG;
+    return io_read_stored_solution(path, n, prim);
+}
+
+int mfcfd_print_primal_output(mfcfd_handle *h, const char *dir) {
+    if (!h || !dir) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    const size_t n = (size_t)h->d.n;
+    std::vector<double> x(n), y(n), z(n), prim(5 * n), flux(5 * n), dq(15 * n);
+    CK(cudaMemcpyAsync(x.data(), h->d.x, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(y.data(), h->d.y, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(z.data(), h->d.z, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(prim.data(), h->d.prim, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(flux.data(), h->d.flux_res, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(dq.data(), h->d.dq, 15 * n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int32_t> status(n);
+    for (size_t i = 0; i < n; ++i) status[i] = h->T.cls[i];   // statuses 0/1/2 are the classes
+    int rc = io_write_primal_output(dir, (int32_t)n, status.data(), x.data(), y.data(), z.data(), prim.data(),
+                                    flux.data(), dq.data());
+    if (rc) return fail(h, rc, g_io_err);
+    return MFCFD_OK;
+}
+
+int mfcfd_write_residue(const char *path, int32_t t0, int32_t iters, const double *res_hist, int32_t append) {
+    if (!path || iters < 0 || (iters > 0 && !res_hist)) return MFCFD_ERR_ARG;
+    return io_write_residue(path, t0, iters, res_hist, append);
 }
 
 }  // extern "C"

@@ -187,6 +187,19 @@ int reduction_blocks(int n);
 // and blocks (one block per SM, some SMs left free); returns the warps, 0 if
 // the kernel cannot run on the device.
 int chain_shape(int device, int want, int *wpb, int *blocks);
+// File formats of the reference program (mfcfd_io.cpp).  Handle-less calls
+// leave their message in g_io_err (mfcfd_last_error(NULL)).
+extern thread_local std::string g_io_err;
+int io_count_input_points(const char *path, int32_t *n);
+int io_read_input_point_data(const char *path, int32_t n, int32_t *status, double *x, double *y,
+                             double *z, double *tan1, double *tan2, double *nor, int32_t *nbhs,
+                             int32_t *conn, double *min_dist);
+int io_read_stored_solution(const char *path, int32_t n, double *prim);
+int io_write_primal_output(const std::string &dir, int32_t n, const int32_t *status, const double *x,
+                           const double *y, const double *z, const double *prim, const double *flux_res,
+                           const double *dq);
+int io_write_residue(const char *path, int32_t t0, int32_t iters, const double *res_hist, int append);
+
 // Allocation-free residual (mfcfd_residual_noalloc); the current device must
 // be the handle's.
 int residual_noalloc(const DevCloud &d, cudaStream_t s, double *res_new, std::string &err);

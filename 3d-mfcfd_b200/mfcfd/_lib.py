@@ -10,7 +10,8 @@ LIB_PATH = os.path.join(_HERE, "libmfcfd.so")
 MFCFD_OK = 0
 ERRORS = {1: "bad argument", 2: "CUDA error", 3: "stencil too wide",
           4: "singular least-squares system", 5: "non-finite residual",
-          6: "unsupported input", 7: "out of device memory", 8: "device wait timed out"}
+          6: "unsupported input", 7: "out of device memory", 8: "device wait timed out",
+          9: "file input/output error"}
 
 FIELD_PRIM, FIELD_U, FIELD_Q, FIELD_QM, FIELD_DQ, FIELD_DELT, FIELD_FLUX_RES, \
     FIELD_DELUP, FIELD_DELUN, FIELD_DINV = range(10)
@@ -23,7 +24,8 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_run", "mfcfd_get", "mfcfd_get_state", "mfcfd_set_state",
            "mfcfd_get_stencils", "mfcfd_get_alias", "mfcfd_get_levels", "mfcfd_get_info",
            "mfcfd_get_stream", "mfcfd_set_profiling", "mfcfd_get_phase_times",
-           "mfcfd_residual_noalloc",
+           "mfcfd_residual_noalloc", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
+           "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
 NOALLOC_MAX_TERMS = 1024 * 4096
 NPHASE = 7
@@ -93,6 +95,12 @@ def lib():
     L.mfcfd_set_profiling.argtypes = [vp, i32]
     L.mfcfd_get_phase_times.argtypes = [vp, vp, vp]
     L.mfcfd_residual_noalloc.argtypes = [vp, vp]
+    cp = ctypes.c_char_p
+    L.mfcfd_count_input_points.argtypes = [cp, vp]
+    L.mfcfd_read_input_point_data.argtypes = [cp, i32] + [vp] * 10
+    L.mfcfd_read_stored_solution.argtypes = [cp, i32, vp]
+    L.mfcfd_print_primal_output.argtypes = [vp, cp]
+    L.mfcfd_write_residue.argtypes = [cp, i32, i32, vp, i32]
     L.mfcfd_destroy.argtypes = [vp]
     L.mfcfd_last_error.argtypes = [vp]
     L.mfcfd_last_error.restype = ctypes.c_char_p

@@ -80,6 +80,12 @@ class Solver:
             self.history.append((t0 + j, float(hist[j, 0]), float(hist[j, 1])))
         return hist
 
+    def print_primal_output(self, directory: str = "."):
+        """post_processor.f90:13-44: primal-solution.dat, flux-residual.dat,
+        qderivatives.dat and an empty normals.dat in `directory`."""
+        import os
+        self._check(_lib.lib().mfcfd_print_primal_output(self.h, os.fsencode(directory)))
+
     # -- data access ---------------------------------------------------------
     def get(self, field: int) -> np.ndarray:
         w = FIELD_WIDTH[field]

@@ -45,8 +45,9 @@ extern "C" {
 #define MFCFD_ERR_UNSUPPORTED  6   /* input the library does not handle */
 #define MFCFD_ERR_NOMEM        7   /* device allocation failed */
 #define MFCFD_ERR_TIMEOUT      8   /* a bounded device wait ran out */
+#define MFCFD_ERR_IO           9   /* a file could not be read, parsed or written */
 
-/* fields for mfcfd_get / mfcfd_set_field (Fortran layout, width x N) */
+/* fields for mfcfd_get (Fortran layout, width x N) */
 #define MFCFD_FIELD_PRIM      0    /* point%prim(5,N)        width 5  */
 #define MFCFD_FIELD_U         1    /* point%U(5,N)           width 5  */
 #define MFCFD_FIELD_Q         2    /* point%q(5,N)           width 5  */
@@ -206,8 +207,38 @@ int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters);
 #define MFCFD_NOALLOC_MAX_TERMS (1024 * 4096)
 int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new);
 
+/*
+ * File formats of the reference program, for a host that replaces the whole
+ * Fortran program (meshfree_solver.f90:20-37), not only its solver loop.
+ * Input follows Fortran list-directed READ (one READ per record; blanks,
+ * commas or line ends between values; r*value repeats; E or D exponents).
+ * Output has the layout of gfortran's list-directed WRITE (17 significant
+ * digits, so the values read back exactly).  Handle-less calls report
+ * through mfcfd_last_error(NULL) (per host thread).
+ */
+/* Number of point records in a 3d_input_data file. */
+int mfcfd_count_input_points(const char *path, int32_t *n);
+/* read_input_point_data (point_preprocessor.f90:25-36): n records of
+ * `idx status x y z tan1(3) tan2(3) nor(3) nbhs conn(1:nbhs) min_dist` into
+ * arrays laid out as mfcfd_create takes them (conn (27,N) zero-padded). */
+int mfcfd_read_input_point_data(const char *path, int32_t n, int32_t *status, double *x, double *y,
+                                double *z, double *tan1, double *tan2, double *nor, int32_t *nbhs,
+                                int32_t *conn, double *min_dist);
+/* initial_conditions (initial_conditions.f90:18-29): stored-solution.dat,
+ * `x y z rho u1 u2 u3 p` per point, into prim (5,N). */
+int mfcfd_read_stored_solution(const char *path, int32_t n, double *prim);
+/* print_primal_output (post_processor.f90:13-44): writes primal-solution.dat
+ * (x y z prim), flux-residual.dat (k status flux_res), qderivatives.dat
+ * (k status dq(3,1:5,k)) and an empty normals.dat into directory dir. */
+int mfcfd_print_primal_output(mfcfd_handle *h, const char *dir);
+/* residue.dat lines `t res_new residue` (q_lskum.f90:22,31) for
+ * t = t0 .. t0+iters-1 from an mfcfd_run history; append != 0 appends. */
+int mfcfd_write_residue(const char *path, int32_t t0, int32_t iters, const double *res_hist, int32_t append);
+
 int mfcfd_destroy(mfcfd_handle *h);
 
+/* Message of the last failure on h; with h = NULL, of the calling thread's
+ * last failed handle-less call (file functions). */
 const char *mfcfd_last_error(const mfcfd_handle *h);
 const char *mfcfd_strerror(int code);
 
