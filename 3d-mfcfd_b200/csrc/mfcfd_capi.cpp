@@ -208,8 +208,13 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     if (!h) return MFCFD_ERR_NOMEM;
     h->P = *params;
     const mfcfd_params &P = h->P;
-    if (P.power != 0.0 || P.inner_iterations != 0 || P.precision != MFCFD_PRECISION_FP64) {
-        h->err = "only power = 0, inner_iterations = 0 and FP64 are implemented";
+    if (P.inner_iterations < 0 || P.inner_iterations > 1000) {
+        h->err = "inner_iterations out of range [0, 1000]";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
+    if (P.power != 0.0 || P.precision != MFCFD_PRECISION_FP64) {
+        h->err = "only power = 0 and FP64 are implemented";
         *out = h;
         return MFCFD_ERR_UNSUPPORTED;
     }
@@ -248,6 +253,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.shared_frame = T.shared_frame;
     std::memcpy(d.frame0, T.frame0, sizeof d.frame0);
     d.power = P.power;
+    d.inner_iterations = P.inner_iterations;
     d.cfl = P.cfl;
     d.rho_inf = P.rho_inf; d.u1_inf = P.u1_inf; d.u2_inf = P.u2_inf;
     d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;
@@ -319,6 +325,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     AL(d.delt, n); AL(d.flux_res, n5); AL(d.dUp, n5); AL(d.dUn, n5); AL(d.dinv, n);
     AL(d.gold, (size_t)n * 30); AL(d.dgf, (size_t)n * DG_STRIDE); AL(d.dgb, (size_t)n * DG_STRIDE);
     AL(d.res_sqr, n); AL(d.partial, 1024); AL(d.res_dev, h->res_cap);
+    if (P.inner_iterations > 0) AL(d.dq_tmp, (size_t)n * 15);
 #undef AL
     CK(cudaMemsetAsync(d.dUp, 0, n5 * 8, h->stream));
     CK(cudaMemsetAsync(d.dUn, 0, n5 * 8, h->stream));

@@ -124,6 +124,7 @@ struct DevCloud {
     int shared_frame;
     double frame0[9];
     double power, cfl;
+    int inner_iterations;         // second-order q-derivative passes
     double rho_inf, u1_inf, u2_inf, u3_inf, pr_inf;
     // geometry
     const double *x, *y, *z;
@@ -161,6 +162,7 @@ struct DevCloud {
     const ChainItem *ch_items[2];
     // state (Fortran layout, point-major)
     double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
+    double *dq_tmp;               // 15 per point: inner-iteration output (or null)
     double *gold;                 // 30 per point: fluxes of prim in frame0
     double *dgf, *dgb;            // DG_STRIDE per point: published flux increments
     double *res_sqr;              // per point (residual sum terms)

@@ -116,6 +116,54 @@ __global__ void __launch_bounds__(128) k_qderiv(DevCloud d) {
     d.delt[i] = min_delt;
 }
 
+// One inner iteration of the second-order q-derivatives
+// (q_derivatives.f90:116-201): least squares over conn of the differences of
+// the half-step reconstructions q - dq.del/2 at both ends, from dq_in into
+// dq_out (the reference's point%temp, copied back after the pass).
+__global__ void __launch_bounds__(128) k_qinner(DevCloud d, const double *dq_in, double *dq_out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.n) return;
+    const double xi = d.x[i], yi = d.y[i], zi = d.z[i];
+    double qi[5], dqi[15];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) qi[r] = d.q[5 * (size_t)i + r];
+#pragma unroll
+    for (int c = 0; c < 15; ++c) dqi[c] = dq_in[15 * (size_t)i + c];
+    double xx = 0, yy = 0, zz = 0, xy = 0, yz = 0, zx = 0;
+    double sx[5] = {0, 0, 0, 0, 0}, sy[5] = {0, 0, 0, 0, 0}, sz[5] = {0, 0, 0, 0, 0};
+    const int nb = d.nbhs[i];
+    const int32_t *cn = d.conn + (size_t)MAX_CONN * i;
+    for (int j = 0; j < nb; ++j) {
+        const int k = cn[j];
+        const double delx = d.x[k] - xi, dely = d.y[k] - yi, delz = d.z[k] - zi;
+        xx = xx + delx * delx;
+        yy = yy + dely * dely;
+        zz = zz + delz * delz;
+        xy = xy + delx * dely;
+        yz = yz + dely * delz;
+        zx = zx + delz * delx;
+        const double *dqk = dq_in + 15 * (size_t)k;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            const double qti = qi[r] - 0.5 * (delx * dqi[3 * r] + dely * dqi[3 * r + 1] + delz * dqi[3 * r + 2]);
+            const double qtn = d.q[5 * (size_t)k + r] - 0.5 * (delx * dqk[3 * r] + dely * dqk[3 * r + 1] + delz * dqk[3 * r + 2]);
+            const double t = qtn - qti;
+            sx[r] = sx[r] + delx * t;
+            sy[r] = sy[r] + dely * t;
+            sz[r] = sz[r] + delz * t;
+        }
+    }
+    const double g[6] = {xx, yy, zz, xy, yz, zx};
+    const double det = xx * (yy * zz - yz * yz) - xy * (xy * zz - yz * zx) + zx * (xy * yz - yy * zx);
+    const double one_by_det = 1.0 / det;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        dq_out[15 * (size_t)i + 3 * r + 0] = cramer_num(0, g, sx[r], sy[r], sz[r]) * one_by_det;
+        dq_out[15 * (size_t)i + 3 * r + 1] = cramer_num(1, g, sx[r], sy[r], sz[r]) * one_by_det;
+        dq_out[15 * (size_t)i + 3 * r + 2] = cramer_num(2, g, sx[r], sy[r], sz[r]) * one_by_det;
+    }
+}
+
 // ---------------------------------------------------------------- hand-off words
 
 // Hand-off of increments between warps.  Before the sweeps, k_dinv_gold sets
@@ -1085,6 +1133,10 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     const int fblocks = (n + FLUX_WARPS - 1) / FLUX_WARPS;
     mark(0, s);
     k_qderiv<<<(n + 127) / 128, 128, 0, s>>>(d);
+    for (int j = 0; j < d.inner_iterations; ++j) {
+        k_qinner<<<(n + 127) / 128, 128, 0, s>>>(d, d.dq, d.dq_tmp);
+        cudaMemcpyAsync(d.dq, d.dq_tmp, sizeof(double) * 15 * (size_t)n, cudaMemcpyDeviceToDevice, s);
+    }
     mark(1, s);
     if (chains) {
         // the flux residual and the sweep inputs run on the side stream beside

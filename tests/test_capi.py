@@ -74,6 +74,9 @@ def test_bad_inputs_are_status_codes(mfcfd_lib, small_cloud):
     with pytest.raises(MfcfdError) as e:
         _create(mfcfd_lib, small_cloud, sweep_mode=3)
     assert e.value.code == 1
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, small_cloud, inner_iterations=-1)
+    assert e.value.code == 1
 
 
 def test_host_only_handle_refuses_device_calls(mfcfd_lib, small_cloud):

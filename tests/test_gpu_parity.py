@@ -14,11 +14,11 @@ pytestmark = pytest.mark.gpu
 FIELDS = ["PRIM", "U", "Q", "QM", "DQ", "DELT", "FLUX_RES", "DELUP", "DELUN"]
 
 
-def _pair(cloud, mach, aoa, libm, oracle_lib, sweep_mode=0):
+def _pair(cloud, mach, aoa, libm, oracle_lib, sweep_mode=0, inner_iterations=0):
     from mfcfd.solver import Solver
     from mfcfd.cloud import initial_state
-    s = Solver(cloud, mach, aoa, sweep_mode=sweep_mode)
-    o = oracle_lib.Oracle(cloud, mach, aoa, libm=libm)
+    s = Solver(cloud, mach, aoa, sweep_mode=sweep_mode, inner_iterations=inner_iterations)
+    o = oracle_lib.Oracle(cloud, mach, aoa, libm=libm, inner_iterations=inner_iterations)
     prim0 = initial_state(cloud, mach, aoa)
     s.initial_conditions(prim0)
     o.set_prim(prim0)
@@ -67,3 +67,15 @@ def test_against_glibc_oracle(small_cloud, oracle_lib, mfcfd_lib):
         assert abs(hist[t - 1, 0] - rc[0]) <= 1e-10 * abs(rc[0]), t
     a, b = s.get(mfcfd_lib.FIELD_PRIM), o.get(oracle_lib.FIELD_PRIM)
     np.testing.assert_allclose(a, b, rtol=1e-11, atol=1e-14)
+
+
+@pytest.mark.parametrize("inner", [1, 3])
+def test_inner_iterations_bitexact(small_cloud, oracle_lib, mfcfd_lib, inner):
+    """Second-order q-derivatives (q_derivatives.f90:116-201), every field."""
+    s, o = _pair(small_cloud, 0.8, 2.0, oracle_lib.LIBM_MFMATH, oracle_lib, inner_iterations=inner)
+    s.q_lskum(3)
+    for t in range(1, 4):
+        o.step(t)
+    for name, fg, fo in _field_ids(oracle_lib):
+        a, b = s.get(fg), o.get(fo)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name

@@ -152,5 +152,5 @@ def test_program_end_to_end(mfcfd_lib, oracle_lib, small_cloud, tmp_path):
     for t in range(1, 6):
         o.step(t)
     a = _table(tmp_path / "primal-solution.dat")
-    assert np.array_equal(a[:, 3:], o.get("prim"))
+    assert np.array_equal(a[:, 3:], o.get(oracle_lib.FIELD_PRIM))
     s.close()
