@@ -326,6 +326,12 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     AL(d.gold, (size_t)n * 30); AL(d.dgf, (size_t)n * DG_STRIDE); AL(d.dgb, (size_t)n * DG_STRIDE);
     AL(d.res_sqr, n); AL(d.partial, 1024); AL(d.res_dev, h->res_cap);
     if (P.inner_iterations > 0) AL(d.dq_tmp, (size_t)n * 15);
+    if (!T.ss_pts.empty()) {
+        AL(d.dU_old, n5);
+        d.n_ss = (int)T.ss_pts.size();
+        if ((rc = upload(h, &d.ss_pts, T.ss_pts))) return rc;
+        if ((rc = upload(h, &d.ss_src, T.ss_src))) return rc;
+    }
 #undef AL
     CK(cudaMemsetAsync(d.dUp, 0, n5 * 8, h->stream));
     CK(cudaMemsetAsync(d.dUn, 0, n5 * 8, h->stream));
@@ -467,7 +473,7 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
     info->n_wall = (int32_t)T.wall_idx.size();
     info->n_outer = (int32_t)T.outer_idx.size();
     info->n_interior = (int32_t)T.interior_idx.size();
-    info->n_supersonic = 0;
+    info->n_supersonic = (int32_t)(T.ss_inlet_idx.size() + T.ss_outlet_idx.size());
     info->n_levels_forward = T.fwd_lvl_ptr.empty() ? 0 : (int32_t)T.fwd_lvl_ptr.size() - 1;
     info->n_levels_backward = T.bwd_lvl_ptr.empty() ? 0 : (int32_t)T.bwd_lvl_ptr.size() - 1;
     info->max_level_width = T.max_level_width;

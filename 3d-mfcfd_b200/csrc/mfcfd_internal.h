@@ -19,7 +19,10 @@ constexpr int LIST_STRIDE = 28;   // bytes per (point, list) entry table: <= 27 
 constexpr int GEO_STRIDE = 48;    // doubles per point: 6 lists x 8
 constexpr int NDIR = 6;           // xpos, xneg, ypos, yneg, zpos, zneg
 
-enum PointClass : int8_t { CLS_INTERIOR = 0, CLS_WALL = 1, CLS_OUTER = 2, CLS_OTHER = 3 };
+// status 0, 1, 2 and 5/6 (supersonic inlet / outlet: not in any split list;
+// the sweeps copy the increment of the nearest neighbour, the state update
+// its state)
+enum PointClass : int8_t { CLS_INTERIOR = 0, CLS_WALL = 1, CLS_OUTER = 2, CLS_SUPERSONIC = 3 };
 
 // geo layout within one list's 8 doubles
 enum { G_XX = 0, G_YY, G_ZZ, G_XY, G_YZ, G_ZX, G_DET, G_DNUM };
@@ -71,6 +74,13 @@ struct Topology {
     double frame0[9] = {0};
     int max_level_width = 0;
     std::vector<int32_t> wall_idx, outer_idx, interior_idx;   // 0-based, index order
+    std::vector<int32_t> ss_inlet_idx, ss_outlet_idx;          // status 5, 6
+    // supersonic points: the sweeps' copy source (nearest neighbour, -1 if
+    // none within 1e6) per point, and the state update's copies in the
+    // reference's order (outlets, then inlets) with their sources (nearest
+    // non-wall neighbour, -1 if none within 1e5)
+    std::vector<int32_t> copy_src;
+    std::vector<int32_t> ss_pts, ss_src;
 };
 
 // One point of a sweep as a warp of the chain schedule reads it: the point,
@@ -86,10 +96,21 @@ enum : uint32_t {
     CI_WALL = 1,      // wall point (LdelU counts its lists twice, zpos skipped)
     CI_SHARED = 2,    // consumer in the shared frame (reads published increments)
     CI_PUBLISH = 4,   // some consumer reads this point's increment from global memory
+    CI_COPY = 8,      // supersonic point: copies its nearest neighbour's increment
 };
 // Bits the chain schedule adds to SweepEntry::pad (bits 0-15: list, slot).
 constexpr int32_t ENT_RING = 1 << 17;   // producer's increment is in the warp's ring
 constexpr int ENT_RING_SHIFT = 18;      // ring slot (4 bits)
+constexpr int32_t ENT_CHAIN_BITS = 0xff << 16;
+// The single entry of a supersonic point: k = the copy source (-1: none).
+// With ENT_COPY_NEW the source is updated earlier in the same sweep (a
+// dependency); without it the copy reads the source's increment from before
+// the sweep (the previous iteration's delUn).
+constexpr int32_t ENT_COPY = 1 << 24;
+constexpr int32_t ENT_COPY_NEW = 1 << 25;
+inline bool entry_is_dependency(const SweepEntry &e) {
+    return !(e.pad & ENT_COPY) || (e.pad & ENT_COPY_NEW);
+}
 constexpr int CHAIN_RING = 8;           // increments a warp keeps in shared memory
 // Published flux increments: per point 6 lists x (5 components + 1 pad), so
 // every list's record starts on a 16-byte boundary (cp.async.cg copies).
@@ -163,6 +184,9 @@ struct DevCloud {
     // state (Fortran layout, point-major)
     double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
     double *dq_tmp;               // 15 per point: inner-iteration output (or null)
+    double *dU_old;               // 5 per point: delUn before the sweeps (supersonic copies)
+    int n_ss;                     // supersonic points (state-update copies)
+    const int32_t *ss_pts, *ss_src;
     double *gold;                 // 30 per point: fluxes of prim in frame0
     double *dgf, *dgb;            // DG_STRIDE per point: published flux increments
     double *res_sqr;              // per point (residual sum terms)

@@ -11,6 +11,7 @@
  *                 on all SMs (k_sweep_df: dynamic topological order;
  *                 k_sweep_levels: one CTA, level by level)
  *   k_update      state_update_implicit + next iteration's U and q
+ *                 (k_update_ss: supersonic points' copies, in order)
  *   k_reduce_*    res_new (deterministic two-pass sum)
  * State stays resident in HBM in the reference's point-major layout.
  *
@@ -289,7 +290,7 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
 #pragma unroll
     for (int r = 0; r < 5; ++r) p[r] = d.prim[5 * (size_t)i + r];
     const bool swept = d.swept[i] != 0;
-    if (swept) {
+    if (swept && d.cls[i] <= CLS_WALL) {   // D_inv of wall and interior points
         const double as = sqrt(1.40 * p[4] / p[0]);
         const double u = (lane >> 1) == 0 ? p[1] : ((lane >> 1) == 1 ? p[2] : p[3]);
         const double t = lane < NDIR ? dinv_term(d, i, lane, u, as) : 0.0;
@@ -457,12 +458,12 @@ __global__ void k_pending(DevCloud d, int inputs) {
         if (d.swept[w / 5]) {
             d.dUp[w] = pend;
             d.dUn[w] = pend;
-            if (inputs) d.flux_res[w] = pend;
+            if (inputs && d.cls[w / 5] <= CLS_WALL) d.flux_res[w] = pend;
         }
     }
     if (inputs) {
         for (size_t w = t0; w < (size_t)d.n; w += stride)
-            if (d.swept[w]) d.dinv[w] = pend;
+            if (d.swept[w] && d.cls[w] <= CLS_WALL) d.dinv[w] = pend;
         if (d.shared_frame)
             for (size_t w = t0; w < n30; w += stride)
                 if (d.swept[w / 30]) d.gold[w] = pend;
@@ -479,7 +480,7 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
     if (i >= d.n) return;
     const int cls = d.cls[i];
     const double *p = d.prim + 5 * (size_t)i;
-    if (d.swept[i]) {
+    if (d.swept[i] && cls <= CLS_WALL) {
         const double as = sqrt(1.40 * p[4] / p[0]);
         double gd[NDIR];
 #pragma unroll
@@ -573,7 +574,8 @@ __device__ __forceinline__ ChainItem make_item(const DevCloud &d, int p, bool fo
     it.cnt = 0;
 #pragma unroll
     for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[e] << (5 * e);
-    it.info = (d.cls[p] == CLS_WALL ? CI_WALL : 0u) | (d.consumer_shared[p] ? CI_SHARED : 0u) | CI_PUBLISH;
+    it.info = (d.cls[p] == CLS_WALL ? CI_WALL : 0u) | (d.consumer_shared[p] ? CI_SHARED : 0u) | CI_PUBLISH |
+              (d.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u);
     return it;
 }
 
@@ -628,7 +630,8 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     const int p = it.p;
     const bool wall = (it.info & CI_WALL) != 0;
     const bool shared = (it.info & CI_SHARED) != 0;
-    const int cls = wall ? CLS_WALL : CLS_INTERIOR;   // swept points are wall or interior
+    const bool copy = (it.info & CI_COPY) != 0;       // supersonic point
+    const int cls = wall ? CLS_WALL : CLS_INTERIOR;   // of the points that solve
     const SweepEntry *E = st->ent;
     const int dd = lane / 5, c = lane - 5 * (lane / 5);
     int total = 0, lo = 0, hi = 0;
@@ -655,7 +658,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     }
     // inputs the concurrent flux kernel had not produced when the stage was copied
     if (lane < 30 && is_pending(gold)) gold = poll_word(d.gold + 30 * (size_t)p + lane, d.err);
-    if (lane < 5) {
+    if (lane < 5 && !copy) {
         if (is_pending(dinv)) dinv = poll_word(d.dinv + p, d.err);
         if (is_pending(base5)) base5 = poll_word((forward ? d.flux_res : d.dUp) + 5 * (size_t)p + lane, d.err);
     }
@@ -664,136 +667,150 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     for (int r = 0; r < 5; ++r) Up[r] = st->U[r];
     Frame Fp;
     load_frame(st->frame, Fp);
-    const uint32_t need = shared ? 0u : st->need;
-    const bool mine = !shared && (need >> lane) & 1u;
-    int k_slot = 0, mask_slot = 0;
-    if (mine) {
-        k_slot = st->slot_nbr[lane];
-        mask_slot = st->slot_mask[lane];
-        double po[5];
-#pragma unroll
-        for (int r = 0; r < 5; ++r) po[r] = d.prim[5 * (size_t)k_slot + r];
-        FluxPre Po;
-        flux_pre(po, Fp, Po);
-        int axes = 0;
-#pragma unroll
-        for (int e = 0; e < NDIR; ++e)
-            if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
-        AxisTerms Ao[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-            if (axes & (1 << a)) axis_terms(Po, a, Ao[a]);
-        for (int e = 0; e < NDIR; ++e) {
-            if (!(mask_slot & (1 << e))) continue;
-            const int kind = flux_kind(cls, e);
-#pragma unroll
-            for (int cc = 0; cc < 5; ++cc) T[(e * MAX_SLOTS + lane) * 5 + cc] = flux_component(kind, cc, Po, Ao);
-        }
-    }
-
-    // ---- phase B
-    if (shared) {
-        // lane owns entries lane, lane+32, lane+64; all their loads are in
-        // flight together, re-polling only the ones still pending
-        const double *src = forward ? d.dgf : d.dgb;
-        uint32_t pend = 0;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const int j = lane + 32 * q;
-            if (j >= total) continue;
-            const int pad = E[j].pad;
-            if (CHAINS && (pad & ENT_RING)) {
-                const double *rs = ring + 30 * ((pad >> ENT_RING_SHIFT) & 15) + 5 * (pad & 255);
-#pragma unroll
-                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = rs[cc];
-            } else {
-                pend |= 1u << q;
-            }
-        }
-        int spins = 0;
-        while (pend) {
-            unsigned long long v[3][5];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                if (!((pend >> q) & 1u)) continue;
-                const int j = lane + 32 * q;
-                const double *gs = src + DG_STRIDE * (size_t)E[j].k + DG_LIST * (E[j].pad & 255);
-                ld_relaxed_v2(gs, v[q][0], v[q][1]);
-                ld_relaxed_v2(gs + 2, v[q][2], v[q][3]);
-                v[q][4] = ld_relaxed_b64(gs + 4);
-            }
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                if (!((pend >> q) & 1u) || !ready5(v[q])) continue;
-                const int j = lane + 32 * q;
-#pragma unroll
-                for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __longlong_as_double(v[q][cc]);
-                pend &= ~(1u << q);
-            }
-            if (pend && !spin_continue(spins, d.err)) break;
-        }
-    } else if (mine) {
-        const double *dsrc = (forward ? d.dUp : d.dUn) + 5 * (size_t)k_slot;
-        unsigned long long v[5];
-        int spins = 0;
-        do {
-#pragma unroll
-            for (int r = 0; r < 5; ++r) v[r] = ld_relaxed_b64(dsrc + r);
-        } while (!ready5(v) && spin_continue(spins, d.err));
-        double U[5], pn[5];
-#pragma unroll
-        for (int r = 0; r < 5; ++r) U[r] = __longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r];
-        Frame Fk;
-        load_frame(d.frame + 9 * (size_t)k_slot, Fk);
-        conserved_to_primitive(U, Fk, pn);
-        FluxPre Pn;
-        flux_pre(pn, Fp, Pn);
-        int axes = 0;
-#pragma unroll
-        for (int e = 0; e < NDIR; ++e)
-            if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
-        AxisTerms An[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-            if (axes & (1 << a)) axis_terms(Pn, a, An[a]);
-        for (int e = 0; e < NDIR; ++e) {
-            if (!(mask_slot & (1 << e))) continue;
-            const int kind = flux_kind(cls, e);
-#pragma unroll
-            for (int cc = 0; cc < 5; ++cc) {
-                double *t = &T[(e * MAX_SLOTS + lane) * 5 + cc];
-                *t = flux_component(kind, cc, Pn, An) - *t;
-            }
-        }
-    }
-    __syncwarp();
-
-    // ---- phase C
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    if (lane < 30) {
-        for (int jj = lo; jj < hi; ++jj) {
-            const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
-            sx = sx + t * E[jj].w[0];
-            sy = sy + t * E[jj].w[1];
-            sz = sz + t * E[jj].w[2];
-        }
-    }
-    double G = 0.0;
-    if (lane < 30) G = cramer_num(dd >> 1, g, sx, sy, sz) / g[6];
-    double gd[NDIR];
-#pragma unroll
-    for (int e = 0; e < NDIR; ++e) gd[e] = __shfl_sync(FULL, G, e * 5 + (lane % 5));
     double dnew = 0.0;
-    if (lane < 5) {
-        double lu;
-        if (wall) lu = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
-        else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
-        if (forward) {
-            dnew = -(dinv * (base5 + lu));
-            st_relaxed_f64(d.dUp + 5 * (size_t)p + lane, dnew);
-        } else {
-            dnew = base5 - dinv * lu;
-            st_relaxed_f64(d.dUn + 5 * (size_t)p + lane, dnew);
+    if (copy) {
+        // implicit_forward_and_reverse_sweeps.f90:38-51 / :69-82: the
+        // nearest neighbour's increment, updated earlier in this sweep or
+        // from before it
+        if (lane < 5) {
+            const int q = E[0].k;
+            double *dst = (forward ? d.dUp : d.dUn) + 5 * (size_t)p + lane;
+            if (q >= 0)
+                dnew = (E[0].pad & ENT_COPY_NEW) ? poll_word((forward ? d.dUp : d.dUn) + 5 * (size_t)q + lane, d.err)
+                                                 : d.dU_old[5 * (size_t)q + lane];
+            st_relaxed_f64(dst, dnew);
+        }
+    } else {
+        const uint32_t need = shared ? 0u : st->need;
+        const bool mine = !shared && (need >> lane) & 1u;
+        int k_slot = 0, mask_slot = 0;
+        if (mine) {
+            k_slot = st->slot_nbr[lane];
+            mask_slot = st->slot_mask[lane];
+            double po[5];
+#pragma unroll
+            for (int r = 0; r < 5; ++r) po[r] = d.prim[5 * (size_t)k_slot + r];
+            FluxPre Po;
+            flux_pre(po, Fp, Po);
+            int axes = 0;
+#pragma unroll
+            for (int e = 0; e < NDIR; ++e)
+                if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
+            AxisTerms Ao[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                if (axes & (1 << a)) axis_terms(Po, a, Ao[a]);
+            for (int e = 0; e < NDIR; ++e) {
+                if (!(mask_slot & (1 << e))) continue;
+                const int kind = flux_kind(cls, e);
+#pragma unroll
+                for (int cc = 0; cc < 5; ++cc) T[(e * MAX_SLOTS + lane) * 5 + cc] = flux_component(kind, cc, Po, Ao);
+            }
+        }
+
+        // ---- phase B
+        if (shared) {
+            // lane owns entries lane, lane+32, lane+64; all their loads are in
+            // flight together, re-polling only the ones still pending
+            const double *src = forward ? d.dgf : d.dgb;
+            uint32_t pend = 0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int j = lane + 32 * q;
+                if (j >= total) continue;
+                const int pad = E[j].pad;
+                if (CHAINS && (pad & ENT_RING)) {
+                    const double *rs = ring + 30 * ((pad >> ENT_RING_SHIFT) & 15) + 5 * (pad & 255);
+#pragma unroll
+                    for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = rs[cc];
+                } else {
+                    pend |= 1u << q;
+                }
+            }
+            int spins = 0;
+            while (pend) {
+                unsigned long long v[3][5];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    if (!((pend >> q) & 1u)) continue;
+                    const int j = lane + 32 * q;
+                    const double *gs = src + DG_STRIDE * (size_t)E[j].k + DG_LIST * (E[j].pad & 255);
+                    ld_relaxed_v2(gs, v[q][0], v[q][1]);
+                    ld_relaxed_v2(gs + 2, v[q][2], v[q][3]);
+                    v[q][4] = ld_relaxed_b64(gs + 4);
+                }
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    if (!((pend >> q) & 1u) || !ready5(v[q])) continue;
+                    const int j = lane + 32 * q;
+#pragma unroll
+                    for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __longlong_as_double(v[q][cc]);
+                    pend &= ~(1u << q);
+                }
+                if (pend && !spin_continue(spins, d.err)) break;
+            }
+        } else if (mine) {
+            const double *dsrc = (forward ? d.dUp : d.dUn) + 5 * (size_t)k_slot;
+            unsigned long long v[5];
+            int spins = 0;
+            do {
+#pragma unroll
+                for (int r = 0; r < 5; ++r) v[r] = ld_relaxed_b64(dsrc + r);
+            } while (!ready5(v) && spin_continue(spins, d.err));
+            double U[5], pn[5];
+#pragma unroll
+            for (int r = 0; r < 5; ++r) U[r] = __longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r];
+            Frame Fk;
+            load_frame(d.frame + 9 * (size_t)k_slot, Fk);
+            conserved_to_primitive(U, Fk, pn);
+            FluxPre Pn;
+            flux_pre(pn, Fp, Pn);
+            int axes = 0;
+#pragma unroll
+            for (int e = 0; e < NDIR; ++e)
+                if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
+            AxisTerms An[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                if (axes & (1 << a)) axis_terms(Pn, a, An[a]);
+            for (int e = 0; e < NDIR; ++e) {
+                if (!(mask_slot & (1 << e))) continue;
+                const int kind = flux_kind(cls, e);
+#pragma unroll
+                for (int cc = 0; cc < 5; ++cc) {
+                    double *t = &T[(e * MAX_SLOTS + lane) * 5 + cc];
+                    *t = flux_component(kind, cc, Pn, An) - *t;
+                }
+            }
+        }
+        __syncwarp();
+
+        // ---- phase C
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        if (lane < 30) {
+            for (int jj = lo; jj < hi; ++jj) {
+                const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
+                sx = sx + t * E[jj].w[0];
+                sy = sy + t * E[jj].w[1];
+                sz = sz + t * E[jj].w[2];
+            }
+        }
+        double G = 0.0;
+        if (lane < 30) G = cramer_num(dd >> 1, g, sx, sy, sz) / g[6];
+        double gd[NDIR];
+#pragma unroll
+        for (int e = 0; e < NDIR; ++e) gd[e] = __shfl_sync(FULL, G, e * 5 + (lane % 5));
+        if (lane < 5) {
+            double lu;
+            if (wall) lu = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+            else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
+            if (forward) {
+                dnew = -(dinv * (base5 + lu));
+                st_relaxed_f64(d.dUp + 5 * (size_t)p + lane, dnew);
+            } else {
+                dnew = base5 - dinv * lu;
+                st_relaxed_f64(d.dUn + 5 * (size_t)p + lane, dnew);
+            }
         }
     }
     if (d.shared_frame) {
@@ -961,6 +978,34 @@ __global__ void k_update(DevCloud d, double *U_next, double *q_next) {
         d.dUp[5 * (size_t)i + r] = dn[r];
         U_next[5 * (size_t)i + r] = Un[r];
         q_next[5 * (size_t)i + r] = qn[r];
+    }
+}
+
+// Supersonic points after the state update (state_update_implicit.f90:
+// 63-94): outlets, then inlets, each in index order, take the new state of
+// their nearest non-wall neighbour.  One thread, in that order, since a
+// source may be a supersonic point copied just before; then their next U
+// and q.
+__global__ void k_update_ss(DevCloud d, double *U_next, double *q_next) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int j = 0; j < d.n_ss; ++j) {
+        const int k = d.ss_pts[j], src = d.ss_src[j];
+        double p[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            p[r] = src >= 0 ? d.prim[5 * (size_t)src + r] : 0.0;
+            d.prim[5 * (size_t)k + r] = p[r];
+        }
+        Frame F;
+        load_frame(d.frame + 9 * (size_t)k, F);
+        double Un[5], qn[5];
+        primitive_to_rotated_conserved(p, F, Un);
+        primitive_to_q(p, qn);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            U_next[5 * (size_t)k + r] = Un[r];
+            q_next[5 * (size_t)k + r] = qn[r];
+        }
     }
 }
 
@@ -1132,6 +1177,9 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     auto mark = [&](int i, cudaStream_t on) { if (ev) cudaEventRecord(ev[i], on); };
     const int fblocks = (n + FLUX_WARPS - 1) / FLUX_WARPS;
     mark(0, s);
+    // supersonic copies may read a neighbour's increment from before the
+    // sweeps, which k_pending is about to mark
+    if (d.dU_old) cudaMemcpyAsync(d.dU_old, d.dUn, sizeof(double) * 5 * (size_t)n, cudaMemcpyDeviceToDevice, s);
     k_qderiv<<<(n + 127) / 128, 128, 0, s>>>(d);
     for (int j = 0; j < d.inner_iterations; ++j) {
         k_qinner<<<(n + 127) / 128, 128, 0, s>>>(d, d.dq, d.dq_tmp);
@@ -1168,6 +1216,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     sweep(0);
     mark(5, s);
     k_update<<<(n + 127) / 128, 128, 0, s>>>(d, U_next, q_next);
+    if (d.n_ss > 0) k_update_ss<<<1, 32, 0, s>>>(d, U_next, q_next);
     mark(6, s);
     const int rb = reduction_blocks(d.n_res);
     k_reduce_partial<<<rb, RED_THREADS, 0, s>>>(d);

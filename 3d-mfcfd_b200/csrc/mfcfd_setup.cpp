@@ -86,7 +86,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     T.n = n;
     T.cap = P.split_capacity > 0 ? P.split_capacity : MAX_CONN;
     const int cap = T.cap;
-    T.cls.assign(n, CLS_OTHER);
+    T.cls.assign(n, CLS_SUPERSONIC);
     for (int i = 0; i < n; ++i) {
         if (nbhs[i] < 0 || nbhs[i] > MAX_CONN) {
             err = "nbhs out of range [0,27] at point " + std::to_string(i + 1);
@@ -103,9 +103,8 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         case 0: T.cls[i] = CLS_INTERIOR; T.interior_idx.push_back(i); break;
         case 1: T.cls[i] = CLS_WALL; T.wall_idx.push_back(i); break;
         case 2: T.cls[i] = CLS_OUTER; T.outer_idx.push_back(i); break;
-        case 5: case 6:
-            err = "supersonic inlet/outlet points (status 5/6) are not supported";
-            return MFCFD_ERR_UNSUPPORTED;
+        case 5: T.cls[i] = CLS_SUPERSONIC; T.ss_inlet_idx.push_back(i); break;
+        case 6: T.cls[i] = CLS_SUPERSONIC; T.ss_outlet_idx.push_back(i); break;
         default:
             err = "unknown point status " + std::to_string(status[i]);
             return MFCFD_ERR_ARG;
@@ -189,7 +188,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         out.clear();
         int cls = T.cls[i];
         bool use_conn = (cls == CLS_WALL && d == 5);
-        bool unused = (cls == CLS_WALL && d == 4) || (cls == CLS_OUTER && d == 5) || cls == CLS_OTHER;
+        bool unused = (cls == CLS_WALL && d == 4) || (cls == CLS_OUTER && d == 5) || cls == CLS_SUPERSONIC;
         if (unused) return true;
         if (use_conn) {
             for (int r = 0; r < nbhs[i]; ++r) out.push_back(conn[(size_t)i * MAX_CONN + r] - 1);
@@ -296,11 +295,35 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         int p = T.point_with_alias[i];
         if (p == 0) continue;   // the reference's out-of-range entry
         int cls = T.cls[p - 1];
-        if (cls == CLS_WALL || cls == CLS_INTERIOR) {
+        if (cls == CLS_WALL || cls == CLS_INTERIOR || cls == CLS_SUPERSONIC) {
             T.swept[p - 1] = 1;
             order.push_back(p - 1);
         }
     }
+    // nearest neighbour in conn order, first of equal distances, starting
+    // from `start` (implicit_forward_and_reverse_sweeps.f90:39-50,
+    // state_update_implicit.f90:63-94); -1 if none is closer than start
+    auto nearest = [&](int p, bool skip_wall, double start) {
+        double min_dist = start;
+        int q = -1;
+        for (int r = 0; r < nbhs[p]; ++r) {
+            const int nbh = conn[(size_t)p * MAX_CONN + r] - 1;
+            const double dx = x[nbh] - x[p], dy = y[nbh] - y[p], dz = z[nbh] - z[p];
+            const double ds = std::sqrt(dx * dx + dy * dy + dz * dz);
+            if (ds < min_dist && (!skip_wall || T.cls[nbh] != CLS_WALL)) {
+                min_dist = ds;
+                q = nbh;
+            }
+        }
+        return q;
+    };
+    T.copy_src.assign(n, -1);
+    T.ss_pts.clear();
+    T.ss_src.clear();
+    for (int i = 0; i < n; ++i)
+        if (T.cls[i] == CLS_SUPERSONIC) T.copy_src[i] = nearest(i, false, 1000000.0);
+    for (int k : T.ss_outlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, true, 100000.0)); }
+    for (int k : T.ss_inlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, true, 100000.0)); }
     auto al = [&](int k) { return T.alias[k]; };
     auto build = [&](bool forward, std::vector<int32_t> &level, std::vector<int32_t> &lptr,
                      std::vector<int32_t> &lpts, std::vector<int32_t> &off,
@@ -314,6 +337,11 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         auto takes = [&](int p, int k) { return forward ? (al(k) < al(p)) : (al(k) > al(p)); };
         parallel_for((int)order.size(), [&](int oi) {
             const int p = order[oi];
+            if (T.cls[p] == CLS_SUPERSONIC) {   // one copy entry
+                cnt[(size_t)p * NDIR] = 1;
+                off[p + 1] += 1;
+                return;
+            }
             for (int d = 0; d < NDIR; ++d) {
                 const int c = T.list_cnt[(size_t)p * NDIR + d];
                 int taken = 0;
@@ -330,6 +358,14 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         ent.resize((size_t)off[n]);
         parallel_for((int)order.size(), [&](int oi) {
             const int p = order[oi];
+            if (T.cls[p] == CLS_SUPERSONIC) {
+                const int q = T.copy_src[p];
+                SweepEntry &e = ent[(size_t)off[p]];
+                e.k = q;
+                e.pad = ENT_COPY | ((q >= 0 && T.swept[q] && takes(p, q)) ? ENT_COPY_NEW : 0);
+                e.w[0] = e.w[1] = e.w[2] = 0.0;
+                return;
+            }
             const double *t1 = tan1 + 3 * (size_t)p, *t2 = tan2 + 3 * (size_t)p, *nn = nor + 3 * (size_t)p;
             size_t e_at = (size_t)off[p];
             for (int d = 0; d < NDIR; ++d) {
@@ -358,6 +394,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         auto visit = [&](int p) {
             int lv = 0;
             for (int e = off[p]; e < off[p + 1]; ++e) {
+                if (!entry_is_dependency(ent[e])) continue;
                 int k = ent[e].k;
                 if (T.swept[k] && level[k] + 1 > lv) lv = level[k] + 1;
             }
@@ -439,6 +476,7 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
         for (int p : lpts) {           // level-major, a topological order
             int best = -1, best_level = -1;
             for (int e = off[p]; e < off[p + 1]; ++e) {
+                if (!entry_is_dependency(ent[e])) continue;
                 const int k = ent[e].k;
                 if (!T.swept[k]) continue;
                 const int w = owner[k];
@@ -485,7 +523,8 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
             const bool shared = T.consumer_shared[p] != 0;
             for (int e = off[p]; e < off[p + 1]; ++e) {
                 SweepEntry &E = went[e];
-                E.pad &= 0xffff;
+                E.pad &= ~ENT_CHAIN_BITS;
+                if (E.pad & ENT_COPY) continue;   // reads dU, never the ring
                 const int k = E.k;
                 if (!T.swept[k]) continue;   // fixed increment written before the sweep
                 const bool same = owner[k] == owner[p];
@@ -511,7 +550,7 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
             it.cnt = 0;
             for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[(size_t)p * NDIR + e] << (5 * e);
             it.info = (T.cls[p] == CLS_WALL ? CI_WALL : 0u) | (T.consumer_shared[p] ? CI_SHARED : 0u) |
-                      (publish[p] ? CI_PUBLISH : 0u);
+                      (publish[p] ? CI_PUBLISH : 0u) | (T.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u);
         }
     }
 }
@@ -528,6 +567,7 @@ void build_pre_order(const Topology &T, std::vector<int32_t> &order) {
     for (int p = 0; p < n; ++p) {
         if (!T.swept[p]) continue;
         for (int e = T.fwd_off[p]; e < T.fwd_off[p + 1]; ++e) {
+            if (T.fwd_ent[e].pad & ENT_COPY) continue;   // copies read dU, not the flux kernel's output
             const int k = T.fwd_ent[e].k;
             if (!T.swept[k]) key[k] = std::min(key[k], 2 * (int64_t)T.fwd_level[p]);
         }

@@ -221,6 +221,20 @@ def small_sphere(n_shells: int = 8, pts_per_shell: int = 150, seed: int = 7,
                        name=f"sphere-{n_shells}x{pts_per_shell}")
 
 
+def with_supersonic_boundary(cloud: PointCloud, fraction: float = 0.3) -> PointCloud:
+    """A copy of `cloud` whose outer points far upstream become supersonic
+    inlet points (status 5) and those far downstream supersonic outlet points
+    (status 6): x below -fraction, or above +fraction, times the outer
+    radius."""
+    st = cloud.status.copy()
+    outer = st == STATUS_OUTER
+    r = np.sqrt(cloud.x ** 2 + cloud.y ** 2 + cloud.z ** 2)
+    rmax = float(r[outer].max()) if outer.any() else 1.0
+    st[outer & (cloud.x < -fraction * rmax)] = STATUS_SUPERSONIC_INLET
+    st[outer & (cloud.x > fraction * rmax)] = STATUS_SUPERSONIC_OUTLET
+    return dataclasses.replace(cloud, status=st, name=cloud.name + "-supersonic")
+
+
 def initial_state(cloud: PointCloud, mach: float, aoa_deg: float) -> np.ndarray:
     """Impulsive-start initial state ``prim(5, N)``.
 

@@ -64,10 +64,10 @@ def test_bad_inputs_are_status_codes(mfcfd_lib, small_cloud):
     assert e.value.code == 1
     c = copy.deepcopy(small_cloud)
     c.status = c.status.copy()
-    c.status[10] = 5
+    c.status[10] = 7
     with pytest.raises(MfcfdError) as e:
         _create(mfcfd_lib, c)
-    assert e.value.code == 6
+    assert e.value.code == 1
     with pytest.raises(MfcfdError) as e:
         _create(mfcfd_lib, small_cloud, power=1.0)
     assert e.value.code == 6

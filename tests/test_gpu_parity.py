@@ -79,3 +79,20 @@ def test_inner_iterations_bitexact(small_cloud, oracle_lib, mfcfd_lib, inner):
     for name, fg, fo in _field_ids(oracle_lib):
         a, b = s.get(fg), o.get(fo)
         assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
+
+
+@pytest.mark.parametrize("sweep_mode", [0, 1, 2])
+def test_supersonic_boundary_bitexact(oracle_lib, mfcfd_lib, sweep_mode):
+    """Status 5/6 points (nearest-neighbour copies in the sweeps and the state
+    update, implicit_forward_and_reverse_sweeps.f90:38-51,
+    state_update_implicit.f90:63-94), every field after 5 iterations."""
+    from mfcfd import cloud
+    c = cloud.with_supersonic_boundary(cloud.small_sphere(6, 100, r1=1.5))
+    s, o = _pair(c, 0.8, 2.0, oracle_lib.LIBM_MFMATH, oracle_lib, sweep_mode)
+    hist = s.q_lskum(5)
+    for t in range(1, 6):
+        rc = o.step(t)
+        assert abs(hist[t - 1, 0] - rc[0]) <= 1e-13 * abs(rc[0])
+    for name, fg, fo in _field_ids(oracle_lib):
+        a, b = s.get(fg), o.get(fo)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name

@@ -88,14 +88,22 @@ def test_point_one_is_not_swept(small_cloud):
     assert s.levels(0)[0] == -1
 
 
+def _nearest(c, p):
+    """implicit_forward_and_reverse_sweeps.f90:39-50: first closest neighbour."""
+    nb = c.conn[p, :c.nbhs[p]] - 1
+    d = np.sqrt((c.x[nb] - c.x[p]) ** 2 + (c.y[nb] - c.y[p]) ** 2 + (c.z[nb] - c.z[p]) ** 2)
+    return int(nb[np.argmin(d)]) if len(nb) and d.min() < 1e6 else -1
+
+
 def _level_check(s, c, direction):
-    """Levels are exactly the longest-path depths over swept dependencies."""
+    """Levels are exactly the longest-path depths over swept dependencies
+    (supersonic points depend on their copy source when it comes first)."""
     counts, lists = s.stencils(27)
     alias, pwa = s.alias()
     st = c.status
     swept = np.zeros(c.n, bool)
     pw = pwa[pwa > 0] - 1
-    swept[pw[(st[pw] == 0) | (st[pw] == 1)]] = True
+    swept[pw[(st[pw] == 0) | (st[pw] == 1) | (st[pw] == 5) | (st[pw] == 6)]] = True
     ps, ks = [], []
     for d in range(6):
         for j in range(27):
@@ -107,6 +115,10 @@ def _level_check(s, c, direction):
         m = c.nbhs[wall] > j
         ps.append(wall[m])
         ks.append(c.conn[wall[m], j] - 1)
+    ss = np.nonzero((st == 5) | (st == 6))[0]
+    src = np.array([_nearest(c, i) for i in ss], dtype=np.int64)
+    ps.append(ss[src >= 0])
+    ks.append(src[src >= 0])
     p, k = np.concatenate(ps), np.concatenate(ks)
     keep = swept[p] & swept[k] & ((alias[k] < alias[p]) if direction == 0 else (alias[k] > alias[p]))
     p, k = p[keep], k[keep]
@@ -131,5 +143,22 @@ def test_large_cloud_parallel_setup(oracle_lib):
     co, lo = o.stencils(27)
     assert np.array_equal(cs, co) and np.array_equal(ls, lo)
     assert all(np.array_equal(x, y) for x, y in zip(s.alias(), o.alias()))
+    for direction in (0, 1):
+        _level_check(s, c, direction)
+
+
+def test_supersonic_points_are_swept_copies(oracle_lib):
+    """Status 5/6 points join the sweep order and copy their nearest
+    neighbour's increment: their level follows the copy source when it comes
+    earlier in the sweep; stencils and alias still equal the oracle's."""
+    from mfcfd import cloud
+    c = cloud.with_supersonic_boundary(cloud.small_sphere(6, 100, r1=1.5))
+    s = _solver(c)
+    info = s.info()
+    assert info["n_supersonic"] == int(((c.status == 5) | (c.status == 6)).sum()) > 0
+    o = oracle_lib.Oracle(c, 0.4, 0.0)
+    cs, ls = s.stencils(27)
+    co, lo = o.stencils(27)
+    assert np.array_equal(cs, co) and np.array_equal(ls, lo)
     for direction in (0, 1):
         _level_check(s, c, direction)

@@ -50,3 +50,24 @@ def test_oracle_inner_iterations_match_translated_reference(oracle_lib):
     assert np.array_equal(r.get("dq"), o.get(oracle_lib.FIELD_DQ))
     assert np.array_equal(r.get("prim"), o.get(oracle_lib.FIELD_PRIM))
     ref_translated.TranslatedReference(c, p0, 0.8, 2.0)   # back to the default
+
+
+def test_oracle_supersonic_points_match_translated_reference(oracle_lib):
+    """Status 5/6 points: the restatement and the reference's own routines
+    agree bit for bit (glibc libm both sides)."""
+    import numpy as np
+    import pytest
+    from mfcfd import cloud
+    from oracle import ref_translated
+    if not ref_translated.available("glibc"):
+        pytest.skip("translated reference not built")
+    c = cloud.with_supersonic_boundary(cloud.small_sphere(6, 100, r1=1.5))
+    p0 = cloud.initial_state(c, 0.8, 2.0)
+    r = ref_translated.TranslatedReference(c, p0, 0.8, 2.0)
+    o = oracle_lib.Oracle(c, 0.8, 2.0)
+    o.set_prim(p0)
+    for t in range(1, 6):
+        assert r.step(t) == o.step(t)
+    for name, fid in (("prim", oracle_lib.FIELD_PRIM), ("delun", oracle_lib.FIELD_DELUN),
+                      ("dq", oracle_lib.FIELD_DQ), ("flux_res", oracle_lib.FIELD_FLUX_RES)):
+        assert np.array_equal(r.get(name), o.get(fid)), name
