@@ -213,8 +213,13 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         *out = h;
         return MFCFD_ERR_ARG;
     }
-    if (P.power != 0.0 || P.precision != MFCFD_PRECISION_FP64) {
-        h->err = "only power = 0 and FP64 are implemented";
+    if (!(P.power >= 0.0 && P.power <= 16.0)) {
+        h->err = "power out of range [0, 16]";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
+    if (P.precision != MFCFD_PRECISION_FP64) {
+        h->err = "only FP64 is implemented";
         *out = h;
         return MFCFD_ERR_UNSUPPORTED;
     }
@@ -299,6 +304,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     UP(cls, T.cls); UP(nbhs, vnb); UP(conn, vconn); UP(eps2, T.eps2);
     UP(slot_nbr, T.slot_nbr); UP(nslot, T.nslot); UP(slot_mask, T.slot_mask);
     UP(list_cnt, T.list_cnt); UP(list_ent, T.list_ent); UP(geo, T.geo);
+    if (!T.wq.empty()) { UP(wq, T.wq); UP(wf, T.wf); }
     UP(swept, T.swept); UP(consumer_shared, T.consumer_shared);
     UP(fwd_lvl_ptr, T.fwd_lvl_ptr); UP(fwd_lvl_pts, T.fwd_lvl_pts);
     UP(bwd_lvl_ptr, T.bwd_lvl_ptr); UP(bwd_lvl_pts, T.bwd_lvl_pts);

@@ -61,6 +61,10 @@ struct Topology {
     std::vector<uint8_t> list_ent;          // n*6*LIST_STRIDE slot indices
     std::vector<double> geo;                // n*GEO_STRIDE
     std::vector<double> eps2;               // (VL*min_dist)^3 squared
+    // least-squares weights 1/dist**power when power != 0 (else empty):
+    // per conn entry (q-derivatives, xyz distance) and per neighbour slot
+    // (fluxes, distance in the point's frame)
+    std::vector<double> wq, wf;
     // sweep schedules (0-based ids)
     std::vector<int32_t> fwd_level, bwd_level;   // per point, -1 if not swept
     std::vector<int32_t> fwd_lvl_ptr, fwd_lvl_pts, bwd_lvl_ptr, bwd_lvl_pts;
@@ -154,6 +158,7 @@ struct DevCloud {
     const int32_t *nbhs;
     const int32_t *conn;          // 27 per point, 0-based
     const double *eps2;
+    const double *wq, *wf;        // weights (power != 0), else null: weight 1
     const int32_t *slot_nbr;
     const uint8_t *nslot;
     const uint8_t *slot_mask;

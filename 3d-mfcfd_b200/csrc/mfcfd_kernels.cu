@@ -58,8 +58,9 @@ __global__ void k_conserved_q(DevCloud d) {
 // ---------------------------------------------------------------- q-derivatives
 
 // eval_q_derivatives (q_derivatives.f90:25-110) and timestep_delt
-// (timestep_delt.f90:227-259), thread per point.  With power = 0 the weights
-// are exactly 1 and the products weights*delx*temp equal delx*temp.
+// (timestep_delt.f90:227-259), thread per point.  Weights come from d.wq
+// (power != 0); with power = 0 they are exactly 1, and delx*delx*1 and
+// 1*delx*temp round like the unweighted products.
 __global__ void __launch_bounds__(128) k_qderiv(DevCloud d) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= d.n) return;
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(128) k_qderiv(DevCloud d) {
     const int32_t *cn = d.conn + (size_t)MAX_CONN * i;
     for (int j = 0; j < nb; ++j) {
         const int k = cn[j];
+        const double w = d.wq ? d.wq[(size_t)MAX_CONN * i + j] : 1.0;
         double qk[5];
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
@@ -83,18 +85,18 @@ __global__ void __launch_bounds__(128) k_qderiv(DevCloud d) {
         }
         const double delx = d.x[k] - xi, dely = d.y[k] - yi, delz = d.z[k] - zi;
         const double dist = sqrt(delx * delx + dely * dely + delz * delz);
-        xx = xx + delx * delx;
-        yy = yy + dely * dely;
-        zz = zz + delz * delz;
-        xy = xy + delx * dely;
-        yz = yz + dely * delz;
-        zx = zx + delz * delx;
+        xx = xx + delx * delx * w;
+        yy = yy + dely * dely * w;
+        zz = zz + delz * delz * w;
+        xy = xy + delx * dely * w;
+        yz = yz + dely * delz * w;
+        zx = zx + delz * delx * w;
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
             const double t = qk[r] - qi[r];
-            sx[r] = sx[r] + delx * t;
-            sy[r] = sy[r] + dely * t;
-            sz[r] = sz[r] + delz * t;
+            sx[r] = sx[r] + w * delx * t;
+            sy[r] = sy[r] + w * dely * t;
+            sz[r] = sz[r] + w * delz * t;
         }
         // timestep_delt.f90:235-253
         const double *pk = d.prim + 5 * (size_t)k;
@@ -137,21 +139,22 @@ __global__ void __launch_bounds__(128) k_qinner(DevCloud d, const double *dq_in,
     for (int j = 0; j < nb; ++j) {
         const int k = cn[j];
         const double delx = d.x[k] - xi, dely = d.y[k] - yi, delz = d.z[k] - zi;
-        xx = xx + delx * delx;
-        yy = yy + dely * dely;
-        zz = zz + delz * delz;
-        xy = xy + delx * dely;
-        yz = yz + dely * delz;
-        zx = zx + delz * delx;
+        const double w = d.wq ? d.wq[(size_t)MAX_CONN * i + j] : 1.0;
+        xx = xx + delx * delx * w;
+        yy = yy + dely * dely * w;
+        zz = zz + delz * delz * w;
+        xy = xy + delx * dely * w;
+        yz = yz + dely * delz * w;
+        zx = zx + delz * delx * w;
         const double *dqk = dq_in + 15 * (size_t)k;
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
             const double qti = qi[r] - 0.5 * (delx * dqi[3 * r] + dely * dqi[3 * r + 1] + delz * dqi[3 * r + 2]);
             const double qtn = d.q[5 * (size_t)k + r] - 0.5 * (delx * dqk[3 * r] + dely * dqk[3 * r + 1] + delz * dqk[3 * r + 2]);
             const double t = qtn - qti;
-            sx[r] = sx[r] + delx * t;
-            sy[r] = sy[r] + dely * t;
-            sz[r] = sz[r] + delz * t;
+            sx[r] = sx[r] + w * delx * t;
+            sy[r] = sy[r] + w * dely * t;
+            sz[r] = sz[r] + w * delz * t;
         }
     }
     const double g[6] = {xx, yy, zz, xy, yz, zx};
@@ -355,9 +358,11 @@ __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
                 Frame F;
                 load_frame(d.frame + 9 * (size_t)p, F);
                 const double delx = d.x[k] - d.x[p], dely = d.y[k] - d.y[p], delz = d.z[k] - d.z[p];
-                W[lane * 3 + 0] = delx * F.t1[0] + dely * F.t1[1] + delz * F.t1[2];
-                W[lane * 3 + 1] = delx * F.t2[0] + dely * F.t2[1] + delz * F.t2[2];
-                W[lane * 3 + 2] = delx * F.n[0] + dely * F.n[1] + delz * F.n[2];
+                // dels*weights, delt*weights, deln*weights (weights 1 for power 0)
+                const double w = d.wf ? d.wf[(size_t)MAX_SLOTS * p + lane] : 1.0;
+                W[lane * 3 + 0] = (delx * F.t1[0] + dely * F.t1[1] + delz * F.t1[2]) * w;
+                W[lane * 3 + 1] = (delx * F.t2[0] + dely * F.t2[1] + delz * F.t2[2]) * w;
+                W[lane * 3 + 2] = (delx * F.n[0] + dely * F.n[1] + delz * F.n[2]) * w;
                 int axes = 0;
 #pragma unroll
                 for (int dd = 0; dd < NDIR; ++dd)

@@ -280,6 +280,32 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         }
     });
 
+    // weights of the q-derivative and flux least squares (q_derivatives.f90:
+    // 44-45, interior_flux_dGxpos.f90:77-78): only for power != 0
+    T.wq.clear();
+    T.wf.clear();
+    if (P.power != 0.0) {
+        T.wq.assign((size_t)n * MAX_CONN, 0.0);
+        T.wf.assign((size_t)n * MAX_SLOTS, 0.0);
+        parallel_for(n, [&](int i) {
+            for (int r = 0; r < nbhs[i]; ++r) {
+                const int k = conn[(size_t)i * MAX_CONN + r] - 1;
+                const double delx = x[k] - x[i], dely = y[k] - y[i], delz = z[k] - z[i];
+                const double dist = std::sqrt(delx * delx + dely * dely + delz * delz);
+                T.wq[(size_t)i * MAX_CONN + r] = 1.0 / std::pow(dist, P.power);
+            }
+            const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
+            for (int s = 0; s < T.nslot[i]; ++s) {
+                const int k = T.slot_nbr[(size_t)i * MAX_SLOTS + s];
+                const double delx = x[k] - x[i], dely = y[k] - y[i], delz = z[k] - z[i];
+                const double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+                const double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+                const double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                T.wf[(size_t)i * MAX_SLOTS + s] = weight(dels, delt, deln);
+            }
+        });
+    }
+
     // limiter epsilon: (VL_CONST*min_dist)**3 squared (limiters.f90:251-253)
     T.eps2.resize(n);
     for (int i = 0; i < n; ++i) {

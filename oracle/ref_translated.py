@@ -100,7 +100,7 @@ class TranslatedReference:
     FIELDS = {"prim": 5, "u": 5, "q": 5, "qm": 10, "dq": 15, "delt": 1, "flux_res": 5,
               "delup": 5, "delun": 5}
 
-    def __init__(self, cloud, prim0, mach, aoa_deg, libm="glibc", inner_iterations=0):
+    def __init__(self, cloud, prim0, mach, aoa_deg, libm="glibc", inner_iterations=0, power=0.0):
         L = lib(libm)
         L.ref_free_all()
         L.ref_register_file(b"3d_input_data", input_text(cloud).encode())
@@ -110,6 +110,7 @@ class TranslatedReference:
         L.ref_set_param(b"aoa", float(aoa_deg))
         # overrides persist in the library: set every one on each construction
         L.ref_set_param(b"inner_iterations", float(inner_iterations))
+        L.ref_set_param(b"power", float(power))
         L.ref_init_parameters()
         for name in (b"allocate_size", b"read_input_point_data", b"initial_conditions",
                      b"generate_split_stencils", b"aliasing"):

@@ -69,7 +69,10 @@ def test_bad_inputs_are_status_codes(mfcfd_lib, small_cloud):
         _create(mfcfd_lib, c)
     assert e.value.code == 1
     with pytest.raises(MfcfdError) as e:
-        _create(mfcfd_lib, small_cloud, power=1.0)
+        _create(mfcfd_lib, small_cloud, power=-1.0)
+    assert e.value.code == 1
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, small_cloud, precision=1)
     assert e.value.code == 6
     with pytest.raises(MfcfdError) as e:
         _create(mfcfd_lib, small_cloud, sweep_mode=3)

@@ -14,11 +14,11 @@ pytestmark = pytest.mark.gpu
 FIELDS = ["PRIM", "U", "Q", "QM", "DQ", "DELT", "FLUX_RES", "DELUP", "DELUN"]
 
 
-def _pair(cloud, mach, aoa, libm, oracle_lib, sweep_mode=0, inner_iterations=0):
+def _pair(cloud, mach, aoa, libm, oracle_lib, sweep_mode=0, inner_iterations=0, power=0.0):
     from mfcfd.solver import Solver
     from mfcfd.cloud import initial_state
-    s = Solver(cloud, mach, aoa, sweep_mode=sweep_mode, inner_iterations=inner_iterations)
-    o = oracle_lib.Oracle(cloud, mach, aoa, libm=libm, inner_iterations=inner_iterations)
+    s = Solver(cloud, mach, aoa, sweep_mode=sweep_mode, inner_iterations=inner_iterations, power=power)
+    o = oracle_lib.Oracle(cloud, mach, aoa, libm=libm, inner_iterations=inner_iterations, power=power)
     prim0 = initial_state(cloud, mach, aoa)
     s.initial_conditions(prim0)
     o.set_prim(prim0)
@@ -93,6 +93,19 @@ def test_supersonic_boundary_bitexact(oracle_lib, mfcfd_lib, sweep_mode):
     for t in range(1, 6):
         rc = o.step(t)
         assert abs(hist[t - 1, 0] - rc[0]) <= 1e-13 * abs(rc[0])
+    for name, fg, fo in _field_ids(oracle_lib):
+        a, b = s.get(fg), o.get(fo)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
+
+
+@pytest.mark.parametrize("power,inner", [(2.0, 0), (0.5, 2)])
+def test_weighted_least_squares_bitexact(small_cloud, oracle_lib, mfcfd_lib, power, inner):
+    """power != 0: weights 1/dist**power in the q-derivative, flux, D_inv and
+    sweep least squares (glibc pow on the host, as the oracle), every field."""
+    s, o = _pair(small_cloud, 0.8, 2.0, oracle_lib.LIBM_MFMATH, oracle_lib, inner_iterations=inner, power=power)
+    s.q_lskum(3)
+    for t in range(1, 4):
+        o.step(t)
     for name, fg, fo in _field_ids(oracle_lib):
         a, b = s.get(fg), o.get(fo)
         assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name

@@ -71,3 +71,24 @@ def test_oracle_supersonic_points_match_translated_reference(oracle_lib):
     for name, fid in (("prim", oracle_lib.FIELD_PRIM), ("delun", oracle_lib.FIELD_DELUN),
                       ("dq", oracle_lib.FIELD_DQ), ("flux_res", oracle_lib.FIELD_FLUX_RES)):
         assert np.array_equal(r.get(name), o.get(fid)), name
+
+
+@pytest.mark.parametrize("power", [2.0, 0.5])
+def test_oracle_weighted_least_squares_match_translated_reference(oracle_lib, power):
+    """power != 0 (parameter.f90:21): restatement and reference agree bit for bit."""
+    import numpy as np
+    from mfcfd import cloud
+    from oracle import ref_translated
+    if not ref_translated.available("glibc"):
+        pytest.skip("translated reference not built")
+    c = cloud.small_sphere(6, 100, r1=1.5)
+    p0 = cloud.initial_state(c, 0.8, 2.0)
+    r = ref_translated.TranslatedReference(c, p0, 0.8, 2.0, power=power)
+    o = oracle_lib.Oracle(c, 0.8, 2.0, power=power)
+    o.set_prim(p0)
+    for t in range(1, 4):
+        assert r.step(t) == o.step(t)
+    for name, fid in (("prim", oracle_lib.FIELD_PRIM), ("dq", oracle_lib.FIELD_DQ),
+                      ("flux_res", oracle_lib.FIELD_FLUX_RES), ("delun", oracle_lib.FIELD_DELUN)):
+        assert np.array_equal(r.get(name), o.get(fid)), name
+    ref_translated.TranslatedReference(c, p0, 0.8, 2.0)   # back to the defaults
