@@ -218,6 +218,11 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         *out = h;
         return MFCFD_ERR_ARG;
     }
+    if (P.update_variant != MFCFD_UPDATE_IMPLICIT && P.update_variant != MFCFD_UPDATE_EXPLICIT) {
+        h->err = "unknown update_variant";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
     if (P.precision != MFCFD_PRECISION_FP64) {
         h->err = "only FP64 is implemented";
         *out = h;
@@ -259,6 +264,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     std::memcpy(d.frame0, T.frame0, sizeof d.frame0);
     d.power = P.power;
     d.inner_iterations = P.inner_iterations;
+    d.update_variant = P.update_variant;
     d.cfl = P.cfl;
     d.rho_inf = P.rho_inf; d.u1_inf = P.u1_inf; d.u2_inf = P.u2_inf;
     d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;

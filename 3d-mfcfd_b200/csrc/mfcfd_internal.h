@@ -150,6 +150,7 @@ struct DevCloud {
     double frame0[9];
     double power, cfl;
     int inner_iterations;         // second-order q-derivative passes
+    int update_variant;           // MFCFD_UPDATE_*
     double rho_inf, u1_inf, u2_inf, u3_inf, pr_inf;
     // geometry
     const double *x, *y, *z;

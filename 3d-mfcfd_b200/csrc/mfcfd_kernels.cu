@@ -943,7 +943,8 @@ static int chain_smem() {
 
 // ---------------------------------------------------------------- state update
 
-// state_update_implicit.f90:119-152 + 189-191, then the next iteration's
+// state_update_implicit.f90:119-152 + 189-191 (or state_update.f90:29-78
+// under MFCFD_UPDATE_EXPLICIT), then the next iteration's
 // compute_conserved_vector / eval_q_variables into the other U/q buffer.
 __global__ void k_update(DevCloud d, double *U_next, double *q_next) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -955,10 +956,12 @@ __global__ void k_update(DevCloud d, double *U_next, double *q_next) {
 #pragma unroll
     for (int r = 0; r < 5; ++r) dn[r] = d.dUn[5 * (size_t)i + r];
     double res = 0.0;
+    const bool expl = d.update_variant == MFCFD_UPDATE_EXPLICIT;
     if (cls == CLS_WALL || cls == CLS_INTERIOR) {
         const double temp = d.U[5 * (size_t)i];
 #pragma unroll
         for (int r = 0; r < 5; ++r) U[r] = d.U[5 * (size_t)i + r] + dn[r];
+        if (expl && cls == CLS_WALL) U[3] = 0.0;   // state_update.f90:37
         res = (U[0] - temp) * (U[0] - temp);
         conserved_to_primitive(U, F, p);
     } else if (cls == CLS_OUTER) {
@@ -966,8 +969,14 @@ __global__ void k_update(DevCloud d, double *U_next, double *q_next) {
 #pragma unroll
         for (int r = 0; r < 5; ++r) pc[r] = d.prim[5 * (size_t)i + r];
         conserved_vector_Ubar(pc, F, d.rho_inf, d.u1_inf, d.u2_inf, d.u3_inf, d.pr_inf, U);
+        if (expl) {   // state_update.f90:55-58
+            const double dt = d.delt[i];
 #pragma unroll
-        for (int r = 0; r < 5; ++r) U[r] = U[r] + dn[r];
+            for (int r = 0; r < 5; ++r) U[r] = U[r] - dt * d.flux_res[5 * (size_t)i + r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < 5; ++r) U[r] = U[r] + dn[r];
+        }
         conserved_to_primitive(U, F, p);
     } else {
 #pragma unroll

@@ -348,8 +348,10 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     T.ss_src.clear();
     for (int i = 0; i < n; ++i)
         if (T.cls[i] == CLS_SUPERSONIC) T.copy_src[i] = nearest(i, false, 1000000.0);
-    for (int k : T.ss_outlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, true, 100000.0)); }
-    for (int k : T.ss_inlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, true, 100000.0)); }
+    // state_update_implicit.f90 skips wall sources; state_update.f90 does not
+    const bool skip_wall = P.update_variant != MFCFD_UPDATE_EXPLICIT;
+    for (int k : T.ss_outlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, skip_wall, 100000.0)); }
+    for (int k : T.ss_inlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, skip_wall, 100000.0)); }
     auto al = [&](int k) { return T.alias[k]; };
     auto build = [&](bool forward, std::vector<int32_t> &level, std::vector<int32_t> &lptr,
                      std::vector<int32_t> &lpts, std::vector<int32_t> &off,

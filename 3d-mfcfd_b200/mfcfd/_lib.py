@@ -40,9 +40,12 @@ class Params(ctypes.Structure):
                 ("u3_inf", ctypes.c_double), ("pr_inf", ctypes.c_double),
                 ("inner_iterations", ctypes.c_int32), ("split_capacity", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("sweep_mode", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7)]
+                ("sweep_mode", ctypes.c_int32), ("update_variant", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 6)]
 
 
+UPDATE_IMPLICIT = 0
+UPDATE_EXPLICIT = 1
 SWEEP_DATAFLOW = 0
 SWEEP_LEVELS = 1
 

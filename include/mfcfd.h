@@ -80,8 +80,17 @@ typedef struct mfcfd_params {
     int32_t device;           /* CUDA device ordinal; -1 builds a host-only handle
                                  (stencils, alias, schedule) without device state */
     int32_t sweep_mode;       /* MFCFD_SWEEP_CHAINS (default), _DATAFLOW or _LEVELS */
-    int32_t reserved[7];
+    int32_t update_variant;   /* MFCFD_UPDATE_IMPLICIT (default) or MFCFD_UPDATE_EXPLICIT */
+    int32_t reserved[6];
 } mfcfd_params;
+
+/* The reference ships two sources of its state_update module; a build
+ * compiles one.  IMPLICIT: state_update_implicit.f90 (the active build).
+ * EXPLICIT: state_update.f90 -- wall normal momentum set to zero, outer
+ * points updated explicitly (Ubar - delt * flux_res), supersonic points
+ * copying their nearest neighbour of any status. */
+#define MFCFD_UPDATE_IMPLICIT 0
+#define MFCFD_UPDATE_EXPLICIT 1
 
 /* LU-SGS sweep schedules.  All give the reference's sequential result bit
  * for bit.  DATAFLOW: warps on all SMs take points in topological order and

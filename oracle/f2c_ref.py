@@ -24,7 +24,7 @@ into zeroed memory does, without touching other arrays' storage.
 Compile-time PARAMETERs become variables so a run can set max_points, Mach
 and the angle of attack; their defining expressions are evaluated at start.
 
-usage: python f2c_ref.py REFERENCE_DIR OUT_C
+usage: python f2c_ref.py REFERENCE_DIR OUT_C [VARIANT ...]
 """
 from __future__ import annotations
 
@@ -851,16 +851,28 @@ class Translator:
         return f"static void f_{s.name}({', '.join(parts) if parts else 'void'})"
 
 
+# Alternative source files of the same modules (the reference compiles one of
+# each pair): name -> (active file, replacement)
+VARIANTS = {
+    "explicit": ("state_update_implicit.f90", "state_update.f90"),
+    "backup": ("implicit_forward_and_reverse_sweeps.f90", "implicit_forward_and_reverse_sweeps_backup.f90"),
+}
+
+
 def main():
     ref_dir, out_c = sys.argv[1], sys.argv[2]
+    files = list(ACTIVE_FILES)
+    for v in sys.argv[3:]:                 # optional variant names
+        old, new = VARIANTS[v]
+        files[files.index(old)] = new
     tr = Translator()
-    for f in ACTIVE_FILES:
+    for f in files:
         tr.load(os.path.join(ref_dir, f))
     src = tr.emit()
     os.makedirs(os.path.dirname(os.path.abspath(out_c)), exist_ok=True)
     with open(out_c, "w") as fh:
         fh.write(src)
-    print(f"translated {len(ACTIVE_FILES)} files, {len(tr.subs)} subroutines -> {out_c}")
+    print(f"translated {len(files)} files, {len(tr.subs)} subroutines -> {out_c}")
 
 
 if __name__ == "__main__":

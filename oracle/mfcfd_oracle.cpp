@@ -44,6 +44,7 @@ struct OracleParams {
     double rho_inf, u1_inf, u2_inf, u3_inf, pr_inf;
     int inner_iterations;
     int split_capacity;   // 22 in the reference
+    int update_variant;   // 0 state_update_implicit.f90, 1 state_update.f90
 };
 
 const double PI = 3.141592653589793;           // 4*datan(1d0), parameter.f90:19
@@ -829,6 +830,48 @@ void state_update(Oracle &o) {
         for (int r = 1; r <= 5; ++r) o.V5(o.delUp, r, i) = o.V5(o.delUn, r, i);
 }
 
+// state_update.f90:14-124, the reference's other state_update_mod: zero
+// normal momentum at the wall, an explicit update of outer points, and
+// supersonic sources that may be wall points.
+void state_update_explicit(Oracle &o) {
+    double sum_res_sqr = 0.0;
+    o.max_res = 0.0;
+    double U[5];
+    for (int k : o.wall_idx) {
+        double temp = o.V5(o.U, 1, k);
+        for (int r = 0; r < 5; ++r) U[r] = o.V5(o.U, r + 1, k) + o.V5(o.delUn, r + 1, k);
+        U[3] = 0.0;
+        double res_sqr = (U[0] - temp) * (U[0] - temp);
+        if (res_sqr > o.max_res) { o.max_res = res_sqr; o.max_res_point = k; }
+        sum_res_sqr = sum_res_sqr + res_sqr;
+        conserved_to_primitive(o, k, U);
+        for (int r = 1; r <= 5; ++r) o.V5(o.delUp, r, k) = o.V5(o.delUn, r, k);
+    }
+    for (int k : o.outer_idx) {
+        conserved_vector_Ubar(o, k, U);
+        for (int r = 0; r < 5; ++r) U[r] = U[r] - o.delt[k] * o.V5(o.flux_res, r + 1, k);
+        conserved_to_primitive(o, k, U);
+    }
+    for (int k : o.interior_idx) {
+        double temp = o.V5(o.U, 1, k);
+        for (int r = 0; r < 5; ++r) U[r] = o.V5(o.U, r + 1, k) + o.V5(o.delUn, r + 1, k);
+        double res_sqr = (U[0] - temp) * (U[0] - temp);
+        if (res_sqr > o.max_res) { o.max_res = res_sqr; o.max_res_point = k; }
+        sum_res_sqr = sum_res_sqr + res_sqr;
+        conserved_to_primitive(o, k, U);
+        for (int r = 1; r <= 5; ++r) o.V5(o.delUp, r, k) = o.V5(o.delUn, r, k);
+    }
+    for (int k : o.ss_outlet_idx) {
+        int p = nearest_neighbour(o, k, false, 100000.0);
+        for (int r = 1; r <= 5; ++r) o.V5(o.prim, r, k) = o.V5(o.prim, r, p);
+    }
+    for (int k : o.ss_inlet_idx) {
+        int p = nearest_neighbour(o, k, false, 100000.0);
+        for (int r = 1; r <= 5; ++r) o.V5(o.prim, r, k) = o.V5(o.prim, r, p);
+    }
+    o.res_new = std::sqrt(sum_res_sqr) / (double)o.N;
+}
+
 // fpi_solver.f90:20-45
 void fpi_solver(Oracle &o, int t) {
     compute_conserved_vector(o);
@@ -837,7 +880,8 @@ void fpi_solver(Oracle &o, int t) {
     timestep_delt(o);
     eval_flux_residual(o);
     implicit_forward_backward_sweeps(o);
-    state_update(o);
+    if (o.P.update_variant) state_update_explicit(o);
+    else state_update(o);
     if (t <= 2) {
         o.res_old = o.res_new;
         o.residue = 0.0;
@@ -857,6 +901,7 @@ struct oracle_params_c {
     double rho_inf, u1_inf, u2_inf, u3_inf, pr_inf;
     int inner_iterations;
     int split_capacity;
+    int update_variant;
 };
 
 void *oracle_create(const oracle_params_c *pp, int N, const int *status, const double *x,
@@ -868,6 +913,7 @@ void *oracle_create(const oracle_params_c *pp, int N, const int *status, const d
     o->P.u3_inf = pp->u3_inf; o->P.pr_inf = pp->pr_inf;
     o->P.inner_iterations = pp->inner_iterations;
     o->P.split_capacity = pp->split_capacity;
+    o->P.update_variant = pp->update_variant;
     o->N = N;
     o->cap = pp->split_capacity;
     size_t n1 = (size_t)N + 1;

@@ -14,11 +14,14 @@ pytestmark = pytest.mark.gpu
 FIELDS = ["PRIM", "U", "Q", "QM", "DQ", "DELT", "FLUX_RES", "DELUP", "DELUN"]
 
 
-def _pair(cloud, mach, aoa, libm, oracle_lib, sweep_mode=0, inner_iterations=0, power=0.0):
+def _pair(cloud, mach, aoa, libm, oracle_lib, sweep_mode=0, inner_iterations=0, power=0.0,
+          update_variant=0):
     from mfcfd.solver import Solver
     from mfcfd.cloud import initial_state
-    s = Solver(cloud, mach, aoa, sweep_mode=sweep_mode, inner_iterations=inner_iterations, power=power)
-    o = oracle_lib.Oracle(cloud, mach, aoa, libm=libm, inner_iterations=inner_iterations, power=power)
+    s = Solver(cloud, mach, aoa, sweep_mode=sweep_mode, inner_iterations=inner_iterations, power=power,
+               update_variant=update_variant)
+    o = oracle_lib.Oracle(cloud, mach, aoa, libm=libm, inner_iterations=inner_iterations, power=power,
+                          update_variant=update_variant)
     prim0 = initial_state(cloud, mach, aoa)
     s.initial_conditions(prim0)
     o.set_prim(prim0)
@@ -106,6 +109,23 @@ def test_weighted_least_squares_bitexact(small_cloud, oracle_lib, mfcfd_lib, pow
     s.q_lskum(3)
     for t in range(1, 4):
         o.step(t)
+    for name, fg, fo in _field_ids(oracle_lib):
+        a, b = s.get(fg), o.get(fo)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
+
+
+@pytest.mark.parametrize("supersonic", [False, True])
+def test_explicit_update_variant_bitexact(oracle_lib, mfcfd_lib, supersonic):
+    """MFCFD_UPDATE_EXPLICIT (state_update.f90), every field after 4 iterations."""
+    from mfcfd import cloud
+    c = cloud.small_sphere(6, 100, r1=1.5)
+    if supersonic:
+        c = cloud.with_supersonic_boundary(c)
+    s, o = _pair(c, 0.8, 2.0, oracle_lib.LIBM_MFMATH, oracle_lib, update_variant=1)
+    hist = s.q_lskum(4)
+    for t in range(1, 5):
+        rc = o.step(t)
+        assert abs(hist[t - 1, 0] - rc[0]) <= 1e-13 * abs(rc[0])
     for name, fg, fo in _field_ids(oracle_lib):
         a, b = s.get(fg), o.get(fo)
         assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name

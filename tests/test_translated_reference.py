@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 REF = "/root/reference"
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "sphere_600.npz")
 
 pytestmark = pytest.mark.skipif(not os.path.isdir(REF), reason="reference checkout absent")
@@ -92,3 +93,36 @@ def test_oracle_weighted_least_squares_match_translated_reference(oracle_lib, po
                       ("flux_res", oracle_lib.FIELD_FLUX_RES), ("delun", oracle_lib.FIELD_DELUN)):
         assert np.array_equal(r.get(name), o.get(fid)), name
     ref_translated.TranslatedReference(c, p0, 0.8, 2.0)   # back to the defaults
+
+
+_EXPLICIT_CHECK = """
+import sys
+sys.path.insert(0, {repo!r}); sys.path.insert(0, {pkg!r})
+import numpy as np
+from mfcfd import cloud
+from oracle import ref_translated, oracle
+for sup in (False, True):
+    c = cloud.small_sphere(6, 100, r1=1.5)
+    if sup:
+        c = cloud.with_supersonic_boundary(c)
+    p0 = cloud.initial_state(c, 0.8, 2.0)
+    r = ref_translated.TranslatedReference(c, p0, 0.8, 2.0, libm="explicit")
+    o = oracle.Oracle(c, 0.8, 2.0, update_variant=1)
+    o.set_prim(p0)
+    assert all(r.step(t) == o.step(t) for t in range(1, 5))
+    for name, fid in (("prim", oracle.FIELD_PRIM), ("delup", oracle.FIELD_DELUP), ("delun", oracle.FIELD_DELUN)):
+        assert np.array_equal(r.get(name), o.get(fid)), (sup, name)
+print("ok")
+"""
+
+
+def test_oracle_explicit_update_matches_translated_reference(oracle_lib):
+    """state_update.f90 (the reference's other state_update_mod), with and
+    without supersonic points: restatement and reference agree bit for bit.
+    Its own process: one translated build per process."""
+    from oracle import ref_translated
+    if not ref_translated.available("explicit"):
+        pytest.skip("translated reference variant not built")
+    code = _EXPLICIT_CHECK.format(repo=REPO, pkg=os.path.join(REPO, "3d-mfcfd_b200"))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stderr[-2000:]
