@@ -218,6 +218,11 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         *out = h;
         return MFCFD_ERR_ARG;
     }
+    if (P.sweep_variant != MFCFD_SWEEPS_ALIAS && P.sweep_variant != MFCFD_SWEEPS_BACKUP) {
+        h->err = "unknown sweep_variant";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
     if (P.update_variant != MFCFD_UPDATE_IMPLICIT && P.update_variant != MFCFD_UPDATE_EXPLICIT) {
         h->err = "unknown update_variant";
         *out = h;
@@ -265,6 +270,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.power = P.power;
     d.inner_iterations = P.inner_iterations;
     d.update_variant = P.update_variant;
+    d.sweep_variant = P.sweep_variant;
     d.cfl = P.cfl;
     d.rho_inf = P.rho_inf; d.u1_inf = P.u1_inf; d.u2_inf = P.u2_inf;
     d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;
@@ -318,6 +324,8 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     UP(fwd_cnt, T.fwd_cnt); UP(bwd_cnt, T.bwd_cnt);
     UP(fwd_ent, T.fwd_ent); UP(bwd_ent, T.bwd_ent);
     UP(fwd_need, T.fwd_need); UP(bwd_need, T.bwd_need);
+    UP(fwd_old, T.fwd_old); UP(bwd_old, T.bwd_old); UP(sweep_slot_mask, T.sweep_slot_mask);
+    if (!T.outer_delt.empty()) UP(outer_delt, T.outer_delt);
     UP(res_order, order);
 #undef UP
     d.n_fwd_levels = (int)T.fwd_lvl_ptr.size() - 1;
@@ -338,8 +346,9 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     AL(d.gold, (size_t)n * 30); AL(d.dgf, (size_t)n * DG_STRIDE); AL(d.dgb, (size_t)n * DG_STRIDE);
     AL(d.res_sqr, n); AL(d.partial, 1024); AL(d.res_dev, h->res_cap);
     if (P.inner_iterations > 0) AL(d.dq_tmp, (size_t)n * 15);
+    if (P.sweep_variant == MFCFD_SWEEPS_BACKUP) AL(d.dg_old, (size_t)n * DG_STRIDE);
+    if (!T.ss_pts.empty() || P.sweep_variant == MFCFD_SWEEPS_BACKUP) AL(d.dU_old, n5);
     if (!T.ss_pts.empty()) {
-        AL(d.dU_old, n5);
         d.n_ss = (int)T.ss_pts.size();
         if ((rc = upload(h, &d.ss_pts, T.ss_pts))) return rc;
         if ((rc = upload(h, &d.ss_src, T.ss_src))) return rc;

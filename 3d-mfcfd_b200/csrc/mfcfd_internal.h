@@ -72,6 +72,10 @@ struct Topology {
     std::vector<uint8_t> fwd_cnt, bwd_cnt;        // n*6
     std::vector<SweepEntry> fwd_ent, bwd_ent;
     std::vector<uint32_t> fwd_need, bwd_need;     // slots with terms in the sweep
+    std::vector<uint32_t> fwd_old, bwd_old;       // slots read from before the sweep (backup driver)
+    std::vector<uint8_t> sweep_slot_mask;         // n*MAX_SLOTS: lists of the sweep terms per slot
+    std::vector<double> outer_delt;               // backup driver: D_inv_outer's 1/delt operand, NaN: time step
+    int sweep_variant = 0;
     std::vector<uint8_t> swept;                   // 1 if the sweeps update the point
     std::vector<uint8_t> consumer_shared;         // 1: reads published flux increments
     int shared_frame = 0;
@@ -101,6 +105,7 @@ enum : uint32_t {
     CI_SHARED = 2,    // consumer in the shared frame (reads published increments)
     CI_PUBLISH = 4,   // some consumer reads this point's increment from global memory
     CI_COPY = 8,      // supersonic point: copies its nearest neighbour's increment
+    CI_OUTER = 16,    // outer point (backup driver): octant lists, z+ over conn, own D_inv
 };
 // Bits the chain schedule adds to SweepEntry::pad (bits 0-15: list, slot).
 constexpr int32_t ENT_RING = 1 << 17;   // producer's increment is in the warp's ring
@@ -112,7 +117,11 @@ constexpr int32_t ENT_CHAIN_BITS = 0xff << 16;
 // the sweep (the previous iteration's delUn).
 constexpr int32_t ENT_COPY = 1 << 24;
 constexpr int32_t ENT_COPY_NEW = 1 << 25;
+// Backup driver: the producer comes later in the sweep's order, so the term
+// uses its increment from before the sweep (published in dg_old / dU_old).
+constexpr int32_t ENT_OLD = 1 << 26;
 inline bool entry_is_dependency(const SweepEntry &e) {
+    if (e.pad & ENT_OLD) return false;
     return !(e.pad & ENT_COPY) || (e.pad & ENT_COPY_NEW);
 }
 constexpr int CHAIN_RING = 8;           // increments a warp keeps in shared memory
@@ -175,6 +184,11 @@ struct DevCloud {
     const uint8_t *fwd_cnt, *bwd_cnt;
     const SweepEntry *fwd_ent, *bwd_ent;
     const uint32_t *fwd_need, *bwd_need;
+    const uint32_t *fwd_old, *bwd_old;
+    const uint8_t *sweep_slot_mask;
+    const double *outer_delt;
+    int sweep_variant;            // MFCFD_SWEEPS_*
+    double *dg_old;               // DG_STRIDE per point: increments from before the sweep (backup)
     const int32_t *res_order;     // wall then interior ids, index order
     int n_res;
     int n_swept;                  // points in each sweep order

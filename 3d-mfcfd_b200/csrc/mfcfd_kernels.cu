@@ -265,9 +265,10 @@ __device__ __forceinline__ void reconstruct(const DevCloud &d, int j, double del
 
 // Per-list diagonal terms of D_inv (implicit_D_inv_interior.f90:46-417 /
 // implicit_D_inv_wall.f90:45-356 with the geometry-only sums precomputed).
-// u: the velocity component of list dd's axis; as: the speed of sound.
-__device__ __forceinline__ double dinv_term(const DevCloud &d, int i, int dd, double u, double as) {
-    const double *g = d.geo + (size_t)i * GEO_STRIDE;
+// u: the velocity component of list dd's axis; as: the speed of sound;
+// row: the geometry row (dd, or 5 for an outer point's z+ over conn).
+__device__ __forceinline__ double dinv_term(const DevCloud &d, int i, int dd, double u, double as, int row) {
+    const double *g = d.geo + (size_t)i * GEO_STRIDE + (row - dd) * 8;
     const double temp = g[dd * 8 + G_DNUM], det = g[dd * 8 + G_DET];
     if ((dd & 1) == 0) {
         const double t1 = u + as;
@@ -275,6 +276,21 @@ __device__ __forceinline__ double dinv_term(const DevCloud &d, int i, int dd, do
     }
     const double t1 = u - as;
     return -(0.50 * fabs(t1 - fabs(t1)) * temp / det);
+}
+
+__device__ __forceinline__ double dinv_term(const DevCloud &d, int i, int dd, double u, double as) {
+    return dinv_term(d, i, dd, u, as, dd);
+}
+
+// implicit_D_inv_outer.f90:17-363 (backup driver) from the terms of rows
+// 0-3 and of row 5 (z+ over conn): no minus on the x-/y- terms, the source's
+// order of operations, and 1/delt of the tangential offset the direction
+// loops leave behind (outer_delt; NaN: the time step).
+__device__ __forceinline__ double dinv_outer(const DevCloud &d, int i, const double g5[5]) {
+    double dt = d.outer_delt[i];
+    if (dt != dt) dt = d.delt[i];
+    const double temp = (1.0 / dt) - g5[0] + (-g5[1]) - g5[2] + (-g5[3]) - g5[4];
+    return 1.0 / temp;
 }
 
 __device__ __forceinline__ double dinv_combine(int cls, double delt, const double gd[NDIR]) {
@@ -301,6 +317,14 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
 #pragma unroll
         for (int dd = 0; dd < NDIR; ++dd) gd[dd] = __shfl_sync(FULL, t, dd);
         if (lane == 0) st_relaxed_f64(d.dinv + i, dinv_combine(d.cls[i], d.delt[i], gd));
+    } else if (swept && d.cls[i] == CLS_OUTER) {      // backup driver
+        const double as = sqrt(1.40 * p[4] / p[0]);
+        const double u = lane < 2 ? p[1] : (lane < 4 ? p[2] : p[3]);
+        const double t = lane < 5 ? dinv_term(d, i, lane, u, as, lane == 4 ? 5 : lane) : 0.0;
+        double g5[5];
+#pragma unroll
+        for (int dd = 0; dd < 5; ++dd) g5[dd] = __shfl_sync(FULL, t, dd);
+        if (lane == 0) st_relaxed_f64(d.dinv + i, dinv_outer(d, i, g5));
     }
     if (d.shared_frame && lane < 30) {
         const int dd = lane / 5, c = lane - 5 * dd;
@@ -326,6 +350,18 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
             const size_t o = DG_STRIDE * (size_t)i + DG_LIST * dd + c;
             st_relaxed_f64(d.dgf + o, v);
             st_relaxed_f64(d.dgb + o, v);
+        }
+        if (d.dg_old) {   // backup driver: the increment from before the sweeps
+            double U[5], pn[5];
+            Frame F;
+            load_frame(d.frame + 9 * (size_t)i, F);
+#pragma unroll
+            for (int r = 0; r < 5; ++r) U[r] = d.dU_old[5 * (size_t)i + r] + d.U[5 * (size_t)i + r];
+            conserved_to_primitive(U, F, pn);
+            flux_pre(pn, F0, P);
+            axis_terms(P, dd >> 1, At);
+            st_relaxed_f64(d.dg_old + DG_STRIDE * (size_t)i + DG_LIST * dd + c,
+                           flux_component(dd, c, P, At, At, At) - gold);
         }
     }
 }
@@ -458,17 +494,18 @@ __global__ void k_pending(DevCloud d, int inputs) {
     for (size_t w = t0; w < ng; w += stride) {
         d.dgf[w] = pend;
         d.dgb[w] = pend;
+        if (inputs && d.dg_old) d.dg_old[w] = pend;   // produced beside the forward sweep
     }
     for (size_t w = t0; w < nu; w += stride) {
         if (d.swept[w / 5]) {
             d.dUp[w] = pend;
             d.dUn[w] = pend;
-            if (inputs && d.cls[w / 5] <= CLS_WALL) d.flux_res[w] = pend;
+            if (inputs && (d.cls[w / 5] <= CLS_WALL || d.cls[w / 5] == CLS_OUTER)) d.flux_res[w] = pend;
         }
     }
     if (inputs) {
         for (size_t w = t0; w < (size_t)d.n; w += stride)
-            if (d.swept[w] && d.cls[w] <= CLS_WALL) d.dinv[w] = pend;
+            if (d.swept[w] && (d.cls[w] <= CLS_WALL || d.cls[w] == CLS_OUTER)) d.dinv[w] = pend;
         if (d.shared_frame)
             for (size_t w = t0; w < n30; w += stride)
                 if (d.swept[w / 30]) d.gold[w] = pend;
@@ -491,6 +528,12 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
 #pragma unroll
         for (int dd = 0; dd < NDIR; ++dd) gd[dd] = dinv_term(d, i, dd, p[1 + (dd >> 1)], as);
         d.dinv[i] = dinv_combine(cls, d.delt[i], gd);
+    } else if (d.swept[i] && cls == CLS_OUTER) {   // backup driver
+        const double as = sqrt(1.40 * p[4] / p[0]);
+        double g5[5];
+#pragma unroll
+        for (int dd = 0; dd < 5; ++dd) g5[dd] = dinv_term(d, i, dd, p[1 + (dd >> 1)], as, dd == 4 ? 5 : dd);
+        d.dinv[i] = dinv_outer(d, i, g5);
     }
     if (d.shared_frame) {
         double prim[5], gold[30];
@@ -515,6 +558,18 @@ __global__ void __launch_bounds__(128) k_dinv_gold(DevCloud d) {
                 d.dgb[o] = v;
             }
         }
+        if (d.dg_old) {   // backup driver: the increment from before the sweeps
+            double U[5], pn[5], gnew[30];
+            Frame F;
+            load_frame(d.frame + 9 * (size_t)i, F);
+#pragma unroll
+            for (int r = 0; r < 5; ++r) U[r] = d.dU_old[5 * (size_t)i + r] + d.U[5 * (size_t)i + r];
+            conserved_to_primitive(U, F, pn);
+            flux6_frame0(d, pn, gnew);
+#pragma unroll
+            for (int c = 0; c < 30; ++c)
+                d.dg_old[DG_STRIDE * (size_t)i + DG_LIST * (c / 5) + c % 5] = gnew[c] - gold[c];
+        }
     }
 }
 
@@ -536,7 +591,8 @@ struct __align__(16) SweepStage {
     int32_t slot_nbr[MAX_SLOTS];
     uint8_t slot_mask[MAX_SLOTS];
     uint32_t need;
-    int32_t pad[3];
+    uint32_t old;                 // slots read from before the sweep (backup driver)
+    int32_t pad[2];
 };
 constexpr int SW_T_DOUBLES = NDIR * MAX_SLOTS * 5;                  // term fluxes, >= SWEEP_MAX_ENTRIES * 5
 constexpr int SW_RING_DOUBLES = CHAIN_RING * 30;                    // chain: last published increments
@@ -580,7 +636,7 @@ __device__ __forceinline__ ChainItem make_item(const DevCloud &d, int p, bool fo
 #pragma unroll
     for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[e] << (5 * e);
     it.info = (d.cls[p] == CLS_WALL ? CI_WALL : 0u) | (d.consumer_shared[p] ? CI_SHARED : 0u) | CI_PUBLISH |
-              (d.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u);
+              (d.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u) | (d.cls[p] == CLS_OUTER ? CI_OUTER : 0u);
     return it;
 }
 
@@ -607,8 +663,9 @@ __device__ __forceinline__ void stage_issue(const DevCloud &d, const ChainItem &
         cp_async8(st->dinv, d.dinv + p);
     } else if (!(it.info & CI_SHARED)) {
         if (lane < 23) cp_async16(st->slot_nbr + 4 * (lane - 15), d.slot_nbr + p * MAX_SLOTS + 4 * (lane - 15));
-        else if (lane < 25) cp_async16(st->slot_mask + 16 * (lane - 23), d.slot_mask + p * MAX_SLOTS + 16 * (lane - 23));
+        else if (lane < 25) cp_async16(st->slot_mask + 16 * (lane - 23), d.sweep_slot_mask + p * MAX_SLOTS + 16 * (lane - 23));
         else if (lane == 25) cp_async4(&st->need, (forward ? d.fwd_need : d.bwd_need) + p);
+        else if (lane == 26) cp_async4(&st->old, (forward ? d.fwd_old : d.bwd_old) + p);
     }
 }
 
@@ -636,7 +693,8 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     const bool wall = (it.info & CI_WALL) != 0;
     const bool shared = (it.info & CI_SHARED) != 0;
     const bool copy = (it.info & CI_COPY) != 0;       // supersonic point
-    const int cls = wall ? CLS_WALL : CLS_INTERIOR;   // of the points that solve
+    const bool outer = (it.info & CI_OUTER) != 0;     // backup driver
+    const int cls = wall ? CLS_WALL : (outer ? CLS_OUTER : CLS_INTERIOR);
     const SweepEntry *E = st->ent;
     const int dd = lane / 5, c = lane - 5 * (lane / 5);
     int total = 0, lo = 0, hi = 0;
@@ -652,8 +710,9 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     double g[7] = {0, 0, 0, 0, 0, 0, 1.0};
     double gold = 0.0;
     if (lane < 30) {
+        const int grow = (outer && dd == 4) ? 5 : dd;   // outer z+ over conn: row 5
 #pragma unroll
-        for (int r = 0; r < 7; ++r) g[r] = st->geo[dd * 8 + r];
+        for (int r = 0; r < 7; ++r) g[r] = st->geo[grow * 8 + r];
         gold = st->gold[lane];
     }
     double dinv = 0.0, base5 = 0.0;
@@ -739,7 +798,9 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                 for (int q = 0; q < 3; ++q) {
                     if (!((pend >> q) & 1u)) continue;
                     const int j = lane + 32 * q;
-                    const double *gs = src + DG_STRIDE * (size_t)E[j].k + DG_LIST * (E[j].pad & 255);
+                    // backup driver: a term from before the sweep reads dg_old
+                    const double *base = (E[j].pad & ENT_OLD) ? d.dg_old : src;
+                    const double *gs = base + DG_STRIDE * (size_t)E[j].k + DG_LIST * (E[j].pad & 255);
                     ld_relaxed_v2(gs, v[q][0], v[q][1]);
                     ld_relaxed_v2(gs + 2, v[q][2], v[q][3]);
                     v[q][4] = ld_relaxed_b64(gs + 4);
@@ -755,7 +816,8 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                 if (pend && !spin_continue(spins, d.err)) break;
             }
         } else if (mine) {
-            const double *dsrc = (forward ? d.dUp : d.dUn) + 5 * (size_t)k_slot;
+            const bool old = (st->old >> lane) & 1u;   // backup driver: from before the sweep
+            const double *dsrc = (old ? d.dU_old : (forward ? d.dUp : d.dUn)) + 5 * (size_t)k_slot;
             unsigned long long v[5];
             int spins = 0;
             do {
@@ -808,6 +870,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         if (lane < 5) {
             double lu;
             if (wall) lu = 2.0 * (gd[0] + gd[1] + gd[2] + gd[3] + gd[5]);
+            else if (outer) lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4];   // *_sweep_outer.f90:406
             else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
             if (forward) {
                 dnew = -(dinv * (base5 + lu));

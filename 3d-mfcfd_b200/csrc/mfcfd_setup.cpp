@@ -247,15 +247,26 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         const double dist = std::sqrt(dels * dels + delt * delt + deln * deln);
         return 1.0 / std::pow(dist, P.power);
     };
+    const bool backup = P.sweep_variant == MFCFD_SWEEPS_BACKUP;
+    T.sweep_variant = P.sweep_variant;
+    // the backup driver's outer routines take z+ over the full conn
+    // (implicit_D_inv_outer.f90:313-315): its moments go to the unused row 5
+    auto conn_z = [&](int i, int d) { return backup && d == 5 && T.cls[i] == CLS_OUTER; };
     parallel_for(n, [&](int i) {
         const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
         for (int d = 0; d < NDIR; ++d) {
-            int c = T.list_cnt[(size_t)i * NDIR + d];
+            const bool cz = conn_z(i, d);
+            int c = cz ? nbhs[i] : T.list_cnt[(size_t)i * NDIR + d];
             Moments m = {0, 0, 0, 0, 0, 0};
             double sdx = 0, sdy = 0, sdz = 0;
             for (int j = 0; j < c; ++j) {
-                int s = T.list_ent[((size_t)i * NDIR + d) * LIST_STRIDE + j];
-                int k = T.slot_nbr[(size_t)i * MAX_SLOTS + s];
+                int k;
+                if (cz) {
+                    k = conn[(size_t)i * MAX_CONN + j] - 1;
+                } else {
+                    int s = T.list_ent[((size_t)i * NDIR + d) * LIST_STRIDE + j];
+                    k = T.slot_nbr[(size_t)i * MAX_SLOTS + s];
+                }
                 double delx = x[k] - x[i], dely = y[k] - y[i], delz = z[k] - z[i];
                 double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
                 double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
@@ -314,16 +325,26 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         T.eps2[i] = e * e;
     }
 
-    // ---- sweep schedules (implicit_forward_and_reverse_sweeps.f90:26-84)
+    // ---- sweep schedules (implicit_forward_and_reverse_sweeps.f90:26-84, or
+    // implicit_forward_and_reverse_sweeps_backup.f90:26-141)
     T.swept.assign(n, 0);
-    std::vector<int> order;   // swept points in forward order (0-based)
-    for (int i = 0; i < n; ++i) {
-        int p = T.point_with_alias[i];
-        if (p == 0) continue;   // the reference's out-of-range entry
-        int cls = T.cls[p - 1];
-        if (cls == CLS_WALL || cls == CLS_INTERIOR || cls == CLS_SUPERSONIC) {
-            T.swept[p - 1] = 1;
-            order.push_back(p - 1);
+    std::vector<int> order_f, order_b;   // swept points in each sweep's order (0-based)
+    if (!backup) {
+        for (int i = 0; i < n; ++i) {
+            int p = T.point_with_alias[i];
+            if (p == 0) continue;   // the reference's out-of-range entry
+            int cls = T.cls[p - 1];
+            if (cls == CLS_WALL || cls == CLS_INTERIOR || cls == CLS_SUPERSONIC) {
+                T.swept[p - 1] = 1;
+                order_f.push_back(p - 1);
+            }
+        }
+        order_b.assign(order_f.rbegin(), order_f.rend());
+    } else {
+        for (const std::vector<int32_t> *cl : {&T.wall_idx, &T.interior_idx, &T.outer_idx, &T.ss_inlet_idx,
+                                               &T.ss_outlet_idx}) {
+            for (int p : *cl) { T.swept[p] = 1; order_f.push_back(p); }
+            for (auto it = cl->rbegin(); it != cl->rend(); ++it) order_b.push_back(*it);
         }
     }
     // nearest neighbour in conn order, first of equal distances, starting
@@ -347,22 +368,76 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     T.ss_pts.clear();
     T.ss_src.clear();
     for (int i = 0; i < n; ++i)
-        if (T.cls[i] == CLS_SUPERSONIC) T.copy_src[i] = nearest(i, false, 1000000.0);
+        if (T.cls[i] == CLS_SUPERSONIC)   // the backup driver skips walls, from 1e5
+            T.copy_src[i] = backup ? nearest(i, true, 100000.0) : nearest(i, false, 1000000.0);
+    // D_inv_outer's 1/delt operand: the tangential offset of the last conn
+    // neighbour, which the direction loops leave in the time-step variable
+    // (implicit_D_inv_outer.f90:47, :74); NaN: no neighbour, the time step
+    T.outer_delt.clear();
+    if (backup) {
+        T.outer_delt.assign(n, std::nan(""));
+        for (int i : T.outer_idx) {
+            if (nbhs[i] < 1) continue;
+            const int k = conn[(size_t)i * MAX_CONN + nbhs[i] - 1] - 1;
+            const double *t2 = tan2 + 3 * (size_t)i;
+            const double delx = x[k] - x[i], dely = y[k] - y[i], delz = z[k] - z[i];
+            T.outer_delt[i] = delx * t2[0] + dely * t2[1] + delz * t2[2];
+        }
+    }
+    // slot membership of the sweeps' term lists (outer z+ over conn under the
+    // backup driver)
+    T.sweep_slot_mask = T.slot_mask;
+    if (backup)
+        for (int i : T.outer_idx)
+            for (int s = 0; s < MAX_SLOTS; ++s) {
+                uint8_t &m = T.sweep_slot_mask[(size_t)i * MAX_SLOTS + s];
+                m &= (uint8_t)~(1u << 4);
+                if (s < T.nslot[i]) {
+                    const int k = T.slot_nbr[(size_t)i * MAX_SLOTS + s];
+                    for (int r = 0; r < nbhs[i]; ++r)
+                        if (conn[(size_t)i * MAX_CONN + r] - 1 == k) { m |= 1u << 4; break; }
+                }
+            }
     // state_update_implicit.f90 skips wall sources; state_update.f90 does not
     const bool skip_wall = P.update_variant != MFCFD_UPDATE_EXPLICIT;
     for (int k : T.ss_outlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, skip_wall, 100000.0)); }
     for (int k : T.ss_inlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, skip_wall, 100000.0)); }
     auto al = [&](int k) { return T.alias[k]; };
-    auto build = [&](bool forward, std::vector<int32_t> &level, std::vector<int32_t> &lptr,
-                     std::vector<int32_t> &lpts, std::vector<int32_t> &off,
-                     std::vector<uint8_t> &cnt, std::vector<SweepEntry> &ent,
-                     std::vector<uint32_t> &need) {
+    std::vector<int32_t> pos(n, -1);
+    // a point's sweep terms of list d in list order: (slot, neighbour)
+    auto for_terms = [&](int p, int d, auto &&fn) {
+        if (backup && d == 4 && T.cls[p] == CLS_OUTER) {   // z+ over conn
+            for (int r = 0; r < nbhs[p]; ++r) {
+                const int k = conn[(size_t)p * MAX_CONN + r] - 1;
+                int s = 0;
+                while (s < T.nslot[p] && T.slot_nbr[(size_t)p * MAX_SLOTS + s] != k) ++s;
+                fn(s, k);
+            }
+            return;
+        }
+        if (T.cls[p] == CLS_OUTER && d == 5) return;
+        const int c = T.list_cnt[(size_t)p * NDIR + d];
+        for (int j = 0; j < c; ++j) {
+            const int s = T.list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
+            fn(s, (int)T.slot_nbr[(size_t)p * MAX_SLOTS + s]);
+        }
+    };
+    auto build = [&](bool forward, const std::vector<int> &order, std::vector<int32_t> &level,
+                     std::vector<int32_t> &lptr, std::vector<int32_t> &lpts, std::vector<int32_t> &off,
+                     std::vector<uint8_t> &cnt, std::vector<SweepEntry> &ent, std::vector<uint32_t> &need,
+                     std::vector<uint32_t> &old) {
         level.assign(n, -1);
         need.assign(n, 0u);
+        old.assign(n, 0u);
         off.assign(n + 1, 0);
         cnt.assign((size_t)n * NDIR, 0);
-        // entries, in point index order of the offsets: count, then fill
+        for (size_t i = 0; i < order.size(); ++i) pos[order[i]] = (int32_t)i;
+        // the terms the reference's L/U routines take (alias test), and
+        // whether the producer's increment is this sweep's (earlier in the
+        // order) or from before it
         auto takes = [&](int p, int k) { return forward ? (al(k) < al(p)) : (al(k) > al(p)); };
+        auto is_old = [&](int p, int k) { return backup && pos[k] > pos[p]; };
+        // entries, in point index order of the offsets: count, then fill
         parallel_for((int)order.size(), [&](int oi) {
             const int p = order[oi];
             if (T.cls[p] == CLS_SUPERSONIC) {   // one copy entry
@@ -371,12 +446,8 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
                 return;
             }
             for (int d = 0; d < NDIR; ++d) {
-                const int c = T.list_cnt[(size_t)p * NDIR + d];
                 int taken = 0;
-                for (int j = 0; j < c; ++j) {
-                    const int s = T.list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
-                    if (takes(p, T.slot_nbr[(size_t)p * MAX_SLOTS + s])) ++taken;
-                }
+                for_terms(p, d, [&](int, int k) { if (takes(p, k)) ++taken; });
                 cnt[(size_t)p * NDIR + d] = (uint8_t)taken;
                 off[p + 1] += taken;
             }
@@ -390,18 +461,16 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
                 const int q = T.copy_src[p];
                 SweepEntry &e = ent[(size_t)off[p]];
                 e.k = q;
-                e.pad = ENT_COPY | ((q >= 0 && T.swept[q] && takes(p, q)) ? ENT_COPY_NEW : 0);
+                const bool fresh = q >= 0 && T.swept[q] && (backup ? pos[q] < pos[p] : takes(p, q));
+                e.pad = ENT_COPY | (fresh ? ENT_COPY_NEW : 0);
                 e.w[0] = e.w[1] = e.w[2] = 0.0;
                 return;
             }
             const double *t1 = tan1 + 3 * (size_t)p, *t2 = tan2 + 3 * (size_t)p, *nn = nor + 3 * (size_t)p;
             size_t e_at = (size_t)off[p];
             for (int d = 0; d < NDIR; ++d) {
-                const int c = T.list_cnt[(size_t)p * NDIR + d];
-                for (int j = 0; j < c; ++j) {
-                    const int s = T.list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
-                    const int k = T.slot_nbr[(size_t)p * MAX_SLOTS + s];
-                    if (!takes(p, k)) continue;
+                for_terms(p, d, [&](int s, int k) {
+                    if (!takes(p, k)) return;
                     double delx = x[k] - x[p], dely = y[k] - y[p], delz = z[k] - z[p];
                     double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
                     double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
@@ -409,15 +478,16 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
                     double w = weight(dels, delt, deln);
                     SweepEntry &e = ent[e_at++];
                     e.k = k;
-                    e.pad = d | (s << 8);   // list and neighbour slot
+                    e.pad = d | (s << 8) | (is_old(p, k) ? ENT_OLD : 0);   // list, neighbour slot
                     e.w[0] = dels * w; e.w[1] = delt * w; e.w[2] = deln * w;
                     need[p] |= 1u << s;
-                }
+                    if (is_old(p, k)) old[p] |= 1u << s;
+                });
             }
         });
         for (int p = 0; p < n; ++p)
             if (off[p + 1] - off[p] > SWEEP_MAX_ENTRIES) return false;
-        // levels: longest path over swept dependencies
+        // levels: longest path over swept dependencies, visited in the order
         int maxl = -1;
         auto visit = [&](int p) {
             int lv = 0;
@@ -429,8 +499,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             level[p] = lv;
             maxl = std::max(maxl, lv);
         };
-        if (forward) for (int p : order) visit(p);
-        else for (auto it = order.rbegin(); it != order.rend(); ++it) visit(*it);
+        for (int p : order) visit(p);
         int nl = maxl + 1;
         lptr.assign(nl + 1, 0);
         for (int p : order) lptr[level[p] + 1]++;
@@ -440,12 +509,13 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         }
         lpts.assign(order.size(), 0);
         std::vector<int32_t> fill(lptr.begin(), lptr.end() - 1);
-        if (forward) for (int p : order) lpts[fill[level[p]]++] = p;
-        else for (auto it = order.rbegin(); it != order.rend(); ++it) lpts[fill[level[*it]]++] = *it;
+        for (int p : order) lpts[fill[level[p]]++] = p;
         return true;
     };
-    if (!build(true, T.fwd_level, T.fwd_lvl_ptr, T.fwd_lvl_pts, T.fwd_off, T.fwd_cnt, T.fwd_ent, T.fwd_need) ||
-        !build(false, T.bwd_level, T.bwd_lvl_ptr, T.bwd_lvl_pts, T.bwd_off, T.bwd_cnt, T.bwd_ent, T.bwd_need)) {
+    if (!build(true, order_f, T.fwd_level, T.fwd_lvl_ptr, T.fwd_lvl_pts, T.fwd_off, T.fwd_cnt, T.fwd_ent,
+               T.fwd_need, T.fwd_old) ||
+        !build(false, order_b, T.bwd_level, T.bwd_lvl_ptr, T.bwd_lvl_pts, T.bwd_off, T.bwd_cnt, T.bwd_ent,
+               T.bwd_need, T.bwd_old)) {
         err = "a point reads more than " + std::to_string(SWEEP_MAX_ENTRIES) + " sweep terms";
         return MFCFD_ERR_STENCIL;
     }
@@ -552,7 +622,7 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
             for (int e = off[p]; e < off[p + 1]; ++e) {
                 SweepEntry &E = went[e];
                 E.pad &= ~ENT_CHAIN_BITS;
-                if (E.pad & ENT_COPY) continue;   // reads dU, never the ring
+                if (E.pad & (ENT_COPY | ENT_OLD)) continue;   // dU or from before the sweep
                 const int k = E.k;
                 if (!T.swept[k]) continue;   // fixed increment written before the sweep
                 const bool same = owner[k] == owner[p];
@@ -578,7 +648,8 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
             it.cnt = 0;
             for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[(size_t)p * NDIR + e] << (5 * e);
             it.info = (T.cls[p] == CLS_WALL ? CI_WALL : 0u) | (T.consumer_shared[p] ? CI_SHARED : 0u) |
-                      (publish[p] ? CI_PUBLISH : 0u) | (T.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u);
+                      (publish[p] ? CI_PUBLISH : 0u) | (T.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u) |
+                      (T.cls[p] == CLS_OUTER ? CI_OUTER : 0u);
         }
     }
 }
@@ -595,7 +666,7 @@ void build_pre_order(const Topology &T, std::vector<int32_t> &order) {
     for (int p = 0; p < n; ++p) {
         if (!T.swept[p]) continue;
         for (int e = T.fwd_off[p]; e < T.fwd_off[p + 1]; ++e) {
-            if (T.fwd_ent[e].pad & ENT_COPY) continue;   // copies read dU, not the flux kernel's output
+            if (T.fwd_ent[e].pad & (ENT_COPY | ENT_OLD)) continue;   // not waiting on the flux kernel
             const int k = T.fwd_ent[e].k;
             if (!T.swept[k]) key[k] = std::min(key[k], 2 * (int64_t)T.fwd_level[p]);
         }

@@ -41,11 +41,13 @@ class Params(ctypes.Structure):
                 ("inner_iterations", ctypes.c_int32), ("split_capacity", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("sweep_mode", ctypes.c_int32), ("update_variant", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 6)]
+                ("sweep_variant", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
 
 
 UPDATE_IMPLICIT = 0
 UPDATE_EXPLICIT = 1
+SWEEPS_ALIAS = 0
+SWEEPS_BACKUP = 1
 SWEEP_DATAFLOW = 0
 SWEEP_LEVELS = 1
 

@@ -81,8 +81,20 @@ typedef struct mfcfd_params {
                                  (stencils, alias, schedule) without device state */
     int32_t sweep_mode;       /* MFCFD_SWEEP_CHAINS (default), _DATAFLOW or _LEVELS */
     int32_t update_variant;   /* MFCFD_UPDATE_IMPLICIT (default) or MFCFD_UPDATE_EXPLICIT */
-    int32_t reserved[6];
+    int32_t sweep_variant;    /* MFCFD_SWEEPS_ALIAS (default) or MFCFD_SWEEPS_BACKUP */
+    int32_t reserved[5];
 } mfcfd_params;
+
+/* The reference ships two drivers of its sweep module.  ALIAS:
+ * implicit_forward_and_reverse_sweeps.f90 (the active build) sweeps wall and
+ * interior points in alias order.  BACKUP:
+ * implicit_forward_and_reverse_sweeps_backup.f90 sweeps the point classes in
+ * turn (wall, interior, outer with their own D_inv and L/U routines, then
+ * supersonic copies), each in index order and reversed for the backward
+ * sweep; a neighbour not yet updated in that order contributes its
+ * increment from before the sweep. */
+#define MFCFD_SWEEPS_ALIAS    0
+#define MFCFD_SWEEPS_BACKUP   1
 
 /* The reference ships two sources of its state_update module; a build
  * compiles one.  IMPLICIT: state_update_implicit.f90 (the active build).

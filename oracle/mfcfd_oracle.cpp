@@ -45,6 +45,7 @@ struct OracleParams {
     int inner_iterations;
     int split_capacity;   // 22 in the reference
     int update_variant;   // 0 state_update_implicit.f90, 1 state_update.f90
+    int sweep_variant;    // 0 implicit_forward_and_reverse_sweeps.f90, 1 ..._backup.f90
 };
 
 const double PI = 3.141592653589793;           // 4*datan(1d0), parameter.f90:19
@@ -755,6 +756,103 @@ int nearest_neighbour(Oracle &o, int p, bool skip_wall, double start) {
     return q;
 }
 
+// implicit_D_inv_outer.f90:17-363.  Every direction's loop assigns the
+// neighbour's tangential offset to the variable that held the time step, so
+// the 1/delt term uses the last conn neighbour's offset (or the time step
+// when the point has no neighbours); the x-/y- terms carry no minus sign and
+// the sum keeps the source's order.
+double implicit_D_inv_outer(Oracle &o, int i) {
+    double delt = o.delt[i];
+    double as = std::sqrt(1.40 * o.V5(o.prim, 5, i) / o.V5(o.prim, 1, i));
+    double dGxp = dinv_dir(o, i, {&o.xpos_conn, o.xpos_nbhs[i]}, AX_X, true, as);
+    double dGxn = -dinv_dir(o, i, {&o.xneg_conn, o.xneg_nbhs[i]}, AX_X, false, as);
+    double dGyp = dinv_dir(o, i, {&o.ypos_conn, o.ypos_nbhs[i]}, AX_Y, true, as);
+    double dGyn = -dinv_dir(o, i, {&o.yneg_conn, o.yneg_nbhs[i]}, AX_Y, false, as);
+    double dGzp = dinv_dir(o, i, {nullptr, o.nbhs[i]}, AX_Z, true, as);
+    const ListRef lists[5] = {{&o.xpos_conn, o.xpos_nbhs[i]}, {&o.xneg_conn, o.xneg_nbhs[i]},
+                              {&o.ypos_conn, o.ypos_nbhs[i]}, {&o.yneg_conn, o.yneg_nbhs[i]},
+                              {nullptr, o.nbhs[i]}};
+    for (const ListRef &L : lists) {
+        if (L.count < 1) continue;
+        int k = list_entry(o, L, L.count, i);
+        double delx = o.x[k] - o.x[i], dely = o.y[k] - o.y[i], delz = o.z[k] - o.z[i];
+        delt = delx * o.TAN2(1, i) + dely * o.TAN2(2, i) + delz * o.TAN2(3, i);
+    }
+    double temp = (1.0 / delt) - dGxp + dGxn - dGyp + dGyn - dGzp;
+    return 1.0 / temp;
+}
+
+// implicit_{LdelU_forward,UdelU_backward}_sweep_outer.f90: octant fluxes on
+// the x/y lists, the z+ split flux over the full conn.
+void sweep_LU_outer(Oracle &o, int i, bool forward, double out[5]) {
+    double a[5], b[5], c[5], d[5], e[5];
+    sweep_dir(o, a, i, {&o.xpos_conn, o.xpos_nbhs[i]}, GOXP, AX_X, forward);
+    sweep_dir(o, b, i, {&o.xneg_conn, o.xneg_nbhs[i]}, GOXN, AX_X, forward);
+    sweep_dir(o, c, i, {&o.ypos_conn, o.ypos_nbhs[i]}, GOYP, AX_Y, forward);
+    sweep_dir(o, d, i, {&o.yneg_conn, o.yneg_nbhs[i]}, GOYN, AX_Y, forward);
+    sweep_dir(o, e, i, {nullptr, o.nbhs[i]}, GZP, AX_Z, forward);
+    for (int r = 0; r < 5; ++r) out[r] = a[r] + b[r] + c[r] + d[r] + e[r];
+}
+
+// implicit_forward_and_reverse_sweeps_backup.f90:16-141: the point classes
+// in turn, each in index order (reversed backward), outer points included;
+// supersonic points copy their nearest non-wall neighbour.
+void sweeps_backup(Oracle &o) {
+    double LU[5];
+    for (int k : o.wall_idx) {
+        double D = implicit_D_inv(o, k, true);
+        o.dinv[k] = D;
+        sweep_LU(o, k, true, true, LU);
+        for (int r = 0; r < 5; ++r) o.V5(o.delUp, r + 1, k) = -(D * (o.V5(o.flux_res, r + 1, k) + LU[r]));
+    }
+    for (int k : o.interior_idx) {
+        double D = implicit_D_inv(o, k, false);
+        o.dinv[k] = D;
+        sweep_LU(o, k, false, true, LU);
+        for (int r = 0; r < 5; ++r) o.V5(o.delUp, r + 1, k) = -(D * (o.V5(o.flux_res, r + 1, k) + LU[r]));
+    }
+    for (int k : o.outer_idx) {
+        double D = implicit_D_inv_outer(o, k);
+        o.dinv[k] = D;
+        sweep_LU_outer(o, k, true, LU);
+        for (int r = 0; r < 5; ++r) o.V5(o.delUp, r + 1, k) = -(D * (o.V5(o.flux_res, r + 1, k) + LU[r]));
+    }
+    for (int k : o.ss_inlet_idx) {
+        int p = nearest_neighbour(o, k, true, 100000.0);
+        for (int r = 1; r <= 5; ++r) o.V5(o.delUp, r, k) = o.V5(o.delUp, r, p);
+    }
+    for (int k : o.ss_outlet_idx) {
+        int p = nearest_neighbour(o, k, true, 100000.0);
+        for (int r = 1; r <= 5; ++r) o.V5(o.delUp, r, k) = o.V5(o.delUp, r, p);
+    }
+    for (auto it = o.wall_idx.rbegin(); it != o.wall_idx.rend(); ++it) {
+        int k = *it;
+        double D = implicit_D_inv(o, k, true);
+        sweep_LU(o, k, true, false, LU);
+        for (int r = 0; r < 5; ++r) o.V5(o.delUn, r + 1, k) = o.V5(o.delUp, r + 1, k) - D * LU[r];
+    }
+    for (auto it = o.interior_idx.rbegin(); it != o.interior_idx.rend(); ++it) {
+        int k = *it;
+        double D = implicit_D_inv(o, k, false);
+        sweep_LU(o, k, false, false, LU);
+        for (int r = 0; r < 5; ++r) o.V5(o.delUn, r + 1, k) = o.V5(o.delUp, r + 1, k) - D * LU[r];
+    }
+    for (auto it = o.outer_idx.rbegin(); it != o.outer_idx.rend(); ++it) {
+        int k = *it;
+        double D = implicit_D_inv_outer(o, k);
+        sweep_LU_outer(o, k, false, LU);
+        for (int r = 0; r < 5; ++r) o.V5(o.delUn, r + 1, k) = o.V5(o.delUp, r + 1, k) - D * LU[r];
+    }
+    for (auto it = o.ss_inlet_idx.rbegin(); it != o.ss_inlet_idx.rend(); ++it) {
+        int k = *it, p = nearest_neighbour(o, k, true, 100000.0);
+        for (int r = 1; r <= 5; ++r) o.V5(o.delUn, r, k) = o.V5(o.delUn, r, p);
+    }
+    for (auto it = o.ss_outlet_idx.rbegin(); it != o.ss_outlet_idx.rend(); ++it) {
+        int k = *it, p = nearest_neighbour(o, k, true, 100000.0);
+        for (int r = 1; r <= 5; ++r) o.V5(o.delUn, r, k) = o.V5(o.delUn, r, p);
+    }
+}
+
 // implicit_forward_and_reverse_sweeps.f90:16-89
 void implicit_forward_backward_sweeps(Oracle &o) {
     double LdelU[5];
@@ -879,7 +977,8 @@ void fpi_solver(Oracle &o, int t) {
     eval_q_derivatives(o);
     timestep_delt(o);
     eval_flux_residual(o);
-    implicit_forward_backward_sweeps(o);
+    if (o.P.sweep_variant) sweeps_backup(o);
+    else implicit_forward_backward_sweeps(o);
     if (o.P.update_variant) state_update_explicit(o);
     else state_update(o);
     if (t <= 2) {
@@ -902,6 +1001,7 @@ struct oracle_params_c {
     int inner_iterations;
     int split_capacity;
     int update_variant;
+    int sweep_variant;
 };
 
 void *oracle_create(const oracle_params_c *pp, int N, const int *status, const double *x,
@@ -914,6 +1014,7 @@ void *oracle_create(const oracle_params_c *pp, int N, const int *status, const d
     o->P.inner_iterations = pp->inner_iterations;
     o->P.split_capacity = pp->split_capacity;
     o->P.update_variant = pp->update_variant;
+    o->P.sweep_variant = pp->sweep_variant;
     o->N = N;
     o->cap = pp->split_capacity;
     size_t n1 = (size_t)N + 1;

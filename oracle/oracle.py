@@ -31,7 +31,7 @@ class _Params(ctypes.Structure):
                 ("u1_inf", ctypes.c_double), ("u2_inf", ctypes.c_double),
                 ("u3_inf", ctypes.c_double), ("pr_inf", ctypes.c_double),
                 ("inner_iterations", ctypes.c_int), ("split_capacity", ctypes.c_int),
-                ("update_variant", ctypes.c_int)]
+                ("update_variant", ctypes.c_int), ("sweep_variant", ctypes.c_int)]
 
 
 _lib = None
@@ -79,12 +79,13 @@ class Oracle:
     """The reference's q-LSKUM iteration on the CPU, one fpi_solver call per step."""
 
     def __init__(self, cloud, mach, aoa_deg, cfl=5.0, vl_const=2.0, power=0.0,
-                 inner_iterations=0, split_capacity=22, libm=LIBM_GLIBC, update_variant=0):
+                 inner_iterations=0, split_capacity=22, libm=LIBM_GLIBC, update_variant=0,
+                 sweep_variant=0):
         from mfcfd.cloud import freestream   # noqa: deferred import
         L = lib()
         rho, u1, u2, u3, pr = freestream(mach, aoa_deg)
         self.params = _Params(power, vl_const, cfl, rho, u1, u2, u3, pr,
-                              inner_iterations, split_capacity, update_variant)
+                              inner_iterations, split_capacity, update_variant, sweep_variant)
         self.n = cloud.n
         self.libm = libm
         self._keep = [np.ascontiguousarray(a) for a in (

@@ -22,7 +22,8 @@ _REF_DIR_DEFAULT = "/root/reference"
 _LIBS = {"glibc": os.path.join(_HERE, "_ref", "libref.so"),
          "mfmath": os.path.join(_HERE, "_ref", "libref_mfmath.so"),
          # the reference's alternative module sources (f2c_ref.VARIANTS), glibc
-         "explicit": os.path.join(_HERE, "_ref", "libref_explicit.so")}
+         "explicit": os.path.join(_HERE, "_ref", "libref_explicit.so"),
+         "backup": os.path.join(_HERE, "_ref", "libref_backup.so")}
 _lib = None
 _lib_kind = None
 
@@ -42,7 +43,7 @@ def build(reference_dir: str = _REF_DIR_DEFAULT) -> bool:
     shim = os.path.join(_HERE, "ref_mfmath_shim.h")
     subprocess.run(common + ["-include", shim, "-o", _LIBS["mfmath"], out_c,
                              os.path.join(_HERE, "ref_runtime.c"), "-lm"], check=True)
-    for variant in ("explicit",):
+    for variant in ("explicit", "backup"):
         out_v = os.path.join(_HERE, "_ref", f"ref_translated_{variant}.c")
         subprocess.run(["python", os.path.join(_HERE, "f2c_ref.py"), reference_dir, out_v, variant],
                        check=True, stdout=subprocess.DEVNULL)
