@@ -38,6 +38,8 @@ struct mfcfd_handle {
     double phase_ms[MFCFD_NPHASE] = {0};
     int64_t prof_iters = 0;
     int64_t chain_terms[3] = {0, 0, 0};   // chain schedule: ring, same-warp, cross-warp terms
+    double *wall_area = nullptr;           // per-point areas for mfcfd_forces (device), or null
+    double *force_out = nullptr;           // 3 doubles (device)
 };
 
 namespace {
@@ -113,59 +115,73 @@ int finish_step(mfcfd_handle *h, int32_t t, double res_new) {
     return MFCFD_OK;
 }
 
+// Launch iteration j of the current chunk (iteration slot j of res_dev).
+int launch_one(mfcfd_handle *h, int j) {
+    DevCloud dc = h->d;
+    dc.U = h->U_buf[h->cur];
+    dc.q = h->q_buf[h->cur];
+    cudaEvent_t *ev = h->profiling ? &h->ev[(size_t)j * (MFCFD_NPHASE + 1)] : nullptr;
+    const IterStreams st{h->stream, h->side, h->fork, h->join};
+    cudaError_t e = launch_iteration(dc, j, st, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], ev);
+    if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+    h->last = h->cur;
+    h->cur = 1 - h->cur;
+    return MFCFD_OK;
+}
+
+// Wait for a chunk of `chunk` launched iterations (t = t0 ..) and do the
+// host bookkeeping; res_hist (may be null) gets (res_new, residue) pairs.
+int finish_chunk(mfcfd_handle *h, int32_t t0, int chunk, double *res_hist, int *status) {
+    std::vector<double> res(chunk);
+    int err_flag = 0;
+    CK(cudaMemcpyAsync(res.data(), h->d.res_dev, sizeof(double) * chunk, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(&err_flag, h->d.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (err_flag) {
+        CK(cudaMemsetAsync(h->d.err, 0, sizeof(int), h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return fail(h, MFCFD_ERR_TIMEOUT, "a sweep wait ran out; the iteration results are invalid");
+    }
+    if (h->profiling) {
+        for (int j = 0; j < chunk; ++j) {
+            const cudaEvent_t *ev = &h->ev[(size_t)j * (MFCFD_NPHASE + 1)];
+            // event pairs per phase; under the chain schedule the flux
+            // residual (ended by event 2, side stream) starts at event 3
+            // and runs beside the forward sweep, after k_pending (1-3)
+            static const int kSeq[MFCFD_NPHASE][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}};
+            static const int kFused[MFCFD_NPHASE][2] = {{0, 1}, {3, 2}, {1, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}};
+            const bool fused = h->d.sweep_mode == MFCFD_SWEEP_CHAINS;
+            for (int ph = 0; ph < MFCFD_NPHASE; ++ph) {
+                float ms = 0.f;
+                const int *pr = fused ? kFused[ph] : kSeq[ph];
+                CK(cudaEventElapsedTime(&ms, ev[pr[0]], ev[pr[1]]));
+                h->phase_ms[ph] += ms;
+            }
+        }
+        h->prof_iters += chunk;
+    }
+    for (int j = 0; j < chunk; ++j) {
+        int rc = finish_step(h, t0 + j, res[j]);
+        if (rc && *status == MFCFD_OK) *status = rc;
+        if (res_hist) {
+            res_hist[2 * (size_t)j] = h->res_new;
+            res_hist[2 * (size_t)j + 1] = h->residue;
+        }
+    }
+    return MFCFD_OK;
+}
+
 int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist) {
     if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
-    std::vector<double> res(h->res_cap);
     int status = MFCFD_OK;
     for (int32_t done = 0; done < iters;) {
         int chunk = std::min<int32_t>(iters - done, h->res_cap);
         for (int j = 0; j < chunk; ++j) {
-            DevCloud dc = h->d;
-            dc.U = h->U_buf[h->cur];
-            dc.q = h->q_buf[h->cur];
-            cudaEvent_t *ev = h->profiling ? &h->ev[(size_t)j * (MFCFD_NPHASE + 1)] : nullptr;
-            const IterStreams st{h->stream, h->side, h->fork, h->join};
-            cudaError_t e = launch_iteration(dc, j, st, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], ev);
-            if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
-            h->last = h->cur;
-            h->cur = 1 - h->cur;
+            int rc = launch_one(h, j);
+            if (rc) return rc;
         }
-        int err_flag = 0;
-        CK(cudaMemcpyAsync(res.data(), h->d.res_dev, sizeof(double) * chunk, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(&err_flag, h->d.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        if (err_flag) {
-            CK(cudaMemsetAsync(h->d.err, 0, sizeof(int), h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-            return fail(h, MFCFD_ERR_TIMEOUT, "a sweep wait ran out; the iteration results are invalid");
-        }
-        if (h->profiling) {
-            for (int j = 0; j < chunk; ++j) {
-                const cudaEvent_t *ev = &h->ev[(size_t)j * (MFCFD_NPHASE + 1)];
-                // event pairs per phase; under the chain schedule the flux
-                // residual (ended by event 2, side stream) starts at event 3
-                // and runs beside the forward sweep, after k_pending (1-3)
-                static const int kSeq[MFCFD_NPHASE][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}};
-                static const int kFused[MFCFD_NPHASE][2] = {{0, 1}, {3, 2}, {1, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}};
-                const bool fused = h->d.sweep_mode == MFCFD_SWEEP_CHAINS;
-                for (int ph = 0; ph < MFCFD_NPHASE; ++ph) {
-                    float ms = 0.f;
-                    const int *pr = fused ? kFused[ph] : kSeq[ph];
-                    CK(cudaEventElapsedTime(&ms, ev[pr[0]], ev[pr[1]]));
-                    h->phase_ms[ph] += ms;
-                }
-            }
-            h->prof_iters += chunk;
-        }
-        for (int j = 0; j < chunk; ++j) {
-            int32_t t = t0 + done + j;
-            int rc = finish_step(h, t, res[j]);
-            if (rc && status == MFCFD_OK) status = rc;
-            if (res_hist) {
-                res_hist[2 * (size_t)(done + j)] = h->res_new;
-                res_hist[2 * (size_t)(done + j) + 1] = h->residue;
-            }
-        }
+        int rc = finish_chunk(h, t0 + done, chunk, res_hist ? res_hist + 2 * (size_t)done : nullptr, &status);
+        if (rc) return rc;
         done += chunk;
     }
     return status;
@@ -289,7 +305,9 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
         // about twice the widest level in warps, all co-resident
         int wpb = 0, blocks = 0;
-        const int w = chain_shape(P.device, 2 * T.max_level_width, &wpb, &blocks);
+        if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
+        const int want = P.chain_warps > 0 ? P.chain_warps : 2 * T.max_level_width;
+        const int w = chain_shape(P.device, want, &wpb, &blocks);
         if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
         ChainSchedule S;
         build_chain_schedule(h->T, w, S);
@@ -331,6 +349,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.n_fwd_levels = (int)T.fwd_lvl_ptr.size() - 1;
     d.n_bwd_levels = (int)T.bwd_lvl_ptr.size() - 1;
     d.n_res = (int)order.size();
+    d.n_wall = (int)T.wall_idx.size();
     d.n_swept = (int)T.fwd_lvl_pts.size();
     d.max_width = T.max_level_width;
     d.sweep_mode = P.sweep_mode;
@@ -542,6 +561,102 @@ int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new) {
     cudaError_t e = cudaSetDevice(h->P.device);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
     return residual_noalloc(h->d, h->stream, res_new, h->err);
+}
+
+int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, int32_t iters, double *res_hist,
+                    int32_t *status) {
+    if (!hs || count < 1 || !t0 || iters < 0) return MFCFD_ERR_ARG;
+    const int dev = hs[0] ? hs[0]->P.device : -1;
+    for (int32_t i = 0; i < count; ++i) {
+        mfcfd_handle *h = hs[i];
+        if (!h || !h->stream || !h->have_state || h->P.device != dev) return MFCFD_ERR_ARG;
+        for (int32_t j = 0; j < i; ++j)
+            if (hs[j] == h) return MFCFD_ERR_ARG;   // each handle once
+        if (status) status[i] = MFCFD_OK;
+    }
+    if (cudaSetDevice(dev) != cudaSuccess) return MFCFD_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int capacity = chain_block_capacity(dev);
+    int first_err = MFCFD_OK;
+    // waves of handles whose chain sweep blocks fit on the device together
+    for (int32_t a = 0; a < count;) {
+        int32_t b = a;
+        int used = 0;
+        while (b < count) {
+            const DevCloud &d = hs[b]->d;
+            const int blocks = d.sweep_mode == MFCFD_SWEEP_CHAINS ? d.ch_warps / d.ch_wpb : 0;
+            if (b > a && used + blocks > capacity) break;
+            used += blocks;
+            ++b;
+        }
+        int cap = iters;
+        for (int32_t i = a; i < b; ++i) cap = std::min(cap, hs[i]->res_cap);
+        for (int32_t done = 0; done < iters;) {
+            const int chunk = std::min<int32_t>(iters - done, std::max(cap, 1));
+            // one iteration of every handle in turn: their streams overlap
+            for (int j = 0; j < chunk; ++j)
+                for (int32_t i = a; i < b; ++i) {
+                    int rc = launch_one(hs[i], j);
+                    if (rc) return rc;
+                }
+            for (int32_t i = a; i < b; ++i) {
+                int st = MFCFD_OK;
+                double *rh = res_hist ? res_hist + 2 * ((size_t)i * iters + done) : nullptr;
+                int rc = finish_chunk(hs[i], t0[i] + done, chunk, rh, &st);
+                if (!rc) rc = st;
+                if (status && rc && status[i] == MFCFD_OK) status[i] = rc;
+                if (rc && first_err == MFCFD_OK) first_err = rc;
+            }
+            done += chunk;
+        }
+        a = b;
+    }
+    return first_err;
+}
+
+int mfcfd_set_wall_areas(mfcfd_handle *h, const double *area) {
+    if (!h) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    CK(cudaSetDevice(h->P.device));
+    if (!area) {
+        h->wall_area = nullptr;   // the allocation stays with the handle
+        return MFCFD_OK;
+    }
+    if (!h->wall_area) {
+        int rc = dalloc(h, &h->wall_area, (size_t)h->d.n);
+        if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(h->wall_area, area, sizeof(double) * (size_t)h->d.n, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return MFCFD_OK;
+}
+
+int mfcfd_forces(mfcfd_handle *h, double wall_area, double ref_area, double *cl, double *cd, double *force) {
+    if (!h) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
+    if (!(ref_area > 0.0)) return fail(h, MFCFD_ERR_ARG, "ref_area must be positive");
+    if (!h->wall_area && (h->d.n_wall < 1 || !(wall_area > 0.0)))
+        return fail(h, MFCFD_ERR_ARG, "wall_area must be positive (or set per-point areas)");
+    CK(cudaSetDevice(h->P.device));
+    if (!h->force_out) {
+        int rc = dalloc(h, &h->force_out, 3);
+        if (rc) return rc;
+    }
+    const double each = h->d.n_wall > 0 ? wall_area / h->d.n_wall : 0.0;
+    CK(launch_forces(h->d, h->stream, each, h->wall_area, h->force_out));
+    double F[3];
+    CK(cudaMemcpyAsync(F, h->force_out, sizeof F, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const double u1 = h->P.u1_inf, u2 = h->P.u2_inf, u3 = h->P.u3_inf;
+    const double v = std::sqrt(u1 * u1 + u2 * u2 + u3 * u3);
+    const double sa = v > 0.0 ? u2 / v : 0.0, ca = v > 0.0 ? u1 / v : 1.0;
+    const double q = 0.5 * h->P.rho_inf * v * v * ref_area;
+    if (cl) *cl = (F[0] * (-sa) + F[1] * ca) / q;
+    if (cd) *cd = (F[0] * ca + F[1] * sa) / q;
+    if (force) { force[0] = F[0]; force[1] = F[1]; force[2] = F[2]; }
+    return MFCFD_OK;
 }
 
 int mfcfd_destroy(mfcfd_handle *h) {

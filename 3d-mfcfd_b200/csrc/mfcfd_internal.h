@@ -191,6 +191,7 @@ struct DevCloud {
     double *dg_old;               // DG_STRIDE per point: increments from before the sweep (backup)
     const int32_t *res_order;     // wall then interior ids, index order
     int n_res;
+    int n_wall;                   // the first n_wall entries of res_order
     int n_swept;                  // points in each sweep order
     int max_width;                // widest sweep level
     int sweep_mode;               // MFCFD_SWEEP_*
@@ -228,11 +229,16 @@ struct IterStreams {
 cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams &st,
                              double *U_next, double *q_next, cudaEvent_t *ev);
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
+// out[0..2] (device) = -sum over wall points of (p - p_inf) A nor
+cudaError_t launch_forces(const DevCloud &d, cudaStream_t s, double area_each, const double *area, double *out);
 int reduction_blocks(int n);
 // Launch shape of the chain sweep for about `want` warps: warps per block
 // and blocks (one block per SM, some SMs left free); returns the warps, 0 if
 // the kernel cannot run on the device.
 int chain_shape(int device, int want, int *wpb, int *blocks);
+// Chain sweep blocks that may be resident at once (one per SM, some SMs
+// left to the flux kernels).
+int chain_block_capacity(int device);
 // File formats of the reference program (mfcfd_io.cpp).  Handle-less calls
 // leave their message in g_io_err (mfcfd_last_error(NULL)).
 extern thread_local std::string g_io_err;

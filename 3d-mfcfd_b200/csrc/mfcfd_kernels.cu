@@ -1112,6 +1112,39 @@ __global__ void k_reduce_final(DevCloud d, int nblocks, int slot) {
     d.res_dev[slot] = sqrt(acc) / (double)d.n;
 }
 
+// ---------------------------------------------------------------- forces
+
+// F = -sum over wall points of (p_i - p_inf) A_i nor_i, one block: thread t
+// sums the wall points t, t + 256, ... in index order, then a fixed tree;
+// A_i from area (per point) or area_each.  out[0..2] = F.
+__global__ void __launch_bounds__(RED_THREADS) k_forces(DevCloud d, double area_each, const double *area,
+                                                          double *out) {
+    __shared__ double s[3][RED_THREADS];
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int j = threadIdx.x; j < d.n_wall; j += RED_THREADS) {
+        const int i = d.res_order[j];          // wall points first, index order
+        const double a = area ? area[i] : area_each;
+        const double dp = d.prim[5 * (size_t)i + 4] - d.pr_inf;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) f[r] = f[r] - dp * a * d.frame[9 * (size_t)i + 6 + r];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) s[r][threadIdx.x] = f[r];
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) s[r][threadIdx.x] += s[r][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 3) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
+cudaError_t launch_forces(const DevCloud &d, cudaStream_t s, double area_each, const double *area, double *out) {
+    k_forces<<<1, RED_THREADS, 0, s>>>(d, area_each, area, out);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- launchers
 
 int reduction_blocks(int n) {
@@ -1196,6 +1229,12 @@ static void set_attributes(int device) {
     cudaFuncSetAttribute(k_sweep_chain<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
     cudaFuncSetAttribute(k_sweep_chain<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     done[device] = true;
+}
+
+int chain_block_capacity(int device) {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return sms - CH_FREE_SMS;
 }
 
 int chain_shape(int device, int want, int *wpb, int *blocks) {

@@ -26,6 +26,7 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_get_stream", "mfcfd_set_profiling", "mfcfd_get_phase_times",
            "mfcfd_residual_noalloc", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
+           "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
 NOALLOC_MAX_TERMS = 1024 * 4096
 NPHASE = 7
@@ -41,7 +42,8 @@ class Params(ctypes.Structure):
                 ("inner_iterations", ctypes.c_int32), ("split_capacity", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("sweep_mode", ctypes.c_int32), ("update_variant", ctypes.c_int32),
-                ("sweep_variant", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("sweep_variant", ctypes.c_int32), ("chain_warps", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
 
 UPDATE_IMPLICIT = 0
@@ -106,6 +108,9 @@ def lib():
     L.mfcfd_read_stored_solution.argtypes = [cp, i32, vp]
     L.mfcfd_print_primal_output.argtypes = [vp, cp]
     L.mfcfd_write_residue.argtypes = [cp, i32, i32, vp, i32]
+    L.mfcfd_forces.argtypes = [vp, dbl, dbl, vp, vp, vp]
+    L.mfcfd_set_wall_areas.argtypes = [vp, vp]
+    L.mfcfd_run_batch.argtypes = [vp, i32, vp, i32, vp, vp]
     L.mfcfd_destroy.argtypes = [vp]
     L.mfcfd_last_error.argtypes = [vp]
     L.mfcfd_last_error.restype = ctypes.c_char_p

@@ -86,6 +86,18 @@ class Solver:
         import os
         self._check(_lib.lib().mfcfd_print_primal_output(self.h, os.fsencode(directory)))
 
+    def forces(self, wall_area: float | None = None, ref_area: float | None = None):
+        """(CL, CD, F) of the current state: F = -sum over wall points of
+        (p - p_inf) A nor with A = wall_area / n_wall (defaults: the cloud's
+        own areas)."""
+        wa = self.cloud.wall_area if wall_area is None else wall_area
+        ra = self.cloud.ref_area if ref_area is None else ref_area
+        cl, cd = ctypes.c_double(), ctypes.c_double()
+        f = np.zeros(3)
+        self._check(_lib.lib().mfcfd_forces(self.h, float(wa), float(ra), ctypes.byref(cl),
+                                            ctypes.byref(cd), ptr(f)))
+        return float(cl.value), float(cd.value), f
+
     # -- data access ---------------------------------------------------------
     def get(self, field: int) -> np.ndarray:
         w = FIELD_WIDTH[field]

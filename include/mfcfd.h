@@ -82,7 +82,9 @@ typedef struct mfcfd_params {
     int32_t sweep_mode;       /* MFCFD_SWEEP_CHAINS (default), _DATAFLOW or _LEVELS */
     int32_t update_variant;   /* MFCFD_UPDATE_IMPLICIT (default) or MFCFD_UPDATE_EXPLICIT */
     int32_t sweep_variant;    /* MFCFD_SWEEPS_ALIAS (default) or MFCFD_SWEEPS_BACKUP */
-    int32_t reserved[5];
+    int32_t chain_warps;      /* CHAINS: warps of the schedule; 0 picks about twice the
+                                 widest level (fewer warps leave SMs to other clouds) */
+    int32_t reserved[4];
 } mfcfd_params;
 
 /* The reference ships two drivers of its sweep module.  ALIAS:
@@ -167,6 +169,18 @@ int mfcfd_fpi_step(mfcfd_handle *h, int32_t t, double *res_new, double *residue)
  * round trips; res_hist (2*iters, may be NULL) receives (res_new, residue)
  * per iteration. */
 int mfcfd_run(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist);
+
+/*
+ * Batches: iterations t0[i] .. t0[i]+iters-1 of `count` handles of one device
+ * (each handle once), run concurrently -- every iteration of each handle is
+ * launched in turn on the handles' own streams, so one cloud's
+ * latency-bound sweeps overlap another's.  Handles whose chain-schedule
+ * sweeps would not all be resident together run in successive waves.
+ * res_hist (may be NULL) is count x iters x (res_new, residue); status (may
+ * be NULL) gets each handle's result; the return value is the first error.
+ */
+int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, int32_t iters,
+                    double *res_hist, int32_t *status);
 
 /* Copy a field to host memory (see MFCFD_FIELD_*). */
 int mfcfd_get(mfcfd_handle *h, int32_t field, double *out);
@@ -255,6 +269,20 @@ int mfcfd_print_primal_output(mfcfd_handle *h, const char *dir);
 /* residue.dat lines `t res_new residue` (q_lskum.f90:22,31) for
  * t = t0 .. t0+iters-1 from an mfcfd_run history; append != 0 appends. */
 int mfcfd_write_residue(const char *path, int32_t t0, int32_t iters, const double *res_hist, int32_t append);
+
+/*
+ * Aerodynamic coefficients of the current state (no counterpart in the
+ * reference, which prints no forces).  F = -sum over wall points of
+ * (p_i - p_inf) A_i nor_i, with A_i = wall_area / (number of wall points)
+ * unless per-point areas were set; CL = F.(-sin a, cos a, 0) / q and
+ * CD = F.(cos a, sin a, 0) / q with q = rho_inf V^2 ref_area / 2 and the
+ * angle a and speed V of (u1_inf, u2_inf).  force (3, may be NULL) receives F.
+ * The wall sum runs on the GPU in a fixed order.
+ */
+int mfcfd_forces(mfcfd_handle *h, double wall_area, double ref_area, double *cl, double *cd, double *force);
+/* Per-point areas A_i (N values; only wall points' are read) for
+ * mfcfd_forces; NULL returns to the uniform wall_area split. */
+int mfcfd_set_wall_areas(mfcfd_handle *h, const double *area);
 
 int mfcfd_destroy(mfcfd_handle *h);
 

@@ -138,3 +138,25 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def forces(cloud, prim, mach, aoa_deg, wall_area=None, ref_area=None):
+    """(CL, CD, F) of a state, summed over wall points in index order (the
+    project's force definition; the reference computes none):
+    F = -sum (p_i - p_inf) A_i nor_i with A_i = wall_area / n_wall."""
+    import math
+    from mfcfd.cloud import freestream
+    rho, u1, u2, u3, pr = freestream(mach, aoa_deg)
+    wa = cloud.wall_area if wall_area is None else wall_area
+    ra = cloud.ref_area if ref_area is None else ref_area
+    wall = np.nonzero(cloud.status == 1)[0]
+    each = wa / len(wall)
+    F = [0.0, 0.0, 0.0]
+    for i in wall:
+        dp = prim[i, 4] - pr
+        for r in range(3):
+            F[r] = F[r] - dp * each * cloud.nor[i, r]
+    v = math.sqrt(u1 * u1 + u2 * u2 + u3 * u3)
+    sa, ca = u2 / v, u1 / v
+    q = 0.5 * rho * v * v * ra
+    return (F[0] * (-sa) + F[1] * ca) / q, (F[0] * ca + F[1] * sa) / q, np.array(F)

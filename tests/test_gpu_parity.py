@@ -153,3 +153,44 @@ def test_backup_sweep_driver_bitexact(oracle_lib, mfcfd_lib, sweep_mode, superso
         assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
     dinv_g, dinv_o = s.get(mfcfd_lib.FIELD_DINV), o.get(oracle_lib.FIELD_DINV)
     assert np.array_equal(dinv_g[dinv_o != 0], dinv_o[dinv_o != 0])
+
+
+def test_forces_match_oracle(small_cloud, oracle_lib, mfcfd_lib):
+    """CL/CD of the state after 10 iterations against the oracle's state and a
+    sequential wall sum: within 1e-10 relative (the sums' order differs)."""
+    s, o = _pair(small_cloud, 0.8, 2.0, oracle_lib.LIBM_MFMATH, oracle_lib)
+    s.q_lskum(10)
+    for t in range(1, 11):
+        o.step(t)
+    cl, cd, f = s.forces()
+    clo, cdo, fo = oracle_lib.forces(small_cloud, o.get(oracle_lib.FIELD_PRIM), 0.8, 2.0)
+    assert abs(cl - clo) <= 1e-10 * abs(clo) and abs(cd - cdo) <= 1e-10 * abs(cdo)
+    np.testing.assert_allclose(f, fo, rtol=1e-10)
+
+
+@pytest.mark.parametrize("chain_warps", [0, 400])
+def test_batch_equals_separate_runs(oracle_lib, mfcfd_lib, chain_warps):
+    """mfcfd_run_batch over clouds of different sizes and flows gives each
+    cloud exactly its separate run (400 warps per cloud forces waves)."""
+    from mfcfd import batch, cloud
+    from mfcfd.solver import Solver
+    clouds = [cloud.small_sphere(6, 100, r1=1.5, seed=3), cloud.small_sphere(8, 150, seed=4),
+              cloud.with_supersonic_boundary(cloud.small_sphere(7, 120, r1=1.6, seed=5))]
+    flows = [(0.4, 0.0), (0.8, 2.0), (0.6, 1.0)]
+    sep, hsep = [], []
+    for c, (m, a) in zip(clouds, flows):
+        s = Solver(c, m, a, chain_warps=chain_warps)
+        s.initial_conditions()
+        hsep.append(s.q_lskum(5))
+        sep.append(s.get(mfcfd_lib.FIELD_PRIM))
+        s.close()
+    solvers = []
+    for c, (m, a) in zip(clouds, flows):
+        s = Solver(c, m, a, chain_warps=chain_warps)
+        s.initial_conditions()
+        solvers.append(s)
+    hist = batch.run_batch(solvers, 5)
+    for i, s in enumerate(solvers):
+        assert np.array_equal(hist[i], hsep[i])
+        assert np.array_equal(s.get(mfcfd_lib.FIELD_PRIM), sep[i])
+        s.close()
