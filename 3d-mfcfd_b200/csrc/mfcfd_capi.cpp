@@ -244,8 +244,13 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         *out = h;
         return MFCFD_ERR_ARG;
     }
-    if (P.precision != MFCFD_PRECISION_FP64) {
-        h->err = "only FP64 is implemented";
+    if (P.precision != MFCFD_PRECISION_FP64 && P.precision != MFCFD_PRECISION_MIXED) {
+        h->err = "unknown precision";
+        *out = h;
+        return MFCFD_ERR_UNSUPPORTED;
+    }
+    if (P.precision == MFCFD_PRECISION_MIXED && P.sweep_mode != MFCFD_SWEEP_CHAINS) {
+        h->err = "mixed precision requires the chain sweep schedule";
         *out = h;
         return MFCFD_ERR_UNSUPPORTED;
     }
@@ -353,6 +358,7 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.n_swept = (int)T.fwd_lvl_pts.size();
     d.max_width = T.max_level_width;
     d.sweep_mode = P.sweep_mode;
+    d.precision = P.precision;
     if ((rc = dalloc(h, &d.sweep_counter, 2))) return rc;
     if ((rc = dalloc(h, &d.err, 1))) return rc;
     CK(cudaMemsetAsync(d.sweep_counter, 0, sizeof(int) * 2, h->stream));

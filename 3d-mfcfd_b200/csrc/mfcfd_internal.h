@@ -195,6 +195,7 @@ struct DevCloud {
     int n_swept;                  // points in each sweep order
     int max_width;                // widest sweep level
     int sweep_mode;               // MFCFD_SWEEP_*
+    int precision;                // MFCFD_PRECISION_*
     int *sweep_counter;           // 2 work counters (forward, backward)
     int *err;                     // set when a bounded poll gave up
     // chain schedule (per direction: 0 forward, 1 backward)

