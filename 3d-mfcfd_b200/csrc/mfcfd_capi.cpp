@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -40,6 +41,15 @@ struct mfcfd_handle {
     int64_t chain_terms[3] = {0, 0, 0};   // chain schedule: ring, same-warp, cross-warp terms
     double *wall_area = nullptr;           // per-point areas for mfcfd_forces (device), or null
     double *force_out = nullptr;           // 3 doubles (device)
+    // host copies held between mfcfd_prepare and mfcfd_attach
+    struct Staged {
+        std::vector<double> x, y, z, frame;
+        std::vector<int32_t> nbhs, conn, pre;
+        ChainSchedule S;
+        int ch_w = 0, ch_wpb = 0;
+    };
+    std::unique_ptr<Staged> staged;
+    bool dry = false;                      // count device bytes, allocate and copy nothing
 };
 
 namespace {
@@ -47,7 +57,7 @@ namespace {
 const char *kStrerr[] = {"ok", "bad argument", "CUDA error", "stencil too wide",
                          "singular least-squares system", "non-finite residual",
                          "unsupported input", "out of device memory", "device wait timed out",
-                         "file input/output error"};
+                         "file input/output error", "request not finished"};
 
 int fail(mfcfd_handle *h, int code, const std::string &msg) {
     if (h) h->err = msg;
@@ -68,6 +78,11 @@ int cuda_fail(mfcfd_handle *h, cudaError_t e, const char *what) {
 template <typename T>
 int dalloc(mfcfd_handle *h, T **p, size_t count) {
     size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+    if (h->dry) {
+        h->bytes += (int64_t)bytes;
+        *p = nullptr;
+        return MFCFD_OK;
+    }
     void *v = nullptr;
     cudaError_t e = cudaMalloc(&v, bytes);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
@@ -82,7 +97,7 @@ int upload(mfcfd_handle *h, const T **dst, const std::vector<T> &src) {
     T *p = nullptr;
     int rc = dalloc(h, &p, src.size());
     if (rc) return rc;
-    if (!src.empty()) CK(cudaMemcpyAsync(p, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, h->stream));
+    if (!src.empty() && !h->dry) CK(cudaMemcpyAsync(p, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, h->stream));
     *dst = p;
     return MFCFD_OK;
 }
@@ -189,6 +204,14 @@ int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist)
 
 }  // namespace
 
+namespace {
+
+int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *z, const double *tan1,
+               const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn);
+int attach_device(mfcfd_handle *h);
+
+}  // namespace
+
 extern "C" {
 
 void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg) {
@@ -211,10 +234,16 @@ void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg) {
     p->sweep_mode = MFCFD_SWEEP_CHAINS;
 }
 
-int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, const double *x,
-                 const double *y, const double *z, const double *tan1, const double *tan2,
-                 const double *nor, const int32_t *nbhs, const int32_t *conn,
-                 const double *min_dist, mfcfd_handle **out) {
+}  // extern "C"
+
+namespace {
+
+// mfcfd_create and mfcfd_prepare: validation and the host set-up; with
+// `attach`, also the device copy.
+int create_impl(const mfcfd_params *params, int32_t n, const int32_t *status, const double *x,
+                const double *y, const double *z, const double *tan1, const double *tan2,
+                const double *nor, const int32_t *nbhs, const int32_t *conn,
+                const double *min_dist, mfcfd_handle **out, bool attach) {
     if (!out) return MFCFD_ERR_ARG;
     *out = nullptr;
     if (!params || n < 1 || !status || !x || !y || !z || !tan1 || !tan2 || !nor || !nbhs ||
@@ -268,11 +297,61 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     int rc = build_topology(P, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, h->T, h->err);
     *out = h;
     if (rc) return rc;
-    const Topology &T = h->T;
     if (P.device < 0) return MFCFD_OK;   // host-only handle: set-up results, no device state
+    if ((rc = stage_host(h, x, y, z, tan1, tan2, nor, nbhs, conn))) return rc;
+    if (attach) {
+        if ((rc = attach_device(h))) return rc;
+        h->staged.reset();
+    }
+    return MFCFD_OK;
+}
 
+// Host copies of the inputs the device needs, in the device layout, and the
+// chain schedule (the kernel's residency on P.device sets its warp count).
+int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *z, const double *tan1,
+               const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn) {
+    const mfcfd_params &P = h->P;
+    const int n = h->T.n;
     if (cudaSetDevice(P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
-    {
+    auto st = std::make_unique<mfcfd_handle::Staged>();
+    st->x.assign(x, x + n);
+    st->y.assign(y, y + n);
+    st->z.assign(z, z + n);
+    st->frame.resize((size_t)n * 9);
+    for (int i = 0; i < n; ++i)
+        for (int r = 0; r < 3; ++r) {
+            st->frame[9 * (size_t)i + r] = tan1[3 * (size_t)i + r];
+            st->frame[9 * (size_t)i + 3 + r] = tan2[3 * (size_t)i + r];
+            st->frame[9 * (size_t)i + 6 + r] = nor[3 * (size_t)i + r];
+        }
+    st->nbhs.assign(nbhs, nbhs + n);
+    st->conn.assign((size_t)n * MAX_CONN, 0);
+    for (size_t j = 0; j < st->conn.size(); ++j) st->conn[j] = conn[j] > 0 ? conn[j] - 1 : 0;
+    if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+        // about twice the widest level in warps, all co-resident; the
+        // schedule also marks the entry lists, so it precedes their upload
+        if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
+        const int want = P.chain_warps > 0 ? P.chain_warps : 2 * h->T.max_level_width;
+        int blocks = 0;
+        st->ch_w = chain_shape(P.device, want, &st->ch_wpb, &blocks);
+        if (st->ch_w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+        build_chain_schedule(h->T, st->ch_w, st->S);
+        build_pre_order(h->T, st->pre);
+    }
+    h->staged = std::move(st);
+    return MFCFD_OK;
+}
+
+// Streams, device arrays and uploads from the staged copies (with h->dry:
+// only the byte count).
+int attach_device(mfcfd_handle *h) {
+    const mfcfd_params &P = h->P;
+    const Topology &T = h->T;
+    const mfcfd_handle::Staged &st = *h->staged;
+    const int n = T.n;
+    int rc = MFCFD_OK;
+    if (!h->dry) {
+        if (cudaSetDevice(P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
         // the main stream outranks the side stream, so the chain sweep's
         // blocks are placed before the concurrent flux kernel's
         int least = 0, greatest = 0;
@@ -296,31 +375,11 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.rho_inf = P.rho_inf; d.u1_inf = P.u1_inf; d.u2_inf = P.u2_inf;
     d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;
 
-    std::vector<double> vx(x, x + n), vy(y, y + n), vz(z, z + n);
-    std::vector<double> frame((size_t)n * 9);
-    for (int i = 0; i < n; ++i)
-        for (int r = 0; r < 3; ++r) {
-            frame[9 * (size_t)i + r] = tan1[3 * (size_t)i + r];
-            frame[9 * (size_t)i + 3 + r] = tan2[3 * (size_t)i + r];
-            frame[9 * (size_t)i + 6 + r] = nor[3 * (size_t)i + r];
-        }
-    std::vector<int32_t> vnb(nbhs, nbhs + n), vconn((size_t)n * MAX_CONN, 0);
-    for (size_t j = 0; j < vconn.size(); ++j) vconn[j] = conn[j] > 0 ? conn[j] - 1 : 0;
-    // chain schedule first: it marks the entry lists before they are uploaded
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
-        // about twice the widest level in warps, all co-resident
-        int wpb = 0, blocks = 0;
-        if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
-        const int want = P.chain_warps > 0 ? P.chain_warps : 2 * T.max_level_width;
-        const int w = chain_shape(P.device, want, &wpb, &blocks);
-        if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
-        ChainSchedule S;
-        build_chain_schedule(h->T, w, S);
-        d.ch_warps = w;
-        d.ch_wpb = wpb;
-        std::vector<int32_t> pre;
-        build_pre_order(T, pre);
-        if ((rc = upload(h, &d.pre_order, pre))) return rc;
+        const ChainSchedule &S = st.S;
+        d.ch_warps = st.ch_w;
+        d.ch_wpb = st.ch_wpb;
+        if ((rc = upload(h, &d.pre_order, st.pre))) return rc;
         for (int dir = 0; dir < 2; ++dir) {
             if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;
             if ((rc = upload(h, &d.ch_pts[dir], S.pts[dir]))) return rc;
@@ -335,8 +394,8 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     order.insert(order.end(), T.wall_idx.begin(), T.wall_idx.end());
     order.insert(order.end(), T.interior_idx.begin(), T.interior_idx.end());
 #define UP(field, vec) if ((rc = upload(h, &d.field, vec))) return rc
-    UP(x, vx); UP(y, vy); UP(z, vz); UP(frame, frame);
-    UP(cls, T.cls); UP(nbhs, vnb); UP(conn, vconn); UP(eps2, T.eps2);
+    UP(x, st.x); UP(y, st.y); UP(z, st.z); UP(frame, st.frame);
+    UP(cls, T.cls); UP(nbhs, st.nbhs); UP(conn, st.conn); UP(eps2, T.eps2);
     UP(slot_nbr, T.slot_nbr); UP(nslot, T.nslot); UP(slot_mask, T.slot_mask);
     UP(list_cnt, T.list_cnt); UP(list_ent, T.list_ent); UP(geo, T.geo);
     if (!T.wq.empty()) { UP(wq, T.wq); UP(wf, T.wf); }
@@ -361,8 +420,6 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
     d.precision = P.precision;
     if ((rc = dalloc(h, &d.sweep_counter, 2))) return rc;
     if ((rc = dalloc(h, &d.err, 1))) return rc;
-    CK(cudaMemsetAsync(d.sweep_counter, 0, sizeof(int) * 2, h->stream));
-    CK(cudaMemsetAsync(d.err, 0, sizeof(int), h->stream));
     size_t n5 = (size_t)n * 5;
 #define AL(ptr, cnt) if ((rc = dalloc(h, &ptr, cnt))) return rc
     AL(d.prim, n5); AL(h->U_buf[0], n5); AL(h->U_buf[1], n5); AL(h->q_buf[0], n5);
@@ -379,14 +436,70 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
         if ((rc = upload(h, &d.ss_src, T.ss_src))) return rc;
     }
 #undef AL
+    d.U = h->U_buf[0];
+    d.q = h->q_buf[0];
+    if (h->dry) return MFCFD_OK;
+    CK(cudaMemsetAsync(d.sweep_counter, 0, sizeof(int) * 2, h->stream));
+    CK(cudaMemsetAsync(d.err, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(d.dUp, 0, n5 * 8, h->stream));
     CK(cudaMemsetAsync(d.dUn, 0, n5 * 8, h->stream));
     CK(cudaMemsetAsync(d.flux_res, 0, n5 * 8, h->stream));
     CK(cudaMemsetAsync(d.dinv, 0, (size_t)n * 8, h->stream));
     CK(cudaMemsetAsync(d.res_sqr, 0, (size_t)n * 8, h->stream));
-    d.U = h->U_buf[0];
-    d.q = h->q_buf[0];
     CK(cudaStreamSynchronize(h->stream));
+    return MFCFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, const double *x,
+                 const double *y, const double *z, const double *tan1, const double *tan2,
+                 const double *nor, const int32_t *nbhs, const int32_t *conn,
+                 const double *min_dist, mfcfd_handle **out) {
+    return create_impl(params, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, out, true);
+}
+
+int mfcfd_prepare(const mfcfd_params *params, int32_t n, const int32_t *status, const double *x,
+                  const double *y, const double *z, const double *tan1, const double *tan2,
+                  const double *nor, const int32_t *nbhs, const int32_t *conn,
+                  const double *min_dist, mfcfd_handle **out) {
+    if (!out) return MFCFD_ERR_ARG;
+    *out = nullptr;
+    if (!params || params->device < 0) return MFCFD_ERR_ARG;
+    return create_impl(params, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, out, false);
+}
+
+int mfcfd_device_bytes(mfcfd_handle *h, int64_t *bytes) {
+    if (!h || !bytes) return MFCFD_ERR_ARG;
+    if (h->stream) {
+        *bytes = h->bytes;
+        return MFCFD_OK;
+    }
+    if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no staged cloud");
+    // the attach sequence with allocation counted, not performed
+    h->dry = true;
+    h->bytes = 0;
+    const int rc = attach_device(h);
+    *bytes = h->bytes;
+    h->dry = false;
+    h->bytes = 0;
+    std::memset(&h->d, 0, sizeof h->d);
+    h->allocs.clear();
+    return rc;
+}
+
+int mfcfd_attach(mfcfd_handle *h) {
+    if (!h) return MFCFD_ERR_ARG;
+    if (h->stream) return MFCFD_OK;
+    if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no staged cloud");
+    const int rc = attach_device(h);
+    if (rc) {
+        release(h);
+        return rc;
+    }
+    h->staged.reset();
     return MFCFD_OK;
 }
 
@@ -678,7 +791,7 @@ const char *mfcfd_last_error(const mfcfd_handle *h) {
 }
 
 const char *mfcfd_strerror(int code) {
-    if (code < 0 || code > MFCFD_ERR_IO) return "unknown error";
+    if (code < 0 || code > MFCFD_ERR_BUSY) return "unknown error";
     return kStrerr[code];
 }
 

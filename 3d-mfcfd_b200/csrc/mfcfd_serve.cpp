@@ -1,0 +1,356 @@
+/*
+ * mfcfd_serve.cpp - the request server of include/mfcfd.h (continuous
+ * batching of steady-state solves on one GPU), built on the public C ABI.
+ *
+ * Threads: `setup_threads` workers run the host set-up of submitted clouds
+ * (mfcfd_prepare) and measure their device footprint (mfcfd_device_bytes);
+ * one scheduler thread owns the device side.  Each scheduler round admits
+ * ready requests (first ready, first admitted) while their bytes fit the
+ * budget beside the live ones, runs `chunk` iterations of every live request
+ * with mfcfd_run_batch (their streams overlap on the device), and retires
+ * the requests that converged, reached max_iters or failed, which frees
+ * their memory for the next round's admissions.  Every request iterates in
+ * whole rounds of `chunk` from t = 1, so its arithmetic, and its result, do
+ * not depend on which other requests share the device.
+ */
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "mfcfd_internal.h"
+
+namespace {
+
+struct Request {
+    int64_t id = 0;
+    mfcfd_params P{};
+    int32_t n = 0;
+    std::vector<int32_t> status, nbhs, conn;
+    std::vector<double> x, y, z, tan1, tan2, nor, min_dist, prim0;
+    int32_t max_iters = 0;
+    double target = 0.0, wall_area = 0.0, ref_area = 0.0;
+    mfcfd_handle *h = nullptr;
+    int64_t bytes = 0;
+    int32_t t = 1;                    // next iteration number
+    mfcfd_result res{};
+    std::vector<double> prim_out;
+    std::string err;
+    bool done = false;
+};
+using RequestPtr = std::shared_ptr<Request>;
+
+}  // namespace
+
+struct mfcfd_server {
+    mfcfd_server_config cfg{};
+    std::chrono::steady_clock::time_point t0;
+    std::mutex mu;
+    std::condition_variable cv_setup, cv_sched, cv_done;
+    std::deque<RequestPtr> to_prepare;   // submitted, not yet taken by a worker
+    std::deque<RequestPtr> ready;        // prepared, in the order they became ready
+    std::map<int64_t, RequestPtr> all;   // every request not yet returned by wait
+    std::vector<RequestPtr> live;        // scheduler thread only
+    int64_t next_id = 1;
+    int64_t preparing = 0, n_live = 0;
+    bool stopping = false;
+    mfcfd_server_stats st{};
+    std::vector<std::thread> workers;
+    std::thread scheduler;
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    // Bookkeeping of a retired request (caller holds mu).
+    void finish_locked(const RequestPtr &r, int status) {
+        r->res.status = status;
+        r->res.t_done = now();
+        r->done = true;
+        if (status == MFCFD_OK) ++st.completed;
+        else ++st.failed;
+        cv_done.notify_all();
+    }
+
+    void worker_loop();
+    void scheduler_loop();
+    void retire(const RequestPtr &r, int status);
+};
+
+void mfcfd_server::worker_loop() {
+    for (;;) {
+        RequestPtr r;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_setup.wait(lk, [&] { return stopping || !to_prepare.empty(); });
+            if (stopping) return;
+            r = to_prepare.front();
+            to_prepare.pop_front();
+            ++preparing;
+        }
+        mfcfd_params P = r->P;
+        P.device = cfg.device;
+        mfcfd_handle *h = nullptr;
+        int rc = mfcfd_prepare(&P, r->n, r->status.data(), r->x.data(), r->y.data(), r->z.data(), r->tan1.data(),
+                               r->tan2.data(), r->nor.data(), r->nbhs.data(), r->conn.data(), r->min_dist.data(),
+                               &h);
+        int64_t bytes = 0;
+        if (!rc) rc = mfcfd_device_bytes(h, &bytes);
+        if (rc && h) r->err = mfcfd_last_error(h);
+        // the handle holds what the device needs; the request keeps prim0
+        std::vector<int32_t>().swap(r->status);
+        std::vector<int32_t>().swap(r->nbhs);
+        std::vector<int32_t>().swap(r->conn);
+        for (auto *v : {&r->x, &r->y, &r->z, &r->tan1, &r->tan2, &r->nor, &r->min_dist})
+            std::vector<double>().swap(*v);
+        if (!rc && bytes > cfg.hbm_budget) {
+            rc = MFCFD_ERR_NOMEM;
+            r->err = "the request needs more device memory than the server's budget";
+        }
+        if (rc && h) {
+            mfcfd_destroy(h);
+            h = nullptr;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        --preparing;
+        r->res.t_ready = now();
+        r->res.device_bytes = bytes;
+        if (rc) {
+            finish_locked(r, rc);
+        } else {
+            r->h = h;
+            r->bytes = bytes;
+            ready.push_back(r);
+            cv_sched.notify_one();
+        }
+    }
+}
+
+// Copy out the state and forces of a live request, free its device memory
+// and record the result (scheduler thread).
+void mfcfd_server::retire(const RequestPtr &r, int status) {
+    if (r->h) {
+        if (status == MFCFD_OK && r->wall_area > 0.0 && r->ref_area > 0.0) {
+            const int rc = mfcfd_forces(r->h, r->wall_area, r->ref_area, &r->res.cl, &r->res.cd, nullptr);
+            if (rc) status = rc;
+        }
+        if (status == MFCFD_OK) {
+            r->prim_out.resize((size_t)r->n * 5);
+            const int rc = mfcfd_get(r->h, MFCFD_FIELD_PRIM, r->prim_out.data());
+            if (rc) status = rc;
+        }
+        if (status != MFCFD_OK && r->err.empty()) r->err = mfcfd_last_error(r->h);
+        mfcfd_destroy(r->h);
+        r->h = nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    st.bytes_live -= r->bytes;
+    --n_live;
+    finish_locked(r, status);
+}
+
+void mfcfd_server::scheduler_loop() {
+    cudaSetDevice(cfg.device);
+    const int chunk = cfg.chunk;
+    for (;;) {
+        std::vector<RequestPtr> admit;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (live.empty()) cv_sched.wait(lk, [&] { return stopping || !ready.empty(); });
+            if (stopping) break;
+            int64_t bytes = st.bytes_live;
+            while (!ready.empty()) {
+                const RequestPtr &r = ready.front();
+                if (cfg.max_live > 0 && (int64_t)(live.size() + admit.size()) >= cfg.max_live) break;
+                if (bytes + r->bytes > cfg.hbm_budget) break;
+                bytes += r->bytes;
+                admit.push_back(r);
+                ready.pop_front();
+            }
+            st.bytes_live = bytes;
+            n_live += (int64_t)admit.size();
+            st.peak_bytes_live = std::max(st.peak_bytes_live, st.bytes_live);
+            st.peak_live = std::max(st.peak_live, n_live);
+        }
+        for (const RequestPtr &r : admit) {
+            int rc = mfcfd_attach(r->h);
+            if (!rc) {
+                rc = mfcfd_set_prim(r->h, r->prim0.data());
+                std::vector<double>().swap(r->prim0);
+            }
+            r->res.t_admit = now();
+            if (rc) retire(r, rc);
+            else live.push_back(r);
+        }
+        if (live.empty()) continue;
+
+        // one round: `chunk` iterations of every live request, overlapped
+        const int32_t count = (int32_t)live.size();
+        std::vector<mfcfd_handle *> hs(count);
+        std::vector<int32_t> t0s(count), status(count, MFCFD_OK);
+        std::vector<double> hist(2 * (size_t)chunk * count);
+        for (int32_t i = 0; i < count; ++i) {
+            hs[i] = live[i]->h;
+            t0s[i] = live[i]->t;
+        }
+        const int rc = mfcfd_run_batch(hs.data(), count, t0s.data(), chunk, hist.data(), status.data());
+        const bool per_request = std::any_of(status.begin(), status.end(), [](int v) { return v != MFCFD_OK; });
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            ++st.rounds;
+            st.iterations += (int64_t)chunk * count;
+        }
+        std::vector<RequestPtr> keep;
+        for (int32_t i = 0; i < count; ++i) {
+            const RequestPtr &r = live[i];
+            int s = status[i];
+            if (rc != MFCFD_OK && !per_request) s = rc;   // a launch failed mid-round: all are suspect
+            r->t += chunk;
+            r->res.iters += chunk;
+            const double *last = &hist[2 * ((size_t)i * chunk + chunk - 1)];
+            r->res.res_new = last[0];
+            r->res.residue = last[1];
+            r->res.converged = s == MFCFD_OK && r->t - 1 > 2 && last[1] <= r->target;
+            if (s != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) retire(r, s);
+            else keep.push_back(r);
+        }
+        live.swap(keep);
+    }
+    // stopping: live requests end with their last round
+    for (const RequestPtr &r : live) retire(r, MFCFD_ERR_BUSY);
+    live.clear();
+}
+
+extern "C" {
+
+int mfcfd_server_create(const mfcfd_server_config *cfg, mfcfd_server **out) {
+    if (!out) return MFCFD_ERR_ARG;
+    *out = nullptr;
+    if (!cfg || cfg->device < 0 || cfg->max_live < 0 || cfg->setup_threads < 1 || cfg->setup_threads > 64 ||
+        cfg->chunk < 1 || cfg->chunk > 1024 || cfg->hbm_budget < 0)
+        return MFCFD_ERR_ARG;
+    if (cudaSetDevice(cfg->device) != cudaSuccess) return MFCFD_ERR_CUDA;
+    auto *s = new (std::nothrow) mfcfd_server();
+    if (!s) return MFCFD_ERR_NOMEM;
+    s->cfg = *cfg;
+    if (s->cfg.hbm_budget == 0) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            delete s;
+            return MFCFD_ERR_CUDA;
+        }
+        s->cfg.hbm_budget = (int64_t)(0.9 * (double)free_b);
+    }
+    s->st.hbm_budget = s->cfg.hbm_budget;
+    s->t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < cfg->setup_threads; ++i) s->workers.emplace_back([s] { s->worker_loop(); });
+    s->scheduler = std::thread([s] { s->scheduler_loop(); });
+    *out = s;
+    return MFCFD_OK;
+}
+
+int mfcfd_server_submit(mfcfd_server *s, const mfcfd_request *q, int64_t *id) {
+    if (!s || !q || !id || q->n < 1 || !q->status || !q->x || !q->y || !q->z || !q->tan1 || !q->tan2 ||
+        !q->nor || !q->nbhs || !q->conn || !q->min_dist || q->max_iters < 1)
+        return MFCFD_ERR_ARG;
+    auto r = std::make_shared<Request>();
+    const size_t n = (size_t)q->n;
+    r->P = q->params;
+    r->n = q->n;
+    r->status.assign(q->status, q->status + n);
+    r->nbhs.assign(q->nbhs, q->nbhs + n);
+    r->conn.assign(q->conn, q->conn + n * mfcfd::MAX_CONN);
+    r->x.assign(q->x, q->x + n);
+    r->y.assign(q->y, q->y + n);
+    r->z.assign(q->z, q->z + n);
+    r->tan1.assign(q->tan1, q->tan1 + 3 * n);
+    r->tan2.assign(q->tan2, q->tan2 + 3 * n);
+    r->nor.assign(q->nor, q->nor + 3 * n);
+    r->min_dist.assign(q->min_dist, q->min_dist + n);
+    if (q->prim) {
+        r->prim0.assign(q->prim, q->prim + 5 * n);
+    } else {
+        // impulsive start: the freestream, without its normal component at
+        // wall points (a uniform freestream is a fixed point of the scheme)
+        const mfcfd_params &P = q->params;
+        r->prim0.resize(5 * n);
+        for (size_t i = 0; i < n; ++i) {
+            double *p = &r->prim0[5 * i];
+            p[0] = P.rho_inf; p[1] = P.u1_inf; p[2] = P.u2_inf; p[3] = P.u3_inf; p[4] = P.pr_inf;
+            if (q->status[i] == 1) {
+                const double *nr = q->nor + 3 * i;
+                const double un = p[1] * nr[0] + p[2] * nr[1] + p[3] * nr[2];
+                for (int k = 0; k < 3; ++k) p[1 + k] = p[1 + k] - un * nr[k];
+            }
+        }
+    }
+    const int32_t c = s->cfg.chunk;
+    r->max_iters = (q->max_iters + c - 1) / c * c;
+    r->target = q->residue_target;
+    r->wall_area = q->wall_area;
+    r->ref_area = q->ref_area;
+    r->res.n = q->n;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) return MFCFD_ERR_ARG;
+    r->id = s->next_id++;
+    r->res.id = r->id;
+    r->res.t_submit = s->now();
+    s->all[r->id] = r;
+    s->to_prepare.push_back(r);
+    ++s->st.submitted;
+    s->cv_setup.notify_one();
+    *id = r->id;
+    return MFCFD_OK;
+}
+
+int mfcfd_server_wait(mfcfd_server *s, int64_t id, double timeout_s, mfcfd_result *res, double *prim) {
+    if (!s || !res) return MFCFD_ERR_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return MFCFD_ERR_ARG;
+    RequestPtr r = it->second;
+    auto pred = [&] { return r->done; };
+    if (timeout_s < 0) s->cv_done.wait(lk, pred);
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) return MFCFD_ERR_BUSY;
+    *res = r->res;
+    if (prim && !r->prim_out.empty()) std::memcpy(prim, r->prim_out.data(), sizeof(double) * r->prim_out.size());
+    s->all.erase(id);
+    return MFCFD_OK;
+}
+
+int mfcfd_server_get_stats(mfcfd_server *s, mfcfd_server_stats *st) {
+    if (!s || !st) return MFCFD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *st = s->st;
+    st->preparing = s->preparing + (int64_t)s->to_prepare.size();
+    st->waiting = (int64_t)s->ready.size();
+    st->live = s->n_live;
+    return MFCFD_OK;
+}
+
+int mfcfd_server_destroy(mfcfd_server *s) {
+    if (!s) return MFCFD_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+    }
+    s->cv_setup.notify_all();
+    s->cv_sched.notify_all();
+    for (std::thread &w : s->workers) w.join();
+    s->scheduler.join();
+    for (const RequestPtr &r : s->ready)
+        if (r->h) mfcfd_destroy(r->h);
+    delete s;
+    return MFCFD_OK;
+}
+
+}  // extern "C"

@@ -11,7 +11,7 @@ MFCFD_OK = 0
 ERRORS = {1: "bad argument", 2: "CUDA error", 3: "stencil too wide",
           4: "singular least-squares system", 5: "non-finite residual",
           6: "unsupported input", 7: "out of device memory", 8: "device wait timed out",
-          9: "file input/output error"}
+          9: "file input/output error", 10: "request not finished"}
 
 FIELD_PRIM, FIELD_U, FIELD_Q, FIELD_QM, FIELD_DQ, FIELD_DELT, FIELD_FLUX_RES, \
     FIELD_DELUP, FIELD_DELUN, FIELD_DINV = range(10)
@@ -27,6 +27,9 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_residual_noalloc", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
            "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch",
+           "mfcfd_prepare", "mfcfd_device_bytes", "mfcfd_attach",
+           "mfcfd_server_create", "mfcfd_server_submit", "mfcfd_server_wait",
+           "mfcfd_server_get_stats", "mfcfd_server_destroy",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
 NOALLOC_MAX_TERMS = 1024 * 4096
 NPHASE = 7
@@ -67,6 +70,37 @@ class Info(ctypes.Structure):
                 ("device_bytes", ctypes.c_int64), ("sweep_mode", ctypes.c_int32),
                 ("chain_warps", ctypes.c_int32), ("chain_terms_ring", ctypes.c_int64),
                 ("chain_terms_local", ctypes.c_int64), ("chain_terms_cross", ctypes.c_int64)]
+
+
+class ServerConfig(ctypes.Structure):
+    """mfcfd_server_config (include/mfcfd.h)."""
+    _fields_ = [("device", ctypes.c_int32), ("max_live", ctypes.c_int32),
+                ("setup_threads", ctypes.c_int32), ("chunk", ctypes.c_int32),
+                ("hbm_budget", ctypes.c_int64), ("reserved", ctypes.c_int32 * 8)]
+
+
+class Request(ctypes.Structure):
+    """mfcfd_request (include/mfcfd.h)."""
+    _fields_ = [("params", Params), ("n", ctypes.c_int32)] + \
+        [(f, ctypes.c_void_p) for f in ("status", "x", "y", "z", "tan1", "tan2", "nor", "nbhs",
+                                        "conn", "min_dist", "prim")] + \
+        [("max_iters", ctypes.c_int32), ("residue_target", ctypes.c_double),
+         ("wall_area", ctypes.c_double), ("ref_area", ctypes.c_double)]
+
+
+class Result(ctypes.Structure):
+    """mfcfd_result (include/mfcfd.h)."""
+    _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("iters", ctypes.c_int32), ("n", ctypes.c_int32)] + \
+        [(f, ctypes.c_double) for f in ("res_new", "residue", "cl", "cd", "t_submit", "t_ready",
+                                        "t_admit", "t_done")] + [("device_bytes", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    """mfcfd_server_stats (include/mfcfd.h)."""
+    _fields_ = [(f, ctypes.c_int64) for f in (
+        "submitted", "completed", "failed", "preparing", "waiting", "live", "bytes_live",
+        "peak_bytes_live", "hbm_budget", "rounds", "iterations", "peak_live")]
 
 
 class MfcfdError(RuntimeError):
@@ -114,6 +148,14 @@ def lib():
     L.mfcfd_forces.argtypes = [vp, dbl, dbl, vp, vp, vp]
     L.mfcfd_set_wall_areas.argtypes = [vp, vp]
     L.mfcfd_run_batch.argtypes = [vp, i32, vp, i32, vp, vp]
+    L.mfcfd_prepare.argtypes = [ctypes.POINTER(Params), i32] + [vp] * 10 + [ctypes.POINTER(vp)]
+    L.mfcfd_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
+    L.mfcfd_attach.argtypes = [vp]
+    L.mfcfd_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+    L.mfcfd_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]
+    L.mfcfd_server_wait.argtypes = [vp, ctypes.c_int64, dbl, ctypes.POINTER(Result), vp]
+    L.mfcfd_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.mfcfd_server_destroy.argtypes = [vp]
     L.mfcfd_destroy.argtypes = [vp]
     L.mfcfd_last_error.argtypes = [vp]
     L.mfcfd_last_error.restype = ctypes.c_char_p

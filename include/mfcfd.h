@@ -46,6 +46,7 @@ extern "C" {
 #define MFCFD_ERR_NOMEM        7   /* device allocation failed */
 #define MFCFD_ERR_TIMEOUT      8   /* a bounded device wait ran out */
 #define MFCFD_ERR_IO           9   /* a file could not be read, parsed or written */
+#define MFCFD_ERR_BUSY        10   /* a served request did not finish within the wait */
 
 /* fields for mfcfd_get (Fortran layout, width x N) */
 #define MFCFD_FIELD_PRIM      0    /* point%prim(5,N)        width 5  */
@@ -162,6 +163,23 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status,
                  const double *tan1, const double *tan2, const double *nor,
                  const int32_t *nbhs, const int32_t *conn, const double *min_dist,
                  mfcfd_handle **out);
+
+/*
+ * mfcfd_create in two steps, for a host that prepares clouds while others
+ * iterate (the request server below).  mfcfd_prepare does the host set-up
+ * (stencils, alias, levels, the chain schedule for params->device, which
+ * must be >= 0) and keeps host copies; mfcfd_device_bytes gives the device
+ * memory that mfcfd_attach will allocate (or holds, once attached);
+ * mfcfd_attach allocates and uploads.  Until attached, only the set-up
+ * queries (stencils, alias, levels, info) and mfcfd_destroy apply.
+ */
+int mfcfd_prepare(const mfcfd_params *params, int32_t n, const int32_t *status,
+                  const double *x, const double *y, const double *z,
+                  const double *tan1, const double *tan2, const double *nor,
+                  const int32_t *nbhs, const int32_t *conn, const double *min_dist,
+                  mfcfd_handle **out);
+int mfcfd_device_bytes(mfcfd_handle *h, int64_t *bytes);
+int mfcfd_attach(mfcfd_handle *h);
 
 /* Set point%prim (5,N) and zero delUp/delUn: initial_conditions.f90:18-29. */
 int mfcfd_set_prim(mfcfd_handle *h, const double *prim);
@@ -296,6 +314,76 @@ int mfcfd_destroy(mfcfd_handle *h);
  * last failed handle-less call (file functions). */
 const char *mfcfd_last_error(const mfcfd_handle *h);
 const char *mfcfd_strerror(int code);
+
+/*
+ * Request server: steady-state solves (cloud, Mach, angle of attack) served
+ * with continuous batching on one GPU (no counterpart in the reference,
+ * whose program runs one solve).  Submitted requests are prepared on host
+ * threads (mfcfd_prepare), admitted in the order they become ready while
+ * their device memory fits the budget (and live < max_live), then iterate
+ * together: every round runs `chunk` iterations of each live request
+ * (mfcfd_run_batch), after which a request whose residue is <= its
+ * residue_target, or that reached max_iters, or that failed, is retired:
+ * its CL/CD are computed, its state copied out and its device memory freed
+ * for the next admission.  A request's iterations do not depend on the
+ * others in the mix: the same request alone gives the same bits.
+ */
+typedef struct mfcfd_server mfcfd_server;
+
+typedef struct mfcfd_server_config {
+    int32_t device;           /* CUDA device ordinal */
+    int32_t max_live;         /* requests iterating at once; 0: memory is the only limit */
+    int32_t setup_threads;    /* host threads preparing submitted clouds (1..64) */
+    int32_t chunk;            /* iterations per live request per round (1..1024) */
+    int64_t hbm_budget;       /* device bytes the live requests may hold; 0: 90% of free memory */
+    int32_t reserved[8];
+} mfcfd_server_config;
+
+typedef struct mfcfd_request {
+    mfcfd_params params;      /* flow, precision, schedule; device is the server's */
+    int32_t n;                /* the cloud, as mfcfd_create takes it (copied at submit) */
+    const int32_t *status;
+    const double *x, *y, *z, *tan1, *tan2, *nor;
+    const int32_t *nbhs, *conn;
+    const double *min_dist;
+    const double *prim;       /* (5,N) initial state; NULL: the freestream of params with
+                                 the normal velocity removed at wall points */
+    int32_t max_iters;        /* upper bound, rounded up to a multiple of chunk */
+    double residue_target;    /* converged when residue <= this after a round */
+    double wall_area, ref_area;   /* CL/CD at retirement when both are > 0 */
+} mfcfd_request;
+
+typedef struct mfcfd_result {
+    int64_t id;
+    int32_t status;           /* MFCFD_OK or the code that retired the request */
+    int32_t converged;        /* residue reached residue_target */
+    int32_t iters;            /* iterations run */
+    int32_t n;
+    double res_new, residue;  /* after the last iteration */
+    double cl, cd;            /* 0 unless areas were given */
+    double t_submit, t_ready, t_admit, t_done;   /* seconds on the server's clock */
+    int64_t device_bytes;
+} mfcfd_result;
+
+typedef struct mfcfd_server_stats {
+    int64_t submitted, completed, failed;
+    int64_t preparing, waiting, live;      /* requests in each state now */
+    int64_t bytes_live, peak_bytes_live, hbm_budget;
+    int64_t rounds, iterations;            /* rounds run; iterations summed over requests */
+    int64_t peak_live;
+} mfcfd_server_stats;
+
+int mfcfd_server_create(const mfcfd_server_config *cfg, mfcfd_server **out);
+/* Copies the request's arrays; *id identifies it for mfcfd_server_wait. */
+int mfcfd_server_submit(mfcfd_server *s, const mfcfd_request *req, int64_t *id);
+/* Waits up to timeout_s (< 0: no limit) for request id to retire; fills
+ * *res and, when prim is not NULL, the final (5,N) state, then forgets the
+ * request.  MFCFD_ERR_BUSY if it has not retired within the wait. */
+int mfcfd_server_wait(mfcfd_server *s, int64_t id, double timeout_s, mfcfd_result *res, double *prim);
+int mfcfd_server_get_stats(mfcfd_server *s, mfcfd_server_stats *st);
+/* Stops admitting, ends live requests after their current round (status
+ * MFCFD_ERR_BUSY), and frees everything. */
+int mfcfd_server_destroy(mfcfd_server *s);
 
 #ifdef __cplusplus
 }

@@ -93,3 +93,23 @@ def test_host_only_handle_refuses_device_calls(mfcfd_lib, small_cloud):
     with pytest.raises(MfcfdError):
         s.residual_noalloc()
     assert s.info()["n_points"] == small_cloud.n
+
+
+def test_prepare_needs_a_device_and_serving_helpers(mfcfd_lib, small_cloud):
+    """mfcfd_prepare refuses a host-only handle; the serving statistics; a
+    server configuration without set-up threads is refused."""
+    from mfcfd import _lib, serve
+    from mfcfd.solver import params_for
+    L = _lib.lib()
+    p = params_for(0.8, 2.0, device=-1)
+    h = ctypes.c_void_p()
+    z = ctypes.c_void_p(0)
+    assert L.mfcfd_prepare(ctypes.byref(p), small_cloud.n, *([z] * 10), ctypes.byref(h)) == 1
+    assert not h.value
+    t = serve.poisson_arrivals(20.0, 2000, seed=5)
+    assert np.all(np.diff(t) > 0) and abs(2000 / t[-1] - 20.0) < 2.0
+    s = serve.latency_summary([1.0, 2.0, 3.0, 4.0])
+    assert s["p50"] == 2.5 and abs(s["p99"] - 3.97) < 1e-9 and s["max"] == 4.0
+    cfg = _lib.ServerConfig(device=0, max_live=0, setup_threads=0, chunk=10)
+    srv = ctypes.c_void_p()
+    assert L.mfcfd_server_create(ctypes.byref(cfg), ctypes.byref(srv)) == 1
