@@ -177,12 +177,22 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mfcfd", choices=["mfcfd", "reference"])
-    ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS) + ["serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--serve-requests", type=int, default=40)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrivals per second")
+    ap.add_argument("--serve-min-points", type=int, default=10000)
+    ap.add_argument("--serve-max-points", type=int, default=160000)
+    ap.add_argument("--serve-target", type=float, default=-1.0, help="residue (log10 drop) to converge to")
+    ap.add_argument("--serve-max-iters", type=int, default=600)
+    ap.add_argument("--serve-chunk", type=int, default=20)
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
+    if args.workload == "serve":
+        return serve_main(args, rank, world, local_rank)
     wl = WORKLOADS[args.workload]
     metric = "point-iters/s FP64"
 
@@ -328,6 +338,14 @@ def main():
                  "pressure_max_rel_err": float(np.max(np.abs(pm - p64) / np.abs(p64)))}
         sm.close()
 
+    # served solves (a reduced stream: 24 requests of 10k-80k points) beside
+    # the point-iteration rate, on one GPU
+    serving = None
+    if world == 1 and not args.no_serving:
+        s.close()
+        serving = serve_measure(args, rank, world, local_rank, 24, 80000)
+        s = None
+
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sps, n, kind = cpu_reference(1, 0, 3, wl["mach"], wl["aoa"])
@@ -352,10 +370,99 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "point-iters/s",
                         "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                 "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks, "mixed": mixed,
+                "serving": serving,
                 "gpu_launches": KERNELS_PER_ITER[args.sweep_mode] * args.steps}
         print(json.dumps(line), flush=True)
-    s.close()
+    if s is not None:
+        s.close()
     replicas.finalize()
+
+
+def serve_main(args, rank, world, local_rank):
+    """Served steady-state solves: a Poisson stream of requests (clouds of
+    log-uniform size, random Mach and angle of attack) through the request
+    server in mixed precision, against the same stream served one request at
+    a time in FP64; latency is submit to retirement.  A sample of the mixed
+    results (at least 5%) is re-solved alone in FP64 for the CL/CD error."""
+    import torch
+    from mfcfd import _lib, replicas, serve
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no request server; its CPU solver is timed by the "
+                              "point-iteration workloads"}), flush=True)
+        return
+    torch.cuda.set_device(local_rank)
+    rank, world = replicas.init("nccl", timeout_s=1800)
+    line = serve_measure(args, rank, world, local_rank, args.serve_requests, args.serve_max_points)
+    if rank == 0:
+        line.update({"metric": "served solves/s", "n_gpus": world, "steps": line["requests"], "warmup": 0,
+                     "ms_per_step": 1e3 / line["value"] * world, "higher_is_better": True,
+                     "scaling": "weak", "vs_baseline": None, "dtype": "mixed f32/f64",
+                     "data": "synthetic (seeded sphere/ellipsoid shell clouds)",
+                     "e2e": {"value": line["value"], "unit": "solves/s",
+                             "h2d_bytes_per_step": line.pop("h2d_bytes_per_request"),
+                             "d2h_bytes_per_step": line.pop("d2h_bytes_per_request")}})
+        print(json.dumps(line), flush=True)
+    replicas.finalize()
+
+
+def serve_measure(args, rank, world, local_rank, count, max_points):
+    """The serving measurement (see serve_main) for `count` requests of
+    clouds up to `max_points` points; returns its summary (rank 0)."""
+    from mfcfd import _lib, replicas, serve
+    arrivals, clouds, reqs = serve.request_stream(count, args.serve_rate,
+                                                  replicas.replica_seed(5000, rank),
+                                                  args.serve_min_points, max_points)
+
+    def run(precision, max_live):
+        with serve.Server(device=local_rank, chunk=args.serve_chunk, setup_threads=4,
+                          max_live=max_live) as srv:
+            replicas.barrier()
+            t0 = time.perf_counter()
+            ids = []
+            for ta, (ci, m, a) in zip(arrivals, reqs):
+                wait = ta - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                ids.append(srv.submit(clouds[ci], m, a, max_iters=args.serve_max_iters,
+                                      residue_target=args.serve_target, precision=precision))
+            res = [srv.wait(i) for i in ids]
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+        return res, replicas.max_over_ranks(wall, device="cuda"), st
+
+    res_m, wall_m, st_m = run(_lib.PRECISION_MIXED, 0)
+    res_b, wall_b, _ = run(_lib.PRECISION_FP64, 1)
+    total = len(reqs) * world
+    lat = serve.latency_summary([r["latency"] for r in res_m])
+    lat_b = serve.latency_summary([r["latency"] for r in res_b])
+    # CL/CD of a sample re-solved alone in FP64
+    k = max(2, -(-len(reqs) // 20))
+    errs = []
+    for j in range(k):
+        ci, m, a = reqs[j]
+        ref = serve.solve_alone(clouds[ci], m, a, args.serve_chunk, args.serve_max_iters, args.serve_target,
+                                device=local_rank)
+        errs.append((abs(res_m[j]["cl"] - ref["cl"]), abs(res_m[j]["cd"] - ref["cd"])))
+    conv = sum(1 for r in res_m if r["converged"])
+    pts = [clouds[ci].n for ci, _, _ in reqs]
+    return {"value": total / wall_m, "unit": "solves/s", "requests": len(reqs),
+            "config": {"workload": "serve", "requests": len(reqs), "rate_per_s": args.serve_rate,
+                       "points_min": min(pts), "points_max": max(pts), "points_total": sum(pts),
+                       "residue_target": args.serve_target, "max_iters": args.serve_max_iters,
+                       "chunk": args.serve_chunk, "precision": "mixed",
+                       "parallelism": f"replicas x{world}"},
+            "latency_s": lat, "converged": conv, "failed": sum(1 for r in res_m if r["status"]),
+            "iterations_mean": float(np.mean([r["iters"] for r in res_m])),
+            "peak_live": st_m["peak_live"], "peak_bytes_live": st_m["peak_bytes_live"],
+            "fp64_one_at_a_time": {"value": total / wall_b, "unit": "solves/s", "latency_s": lat_b},
+            "speedup_vs_fp64_one_at_a_time": wall_b / wall_m,
+            "fp64_resolve_sample": {"requests": k, "max_abs_dCL": max(e[0] for e in errs),
+                                    "max_abs_dCD": max(e[1] for e in errs)},
+            # per point: status, xyz, frames, nbhs, conn(27), min_dist, prim in; prim out
+            "h2d_bytes_per_request": int(np.mean(pts) * (4 + 24 + 72 + 4 + 108 + 8 + 40)),
+            "d2h_bytes_per_request": int(np.mean(pts) * 5 * 8)}
 
 
 if __name__ == "__main__":
