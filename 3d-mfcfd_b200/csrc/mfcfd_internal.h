@@ -144,6 +144,19 @@ struct ChainSchedule {
     int64_t terms_ring = 0, terms_local = 0, terms_cross = 0;   // swept producers
 };
 void build_chain_schedule(Topology &T, int warps, ChainSchedule &S);
+
+// Set-up passes on the GPU (mfcfd_prep.cu), equal to the host's.  The split
+// pass leaves T untouched and sets *overflow when a list exceeds `cap`
+// (the caller then stores the lists on the host, in the reference's order).
+int prep_split_gpu(int device, int n, int cap, const std::vector<int8_t> &cls, const double *x, const double *y,
+                   const double *z, const double *tan1, const double *tan2, const double *nor, const int32_t *nbhs,
+                   const int32_t *conn, Topology &T, bool *overflow, std::string &err);
+int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, std::vector<int32_t> &alias,
+                   std::vector<int32_t> &pwa, std::string &err);
+// level[p] of every point of `order` from its dependencies deps[doff[p] ..
+// doff[p+1]) (0-based ids); other points get -1.
+int prep_levels_gpu(int device, int n, const std::vector<int> &order, const std::vector<int32_t> &doff,
+                    const std::vector<int32_t> &deps, std::vector<int32_t> &level, std::string &err);
 void build_pre_order(const Topology &T, std::vector<int32_t> &order);
 
 // Build everything above.  Returns MFCFD_OK or an error code with a message.

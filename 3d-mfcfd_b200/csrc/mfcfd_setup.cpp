@@ -111,9 +111,17 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         }
     }
 
+    const bool gpu = P.gpu_setup != 0 && P.device >= 0;
     // ---- split stencils with the reference's storage (generate_connectivity.f90)
+    bool split_done = false;
+    if (gpu) {
+        bool over = false;
+        const int rc = prep_split_gpu(P.device, n, cap, T.cls, x, y, z, tan1, tan2, nor, nbhs, conn, T, &over, err);
+        if (rc) return rc;
+        split_done = !over;
+    }
     const size_t flat = (size_t)n * cap + 64;
-    for (int d = 0; d < NDIR; ++d) {
+    for (int d = 0; d < NDIR && !split_done; ++d) {
         T.split[d].assign(flat, 0);
         T.split_cnt[d].assign(n, 0);
     }
@@ -152,31 +160,38 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             }
         }
     };
-    for (int i : T.interior_idx) classify(i, CLS_INTERIOR);
-    for (int i : T.wall_idx) classify(i, CLS_WALL);
-    for (int i : T.outer_idx) classify(i, CLS_OUTER);
+    if (!split_done) {
+        for (int i : T.interior_idx) classify(i, CLS_INTERIOR);
+        for (int i : T.wall_idx) classify(i, CLS_WALL);
+        for (int i : T.outer_idx) classify(i, CLS_OUTER);
+    }
 
     // ---- alias breadth-first search (implicit_aliasing.f90:21-42).
     // Index 0 of the 1-based arrays is a zero guard: point_with_alias(i) = 0
     // makes the inner loop run over nbhs(0) = 0 neighbours.
-    std::vector<int32_t> alias1(n + 1, 0), pwa1(n + 1, 0);
-    alias1[1] = 1;
-    pwa1[1] = 1;
-    int count = 0;
-    for (int i = 1; i <= n; ++i) {
-        int p = pwa1[i];
-        int nb = p > 0 ? nbhs[p - 1] : 0;
-        for (int j = 0; j < nb; ++j) {
-            int k = conn[(size_t)(p - 1) * MAX_CONN + j];
-            if (alias1[k] == 0) {
-                count = count + 1;
-                alias1[k] = count;
-                pwa1[count] = k;
+    if (gpu) {
+        const int rc = prep_alias_gpu(P.device, n, nbhs, conn, T.alias, T.point_with_alias, err);
+        if (rc) return rc;
+    } else {
+        std::vector<int32_t> alias1(n + 1, 0), pwa1(n + 1, 0);
+        alias1[1] = 1;
+        pwa1[1] = 1;
+        int count = 0;
+        for (int i = 1; i <= n; ++i) {
+            int p = pwa1[i];
+            int nb = p > 0 ? nbhs[p - 1] : 0;
+            for (int j = 0; j < nb; ++j) {
+                int k = conn[(size_t)(p - 1) * MAX_CONN + j];
+                if (alias1[k] == 0) {
+                    count = count + 1;
+                    alias1[k] = count;
+                    pwa1[count] = k;
+                }
             }
         }
+        T.alias.assign(alias1.begin() + 1, alias1.end());
+        T.point_with_alias.assign(pwa1.begin() + 1, pwa1.end());
     }
-    T.alias.assign(alias1.begin() + 1, alias1.end());
-    T.point_with_alias.assign(pwa1.begin() + 1, pwa1.end());
 
     // ---- effective lists and neighbour slots
     T.slot_nbr.assign((size_t)n * MAX_SLOTS, -1);
@@ -403,6 +418,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     for (int k : T.ss_outlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, skip_wall, 100000.0)); }
     for (int k : T.ss_inlet_idx) { T.ss_pts.push_back(k); T.ss_src.push_back(nearest(k, skip_wall, 100000.0)); }
     auto al = [&](int k) { return T.alias[k]; };
+    int gpu_rc = MFCFD_OK;
     std::vector<int32_t> pos(n, -1);
     // a point's sweep terms of list d in list order: (slot, neighbour)
     auto for_terms = [&](int p, int d, auto &&fn) {
@@ -489,17 +505,38 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             if (off[p + 1] - off[p] > SWEEP_MAX_ENTRIES) return false;
         // levels: longest path over swept dependencies, visited in the order
         int maxl = -1;
-        auto visit = [&](int p) {
-            int lv = 0;
-            for (int e = off[p]; e < off[p + 1]; ++e) {
-                if (!entry_is_dependency(ent[e])) continue;
-                int k = ent[e].k;
-                if (T.swept[k] && level[k] + 1 > lv) lv = level[k] + 1;
-            }
-            level[p] = lv;
-            maxl = std::max(maxl, lv);
-        };
-        for (int p : order) visit(p);
+        auto is_dep = [&](const SweepEntry &E) { return entry_is_dependency(E) && T.swept[E.k]; };
+        if (gpu) {
+            std::vector<int32_t> doff(n + 1, 0), deps;
+            parallel_for((int)order.size(), [&](int oi) {
+                const int p = order[oi];
+                int c = 0;
+                for (int e = off[p]; e < off[p + 1]; ++e) c += is_dep(ent[e]) ? 1 : 0;
+                doff[p + 1] = c;
+            });
+            for (int p = 0; p < n; ++p) doff[p + 1] += doff[p];
+            deps.resize((size_t)doff[n]);
+            parallel_for((int)order.size(), [&](int oi) {
+                const int p = order[oi];
+                int at = doff[p];
+                for (int e = off[p]; e < off[p + 1]; ++e)
+                    if (is_dep(ent[e])) deps[at++] = ent[e].k;
+            });
+            if ((gpu_rc = prep_levels_gpu(P.device, n, order, doff, deps, level, err))) return false;
+            for (int p : order) maxl = std::max(maxl, (int)level[p]);
+        } else {
+            auto visit = [&](int p) {
+                int lv = 0;
+                for (int e = off[p]; e < off[p + 1]; ++e) {
+                    if (!is_dep(ent[e])) continue;
+                    const int k = ent[e].k;
+                    if (level[k] + 1 > lv) lv = level[k] + 1;
+                }
+                level[p] = lv;
+                maxl = std::max(maxl, lv);
+            };
+            for (int p : order) visit(p);
+        }
         int nl = maxl + 1;
         lptr.assign(nl + 1, 0);
         for (int p : order) lptr[level[p] + 1]++;
@@ -516,6 +553,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
                T.fwd_need, T.fwd_old) ||
         !build(false, order_b, T.bwd_level, T.bwd_lvl_ptr, T.bwd_lvl_pts, T.bwd_off, T.bwd_cnt, T.bwd_ent,
                T.bwd_need, T.bwd_old)) {
+        if (gpu_rc) return gpu_rc;
         err = "a point reads more than " + std::to_string(SWEEP_MAX_ENTRIES) + " sweep terms";
         return MFCFD_ERR_STENCIL;
     }

@@ -46,7 +46,7 @@ class Params(ctypes.Structure):
                 ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("sweep_mode", ctypes.c_int32), ("update_variant", ctypes.c_int32),
                 ("sweep_variant", ctypes.c_int32), ("chain_warps", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 4)]
+                ("gpu_setup", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
 
 PRECISION_FP64 = 0

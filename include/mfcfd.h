@@ -91,7 +91,9 @@ typedef struct mfcfd_params {
     int32_t sweep_variant;    /* MFCFD_SWEEPS_ALIAS (default) or MFCFD_SWEEPS_BACKUP */
     int32_t chain_warps;      /* CHAINS: warps of the schedule; 0 picks about twice the
                                  widest level (fewer warps leave SMs to other clouds) */
-    int32_t reserved[4];
+    int32_t gpu_setup;        /* 1: split stencils, alias search and sweep levels of the
+                                 set-up run on params->device (same results as the host) */
+    int32_t reserved[3];
 } mfcfd_params;
 
 /* The reference ships two drivers of its sweep module.  ALIAS:
