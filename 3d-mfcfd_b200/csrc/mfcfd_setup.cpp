@@ -26,6 +26,7 @@
  * values equal those the reference computes inline.
  */
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -161,9 +162,52 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         }
     };
     if (!split_done) {
-        for (int i : T.interior_idx) classify(i, CLS_INTERIOR);
-        for (int i : T.wall_idx) classify(i, CLS_WALL);
-        for (int i : T.outer_idx) classify(i, CLS_OUTER);
+        // No list longer than the capacity: every point writes only its own
+        // column, so the points are classified in parallel (a counting pass,
+        // then the fill).  Otherwise the reference's order decides what the
+        // overflow overwrites, and the points go one at a time in that order.
+        std::vector<uint8_t> longer(n, 0);
+        parallel_for(n, [&](int i) {
+            const int c = T.cls[i];
+            if (c != CLS_INTERIOR && c != CLS_WALL && c != CLS_OUTER) return;
+            int cn[NDIR] = {0, 0, 0, 0, 0, 0};
+            const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
+            for (int r = 0; r < nbhs[i]; ++r) {
+                const int k = conn[(size_t)i * MAX_CONN + r];
+                const double delx = x[k - 1] - x[i], dely = y[k - 1] - y[i], delz = z[k - 1] - z[i];
+                const double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+                const double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+                if (c == CLS_INTERIOR) {
+                    const double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                    if (dels <= 0.0) ++cn[0];
+                    if (dels > 0.0) ++cn[1];
+                    if (delt <= 0.0) ++cn[2];
+                    if (delt > 0.0) ++cn[3];
+                    if (deln <= 0.0) ++cn[4];
+                    if (deln > 0.0) ++cn[5];
+                } else {
+                    if (dels <= 0.0) ++cn[0];
+                    if (dels >= 0.0) ++cn[1];
+                    if (delt <= 0.0) ++cn[2];
+                    if (delt >= 0.0) ++cn[3];
+                    ++cn[c == CLS_WALL ? 5 : 4];
+                }
+            }
+            for (int d = 0; d < NDIR; ++d)
+                if (cn[d] > cap) longer[i] = 1;
+        });
+        bool any_longer = false;
+        for (int i = 0; i < n && !any_longer; ++i) any_longer = longer[i] != 0;
+        if (!any_longer) {
+            parallel_for(n, [&](int i) {
+                const int c = T.cls[i];
+                if (c == CLS_INTERIOR || c == CLS_WALL || c == CLS_OUTER) classify(i, c);
+            });
+        } else {
+            for (int i : T.interior_idx) classify(i, CLS_INTERIOR);
+            for (int i : T.wall_idx) classify(i, CLS_WALL);
+            for (int i : T.outer_idx) classify(i, CLS_OUTER);
+        }
     }
 
     // ---- alias breadth-first search (implicit_aliasing.f90:21-42).
@@ -609,21 +653,39 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
         };
         for (int w = 0; w < warps; ++w) heap.push_back({-1, w});
         std::make_heap(heap.begin(), heap.end(), cmp);
-        for (int p : lpts) {           // level-major, a topological order
-            int best = -1, best_level = -1;
+        // each point's dependencies of the deepest level, in entry order
+        // (computed in parallel; the assignment below only reads them)
+        std::vector<int32_t> coff(n + 1, 0), cand;
+        parallel_for(n, [&](int p) {
+            int best_level = -1, c = 0;
             for (int e = off[p]; e < off[p + 1]; ++e) {
-                if (!entry_is_dependency(ent[e])) continue;
-                const int k = ent[e].k;
-                if (!T.swept[k]) continue;
-                const int w = owner[k];
-                const bool cont = last_point[w] == k;
-                if (level[k] > best_level || (level[k] == best_level && cont)) {
-                    best_level = level[k];
-                    best = k;
-                }
+                if (!entry_is_dependency(ent[e]) || !T.swept[ent[e].k]) continue;
+                const int lv = level[ent[e].k];
+                if (lv > best_level) { best_level = lv; c = 1; }
+                else if (lv == best_level) ++c;
             }
+            coff[p + 1] = c;
+        });
+        for (int p = 0; p < n; ++p) coff[p + 1] += coff[p];
+        cand.resize((size_t)coff[n]);
+        parallel_for(n, [&](int p) {
+            int best_level = -1, at = coff[p];
+            for (int e = off[p]; e < off[p + 1]; ++e) {
+                if (!entry_is_dependency(ent[e]) || !T.swept[ent[e].k]) continue;
+                const int lv = level[ent[e].k];
+                if (lv > best_level) { best_level = lv; at = coff[p]; }
+                if (lv == best_level) cand[at++] = ent[e].k;
+            }
+        });
+        for (int p : lpts) {           // level-major, a topological order
+            // continue the warp of the last deepest dependency that is its
+            // warp's latest point; otherwise the warp whose latest point is
+            // shallowest
+            int best = -1;
+            for (int c = coff[p]; c < coff[p + 1]; ++c)
+                if (last_point[owner[cand[c]]] == cand[c]) best = cand[c];
             int w = -1;
-            if (best >= 0 && last_point[owner[best]] == best) {
+            if (best >= 0) {
                 w = owner[best];
             } else {
                 while (true) {     // pop stale heap entries
@@ -654,9 +716,13 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
         for (int w = 0; w < warps; ++w)
             for (int i = S.ptr[dir][w]; i < S.ptr[dir][w + 1]; ++i) pos[S.pts[dir][i]] = i - S.ptr[dir][w];
         std::vector<SweepEntry> &went = fwd ? T.fwd_ent : T.bwd_ent;
-        std::vector<uint8_t> publish(n, 0);
-        for (int p : lpts) {
+        std::vector<std::atomic<uint8_t>> publish(n);
+        for (auto &v : publish) v.store(0, std::memory_order_relaxed);
+        std::atomic<int64_t> n_ring{0}, n_local{0}, n_cross{0};
+        parallel_for((int)lpts.size(), [&](int li) {
+            const int p = lpts[li];
             const bool shared = T.consumer_shared[p] != 0;
+            int64_t ring = 0, local = 0, cross = 0;
             for (int e = off[p]; e < off[p + 1]; ++e) {
                 SweepEntry &E = went[e];
                 E.pad &= ~ENT_CHAIN_BITS;
@@ -667,14 +733,20 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
                 if (!shared) continue;       // reads dU of its slots directly
                 if (same && pos[p] - pos[k] <= CHAIN_RING) {
                     E.pad |= ENT_RING | ((pos[k] % CHAIN_RING) << ENT_RING_SHIFT);
-                    ++S.terms_ring;
+                    ++ring;
                 } else {
-                    publish[k] = 1;
-                    if (same) ++S.terms_local;
-                    else ++S.terms_cross;
+                    publish[k].store(1, std::memory_order_relaxed);
+                    if (same) ++local;
+                    else ++cross;
                 }
             }
-        }
+            n_ring += ring;
+            n_local += local;
+            n_cross += cross;
+        });
+        S.terms_ring += n_ring;
+        S.terms_local += n_local;
+        S.terms_cross += n_cross;
         const std::vector<uint8_t> &cnt = fwd ? T.fwd_cnt : T.bwd_cnt;
         std::vector<ChainItem> &items = S.items[dir];
         items.resize(S.pts[dir].size());
@@ -686,7 +758,8 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
             it.cnt = 0;
             for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[(size_t)p * NDIR + e] << (5 * e);
             it.info = (T.cls[p] == CLS_WALL ? CI_WALL : 0u) | (T.consumer_shared[p] ? CI_SHARED : 0u) |
-                      (publish[p] ? CI_PUBLISH : 0u) | (T.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u) |
+                      (publish[p].load(std::memory_order_relaxed) ? CI_PUBLISH : 0u) |
+                      (T.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u) |
                       (T.cls[p] == CLS_OUTER ? CI_OUTER : 0u);
         }
     }
