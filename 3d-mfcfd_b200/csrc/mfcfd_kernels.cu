@@ -445,6 +445,7 @@ __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
                 const int cnt = d.list_cnt[(size_t)p * NDIR + dd];
                 const uint8_t *ent = d.list_ent + ((size_t)p * NDIR + dd) * LIST_STRIDE;
                 double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll 4
                 for (int j = 0; j < cnt; ++j) {
                     const int s = ent[j];
                     const double t = T[(dd * MAX_SLOTS + s) * 5 + c];
@@ -869,6 +870,9 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         // ---- phase C
         double sx = 0.0, sy = 0.0, sz = 0.0;
         if (lane < 30) {
+            // unrolled so the next terms' shared-memory loads overlap; the
+            // additions keep their order
+#pragma unroll 4
             for (int jj = lo; jj < hi; ++jj) {
                 const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
                 sx = sx + t * E[jj].w[0];
