@@ -5,6 +5,7 @@
  * each reference entry point (fpi_solver, the q_lskum loop, the setup
  * routines) onto kernel launches on the handle's stream.
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -102,6 +103,16 @@ int upload(mfcfd_handle *h, const T **dst, const std::vector<T> &src) {
     return MFCFD_OK;
 }
 
+// Free one device array of the handle.
+void dfree(mfcfd_handle *h, const void *p) {
+    for (size_t i = 0; i < h->allocs.size(); ++i)
+        if (h->allocs[i] == p) {
+            cudaFree(h->allocs[i]);
+            h->allocs.erase(h->allocs.begin() + (long)i);
+            return;
+        }
+}
+
 void release(mfcfd_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->side) cudaStreamSynchronize(h->side);
@@ -184,6 +195,44 @@ int finish_chunk(mfcfd_handle *h, int32_t t0, int chunk, double *res_hist, int *
         }
     }
     return MFCFD_OK;
+}
+
+// Rebuild the chain schedule for about `want` warps on the handle's
+// topology and replace its device copy (the term records are re-marked, so
+// they are copied again).  Returns the warps of the new schedule, or < 0.
+int apply_chain_schedule(mfcfd_handle *h, int want) {
+    int wpb = 0, blocks = 0;
+    const int w = chain_shape(h->P.device, want, &wpb, &blocks);
+    if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident") * -1;
+    ChainSchedule S;
+    build_chain_schedule(h->T, w, S);
+    DevCloud &d = h->d;
+    int rc = MFCFD_OK;
+    for (int dir = 0; dir < 2; ++dir) {
+        dfree(h, d.ch_ptr[dir]);
+        dfree(h, d.ch_pts[dir]);
+        dfree(h, d.ch_own[dir]);
+        dfree(h, d.ch_items[dir]);
+        if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir])) || (rc = upload(h, &d.ch_pts[dir], S.pts[dir])) ||
+            (rc = upload(h, &d.ch_own[dir], S.owner[dir])) || (rc = upload(h, &d.ch_items[dir], S.items[dir])))
+            return -rc;
+    }
+    const std::vector<SweepEntry> *ents[2] = {&h->T.fwd_ent, &h->T.bwd_ent};
+    const SweepEntry *dents[2] = {d.fwd_ent, d.bwd_ent};
+    for (int dir = 0; dir < 2; ++dir)
+        if (!ents[dir]->empty()) {
+            cudaError_t e = cudaMemcpyAsync((void *)dents[dir], ents[dir]->data(), sizeof(SweepEntry) * ents[dir]->size(),
+                                            cudaMemcpyHostToDevice, h->stream);
+            if (e != cudaSuccess) return -cuda_fail(h, e, "cudaMemcpyAsync");
+        }
+    d.ch_warps = w;
+    d.ch_wpb = wpb;
+    h->chain_terms[0] = S.terms_ring;
+    h->chain_terms[1] = S.terms_local;
+    h->chain_terms[2] = S.terms_cross;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return -cuda_fail(h, e, "cudaStreamSynchronize");
+    return w;
 }
 
 int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist) {
@@ -732,6 +781,68 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
         a = b;
     }
     return first_err;
+}
+
+int mfcfd_tune_chain(mfcfd_handle *h, const int32_t *candidates, int32_t count, int32_t iters, int32_t *chosen,
+                     double *ms) {
+    if (!h || !chosen || iters < 1 || iters > 1000 || count < 0 || (count > 0 && !candidates)) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
+    if (h->d.sweep_mode != MFCFD_SWEEP_CHAINS) return fail(h, MFCFD_ERR_ARG, "tuning applies to the chain schedule");
+    CK(cudaSetDevice(h->P.device));
+    std::vector<int> wants;
+    if (count == 0) {
+        const int width = std::max(1, h->T.max_level_width);
+        for (int num : {3, 4, 6, 8}) wants.push_back(std::max(1, num * width / 2));   // 1.5x .. 4x the widest level
+    } else {
+        for (int32_t i = 0; i < count; ++i) {
+            if (candidates[i] < 1) return fail(h, MFCFD_ERR_ARG, "candidate warp counts must be positive");
+            wants.push_back(candidates[i]);
+        }
+    }
+    const size_t n5 = (size_t)h->d.n * 5;
+    std::vector<double> prim(n5), delu(n5);
+    double res_old = 0.0;
+    int rc = mfcfd_get_state(h, prim.data(), delu.data(), &res_old);
+    if (rc) return rc;
+    const int start = h->d.ch_warps;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best_ms = 0.0;
+    int best = start;
+    for (size_t c = 0; c < wants.size() && rc == MFCFD_OK; ++c) {
+        const int w = apply_chain_schedule(h, wants[c]);
+        if (w < 0) {
+            rc = -w;
+            break;
+        }
+        // one untimed iteration, then `iters` timed ones, from the saved state
+        if ((rc = mfcfd_set_state(h, prim.data(), delu.data(), res_old))) break;
+        if ((rc = run_iterations(h, 3, 1, nullptr))) break;
+        if ((rc = mfcfd_set_state(h, prim.data(), delu.data(), res_old))) break;
+        cudaEventRecord(e0, h->stream);
+        if ((rc = run_iterations(h, 3, iters, nullptr))) break;
+        cudaEventRecord(e1, h->stream);
+        cudaEventSynchronize(e1);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        const double per = t / iters;
+        if (ms) ms[c] = per;
+        if (c == 0 || per < best_ms) {
+            best_ms = per;
+            best = w;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // keep the fastest schedule (or the original one after a failure)
+    const int w = apply_chain_schedule(h, rc == MFCFD_OK ? best : start);
+    if (w < 0 && rc == MFCFD_OK) rc = -w;
+    const int rs = mfcfd_set_state(h, prim.data(), delu.data(), res_old);
+    if (rc == MFCFD_OK) rc = rs;
+    *chosen = h->d.ch_warps;
+    return rc;
 }
 
 int mfcfd_set_wall_areas(mfcfd_handle *h, const double *area) {

@@ -27,7 +27,7 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_residual_noalloc", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
            "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch",
-           "mfcfd_prepare", "mfcfd_device_bytes", "mfcfd_attach",
+           "mfcfd_prepare", "mfcfd_device_bytes", "mfcfd_attach", "mfcfd_tune_chain",
            "mfcfd_server_create", "mfcfd_server_submit", "mfcfd_server_wait",
            "mfcfd_server_get_stats", "mfcfd_server_destroy",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
@@ -151,6 +151,7 @@ def lib():
     L.mfcfd_prepare.argtypes = [ctypes.POINTER(Params), i32] + [vp] * 10 + [ctypes.POINTER(vp)]
     L.mfcfd_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.mfcfd_attach.argtypes = [vp]
+    L.mfcfd_tune_chain.argtypes = [vp, vp, i32, i32, ctypes.POINTER(i32), vp]
     L.mfcfd_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.mfcfd_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]
     L.mfcfd_server_wait.argtypes = [vp, ctypes.c_int64, dbl, ctypes.POINTER(Result), vp]

@@ -34,3 +34,9 @@ def run_batch(solvers, iters: int, t0=None):
     if rc != 0:
         raise MfcfdError(rc, "batch failed")
     return hist
+
+
+def tune_all(solvers, iters: int = 3, candidates=None):
+    """Autotune each Solver's chain schedule (mfcfd_tune_chain) before a
+    batch; returns the chosen warp counts.  States are left unchanged."""
+    return [s.tune_chain(candidates, iters)[0] for s in solvers]

@@ -98,6 +98,19 @@ class Solver:
                                             ctypes.byref(cd), ptr(f)))
         return float(cl.value), float(cd.value), f
 
+    def tune_chain(self, candidates=None, iters: int = 3):
+        """mfcfd_tune_chain: time the chain schedule for each candidate warp
+        count (default 1.5, 2, 3, 4 times the widest level) from the current
+        state, keep the fastest; the state is left as it was.  Returns the
+        kept warp count and {candidate index: ms per iteration}."""
+        cand = None if candidates is None else np.ascontiguousarray(candidates, dtype=np.int32)
+        count = 0 if cand is None else len(cand)
+        ms = np.zeros(max(count, 4))
+        chosen = ctypes.c_int32()
+        self._check(_lib.lib().mfcfd_tune_chain(self.h, None if cand is None else ptr(cand), count, int(iters),
+                                                ctypes.byref(chosen), ptr(ms)))
+        return chosen.value, ms[:count if count else 4]
+
     # -- data access ---------------------------------------------------------
     def get(self, field: int) -> np.ndarray:
         w = FIELD_WIDTH[field]

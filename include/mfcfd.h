@@ -306,6 +306,19 @@ int mfcfd_write_residue(const char *path, int32_t t0, int32_t iters, const doubl
  * The wall sum runs on the GPU in a fixed order.
  */
 int mfcfd_forces(mfcfd_handle *h, double wall_area, double ref_area, double *cl, double *cd, double *force);
+
+/*
+ * Autotuner of the chain schedule (no counterpart in the reference): times
+ * `iters` iterations (after one untimed) of each candidate warp count from
+ * the current state, restores that state after each, and keeps the
+ * fastest schedule.  candidates NULL with count 0 tries 1.5, 2, 3 and 4
+ * times the widest sweep level (the default schedule uses 2).  *chosen
+ * receives the kept schedule's warps and ms (count or 4 entries, may be
+ * NULL) each candidate's milliseconds per iteration.  The schedule orders
+ * the work only: results are the same bits with any choice.
+ */
+int mfcfd_tune_chain(mfcfd_handle *h, const int32_t *candidates, int32_t count, int32_t iters, int32_t *chosen,
+                     double *ms);
 /* Per-point areas A_i (N values; only wall points' are read) for
  * mfcfd_forces; NULL returns to the uniform wall_area split. */
 int mfcfd_set_wall_areas(mfcfd_handle *h, const double *area);
