@@ -51,6 +51,14 @@ struct mfcfd_handle {
     };
     std::unique_ptr<Staged> staged;
     bool dry = false;                      // count device bytes, allocate and copy nothing
+    // captured chunks of iterations: (chunk length, U/q buffer at its start)
+    struct GraphSlot {
+        int chunk = -1, parity = -1;
+        cudaGraphExec_t exec = nullptr;
+    };
+    GraphSlot graphs[2];
+    int graph_next = 0;
+    bool graphs_off = false;               // a capture failed: launch one by one
 };
 
 namespace {
@@ -113,8 +121,16 @@ void dfree(mfcfd_handle *h, const void *p) {
         }
 }
 
+void drop_graphs(mfcfd_handle *h) {
+    for (auto &g : h->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = mfcfd_handle::GraphSlot();
+    }
+}
+
 void release(mfcfd_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
     if (h->side) cudaStreamSynchronize(h->side);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
@@ -152,6 +168,61 @@ int launch_one(mfcfd_handle *h, int j) {
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     h->last = h->cur;
     h->cur = 1 - h->cur;
+    return MFCFD_OK;
+}
+
+// Launch the iterations of one chunk (slots 0 .. chunk-1).  With graphs, the
+// chunk is captured once per (length, starting U/q buffer) and replayed;
+// the host-side buffer state then advances as the captured launches did.
+int launch_chunk(mfcfd_handle *h, int chunk, bool batch) {
+    if (h->P.graphs < (batch ? 1 : 2) || h->graphs_off || h->profiling) {
+        for (int j = 0; j < chunk; ++j) {
+            int rc = launch_one(h, j);
+            if (rc) return rc;
+        }
+        return MFCFD_OK;
+    }
+    const int c0 = h->cur;
+    mfcfd_handle::GraphSlot *g = nullptr;
+    for (auto &s : h->graphs)
+        if (s.exec && s.chunk == chunk && s.parity == c0) g = &s;
+    if (!g) {
+        prepare_launches(h->P.device);
+        mfcfd_handle::GraphSlot &slot = h->graphs[h->graph_next];
+        h->graph_next ^= 1;
+        if (slot.exec) cudaGraphExecDestroy(slot.exec);
+        slot = mfcfd_handle::GraphSlot();
+        const int last0 = h->last;
+        cudaGraph_t graph = nullptr;
+        int rc = MFCFD_OK;
+        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            for (int j = 0; j < chunk && rc == MFCFD_OK; ++j) rc = launch_one(h, j);
+            e = cudaStreamEndCapture(h->stream, &graph);
+        }
+        h->cur = c0;
+        h->last = last0;
+        if (e == cudaSuccess && rc == MFCFD_OK) e = cudaGraphInstantiate(&slot.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess || rc != MFCFD_OK || !slot.exec) {
+            // no graph on this handle: launch one by one from now on
+            (void)cudaGetLastError();
+            slot = mfcfd_handle::GraphSlot();
+            h->graphs_off = true;
+            h->err.clear();
+            for (int j = 0; j < chunk; ++j) {
+                int rc2 = launch_one(h, j);
+                if (rc2) return rc2;
+            }
+            return MFCFD_OK;
+        }
+        slot.chunk = chunk;
+        slot.parity = c0;
+        g = &slot;
+    }
+    CK(cudaGraphLaunch(g->exec, h->stream));
+    h->last = (chunk & 1) ? c0 : 1 - c0;
+    h->cur = (chunk & 1) ? 1 - c0 : c0;
     return MFCFD_OK;
 }
 
@@ -227,6 +298,7 @@ int apply_chain_schedule(mfcfd_handle *h, int want) {
         }
     d.ch_warps = w;
     d.ch_wpb = wpb;
+    drop_graphs(h);                        // their launches name the old schedule
     h->chain_terms[0] = S.terms_ring;
     h->chain_terms[1] = S.terms_local;
     h->chain_terms[2] = S.terms_cross;
@@ -240,11 +312,9 @@ int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist)
     int status = MFCFD_OK;
     for (int32_t done = 0; done < iters;) {
         int chunk = std::min<int32_t>(iters - done, h->res_cap);
-        for (int j = 0; j < chunk; ++j) {
-            int rc = launch_one(h, j);
-            if (rc) return rc;
-        }
-        int rc = finish_chunk(h, t0 + done, chunk, res_hist ? res_hist + 2 * (size_t)done : nullptr, &status);
+        int rc = launch_chunk(h, chunk, false);
+        if (rc) return rc;
+        rc = finish_chunk(h, t0 + done, chunk, res_hist ? res_hist + 2 * (size_t)done : nullptr, &status);
         if (rc) return rc;
         done += chunk;
     }
@@ -281,6 +351,7 @@ void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg) {
     p->precision = MFCFD_PRECISION_FP64;
     p->device = 0;
     p->sweep_mode = MFCFD_SWEEP_CHAINS;
+    p->graphs = 1;
 }
 
 }  // extern "C"
@@ -762,12 +833,23 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
         for (int32_t i = a; i < b; ++i) cap = std::min(cap, hs[i]->res_cap);
         for (int32_t done = 0; done < iters;) {
             const int chunk = std::min<int32_t>(iters - done, std::max(cap, 1));
-            // one iteration of every handle in turn: their streams overlap
-            for (int j = 0; j < chunk; ++j)
+            // every handle's chunk on its own stream (their streams overlap):
+            // captured graphs, or one iteration of every handle in turn
+            bool graphs = true;
+            for (int32_t i = a; i < b; ++i)
+                graphs = graphs && hs[i]->P.graphs >= 1 && !hs[i]->graphs_off && !hs[i]->profiling;
+            if (graphs) {
                 for (int32_t i = a; i < b; ++i) {
-                    int rc = launch_one(hs[i], j);
+                    int rc = launch_chunk(hs[i], chunk, true);
                     if (rc) return rc;
                 }
+            } else {
+                for (int j = 0; j < chunk; ++j)
+                    for (int32_t i = a; i < b; ++i) {
+                        int rc = launch_one(hs[i], j);
+                        if (rc) return rc;
+                    }
+            }
             for (int32_t i = a; i < b; ++i) {
                 int st = MFCFD_OK;
                 double *rh = res_hist ? res_hist + 2 * ((size_t)i * iters + done) : nullptr;

@@ -250,6 +250,8 @@ int reduction_blocks(int n);
 // and blocks (one block per SM, some SMs left free); returns the warps, 0 if
 // the kernel cannot run on the device.
 int chain_shape(int device, int want, int *wpb, int *blocks);
+// Per-device launch set-up (kernel attributes), done before a stream capture.
+void prepare_launches(int device);
 // Chain sweep blocks that may be resident at once (one per SM, some SMs
 // left to the flux kernels).
 int chain_block_capacity(int device);

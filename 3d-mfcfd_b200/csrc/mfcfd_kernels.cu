@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <utility>
 #include <string>
 
 #include "mfcfd_internal.h"
@@ -1252,6 +1253,8 @@ static void set_attributes(int device) {
     done[device] = true;
 }
 
+void prepare_launches(int device) { set_attributes(device); }
+
 int chain_block_capacity(int device) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1286,6 +1289,32 @@ cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// A launch with an explicit scheduling priority.  The chain sweep must have
+// its blocks placed before those of the flux kernel beside it (which never
+// waits, so it cannot hold the sweep up for good); the priority travels with
+// the launch, so it holds in a captured graph as on a stream.
+template <typename... Args, typename... Act>
+static cudaError_t launch_prio(void (*kern)(Args...), int grid, int block, size_t smem, cudaStream_t s, bool high,
+                               Act &&...args) {
+    static int prio[2] = {0, 0};
+    static bool have = false;
+    if (!have) {
+        cudaDeviceGetStreamPriorityRange(&prio[0], &prio[1]);   // least, greatest
+        have = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = high ? prio[1] : prio[0];
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);
+}
+
 cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams &st, double *U_next,
                              double *q_next, cudaEvent_t *ev) {
     const int n = d.n;
@@ -1304,11 +1333,11 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         if (chains) {
             const int blocks = d.ch_warps / d.ch_wpb;
             if (mixed) {
-                if (d.ch_wpb == 4) k_sweep_chain<4, float><<<blocks, 4 * 32, chain_smem<4>(), s>>>(d, forward);
-                else k_sweep_chain<8, float><<<blocks, 8 * 32, chain_smem<8>(), s>>>(d, forward);
+                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float>, blocks, 4 * 32, chain_smem<4>(), s, true, d, forward);
+                else launch_prio(k_sweep_chain<8, float>, blocks, 8 * 32, chain_smem<8>(), s, true, d, forward);
             } else {
-                if (d.ch_wpb == 4) k_sweep_chain<4, double><<<blocks, 4 * 32, chain_smem<4>(), s>>>(d, forward);
-                else k_sweep_chain<8, double><<<blocks, 8 * 32, chain_smem<8>(), s>>>(d, forward);
+                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, double>, blocks, 4 * 32, chain_smem<4>(), s, true, d, forward);
+                else launch_prio(k_sweep_chain<8, double>, blocks, 8 * 32, chain_smem<8>(), s, true, d, forward);
             }
         } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);
@@ -1341,8 +1370,9 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         mark(3, s);
         cudaEventRecord(st.fork, s);
         cudaStreamWaitEvent(st.side, st.fork, 0);
-        if (mixed) k_flux<true, float><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, st.side>>>(d);
-        else k_flux<true, double><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, st.side>>>(d);
+        const size_t fsm = FLUX_WARPS * FLUX_SMEM_PER_WARP * 8;
+        if (mixed) launch_prio(k_flux<true, float>, fblocks, FLUX_WARPS * 32, fsm, st.side, false, d);
+        else launch_prio(k_flux<true, double>, fblocks, FLUX_WARPS * 32, fsm, st.side, false, d);
         mark(2, st.side);
         cudaEventRecord(st.join, st.side);
         sweep(1);

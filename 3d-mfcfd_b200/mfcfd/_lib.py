@@ -46,7 +46,8 @@ class Params(ctypes.Structure):
                 ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("sweep_mode", ctypes.c_int32), ("update_variant", ctypes.c_int32),
                 ("sweep_variant", ctypes.c_int32), ("chain_warps", ctypes.c_int32),
-                ("gpu_setup", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("gpu_setup", ctypes.c_int32), ("graphs", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
 
 
 PRECISION_FP64 = 0

@@ -418,6 +418,10 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
     def run(precision, max_live):
         with serve.Server(device=local_rank, chunk=args.serve_chunk, setup_threads=4,
                           max_live=max_live) as srv:
+            # warm-up request (untimed): first graph capture and launches in the process
+            small = min(range(len(clouds)), key=lambda i: clouds[i].n)
+            srv.wait(srv.submit(clouds[small], 0.5, 0.0, max_iters=args.serve_chunk, residue_target=-99.0,
+                                precision=precision))
             replicas.barrier()
             t0 = time.perf_counter()
             ids = []

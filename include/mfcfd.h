@@ -93,7 +93,10 @@ typedef struct mfcfd_params {
                                  widest level (fewer warps leave SMs to other clouds) */
     int32_t gpu_setup;        /* 1: split stencils, alias search and sweep levels of the
                                  set-up run on params->device (same results as the host) */
-    int32_t reserved[3];
+    int32_t graphs;           /* chunks of iterations captured once as CUDA graphs and
+                                 replayed: 1 (default) in mfcfd_run_batch, 2 also in
+                                 single-handle runs, 0 never (kernels one by one) */
+    int32_t reserved[2];
 } mfcfd_params;
 
 /* The reference ships two drivers of its sweep module.  ALIAS:
