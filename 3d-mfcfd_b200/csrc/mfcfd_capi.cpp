@@ -816,7 +816,7 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
     if (cudaSetDevice(dev) != cudaSuccess) return MFCFD_ERR_CUDA;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int capacity = chain_block_capacity(dev);
+    const int capacity = chain_slot_capacity(dev);
     int first_err = MFCFD_OK;
     // waves of handles whose chain sweep blocks fit on the device together
     for (int32_t a = 0; a < count;) {
@@ -824,9 +824,10 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
         int used = 0;
         while (b < count) {
             const DevCloud &d = hs[b]->d;
-            const int blocks = d.sweep_mode == MFCFD_SWEEP_CHAINS ? d.ch_warps / d.ch_wpb : 0;
-            if (b > a && used + blocks > capacity) break;
-            used += blocks;
+            const int slots =
+                d.sweep_mode == MFCFD_SWEEP_CHAINS ? d.ch_warps / d.ch_wpb * chain_block_slots(d.ch_wpb) : 0;
+            if (b > a && used + slots > capacity) break;
+            used += slots;
             ++b;
         }
         int cap = iters;

@@ -247,14 +247,15 @@ cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
 cudaError_t launch_forces(const DevCloud &d, cudaStream_t s, double area_each, const double *area, double *out);
 int reduction_blocks(int n);
 // Launch shape of the chain sweep for about `want` warps: warps per block
-// and blocks (one block per SM, some SMs left free); returns the warps, 0 if
-// the kernel cannot run on the device.
+// and blocks (at most SMs - 16 blocks); returns the warps, 0 if the kernel
+// cannot run on the device.
 int chain_shape(int device, int want, int *wpb, int *blocks);
 // Per-device launch set-up (kernel attributes), done before a stream capture.
 void prepare_launches(int device);
-// Chain sweep blocks that may be resident at once (one per SM, some SMs
-// left to the flux kernels).
-int chain_block_capacity(int device);
+// Chain-sweep blocks that may run at once, in slots: a 4-warp block takes
+// one, an 8-warp block two (see k_sweep_chain).
+int chain_slot_capacity(int device);
+inline int chain_block_slots(int wpb) { return wpb == 8 ? 2 : 1; }
 // File formats of the reference program (mfcfd_io.cpp).  Handle-less calls
 // leave their message in g_io_err (mfcfd_last_error(NULL)).
 extern thread_local std::string g_io_err;

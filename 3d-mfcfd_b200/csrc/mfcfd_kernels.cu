@@ -977,11 +977,16 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
 
 // Chain sweep: each warp walks its own list of point records (fixed at
 // set-up, topological order).  The stage of the next point is copied in
-// while the current one is processed (two stage buffers).  One block of WPB
-// warps per SM (the dynamic shared memory is sized for that), on at most
-// all SMs but CH_FREE_SMS, so all blocks are resident and the concurrent
-// flux kernel keeps SMs of its own: every poll ends.
-constexpr int CH_SMEM_MIN = 116 * 1024;   // over half an SM's shared memory
+// while the current one is processed (two stage buffers).
+//
+// Residency: an SM holds two 4-warp blocks or one 8-warp block (shared
+// memory and registers allow no more), i.e. two "slots", and the chain
+// blocks running at once (one cloud, or a wave of a batch) take at most
+// 2 * (SMs - CH_FREE_SMS) slots.  So all of them fit together, and at least
+// 2 * CH_FREE_SMS slots stay free, each on an SM with room for a block of
+// the concurrent flux kernel, whose outputs the forward sweep polls for
+// (the flux kernel never waits, so the blocks it holds are released):
+// every poll ends.
 constexpr int CH_FREE_SMS = 16;
 
 template <int WPB, typename R>
@@ -1019,7 +1024,7 @@ __global__ void __launch_bounds__(WPB * 32, 1) k_sweep_chain(DevCloud d, int for
 
 template <int WPB>
 static int chain_smem() {
-    return WPB * CHAIN_SMEM_BYTES > CH_SMEM_MIN ? WPB * CHAIN_SMEM_BYTES : CH_SMEM_MIN;
+    return WPB * CHAIN_SMEM_BYTES;
 }
 
 // ---------------------------------------------------------------- state update
@@ -1255,10 +1260,10 @@ static void set_attributes(int device) {
 
 void prepare_launches(int device) { set_attributes(device); }
 
-int chain_block_capacity(int device) {
+int chain_slot_capacity(int device) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    return sms - CH_FREE_SMS;
+    return 2 * (sms - CH_FREE_SMS);
 }
 
 int chain_shape(int device, int want, int *wpb, int *blocks) {
