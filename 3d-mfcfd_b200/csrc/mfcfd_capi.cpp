@@ -866,6 +866,29 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
     return first_err;
 }
 
+int mfcfd_set_chain_warps(mfcfd_handle *h, int32_t warps, int32_t *actual) {
+    if (!h || warps < 1) return MFCFD_ERR_ARG;
+    if (h->P.sweep_mode != MFCFD_SWEEP_CHAINS) return fail(h, MFCFD_ERR_ARG, "the handle does not use the chain schedule");
+    if (h->stream) {
+        CK(cudaSetDevice(h->P.device));
+        const int w = apply_chain_schedule(h, warps);
+        if (w < 0) return -w;
+        if (actual) *actual = w;
+        return MFCFD_OK;
+    }
+    if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+    // a prepared handle: rebuild the staged schedule before it is attached
+    mfcfd_handle::Staged &st = *h->staged;
+    int blocks = 0;
+    const int w = chain_shape(h->P.device, warps, &st.ch_wpb, &blocks);
+    if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+    st.S = ChainSchedule();
+    build_chain_schedule(h->T, w, st.S);
+    st.ch_w = w;
+    if (actual) *actual = w;
+    return MFCFD_OK;
+}
+
 int mfcfd_tune_chain(mfcfd_handle *h, const int32_t *candidates, int32_t count, int32_t iters, int32_t *chosen,
                      double *ms) {
     if (!h || !chosen || iters < 1 || iters > 1000 || count < 0 || (count > 0 && !candidates)) return MFCFD_ERR_ARG;

@@ -103,6 +103,13 @@ void mfcfd_server::worker_loop() {
         int rc = mfcfd_prepare(&P, r->n, r->status.data(), r->x.data(), r->y.data(), r->z.data(), r->tan1.data(),
                                r->tan2.data(), r->nor.data(), r->nbhs.data(), r->conn.data(), r->min_dist.data(),
                                &h);
+        if (!rc && cfg.chain_percent > 0 && P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+            mfcfd_info info;
+            rc = mfcfd_get_info(h, &info);
+            if (!rc)
+                rc = mfcfd_set_chain_warps(h, std::max(4, (int)((int64_t)info.max_level_width * cfg.chain_percent / 100)),
+                                           nullptr);
+        }
         int64_t bytes = 0;
         if (!rc) rc = mfcfd_device_bytes(h, &bytes);
         if (rc && h) r->err = mfcfd_last_error(h);
@@ -236,7 +243,8 @@ int mfcfd_server_create(const mfcfd_server_config *cfg, mfcfd_server **out) {
     if (!out) return MFCFD_ERR_ARG;
     *out = nullptr;
     if (!cfg || cfg->device < 0 || cfg->max_live < 0 || cfg->setup_threads < 1 || cfg->setup_threads > 64 ||
-        cfg->chunk < 1 || cfg->chunk > 1024 || cfg->hbm_budget < 0)
+        cfg->chunk < 1 || cfg->chunk > 1024 || cfg->hbm_budget < 0 || cfg->chain_percent < 0 ||
+        cfg->chain_percent > 1000)
         return MFCFD_ERR_ARG;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return MFCFD_ERR_CUDA;
     auto *s = new (std::nothrow) mfcfd_server();

@@ -28,6 +28,7 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
            "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch",
            "mfcfd_prepare", "mfcfd_device_bytes", "mfcfd_attach", "mfcfd_tune_chain",
+           "mfcfd_set_chain_warps",
            "mfcfd_server_create", "mfcfd_server_submit", "mfcfd_server_wait",
            "mfcfd_server_get_stats", "mfcfd_server_destroy",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
@@ -77,7 +78,8 @@ class ServerConfig(ctypes.Structure):
     """mfcfd_server_config (include/mfcfd.h)."""
     _fields_ = [("device", ctypes.c_int32), ("max_live", ctypes.c_int32),
                 ("setup_threads", ctypes.c_int32), ("chunk", ctypes.c_int32),
-                ("hbm_budget", ctypes.c_int64), ("reserved", ctypes.c_int32 * 8)]
+                ("hbm_budget", ctypes.c_int64), ("chain_percent", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 7)]
 
 
 class Request(ctypes.Structure):
@@ -153,6 +155,7 @@ def lib():
     L.mfcfd_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.mfcfd_attach.argtypes = [vp]
     L.mfcfd_tune_chain.argtypes = [vp, vp, i32, i32, ctypes.POINTER(i32), vp]
+    L.mfcfd_set_chain_warps.argtypes = [vp, i32, ctypes.POINTER(i32)]
     L.mfcfd_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.mfcfd_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]
     L.mfcfd_server_wait.argtypes = [vp, ctypes.c_int64, dbl, ctypes.POINTER(Result), vp]

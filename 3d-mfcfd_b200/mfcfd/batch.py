@@ -40,3 +40,37 @@ def tune_all(solvers, iters: int = 3, candidates=None):
     """Autotune each Solver's chain schedule (mfcfd_tune_chain) before a
     batch; returns the chosen warp counts.  States are left unchanged."""
     return [s.tune_chain(candidates, iters)[0] for s in solvers]
+
+
+def tune_batch(solvers, percents=(75, 100, 125, 150, 200), iters: int = 4):
+    """Autotune a batch as a whole: for each candidate, every cloud's chain
+    schedule gets that percentage of its widest sweep level in warps, and a
+    round of `iters` batched iterations is timed (after an untimed round that
+    captures the graphs).  Fewer warps per cloud let more clouds share the
+    device at once; the fastest percentage is kept.  States and histories
+    are restored; results do not depend on the choice.  Returns (percent,
+    {percent: seconds per round})."""
+    import time
+    states = [s.get_state() for s in solvers]
+    hist = [len(s.history) for s in solvers]
+    widths = [s.info()["max_level_width"] for s in solvers]
+
+    def restore():
+        for s, st, h in zip(solvers, states, hist):
+            s.set_state(*st)
+            del s.history[h:]
+
+    times = {}
+    for pc in percents:
+        for s, w in zip(solvers, widths):
+            s.set_chain_warps(max(4, w * pc // 100))
+        for rep in range(2 if iters % 2 == 0 else 3):
+            restore()
+            t = time.perf_counter()
+            run_batch(solvers, iters)
+            times[pc] = time.perf_counter() - t
+    best = min(times, key=times.get)
+    for s, w in zip(solvers, widths):
+        s.set_chain_warps(max(4, w * best // 100))
+    restore()
+    return best, times

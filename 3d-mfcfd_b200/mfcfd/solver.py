@@ -111,6 +111,13 @@ class Solver:
                                                 ctypes.byref(chosen), ptr(ms)))
         return chosen.value, ms[:count if count else 4]
 
+    def set_chain_warps(self, warps: int) -> int:
+        """mfcfd_set_chain_warps: rebuild the chain schedule for about
+        `warps` warps; returns the schedule's warps."""
+        actual = ctypes.c_int32()
+        self._check(_lib.lib().mfcfd_set_chain_warps(self.h, int(warps), ctypes.byref(actual)))
+        return actual.value
+
     # -- data access ---------------------------------------------------------
     def get(self, field: int) -> np.ndarray:
         w = FIELD_WIDTH[field]

@@ -177,7 +177,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mfcfd", choices=["mfcfd", "reference"])
-    ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS) + ["serve"])
+    ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS) + ["serve", "batch"])
+    ap.add_argument("--batch-clouds", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
@@ -193,6 +194,8 @@ def main():
     rank, world, local_rank = dist_env()
     if args.workload == "serve":
         return serve_main(args, rank, world, local_rank)
+    if args.workload == "batch":
+        return batch_main(args, rank, world, local_rank)
     wl = WORKLOADS[args.workload]
     metric = "point-iters/s FP64"
 
@@ -378,6 +381,85 @@ def main():
     replicas.finalize()
 
 
+def batch_main(args, rank, world, local_rank):
+    """Batched clouds: a seeded set of sphere and ellipsoid clouds of uneven
+    size (log-uniform 20k-100k points) iterated together in mixed precision,
+    each chunk a captured graph and the chain schedules autotuned for the batch,
+    against the same clouds run one after another on the plain FP64 path.
+    Both are device-timed over the same iterations; point-iters/s aggregate."""
+    import torch
+    from mfcfd import _lib, batch, replicas, serve
+    from mfcfd.solver import Solver
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no batch runner; its CPU solver is timed by the "
+                              "point-iteration workloads"}), flush=True)
+        return
+    torch.cuda.set_device(local_rank)
+    rank, world = replicas.init("nccl", timeout_s=1800)
+    _, clouds, reqs = serve.request_stream(args.batch_clouds, 1.0, replicas.replica_seed(7000, rank),
+                                           20000, 100000, pool=args.batch_clouds)
+    flows = [(reqs[i][1], reqs[i][2]) for i in range(len(clouds))]
+    pts = sum(c.n for c in clouds)
+    # plain FP64 path, one cloud after another (device time of `steps` iterations each)
+    seq_ms = 0.0
+    for c, (m, a) in zip(clouds, flows):
+        s = Solver(c, m, a, device=local_rank)
+        s.initial_conditions()
+        s.q_lskum(args.warmup)
+        st = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.q_lskum(args.steps, t0=1 + args.warmup)
+        e1.record(st)
+        torch.cuda.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        s.close()
+    # batched: mixed precision, tuned schedules, graph-captured chunks
+    ss = []
+    for c, (m, a) in zip(clouds, flows):
+        s = Solver(c, m, a, device=local_rank, precision=_lib.PRECISION_MIXED)
+        s.initial_conditions()
+        ss.append(s)
+    t_tune = time.perf_counter()
+    percent, tune_times = batch.tune_batch(ss, iters=4)
+    t_tune = time.perf_counter() - t_tune
+    warps = [s.info()["chain_warps"] for s in ss]
+    # warm-up: the timed chunk length, for both U/q parities (graphs captured)
+    batch.run_batch(ss, args.warmup)
+    for _ in range(1 if args.steps % 2 == 0 else 2):
+        batch.run_batch(ss, args.steps)
+    replicas.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.run_batch(ss, args.steps)
+    torch.cuda.synchronize()
+    bat_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    for s in ss:
+        s.close()
+    seq_s = replicas.max_over_ranks(seq_ms / 1e3, device="cuda")
+    value = pts * args.steps * world / bat_s
+    if rank == 0:
+        line = {"metric": "point-iters/s batched mixed vs FP64 one at a time", "value": value,
+                "unit": "point-iters/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": bat_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "mixed f32/f64",
+                "data": "synthetic (seeded sphere/ellipsoid shell clouds)",
+                "config": {"workload": "batch", "clouds": len(clouds), "points_total": pts,
+                           "points_min": min(c.n for c in clouds), "points_max": max(c.n for c in clouds),
+                           "tuned_percent_of_widest_level": percent,
+                           "tune_round_s": {str(k): v for k, v in tune_times.items()},
+                           "tuned_warps": warps, "tune_s": t_tune, "parallelism": f"replicas x{world}",
+                           "timing": "batched: wall clock with device synchronisation around the K "
+                                     "iterations; FP64: device events, clouds one after another"},
+                "fp64_one_at_a_time": {"value": pts * args.steps * world / seq_s, "unit": "point-iters/s",
+                                       "ms_per_step": seq_s * 1e3 / args.steps},
+                "speedup_vs_fp64_one_at_a_time": seq_s / bat_s}
+        print(json.dumps(line), flush=True)
+    replicas.finalize()
+
+
 def serve_main(args, rank, world, local_rank):
     """Served steady-state solves: a Poisson stream of requests (clouds of
     log-uniform size, random Mach and angle of attack) through the request
@@ -416,8 +498,10 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
                                                   args.serve_min_points, max_points)
 
     def run(precision, max_live):
+        # many requests at once: chain schedules of the widest level's width;
+        # one at a time: each request's own (twice that)
         with serve.Server(device=local_rank, chunk=args.serve_chunk, setup_threads=4,
-                          max_live=max_live) as srv:
+                          max_live=max_live, chain_percent=100 if max_live == 0 else 0) as srv:
             # warm-up request (untimed): first graph capture and launches in the process
             small = min(range(len(clouds)), key=lambda i: clouds[i].n)
             srv.wait(srv.submit(clouds[small], 0.5, 0.0, max_iters=args.serve_chunk, residue_target=-99.0,

@@ -322,6 +322,11 @@ int mfcfd_forces(mfcfd_handle *h, double wall_area, double ref_area, double *cl,
  */
 int mfcfd_tune_chain(mfcfd_handle *h, const int32_t *candidates, int32_t count, int32_t iters, int32_t *chosen,
                      double *ms);
+/* Rebuild the chain schedule for about `warps` warps (prepared or attached
+ * handle); *actual (may be NULL) receives the schedule's warps.  In a batch,
+ * fewer warps per cloud (about the widest level) let more clouds share the
+ * device; alone, about twice the widest level is fastest. */
+int mfcfd_set_chain_warps(mfcfd_handle *h, int32_t warps, int32_t *actual);
 /* Per-point areas A_i (N values; only wall points' are read) for
  * mfcfd_forces; NULL returns to the uniform wall_area split. */
 int mfcfd_set_wall_areas(mfcfd_handle *h, const double *area);
@@ -354,7 +359,10 @@ typedef struct mfcfd_server_config {
     int32_t setup_threads;    /* host threads preparing submitted clouds (1..64) */
     int32_t chunk;            /* iterations per live request per round (1..1024) */
     int64_t hbm_budget;       /* device bytes the live requests may hold; 0: 90% of free memory */
-    int32_t reserved[8];
+    int32_t chain_percent;    /* chain schedule of each request: this percentage of its widest
+                                 sweep level in warps (100 suits many requests at once);
+                                 0: the request's own setting */
+    int32_t reserved[7];
 } mfcfd_server_config;
 
 typedef struct mfcfd_request {
