@@ -189,7 +189,8 @@ def main():
     ap.add_argument("--serve-max-points", type=int, default=160000)
     ap.add_argument("--serve-target", type=float, default=-1.0, help="residue (log10 drop) to converge to")
     ap.add_argument("--serve-max-iters", type=int, default=600)
-    ap.add_argument("--serve-chunk", type=int, default=20)
+    ap.add_argument("--serve-chunk", type=int, default=10)
+    ap.add_argument("--serve-setup-threads", type=int, default=8)
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.workload == "serve":
@@ -500,7 +501,7 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
     def run(precision, max_live):
         # many requests at once: chain schedules of the widest level's width;
         # one at a time: each request's own (twice that)
-        with serve.Server(device=local_rank, chunk=args.serve_chunk, setup_threads=4,
+        with serve.Server(device=local_rank, chunk=args.serve_chunk, setup_threads=args.serve_setup_threads,
                           max_live=max_live, chain_percent=100 if max_live == 0 else 0) as srv:
             # warm-up request (untimed): first graph capture and launches in the process
             small = min(range(len(clouds)), key=lambda i: clouds[i].n)
