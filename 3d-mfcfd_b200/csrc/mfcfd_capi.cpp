@@ -699,7 +699,7 @@ int mfcfd_set_state(mfcfd_handle *h, const double *prim, const double *delu, dou
     size_t n5 = (size_t)h->d.n * 5;
     CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->d.dUn, delu, n5 * 8, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d.dUp, delu, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d.dUp, h->d.dUn, n5 * 8, cudaMemcpyDeviceToDevice, h->stream));
     DevCloud dc = h->d;
     dc.U = h->U_buf[h->cur];
     dc.q = h->q_buf[h->cur];

@@ -125,9 +125,10 @@ class Solver:
         self._check(_lib.lib().mfcfd_get(self.h, int(field), ptr(out)))
         return out if w > 1 else out[:, 0]
 
-    def get_state(self):
-        prim = np.empty((self.n, 5))
-        delu = np.empty((self.n, 5))
+    def get_state(self, out=None):
+        """(prim, delUn, res_old); `out` = (prim, delu) arrays (N, 5) to fill,
+        e.g. pinned host buffers, instead of new ones."""
+        prim, delu = out if out is not None else (np.empty((self.n, 5)), np.empty((self.n, 5)))
         ro = np.zeros(1)
         self._check(_lib.lib().mfcfd_get_state(self.h, ptr(prim), ptr(delu), ptr(ro)))
         return prim, delu, float(ro[0])
