@@ -408,7 +408,8 @@ int mfcfd_server_submit(mfcfd_server *s, const mfcfd_request *req, int64_t *id);
 int mfcfd_server_wait(mfcfd_server *s, int64_t id, double timeout_s, mfcfd_result *res, double *prim);
 int mfcfd_server_get_stats(mfcfd_server *s, mfcfd_server_stats *st);
 /* Stops admitting, ends live requests after their current round (status
- * MFCFD_ERR_BUSY), and frees everything. */
+ * MFCFD_ERR_BUSY), and frees everything.  No other call on the server may be
+ * in progress (a thread blocked in mfcfd_server_wait included) or follow. */
 int mfcfd_server_destroy(mfcfd_server *s);
 
 #ifdef __cplusplus
