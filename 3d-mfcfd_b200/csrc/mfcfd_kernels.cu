@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <type_traits>
 #include <utility>
 #include <string>
 
@@ -869,20 +870,32 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         __syncwarp();
 
         // ---- phase C
-        double sx = 0.0, sy = 0.0, sz = 0.0;
-        if (lane < 30) {
-            // unrolled so the next terms' shared-memory loads overlap; the
-            // additions keep their order
-#pragma unroll 4
-            for (int jj = lo; jj < hi; ++jj) {
-                const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
-                sx = sx + t * E[jj].w[0];
-                sy = sy + t * E[jj].w[1];
-                sz = sz + t * E[jj].w[2];
-            }
-        }
         double G = 0.0;
-        if (lane < 30) G = cramer_num(dd >> 1, g, sx, sy, sz) / g[6];
+        if constexpr (std::is_same<R, float>::value) {
+            // mixed precision: each term's weight already carries the list's
+            // 3x3 solve (cofactors / det, FP64, computed at set-up)
+            if (lane < 30) {
+#pragma unroll 4
+                for (int jj = lo; jj < hi; ++jj) {
+                    const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
+                    G = G + t * E[jj].w[0];
+                }
+            }
+        } else {
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+            if (lane < 30) {
+                // unrolled so the next terms' shared-memory loads overlap; the
+                // additions keep their order
+#pragma unroll 4
+                for (int jj = lo; jj < hi; ++jj) {
+                    const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
+                    sx = sx + t * E[jj].w[0];
+                    sy = sy + t * E[jj].w[1];
+                    sz = sz + t * E[jj].w[2];
+                }
+            }
+            if (lane < 30) G = cramer_num(dd >> 1, g, sx, sy, sz) / g[6];
+        }
         double gd[NDIR];
 #pragma unroll
         for (int e = 0; e < NDIR; ++e) gd[e] = __shfl_sync(FULL, G, e * 5 + (lane % 5));
