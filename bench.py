@@ -46,10 +46,10 @@ PHASE_BYTES = {"qderiv": 372 + 180, "flux": 724, "dinv": 488, "sweep_fwd": 608,
                "sweep_bwd": 608, "update": 196, "residual": 8}
 TOTAL_BYTES = 3368
 # DRAM bytes (read + write) per swept point of one chain-sweep launch, from
-# the ncu capture of the 62,400-point sphere's forward sweep (161.96 MB per
+# the ncu capture of the 62,400-point sphere's forward sweep (160.78 MB per
 # launch, profiles/ncu_k_sweep_chain_sphere62k.txt); traffic grows with the
 # point count, so a launch of n points moves about n times this.
-SWEEP_TRAFFIC_PER_POINT = 161.96e6 / 62400
+SWEEP_TRAFFIC_PER_POINT = 160.78e6 / 62400
 
 WORKLOADS = {
     "sphere-1.1M": dict(shells=96, per_shell=11500, jitter=0.01, mach=0.8, aoa=2.0, seed=2001),
