@@ -6,6 +6,9 @@
  * routines) onto kernel launches on the handle's stream.
  */
 #include <algorithm>
+#include <chrono>
+#include <deque>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -58,6 +61,7 @@ struct mfcfd_handle {
     };
     GraphSlot graphs[2];
     int graph_next = 0;
+    cudaEvent_t batch_ev = nullptr;        // end of the handle's chunk in mfcfd_run_batch
     bool graphs_off = false;               // a capture failed: launch one by one
 };
 
@@ -136,6 +140,8 @@ void release(mfcfd_handle *h) {
     h->ev.clear();
     for (void *p : h->allocs) cudaFree(p);
     h->allocs.clear();
+    if (h->batch_ev) cudaEventDestroy(h->batch_ev);
+    h->batch_ev = nullptr;
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);
     h->fork = h->join = nullptr;
@@ -814,54 +820,64 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
         if (status) status[i] = MFCFD_OK;
     }
     if (cudaSetDevice(dev) != cudaSuccess) return MFCFD_ERR_CUDA;
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int capacity = chain_slot_capacity(dev);
     int first_err = MFCFD_OK;
-    // waves of handles whose chain sweep blocks fit on the device together
-    for (int32_t a = 0; a < count;) {
-        int32_t b = a;
-        int used = 0;
-        while (b < count) {
-            const DevCloud &d = hs[b]->d;
-            const int slots =
-                d.sweep_mode == MFCFD_SWEEP_CHAINS ? d.ch_warps / d.ch_wpb * chain_block_slots(d.ch_wpb) : 0;
-            if (b > a && used + slots > capacity) break;
-            used += slots;
-            ++b;
+    // Continuous scheduling on SM slots: a handle's next chunk starts as
+    // soon as its chain blocks fit beside the chunks running, and a chunk's
+    // slots return when its completion event has fired.  So all running
+    // chain blocks are always resident together (see k_sweep_chain), and no
+    // handle waits for a whole group of others to finish.
+    std::vector<int32_t> done(count, 0);
+    std::vector<int> chunk_of(count, 0);
+    std::deque<int32_t> ready;
+    std::vector<int32_t> running;
+    for (int32_t i = 0; i < count; ++i) {
+        if (iters > 0) ready.push_back(i);
+        if (!hs[i]->batch_ev && cudaEventCreateWithFlags(&hs[i]->batch_ev, cudaEventDisableTiming) != cudaSuccess)
+            return cuda_fail(hs[i], cudaGetLastError(), "cudaEventCreateWithFlags");
+    }
+    auto slots_of = [&](int32_t i) {
+        const DevCloud &d = hs[i]->d;
+        return d.sweep_mode == MFCFD_SWEEP_CHAINS ? d.ch_warps / d.ch_wpb * chain_block_slots(d.ch_wpb) : 0;
+    };
+    int used = 0;
+    while (!ready.empty() || !running.empty()) {
+        while (!ready.empty()) {
+            const int32_t i = ready.front();
+            const int sl = slots_of(i);
+            if (!running.empty() && used + sl > capacity) break;
+            ready.pop_front();
+            mfcfd_handle *h = hs[i];
+            const int chunk = std::min<int32_t>(iters - done[i], std::max(h->res_cap, 1));
+            int rc = launch_chunk(h, chunk, true);
+            if (rc) return rc;
+            cudaError_t e = cudaEventRecord(h->batch_ev, h->stream);
+            if (e != cudaSuccess) return cuda_fail(h, e, "cudaEventRecord");
+            chunk_of[i] = chunk;
+            used += sl;
+            running.push_back(i);
         }
-        int cap = iters;
-        for (int32_t i = a; i < b; ++i) cap = std::min(cap, hs[i]->res_cap);
-        for (int32_t done = 0; done < iters;) {
-            const int chunk = std::min<int32_t>(iters - done, std::max(cap, 1));
-            // every handle's chunk on its own stream (their streams overlap):
-            // captured graphs, or one iteration of every handle in turn
-            bool graphs = true;
-            for (int32_t i = a; i < b; ++i)
-                graphs = graphs && hs[i]->P.graphs >= 1 && !hs[i]->graphs_off && !hs[i]->profiling;
-            if (graphs) {
-                for (int32_t i = a; i < b; ++i) {
-                    int rc = launch_chunk(hs[i], chunk, true);
-                    if (rc) return rc;
-                }
-            } else {
-                for (int j = 0; j < chunk; ++j)
-                    for (int32_t i = a; i < b; ++i) {
-                        int rc = launch_one(hs[i], j);
-                        if (rc) return rc;
-                    }
+        // wait for the first of the running chunks to complete
+        int found = -1;
+        while (found < 0) {
+            for (size_t r = 0; r < running.size() && found < 0; ++r) {
+                const cudaError_t q = cudaEventQuery(hs[running[r]]->batch_ev);
+                if (q == cudaSuccess) found = (int)r;
+                else if (q != cudaErrorNotReady) return cuda_fail(hs[running[r]], q, "cudaEventQuery");
             }
-            for (int32_t i = a; i < b; ++i) {
-                int st = MFCFD_OK;
-                double *rh = res_hist ? res_hist + 2 * ((size_t)i * iters + done) : nullptr;
-                int rc = finish_chunk(hs[i], t0[i] + done, chunk, rh, &st);
-                if (!rc) rc = st;
-                if (status && rc && status[i] == MFCFD_OK) status[i] = rc;
-                if (rc && first_err == MFCFD_OK) first_err = rc;
-            }
-            done += chunk;
+            if (found < 0) std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
-        a = b;
+        const int32_t i = running[found];
+        running.erase(running.begin() + found);
+        used -= slots_of(i);
+        int st = MFCFD_OK;
+        double *rh = res_hist ? res_hist + 2 * ((size_t)i * iters + done[i]) : nullptr;
+        int rc = finish_chunk(hs[i], t0[i] + done[i], chunk_of[i], rh, &st);
+        if (!rc) rc = st;
+        if (status && rc && status[i] == MFCFD_OK) status[i] = rc;
+        if (rc && first_err == MFCFD_OK) first_err = rc;
+        done[i] += chunk_of[i];
+        if (done[i] < iters) ready.push_back(i);
     }
     return first_err;
 }
