@@ -61,7 +61,9 @@ struct mfcfd_handle {
     };
     GraphSlot graphs[2];
     int graph_next = 0;
-    cudaEvent_t batch_ev = nullptr;        // end of the handle's chunk in mfcfd_run_batch
+    cudaEvent_t batch_ev = nullptr;        // end of the handle's chunk in mfcfd_run_batch / mfcfd_launch
+    int pending_chunk = 0;                 // mfcfd_launch: iterations not yet completed
+    int32_t pending_t0 = 0;
     bool graphs_off = false;               // a capture failed: launch one by one
 };
 
@@ -96,8 +98,9 @@ int dalloc(mfcfd_handle *h, T **p, size_t count) {
         *p = nullptr;
         return MFCFD_OK;
     }
+    // stream-ordered: freeing later does not synchronise the whole device
     void *v = nullptr;
-    cudaError_t e = cudaMalloc(&v, bytes);
+    cudaError_t e = h->stream ? cudaMallocAsync(&v, bytes, h->stream) : cudaMalloc(&v, bytes);
     if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
     h->allocs.push_back(v);
     h->bytes += (int64_t)bytes;
@@ -119,7 +122,8 @@ int upload(mfcfd_handle *h, const T **dst, const std::vector<T> &src) {
 void dfree(mfcfd_handle *h, const void *p) {
     for (size_t i = 0; i < h->allocs.size(); ++i)
         if (h->allocs[i] == p) {
-            cudaFree(h->allocs[i]);
+            if (h->stream) cudaFreeAsync(h->allocs[i], h->stream);
+            else cudaFree(h->allocs[i]);
             h->allocs.erase(h->allocs.begin() + (long)i);
             return;
         }
@@ -138,7 +142,11 @@ void release(mfcfd_handle *h) {
     if (h->side) cudaStreamSynchronize(h->side);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
-    for (void *p : h->allocs) cudaFree(p);
+    for (void *p : h->allocs) {
+        if (h->stream) cudaFreeAsync(p, h->stream);
+        else cudaFree(p);
+    }
+    if (h->stream) cudaStreamSynchronize(h->stream);
     h->allocs.clear();
     if (h->batch_ev) cudaEventDestroy(h->batch_ev);
     h->batch_ev = nullptr;
@@ -657,6 +665,39 @@ int mfcfd_fpi_step(mfcfd_handle *h, int32_t t, double *res_new, double *residue)
     return rc;
 }
 
+int mfcfd_launch(mfcfd_handle *h, int32_t t0, int32_t iters) {
+    if (!h || iters < 1) return MFCFD_ERR_ARG;
+    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+    if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
+    if (h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "a launch is already pending on this handle");
+    if (iters > h->res_cap) return fail(h, MFCFD_ERR_ARG, "at most 1024 iterations per launch");
+    CK(cudaSetDevice(h->P.device));
+    if (!h->batch_ev) CK(cudaEventCreateWithFlags(&h->batch_ev, cudaEventDisableTiming));
+    int rc = launch_chunk(h, iters, true);
+    if (rc) return rc;
+    CK(cudaEventRecord(h->batch_ev, h->stream));
+    h->pending_chunk = iters;
+    h->pending_t0 = t0;
+    return MFCFD_OK;
+}
+
+int mfcfd_complete(mfcfd_handle *h, int32_t wait, double *res_hist, int32_t *done) {
+    if (!h || !done) return MFCFD_ERR_ARG;
+    *done = 0;
+    if (!h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "no launch is pending on this handle");
+    if (!wait) {
+        const cudaError_t q = cudaEventQuery(h->batch_ev);
+        if (q == cudaErrorNotReady) return MFCFD_OK;
+        if (q != cudaSuccess) return cuda_fail(h, q, "cudaEventQuery");
+    }
+    int st = MFCFD_OK;
+    const int chunk = h->pending_chunk;
+    h->pending_chunk = 0;
+    int rc = finish_chunk(h, h->pending_t0, chunk, res_hist, &st);
+    *done = 1;
+    return rc ? rc : st;
+}
+
 int mfcfd_run(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist) {
     if (!h || iters < 0) return MFCFD_ERR_ARG;
     if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
@@ -770,6 +811,13 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
     info->chain_terms_ring = h->chain_terms[0];
     info->chain_terms_local = h->chain_terms[1];
     info->chain_terms_cross = h->chain_terms[2];
+    if (h->P.sweep_mode == MFCFD_SWEEP_CHAINS && h->P.device >= 0) {
+        const int wpb = h->stream ? h->d.ch_wpb : (h->staged ? h->staged->ch_wpb : 0);
+        const int w = h->stream ? h->d.ch_warps : (h->staged ? h->staged->ch_w : 0);
+        info->chain_slots = wpb > 0 ? w / wpb * chain_block_slots(wpb) : 0;
+        info->chain_slot_capacity = chain_slot_capacity(h->P.device);
+        if (!info->chain_warps) info->chain_warps = w;
+    }
     return MFCFD_OK;
 }
 

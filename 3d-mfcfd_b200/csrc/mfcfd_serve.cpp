@@ -4,14 +4,16 @@
  *
  * Threads: `setup_threads` workers run the host set-up of submitted clouds
  * (mfcfd_prepare) and measure their device footprint (mfcfd_device_bytes);
- * one scheduler thread owns the device side.  Each scheduler round admits
- * ready requests (first ready, first admitted) while their bytes fit the
- * budget beside the live ones, runs `chunk` iterations of every live request
- * with mfcfd_run_batch (their streams overlap on the device), and retires
- * the requests that converged, reached max_iters or failed, which frees
- * their memory for the next round's admissions.  Every request iterates in
- * whole rounds of `chunk` from t = 1, so its arithmetic, and its result, do
- * not depend on which other requests share the device.
+ * one scheduler thread owns the device side.  It admits ready requests
+ * (first ready, first admitted) while their bytes fit the budget beside the
+ * live ones, launches the next `chunk` iterations of every idle live
+ * request whose chain sweep fits beside the running ones (mfcfd_launch;
+ * their streams overlap on the device), and as each chunk completes
+ * (mfcfd_complete) retires its request if it converged, reached max_iters
+ * or failed, which frees its memory, or lets it go on.  No request waits
+ * for the others.  Every request iterates in whole chunks of `chunk` from
+ * t = 1, so its arithmetic, and its result, do not depend on which other
+ * requests share the device.
  */
 #include <algorithm>
 #include <chrono>
@@ -46,6 +48,9 @@ struct Request {
     std::vector<double> prim_out;
     std::string err;
     bool done = false;
+    int slots = 0;                    // SM slots of its chain sweep (mfcfd_info)
+    bool running = false;             // a chunk is launched and not yet completed
+    int fail = MFCFD_OK;              // status it retires with
 };
 using RequestPtr = std::shared_ptr<Request>;
 
@@ -168,7 +173,18 @@ void mfcfd_server::retire(const RequestPtr &r, int status) {
 void mfcfd_server::scheduler_loop() {
     cudaSetDevice(cfg.device);
     const int chunk = cfg.chunk;
+    std::vector<double> hist(2 * (size_t)chunk);
+    int used = 0, running = 0, capacity = 0;
+    auto wait_running = [&] {   // let every launched chunk finish (stopping)
+        for (const RequestPtr &r : live)
+            if (r->running) {
+                int32_t done = 0;
+                mfcfd_complete(r->h, 1, nullptr, &done);
+                r->running = false;
+            }
+    };
     for (;;) {
+        // admissions: ready requests in order while memory (and max_live) allow
         std::vector<RequestPtr> admit;
         {
             std::unique_lock<std::mutex> lk(mu);
@@ -194,45 +210,71 @@ void mfcfd_server::scheduler_loop() {
                 rc = mfcfd_set_prim(r->h, r->prim0.data());
                 std::vector<double>().swap(r->prim0);
             }
+            mfcfd_info info;
+            if (!rc) rc = mfcfd_get_info(r->h, &info);
             r->res.t_admit = now();
-            if (rc) retire(r, rc);
-            else live.push_back(r);
+            if (rc) {
+                retire(r, rc);
+                continue;
+            }
+            r->slots = info.chain_slots;
+            if (info.chain_slot_capacity > 0) capacity = info.chain_slot_capacity;
+            live.push_back(r);
         }
-        if (live.empty()) continue;
 
-        // one round: `chunk` iterations of every live request, overlapped
-        const int32_t count = (int32_t)live.size();
-        std::vector<mfcfd_handle *> hs(count);
-        std::vector<int32_t> t0s(count), status(count, MFCFD_OK);
-        std::vector<double> hist(2 * (size_t)chunk * count);
-        for (int32_t i = 0; i < count; ++i) {
-            hs[i] = live[i]->h;
-            t0s[i] = live[i]->t;
+        // launches: the next chunk of every idle request whose chain sweeps fit
+        // beside the running ones (one always may run)
+        std::vector<RequestPtr> failed;
+        for (const RequestPtr &r : live) {
+            if (r->running) continue;
+            if (running > 0 && used + r->slots > capacity) continue;
+            const int rc = mfcfd_launch(r->h, r->t, chunk);
+            if (rc) {
+                r->fail = rc;
+                failed.push_back(r);
+                continue;
+            }
+            r->running = true;
+            used += r->slots;
+            ++running;
         }
-        const int rc = mfcfd_run_batch(hs.data(), count, t0s.data(), chunk, hist.data(), status.data());
-        const bool per_request = std::any_of(status.begin(), status.end(), [](int v) { return v != MFCFD_OK; });
-        {
-            std::lock_guard<std::mutex> lk(mu);
-            ++st.rounds;
-            st.iterations += (int64_t)chunk * count;
-        }
-        std::vector<RequestPtr> keep;
-        for (int32_t i = 0; i < count; ++i) {
-            const RequestPtr &r = live[i];
-            int s = status[i];
-            if (rc != MFCFD_OK && !per_request) s = rc;   // a launch failed mid-round: all are suspect
+
+        // completions: each request retires or goes on by itself
+        bool any = false;
+        for (const RequestPtr &r : live) {
+            if (!r->running) continue;
+            int32_t done = 0;
+            const int rc = mfcfd_complete(r->h, 0, hist.data(), &done);
+            if (!done && rc == MFCFD_OK) continue;
+            any = true;
+            r->running = false;
+            used -= r->slots;
+            --running;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                ++st.rounds;
+                st.iterations += chunk;
+            }
             r->t += chunk;
             r->res.iters += chunk;
-            const double *last = &hist[2 * ((size_t)i * chunk + chunk - 1)];
-            r->res.res_new = last[0];
-            r->res.residue = last[1];
-            r->res.converged = s == MFCFD_OK && r->t - 1 > 2 && last[1] <= r->target;
-            if (s != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) retire(r, s);
-            else keep.push_back(r);
+            r->res.res_new = hist[2 * (size_t)(chunk - 1)];
+            r->res.residue = hist[2 * (size_t)(chunk - 1) + 1];
+            r->res.converged = rc == MFCFD_OK && r->t - 1 > 2 && r->res.residue <= r->target;
+            if (rc != MFCFD_OK) r->fail = rc;
+            if (rc != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) failed.push_back(r);
         }
-        live.swap(keep);
+        for (const RequestPtr &r : failed) {
+            retire(r, r->fail);
+            live.erase(std::find(live.begin(), live.end(), r));
+        }
+        if (!any && failed.empty() && running > 0) {
+            // nothing finished yet: wait a little, or until a request is ready
+            std::unique_lock<std::mutex> lk(mu);
+            cv_sched.wait_for(lk, std::chrono::microseconds(50), [&] { return stopping || !ready.empty(); });
+        }
     }
-    // stopping: live requests end with their last round
+    // stopping: running chunks finish, then every live request ends
+    wait_running();
     for (const RequestPtr &r : live) retire(r, MFCFD_ERR_BUSY);
     live.clear();
 }

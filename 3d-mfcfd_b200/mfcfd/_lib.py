@@ -28,7 +28,7 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
            "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch",
            "mfcfd_prepare", "mfcfd_device_bytes", "mfcfd_attach", "mfcfd_tune_chain",
-           "mfcfd_set_chain_warps",
+           "mfcfd_set_chain_warps", "mfcfd_launch", "mfcfd_complete",
            "mfcfd_server_create", "mfcfd_server_submit", "mfcfd_server_wait",
            "mfcfd_server_get_stats", "mfcfd_server_destroy",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
@@ -71,7 +71,8 @@ class Info(ctypes.Structure):
                 ("split_overflows", ctypes.c_int32), ("shared_frame", ctypes.c_int32),
                 ("device_bytes", ctypes.c_int64), ("sweep_mode", ctypes.c_int32),
                 ("chain_warps", ctypes.c_int32), ("chain_terms_ring", ctypes.c_int64),
-                ("chain_terms_local", ctypes.c_int64), ("chain_terms_cross", ctypes.c_int64)]
+                ("chain_terms_local", ctypes.c_int64), ("chain_terms_cross", ctypes.c_int64),
+                ("chain_slots", ctypes.c_int32), ("chain_slot_capacity", ctypes.c_int32)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -156,6 +157,8 @@ def lib():
     L.mfcfd_attach.argtypes = [vp]
     L.mfcfd_tune_chain.argtypes = [vp, vp, i32, i32, ctypes.POINTER(i32), vp]
     L.mfcfd_set_chain_warps.argtypes = [vp, i32, ctypes.POINTER(i32)]
+    L.mfcfd_launch.argtypes = [vp, i32, i32]
+    L.mfcfd_complete.argtypes = [vp, i32, vp, ctypes.POINTER(i32)]
     L.mfcfd_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.mfcfd_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]
     L.mfcfd_server_wait.argtypes = [vp, ctypes.c_int64, dbl, ctypes.POINTER(Result), vp]

@@ -2,8 +2,9 @@
 
 Python side of mfcfd_server_* (include/mfcfd.h).  Requests (a point cloud,
 Mach number, angle of attack) are prepared on host threads, admitted while
-their device memory fits the budget, iterate together in rounds of `chunk`
-iterations and retire when their residue reaches the target (or at
+their device memory fits the budget, iterate side by side in chunks of
+`chunk` iterations (each started as soon as its chain sweep fits on the
+device) and retire when their residue reaches the target (or at
 max_iters).  Each result equals the same request solved alone.
 """
 from __future__ import annotations

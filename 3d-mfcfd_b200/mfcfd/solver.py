@@ -111,6 +111,24 @@ class Solver:
                                                 ctypes.byref(chosen), ptr(ms)))
         return chosen.value, ms[:count if count else 4]
 
+    def launch(self, t0: int, iters: int):
+        """mfcfd_launch: queue iterations t0 .. t0+iters-1 and return."""
+        self._check(_lib.lib().mfcfd_launch(self.h, int(t0), int(iters)))
+        self._pending = (int(t0), int(iters))
+
+    def complete(self, wait: bool = True):
+        """mfcfd_complete: None while the launched iterations run (wait
+        False), else their (iters, 2) (res_new, residue) history."""
+        t0, iters = self._pending
+        hist = np.zeros((iters, 2))
+        done = ctypes.c_int32()
+        self._check(_lib.lib().mfcfd_complete(self.h, 1 if wait else 0, ptr(hist), ctypes.byref(done)))
+        if not done.value:
+            return None
+        for j in range(iters):
+            self.history.append((t0 + j, float(hist[j, 0]), float(hist[j, 1])))
+        return hist
+
     def set_chain_warps(self, warps: int) -> int:
         """mfcfd_set_chain_warps: rebuild the chain schedule for about
         `warps` warps; returns the schedule's warps."""

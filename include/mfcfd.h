@@ -146,6 +146,10 @@ typedef struct mfcfd_info {
      * shared-memory ring, global memory written by the same warp, or global
      * memory written by another warp */
     int64_t chain_terms_ring, chain_terms_local, chain_terms_cross;
+    /* CHAINS: SM slots the handle's chain sweep holds while it runs (a
+     * 4-warp block one, an 8-warp block two), and the slots all chain sweeps
+     * running at once may hold on the device (mfcfd_launch) */
+    int32_t chain_slots, chain_slot_capacity;
 } mfcfd_info;
 
 typedef struct mfcfd_handle mfcfd_handle;
@@ -193,6 +197,19 @@ int mfcfd_set_prim(mfcfd_handle *h, const double *prim);
  * GPU; returns res_new (state_update_implicit.f90:187) and residue
  * (fpi_solver.f90:38-43).  Either output pointer may be NULL. */
 int mfcfd_fpi_step(mfcfd_handle *h, int32_t t, double *res_new, double *residue);
+
+/*
+ * mfcfd_run in two halves, for a host that keeps several handles busy
+ * (the request server): mfcfd_launch queues iterations t0 .. t0+iters-1
+ * (1 <= iters <= 1024) on the handle's stream and returns; mfcfd_complete
+ * then reports whether they have finished (*done), or waits for them with
+ * wait != 0, and on completion fills res_hist (2*iters, may be NULL) as
+ * mfcfd_run does.  One launch may be pending per handle.  Chain sweeps of
+ * handles running at once must fit the device together: the launches'
+ * mfcfd_info.chain_slots may add up to chain_slot_capacity at most.
+ */
+int mfcfd_launch(mfcfd_handle *h, int32_t t0, int32_t iters);
+int mfcfd_complete(mfcfd_handle *h, int32_t wait, double *res_hist, int32_t *done);
 
 /* The q_lskum loop (q_lskum.f90:28-32) for t = t0 .. t0+iters-1 without host
  * round trips; res_hist (2*iters, may be NULL) receives (res_new, residue)
@@ -344,12 +361,14 @@ const char *mfcfd_strerror(int code);
  * whose program runs one solve).  Submitted requests are prepared on host
  * threads (mfcfd_prepare), admitted in the order they become ready while
  * their device memory fits the budget (and live < max_live), then iterate
- * together: every round runs `chunk` iterations of each live request
- * (mfcfd_run_batch), after which a request whose residue is <= its
- * residue_target, or that reached max_iters, or that failed, is retired:
- * its CL/CD are computed, its state copied out and its device memory freed
- * for the next admission.  A request's iterations do not depend on the
- * others in the mix: the same request alone gives the same bits.
+ * side by side in chunks of `chunk` iterations, each launched as soon as
+ * its chain sweep fits beside the running ones (mfcfd_launch).  When a
+ * chunk completes, a request whose residue is <= its residue_target, or
+ * that reached max_iters, or that failed, is retired: its CL/CD are
+ * computed, its state copied out and its device memory freed for the next
+ * admission; the others go on without waiting for each other.  A request's
+ * iterations do not depend on the others in the mix: the same request
+ * alone gives the same bits.
  */
 typedef struct mfcfd_server mfcfd_server;
 
@@ -395,7 +414,7 @@ typedef struct mfcfd_server_stats {
     int64_t submitted, completed, failed;
     int64_t preparing, waiting, live;      /* requests in each state now */
     int64_t bytes_live, peak_bytes_live, hbm_budget;
-    int64_t rounds, iterations;            /* rounds run; iterations summed over requests */
+    int64_t rounds, iterations;            /* chunks completed; iterations summed over requests */
     int64_t peak_live;
 } mfcfd_server_stats;
 
