@@ -115,3 +115,27 @@ def test_default_initial_state_is_the_impulsive_start(mfcfd_lib):
         r = srv.wait(rid.value, timeout=100)
         r2 = srv.wait(srv.submit(c, 0.8, 2.0, max_iters=10, residue_target=-9.0, forces=False), timeout=100)
     assert r["status"] == 0 and np.allclose(r["prim"], r2["prim"], rtol=1e-12, atol=1e-14)
+
+
+def test_malformed_request_fails_alone(mfcfd_lib):
+    """A request whose connectivity names a point that does not exist
+    fails in set-up with MFCFD_ERR_ARG; the requests beside it complete
+    with the same bits as alone."""
+    import copy
+    from mfcfd import cloud, serve
+    good = cloud.small_sphere(6, 100, r1=1.5, seed=3)
+    bad = copy.deepcopy(good)
+    bad.conn = bad.conn.copy()
+    bad.conn[5, 0] = bad.n + 7
+    with serve.Server(chunk=10) as srv:
+        ids = [srv.submit(good, 0.6, 1.0, max_iters=20, residue_target=-9.0),
+               srv.submit(bad, 0.6, 1.0, max_iters=20, residue_target=-9.0),
+               srv.submit(good, 0.6, 1.0, max_iters=20, residue_target=-9.0)]
+        res = [srv.wait(i, timeout=120) for i in ids]
+        st = srv.stats()
+    assert res[1]["status"] == 1 and "prim" not in res[1]
+    assert res[0]["status"] == 0 and res[2]["status"] == 0
+    assert np.array_equal(res[0]["prim"], res[2]["prim"])
+    assert st["failed"] == 1 and st["completed"] == 2
+    alone = serve.solve_alone(good, 0.6, 1.0, 10, 20, -9.0)
+    assert np.array_equal(res[0]["prim"], alone["prim"])
