@@ -27,7 +27,7 @@ def _cloud_arrays(cloud: PointCloud):
 
 class Server:
     def __init__(self, device: int = 0, max_live: int = 0, setup_threads: int = 2, chunk: int = 20,
-                 hbm_budget: int = 0, chain_percent: int = 0):
+                 hbm_budget: int = 0, chain_percent: int = 100):
         cfg = _lib.ServerConfig(device=device, max_live=max_live, setup_threads=setup_threads,
                                 chunk=chunk, hbm_budget=hbm_budget, chain_percent=chain_percent)
         self.chunk = chunk
