@@ -57,7 +57,8 @@ def test_admission_by_device_memory(mfcfd_lib):
     b = serve.device_bytes(c, 0.8, 2.0)
     big = cloud.small_sphere(12, 400, r1=2.2, seed=6)
     assert serve.device_bytes(big, 0.8, 2.0) > int(1.5 * b)
-    with serve.Server(chunk=10, hbm_budget=int(1.5 * b)) as srv:
+    # chain_percent 0: each request keeps the schedule device_bytes measured
+    with serve.Server(chunk=10, hbm_budget=int(1.5 * b), chain_percent=0) as srv:
         ids = [srv.submit(c, 0.8, 2.0, max_iters=20, residue_target=-9.0) for _ in range(3)]
         bad = srv.submit(big, 0.8, 2.0, max_iters=20)
         res = [srv.wait(i, timeout=300) for i in ids]
