@@ -14,13 +14,17 @@ module mfcfd_interface
         MFCFD_FIELD_DELUP = 7, MFCFD_FIELD_DELUN = 8, MFCFD_FIELD_DINV = 9
     integer(c_int32_t), parameter :: MFCFD_SWEEP_DATAFLOW = 0, MFCFD_SWEEP_LEVELS = 1, &
         MFCFD_SWEEP_CHAINS = 2
+    integer(c_int32_t), parameter :: MFCFD_PRECISION_FP64 = 0, MFCFD_PRECISION_MIXED = 1
+    integer(c_int32_t), parameter :: MFCFD_UPDATE_IMPLICIT = 0, MFCFD_UPDATE_EXPLICIT = 1
+    integer(c_int32_t), parameter :: MFCFD_SWEEPS_ALIAS = 0, MFCFD_SWEEPS_BACKUP = 1
 
     ! mirror of struct mfcfd_params
     type, bind(C) :: mfcfd_params
         real(c_double) :: power, vl_const, cfl
         real(c_double) :: rho_inf, u1_inf, u2_inf, u3_inf, pr_inf
         integer(c_int32_t) :: inner_iterations, split_capacity, precision, device, sweep_mode
-        integer(c_int32_t) :: reserved(7)
+        integer(c_int32_t) :: update_variant, sweep_variant, chain_warps, gpu_setup, graphs
+        integer(c_int32_t) :: reserved(2)
     end type mfcfd_params
 
     interface
@@ -101,6 +105,91 @@ module mfcfd_interface
             real(c_double), intent(out) :: res_new
             integer(c_int) :: rc
         end function mfcfd_residual_noalloc
+
+        ! the reference program's files (meshfree_solver.f90:20-37)
+        function mfcfd_count_input_points(path, n) result(rc) bind(C, name="mfcfd_count_input_points")
+            import :: c_char, c_int32_t, c_int
+            character(kind=c_char), dimension(*), intent(in) :: path
+            integer(c_int32_t), intent(out) :: n
+            integer(c_int) :: rc
+        end function mfcfd_count_input_points
+
+        function mfcfd_read_input_point_data(path, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, &
+                                             min_dist) result(rc) bind(C, name="mfcfd_read_input_point_data")
+            import :: c_char, c_int32_t, c_double, c_int
+            character(kind=c_char), dimension(*), intent(in) :: path
+            integer(c_int32_t), value :: n
+            integer(c_int32_t), intent(out) :: status(*), nbhs(*), conn(27, *)
+            real(c_double), intent(out) :: x(*), y(*), z(*), tan1(3, *), tan2(3, *), nor(3, *), min_dist(*)
+            integer(c_int) :: rc
+        end function mfcfd_read_input_point_data
+
+        function mfcfd_read_stored_solution(path, n, prim) result(rc) bind(C, name="mfcfd_read_stored_solution")
+            import :: c_char, c_int32_t, c_double, c_int
+            character(kind=c_char), dimension(*), intent(in) :: path
+            integer(c_int32_t), value :: n
+            real(c_double), intent(out) :: prim(5, *)
+            integer(c_int) :: rc
+        end function mfcfd_read_stored_solution
+
+        function mfcfd_print_primal_output(h, dir) result(rc) bind(C, name="mfcfd_print_primal_output")
+            import :: c_ptr, c_char, c_int
+            type(c_ptr), value :: h
+            character(kind=c_char), dimension(*), intent(in) :: dir
+            integer(c_int) :: rc
+        end function mfcfd_print_primal_output
+
+        function mfcfd_write_residue(path, t0, iters, res_hist, append) result(rc) bind(C, name="mfcfd_write_residue")
+            import :: c_char, c_int32_t, c_double, c_int
+            character(kind=c_char), dimension(*), intent(in) :: path
+            integer(c_int32_t), value :: t0, iters, append
+            real(c_double), intent(in) :: res_hist(2, *)
+            integer(c_int) :: rc
+        end function mfcfd_write_residue
+
+        ! CL/CD of the current state (no counterpart in the reference)
+        function mfcfd_forces(h, wall_area, ref_area, cl, cd, force) result(rc) bind(C, name="mfcfd_forces")
+            import :: c_ptr, c_double, c_int
+            type(c_ptr), value :: h
+            real(c_double), value :: wall_area, ref_area
+            real(c_double), intent(out) :: cl, cd, force(3)
+            integer(c_int) :: rc
+        end function mfcfd_forces
+
+        ! several clouds at once: hs(count) handles, t0(count), res_hist(2, iters, count)
+        function mfcfd_run_batch(hs, count, t0, iters, res_hist, status) result(rc) bind(C, name="mfcfd_run_batch")
+            import :: c_ptr, c_int32_t, c_double, c_int
+            type(c_ptr), intent(in) :: hs(*)
+            integer(c_int32_t), value :: count, iters
+            integer(c_int32_t), intent(in) :: t0(*)
+            real(c_double), intent(out) :: res_hist(*)
+            integer(c_int32_t), intent(out) :: status(*)
+            integer(c_int) :: rc
+        end function mfcfd_run_batch
+
+        function mfcfd_tune_chain(h, candidates, count, iters, chosen, ms) result(rc) bind(C, name="mfcfd_tune_chain")
+            import :: c_ptr, c_int32_t, c_int
+            type(c_ptr), value :: h, candidates, ms
+            integer(c_int32_t), value :: count, iters
+            integer(c_int32_t), intent(out) :: chosen
+            integer(c_int) :: rc
+        end function mfcfd_tune_chain
+
+        function mfcfd_launch(h, t0, iters) result(rc) bind(C, name="mfcfd_launch")
+            import :: c_ptr, c_int32_t, c_int
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: t0, iters
+            integer(c_int) :: rc
+        end function mfcfd_launch
+
+        function mfcfd_complete(h, wait, res_hist, done) result(rc) bind(C, name="mfcfd_complete")
+            import :: c_ptr, c_int32_t, c_double, c_int
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: wait
+            real(c_double), intent(out) :: res_hist(*)
+            integer(c_int32_t), intent(out) :: done
+            integer(c_int) :: rc
+        end function mfcfd_complete
 
         function mfcfd_destroy(h) result(rc) bind(C, name="mfcfd_destroy")
             import :: c_ptr, c_int
