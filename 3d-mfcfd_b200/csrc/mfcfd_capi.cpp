@@ -284,11 +284,11 @@ int finish_chunk(mfcfd_handle *h, int32_t t0, int chunk, double *res_hist, int *
 
 // Rebuild the chain schedule for about `want` warps on the handle's
 // topology and replace its device copy (the term records are re-marked, so
-// they are copied again).  Returns the warps of the new schedule, or < 0.
-int apply_chain_schedule(mfcfd_handle *h, int want) {
+// they are copied again); *warps receives the new schedule's warps.
+int apply_chain_schedule(mfcfd_handle *h, int want, int *warps) {
     int wpb = 0, blocks = 0;
     const int w = chain_shape(h->P.device, want, &wpb, &blocks);
-    if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident") * -1;
+    if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
     ChainSchedule S;
     build_chain_schedule(h->T, w, S);
     DevCloud &d = h->d;
@@ -300,7 +300,7 @@ int apply_chain_schedule(mfcfd_handle *h, int want) {
         dfree(h, d.ch_items[dir]);
         if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir])) || (rc = upload(h, &d.ch_pts[dir], S.pts[dir])) ||
             (rc = upload(h, &d.ch_own[dir], S.owner[dir])) || (rc = upload(h, &d.ch_items[dir], S.items[dir])))
-            return -rc;
+            return rc;
     }
     const std::vector<SweepEntry> *ents[2] = {&h->T.fwd_ent, &h->T.bwd_ent};
     const SweepEntry *dents[2] = {d.fwd_ent, d.bwd_ent};
@@ -308,7 +308,7 @@ int apply_chain_schedule(mfcfd_handle *h, int want) {
         if (!ents[dir]->empty()) {
             cudaError_t e = cudaMemcpyAsync((void *)dents[dir], ents[dir]->data(), sizeof(SweepEntry) * ents[dir]->size(),
                                             cudaMemcpyHostToDevice, h->stream);
-            if (e != cudaSuccess) return -cuda_fail(h, e, "cudaMemcpyAsync");
+            if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpyAsync");
         }
     d.ch_warps = w;
     d.ch_wpb = wpb;
@@ -317,8 +317,9 @@ int apply_chain_schedule(mfcfd_handle *h, int want) {
     h->chain_terms[1] = S.terms_local;
     h->chain_terms[2] = S.terms_cross;
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return -cuda_fail(h, e, "cudaStreamSynchronize");
-    return w;
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamSynchronize");
+    *warps = w;
+    return MFCFD_OK;
 }
 
 int run_iterations(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist) {
@@ -935,8 +936,9 @@ int mfcfd_set_chain_warps(mfcfd_handle *h, int32_t warps, int32_t *actual) {
     if (h->P.sweep_mode != MFCFD_SWEEP_CHAINS) return fail(h, MFCFD_ERR_ARG, "the handle does not use the chain schedule");
     if (h->stream) {
         CK(cudaSetDevice(h->P.device));
-        const int w = apply_chain_schedule(h, warps);
-        if (w < 0) return -w;
+        int w = 0;
+        const int rc = apply_chain_schedule(h, warps, &w);
+        if (rc) return rc;
         if (actual) *actual = w;
         return MFCFD_OK;
     }
@@ -982,11 +984,8 @@ int mfcfd_tune_chain(mfcfd_handle *h, const int32_t *candidates, int32_t count, 
     double best_ms = 0.0;
     int best = start;
     for (size_t c = 0; c < wants.size() && rc == MFCFD_OK; ++c) {
-        const int w = apply_chain_schedule(h, wants[c]);
-        if (w < 0) {
-            rc = -w;
-            break;
-        }
+        int w = 0;
+        if ((rc = apply_chain_schedule(h, wants[c], &w))) break;
         // one untimed iteration, then `iters` timed ones, from the saved state
         if ((rc = mfcfd_set_state(h, prim.data(), delu.data(), res_old))) break;
         if ((rc = run_iterations(h, 3, 1, nullptr))) break;
@@ -1007,8 +1006,9 @@ int mfcfd_tune_chain(mfcfd_handle *h, const int32_t *candidates, int32_t count, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     // keep the fastest schedule (or the original one after a failure)
-    const int w = apply_chain_schedule(h, rc == MFCFD_OK ? best : start);
-    if (w < 0 && rc == MFCFD_OK) rc = -w;
+    int w = 0;
+    const int ra = apply_chain_schedule(h, rc == MFCFD_OK ? best : start, &w);
+    if (ra && rc == MFCFD_OK) rc = ra;
     const int rs = mfcfd_set_state(h, prim.data(), delu.data(), res_old);
     if (rc == MFCFD_OK) rc = rs;
     *chosen = h->d.ch_warps;
