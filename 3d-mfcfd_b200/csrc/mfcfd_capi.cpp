@@ -464,14 +464,13 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
     for (size_t j = 0; j < st->conn.size(); ++j) st->conn[j] = conn[j] > 0 ? conn[j] - 1 : 0;
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
         // about twice the widest level in warps, all co-resident; the
-        // schedule also marks the entry lists, so it precedes their upload
+        // schedule itself is built when first needed (attach_device), so a
+        // warp count set before then costs one build
         if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
         const int want = P.chain_warps > 0 ? P.chain_warps : 2 * h->T.max_level_width;
         int blocks = 0;
         st->ch_w = chain_shape(P.device, want, &st->ch_wpb, &blocks);
         if (st->ch_w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
-        build_chain_schedule(h->T, st->ch_w, st->S);
-        build_pre_order(h->T, st->pre);
     }
     h->staged = std::move(st);
     return MFCFD_OK;
@@ -511,6 +510,13 @@ int attach_device(mfcfd_handle *h) {
     d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;
 
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+        // the schedule marks the entry lists, so it precedes their upload
+        mfcfd_handle::Staged &ms = *h->staged;
+        if (ms.S.warps != ms.ch_w) {
+            ms.S = ChainSchedule();
+            build_chain_schedule(h->T, ms.ch_w, ms.S);
+        }
+        if (ms.pre.empty()) build_pre_order(h->T, ms.pre);
         const ChainSchedule &S = st.S;
         d.ch_warps = st.ch_w;
         d.ch_wpb = st.ch_wpb;
@@ -948,8 +954,7 @@ int mfcfd_set_chain_warps(mfcfd_handle *h, int32_t warps, int32_t *actual) {
     int blocks = 0;
     const int w = chain_shape(h->P.device, warps, &st.ch_wpb, &blocks);
     if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
-    st.S = ChainSchedule();
-    build_chain_schedule(h->T, w, st.S);
+    st.S = ChainSchedule();   // built for w at the next dry run or attach
     st.ch_w = w;
     if (actual) *actual = w;
     return MFCFD_OK;

@@ -159,6 +159,13 @@ int prep_levels_gpu(int device, int n, const std::vector<int> &order, const std:
                     const std::vector<int32_t> &deps, std::vector<int32_t> &level, std::string &err);
 void build_pre_order(const Topology &T, std::vector<int32_t> &order);
 
+// Host threads for the set-up passes, one pool for every set-up running in
+// the process at once (the host's cores less one).  take_setup_threads
+// grants up to `want` (possibly 0); give_setup_threads returns them.  A
+// thread that runs set-ups for others (a server worker) holds one for itself.
+int take_setup_threads(int want);
+void give_setup_threads(int k);
+
 // Build everything above.  Returns MFCFD_OK or an error code with a message.
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
                    const double *y, const double *z, const double *tan1, const double *tan2,

@@ -50,6 +50,7 @@ struct Request {
     bool done = false;
     int slots = 0;                    // SM slots of its chain sweep (mfcfd_info)
     bool running = false;             // a chunk is launched and not yet completed
+    double t_launch = 0.0;            // server clock at its running chunk's launch
     int fail = MFCFD_OK;              // status it retires with
 };
 using RequestPtr = std::shared_ptr<Request>;
@@ -105,9 +106,13 @@ void mfcfd_server::worker_loop() {
         mfcfd_params P = r->P;
         P.device = cfg.device;
         mfcfd_handle *h = nullptr;
+        // this worker's own core counts against the set-up pool, so that the
+        // passes of requests prepared at once share the host's cores
+        const int own = mfcfd::take_setup_threads(1);
         int rc = mfcfd_prepare(&P, r->n, r->status.data(), r->x.data(), r->y.data(), r->z.data(), r->tan1.data(),
                                r->tan2.data(), r->nor.data(), r->nbhs.data(), r->conn.data(), r->min_dist.data(),
                                &h);
+        mfcfd::give_setup_threads(own);
         if (!rc && cfg.chain_percent > 0 && P.sweep_mode == MFCFD_SWEEP_CHAINS) {
             mfcfd_info info;
             rc = mfcfd_get_info(h, &info);
@@ -175,6 +180,15 @@ void mfcfd_server::scheduler_loop() {
     const int chunk = cfg.chunk;
     std::vector<double> hist(2 * (size_t)chunk);
     int used = 0, running = 0, capacity = 0;
+    double t_acc = now();   // slot-seconds and busy time accumulated up to here
+    auto account = [&] {
+        const double t = now(), dt = t - t_acc;
+        t_acc = t;
+        std::lock_guard<std::mutex> lk(mu);
+        if (running > 0) st.busy_s += dt;
+        st.slot_s += used * dt;
+        st.slot_capacity = capacity;
+    };
     auto wait_running = [&] {   // let every launched chunk finish (stopping)
         for (const RequestPtr &r : live)
             if (r->running) {
@@ -184,11 +198,15 @@ void mfcfd_server::scheduler_loop() {
             }
     };
     for (;;) {
+        account();
         // admissions: ready requests in order while memory (and max_live) allow
         std::vector<RequestPtr> admit;
         {
             std::unique_lock<std::mutex> lk(mu);
-            if (live.empty()) cv_sched.wait(lk, [&] { return stopping || !ready.empty(); });
+            if (live.empty()) {
+                cv_sched.wait(lk, [&] { return stopping || !ready.empty(); });
+                t_acc = now();   // idle, with nothing running
+            }
             if (stopping) break;
             int64_t bytes = st.bytes_live;
             while (!ready.empty()) {
@@ -234,7 +252,9 @@ void mfcfd_server::scheduler_loop() {
                 failed.push_back(r);
                 continue;
             }
+            account();
             r->running = true;
+            r->t_launch = now();
             used += r->slots;
             ++running;
         }
@@ -247,6 +267,8 @@ void mfcfd_server::scheduler_loop() {
             const int rc = mfcfd_complete(r->h, 0, hist.data(), &done);
             if (!done && rc == MFCFD_OK) continue;
             any = true;
+            account();
+            r->res.run_s += now() - r->t_launch;
             r->running = false;
             used -= r->slots;
             --running;

@@ -39,24 +39,32 @@ namespace {
 
 struct Moments { double xx, yy, zz, xy, yz, zx; };
 
-// f(i) for i in [0, n) on the host's cores; every i writes only its own
-// outputs, so the result does not depend on the thread count.
+// at least this many indices per thread: starting a thread costs about as
+// much as a few thousand of the cheapest passes' indices
+constexpr int PAR_GRAIN = 4096;
+
+// f(i) for i in [0, n) on the calling thread and up to 31 threads from the
+// set-up pool; every i writes only its own outputs, so the result does not
+// depend on the thread count.
 template <class F>
 void parallel_for(int n, const F &f) {
-    unsigned nt = std::thread::hardware_concurrency();
-    nt = nt < 1 ? 1 : (nt > 32 ? 32 : nt);
-    if (n < (1 << 16) || nt == 1) {
+    const int want = std::min(31, n / PAR_GRAIN - 1);
+    const int extra = want > 0 ? take_setup_threads(want) : 0;
+    if (extra == 0) {
         for (int i = 0; i < n; ++i) f(i);
         return;
     }
-    const int chunk = (n + (int)nt - 1) / (int)nt;
+    const int nt = extra + 1;
+    const int chunk = (n + nt - 1) / nt;
     std::vector<std::thread> th;
-    for (unsigned t = 0; t < nt; ++t) {
-        const int a = (int)t * chunk, b = std::min(n, a + chunk);
+    for (int t = 1; t < nt; ++t) {
+        const int a = t * chunk, b = std::min(n, a + chunk);
         if (a >= b) break;
         th.emplace_back([a, b, &f] { for (int i = a; i < b; ++i) f(i); });
     }
+    for (int i = 0; i < std::min(n, chunk); ++i) f(i);
     for (auto &t : th) t.join();
+    give_setup_threads(extra);
 }
 
 inline double det_of(const Moments &m) {
@@ -78,7 +86,26 @@ inline double numerator(int axis, const Moments &m, double fx, double fy, double
          + m.zx * (m.xy * fy - fx * m.yy);
 }
 
+std::atomic<int> &setup_pool() {
+    static std::atomic<int> pool{std::max(0, (int)std::thread::hardware_concurrency() - 1)};
+    return pool;
+}
+
 }  // namespace
+
+int take_setup_threads(int want) {
+    std::atomic<int> &pool = setup_pool();
+    int avail = pool.load(std::memory_order_relaxed);
+    while (avail > 0) {
+        const int got = std::min(avail, want);
+        if (pool.compare_exchange_weak(avail, avail - got, std::memory_order_relaxed)) return got;
+    }
+    return 0;
+}
+
+void give_setup_threads(int k) {
+    if (k > 0) setup_pool().fetch_add(k, std::memory_order_relaxed);
+}
 
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
                    const double *y, const double *z, const double *tan1, const double *tan2,
@@ -127,18 +154,12 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         T.split_cnt[d].assign(n, 0);
     }
     T.split_overflows = 0;
-    auto push = [&](int d, int i, int k) {   // i 0-based point, k 1-based id
-        int c = ++T.split_cnt[d][i];
-        if (c > cap) T.split_overflows++;
-        T.split[d][(size_t)i * cap + (c - 1)] = k;
-    };
-    auto classify = [&](int i, int cls) {
+    // a point's neighbours in list order: put(d, k) for each list d that
+    // takes neighbour k (1-based id); interior points split all three axes,
+    // wall and outer points put every neighbour in their one z list
+    auto classify = [&](int i, int cls, auto &&put) {
         const double xi = x[i], yi = y[i], zi = z[i];
         const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
-        // counts reset as the reference does (outer points leave zpos alone)
-        T.split_cnt[0][i] = 0; T.split_cnt[1][i] = 0; T.split_cnt[2][i] = 0;
-        T.split_cnt[3][i] = 0; T.split_cnt[5][i] = 0;
-        if (cls == CLS_INTERIOR) T.split_cnt[4][i] = 0;
         for (int r = 0; r < nbhs[i]; ++r) {
             int k = conn[(size_t)i * MAX_CONN + r];
             double delx = x[k - 1] - xi, dely = y[k - 1] - yi, delz = z[k - 1] - zi;
@@ -146,68 +167,57 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
             if (cls == CLS_INTERIOR) {
                 double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
-                if (dels <= 0.0) push(0, i, k);
-                if (dels > 0.0) push(1, i, k);
-                if (delt <= 0.0) push(2, i, k);
-                if (delt > 0.0) push(3, i, k);
-                if (deln <= 0.0) push(4, i, k);
-                if (deln > 0.0) push(5, i, k);
+                if (dels <= 0.0) put(0, k);
+                if (dels > 0.0) put(1, k);
+                if (delt <= 0.0) put(2, k);
+                if (delt > 0.0) put(3, k);
+                if (deln <= 0.0) put(4, k);
+                if (deln > 0.0) put(5, k);
             } else {
-                if (dels <= 0.0) push(0, i, k);
-                if (dels >= 0.0) push(1, i, k);
-                if (delt <= 0.0) push(2, i, k);
-                if (delt >= 0.0) push(3, i, k);
-                push(cls == CLS_WALL ? 5 : 4, i, k);
+                if (dels <= 0.0) put(0, k);
+                if (dels >= 0.0) put(1, k);
+                if (delt <= 0.0) put(2, k);
+                if (delt >= 0.0) put(3, k);
+                put(cls == CLS_WALL ? 5 : 4, k);
             }
         }
     };
     if (!split_done) {
-        // No list longer than the capacity: every point writes only its own
-        // column, so the points are classified in parallel (a counting pass,
-        // then the fill).  Otherwise the reference's order decides what the
-        // overflow overwrites, and the points go one at a time in that order.
-        std::vector<uint8_t> longer(n, 0);
+        // The reference stores list d of point i at i*cap + j, and an entry
+        // past the capacity lands in the following points' storage; it visits
+        // the interior, then the wall, then the outer points, each once from
+        // zeroed counts, so a cell ends with the value of its last writer in
+        // that order.  Each point first fills its own cells (in parallel);
+        // then the spilled entries, in that order, replace an owner's value
+        // that came earlier or was never written.
+        std::vector<int32_t> visit(n, -1);
+        int at = 0;
+        for (const std::vector<int32_t> *cl : {&T.interior_idx, &T.wall_idx, &T.outer_idx})
+            for (int i : *cl) visit[i] = at++;
+        std::vector<uint8_t> spills(n, 0);
         parallel_for(n, [&](int i) {
             const int c = T.cls[i];
             if (c != CLS_INTERIOR && c != CLS_WALL && c != CLS_OUTER) return;
-            int cn[NDIR] = {0, 0, 0, 0, 0, 0};
-            const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
-            for (int r = 0; r < nbhs[i]; ++r) {
-                const int k = conn[(size_t)i * MAX_CONN + r];
-                const double delx = x[k - 1] - x[i], dely = y[k - 1] - y[i], delz = z[k - 1] - z[i];
-                const double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
-                const double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
-                if (c == CLS_INTERIOR) {
-                    const double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
-                    if (dels <= 0.0) ++cn[0];
-                    if (dels > 0.0) ++cn[1];
-                    if (delt <= 0.0) ++cn[2];
-                    if (delt > 0.0) ++cn[3];
-                    if (deln <= 0.0) ++cn[4];
-                    if (deln > 0.0) ++cn[5];
-                } else {
-                    if (dels <= 0.0) ++cn[0];
-                    if (dels >= 0.0) ++cn[1];
-                    if (delt <= 0.0) ++cn[2];
-                    if (delt >= 0.0) ++cn[3];
-                    ++cn[c == CLS_WALL ? 5 : 4];
-                }
-            }
-            for (int d = 0; d < NDIR; ++d)
-                if (cn[d] > cap) longer[i] = 1;
-        });
-        bool any_longer = false;
-        for (int i = 0; i < n && !any_longer; ++i) any_longer = longer[i] != 0;
-        if (!any_longer) {
-            parallel_for(n, [&](int i) {
-                const int c = T.cls[i];
-                if (c == CLS_INTERIOR || c == CLS_WALL || c == CLS_OUTER) classify(i, c);
+            classify(i, c, [&](int d, int k) {
+                const int j = T.split_cnt[d][i]++;
+                if (j < cap) T.split[d][(size_t)i * cap + j] = k;
+                else spills[i] = 1;
             });
-        } else {
-            for (int i : T.interior_idx) classify(i, CLS_INTERIOR);
-            for (int i : T.wall_idx) classify(i, CLS_WALL);
-            for (int i : T.outer_idx) classify(i, CLS_OUTER);
-        }
+        });
+        for (int d = 0; d < NDIR; ++d)
+            for (int i = 0; i < n; ++i) T.split_overflows += std::max(0, T.split_cnt[d][i] - cap);
+        for (const std::vector<int32_t> *cl : {&T.interior_idx, &T.wall_idx, &T.outer_idx})
+            for (int s : *cl) {
+                if (!spills[s]) continue;
+                int cnt[NDIR] = {0, 0, 0, 0, 0, 0};
+                classify(s, T.cls[s], [&](int d, int k) {
+                    const int j = cnt[d]++;
+                    if (j < cap) return;
+                    const int t = s + j / cap, slot = j % cap;   // the cell's owner and its slot
+                    const bool owner_wrote = t < n && visit[t] >= 0 && T.split_cnt[d][t] > slot;
+                    if (!owner_wrote || visit[t] < visit[s]) T.split[d][(size_t)s * cap + j] = k;
+                });
+            }
     }
 
     // ---- alias breadth-first search (implicit_aliasing.f90:21-42).
