@@ -97,14 +97,16 @@ class Result(ctypes.Structure):
     _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int32), ("converged", ctypes.c_int32),
                 ("iters", ctypes.c_int32), ("n", ctypes.c_int32)] + \
         [(f, ctypes.c_double) for f in ("res_new", "residue", "cl", "cd", "t_submit", "t_ready",
-                                        "t_admit", "t_done")] + [("device_bytes", ctypes.c_int64)]
+                                        "t_admit", "t_done")] + [("device_bytes", ctypes.c_int64),
+                                                                 ("run_s", ctypes.c_double)]
 
 
 class ServerStats(ctypes.Structure):
     """mfcfd_server_stats (include/mfcfd.h)."""
     _fields_ = [(f, ctypes.c_int64) for f in (
         "submitted", "completed", "failed", "preparing", "waiting", "live", "bytes_live",
-        "peak_bytes_live", "hbm_budget", "rounds", "iterations", "peak_live")]
+        "peak_bytes_live", "hbm_budget", "rounds", "iterations", "peak_live", "slot_capacity")] + \
+        [("busy_s", ctypes.c_double), ("slot_s", ctypes.c_double)]
 
 
 class MfcfdError(RuntimeError):

@@ -505,6 +505,7 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
             srv.wait(srv.submit(clouds[small], 0.5, 0.0, max_iters=args.serve_chunk, residue_target=-99.0,
                                 precision=precision))
             replicas.barrier()
+            st0 = srv.stats()
             t0 = time.perf_counter()
             ids = []
             for ta, (ci, m, a) in zip(arrivals, reqs):
@@ -516,6 +517,8 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
             res = [srv.wait(i) for i in ids]
             wall = time.perf_counter() - t0
             st = srv.stats()
+            for k in ("busy_s", "slot_s"):   # the stream's share, not the warm-up's
+                st[k] -= st0[k]
         return res, replicas.max_over_ranks(wall, device="cuda"), st
 
     res_m, wall_m, st_m = run(_lib.PRECISION_MIXED, 0)
@@ -532,6 +535,13 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
                                 device=local_rank)
         errs.append((abs(res_m[j]["cl"] - ref["cl"]), abs(res_m[j]["cd"] - ref["cd"])))
     conv = sum(1 for r in res_m if r["converged"])
+
+    def phases(res):
+        # host preparation, wait for HBM / SM slots, time on the GPU
+        return {"prepare": float(np.mean([r["t_ready"] - r["t_submit"] for r in res])),
+                "admit_wait": float(np.mean([r["t_admit"] - r["t_ready"] for r in res])),
+                "solve": float(np.mean([r["t_done"] - r["t_admit"] for r in res])),
+                "of_which_running": float(np.mean([r["run_s"] for r in res]))}
     pts = [clouds[ci].n for ci, _, _ in reqs]
     return {"value": total / wall_m, "unit": "solves/s", "requests": len(reqs),
             "config": {"workload": "serve", "requests": len(reqs), "rate_per_s": args.serve_rate,
@@ -539,10 +549,15 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
                        "residue_target": args.serve_target, "max_iters": args.serve_max_iters,
                        "chunk": args.serve_chunk, "precision": "mixed",
                        "parallelism": f"replicas x{world}"},
-            "latency_s": lat, "converged": conv, "failed": sum(1 for r in res_m if r["status"]),
+            "latency_s": lat, "latency_phases_mean_s": phases(res_m), "converged": conv, "failed": sum(1 for r in res_m if r["status"]),
             "iterations_mean": float(np.mean([r["iters"] for r in res_m])),
             "peak_live": st_m["peak_live"], "peak_bytes_live": st_m["peak_bytes_live"],
-            "fp64_one_at_a_time": {"value": total / wall_b, "unit": "solves/s", "latency_s": lat_b},
+            # seconds with a chunk on the GPU, and the chain-sweep slots held,
+            # over the stream's wall time (slot_capacity slots in all)
+            "gpu_busy_frac": st_m["busy_s"] / wall_m,
+            "slot_occupancy": st_m["slot_s"] / (st_m["slot_capacity"] * wall_m) if st_m["slot_capacity"] else None,
+            "fp64_one_at_a_time": {"value": total / wall_b, "unit": "solves/s", "latency_s": lat_b,
+                                   "latency_phases_mean_s": phases(res_b)},
             "speedup_vs_fp64_one_at_a_time": wall_b / wall_m,
             "fp64_resolve_sample": {"requests": k, "max_abs_dCL": max(e[0] for e in errs),
                                     "max_abs_dCD": max(e[1] for e in errs)},

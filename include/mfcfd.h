@@ -408,6 +408,7 @@ typedef struct mfcfd_result {
     double cl, cd;            /* 0 unless areas were given */
     double t_submit, t_ready, t_admit, t_done;   /* seconds on the server's clock */
     int64_t device_bytes;
+    double run_s;             /* seconds its chunks ran: launch to observed completion, summed */
 } mfcfd_result;
 
 typedef struct mfcfd_server_stats {
@@ -416,6 +417,9 @@ typedef struct mfcfd_server_stats {
     int64_t bytes_live, peak_bytes_live, hbm_budget;
     int64_t rounds, iterations;            /* chunks completed; iterations summed over requests */
     int64_t peak_live;
+    int64_t slot_capacity;                 /* chain-sweep slots of the device (0 before the first admission) */
+    double busy_s;                         /* seconds with at least one chunk running */
+    double slot_s;                         /* occupied slots integrated over time (slot-seconds) */
 } mfcfd_server_stats;
 
 int mfcfd_server_create(const mfcfd_server_config *cfg, mfcfd_server **out);

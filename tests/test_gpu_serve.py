@@ -36,9 +36,14 @@ def test_results_equal_alone_and_in_the_mix(mfcfd_lib, target, max_iters):
         st = srv.stats()
     assert st["completed"] == len(cases) and st["failed"] == 0 and st["live"] == 0
     assert st["peak_live"] >= 2            # they did share the device
+    # utilisation: busy time and held slots accumulate; a request runs only
+    # between its admission and its retirement
+    assert st["slot_capacity"] > 0 and 0 < st["busy_s"] and 0 < st["slot_s"]
+    assert st["slot_s"] <= st["slot_capacity"] * st["busy_s"] * (1 + 1e-9)
     for (c, m, a, kw), r in zip(cases, res):
         alone = serve.solve_alone(c, m, a, chunk, max_iters, target, **kw)
         assert r["status"] == 0
+        assert 0 < r["run_s"] <= r["t_done"] - r["t_admit"]
         assert r["iters"] == alone["iters"] and bool(r["converged"]) == alone["converged"]
         assert np.array_equal(r["prim"], alone["prim"])
         assert r["res_new"] == alone["res_new"] and r["residue"] == alone["residue"]
