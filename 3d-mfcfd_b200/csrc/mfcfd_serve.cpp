@@ -4,14 +4,16 @@
  *
  * Threads: `setup_threads` workers run the host set-up of submitted clouds
  * (mfcfd_prepare) and measure their device footprint (mfcfd_device_bytes);
- * one scheduler thread owns the device side.  It admits ready requests
+ * one scheduler thread launches and polls.  It admits ready requests
  * (first ready, first admitted) while their bytes fit the budget beside the
  * live ones, launches the next `chunk` iterations of every idle live
  * request whose chain sweep fits beside the running ones (mfcfd_launch;
  * their streams overlap on the device), and as each chunk completes
- * (mfcfd_complete) retires its request if it converged, reached max_iters
- * or failed, which frees its memory, or lets it go on.  No request waits
- * for the others.  Every request iterates in whole chunks of `chunk` from
+ * (mfcfd_complete) lets the request go on, or hands it back for retirement
+ * if it converged, reached max_iters or failed.  The workers also attach
+ * admitted requests (uploads, allocation) and retire finished ones (state
+ * copy-out, freeing), before any set-up, so the scheduler thread spends
+ * its time on launches and completions.  No request waits for the others.  Every request iterates in whole chunks of `chunk` from
  * t = 1, so its arithmetic, and its result, do not depend on which other
  * requests share the device.
  */
@@ -49,6 +51,7 @@ struct Request {
     std::string err;
     bool done = false;
     int slots = 0;                    // SM slots of its chain sweep (mfcfd_info)
+    int slot_capacity = 0;            // the device's chain slots (mfcfd_info)
     bool running = false;             // a chunk is launched and not yet completed
     double t_launch = 0.0;            // server clock at its running chunk's launch
     int fail = MFCFD_OK;              // status it retires with
@@ -64,6 +67,10 @@ struct mfcfd_server {
     std::condition_variable cv_setup, cv_sched, cv_done;
     std::deque<RequestPtr> to_prepare;   // submitted, not yet taken by a worker
     std::deque<RequestPtr> ready;        // prepared, in the order they became ready
+    std::deque<RequestPtr> to_attach;    // admitted (memory reserved), for a worker to attach
+    std::deque<RequestPtr> attached;     // attached, for the scheduler to take live
+    std::deque<RequestPtr> to_retire;    // finished, for a worker to retire
+    uint64_t events = 0;                 // bumped when the scheduler has something new to do
     std::map<int64_t, RequestPtr> all;   // every request not yet returned by wait
     std::vector<RequestPtr> live;        // scheduler thread only
     int64_t next_id = 1;
@@ -95,13 +102,41 @@ struct mfcfd_server {
 void mfcfd_server::worker_loop() {
     for (;;) {
         RequestPtr r;
+        enum { RETIRE, ATTACH, PREPARE } job;
         {
             std::unique_lock<std::mutex> lk(mu);
-            cv_setup.wait(lk, [&] { return stopping || !to_prepare.empty(); });
+            cv_setup.wait(lk, [&] {
+                return stopping || !to_retire.empty() || !to_attach.empty() || !to_prepare.empty();
+            });
             if (stopping) return;
-            r = to_prepare.front();
-            to_prepare.pop_front();
-            ++preparing;
+            // freeing memory first, then the requests already admitted
+            std::deque<RequestPtr> &q = !to_retire.empty() ? to_retire : !to_attach.empty() ? to_attach : to_prepare;
+            job = &q == &to_retire ? RETIRE : &q == &to_attach ? ATTACH : PREPARE;
+            r = q.front();
+            q.pop_front();
+            if (job == PREPARE) ++preparing;
+        }
+        if (job == RETIRE) {
+            retire(r, r->fail);
+            continue;
+        }
+        if (job == ATTACH) {
+            int rc = mfcfd_attach(r->h);
+            if (!rc) rc = mfcfd_set_prim(r->h, r->prim0.data());
+            std::vector<double>().swap(r->prim0);
+            mfcfd_info info;
+            if (!rc) rc = mfcfd_get_info(r->h, &info);
+            if (rc) {
+                retire(r, rc);
+                continue;
+            }
+            r->slots = info.chain_slots;
+            r->slot_capacity = info.chain_slot_capacity;
+            std::lock_guard<std::mutex> lk(mu);
+            attached.push_back(r);
+            ++events;
+            cv_sched.notify_one();
+            continue;
         }
         mfcfd_params P = r->P;
         P.device = cfg.device;
@@ -147,13 +182,15 @@ void mfcfd_server::worker_loop() {
             r->h = h;
             r->bytes = bytes;
             ready.push_back(r);
+            ++events;
             cv_sched.notify_one();
         }
     }
 }
 
-// Copy out the state and forces of a live request, free its device memory
-// and record the result (scheduler thread).
+// Copy out the state and forces of an admitted request, free its device
+// memory and record the result (a worker; the scheduler thread when
+// stopping).
 void mfcfd_server::retire(const RequestPtr &r, int status) {
     if (r->h) {
         if (status == MFCFD_OK && r->wall_area > 0.0 && r->ref_area > 0.0) {
@@ -173,6 +210,8 @@ void mfcfd_server::retire(const RequestPtr &r, int status) {
     st.bytes_live -= r->bytes;
     --n_live;
     finish_locked(r, status);
+    ++events;   // memory freed: waiting requests may fit
+    cv_sched.notify_one();
 }
 
 void mfcfd_server::scheduler_loop() {
@@ -199,57 +238,51 @@ void mfcfd_server::scheduler_loop() {
     };
     for (;;) {
         account();
-        // admissions: ready requests in order while memory (and max_live) allow
-        std::vector<RequestPtr> admit;
+        // admissions: ready requests in order while memory (and max_live)
+        // allow, handed to the workers to attach; attached ones go live
+        std::vector<RequestPtr> now_live;
+        uint64_t seen = 0;
         {
             std::unique_lock<std::mutex> lk(mu);
-            if (live.empty()) {
-                cv_sched.wait(lk, [&] { return stopping || !ready.empty(); });
-                t_acc = now();   // idle, with nothing running
-            }
             if (stopping) break;
+            seen = events;
             int64_t bytes = st.bytes_live;
+            int admitted = 0;
             while (!ready.empty()) {
                 const RequestPtr &r = ready.front();
-                if (cfg.max_live > 0 && (int64_t)(live.size() + admit.size()) >= cfg.max_live) break;
+                if (cfg.max_live > 0 && n_live >= cfg.max_live) break;
                 if (bytes + r->bytes > cfg.hbm_budget) break;
                 bytes += r->bytes;
-                admit.push_back(r);
+                r->res.t_admit = now();
+                to_attach.push_back(r);
                 ready.pop_front();
+                ++n_live;
+                ++admitted;
             }
+            if (admitted) cv_setup.notify_all();
             st.bytes_live = bytes;
-            n_live += (int64_t)admit.size();
             st.peak_bytes_live = std::max(st.peak_bytes_live, st.bytes_live);
             st.peak_live = std::max(st.peak_live, n_live);
+            now_live.assign(attached.begin(), attached.end());
+            attached.clear();
         }
-        for (const RequestPtr &r : admit) {
-            int rc = mfcfd_attach(r->h);
-            if (!rc) {
-                rc = mfcfd_set_prim(r->h, r->prim0.data());
-                std::vector<double>().swap(r->prim0);
-            }
-            mfcfd_info info;
-            if (!rc) rc = mfcfd_get_info(r->h, &info);
-            r->res.t_admit = now();
-            if (rc) {
-                retire(r, rc);
-                continue;
-            }
-            r->slots = info.chain_slots;
-            if (info.chain_slot_capacity > 0) capacity = info.chain_slot_capacity;
+        for (const RequestPtr &r : now_live) {
+            if (r->slot_capacity > 0) capacity = r->slot_capacity;
             live.push_back(r);
         }
 
         // launches: the next chunk of every idle request whose chain sweeps fit
         // beside the running ones (one always may run)
-        std::vector<RequestPtr> failed;
+        std::vector<RequestPtr> finished;
+        bool progress = !now_live.empty();
         for (const RequestPtr &r : live) {
             if (r->running) continue;
             if (running > 0 && used + r->slots > capacity) continue;
             const int rc = mfcfd_launch(r->h, r->t, chunk);
+            progress = true;
             if (rc) {
                 r->fail = rc;
-                failed.push_back(r);
+                finished.push_back(r);
                 continue;
             }
             account();
@@ -259,14 +292,13 @@ void mfcfd_server::scheduler_loop() {
             ++running;
         }
 
-        // completions: each request retires or goes on by itself
-        bool any = false;
+        // completions: each request goes on by itself, or is retired
         for (const RequestPtr &r : live) {
             if (!r->running) continue;
             int32_t done = 0;
             const int rc = mfcfd_complete(r->h, 0, hist.data(), &done);
             if (!done && rc == MFCFD_OK) continue;
-            any = true;
+            progress = true;
             account();
             r->res.run_s += now() - r->t_launch;
             r->running = false;
@@ -283,16 +315,25 @@ void mfcfd_server::scheduler_loop() {
             r->res.residue = hist[2 * (size_t)(chunk - 1) + 1];
             r->res.converged = rc == MFCFD_OK && r->t - 1 > 2 && r->res.residue <= r->target;
             if (rc != MFCFD_OK) r->fail = rc;
-            if (rc != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) failed.push_back(r);
+            if (rc != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) finished.push_back(r);
         }
-        for (const RequestPtr &r : failed) {
-            retire(r, r->fail);
-            live.erase(std::find(live.begin(), live.end(), r));
+        if (!finished.empty()) {
+            for (const RequestPtr &r : finished) live.erase(std::find(live.begin(), live.end(), r));
+            std::lock_guard<std::mutex> lk(mu);
+            for (const RequestPtr &r : finished) to_retire.push_back(r);
+            cv_setup.notify_all();
         }
-        if (!any && failed.empty() && running > 0) {
-            // nothing finished yet: wait a little, or until a request is ready
+        if (!progress) {
+            // nothing to do: poll the running chunks again shortly, or sleep
+            // until a request is ready, attached or retired
             std::unique_lock<std::mutex> lk(mu);
-            cv_sched.wait_for(lk, std::chrono::microseconds(50), [&] { return stopping || !ready.empty(); });
+            auto changed = [&] { return stopping || events != seen; };
+            if (running > 0) {
+                cv_sched.wait_for(lk, std::chrono::microseconds(50), changed);
+            } else {
+                cv_sched.wait(lk, changed);
+                t_acc = now();   // idle, with nothing running
+            }
         }
     }
     // stopping: running chunks finish, then every live request ends
@@ -419,8 +460,10 @@ int mfcfd_server_destroy(mfcfd_server *s) {
     s->cv_sched.notify_all();
     for (std::thread &w : s->workers) w.join();
     s->scheduler.join();
-    for (const RequestPtr &r : s->ready)
-        if (r->h) mfcfd_destroy(r->h);
+    // requests between the threads when they stopped
+    for (auto *q : {&s->ready, &s->to_attach, &s->attached, &s->to_retire})
+        for (const RequestPtr &r : *q)
+            if (r->h) mfcfd_destroy(r->h);
     delete s;
     return MFCFD_OK;
 }
