@@ -821,7 +821,8 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
     if (h->P.sweep_mode == MFCFD_SWEEP_CHAINS && h->P.device >= 0) {
         const int wpb = h->stream ? h->d.ch_wpb : (h->staged ? h->staged->ch_wpb : 0);
         const int w = h->stream ? h->d.ch_warps : (h->staged ? h->staged->ch_w : 0);
-        info->chain_slots = wpb > 0 ? w / wpb * chain_block_slots(wpb) : 0;
+        info->chain_slots =
+            wpb > 0 ? w / wpb * chain_block_slots(h->P.device, wpb, h->P.precision == MFCFD_PRECISION_MIXED) : 0;
         info->chain_slot_capacity = chain_slot_capacity(h->P.device);
         if (!info->chain_warps) info->chain_warps = w;
     }
@@ -893,7 +894,10 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
     }
     auto slots_of = [&](int32_t i) {
         const DevCloud &d = hs[i]->d;
-        return d.sweep_mode == MFCFD_SWEEP_CHAINS ? d.ch_warps / d.ch_wpb * chain_block_slots(d.ch_wpb) : 0;
+        return d.sweep_mode == MFCFD_SWEEP_CHAINS
+                   ? d.ch_warps / d.ch_wpb *
+                         chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision == MFCFD_PRECISION_MIXED)
+                   : 0;
     };
     int used = 0;
     while (!ready.empty() || !running.empty()) {

@@ -160,7 +160,7 @@ int prep_levels_gpu(int device, int n, const std::vector<int> &order, const std:
 void build_pre_order(const Topology &T, std::vector<int32_t> &order);
 
 // Host threads for the set-up passes, one pool for every set-up running in
-// the process at once (the host's cores less one).  take_setup_threads
+// the process at once (the host's cores less two).  take_setup_threads
 // grants up to `want` (possibly 0); give_setup_threads returns them.  A
 // thread that runs set-ups for others (a server worker) holds one for itself.
 int take_setup_threads(int want);
@@ -259,10 +259,12 @@ int reduction_blocks(int n);
 int chain_shape(int device, int want, int *wpb, int *blocks);
 // Per-device launch set-up (kernel attributes), done before a stream capture.
 void prepare_launches(int device);
-// Chain-sweep blocks that may run at once, in slots: a 4-warp block takes
-// one, an 8-warp block two (see k_sweep_chain).
+// Chain-sweep blocks that may run at once, in slots of a sixth of an SM: a
+// block takes 6 / (its blocks per SM, at most 3), i.e. 2 for a 4-warp block
+// of the mixed-precision sweep (three per SM), 3 for a 4-warp block of the
+// FP64 sweep, 6 for an 8-warp block; see k_sweep_chain.
 int chain_slot_capacity(int device);
-inline int chain_block_slots(int wpb) { return wpb == 8 ? 2 : 1; }
+int chain_block_slots(int device, int wpb, bool mixed);
 // File formats of the reference program (mfcfd_io.cpp).  Handle-less calls
 // leave their message in g_io_err (mfcfd_last_error(NULL)).
 extern thread_local std::string g_io_err;

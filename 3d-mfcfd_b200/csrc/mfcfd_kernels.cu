@@ -992,18 +992,25 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
 // set-up, topological order).  The stage of the next point is copied in
 // while the current one is processed (two stage buffers).
 //
-// Residency: an SM holds two 4-warp blocks or one 8-warp block (shared
-// memory and registers allow no more), i.e. two "slots", and the chain
-// blocks running at once (one cloud, or a wave of a batch) take at most
-// 2 * (SMs - CH_FREE_SMS) slots.  So all of them fit together, and at least
-// 2 * CH_FREE_SMS slots stay free, each on an SM with room for a block of
-// the concurrent flux kernel, whose outputs the forward sweep polls for
-// (the flux kernel never waits, so the blocks it holds are released):
-// every poll ends.
+// Residency: an SM holds three 4-warp blocks of the mixed-precision sweep
+// (71 KB of shared memory each; at most 168 registers, which the launch
+// bounds below ask for), two 4-warp blocks of the FP64 sweep (226
+// registers) or one 8-warp block; in slots of a sixth of an SM, 2, 3 or 6
+// (chain_block_slots).  The chain blocks running at once (one cloud, or the
+// handles of a batch) take at most 6 * (SMs - CH_FREE_SMS) slots.  So all of
+// them fit together, and at least CH_FREE_SMS SMs' worth of room stays
+// free for blocks of the concurrent flux kernels, whose outputs the forward
+// sweeps poll for (a flux kernel never waits, so the blocks it holds are
+// released): every poll ends.
 constexpr int CH_FREE_SMS = 16;
 
 template <int WPB, typename R>
-__global__ void __launch_bounds__(WPB * 32, 1) k_sweep_chain(DevCloud d, int forward) {
+constexpr int chain_min_blocks() {
+    return (WPB == 4 && std::is_same<R, float>::value) ? 3 : 1;
+}
+
+template <int WPB, typename R>
+__global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, R>()) k_sweep_chain(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char *smb = reinterpret_cast<char *>(smem) + warp * CHAIN_SMEM_BYTES;
@@ -1039,6 +1046,8 @@ template <int WPB>
 static int chain_smem() {
     return WPB * CHAIN_SMEM_BYTES;
 }
+// three 4-warp blocks per SM: 228 KB of shared memory, 1 KB of it reserved per block
+static_assert(3 * (4 * CHAIN_SMEM_BYTES + 1024) <= 228 * 1024, "three 4-warp chain blocks per SM");
 
 // ---------------------------------------------------------------- state update
 
@@ -1264,6 +1273,15 @@ static void set_attributes(int device) {
     cudaFuncSetAttribute(k_sweep_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SWEEP_WARPS * SWEEP_SMEM_BYTES);
     cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize, DF_WARPS * SWEEP_SMEM_BYTES);
+    // the chain blocks' residency assumes the largest shared-memory carveout
+    cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(k_sweep_chain<8, double>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(k_sweep_chain<8, float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
     cudaFuncSetAttribute(k_sweep_chain<8, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
@@ -1276,7 +1294,34 @@ void prepare_launches(int device) { set_attributes(device); }
 int chain_slot_capacity(int device) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    return 2 * (sms - CH_FREE_SMS);
+    return 6 * (sms - CH_FREE_SMS);
+}
+
+int chain_block_slots(int device, int wpb, bool mixed) {
+    static std::mutex mu;
+    static int cache[256][2][2] = {};
+    if (device < 0 || device >= 256) return 6;
+    const int w8 = wpb == 8 ? 1 : 0, m = mixed ? 1 : 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (cache[device][w8][m]) return cache[device][w8][m];
+    }
+    set_attributes(device);
+    int per_sm = 0;
+    cudaError_t e;
+    if (w8)
+        e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, float>, 256, chain_smem<8>())
+                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, double>, 256, chain_smem<8>());
+    else
+        e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, float>, 128, chain_smem<4>())
+                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double>, 128, chain_smem<4>());
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        per_sm = 1;
+    }
+    per_sm = per_sm < 1 ? 1 : (per_sm > 3 ? 3 : per_sm);
+    std::lock_guard<std::mutex> lock(mu);
+    return cache[device][w8][m] = 6 / per_sm;
 }
 
 int chain_shape(int device, int want, int *wpb, int *blocks) {

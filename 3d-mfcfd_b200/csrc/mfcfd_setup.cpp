@@ -86,8 +86,10 @@ inline double numerator(int axis, const Moments &m, double fx, double fy, double
          + m.zx * (m.xy * fy - fx * m.yy);
 }
 
+// the host's cores less two: one for the calling thread, one for a thread
+// that keeps a device busy meanwhile (the request server's scheduler)
 std::atomic<int> &setup_pool() {
-    static std::atomic<int> pool{std::max(0, (int)std::thread::hardware_concurrency() - 1)};
+    static std::atomic<int> pool{std::max(0, (int)std::thread::hardware_concurrency() - 2)};
     return pool;
 }
 
