@@ -1273,14 +1273,10 @@ static void set_attributes(int device) {
     cudaFuncSetAttribute(k_sweep_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SWEEP_WARPS * SWEEP_SMEM_BYTES);
     cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize, DF_WARPS * SWEEP_SMEM_BYTES);
-    // the chain blocks' residency assumes the largest shared-memory carveout
-    cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    cudaFuncSetAttribute(k_sweep_chain<8, double>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
+    // three 4-warp blocks of the mixed-precision sweep per SM need the largest
+    // shared-memory carveout; the other variants leave the choice to the
+    // driver, which keeps more L1 for their loads and the flux kernel's
     cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    cudaFuncSetAttribute(k_sweep_chain<8, float>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
     cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
     cudaFuncSetAttribute(k_sweep_chain<8, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
