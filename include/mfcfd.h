@@ -146,9 +146,10 @@ typedef struct mfcfd_info {
      * shared-memory ring, global memory written by the same warp, or global
      * memory written by another warp */
     int64_t chain_terms_ring, chain_terms_local, chain_terms_cross;
-    /* CHAINS: SM slots the handle's chain sweep holds while it runs (a
-     * 4-warp block one, an 8-warp block two), and the slots all chain sweeps
-     * running at once may hold on the device (mfcfd_launch) */
+    /* CHAINS: slots (sixths of an SM) the handle's chain sweep holds while it
+     * runs (a 4-warp block 2 in mixed precision, 3 in FP64; an 8-warp block
+     * 6), and the slots all chain sweeps running at once may hold on the
+     * device (mfcfd_launch) */
     int32_t chain_slots, chain_slot_capacity;
 } mfcfd_info;
 
