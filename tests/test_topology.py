@@ -162,3 +162,22 @@ def test_supersonic_points_are_swept_copies(oracle_lib):
     assert np.array_equal(cs, co) and np.array_equal(ls, lo)
     for direction in (0, 1):
         _level_check(s, c, direction)
+
+
+@pytest.mark.parametrize("capacity", [22, 20])
+def test_overflowing_lists_split_on_several_threads(oracle_lib, capacity):
+    """Lists longer than the storage spill into the following points' cells,
+    and the reference's visiting order decides which value a cell keeps.  At
+    15,000 points the split runs on several host threads (own cells first,
+    then the spilled entries in that order); the effective lists still equal
+    the oracle's."""
+    from mfcfd import cloud
+    c = cloud.shell_cloud(10, 1500, r1=2.0, seed=77)
+    assert c.n >= 2 * 4096
+    s = _solver(c, split_capacity=capacity)
+    assert s.info()["split_overflows"] > 0
+    o = oracle_lib.Oracle(c, 0.4, 0.0, split_capacity=capacity)
+    cs, ls = s.stencils(27)
+    co, lo = o.stencils(27)
+    assert np.array_equal(cs, co) and np.array_equal(ls, lo)
+    assert all(np.array_equal(x, y) for x, y in zip(s.alias(), o.alias()))
