@@ -71,7 +71,7 @@ namespace {
 
 const char *kStrerr[] = {"ok", "bad argument", "CUDA error", "stencil too wide",
                          "singular least-squares system", "non-finite residual",
-                         "unsupported input", "out of device memory", "device wait timed out",
+                         "unsupported input", "out of memory", "device wait timed out",
                          "file input/output error", "request not finished"};
 
 int fail(mfcfd_handle *h, int code, const std::string &msg) {
@@ -429,16 +429,18 @@ int create_impl(const mfcfd_params *params, int32_t n, const int32_t *status, co
         *out = h;
         return MFCFD_ERR_ARG;
     }
-    int rc = build_topology(P, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, h->T, h->err);
-    *out = h;
-    if (rc) return rc;
-    if (P.device < 0) return MFCFD_OK;   // host-only handle: set-up results, no device state
-    if ((rc = stage_host(h, x, y, z, tan1, tan2, nor, nbhs, conn))) return rc;
-    if (attach) {
-        if ((rc = attach_device(h))) return rc;
-        h->staged.reset();
-    }
-    return MFCFD_OK;
+    *out = h;   // also on failure: it holds the message
+    return host_guard(&h->err, [&]() -> int {
+        int rc = build_topology(P, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, h->T, h->err);
+        if (rc) return rc;
+        if (P.device < 0) return MFCFD_OK;   // host-only handle: set-up results, no device state
+        if ((rc = stage_host(h, x, y, z, tan1, tan2, nor, nbhs, conn))) return rc;
+        if (attach) {
+            if ((rc = attach_device(h))) return rc;
+            h->staged.reset();
+        }
+        return MFCFD_OK;
+    });
 }
 
 // Host copies of the inputs the device needs, in the device layout, and the
@@ -599,473 +601,523 @@ int mfcfd_create(const mfcfd_params *params, int32_t n, const int32_t *status, c
                  const double *y, const double *z, const double *tan1, const double *tan2,
                  const double *nor, const int32_t *nbhs, const int32_t *conn,
                  const double *min_dist, mfcfd_handle **out) {
-    return create_impl(params, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, out, true);
+    return host_guard(nullptr, [&]() -> int {
+        return create_impl(params, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, out, true);
+    });
 }
 
 int mfcfd_prepare(const mfcfd_params *params, int32_t n, const int32_t *status, const double *x,
                   const double *y, const double *z, const double *tan1, const double *tan2,
                   const double *nor, const int32_t *nbhs, const int32_t *conn,
                   const double *min_dist, mfcfd_handle **out) {
-    if (!out) return MFCFD_ERR_ARG;
-    *out = nullptr;
-    if (!params || params->device < 0) return MFCFD_ERR_ARG;
-    return create_impl(params, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, out, false);
+    return host_guard(nullptr, [&]() -> int {
+        if (!out) return MFCFD_ERR_ARG;
+        *out = nullptr;
+        if (!params || params->device < 0) return MFCFD_ERR_ARG;
+        return create_impl(params, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, out, false);
+    });
 }
 
 int mfcfd_device_bytes(mfcfd_handle *h, int64_t *bytes) {
-    if (!h || !bytes) return MFCFD_ERR_ARG;
-    if (h->stream) {
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !bytes) return MFCFD_ERR_ARG;
+        if (h->stream) {
+            *bytes = h->bytes;
+            return MFCFD_OK;
+        }
+        if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no staged cloud");
+        // the attach sequence with allocation counted, not performed
+        h->dry = true;
+        h->bytes = 0;
+        const int rc = attach_device(h);
         *bytes = h->bytes;
-        return MFCFD_OK;
-    }
-    if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no staged cloud");
-    // the attach sequence with allocation counted, not performed
-    h->dry = true;
-    h->bytes = 0;
-    const int rc = attach_device(h);
-    *bytes = h->bytes;
-    h->dry = false;
-    h->bytes = 0;
-    std::memset(&h->d, 0, sizeof h->d);
-    h->allocs.clear();
-    return rc;
+        h->dry = false;
+        h->bytes = 0;
+        std::memset(&h->d, 0, sizeof h->d);
+        h->allocs.clear();
+        return rc;
+    });
 }
 
 int mfcfd_attach(mfcfd_handle *h) {
-    if (!h) return MFCFD_ERR_ARG;
-    if (h->stream) return MFCFD_OK;
-    if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no staged cloud");
-    const int rc = attach_device(h);
-    if (rc) {
-        release(h);
-        return rc;
-    }
-    h->staged.reset();
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h) return MFCFD_ERR_ARG;
+        if (h->stream) return MFCFD_OK;
+        if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no staged cloud");
+        const int rc = attach_device(h);
+        if (rc) {
+            release(h);
+            return rc;
+        }
+        h->staged.reset();
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_set_prim(mfcfd_handle *h, const double *prim) {
-    if (!h || !prim) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    size_t n5 = (size_t)h->d.n * 5;
-    CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemsetAsync(h->d.dUp, 0, n5 * 8, h->stream));
-    CK(cudaMemsetAsync(h->d.dUn, 0, n5 * 8, h->stream));
-    DevCloud dc = h->d;
-    dc.U = h->U_buf[h->cur];
-    dc.q = h->q_buf[h->cur];
-    CK(launch_conserved_q(dc, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    h->last = h->cur;
-    h->res_old = h->res_new = h->residue = 0.0;
-    h->have_state = true;
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !prim) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        size_t n5 = (size_t)h->d.n * 5;
+        CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemsetAsync(h->d.dUp, 0, n5 * 8, h->stream));
+        CK(cudaMemsetAsync(h->d.dUn, 0, n5 * 8, h->stream));
+        DevCloud dc = h->d;
+        dc.U = h->U_buf[h->cur];
+        dc.q = h->q_buf[h->cur];
+        CK(launch_conserved_q(dc, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->last = h->cur;
+        h->res_old = h->res_new = h->residue = 0.0;
+        h->have_state = true;
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_fpi_step(mfcfd_handle *h, int32_t t, double *res_new, double *residue) {
-    if (!h) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    double hist[2];
-    int rc = run_iterations(h, t, 1, hist);
-    if (res_new) *res_new = hist[0];
-    if (residue) *residue = hist[1];
-    return rc;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        double hist[2];
+        int rc = run_iterations(h, t, 1, hist);
+        if (res_new) *res_new = hist[0];
+        if (residue) *residue = hist[1];
+        return rc;
+    });
 }
 
 int mfcfd_launch(mfcfd_handle *h, int32_t t0, int32_t iters) {
-    if (!h || iters < 1) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
-    if (h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "a launch is already pending on this handle");
-    if (iters > h->res_cap) return fail(h, MFCFD_ERR_ARG, "at most 1024 iterations per launch");
-    CK(cudaSetDevice(h->P.device));
-    if (!h->batch_ev) CK(cudaEventCreateWithFlags(&h->batch_ev, cudaEventDisableTiming));
-    int rc = launch_chunk(h, iters, true);
-    if (rc) return rc;
-    CK(cudaEventRecord(h->batch_ev, h->stream));
-    h->pending_chunk = iters;
-    h->pending_t0 = t0;
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || iters < 1) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
+        if (h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "a launch is already pending on this handle");
+        if (iters > h->res_cap) return fail(h, MFCFD_ERR_ARG, "at most 1024 iterations per launch");
+        CK(cudaSetDevice(h->P.device));
+        if (!h->batch_ev) CK(cudaEventCreateWithFlags(&h->batch_ev, cudaEventDisableTiming));
+        int rc = launch_chunk(h, iters, true);
+        if (rc) return rc;
+        CK(cudaEventRecord(h->batch_ev, h->stream));
+        h->pending_chunk = iters;
+        h->pending_t0 = t0;
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_complete(mfcfd_handle *h, int32_t wait, double *res_hist, int32_t *done) {
-    if (!h || !done) return MFCFD_ERR_ARG;
-    *done = 0;
-    if (!h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "no launch is pending on this handle");
-    if (!wait) {
-        const cudaError_t q = cudaEventQuery(h->batch_ev);
-        if (q == cudaErrorNotReady) return MFCFD_OK;
-        if (q != cudaSuccess) return cuda_fail(h, q, "cudaEventQuery");
-    }
-    int st = MFCFD_OK;
-    const int chunk = h->pending_chunk;
-    h->pending_chunk = 0;
-    int rc = finish_chunk(h, h->pending_t0, chunk, res_hist, &st);
-    *done = 1;
-    return rc ? rc : st;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !done) return MFCFD_ERR_ARG;
+        *done = 0;
+        if (!h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "no launch is pending on this handle");
+        if (!wait) {
+            const cudaError_t q = cudaEventQuery(h->batch_ev);
+            if (q == cudaErrorNotReady) return MFCFD_OK;
+            if (q != cudaSuccess) return cuda_fail(h, q, "cudaEventQuery");
+        }
+        int st = MFCFD_OK;
+        const int chunk = h->pending_chunk;
+        h->pending_chunk = 0;
+        int rc = finish_chunk(h, h->pending_t0, chunk, res_hist, &st);
+        *done = 1;
+        return rc ? rc : st;
+    });
 }
 
 int mfcfd_run(mfcfd_handle *h, int32_t t0, int32_t iters, double *res_hist) {
-    if (!h || iters < 0) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    return run_iterations(h, t0, iters, res_hist);
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || iters < 0) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        return run_iterations(h, t0, iters, res_hist);
+    });
 }
 
 int mfcfd_get(mfcfd_handle *h, int32_t field, double *out) {
-    if (!h || !out) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    const DevCloud &d = h->d;
-    size_t n = (size_t)d.n;
-    const double *src = nullptr;
-    size_t w = 0;
-    switch (field) {
-    case MFCFD_FIELD_PRIM: src = d.prim; w = 5; break;
-    case MFCFD_FIELD_U: src = h->U_buf[h->last]; w = 5; break;
-    case MFCFD_FIELD_Q: src = h->q_buf[h->last]; w = 5; break;
-    case MFCFD_FIELD_QM: src = d.qm; w = 10; break;
-    case MFCFD_FIELD_DQ: src = d.dq; w = 15; break;
-    case MFCFD_FIELD_DELT: src = d.delt; w = 1; break;
-    case MFCFD_FIELD_FLUX_RES: src = d.flux_res; w = 5; break;
-    case MFCFD_FIELD_DELUP: src = d.dUp; w = 5; break;
-    case MFCFD_FIELD_DELUN: src = d.dUn; w = 5; break;
-    case MFCFD_FIELD_DINV: src = d.dinv; w = 1; break;
-    default: return fail(h, MFCFD_ERR_ARG, "unknown field");
-    }
-    CK(cudaMemcpyAsync(out, src, n * w * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !out) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        const DevCloud &d = h->d;
+        size_t n = (size_t)d.n;
+        const double *src = nullptr;
+        size_t w = 0;
+        switch (field) {
+        case MFCFD_FIELD_PRIM: src = d.prim; w = 5; break;
+        case MFCFD_FIELD_U: src = h->U_buf[h->last]; w = 5; break;
+        case MFCFD_FIELD_Q: src = h->q_buf[h->last]; w = 5; break;
+        case MFCFD_FIELD_QM: src = d.qm; w = 10; break;
+        case MFCFD_FIELD_DQ: src = d.dq; w = 15; break;
+        case MFCFD_FIELD_DELT: src = d.delt; w = 1; break;
+        case MFCFD_FIELD_FLUX_RES: src = d.flux_res; w = 5; break;
+        case MFCFD_FIELD_DELUP: src = d.dUp; w = 5; break;
+        case MFCFD_FIELD_DELUN: src = d.dUn; w = 5; break;
+        case MFCFD_FIELD_DINV: src = d.dinv; w = 1; break;
+        default: return fail(h, MFCFD_ERR_ARG, "unknown field");
+        }
+        CK(cudaMemcpyAsync(out, src, n * w * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_get_state(mfcfd_handle *h, double *prim, double *delu, double *res_old) {
-    if (!h || !prim || !delu) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    size_t n5 = (size_t)h->d.n * 5;
-    CK(cudaMemcpyAsync(prim, h->d.prim, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(delu, h->d.dUn, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    if (res_old) *res_old = h->res_old;
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !prim || !delu) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        size_t n5 = (size_t)h->d.n * 5;
+        CK(cudaMemcpyAsync(prim, h->d.prim, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(delu, h->d.dUn, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (res_old) *res_old = h->res_old;
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_set_state(mfcfd_handle *h, const double *prim, const double *delu, double res_old) {
-    if (!h || !prim || !delu) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    size_t n5 = (size_t)h->d.n * 5;
-    CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d.dUn, delu, n5 * 8, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->d.dUp, h->d.dUn, n5 * 8, cudaMemcpyDeviceToDevice, h->stream));
-    DevCloud dc = h->d;
-    dc.U = h->U_buf[h->cur];
-    dc.q = h->q_buf[h->cur];
-    CK(launch_conserved_q(dc, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    h->last = h->cur;
-    h->res_old = res_old;
-    h->have_state = true;
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !prim || !delu) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        size_t n5 = (size_t)h->d.n * 5;
+        CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d.dUn, delu, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->d.dUp, h->d.dUn, n5 * 8, cudaMemcpyDeviceToDevice, h->stream));
+        DevCloud dc = h->d;
+        dc.U = h->U_buf[h->cur];
+        dc.q = h->q_buf[h->cur];
+        CK(launch_conserved_q(dc, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->last = h->cur;
+        h->res_old = res_old;
+        h->have_state = true;
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_get_stencils(mfcfd_handle *h, int32_t *counts, int32_t *lists, int32_t width) {
-    if (!h || !counts || !lists || width < 1) return MFCFD_ERR_ARG;
-    const Topology &T = h->T;
-    if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    for (int i = 0; i < T.n; ++i)
-        for (int dd = 0; dd < NDIR; ++dd) {
-            int c = T.split_cnt[dd][i];
-            counts[(size_t)i * NDIR + dd] = c;
-            for (int j = 0; j < width; ++j)
-                lists[((size_t)i * NDIR + dd) * width + j] =
-                    j < c ? T.split[dd][(size_t)i * T.cap + j] : 0;
-        }
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !counts || !lists || width < 1) return MFCFD_ERR_ARG;
+        const Topology &T = h->T;
+        if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        for (int i = 0; i < T.n; ++i)
+            for (int dd = 0; dd < NDIR; ++dd) {
+                int c = T.split_cnt[dd][i];
+                counts[(size_t)i * NDIR + dd] = c;
+                for (int j = 0; j < width; ++j)
+                    lists[((size_t)i * NDIR + dd) * width + j] =
+                        j < c ? T.split[dd][(size_t)i * T.cap + j] : 0;
+            }
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_get_alias(mfcfd_handle *h, int32_t *alias, int32_t *point_with_alias) {
-    if (!h || !alias || !point_with_alias) return MFCFD_ERR_ARG;
-    const Topology &T = h->T;
-    if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    std::memcpy(alias, T.alias.data(), sizeof(int32_t) * T.n);
-    std::memcpy(point_with_alias, T.point_with_alias.data(), sizeof(int32_t) * T.n);
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !alias || !point_with_alias) return MFCFD_ERR_ARG;
+        const Topology &T = h->T;
+        if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        std::memcpy(alias, T.alias.data(), sizeof(int32_t) * T.n);
+        std::memcpy(point_with_alias, T.point_with_alias.data(), sizeof(int32_t) * T.n);
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level) {
-    if (!h || !level || (dir != 0 && dir != 1)) return MFCFD_ERR_ARG;
-    const Topology &T = h->T;
-    if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
-    const std::vector<int32_t> &src = dir == 0 ? T.fwd_level : T.bwd_level;
-    std::memcpy(level, src.data(), sizeof(int32_t) * T.n);
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !level || (dir != 0 && dir != 1)) return MFCFD_ERR_ARG;
+        const Topology &T = h->T;
+        if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        const std::vector<int32_t> &src = dir == 0 ? T.fwd_level : T.bwd_level;
+        std::memcpy(level, src.data(), sizeof(int32_t) * T.n);
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
-    if (!h || !info) return MFCFD_ERR_ARG;
-    const Topology &T = h->T;
-    std::memset(info, 0, sizeof *info);
-    info->n_points = T.n;
-    info->n_wall = (int32_t)T.wall_idx.size();
-    info->n_outer = (int32_t)T.outer_idx.size();
-    info->n_interior = (int32_t)T.interior_idx.size();
-    info->n_supersonic = (int32_t)(T.ss_inlet_idx.size() + T.ss_outlet_idx.size());
-    info->n_levels_forward = T.fwd_lvl_ptr.empty() ? 0 : (int32_t)T.fwd_lvl_ptr.size() - 1;
-    info->n_levels_backward = T.bwd_lvl_ptr.empty() ? 0 : (int32_t)T.bwd_lvl_ptr.size() - 1;
-    info->max_level_width = T.max_level_width;
-    info->split_overflows = T.split_overflows;
-    info->shared_frame = T.shared_frame;
-    info->device_bytes = h->bytes;
-    info->sweep_mode = h->P.sweep_mode;
-    info->chain_warps = h->d.ch_warps;
-    info->chain_terms_ring = h->chain_terms[0];
-    info->chain_terms_local = h->chain_terms[1];
-    info->chain_terms_cross = h->chain_terms[2];
-    if (h->P.sweep_mode == MFCFD_SWEEP_CHAINS && h->P.device >= 0) {
-        const int wpb = h->stream ? h->d.ch_wpb : (h->staged ? h->staged->ch_wpb : 0);
-        const int w = h->stream ? h->d.ch_warps : (h->staged ? h->staged->ch_w : 0);
-        info->chain_slots =
-            wpb > 0 ? w / wpb * chain_block_slots(h->P.device, wpb, h->P.precision == MFCFD_PRECISION_MIXED) : 0;
-        info->chain_slot_capacity = chain_slot_capacity(h->P.device);
-        if (!info->chain_warps) info->chain_warps = w;
-    }
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !info) return MFCFD_ERR_ARG;
+        const Topology &T = h->T;
+        std::memset(info, 0, sizeof *info);
+        info->n_points = T.n;
+        info->n_wall = (int32_t)T.wall_idx.size();
+        info->n_outer = (int32_t)T.outer_idx.size();
+        info->n_interior = (int32_t)T.interior_idx.size();
+        info->n_supersonic = (int32_t)(T.ss_inlet_idx.size() + T.ss_outlet_idx.size());
+        info->n_levels_forward = T.fwd_lvl_ptr.empty() ? 0 : (int32_t)T.fwd_lvl_ptr.size() - 1;
+        info->n_levels_backward = T.bwd_lvl_ptr.empty() ? 0 : (int32_t)T.bwd_lvl_ptr.size() - 1;
+        info->max_level_width = T.max_level_width;
+        info->split_overflows = T.split_overflows;
+        info->shared_frame = T.shared_frame;
+        info->device_bytes = h->bytes;
+        info->sweep_mode = h->P.sweep_mode;
+        info->chain_warps = h->d.ch_warps;
+        info->chain_terms_ring = h->chain_terms[0];
+        info->chain_terms_local = h->chain_terms[1];
+        info->chain_terms_cross = h->chain_terms[2];
+        if (h->P.sweep_mode == MFCFD_SWEEP_CHAINS && h->P.device >= 0) {
+            const int wpb = h->stream ? h->d.ch_wpb : (h->staged ? h->staged->ch_wpb : 0);
+            const int w = h->stream ? h->d.ch_warps : (h->staged ? h->staged->ch_w : 0);
+            info->chain_slots =
+                wpb > 0 ? w / wpb * chain_block_slots(h->P.device, wpb, h->P.precision == MFCFD_PRECISION_MIXED) : 0;
+            info->chain_slot_capacity = chain_slot_capacity(h->P.device);
+            if (!info->chain_warps) info->chain_warps = w;
+        }
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_get_stream(mfcfd_handle *h, void **stream) {
-    if (!h || !stream) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    *stream = (void *)h->stream;
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !stream) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        *stream = (void *)h->stream;
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_set_profiling(mfcfd_handle *h, int32_t on) {
-    if (!h) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    if (on && h->ev.empty()) {
-        h->ev.resize((size_t)h->res_cap * (MFCFD_NPHASE + 1));
-        for (auto &e : h->ev) CK(cudaEventCreate(&e));
-    }
-    h->profiling = on != 0;
-    for (double &v : h->phase_ms) v = 0.0;
-    h->prof_iters = 0;
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        if (on && h->ev.empty()) {
+            h->ev.resize((size_t)h->res_cap * (MFCFD_NPHASE + 1));
+            for (auto &e : h->ev) CK(cudaEventCreate(&e));
+        }
+        h->profiling = on != 0;
+        for (double &v : h->phase_ms) v = 0.0;
+        h->prof_iters = 0;
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters) {
-    if (!h || !ms) return MFCFD_ERR_ARG;
-    for (int p = 0; p < MFCFD_NPHASE; ++p) ms[p] = h->phase_ms[p];
-    if (iters) *iters = h->prof_iters;
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !ms) return MFCFD_ERR_ARG;
+        for (int p = 0; p < MFCFD_NPHASE; ++p) ms[p] = h->phase_ms[p];
+        if (iters) *iters = h->prof_iters;
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new) {
-    if (!h || !res_new) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    cudaError_t e = cudaSetDevice(h->P.device);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
-    return residual_noalloc(h->d, h->stream, res_new, h->err);
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !res_new) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        cudaError_t e = cudaSetDevice(h->P.device);
+        if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+        return residual_noalloc(h->d, h->stream, res_new, h->err);
+    });
 }
 
 int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, int32_t iters, double *res_hist,
                     int32_t *status) {
-    if (!hs || count < 1 || !t0 || iters < 0) return MFCFD_ERR_ARG;
-    const int dev = hs[0] ? hs[0]->P.device : -1;
-    for (int32_t i = 0; i < count; ++i) {
-        mfcfd_handle *h = hs[i];
-        if (!h || !h->stream || !h->have_state || h->P.device != dev) return MFCFD_ERR_ARG;
-        for (int32_t j = 0; j < i; ++j)
-            if (hs[j] == h) return MFCFD_ERR_ARG;   // each handle once
-        if (status) status[i] = MFCFD_OK;
-    }
-    if (cudaSetDevice(dev) != cudaSuccess) return MFCFD_ERR_CUDA;
-    const int capacity = chain_slot_capacity(dev);
-    int first_err = MFCFD_OK;
-    // Continuous scheduling on SM slots: a handle's next chunk starts as
-    // soon as its chain blocks fit beside the chunks running, and a chunk's
-    // slots return when its completion event has fired.  So all running
-    // chain blocks are always resident together (see k_sweep_chain), and no
-    // handle waits for a whole group of others to finish.
-    std::vector<int32_t> done(count, 0);
-    std::vector<int> chunk_of(count, 0);
-    std::deque<int32_t> ready;
-    std::vector<int32_t> running;
-    for (int32_t i = 0; i < count; ++i) {
-        if (iters > 0) ready.push_back(i);
-        if (!hs[i]->batch_ev && cudaEventCreateWithFlags(&hs[i]->batch_ev, cudaEventDisableTiming) != cudaSuccess)
-            return cuda_fail(hs[i], cudaGetLastError(), "cudaEventCreateWithFlags");
-    }
-    auto slots_of = [&](int32_t i) {
-        const DevCloud &d = hs[i]->d;
-        return d.sweep_mode == MFCFD_SWEEP_CHAINS
-                   ? d.ch_warps / d.ch_wpb *
-                         chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision == MFCFD_PRECISION_MIXED)
-                   : 0;
-    };
-    int used = 0;
-    while (!ready.empty() || !running.empty()) {
-        while (!ready.empty()) {
-            const int32_t i = ready.front();
-            const int sl = slots_of(i);
-            if (!running.empty() && used + sl > capacity) break;
-            ready.pop_front();
+    return host_guard(hs && count > 0 && hs[0] ? &hs[0]->err : nullptr, [&]() -> int {
+        if (!hs || count < 1 || !t0 || iters < 0) return MFCFD_ERR_ARG;
+        const int dev = hs[0] ? hs[0]->P.device : -1;
+        for (int32_t i = 0; i < count; ++i) {
             mfcfd_handle *h = hs[i];
-            const int chunk = std::min<int32_t>(iters - done[i], std::max(h->res_cap, 1));
-            int rc = launch_chunk(h, chunk, true);
-            if (rc) return rc;
-            cudaError_t e = cudaEventRecord(h->batch_ev, h->stream);
-            if (e != cudaSuccess) return cuda_fail(h, e, "cudaEventRecord");
-            chunk_of[i] = chunk;
-            used += sl;
-            running.push_back(i);
+            if (!h || !h->stream || !h->have_state || h->P.device != dev) return MFCFD_ERR_ARG;
+            for (int32_t j = 0; j < i; ++j)
+                if (hs[j] == h) return MFCFD_ERR_ARG;   // each handle once
+            if (status) status[i] = MFCFD_OK;
         }
-        // wait for the first of the running chunks to complete
-        int found = -1;
-        while (found < 0) {
-            for (size_t r = 0; r < running.size() && found < 0; ++r) {
-                const cudaError_t q = cudaEventQuery(hs[running[r]]->batch_ev);
-                if (q == cudaSuccess) found = (int)r;
-                else if (q != cudaErrorNotReady) return cuda_fail(hs[running[r]], q, "cudaEventQuery");
+        if (cudaSetDevice(dev) != cudaSuccess) return MFCFD_ERR_CUDA;
+        const int capacity = chain_slot_capacity(dev);
+        int first_err = MFCFD_OK;
+        // Continuous scheduling on SM slots: a handle's next chunk starts as
+        // soon as its chain blocks fit beside the chunks running, and a chunk's
+        // slots return when its completion event has fired.  So all running
+        // chain blocks are always resident together (see k_sweep_chain), and no
+        // handle waits for a whole group of others to finish.
+        std::vector<int32_t> done(count, 0);
+        std::vector<int> chunk_of(count, 0);
+        std::deque<int32_t> ready;
+        std::vector<int32_t> running;
+        for (int32_t i = 0; i < count; ++i) {
+            if (iters > 0) ready.push_back(i);
+            if (!hs[i]->batch_ev && cudaEventCreateWithFlags(&hs[i]->batch_ev, cudaEventDisableTiming) != cudaSuccess)
+                return cuda_fail(hs[i], cudaGetLastError(), "cudaEventCreateWithFlags");
+        }
+        auto slots_of = [&](int32_t i) {
+            const DevCloud &d = hs[i]->d;
+            return d.sweep_mode == MFCFD_SWEEP_CHAINS
+                       ? d.ch_warps / d.ch_wpb *
+                             chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision == MFCFD_PRECISION_MIXED)
+                       : 0;
+        };
+        int used = 0;
+        while (!ready.empty() || !running.empty()) {
+            while (!ready.empty()) {
+                const int32_t i = ready.front();
+                const int sl = slots_of(i);
+                if (!running.empty() && used + sl > capacity) break;
+                ready.pop_front();
+                mfcfd_handle *h = hs[i];
+                const int chunk = std::min<int32_t>(iters - done[i], std::max(h->res_cap, 1));
+                int rc = launch_chunk(h, chunk, true);
+                if (rc) return rc;
+                cudaError_t e = cudaEventRecord(h->batch_ev, h->stream);
+                if (e != cudaSuccess) return cuda_fail(h, e, "cudaEventRecord");
+                chunk_of[i] = chunk;
+                used += sl;
+                running.push_back(i);
             }
-            if (found < 0) std::this_thread::sleep_for(std::chrono::microseconds(20));
+            // wait for the first of the running chunks to complete
+            int found = -1;
+            while (found < 0) {
+                for (size_t r = 0; r < running.size() && found < 0; ++r) {
+                    const cudaError_t q = cudaEventQuery(hs[running[r]]->batch_ev);
+                    if (q == cudaSuccess) found = (int)r;
+                    else if (q != cudaErrorNotReady) return cuda_fail(hs[running[r]], q, "cudaEventQuery");
+                }
+                if (found < 0) std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
+            const int32_t i = running[found];
+            running.erase(running.begin() + found);
+            used -= slots_of(i);
+            int st = MFCFD_OK;
+            double *rh = res_hist ? res_hist + 2 * ((size_t)i * iters + done[i]) : nullptr;
+            int rc = finish_chunk(hs[i], t0[i] + done[i], chunk_of[i], rh, &st);
+            if (!rc) rc = st;
+            if (status && rc && status[i] == MFCFD_OK) status[i] = rc;
+            if (rc && first_err == MFCFD_OK) first_err = rc;
+            done[i] += chunk_of[i];
+            if (done[i] < iters) ready.push_back(i);
         }
-        const int32_t i = running[found];
-        running.erase(running.begin() + found);
-        used -= slots_of(i);
-        int st = MFCFD_OK;
-        double *rh = res_hist ? res_hist + 2 * ((size_t)i * iters + done[i]) : nullptr;
-        int rc = finish_chunk(hs[i], t0[i] + done[i], chunk_of[i], rh, &st);
-        if (!rc) rc = st;
-        if (status && rc && status[i] == MFCFD_OK) status[i] = rc;
-        if (rc && first_err == MFCFD_OK) first_err = rc;
-        done[i] += chunk_of[i];
-        if (done[i] < iters) ready.push_back(i);
-    }
-    return first_err;
+        return first_err;
+    });
 }
 
 int mfcfd_set_chain_warps(mfcfd_handle *h, int32_t warps, int32_t *actual) {
-    if (!h || warps < 1) return MFCFD_ERR_ARG;
-    if (h->P.sweep_mode != MFCFD_SWEEP_CHAINS) return fail(h, MFCFD_ERR_ARG, "the handle does not use the chain schedule");
-    if (h->stream) {
-        CK(cudaSetDevice(h->P.device));
-        int w = 0;
-        const int rc = apply_chain_schedule(h, warps, &w);
-        if (rc) return rc;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || warps < 1) return MFCFD_ERR_ARG;
+        if (h->P.sweep_mode != MFCFD_SWEEP_CHAINS) return fail(h, MFCFD_ERR_ARG, "the handle does not use the chain schedule");
+        if (h->stream) {
+            CK(cudaSetDevice(h->P.device));
+            int w = 0;
+            const int rc = apply_chain_schedule(h, warps, &w);
+            if (rc) return rc;
+            if (actual) *actual = w;
+            return MFCFD_OK;
+        }
+        if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        // a prepared handle: rebuild the staged schedule before it is attached
+        mfcfd_handle::Staged &st = *h->staged;
+        int blocks = 0;
+        const int w = chain_shape(h->P.device, warps, &st.ch_wpb, &blocks);
+        if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+        st.S = ChainSchedule();   // built for w at the next dry run or attach
+        st.ch_w = w;
         if (actual) *actual = w;
         return MFCFD_OK;
-    }
-    if (!h->staged) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    // a prepared handle: rebuild the staged schedule before it is attached
-    mfcfd_handle::Staged &st = *h->staged;
-    int blocks = 0;
-    const int w = chain_shape(h->P.device, warps, &st.ch_wpb, &blocks);
-    if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
-    st.S = ChainSchedule();   // built for w at the next dry run or attach
-    st.ch_w = w;
-    if (actual) *actual = w;
-    return MFCFD_OK;
+    });
 }
 
 int mfcfd_tune_chain(mfcfd_handle *h, const int32_t *candidates, int32_t count, int32_t iters, int32_t *chosen,
                      double *ms) {
-    if (!h || !chosen || iters < 1 || iters > 1000 || count < 0 || (count > 0 && !candidates)) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
-    if (h->d.sweep_mode != MFCFD_SWEEP_CHAINS) return fail(h, MFCFD_ERR_ARG, "tuning applies to the chain schedule");
-    CK(cudaSetDevice(h->P.device));
-    std::vector<int> wants;
-    if (count == 0) {
-        const int width = std::max(1, h->T.max_level_width);
-        for (int num : {3, 4, 6, 8}) wants.push_back(std::max(1, num * width / 2));   // 1.5x .. 4x the widest level
-    } else {
-        for (int32_t i = 0; i < count; ++i) {
-            if (candidates[i] < 1) return fail(h, MFCFD_ERR_ARG, "candidate warp counts must be positive");
-            wants.push_back(candidates[i]);
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !chosen || iters < 1 || iters > 1000 || count < 0 || (count > 0 && !candidates)) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
+        if (h->d.sweep_mode != MFCFD_SWEEP_CHAINS) return fail(h, MFCFD_ERR_ARG, "tuning applies to the chain schedule");
+        CK(cudaSetDevice(h->P.device));
+        std::vector<int> wants;
+        if (count == 0) {
+            const int width = std::max(1, h->T.max_level_width);
+            for (int num : {3, 4, 6, 8}) wants.push_back(std::max(1, num * width / 2));   // 1.5x .. 4x the widest level
+        } else {
+            for (int32_t i = 0; i < count; ++i) {
+                if (candidates[i] < 1) return fail(h, MFCFD_ERR_ARG, "candidate warp counts must be positive");
+                wants.push_back(candidates[i]);
+            }
         }
-    }
-    const size_t n5 = (size_t)h->d.n * 5;
-    std::vector<double> prim(n5), delu(n5);
-    double res_old = 0.0;
-    int rc = mfcfd_get_state(h, prim.data(), delu.data(), &res_old);
-    if (rc) return rc;
-    const int start = h->d.ch_warps;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    double best_ms = 0.0;
-    int best = start;
-    for (size_t c = 0; c < wants.size() && rc == MFCFD_OK; ++c) {
+        const size_t n5 = (size_t)h->d.n * 5;
+        std::vector<double> prim(n5), delu(n5);
+        double res_old = 0.0;
+        int rc = mfcfd_get_state(h, prim.data(), delu.data(), &res_old);
+        if (rc) return rc;
+        const int start = h->d.ch_warps;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        double best_ms = 0.0;
+        int best = start;
+        for (size_t c = 0; c < wants.size() && rc == MFCFD_OK; ++c) {
+            int w = 0;
+            if ((rc = apply_chain_schedule(h, wants[c], &w))) break;
+            // one untimed iteration, then `iters` timed ones, from the saved state
+            if ((rc = mfcfd_set_state(h, prim.data(), delu.data(), res_old))) break;
+            if ((rc = run_iterations(h, 3, 1, nullptr))) break;
+            if ((rc = mfcfd_set_state(h, prim.data(), delu.data(), res_old))) break;
+            cudaEventRecord(e0, h->stream);
+            if ((rc = run_iterations(h, 3, iters, nullptr))) break;
+            cudaEventRecord(e1, h->stream);
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            const double per = t / iters;
+            if (ms) ms[c] = per;
+            if (c == 0 || per < best_ms) {
+                best_ms = per;
+                best = w;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        // keep the fastest schedule (or the original one after a failure)
         int w = 0;
-        if ((rc = apply_chain_schedule(h, wants[c], &w))) break;
-        // one untimed iteration, then `iters` timed ones, from the saved state
-        if ((rc = mfcfd_set_state(h, prim.data(), delu.data(), res_old))) break;
-        if ((rc = run_iterations(h, 3, 1, nullptr))) break;
-        if ((rc = mfcfd_set_state(h, prim.data(), delu.data(), res_old))) break;
-        cudaEventRecord(e0, h->stream);
-        if ((rc = run_iterations(h, 3, iters, nullptr))) break;
-        cudaEventRecord(e1, h->stream);
-        cudaEventSynchronize(e1);
-        float t = 0.f;
-        cudaEventElapsedTime(&t, e0, e1);
-        const double per = t / iters;
-        if (ms) ms[c] = per;
-        if (c == 0 || per < best_ms) {
-            best_ms = per;
-            best = w;
-        }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    // keep the fastest schedule (or the original one after a failure)
-    int w = 0;
-    const int ra = apply_chain_schedule(h, rc == MFCFD_OK ? best : start, &w);
-    if (ra && rc == MFCFD_OK) rc = ra;
-    const int rs = mfcfd_set_state(h, prim.data(), delu.data(), res_old);
-    if (rc == MFCFD_OK) rc = rs;
-    *chosen = h->d.ch_warps;
-    return rc;
+        const int ra = apply_chain_schedule(h, rc == MFCFD_OK ? best : start, &w);
+        if (ra && rc == MFCFD_OK) rc = ra;
+        const int rs = mfcfd_set_state(h, prim.data(), delu.data(), res_old);
+        if (rc == MFCFD_OK) rc = rs;
+        *chosen = h->d.ch_warps;
+        return rc;
+    });
 }
 
 int mfcfd_set_wall_areas(mfcfd_handle *h, const double *area) {
-    if (!h) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    CK(cudaSetDevice(h->P.device));
-    if (!area) {
-        h->wall_area = nullptr;   // the allocation stays with the handle
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        CK(cudaSetDevice(h->P.device));
+        if (!area) {
+            h->wall_area = nullptr;   // the allocation stays with the handle
+            return MFCFD_OK;
+        }
+        if (!h->wall_area) {
+            int rc = dalloc(h, &h->wall_area, (size_t)h->d.n);
+            if (rc) return rc;
+        }
+        CK(cudaMemcpyAsync(h->wall_area, area, sizeof(double) * (size_t)h->d.n, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
         return MFCFD_OK;
-    }
-    if (!h->wall_area) {
-        int rc = dalloc(h, &h->wall_area, (size_t)h->d.n);
-        if (rc) return rc;
-    }
-    CK(cudaMemcpyAsync(h->wall_area, area, sizeof(double) * (size_t)h->d.n, cudaMemcpyHostToDevice, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    return MFCFD_OK;
+    });
 }
 
 int mfcfd_forces(mfcfd_handle *h, double wall_area, double ref_area, double *cl, double *cd, double *force) {
-    if (!h) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
-    if (!(ref_area > 0.0)) return fail(h, MFCFD_ERR_ARG, "ref_area must be positive");
-    if (!h->wall_area && (h->d.n_wall < 1 || !(wall_area > 0.0)))
-        return fail(h, MFCFD_ERR_ARG, "wall_area must be positive (or set per-point areas)");
-    CK(cudaSetDevice(h->P.device));
-    if (!h->force_out) {
-        int rc = dalloc(h, &h->force_out, 3);
-        if (rc) return rc;
-    }
-    const double each = h->d.n_wall > 0 ? wall_area / h->d.n_wall : 0.0;
-    CK(launch_forces(h->d, h->stream, each, h->wall_area, h->force_out));
-    double F[3];
-    CK(cudaMemcpyAsync(F, h->force_out, sizeof F, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    const double u1 = h->P.u1_inf, u2 = h->P.u2_inf, u3 = h->P.u3_inf;
-    const double v = std::sqrt(u1 * u1 + u2 * u2 + u3 * u3);
-    const double sa = v > 0.0 ? u2 / v : 0.0, ca = v > 0.0 ? u1 / v : 1.0;
-    const double q = 0.5 * h->P.rho_inf * v * v * ref_area;
-    if (cl) *cl = (F[0] * (-sa) + F[1] * ca) / q;
-    if (cd) *cd = (F[0] * ca + F[1] * sa) / q;
-    if (force) { force[0] = F[0]; force[1] = F[1]; force[2] = F[2]; }
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        if (!h->have_state) return fail(h, MFCFD_ERR_ARG, "no state: call mfcfd_set_prim first");
+        if (!(ref_area > 0.0)) return fail(h, MFCFD_ERR_ARG, "ref_area must be positive");
+        if (!h->wall_area && (h->d.n_wall < 1 || !(wall_area > 0.0)))
+            return fail(h, MFCFD_ERR_ARG, "wall_area must be positive (or set per-point areas)");
+        CK(cudaSetDevice(h->P.device));
+        if (!h->force_out) {
+            int rc = dalloc(h, &h->force_out, 3);
+            if (rc) return rc;
+        }
+        const double each = h->d.n_wall > 0 ? wall_area / h->d.n_wall : 0.0;
+        CK(launch_forces(h->d, h->stream, each, h->wall_area, h->force_out));
+        double F[3];
+        CK(cudaMemcpyAsync(F, h->force_out, sizeof F, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const double u1 = h->P.u1_inf, u2 = h->P.u2_inf, u3 = h->P.u3_inf;
+        const double v = std::sqrt(u1 * u1 + u2 * u2 + u3 * u3);
+        const double sa = v > 0.0 ? u2 / v : 0.0, ca = v > 0.0 ? u1 / v : 1.0;
+        const double q = 0.5 * h->P.rho_inf * v * v * ref_area;
+        if (cl) *cl = (F[0] * (-sa) + F[1] * ca) / q;
+        if (cd) *cd = (F[0] * ca + F[1] * sa) / q;
+        if (force) { force[0] = F[0]; force[1] = F[1]; force[2] = F[2]; }
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_destroy(mfcfd_handle *h) {
@@ -1086,46 +1138,56 @@ const char *mfcfd_strerror(int code) {
 }
 
 int mfcfd_count_input_points(const char *path, int32_t *n) {
-    if (!path || !n) return MFCFD_ERR_ARG;
-    return io_count_input_points(path, n);
+    return host_guard(&g_io_err, [&]() -> int {
+        if (!path || !n) return MFCFD_ERR_ARG;
+        return io_count_input_points(path, n);
+    });
 }
 
 int mfcfd_read_input_point_data(const char *path, int32_t n, int32_t *status, double *x, double *y,
                                 double *z, double *tan1, double *tan2, double *nor, int32_t *nbhs,
                                 int32_t *conn, double *min_dist) {
-    if (!path || n < 1 || !status || !x || !y || !z || !tan1 || !tan2 || !nor || !nbhs || !conn || !min_dist)
-        return MFCFD_ERR_ARG;
-    return io_read_input_point_data(path, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist);
+    return host_guard(&g_io_err, [&]() -> int {
+        if (!path || n < 1 || !status || !x || !y || !z || !tan1 || !tan2 || !nor || !nbhs || !conn || !min_dist)
+            return MFCFD_ERR_ARG;
+        return io_read_input_point_data(path, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist);
+    });
 }
 
 int mfcfd_read_stored_solution(const char *path, int32_t n, double *prim) {
-    if (!path || n < 1 || !prim) return MFCFD_ERR_ARG;
-    return io_read_stored_solution(path, n, prim);
+    return host_guard(&g_io_err, [&]() -> int {
+        if (!path || n < 1 || !prim) return MFCFD_ERR_ARG;
+        return io_read_stored_solution(path, n, prim);
+    });
 }
 
 int mfcfd_print_primal_output(mfcfd_handle *h, const char *dir) {
-    if (!h || !dir) return MFCFD_ERR_ARG;
-    if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
-    const size_t n = (size_t)h->d.n;
-    std::vector<double> x(n), y(n), z(n), prim(5 * n), flux(5 * n), dq(15 * n);
-    CK(cudaMemcpyAsync(x.data(), h->d.x, n * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(y.data(), h->d.y, n * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(z.data(), h->d.z, n * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(prim.data(), h->d.prim, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(flux.data(), h->d.flux_res, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(dq.data(), h->d.dq, 15 * n * 8, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    std::vector<int32_t> status(n);
-    for (size_t i = 0; i < n; ++i) status[i] = h->T.cls[i];   // statuses 0/1/2 are the classes
-    int rc = io_write_primal_output(dir, (int32_t)n, status.data(), x.data(), y.data(), z.data(), prim.data(),
-                                    flux.data(), dq.data());
-    if (rc) return fail(h, rc, g_io_err);
-    return MFCFD_OK;
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !dir) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        const size_t n = (size_t)h->d.n;
+        std::vector<double> x(n), y(n), z(n), prim(5 * n), flux(5 * n), dq(15 * n);
+        CK(cudaMemcpyAsync(x.data(), h->d.x, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(y.data(), h->d.y, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(z.data(), h->d.z, n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(prim.data(), h->d.prim, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(flux.data(), h->d.flux_res, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(dq.data(), h->d.dq, 15 * n * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        std::vector<int32_t> status(n);
+        for (size_t i = 0; i < n; ++i) status[i] = h->T.cls[i];   // statuses 0/1/2 are the classes
+        int rc = io_write_primal_output(dir, (int32_t)n, status.data(), x.data(), y.data(), z.data(), prim.data(),
+                                        flux.data(), dq.data());
+        if (rc) return fail(h, rc, g_io_err);
+        return MFCFD_OK;
+    });
 }
 
 int mfcfd_write_residue(const char *path, int32_t t0, int32_t iters, const double *res_hist, int32_t append) {
-    if (!path || iters < 0 || (iters > 0 && !res_hist)) return MFCFD_ERR_ARG;
-    return io_write_residue(path, t0, iters, res_hist, append);
+    return host_guard(&g_io_err, [&]() -> int {
+        if (!path || iters < 0 || (iters > 0 && !res_hist)) return MFCFD_ERR_ARG;
+        return io_write_residue(path, t0, iters, res_hist, append);
+    });
 }
 
 }  // extern "C"

@@ -4,7 +4,10 @@
 #pragma once
 
 #include <stdint.h>
+#include <new>
+#include <stdexcept>
 #include <string>
+#include <system_error>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -165,6 +168,34 @@ void build_pre_order(const Topology &T, std::vector<int32_t> &order);
 // thread that runs set-ups for others (a server worker) holds one for itself.
 int take_setup_threads(int want);
 void give_setup_threads(int k);
+
+// Runs f (the body of an entry point) and turns an exception into a status,
+// with the message in *err when err is not null, so that nothing is thrown
+// across the C ABI.  Host memory or a host thread that cannot be had gives
+// MFCFD_ERR_NOMEM.
+template <class F>
+int host_guard(std::string *err, F &&f) noexcept {
+    int code;
+    const char *msg;
+    try {
+        return f();
+    } catch (const std::bad_alloc &) {
+        code = MFCFD_ERR_NOMEM, msg = "host memory exhausted";
+    } catch (const std::length_error &) {
+        code = MFCFD_ERR_NOMEM, msg = "host allocation too large";
+    } catch (const std::system_error &) {
+        code = MFCFD_ERR_NOMEM, msg = "a host thread could not be started";
+    } catch (...) {
+        code = MFCFD_ERR_UNSUPPORTED, msg = "unexpected host failure";
+    }
+    if (err) {
+        try {
+            *err = msg;
+        } catch (...) {
+        }
+    }
+    return code;
+}
 
 // Build everything above.  Returns MFCFD_OK or an error code with a message.
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,

@@ -54,9 +54,19 @@ struct Request {
     int slot_capacity = 0;            // the device's chain slots (mfcfd_info)
     bool running = false;             // a chunk is launched and not yet completed
     double t_launch = 0.0;            // server clock at its running chunk's launch
+    bool retiring = false;            // finished: to be handed to the workers for retirement
+    bool handed = false;              // queued for retirement (no longer live)
     int fail = MFCFD_OK;              // status it retires with
 };
 using RequestPtr = std::shared_ptr<Request>;
+
+// A request's error message, kept if host memory allows.
+void set_message(std::string &to, const char *msg) noexcept {
+    try {
+        to = msg;
+    } catch (...) {
+    }
+}
 
 }  // namespace
 
@@ -97,6 +107,7 @@ struct mfcfd_server {
     void worker_loop();
     void scheduler_loop();
     void retire(const RequestPtr &r, int status);
+    int submit(const mfcfd_request *q, int64_t *id);
 };
 
 void mfcfd_server::worker_loop() {
@@ -132,10 +143,18 @@ void mfcfd_server::worker_loop() {
             }
             r->slots = info.chain_slots;
             r->slot_capacity = info.chain_slot_capacity;
-            std::lock_guard<std::mutex> lk(mu);
-            attached.push_back(r);
-            ++events;
-            cv_sched.notify_one();
+            bool queued = false;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                try {
+                    attached.push_back(r);
+                    queued = true;
+                } catch (...) {
+                }
+                ++events;
+                cv_sched.notify_one();
+            }
+            if (!queued) retire(r, MFCFD_ERR_NOMEM);
             continue;
         }
         mfcfd_params P = r->P;
@@ -157,7 +176,7 @@ void mfcfd_server::worker_loop() {
         }
         int64_t bytes = 0;
         if (!rc) rc = mfcfd_device_bytes(h, &bytes);
-        if (rc && h) r->err = mfcfd_last_error(h);
+        if (rc && h) set_message(r->err, mfcfd_last_error(h));
         // the handle holds what the device needs; the request keeps prim0
         std::vector<int32_t>().swap(r->status);
         std::vector<int32_t>().swap(r->nbhs);
@@ -166,22 +185,28 @@ void mfcfd_server::worker_loop() {
             std::vector<double>().swap(*v);
         if (!rc && bytes > cfg.hbm_budget) {
             rc = MFCFD_ERR_NOMEM;
-            r->err = "the request needs more device memory than the server's budget";
-        }
-        if (rc && h) {
-            mfcfd_destroy(h);
-            h = nullptr;
+            set_message(r->err, "the request needs more device memory than the server's budget");
         }
         std::lock_guard<std::mutex> lk(mu);
         --preparing;
         r->res.t_ready = now();
         r->res.device_bytes = bytes;
+        if (!rc) {
+            try {
+                ready.push_back(r);
+            } catch (...) {
+                rc = MFCFD_ERR_NOMEM;
+            }
+        }
+        if (rc && h) {
+            mfcfd_destroy(h);
+            h = nullptr;
+        }
         if (rc) {
             finish_locked(r, rc);
         } else {
             r->h = h;
             r->bytes = bytes;
-            ready.push_back(r);
             ++events;
             cv_sched.notify_one();
         }
@@ -198,11 +223,14 @@ void mfcfd_server::retire(const RequestPtr &r, int status) {
             if (rc) status = rc;
         }
         if (status == MFCFD_OK) {
-            r->prim_out.resize((size_t)r->n * 5);
-            const int rc = mfcfd_get(r->h, MFCFD_FIELD_PRIM, r->prim_out.data());
+            int rc = mfcfd::host_guard(&r->err, [&]() -> int {
+                r->prim_out.resize((size_t)r->n * 5);
+                return MFCFD_OK;
+            });
+            if (!rc) rc = mfcfd_get(r->h, MFCFD_FIELD_PRIM, r->prim_out.data());
             if (rc) status = rc;
         }
-        if (status != MFCFD_OK && r->err.empty()) r->err = mfcfd_last_error(r->h);
+        if (status != MFCFD_OK && r->err.empty()) set_message(r->err, mfcfd_last_error(r->h));
         mfcfd_destroy(r->h);
         r->h = nullptr;
     }
@@ -236,104 +264,128 @@ void mfcfd_server::scheduler_loop() {
                 r->running = false;
             }
     };
+    // Every allocation of a pass comes before the state it would change, so
+    // an exception (host memory exhausted) leaves each request in exactly one
+    // place; the pass is then tried again.
+    std::vector<RequestPtr> finished;
     for (;;) {
-        account();
-        // admissions: ready requests in order while memory (and max_live)
-        // allow, handed to the workers to attach; attached ones go live
-        std::vector<RequestPtr> now_live;
-        uint64_t seen = 0;
-        {
-            std::unique_lock<std::mutex> lk(mu);
-            if (stopping) break;
-            seen = events;
-            int64_t bytes = st.bytes_live;
-            int admitted = 0;
-            while (!ready.empty()) {
-                const RequestPtr &r = ready.front();
-                if (cfg.max_live > 0 && n_live >= cfg.max_live) break;
-                if (bytes + r->bytes > cfg.hbm_budget) break;
-                bytes += r->bytes;
-                r->res.t_admit = now();
-                to_attach.push_back(r);
-                ready.pop_front();
-                ++n_live;
-                ++admitted;
-            }
-            if (admitted) cv_setup.notify_all();
-            st.bytes_live = bytes;
-            st.peak_bytes_live = std::max(st.peak_bytes_live, st.bytes_live);
-            st.peak_live = std::max(st.peak_live, n_live);
-            now_live.assign(attached.begin(), attached.end());
-            attached.clear();
-        }
-        for (const RequestPtr &r : now_live) {
-            if (r->slot_capacity > 0) capacity = r->slot_capacity;
-            live.push_back(r);
-        }
-
-        // launches: the next chunk of every idle request whose chain sweeps fit
-        // beside the running ones (one always may run)
-        std::vector<RequestPtr> finished;
-        bool progress = !now_live.empty();
-        for (const RequestPtr &r : live) {
-            if (r->running) continue;
-            if (running > 0 && used + r->slots > capacity) continue;
-            const int rc = mfcfd_launch(r->h, r->t, chunk);
-            progress = true;
-            if (rc) {
-                r->fail = rc;
-                finished.push_back(r);
-                continue;
-            }
+        try {
             account();
-            r->running = true;
-            r->t_launch = now();
-            used += r->slots;
-            ++running;
-        }
-
-        // completions: each request goes on by itself, or is retired
-        for (const RequestPtr &r : live) {
-            if (!r->running) continue;
-            int32_t done = 0;
-            const int rc = mfcfd_complete(r->h, 0, hist.data(), &done);
-            if (!done && rc == MFCFD_OK) continue;
-            progress = true;
-            account();
-            r->res.run_s += now() - r->t_launch;
-            r->running = false;
-            used -= r->slots;
-            --running;
+            finished.clear();
+            finished.reserve(live.size());
+            // admissions: ready requests in order while memory (and max_live)
+            // allow, handed to the workers to attach; attached ones go live
+            uint64_t seen = 0;
+            bool progress = false;
             {
-                std::lock_guard<std::mutex> lk(mu);
-                ++st.rounds;
-                st.iterations += chunk;
+                std::unique_lock<std::mutex> lk(mu);
+                if (stopping) break;
+                seen = events;
+                int admitted = 0;
+                while (!ready.empty()) {
+                    const RequestPtr &r = ready.front();
+                    if (cfg.max_live > 0 && n_live >= cfg.max_live) break;
+                    if (st.bytes_live + r->bytes > cfg.hbm_budget) break;
+                    to_attach.push_back(r);
+                    r->res.t_admit = now();
+                    st.bytes_live += r->bytes;
+                    ++n_live;
+                    ready.pop_front();
+                    ++admitted;
+                }
+                if (admitted) cv_setup.notify_all();
+                st.peak_bytes_live = std::max(st.peak_bytes_live, st.bytes_live);
+                st.peak_live = std::max(st.peak_live, n_live);
+                live.reserve(live.size() + attached.size());
+                finished.reserve(live.size() + attached.size());
+                progress = !attached.empty();
+                for (const RequestPtr &r : attached) {
+                    if (r->slot_capacity > 0) capacity = r->slot_capacity;
+                    live.push_back(r);
+                }
+                attached.clear();
             }
-            r->t += chunk;
-            r->res.iters += chunk;
-            r->res.res_new = hist[2 * (size_t)(chunk - 1)];
-            r->res.residue = hist[2 * (size_t)(chunk - 1) + 1];
-            r->res.converged = rc == MFCFD_OK && r->t - 1 > 2 && r->res.residue <= r->target;
-            if (rc != MFCFD_OK) r->fail = rc;
-            if (rc != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) finished.push_back(r);
-        }
-        if (!finished.empty()) {
-            for (const RequestPtr &r : finished) live.erase(std::find(live.begin(), live.end(), r));
-            std::lock_guard<std::mutex> lk(mu);
-            for (const RequestPtr &r : finished) to_retire.push_back(r);
-            cv_setup.notify_all();
-        }
-        if (!progress) {
-            // nothing to do: poll the running chunks again shortly, or sleep
-            // until a request is ready, attached or retired
-            std::unique_lock<std::mutex> lk(mu);
-            auto changed = [&] { return stopping || events != seen; };
-            if (running > 0) {
-                cv_sched.wait_for(lk, std::chrono::microseconds(50), changed);
-            } else {
-                cv_sched.wait(lk, changed);
-                t_acc = now();   // idle, with nothing running
+
+            // launches: the next chunk of every idle request whose chain sweeps
+            // fit beside the running ones (one always may run)
+            for (const RequestPtr &r : live) {
+                if (r->running || r->retiring) continue;
+                if (running > 0 && used + r->slots > capacity) continue;
+                const int rc = mfcfd_launch(r->h, r->t, chunk);
+                progress = true;
+                if (rc) {
+                    r->fail = rc;
+                    r->retiring = true;
+                    continue;
+                }
+                account();
+                r->running = true;
+                r->t_launch = now();
+                used += r->slots;
+                ++running;
             }
+
+            // completions: each request goes on by itself, or is retired
+            for (const RequestPtr &r : live) {
+                if (!r->running) continue;
+                int32_t done = 0;
+                const int rc = mfcfd_complete(r->h, 0, hist.data(), &done);
+                if (!done && rc == MFCFD_OK) continue;
+                progress = true;
+                account();
+                r->res.run_s += now() - r->t_launch;
+                r->running = false;
+                used -= r->slots;
+                --running;
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    ++st.rounds;
+                    st.iterations += chunk;
+                }
+                r->t += chunk;
+                r->res.iters += chunk;
+                r->res.res_new = hist[2 * (size_t)(chunk - 1)];
+                r->res.residue = hist[2 * (size_t)(chunk - 1) + 1];
+                r->res.converged = rc == MFCFD_OK && r->t - 1 > 2 && r->res.residue <= r->target;
+                if (rc != MFCFD_OK) r->fail = rc;
+                if (rc != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) r->retiring = true;
+            }
+
+            // hand the finished requests to the workers; one that could not be
+            // queued stays live (not launched) and is handed over next pass
+            for (const RequestPtr &r : live)
+                if (r->retiring) finished.push_back(r);
+            if (!finished.empty()) {
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    try {
+                        for (const RequestPtr &r : finished) {
+                            to_retire.push_back(r);
+                            r->handed = true;
+                        }
+                    } catch (...) {
+                    }
+                    cv_setup.notify_all();
+                }
+                live.erase(std::remove_if(live.begin(), live.end(), [](const RequestPtr &r) { return r->handed; }),
+                           live.end());
+            }
+            if (!progress) {
+                // nothing to do: poll the running chunks (or hand over finished
+                // requests) again shortly, or sleep until a request is ready,
+                // attached or retired
+                std::unique_lock<std::mutex> lk(mu);
+                auto changed = [&] { return stopping || events != seen; };
+                if (running > 0 || !live.empty()) {
+                    cv_sched.wait_for(lk, std::chrono::microseconds(50), changed);
+                } else {
+                    cv_sched.wait(lk, changed);
+                    t_acc = now();   // idle, with nothing running
+                }
+            }
+        } catch (...) {
+            // host memory ran out in this pass: try again a little later
+            std::this_thread::sleep_for(std::chrono::milliseconds(1));
         }
     }
     // stopping: running chunks finish, then every live request ends
@@ -365,8 +417,25 @@ int mfcfd_server_create(const mfcfd_server_config *cfg, mfcfd_server **out) {
     }
     s->st.hbm_budget = s->cfg.hbm_budget;
     s->t0 = std::chrono::steady_clock::now();
-    for (int i = 0; i < cfg->setup_threads; ++i) s->workers.emplace_back([s] { s->worker_loop(); });
-    s->scheduler = std::thread([s] { s->scheduler_loop(); });
+    const int rc = mfcfd::host_guard(nullptr, [&]() -> int {
+        s->workers.reserve((size_t)cfg->setup_threads);
+        for (int i = 0; i < cfg->setup_threads; ++i) s->workers.emplace_back([s] { s->worker_loop(); });
+        s->scheduler = std::thread([s] { s->scheduler_loop(); });
+        return MFCFD_OK;
+    });
+    if (rc) {
+        // a thread could not be started: stop the ones that were
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stopping = true;
+        }
+        s->cv_setup.notify_all();
+        s->cv_sched.notify_all();
+        for (std::thread &w : s->workers) w.join();
+        if (s->scheduler.joinable()) s->scheduler.join();
+        delete s;
+        return rc;
+    }
     *out = s;
     return MFCFD_OK;
 }
@@ -375,6 +444,11 @@ int mfcfd_server_submit(mfcfd_server *s, const mfcfd_request *q, int64_t *id) {
     if (!s || !q || !id || q->n < 1 || !q->status || !q->x || !q->y || !q->z || !q->tan1 || !q->tan2 ||
         !q->nor || !q->nbhs || !q->conn || !q->min_dist || q->max_iters < 1)
         return MFCFD_ERR_ARG;
+    return mfcfd::host_guard(nullptr, [&]() -> int { return s->submit(q, id); });
+}
+
+int mfcfd_server::submit(const mfcfd_request *q, int64_t *id) {
+    mfcfd_server *s = this;
     auto r = std::make_shared<Request>();
     const size_t n = (size_t)q->n;
     r->P = q->params;
@@ -418,7 +492,12 @@ int mfcfd_server_submit(mfcfd_server *s, const mfcfd_request *q, int64_t *id) {
     r->res.id = r->id;
     r->res.t_submit = s->now();
     s->all[r->id] = r;
-    s->to_prepare.push_back(r);
+    try {
+        s->to_prepare.push_back(r);
+    } catch (...) {
+        s->all.erase(r->id);   // leaves no trace of the request
+        throw;
+    }
     ++s->st.submitted;
     s->cv_setup.notify_one();
     *id = r->id;

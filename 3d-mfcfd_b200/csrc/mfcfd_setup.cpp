@@ -29,6 +29,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <thread>
 
 #include "mfcfd_internal.h"
@@ -46,6 +47,10 @@ constexpr int PAR_GRAIN = 4096;
 // f(i) for i in [0, n) on the calling thread and up to 31 threads from the
 // set-up pool; every i writes only its own outputs, so the result does not
 // depend on the thread count.
+//
+// An exception in any chunk (host memory exhausted) reaches the caller after
+// every thread has ended; a chunk whose thread cannot be started runs on the
+// calling thread.
 template <class F>
 void parallel_for(int n, const F &f) {
     const int want = std::min(31, n / PAR_GRAIN - 1);
@@ -54,17 +59,41 @@ void parallel_for(int n, const F &f) {
         for (int i = 0; i < n; ++i) f(i);
         return;
     }
+    struct Tokens {
+        int k;
+        ~Tokens() { give_setup_threads(k); }
+    } tokens{extra};
     const int nt = extra + 1;
     const int chunk = (n + nt - 1) / nt;
+    std::vector<std::exception_ptr> errs((size_t)nt);
     std::vector<std::thread> th;
+    th.reserve((size_t)extra);
+    int threaded = 1;   // chunks 1 .. threaded-1 run on their own threads
     for (int t = 1; t < nt; ++t) {
         const int a = t * chunk, b = std::min(n, a + chunk);
         if (a >= b) break;
-        th.emplace_back([a, b, &f] { for (int i = a; i < b; ++i) f(i); });
+        try {
+            th.emplace_back([a, b, t, &f, &errs] {
+                try {
+                    for (int i = a; i < b; ++i) f(i);
+                } catch (...) {
+                    errs[(size_t)t] = std::current_exception();
+                }
+            });
+        } catch (...) {
+            break;
+        }
+        threaded = t + 1;
     }
-    for (int i = 0; i < std::min(n, chunk); ++i) f(i);
+    try {
+        for (int i = 0; i < std::min(n, chunk); ++i) f(i);
+        for (int i = threaded * chunk; i < n; ++i) f(i);
+    } catch (...) {
+        errs[0] = std::current_exception();
+    }
     for (auto &t : th) t.join();
-    give_setup_threads(extra);
+    for (const std::exception_ptr &e : errs)
+        if (e) std::rethrow_exception(e);
 }
 
 inline double det_of(const Moments &m) {

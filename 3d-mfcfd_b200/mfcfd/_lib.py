@@ -10,7 +10,7 @@ LIB_PATH = os.path.join(_HERE, "libmfcfd.so")
 MFCFD_OK = 0
 ERRORS = {1: "bad argument", 2: "CUDA error", 3: "stencil too wide",
           4: "singular least-squares system", 5: "non-finite residual",
-          6: "unsupported input", 7: "out of device memory", 8: "device wait timed out",
+          6: "unsupported input", 7: "out of memory", 8: "device wait timed out",
           9: "file input/output error", 10: "request not finished"}
 
 FIELD_PRIM, FIELD_U, FIELD_Q, FIELD_QM, FIELD_DQ, FIELD_DELT, FIELD_FLUX_RES, \

@@ -43,7 +43,7 @@ extern "C" {
 #define MFCFD_ERR_SINGULAR     4   /* a least-squares determinant is zero */
 #define MFCFD_ERR_NONFINITE    5   /* the density residual is not finite */
 #define MFCFD_ERR_UNSUPPORTED  6   /* input the library does not handle */
-#define MFCFD_ERR_NOMEM        7   /* device allocation failed */
+#define MFCFD_ERR_NOMEM        7   /* device or host memory, or a host thread, could not be had */
 #define MFCFD_ERR_TIMEOUT      8   /* a bounded device wait ran out */
 #define MFCFD_ERR_IO           9   /* a file could not be read, parsed or written */
 #define MFCFD_ERR_BUSY        10   /* a served request did not finish within the wait */

@@ -113,3 +113,42 @@ def test_prepare_needs_a_device_and_serving_helpers(mfcfd_lib, small_cloud):
     cfg = _lib.ServerConfig(device=0, max_live=0, setup_threads=0, chunk=10)
     srv = ctypes.c_void_p()
     assert L.mfcfd_server_create(ctypes.byref(cfg), ctypes.byref(srv)) == 1
+
+
+def test_host_memory_exhaustion_is_a_status_not_a_crash():
+    """No exception crosses the C ABI: with the process's address space
+    capped just above what it uses, a 72k-point set-up (worker threads and
+    large tables) returns MFCFD_ERR_NOMEM with a message, and the process
+    goes on."""
+    import subprocess
+    import sys
+    import textwrap
+    script = textwrap.dedent('''
+        import ctypes, resource, sys
+        sys.path.insert(0, sys.argv[1])
+        from mfcfd import _lib, cloud
+        from mfcfd._lib import ptr
+        from mfcfd.serve import _cloud_arrays
+        from mfcfd.solver import params_for
+        c = cloud.shell_cloud(12, 6000, r1=3.0, seed=4242)
+        arrs = _cloud_arrays(c)
+        L = _lib.lib()
+        p = params_for(0.4, 0.0, device=-1)
+        h = ctypes.c_void_p()
+        vm = int(open("/proc/self/statm").read().split()[0]) * resource.getpagesize()
+        soft, hard = resource.getrlimit(resource.RLIMIT_AS)
+        resource.setrlimit(resource.RLIMIT_AS, (vm + (32 << 20), hard))
+        rc = L.mfcfd_create(ctypes.byref(p), c.n, *[ptr(a) for a in arrs], ctypes.byref(h))
+        resource.setrlimit(resource.RLIMIT_AS, (soft, hard))
+        msg = L.mfcfd_last_error(h).decode() if h.value else ""
+        if h.value:
+            L.mfcfd_destroy(h)
+        print(rc, msg)
+    ''')
+    import os
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "3d-mfcfd_b200")
+    out = subprocess.run([sys.executable, "-c", script, pkg], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    rc, _, msg = out.stdout.strip().partition(" ")
+    assert int(rc) == 7, out.stdout
+    assert "host" in msg, msg
