@@ -532,6 +532,11 @@ int attach_device(mfcfd_handle *h) {
         h->chain_terms[0] = S.terms_ring;
         h->chain_terms[1] = S.terms_local;
         h->chain_terms[2] = S.terms_cross;
+        if (!T.g0_pts.empty()) {
+            if ((rc = upload(h, &d.g0_pts, T.g0_pts))) return rc;
+            if ((rc = dalloc(h, &d.g0, T.g0_pts.size() * (size_t)G0_DOUBLES))) return rc;
+            d.n_g0 = (int)T.g0_pts.size();
+        }
     }
     std::vector<int32_t> order;
     order.insert(order.end(), T.wall_idx.begin(), T.wall_idx.end());
@@ -858,6 +863,7 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
                 wpb > 0 ? w / wpb * chain_block_slots(h->P.device, wpb, h->P.precision == MFCFD_PRECISION_MIXED) : 0;
             info->chain_slot_capacity = chain_slot_capacity(h->P.device);
             if (!info->chain_warps) info->chain_warps = w;
+            info->g0_points = (int32_t)h->T.g0_pts.size();
         }
         return MFCFD_OK;
     });

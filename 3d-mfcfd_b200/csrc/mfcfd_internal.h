@@ -92,6 +92,11 @@ struct Topology {
     // non-wall neighbour, -1 if none within 1e5)
     std::vector<int32_t> copy_src;
     std::vector<int32_t> ss_pts, ss_src;
+    // swept points outside the shared frame (walls; outer points under the
+    // backup driver) whose phase-A neighbour fluxes the chain schedule takes
+    // from a kernel run before the sweeps; empty when they are more than an
+    // eighth of the cloud (the table would cost more memory than it saves)
+    std::vector<int32_t> g0_pts;
 };
 
 // One point of a sweep as a warp of the chain schedule reads it: the point,
@@ -109,7 +114,13 @@ enum : uint32_t {
     CI_PUBLISH = 4,   // some consumer reads this point's increment from global memory
     CI_COPY = 8,      // supersonic point: copies its nearest neighbour's increment
     CI_OUTER = 16,    // outer point (backup driver): octant lists, z+ over conn, own D_inv
+    CI_G0 = 32,       // the neighbour fluxes of phase A were computed before the sweep
+                      // (k_g0), at block info >> CI_G0_SHIFT of DevCloud::g0
 };
+constexpr int CI_G0_SHIFT = 8;
+// Doubles per point of DevCloud::g0: the sweep's T layout, (list * MAX_SLOTS +
+// slot) * 5 + component.
+constexpr int G0_DOUBLES = NDIR * MAX_SLOTS * 5;
 // Bits the chain schedule adds to SweepEntry::pad (bits 0-15: list, slot).
 constexpr int32_t ENT_RING = 1 << 17;   // producer's increment is in the warp's ring
 constexpr int ENT_RING_SHIFT = 18;      // ring slot (4 bits)
@@ -254,6 +265,9 @@ struct DevCloud {
     const int32_t *pre_order;     // all points, forward sweep order first (fused flux)
     const int32_t *ch_ptr[2], *ch_pts[2], *ch_own[2];
     const ChainItem *ch_items[2];
+    const int32_t *g0_pts;        // points of the g0 blocks (Topology::g0_pts)
+    double *g0;                   // G0_DOUBLES per g0 point, computed by k_g0 each iteration
+    int n_g0;
     // state (Fortran layout, point-major)
     double *prim, *U, *q, *qm, *dq, *delt, *flux_res, *dUp, *dUn, *dinv;
     double *dq_tmp;               // 15 per point: inner-iteration output (or null)

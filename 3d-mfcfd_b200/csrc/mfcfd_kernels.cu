@@ -612,6 +612,7 @@ constexpr int SW_RING_DOUBLES = CHAIN_RING * 30;                    // chain: la
 constexpr int SWEEP_SMEM_BYTES = SW_T_DOUBLES * 8 + (int)sizeof(SweepStage);   // one stage
 constexpr int CHAIN_SMEM_BYTES = (SW_T_DOUBLES + SW_RING_DOUBLES) * 8 + 2 * (int)sizeof(SweepStage);
 static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
+static_assert(SW_T_DOUBLES == G0_DOUBLES && G0_DOUBLES % 2 == 0, "a g0 block is one T buffer of 16-byte pairs");
 static_assert(SWEEP_MAX_ENTRIES <= 96, "entries are polled in three passes of 32");
 static_assert(sizeof(SweepStage) % 16 == 0 && SWEEP_SMEM_BYTES % 16 == 0 && CHAIN_SMEM_BYTES % 16 == 0,
               "stage alignment");
@@ -635,6 +636,7 @@ __device__ __forceinline__ void cp_async4(void *s, const void *g) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ int item_count(uint32_t cnt, int e) { return (int)((cnt >> (5 * e)) & 31u); }
 
@@ -682,6 +684,53 @@ __device__ __forceinline__ void stage_issue(const DevCloud &d, const ChainItem &
     }
 }
 
+// Phase A of a point outside the shared frame, one lane per neighbour slot:
+// the fluxes of the neighbour's state at the start of the sweep in the
+// point's frame, for every list the slot is in, into
+// T[(list * MAX_SLOTS + slot) * 5 + component].  The sweep runs it in place,
+// or k_g0 runs it for all such points before the sweeps (the same code, so
+// the same bits).
+template <typename R>
+__device__ __forceinline__ void neighbour_fluxes(const DevCloud &d, int cls, const FrameT<R> &Fp, int k_slot,
+                                                 int mask_slot, int lane, double *T) {
+    R po[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) po[r] = (R)d.prim[5 * (size_t)k_slot + r];
+    FluxPreT<R> Po;
+    flux_pre(po, Fp, Po);
+    int axes = 0;
+#pragma unroll
+    for (int e = 0; e < NDIR; ++e)
+        if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
+    AxisTermsT<R> Ao[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        if (axes & (1 << a)) axis_terms(Po, a, Ao[a]);
+    for (int e = 0; e < NDIR; ++e) {
+        if (!(mask_slot & (1 << e))) continue;
+        const int kind = flux_kind(cls, e);
+#pragma unroll
+        for (int cc = 0; cc < 5; ++cc)
+            T[(e * MAX_SLOTS + lane) * 5 + cc] = (double)flux_component(kind, cc, Po, Ao);
+    }
+}
+
+// Phase A of every g0 point (Topology::g0_pts) from the state at the start
+// of the iteration, which both sweeps read: one warp per point.
+template <typename R>
+__global__ void __launch_bounds__(128) k_g0(DevCloud d) {
+    const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= d.n_g0) return;
+    const int p = d.g0_pts[w];
+    if (lane >= d.nslot[p]) return;
+    const int mask = d.sweep_slot_mask[(size_t)p * MAX_SLOTS + lane];
+    if (!mask) return;
+    FrameT<R> Fp;
+    load_frame(d.frame + 9 * (size_t)p, Fp);
+    neighbour_fluxes<R>(d, d.cls[p], Fp, d.slot_nbr[(size_t)p * MAX_SLOTS + lane], mask, lane,
+                        d.g0 + (size_t)w * G0_DOUBLES);
+}
+
 // One point of the forward (LdelU) or backward (UdelU) sweep, processed by
 // one warp (implicit_forward_and_reverse_sweeps.f90:30-37 / :61-68), from its
 // stage in shared memory.
@@ -701,9 +750,13 @@ __device__ __forceinline__ void stage_issue(const DevCloud &d, const ChainItem &
 //
 // R: the type of the flux evaluations (float in mixed precision); the list
 // sums, 3x3 solves, D_inv and the increments themselves are double.
+//
+// A CI_G0 point's phase A is a copy of its k_g0 block into T, which the
+// chain kernel issued as a cp.async group before this call (followed by one
+// more group, the next point's stage, when g0_newer); phase B waits for it.
 template <int MODE, typename R>
 __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepStage *st, bool forward, int lane,
-                            double *T, double *ring, int ring_slot) {
+                            double *T, double *ring, int ring_slot, bool g0_newer = false) {
     constexpr bool CHAINS = MODE == MODE_CHAINS;
     const int p = it.p;
     const bool wall = (it.info & CI_WALL) != 0;
@@ -763,30 +816,12 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     } else {
         const uint32_t need = shared ? 0u : st->need;
         const bool mine = !shared && (need >> lane) & 1u;
+        const bool g0 = CHAINS && (it.info & CI_G0) != 0;   // warp-uniform
         int k_slot = 0, mask_slot = 0;
         if (mine) {
             k_slot = st->slot_nbr[lane];
             mask_slot = st->slot_mask[lane];
-            R po[5];
-#pragma unroll
-            for (int r = 0; r < 5; ++r) po[r] = (R)d.prim[5 * (size_t)k_slot + r];
-            FluxPreT<R> Po;
-            flux_pre(po, Fp, Po);
-            int axes = 0;
-#pragma unroll
-            for (int e = 0; e < NDIR; ++e)
-                if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
-            AxisTermsT<R> Ao[3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-                if (axes & (1 << a)) axis_terms(Po, a, Ao[a]);
-            for (int e = 0; e < NDIR; ++e) {
-                if (!(mask_slot & (1 << e))) continue;
-                const int kind = flux_kind(cls, e);
-#pragma unroll
-                for (int cc = 0; cc < 5; ++cc)
-                    T[(e * MAX_SLOTS + lane) * 5 + cc] = (double)flux_component(kind, cc, Po, Ao);
-            }
+            if (!g0) neighbour_fluxes<R>(d, cls, Fp, k_slot, mask_slot, lane, T);
         }
 
         // ---- phase B
@@ -832,38 +867,48 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                 }
                 if (pend && !spin_continue(spins, d.err)) break;
             }
-        } else if (mine) {
-            const bool old = (st->old >> lane) & 1u;   // backup driver: from before the sweep
-            const double *dsrc = (old ? d.dU_old : (forward ? d.dUp : d.dUn)) + 5 * (size_t)k_slot;
-            unsigned long long v[5];
-            int spins = 0;
-            do {
-#pragma unroll
-                for (int r = 0; r < 5; ++r) v[r] = ld_relaxed_b64(dsrc + r);
-            } while (!ready5(v) && spin_continue(spins, d.err));
-            R U[5], pn[5];
-#pragma unroll
-            for (int r = 0; r < 5; ++r) U[r] = (R)(__longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r]);
-            FrameT<R> Fk;
-            load_frame(d.frame + 9 * (size_t)k_slot, Fk);
-            conserved_to_primitive(U, Fk, pn);
+        } else {
             FluxPreT<R> Pn;
-            flux_pre(pn, Fp, Pn);
-            int axes = 0;
-#pragma unroll
-            for (int e = 0; e < NDIR; ++e)
-                if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
             AxisTermsT<R> An[3];
+            if (mine) {
+                const bool old = (st->old >> lane) & 1u;   // backup driver: from before the sweep
+                const double *dsrc = (old ? d.dU_old : (forward ? d.dUp : d.dUn)) + 5 * (size_t)k_slot;
+                unsigned long long v[5];
+                int spins = 0;
+                do {
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
-                if (axes & (1 << a)) axis_terms(Pn, a, An[a]);
-            for (int e = 0; e < NDIR; ++e) {
-                if (!(mask_slot & (1 << e))) continue;
-                const int kind = flux_kind(cls, e);
+                    for (int r = 0; r < 5; ++r) v[r] = ld_relaxed_b64(dsrc + r);
+                } while (!ready5(v) && spin_continue(spins, d.err));
+                R U[5], pn[5];
 #pragma unroll
-                for (int cc = 0; cc < 5; ++cc) {
-                    double *t = &T[(e * MAX_SLOTS + lane) * 5 + cc];
-                    *t = (double)(flux_component(kind, cc, Pn, An) - (R)*t);
+                for (int r = 0; r < 5; ++r) U[r] = (R)(__longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r]);
+                FrameT<R> Fk;
+                load_frame(d.frame + 9 * (size_t)k_slot, Fk);
+                conserved_to_primitive(U, Fk, pn);
+                flux_pre(pn, Fp, Pn);
+                int axes = 0;
+#pragma unroll
+                for (int e = 0; e < NDIR; ++e)
+                    if (mask_slot & (1 << e)) axes |= kind_axes(flux_kind(cls, e));
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                    if (axes & (1 << a)) axis_terms(Pn, a, An[a]);
+            }
+            if (g0) {
+                // the copied phase-A fluxes: every lane's copies have landed
+                if (g0_newer) cp_async_wait_one();
+                else cp_async_wait_all();
+                __syncwarp();
+            }
+            if (mine) {
+                for (int e = 0; e < NDIR; ++e) {
+                    if (!(mask_slot & (1 << e))) continue;
+                    const int kind = flux_kind(cls, e);
+#pragma unroll
+                    for (int cc = 0; cc < 5; ++cc) {
+                        double *t = &T[(e * MAX_SLOTS + lane) * 5 + cc];
+                        *t = (double)(flux_component(kind, cc, Pn, An) - (R)*t);
+                    }
                 }
             }
         }
@@ -1031,12 +1076,20 @@ __global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, R>()) k_sweep_
         const int s = (idx - a) & 1;
         cp_async_wait_all();
         __syncwarp();
+        if (cur.info & CI_G0) {
+            // phase A of this point, computed before the sweep (k_g0): into T,
+            // which the previous point no longer uses
+            const char *src = reinterpret_cast<const char *>(d.g0 + (size_t)(cur.info >> CI_G0_SHIFT) * G0_DOUBLES);
+            char *dst = reinterpret_cast<char *>(T);
+            for (int j = lane; j < G0_DOUBLES / 2; j += 32) cp_async16(dst + 16 * j, src + 16 * j);
+            cp_async_commit();
+        }
         if (idx + 1 < b) {
             stage_issue(d, nxt, forward != 0, lane, &stg[s ^ 1]);
             cp_async_commit();
         }
         const ChainItem after = idx + 2 < b ? items[idx + 2] : nxt;
-        sweep_point<MODE_CHAINS, R>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING);
+        sweep_point<MODE_CHAINS, R>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING, idx + 1 < b);
         cur = nxt;
         nxt = after;
     }
@@ -1417,6 +1470,12 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         cudaMemcpyAsync(d.dq, d.dq_tmp, sizeof(double) * 15 * (size_t)n, cudaMemcpyDeviceToDevice, s);
     }
     mark(1, s);
+    if (chains && d.n_g0 > 0) {
+        // phase A of the points outside the shared frame, for both sweeps
+        const int gb = (int)(((size_t)d.n_g0 * 32 + 127) / 128);
+        if (mixed) k_g0<float><<<gb, 128, 0, s>>>(d);
+        else k_g0<double><<<gb, 128, 0, s>>>(d);
+    }
     if (chains) {
         // the flux residual and the sweep inputs run on the side stream beside
         // the forward sweep, in its order; the sweep polls for them.  The flux

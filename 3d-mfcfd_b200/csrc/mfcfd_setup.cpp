@@ -701,12 +701,21 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     T.consumer_shared.assign(n, 0);
     for (int i = 0; i < n; ++i)
         T.consumer_shared[i] = (T.swept[i] && T.cls[i] == CLS_INTERIOR && T.shared_frame) ? 1 : 0;
+    // points whose phase-A fluxes are computed before the sweeps: swept
+    // points that evaluate their neighbours in their own frame
+    T.g0_pts.clear();
+    for (int i = 0; i < n; ++i)
+        if (T.swept[i] && !T.consumer_shared[i] && T.cls[i] != CLS_SUPERSONIC) T.g0_pts.push_back(i);
+    if (T.g0_pts.size() > (size_t)std::max(4096, n / 8) || T.g0_pts.size() >= (size_t)1 << 24)
+        T.g0_pts.clear();
     return MFCFD_OK;
 }
 
 void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
     S.warps = warps;
     const int n = T.n;
+    std::vector<int32_t> g0_of(n, -1);
+    for (size_t j = 0; j < T.g0_pts.size(); ++j) g0_of[T.g0_pts[j]] = (int32_t)j;
     for (int dir = 0; dir < 2; ++dir) {
         const bool fwd = dir == 0;
         const std::vector<int32_t> &lpts = fwd ? T.fwd_lvl_pts : T.bwd_lvl_pts;
@@ -832,6 +841,7 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
                       (publish[p].load(std::memory_order_relaxed) ? CI_PUBLISH : 0u) |
                       (T.cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u) |
                       (T.cls[p] == CLS_OUTER ? CI_OUTER : 0u);
+            if (g0_of[p] >= 0) it.info |= CI_G0 | ((uint32_t)g0_of[p] << CI_G0_SHIFT);
         }
     }
 }

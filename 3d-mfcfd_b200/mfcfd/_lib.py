@@ -72,7 +72,8 @@ class Info(ctypes.Structure):
                 ("device_bytes", ctypes.c_int64), ("sweep_mode", ctypes.c_int32),
                 ("chain_warps", ctypes.c_int32), ("chain_terms_ring", ctypes.c_int64),
                 ("chain_terms_local", ctypes.c_int64), ("chain_terms_cross", ctypes.c_int64),
-                ("chain_slots", ctypes.c_int32), ("chain_slot_capacity", ctypes.c_int32)]
+                ("chain_slots", ctypes.c_int32), ("chain_slot_capacity", ctypes.c_int32),
+                ("g0_points", ctypes.c_int32)]
 
 
 class ServerConfig(ctypes.Structure):

@@ -56,7 +56,8 @@ WORKLOADS = {
     "sphere-62k": dict(shells=48, per_shell=1300, jitter=0.02, mach=0.4, aoa=0.0, seed=1001),
 }
 # kernels of one iteration per sweep mode (2 chains: k_qderiv, k_pending,
-# k_flux, two k_sweep_chain, k_update, two reductions; 0/1 add k_dinv_gold)
+# k_flux, two k_sweep_chain, k_update, two reductions, and k_g0 when the
+# cloud has points outside the shared frame; 0/1 add k_dinv_gold)
 KERNELS_PER_ITER = {2: 8, 0: 9, 1: 9}
 
 
@@ -372,7 +373,7 @@ def main():
                         "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                 "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks, "mixed": mixed,
                 "serving": serving,
-                "gpu_launches": KERNELS_PER_ITER[args.sweep_mode] * args.steps}
+                "gpu_launches": (KERNELS_PER_ITER[args.sweep_mode] + (1 if info.get("g0_points") else 0)) * args.steps}
         print(json.dumps(line), flush=True)
     if s is not None:
         s.close()

@@ -151,6 +151,10 @@ typedef struct mfcfd_info {
      * 6), and the slots all chain sweeps running at once may hold on the
      * device (mfcfd_launch) */
     int32_t chain_slots, chain_slot_capacity;
+    /* CHAINS: swept points outside the shared frame (walls) whose neighbour
+     * fluxes at the start of the sweeps one extra kernel per iteration
+     * computes for both sweeps; 0 when there are none or too many */
+    int32_t g0_points;
 } mfcfd_info;
 
 typedef struct mfcfd_handle mfcfd_handle;
