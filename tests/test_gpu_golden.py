@@ -4,7 +4,7 @@ With the solver's exp/log/erf on both sides the reference's own routines and
 the GPU produce identical fields (the density residual differs only by the
 summation order of its parallel reduction).  Against the build with glibc's
 exp/log/erf (what the Fortran reference calls) the residual agrees within
-1e-10 relative, the north-star tolerance, and prim within 1e-12.
+1e-10 relative, the tolerance the FP64 path is held to, and prim within 1e-12.
 """
 import json
 

@@ -4,7 +4,7 @@ The oracle runs with the solver's own exp/log/erf (libm mode 1), so every
 field must match bit for bit: the GPU path rounds every operation exactly as
 the reference's FP64 build does.  Against the oracle with glibc's exp/log/erf
 (what the Fortran reference calls) the fields agree to a few ulp per call;
-the density residual is checked to 1e-10 relative, the north-star tolerance.
+the density residual is checked to 1e-10 relative, the tolerance the FP64 path is held to.
 """
 import numpy as np
 import pytest
