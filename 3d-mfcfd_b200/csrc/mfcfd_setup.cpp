@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <thread>
@@ -116,9 +117,18 @@ inline double numerator(int axis, const Moments &m, double fx, double fy, double
 }
 
 // the host's cores less two: one for the calling thread, one for a thread
-// that keeps a device busy meanwhile (the request server's scheduler)
+// that keeps a device busy meanwhile (the request server's scheduler); or
+// MFCFD_SETUP_THREADS - 1 when that is set (1: every pass on its caller)
+int initial_pool() {
+    if (const char *v = std::getenv("MFCFD_SETUP_THREADS")) {
+        const int t = std::atoi(v);
+        if (t >= 1) return std::min(t, 256) - 1;
+    }
+    return std::max(0, (int)std::thread::hardware_concurrency() - 2);
+}
+
 std::atomic<int> &setup_pool() {
-    static std::atomic<int> pool{std::max(0, (int)std::thread::hardware_concurrency() - 2)};
+    static std::atomic<int> pool{initial_pool()};
     return pool;
 }
 

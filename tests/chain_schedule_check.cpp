@@ -54,6 +54,21 @@ bool read_all(const std::string &path, std::vector<T> &v, size_t n) {
         }                                              \
     } while (0)
 
+// FNV-1a over the bytes of a table
+struct Hash {
+    uint64_t h = 1469598103934665603ull;
+    void bytes(const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+    }
+    template <class T>
+    void vec(const std::vector<T> &v) {
+        const uint64_t n = v.size();
+        bytes(&n, sizeof n);
+        if (n) bytes(v.data(), sizeof(T) * n);
+    }
+};
+
 bool same_items(const ChainSchedule &a, const ChainSchedule &b) {
     for (int d = 0; d < 2; ++d) {
         if (a.pts[d] != b.pts[d] || a.ptr[d] != b.ptr[d] || a.items[d].size() != b.items[d].size()) return false;
@@ -174,6 +189,22 @@ int main(int argc, char **argv) {
             }
         }
     }
-    std::printf("ok ring %ld global %ld g0 %zu\n", ring_terms, global_terms, T.g0_pts.size());
+    Hash H;
+    for (int d = 0; d < NDIR; ++d) {
+        H.vec(T.split[d]);
+        H.vec(T.split_cnt[d]);
+    }
+    H.vec(T.alias); H.vec(T.point_with_alias); H.vec(T.slot_nbr); H.vec(T.nslot); H.vec(T.slot_mask);
+    H.vec(T.list_cnt); H.vec(T.list_ent); H.vec(T.geo); H.vec(T.eps2);
+    H.vec(T.fwd_level); H.vec(T.bwd_level); H.vec(T.fwd_lvl_pts); H.vec(T.bwd_lvl_pts);
+    H.vec(T.fwd_off); H.vec(T.bwd_off); H.vec(T.fwd_cnt); H.vec(T.bwd_cnt);
+    H.vec(T.fwd_ent); H.vec(T.bwd_ent); H.vec(T.fwd_need); H.vec(T.bwd_need); H.vec(T.g0_pts);
+    for (int d = 0; d < 2; ++d) {
+        H.vec(S.ptr[d]);
+        H.vec(S.pts[d]);
+        H.vec(S.items[d]);
+    }
+    std::printf("ok ring %ld global %ld g0 %zu hash %016llx\n", ring_terms, global_terms, T.g0_pts.size(),
+                (unsigned long long)H.h);
     return 0;
 }

@@ -29,14 +29,14 @@ def checker(tmp_path_factory):
     return exe
 
 
-def _check(checker, tmp_path, c, warps, variant=0):
+def _check(checker, tmp_path, c, warps, variant=0, env=None):
     for name, a, t in (("status", c.status, np.int32), ("x", c.x, np.float64), ("y", c.y, np.float64),
                        ("z", c.z, np.float64), ("tan1", c.tan1, np.float64), ("tan2", c.tan2, np.float64),
                        ("nor", c.nor, np.float64), ("nbhs", c.nbhs, np.int32), ("conn", c.conn, np.int32),
                        ("md", c.min_dist, np.float64)):
         np.ascontiguousarray(a, dtype=t).tofile(str(tmp_path / f"{name}.bin"))
     out = subprocess.run([checker, str(tmp_path), str(c.n), str(warps), str(variant)], capture_output=True,
-                         text=True, timeout=300)
+                         text=True, timeout=300, env=env)
     assert out.returncode == 0, out.stdout + out.stderr
     return out.stdout
 
@@ -55,7 +55,15 @@ def test_schedule_invariants_supersonic_and_backup_driver(checker, tmp_path, var
 
 
 def test_schedule_invariants_threaded_build(checker, tmp_path):
-    """15,000 points: the term marking runs on several host threads."""
+    """15,000 points: the set-up passes and the term marking run on several
+    host threads, and every table and the schedule are the same bytes as with
+    one thread (MFCFD_SETUP_THREADS=1)."""
     from mfcfd import cloud
     c = cloud.shell_cloud(10, 1500, r1=2.0, seed=77)
-    assert _check(checker, tmp_path, c, -100).startswith("ok")
+    outs = []
+    for threads in ("1", "4", "16"):
+        env = dict(os.environ, MFCFD_SETUP_THREADS=threads)
+        out = _check(checker, tmp_path, c, -100, env=env)
+        assert out.startswith("ok")
+        outs.append(out.split("hash")[1].strip())
+    assert outs[0] == outs[1] == outs[2]
