@@ -448,7 +448,6 @@ int mfcfd_server_submit(mfcfd_server *s, const mfcfd_request *q, int64_t *id) {
 }
 
 int mfcfd_server::submit(const mfcfd_request *q, int64_t *id) {
-    mfcfd_server *s = this;
     auto r = std::make_shared<Request>();
     const size_t n = (size_t)q->n;
     r->P = q->params;
@@ -480,26 +479,26 @@ int mfcfd_server::submit(const mfcfd_request *q, int64_t *id) {
             }
         }
     }
-    const int32_t c = s->cfg.chunk;
+    const int32_t c = cfg.chunk;
     r->max_iters = (q->max_iters + c - 1) / c * c;
     r->target = q->residue_target;
     r->wall_area = q->wall_area;
     r->ref_area = q->ref_area;
     r->res.n = q->n;
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->stopping) return MFCFD_ERR_ARG;
-    r->id = s->next_id++;
+    std::lock_guard<std::mutex> lk(mu);
+    if (stopping) return MFCFD_ERR_ARG;
+    r->id = next_id++;
     r->res.id = r->id;
-    r->res.t_submit = s->now();
-    s->all[r->id] = r;
+    r->res.t_submit = now();
+    all[r->id] = r;
     try {
-        s->to_prepare.push_back(r);
+        to_prepare.push_back(r);
     } catch (...) {
-        s->all.erase(r->id);   // leaves no trace of the request
+        all.erase(r->id);   // leaves no trace of the request
         throw;
     }
-    ++s->st.submitted;
-    s->cv_setup.notify_one();
+    ++st.submitted;
+    cv_setup.notify_one();
     *id = r->id;
     return MFCFD_OK;
 }
