@@ -38,6 +38,7 @@ struct mfcfd_handle {
     int res_cap = 1024;
     int64_t bytes = 0;
     bool have_state = false;
+    bool res_valid = false;                // res_sqr holds the terms of a completed iteration
     bool profiling = false;
     std::vector<cudaEvent_t> ev;          // (MFCFD_NPHASE+1) per iteration slot
     double phase_ms[MFCFD_NPHASE] = {0};
@@ -189,6 +190,7 @@ int launch_one(mfcfd_handle *h, int j) {
 // chunk is captured once per (length, starting U/q buffer) and replayed;
 // the host-side buffer state then advances as the captured launches did.
 int launch_chunk(mfcfd_handle *h, int chunk, bool batch) {
+    h->res_valid = false;                  // valid again once the chunk has completed
     if (h->P.graphs < (batch ? 1 : 2) || h->graphs_off || h->profiling) {
         for (int j = 0; j < chunk; ++j) {
             int rc = launch_one(h, j);
@@ -253,6 +255,7 @@ int finish_chunk(mfcfd_handle *h, int32_t t0, int chunk, double *res_hist, int *
         CK(cudaStreamSynchronize(h->stream));
         return fail(h, MFCFD_ERR_TIMEOUT, "a sweep wait ran out; the iteration results are invalid");
     }
+    h->res_valid = true;
     if (h->profiling) {
         for (int j = 0; j < chunk; ++j) {
             const cudaEvent_t *ev = &h->ev[(size_t)j * (MFCFD_NPHASE + 1)];
@@ -675,6 +678,7 @@ int mfcfd_set_prim(mfcfd_handle *h, const double *prim) {
         h->last = h->cur;
         h->res_old = h->res_new = h->residue = 0.0;
         h->have_state = true;
+        h->res_valid = false;
         return MFCFD_OK;
     });
 }
@@ -792,6 +796,7 @@ int mfcfd_set_state(mfcfd_handle *h, const double *prim, const double *delu, dou
         h->last = h->cur;
         h->res_old = res_old;
         h->have_state = true;
+        h->res_valid = false;
         return MFCFD_OK;
     });
 }
@@ -906,9 +911,25 @@ int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new) {
     return host_guard(h ? &h->err : nullptr, [&]() -> int {
         if (!h || !res_new) return MFCFD_ERR_ARG;
         if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        if (!h->res_valid)
+            return fail(h, MFCFD_ERR_ARG,
+                        "no completed iteration since the state was last set (or the last one timed out)");
         cudaError_t e = cudaSetDevice(h->P.device);
         if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
         return residual_noalloc(h->d, h->stream, res_new, h->err);
+    });
+}
+
+int mfcfd_set_fault_hook(mfcfd_handle *h, int32_t point, int32_t wait_limit) {
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || point < 0 || wait_limit < 0) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        if (point > h->d.n) return fail(h, MFCFD_ERR_ARG, "point out of range");
+        if (h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "a launch is pending on this handle");
+        h->d.withhold1 = point;
+        h->d.spin_limit = wait_limit;
+        drop_graphs(h);                    // their launches carry the old settings
+        return MFCFD_OK;
     });
 }
 

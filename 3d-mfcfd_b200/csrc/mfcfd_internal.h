@@ -260,6 +260,9 @@ struct DevCloud {
     int precision;                // MFCFD_PRECISION_*
     int *sweep_counter;           // 2 work counters (forward, backward)
     int *err;                     // set when a bounded poll gave up
+    int spin_limit;               // poll rounds before a wait gives up (0: the default)
+    int withhold1;                // failure-detection hook: this point (1-based) publishes
+                                  // none of its sweep increments; 0: off
     // chain schedule (per direction: 0 forward, 1 backward)
     int ch_warps, ch_wpb;         // warps and warps per block
     const int32_t *pre_order;     // all points, forward sweep order first (fused flux)
@@ -298,6 +301,8 @@ cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
 // out[0..2] (device) = -sum over wall points of (p - p_inf) A nor
 cudaError_t launch_forces(const DevCloud &d, cudaStream_t s, double area_each, const double *area, double *out);
 int reduction_blocks(int n);
+// streaming multiprocessors of a device (cached per device)
+int device_sms(int device);
 // Launch shape of the chain sweep for about `want` warps: warps per block
 // and blocks (at most SMs - 16 blocks); returns the warps, 0 if the kernel
 // cannot run on the device.

@@ -195,19 +195,19 @@ __device__ __forceinline__ void st_relaxed_f64(double *p, double v) {
     asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
 
-// Polls give up after SPIN_LIMIT rounds (about a second), or soon after
-// another lane gave up: the failure goes to *err (the host reports
-// MFCFD_ERR_TIMEOUT and the iteration's results are invalid).
+// Polls give up after SPIN_LIMIT rounds (about a second; d.spin_limit when
+// set), or soon after another lane gave up: the failure goes to *d.err (the
+// host reports MFCFD_ERR_TIMEOUT and the iteration's results are invalid).
 constexpr int SPIN_LIMIT = 1 << 21;
 
-__device__ __forceinline__ bool spin_continue(int &it, int *err) {
+__device__ __forceinline__ bool spin_continue(int &it, const DevCloud &d) {
     ++it;
     if ((it & 1023) == 0) {
-        if (*(volatile int *)err) return false;
+        if (*(volatile int *)d.err) return false;
         __nanosleep(64);
     }
-    if (it > SPIN_LIMIT) {
-        atomicExch(err, 1);
+    if (it > (d.spin_limit > 0 ? d.spin_limit : SPIN_LIMIT)) {
+        atomicExch(d.err, 1);
         return false;
     }
     return true;
@@ -218,12 +218,12 @@ __device__ __forceinline__ bool is_pending(double v) {
 }
 
 // Poll one word until it is published.
-__device__ __forceinline__ double poll_word(const double *p, int *err) {
+__device__ __forceinline__ double poll_word(const double *p, const DevCloud &d) {
     unsigned long long v;
     int spins = 0;
     do {
         v = ld_relaxed_b64(p);
-    } while (v == DU_PENDING && spin_continue(spins, err));
+    } while (v == DU_PENDING && spin_continue(spins, d));
     return __longlong_as_double((long long)v);
 }
 
@@ -763,6 +763,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
     const bool shared = (it.info & CI_SHARED) != 0;
     const bool copy = (it.info & CI_COPY) != 0;       // supersonic point
     const bool outer = (it.info & CI_OUTER) != 0;     // backup driver
+    const bool hold = p + 1 == d.withhold1;           // failure-detection hook: publish nothing
     const int cls = wall ? CLS_WALL : (outer ? CLS_OUTER : CLS_INTERIOR);
     const SweepEntry *E = st->ent;
     const int dd = lane / 5, c = lane - 5 * (lane / 5);
@@ -790,10 +791,10 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         base5 = st->base[lane];
     }
     // inputs the concurrent flux kernel had not produced when the stage was copied
-    if (lane < 30 && is_pending(gold)) gold = poll_word(d.gold + 30 * (size_t)p + lane, d.err);
+    if (lane < 30 && is_pending(gold)) gold = poll_word(d.gold + 30 * (size_t)p + lane, d);
     if (lane < 5 && !copy) {
-        if (is_pending(dinv)) dinv = poll_word(d.dinv + p, d.err);
-        if (is_pending(base5)) base5 = poll_word((forward ? d.flux_res : d.dUp) + 5 * (size_t)p + lane, d.err);
+        if (is_pending(dinv)) dinv = poll_word(d.dinv + p, d);
+        if (is_pending(base5)) base5 = poll_word((forward ? d.flux_res : d.dUp) + 5 * (size_t)p + lane, d);
     }
     double Up[5];
 #pragma unroll
@@ -809,9 +810,9 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
             const int q = E[0].k;
             double *dst = (forward ? d.dUp : d.dUn) + 5 * (size_t)p + lane;
             if (q >= 0)
-                dnew = (E[0].pad & ENT_COPY_NEW) ? poll_word((forward ? d.dUp : d.dUn) + 5 * (size_t)q + lane, d.err)
+                dnew = (E[0].pad & ENT_COPY_NEW) ? poll_word((forward ? d.dUp : d.dUn) + 5 * (size_t)q + lane, d)
                                                  : d.dU_old[5 * (size_t)q + lane];
-            st_relaxed_f64(dst, dnew);
+            if (!hold) st_relaxed_f64(dst, dnew);
         }
     } else {
         const uint32_t need = shared ? 0u : st->need;
@@ -865,7 +866,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                     for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __longlong_as_double(v[q][cc]);
                     pend &= ~(1u << q);
                 }
-                if (pend && !spin_continue(spins, d.err)) break;
+                if (pend && !spin_continue(spins, d)) break;
             }
         } else {
             FluxPreT<R> Pn;
@@ -878,7 +879,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                 do {
 #pragma unroll
                     for (int r = 0; r < 5; ++r) v[r] = ld_relaxed_b64(dsrc + r);
-                } while (!ready5(v) && spin_continue(spins, d.err));
+                } while (!ready5(v) && spin_continue(spins, d));
                 R U[5], pn[5];
 #pragma unroll
                 for (int r = 0; r < 5; ++r) U[r] = (R)(__longlong_as_double(v[r]) + d.U[5 * (size_t)k_slot + r]);
@@ -951,10 +952,10 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
             else lu = gd[0] + gd[1] + gd[2] + gd[3] + gd[4] + gd[5];
             if (forward) {
                 dnew = -(dinv * (base5 + lu));
-                st_relaxed_f64(d.dUp + 5 * (size_t)p + lane, dnew);
+                if (!hold) st_relaxed_f64(d.dUp + 5 * (size_t)p + lane, dnew);
             } else {
                 dnew = base5 - dinv * lu;
-                st_relaxed_f64(d.dUn + 5 * (size_t)p + lane, dnew);
+                if (!hold) st_relaxed_f64(d.dUn + 5 * (size_t)p + lane, dnew);
             }
         }
     }
@@ -972,7 +973,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
             AxisTermsT<R> At;
             axis_terms(P, dd >> 1, At);
             const double v = (double)(flux_component(dd, c, P, At, At, At) - (R)gold);
-            if (it.info & CI_PUBLISH)
+            if ((it.info & CI_PUBLISH) && !hold)
                 st_relaxed_f64((forward ? d.dgf : d.dgb) + DG_STRIDE * (size_t)p + DG_LIST * dd + c, v);
             if (CHAINS) ring[30 * ring_slot + lane] = v;
         }
@@ -1245,6 +1246,22 @@ cudaError_t launch_forces(const DevCloud &d, cudaStream_t s, double area_each, c
 
 // ---------------------------------------------------------------- launchers
 
+int device_sms(int device) {
+    static std::mutex mu;
+    static int cache[256] = {0};
+    if (device < 0 || device >= 256) return 1;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cache[device]) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms < 1) {
+            (void)cudaGetLastError();
+            sms = 1;
+        }
+        cache[device] = sms;
+    }
+    return cache[device];
+}
+
 int reduction_blocks(int n) {
     int b = (n + 4095) / 4096;
     return b < 1 ? 1 : (b > 1024 ? 1024 : b);
@@ -1436,8 +1453,9 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     set_attributes(dev);
     // dataflow grid: about the widest level in warps (more warps only add
     // pollers), within 8 per SM
+    const int sms = device_sms(dev);
     int df_warps = d.max_width;
-    df_warps = df_warps < 64 ? 64 : (df_warps > 148 * 8 ? 148 * 8 : df_warps);
+    df_warps = df_warps < 64 ? 64 : (df_warps > sms * 8 ? sms * 8 : df_warps);
     const int df_blocks = (df_warps + DF_WARPS - 1) / DF_WARPS;
     const bool chains = d.sweep_mode == MFCFD_SWEEP_CHAINS;
     const bool mixed = d.precision == MFCFD_PRECISION_MIXED;   // chain schedule only
@@ -1484,7 +1502,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         // never waits on the sweep, so no order of execution can stall.  The
         // main stream's higher priority places the sweep's blocks first when
         // both run.
-        k_pending<<<148 * 8, 256, 0, s>>>(d, 1);
+        k_pending<<<sms * 8, 256, 0, s>>>(d, 1);
         mark(3, s);
         cudaEventRecord(st.fork, s);
         cudaStreamWaitEvent(st.side, st.fork, 0);
@@ -1499,7 +1517,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     } else {
         k_flux<false, double><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
         mark(2, s);
-        k_pending<<<148 * 8, 256, 0, s>>>(d, 0);
+        k_pending<<<sms * 8, 256, 0, s>>>(d, 0);
         k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);
         mark(3, s);
         sweep(1);

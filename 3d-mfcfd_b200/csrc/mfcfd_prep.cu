@@ -367,7 +367,7 @@ int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, 
     int32_t *front = d_fa, *next = d_fb;
     while (m > 0) {
         const size_t len = (size_t)m * MAX_CONN;
-        const int grid = (int)std::min<size_t>((len + PREP_THREADS - 1) / PREP_THREADS, 148 * 16);
+        const int grid = (int)std::min<size_t>((len + PREP_THREADS - 1) / PREP_THREADS, (size_t)device_sms(device) * 16);
         k_bfs_offer<<<grid, PREP_THREADS, 0, s>>>(front + skip, m, d_nb, d_conn, d_alias, d_key);
         k_bfs_winners<<<grid, PREP_THREADS, 0, s>>>(front + skip, m, d_nb, d_conn, d_alias, d_key, d_flag);
         int rc = exclusive_scan(d_flag, d_pos, (int)len, d_sums, d_total, s, err);

@@ -74,18 +74,41 @@ def freestream_prim(n: int, mach: float, aoa_deg: float) -> np.ndarray:
     return np.tile(np.array(freestream(mach, aoa_deg), dtype=np.float64), (n, 1))
 
 
+# The generators use only operations whose results do not depend on the host
+# CPU: IEEE +, -, *, / and sqrt (numpy rounds these exactly on every SIMD
+# path), and the C library's scalar sin/cos through `math`.  numpy's
+# vectorised sin/cos and BLAS products may round differently on different
+# CPUs, and a cloud must be the same bits on every machine that regenerates
+# it for a parity check.
+
+
 def _fibonacci_sphere(m: int) -> np.ndarray:
     i = np.arange(m, dtype=np.float64) + 0.5
     zz = 1.0 - 2.0 * i / m
     rr = np.sqrt(np.maximum(0.0, 1.0 - zz * zz))
     phi = i * (math.pi * (3.0 - math.sqrt(5.0)))
-    return np.stack([rr * np.cos(phi), rr * np.sin(phi), zz], axis=1)
+    cphi = np.array([math.cos(v) for v in phi.tolist()], dtype=np.float64)
+    sphi = np.array([math.sin(v) for v in phi.tolist()], dtype=np.float64)
+    return np.stack([rr * cphi, rr * sphi, zz], axis=1)
+
+
+def _rows_norm(v: np.ndarray) -> np.ndarray:
+    """Euclidean norm of each row of an (n, 3) array, summed in a fixed order."""
+    return np.sqrt(v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1] + v[:, 2] * v[:, 2])
+
+
+def _rotate(u: np.ndarray, rot: np.ndarray) -> np.ndarray:
+    """u @ rot.T written out, so every product and sum rounds the same way."""
+    out = np.empty_like(u)
+    for r in range(3):
+        out[:, r] = u[:, 0] * rot[r, 0] + u[:, 1] * rot[r, 1] + u[:, 2] * rot[r, 2]
+    return out
 
 
 def _random_rotation(rng: np.random.Generator) -> np.ndarray:
-    q = rng.standard_normal(4)
-    q /= np.linalg.norm(q)
-    a, b, c, d = q
+    q = [float(v) for v in rng.standard_normal(4)]
+    nq = math.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+    a, b, c, d = (v / nq for v in q)
     return np.array([
         [a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
         [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
@@ -101,8 +124,11 @@ def _boundary_frames(nor: np.ndarray):
     tan1[ok, 0] = -ny[ok] / h[ok]
     tan1[ok, 1] = nx[ok] / h[ok]
     tan1[~ok, 0] = 1.0
-    tan2 = np.cross(nor, tan1)
-    tan2 /= np.linalg.norm(tan2, axis=1)[:, None]
+    tan2 = np.empty_like(nor)
+    tan2[:, 0] = nor[:, 1] * tan1[:, 2] - nor[:, 2] * tan1[:, 1]
+    tan2[:, 1] = nor[:, 2] * tan1[:, 0] - nor[:, 0] * tan1[:, 2]
+    tan2[:, 2] = nor[:, 0] * tan1[:, 1] - nor[:, 1] * tan1[:, 0]
+    tan2 /= _rows_norm(tan2)[:, None]
     return tan1, tan2
 
 
@@ -156,7 +182,7 @@ def shell_cloud(n_shells: int, pts_per_shell: int, r0: float = 0.5,
     for s in range(n_shells):
         r = r0 * (r1 / r0) ** (s / (n_shells - 1))
         rot = _random_rotation(rng)
-        u = unit @ rot.T
+        u = _rotate(unit, rot)
         if 0 < s < n_shells - 1:
             scale = r * (1.0 + jitter * rng.uniform(-1.0, 1.0, size=pts_per_shell))
         else:
@@ -171,7 +197,7 @@ def shell_cloud(n_shells: int, pts_per_shell: int, r0: float = 0.5,
         status.append(np.full(pts_per_shell, st, dtype=np.int32))
         # outward normal of the ellipsoid x^2/a^2 + ... = r^2 at p
         g = p / (ax[None, :] ** 2)
-        nors.append(g / np.linalg.norm(g, axis=1)[:, None])
+        nors.append(g / _rows_norm(g)[:, None])
     pts = np.concatenate(pts)
     status = np.concatenate(status)
     nor_b = np.concatenate(nors)

@@ -200,6 +200,12 @@ class Solver:
         self._check(_lib.lib().mfcfd_residual_noalloc(self.h, ptr(out)))
         return float(out[0])
 
+    def set_fault_hook(self, point: int, wait_limit: int = 0):
+        """Failure-detection test hook (mfcfd_set_fault_hook): point (1-based,
+        0 off) publishes none of its sweep increments, and device waits give
+        up after wait_limit poll rounds (0: the default)."""
+        self._check(_lib.lib().mfcfd_set_fault_hook(self.h, int(point), int(wait_limit)))
+
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             _lib.lib().mfcfd_destroy(self.h)

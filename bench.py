@@ -16,9 +16,11 @@ cloud is seeded synthetic data from the package generator.  Its state
 Multi-GPU: independent replicas, one per rank (the LU-SGS sweep order is
 global, so one cloud does not shard); value sums the ranks' points.
 
-``--impl reference`` times the CPU oracle (the reference's algorithm restated
-in C++, glibc libm) instead: one independent solve per host core on a 62,400
-point sphere sample, one iteration per step.
+``--impl reference`` times the reference's own routines on the host cores
+instead: its Fortran translated mechanically to C (oracle/_ref/libref.so,
+glibc libm), or the C++ restatement of them when that build is absent; one
+independent solve per host core on a 62,400-point sphere sample, one
+iteration per step.
 """
 from __future__ import annotations
 

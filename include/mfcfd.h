@@ -284,14 +284,34 @@ int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters);
  * loading the library holds until the process exits.
  *
  * Limit: at most MFCFD_NOALLOC_MAX_TERMS residual terms (wall plus interior
- * points); larger clouds get MFCFD_ERR_UNSUPPORTED.  The first call on a
- * device looks up the scratch array's device address; make that first call
- * before any stream capture.  All calls share the one array and it keeps the
- * last call's contents (every call overwrites all of it that it reads), so
- * calls that overlap on the GPU race: do not run two at once, on any stream.
+ * points); larger clouds get MFCFD_ERR_UNSUPPORTED.  Before the first
+ * completed iteration, after mfcfd_set_prim or mfcfd_set_state, and after an
+ * iteration that returned MFCFD_ERR_TIMEOUT there is no valid residual, and
+ * the call returns MFCFD_ERR_ARG.  The first call on a device looks up the
+ * scratch array's device address.  The call is synchronous: it ends with a
+ * device-to-host copy and a wait on the handle's stream, so it must never be
+ * made while the handle's stream, or a stream joined to it, is being
+ * captured.  All calls share the one array and it keeps the last call's
+ * contents (every call overwrites all of it that it reads), so calls that
+ * overlap on the GPU race: do not run two at once, on any stream.
  */
 #define MFCFD_NOALLOC_MAX_TERMS (1024 * 4096)
 int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new);
+
+/*
+ * Failure-detection test hook (no counterpart in the reference, which has no
+ * failure detection).  Every device wait of the sweeps is bounded: when one
+ * runs out, the kernel sets an error word and returns, and the step reports
+ * MFCFD_ERR_TIMEOUT with that iteration's results invalid.  This hook makes
+ * that happen on purpose without faulting or hanging the GPU: from the next
+ * iteration on, point `point` (1-based; 0 turns the hook off) publishes none
+ * of its sweep increments, so the points that read them wait until their
+ * bound runs out.  wait_limit > 0 sets that bound in poll rounds (0: the
+ * default, about a second).  After MFCFD_ERR_TIMEOUT the handle stays
+ * usable: turn the hook off and set the state again (mfcfd_set_prim or
+ * mfcfd_set_state) before the next step.
+ */
+int mfcfd_set_fault_hook(mfcfd_handle *h, int32_t point, int32_t wait_limit);
 
 /*
  * File formats of the reference program, for a host that replaces the whole

@@ -18,7 +18,9 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_REF_DIR_DEFAULT = "/root/reference"
+# Where the reference's Fortran sources lie; the translation is rebuilt only
+# when this is set (elsewhere the prebuilt libraries under _ref/ are used).
+REF_DIR_ENV = "MFCFD_REFERENCE_DIR"
 _LIBS = {"glibc": os.path.join(_HERE, "_ref", "libref.so"),
          "mfmath": os.path.join(_HERE, "_ref", "libref_mfmath.so"),
          # the reference's alternative module sources (f2c_ref.VARIANTS), glibc
@@ -28,11 +30,20 @@ _lib = None
 _lib_kind = None
 
 
-def build(reference_dir: str = _REF_DIR_DEFAULT) -> bool:
+def reference_dir():
+    """The reference checkout named by $MFCFD_REFERENCE_DIR, or None."""
+    d = os.environ.get(REF_DIR_ENV)
+    return d if d and os.path.isdir(d) else None
+
+
+def build(reference_dir: str = None) -> bool:
     """Translate and compile two builds: with glibc's exp/log/erf (what the
     Fortran reference calls) and with the solver's mfmath.h functions.
-    Returns False when the reference is absent and nothing was built before."""
-    if not os.path.isdir(reference_dir):
+    reference_dir defaults to $MFCFD_REFERENCE_DIR.  Returns False when the
+    reference is absent and nothing was built before."""
+    if reference_dir is None:
+        reference_dir = os.environ.get(REF_DIR_ENV, "")
+    if not reference_dir or not os.path.isdir(reference_dir):
         return all(os.path.exists(p) for p in _LIBS.values())
     out_c = os.path.join(_HERE, "_ref", "ref_translated.c")
     subprocess.run(["python", os.path.join(_HERE, "f2c_ref.py"), reference_dir, out_c],

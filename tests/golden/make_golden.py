@@ -14,7 +14,7 @@ clouds and stores its outputs:
                       with glibc's exp/log/erf ("glibc") and the build with the
                       solver's own exp/log/erf ("mfmath").
 
-Usage: python tests/golden/make_golden.py   (needs the reference checkout)
+Usage: MFCFD_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py
 """
 import json
 import os
@@ -66,7 +66,7 @@ def main():
         return
     from oracle import ref_translated as R
     if not R.build():
-        sys.exit("the reference checkout is needed to build the translated reference")
+        sys.exit("set MFCFD_REFERENCE_DIR to the reference checkout to build the translated reference")
     c = golden_cloud()
     from mfcfd import cloud as cl
     data = {"status": c.status, "x": c.x, "y": c.y, "z": c.z, "tan1": c.tan1, "tan2": c.tan2,

@@ -8,13 +8,11 @@ import sys
 import numpy as np
 import pytest
 
-REF = "/root/reference"
+REF = os.environ.get("MFCFD_REFERENCE_DIR", "")
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "sphere_600.npz")
 
-pytestmark = pytest.mark.skipif(not os.path.isdir(REF), reason="reference checkout absent")
-
-
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="MFCFD_REFERENCE_DIR is not set")
 def test_translation_reproduces_fixtures(tmp_path):
     repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, repo)

@@ -25,3 +25,24 @@ def test_residual_noalloc_matches_fpi_step(mfcfd_lib):
         assert res_new > 0.0
         assert abs(again - res_new) <= 1e-13 * abs(res_new), (t, again, res_new)
     s.close()
+
+
+def test_residual_noalloc_without_a_completed_iteration(mfcfd_lib):
+    """Before the first iteration and after the state is set again there is
+    no residual to recompute: the call says so instead of returning a stale
+    or zero value."""
+    from mfcfd import _lib, cloud
+    from mfcfd.solver import Solver
+    c = cloud.small_sphere()
+    s = Solver(c, 0.4, 0.0)
+    s.initial_conditions()
+    with pytest.raises(_lib.MfcfdError) as e:
+        s.residual_noalloc()
+    assert e.value.code == 1
+    res_new, _ = s.fpi_solver(1)
+    assert abs(s.residual_noalloc() - res_new) <= 1e-13 * abs(res_new)
+    s.initial_conditions()
+    with pytest.raises(_lib.MfcfdError) as e:
+        s.residual_noalloc()
+    assert e.value.code == 1
+    s.close()
