@@ -45,6 +45,8 @@ struct mfcfd_handle {
     int64_t prof_iters = 0;
     int64_t chain_terms[3] = {0, 0, 0};   // chain schedule: ring, same-warp, cross-warp terms
     double *wall_area = nullptr;           // per-point areas for mfcfd_forces (device), or null
+    int32_t *perm_dev = nullptr;           // storage index of each point (device); null: index order
+    double *xfer = nullptr;                // 5 doubles per point: index-order transfer buffer
     double *force_out = nullptr;           // 3 doubles (device)
     // host copies held between mfcfd_prepare and mfcfd_attach
     struct Staged {
@@ -116,6 +118,41 @@ int upload(mfcfd_handle *h, const T **dst, const std::vector<T> &src) {
     if (rc) return rc;
     if (!src.empty() && !h->dry) CK(cudaMemcpyAsync(p, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, h->stream));
     *dst = p;
+    return MFCFD_OK;
+}
+
+// n rows of w doubles from host memory in the reference's index order to
+// device memory in storage order, through the transfer buffer when the
+// cloud is stored permuted (stream-ordered; the caller synchronises).
+int rows_to_device(mfcfd_handle *h, double *dst, const double *src, int w) {
+    const size_t n = (size_t)h->d.n;
+    if (!h->perm_dev) {
+        CK(cudaMemcpyAsync(dst, src, n * w * 8, cudaMemcpyHostToDevice, h->stream));
+        return MFCFD_OK;
+    }
+    const size_t per = std::max<size_t>(1, n * 5 / (size_t)w);
+    for (size_t a = 0; a < n; a += per) {
+        const size_t rows = std::min(per, n - a);
+        CK(cudaMemcpyAsync(h->xfer, src + a * w, rows * w * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(launch_rows(h->xfer, dst, h->perm_dev, (int)a, (int)rows, w, true, h->stream));
+    }
+    return MFCFD_OK;
+}
+
+// The reverse: n rows of w doubles of device memory in storage order to host
+// memory in index order.
+int rows_to_host(mfcfd_handle *h, double *dst, const double *src, int w) {
+    const size_t n = (size_t)h->d.n;
+    if (!h->perm_dev) {
+        CK(cudaMemcpyAsync(dst, src, n * w * 8, cudaMemcpyDeviceToHost, h->stream));
+        return MFCFD_OK;
+    }
+    const size_t per = std::max<size_t>(1, n * 5 / (size_t)w);
+    for (size_t a = 0; a < n; a += per) {
+        const size_t rows = std::min(per, n - a);
+        CK(launch_rows(src, h->xfer, h->perm_dev, (int)a, (int)rows, w, false, h->stream));
+        CK(cudaMemcpyAsync(dst + a * w, h->xfer, rows * w * 8, cudaMemcpyDeviceToHost, h->stream));
+    }
     return MFCFD_OK;
 }
 
@@ -290,7 +327,7 @@ int finish_chunk(mfcfd_handle *h, int32_t t0, int chunk, double *res_hist, int *
 // they are copied again); *warps receives the new schedule's warps.
 int apply_chain_schedule(mfcfd_handle *h, int want, int *warps) {
     int wpb = 0, blocks = 0;
-    const int w = chain_shape(h->P.device, want, &wpb, &blocks);
+    const int w = chain_shape(h->P.device, want, h->P.chain_spread, &wpb, &blocks);
     if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
     ChainSchedule S;
     build_chain_schedule(h->T, w, S);
@@ -315,6 +352,7 @@ int apply_chain_schedule(mfcfd_handle *h, int want, int *warps) {
         }
     d.ch_warps = w;
     d.ch_wpb = wpb;
+    d.ch_spread = h->P.chain_spread;
     drop_graphs(h);                        // their launches name the old schedule
     h->chain_terms[0] = S.terms_ring;
     h->chain_terms[1] = S.terms_local;
@@ -370,6 +408,7 @@ void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg) {
     p->device = 0;
     p->sweep_mode = MFCFD_SWEEP_CHAINS;
     p->graphs = 1;
+    p->storage_order = MFCFD_ORDER_MORTON;
 }
 
 }  // extern "C"
@@ -432,11 +471,23 @@ int create_impl(const mfcfd_params *params, int32_t n, const int32_t *status, co
         *out = h;
         return MFCFD_ERR_ARG;
     }
+    if (P.storage_order != MFCFD_ORDER_INDEX && P.storage_order != MFCFD_ORDER_MORTON) {
+        h->err = "unknown storage_order";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
     *out = h;   // also on failure: it holds the message
     return host_guard(&h->err, [&]() -> int {
         int rc = build_topology(P, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, h->T, h->err);
         if (rc) return rc;
         if (P.device < 0) return MFCFD_OK;   // host-only handle: set-up results, no device state
+        if (P.storage_order == MFCFD_ORDER_MORTON && n > 1) {
+            // the device layout follows a space-filling curve; the set-up
+            // above ran on the reference's indices and is relabelled
+            std::vector<int32_t> perm;
+            morton_order(n, x, y, z, perm);
+            permute_topology(h->T, perm);
+        }
         if ((rc = stage_host(h, x, y, z, tan1, tan2, nor, nbhs, conn))) return rc;
         if (attach) {
             if ((rc = attach_device(h))) return rc;
@@ -454,19 +505,31 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
     const int n = h->T.n;
     if (cudaSetDevice(P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
     auto st = std::make_unique<mfcfd_handle::Staged>();
-    st->x.assign(x, x + n);
-    st->y.assign(y, y + n);
-    st->z.assign(z, z + n);
+    // in storage order (T.perm; the identity when it is empty)
+    const std::vector<int32_t> &perm = h->T.perm;
+    auto at = [&](int i) { return perm.empty() ? (size_t)i : (size_t)perm[i]; };
+    st->x.resize(n);
+    st->y.resize(n);
+    st->z.resize(n);
     st->frame.resize((size_t)n * 9);
-    for (int i = 0; i < n; ++i)
-        for (int r = 0; r < 3; ++r) {
-            st->frame[9 * (size_t)i + r] = tan1[3 * (size_t)i + r];
-            st->frame[9 * (size_t)i + 3 + r] = tan2[3 * (size_t)i + r];
-            st->frame[9 * (size_t)i + 6 + r] = nor[3 * (size_t)i + r];
-        }
-    st->nbhs.assign(nbhs, nbhs + n);
+    st->nbhs.resize(n);
     st->conn.assign((size_t)n * MAX_CONN, 0);
-    for (size_t j = 0; j < st->conn.size(); ++j) st->conn[j] = conn[j] > 0 ? conn[j] - 1 : 0;
+    for (int i = 0; i < n; ++i) {
+        const size_t s = at(i);
+        st->x[s] = x[i];
+        st->y[s] = y[i];
+        st->z[s] = z[i];
+        for (int r = 0; r < 3; ++r) {
+            st->frame[9 * s + r] = tan1[3 * (size_t)i + r];
+            st->frame[9 * s + 3 + r] = tan2[3 * (size_t)i + r];
+            st->frame[9 * s + 6 + r] = nor[3 * (size_t)i + r];
+        }
+        st->nbhs[s] = nbhs[i];
+        for (int r = 0; r < MAX_CONN; ++r) {
+            const int32_t k = conn[(size_t)i * MAX_CONN + r];
+            st->conn[s * MAX_CONN + r] = k > 0 ? (int32_t)at(k - 1) : 0;
+        }
+    }
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
         // about twice the widest level in warps, all co-resident; the
         // schedule itself is built when first needed (attach_device), so a
@@ -474,7 +537,8 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
         if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
         const int want = P.chain_warps > 0 ? P.chain_warps : 2 * h->T.max_level_width;
         int blocks = 0;
-        st->ch_w = chain_shape(P.device, want, &st->ch_wpb, &blocks);
+        if (P.chain_spread < 0 || P.chain_spread > 1) return fail(h, MFCFD_ERR_ARG, "chain_spread must be 0 or 1");
+        st->ch_w = chain_shape(P.device, want, P.chain_spread, &st->ch_wpb, &blocks);
         if (st->ch_w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
     }
     h->staged = std::move(st);
@@ -525,6 +589,7 @@ int attach_device(mfcfd_handle *h) {
         const ChainSchedule &S = st.S;
         d.ch_warps = st.ch_w;
         d.ch_wpb = st.ch_wpb;
+        d.ch_spread = P.chain_spread;
         if ((rc = upload(h, &d.pre_order, st.pre))) return rc;
         for (int dir = 0; dir < 2; ++dir) {
             if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;
@@ -560,6 +625,12 @@ int attach_device(mfcfd_handle *h) {
     UP(fwd_old, T.fwd_old); UP(bwd_old, T.bwd_old); UP(sweep_slot_mask, T.sweep_slot_mask);
     if (!T.outer_delt.empty()) UP(outer_delt, T.outer_delt);
     UP(res_order, order);
+    if (!T.perm.empty()) {
+        const int32_t *pd = nullptr;
+        if ((rc = upload(h, &pd, T.perm))) return rc;
+        h->perm_dev = const_cast<int32_t *>(pd);
+        if ((rc = dalloc(h, &h->xfer, (size_t)n * 5))) return rc;
+    }
 #undef UP
     d.n_fwd_levels = (int)T.fwd_lvl_ptr.size() - 1;
     d.n_bwd_levels = (int)T.bwd_lvl_ptr.size() - 1;
@@ -667,7 +738,8 @@ int mfcfd_set_prim(mfcfd_handle *h, const double *prim) {
         if (!h || !prim) return MFCFD_ERR_ARG;
         if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
         size_t n5 = (size_t)h->d.n * 5;
-        CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+        int rc = rows_to_device(h, h->d.prim, prim, 5);
+        if (rc) return rc;
         CK(cudaMemsetAsync(h->d.dUp, 0, n5 * 8, h->stream));
         CK(cudaMemsetAsync(h->d.dUn, 0, n5 * 8, h->stream));
         DevCloud dc = h->d;
@@ -761,7 +833,9 @@ int mfcfd_get(mfcfd_handle *h, int32_t field, double *out) {
         case MFCFD_FIELD_DINV: src = d.dinv; w = 1; break;
         default: return fail(h, MFCFD_ERR_ARG, "unknown field");
         }
-        CK(cudaMemcpyAsync(out, src, n * w * 8, cudaMemcpyDeviceToHost, h->stream));
+        (void)n;
+        int rc = rows_to_host(h, out, src, (int)w);
+        if (rc) return rc;
         CK(cudaStreamSynchronize(h->stream));
         return MFCFD_OK;
     });
@@ -772,8 +846,10 @@ int mfcfd_get_state(mfcfd_handle *h, double *prim, double *delu, double *res_old
         if (!h || !prim || !delu) return MFCFD_ERR_ARG;
         if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
         size_t n5 = (size_t)h->d.n * 5;
-        CK(cudaMemcpyAsync(prim, h->d.prim, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(delu, h->d.dUn, n5 * 8, cudaMemcpyDeviceToHost, h->stream));
+        (void)n5;
+        int rc = rows_to_host(h, prim, h->d.prim, 5);
+        if (!rc) rc = rows_to_host(h, delu, h->d.dUn, 5);
+        if (rc) return rc;
         CK(cudaStreamSynchronize(h->stream));
         if (res_old) *res_old = h->res_old;
         return MFCFD_OK;
@@ -785,8 +861,9 @@ int mfcfd_set_state(mfcfd_handle *h, const double *prim, const double *delu, dou
         if (!h || !prim || !delu) return MFCFD_ERR_ARG;
         if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
         size_t n5 = (size_t)h->d.n * 5;
-        CK(cudaMemcpyAsync(h->d.prim, prim, n5 * 8, cudaMemcpyHostToDevice, h->stream));
-        CK(cudaMemcpyAsync(h->d.dUn, delu, n5 * 8, cudaMemcpyHostToDevice, h->stream));
+        int rc = rows_to_device(h, h->d.prim, prim, 5);
+        if (!rc) rc = rows_to_device(h, h->d.dUn, delu, 5);
+        if (rc) return rc;
         CK(cudaMemcpyAsync(h->d.dUp, h->d.dUn, n5 * 8, cudaMemcpyDeviceToDevice, h->stream));
         DevCloud dc = h->d;
         dc.U = h->U_buf[h->cur];
@@ -835,7 +912,9 @@ int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level) {
         const Topology &T = h->T;
         if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
         const std::vector<int32_t> &src = dir == 0 ? T.fwd_level : T.bwd_level;
-        std::memcpy(level, src.data(), sizeof(int32_t) * T.n);
+        if (T.perm.empty()) std::memcpy(level, src.data(), sizeof(int32_t) * T.n);
+        else
+            for (int i = 0; i < T.n; ++i) level[i] = src[T.perm[i]];
         return MFCFD_OK;
     });
 }
@@ -865,7 +944,9 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
             const int wpb = h->stream ? h->d.ch_wpb : (h->staged ? h->staged->ch_wpb : 0);
             const int w = h->stream ? h->d.ch_warps : (h->staged ? h->staged->ch_w : 0);
             info->chain_slots =
-                wpb > 0 ? w / wpb * chain_block_slots(h->P.device, wpb, h->P.precision == MFCFD_PRECISION_MIXED) : 0;
+                wpb > 0 ? (w + wpb - 1) / wpb * chain_block_slots(h->P.device, wpb, h->P.precision == MFCFD_PRECISION_MIXED,
+                                                      h->P.chain_spread)
+                        : 0;
             info->chain_slot_capacity = chain_slot_capacity(h->P.device);
             if (!info->chain_warps) info->chain_warps = w;
             info->g0_points = (int32_t)h->T.g0_pts.size();
@@ -965,8 +1046,9 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
         auto slots_of = [&](int32_t i) {
             const DevCloud &d = hs[i]->d;
             return d.sweep_mode == MFCFD_SWEEP_CHAINS
-                       ? d.ch_warps / d.ch_wpb *
-                             chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision == MFCFD_PRECISION_MIXED)
+                       ? (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb *
+                             chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision == MFCFD_PRECISION_MIXED,
+                                               d.ch_spread)
                        : 0;
         };
         int used = 0;
@@ -1028,7 +1110,7 @@ int mfcfd_set_chain_warps(mfcfd_handle *h, int32_t warps, int32_t *actual) {
         // a prepared handle: rebuild the staged schedule before it is attached
         mfcfd_handle::Staged &st = *h->staged;
         int blocks = 0;
-        const int w = chain_shape(h->P.device, warps, &st.ch_wpb, &blocks);
+        const int w = chain_shape(h->P.device, warps, h->P.chain_spread, &st.ch_wpb, &blocks);
         if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
         st.S = ChainSchedule();   // built for w at the next dry run or attach
         st.ch_w = w;
@@ -1112,7 +1194,8 @@ int mfcfd_set_wall_areas(mfcfd_handle *h, const double *area) {
             int rc = dalloc(h, &h->wall_area, (size_t)h->d.n);
             if (rc) return rc;
         }
-        CK(cudaMemcpyAsync(h->wall_area, area, sizeof(double) * (size_t)h->d.n, cudaMemcpyHostToDevice, h->stream));
+        int rc = rows_to_device(h, h->wall_area, area, 1);
+        if (rc) return rc;
         CK(cudaStreamSynchronize(h->stream));
         return MFCFD_OK;
     });
@@ -1194,16 +1277,18 @@ int mfcfd_print_primal_output(mfcfd_handle *h, const char *dir) {
         if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
         const size_t n = (size_t)h->d.n;
         std::vector<double> x(n), y(n), z(n), prim(5 * n), flux(5 * n), dq(15 * n);
-        CK(cudaMemcpyAsync(x.data(), h->d.x, n * 8, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(y.data(), h->d.y, n * 8, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(z.data(), h->d.z, n * 8, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(prim.data(), h->d.prim, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(flux.data(), h->d.flux_res, 5 * n * 8, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaMemcpyAsync(dq.data(), h->d.dq, 15 * n * 8, cudaMemcpyDeviceToHost, h->stream));
+        int rc = rows_to_host(h, x.data(), h->d.x, 1);
+        if (!rc) rc = rows_to_host(h, y.data(), h->d.y, 1);
+        if (!rc) rc = rows_to_host(h, z.data(), h->d.z, 1);
+        if (!rc) rc = rows_to_host(h, prim.data(), h->d.prim, 5);
+        if (!rc) rc = rows_to_host(h, flux.data(), h->d.flux_res, 5);
+        if (!rc) rc = rows_to_host(h, dq.data(), h->d.dq, 15);
+        if (rc) return rc;
         CK(cudaStreamSynchronize(h->stream));
         std::vector<int32_t> status(n);
-        for (size_t i = 0; i < n; ++i) status[i] = h->T.cls[i];   // statuses 0/1/2 are the classes
-        int rc = io_write_primal_output(dir, (int32_t)n, status.data(), x.data(), y.data(), z.data(), prim.data(),
+        const std::vector<int32_t> &perm = h->T.perm;   // statuses 0/1/2 are the classes
+        for (size_t i = 0; i < n; ++i) status[i] = h->T.cls[perm.empty() ? i : (size_t)perm[i]];
+        rc = io_write_primal_output(dir, (int32_t)n, status.data(), x.data(), y.data(), z.data(), prim.data(),
                                         flux.data(), dq.data());
         if (rc) return fail(h, rc, g_io_err);
         return MFCFD_OK;

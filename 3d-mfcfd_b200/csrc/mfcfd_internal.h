@@ -97,6 +97,11 @@ struct Topology {
     // from a kernel run before the sweeps; empty when they are more than an
     // eighth of the cloud (the table would cost more memory than it saves)
     std::vector<int32_t> g0_pts;
+    // storage permutation (empty: storage is the reference's index order):
+    // perm[logical] = storage index, inv[storage] = logical index.  The split
+    // lists, alias and point_with_alias keep logical ids; everything else
+    // above is in storage order once permute_topology has run.
+    std::vector<int32_t> perm, inv;
 };
 
 // One point of a sweep as a warp of the chain schedule reads it: the point,
@@ -172,6 +177,16 @@ int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, 
 int prep_levels_gpu(int device, int n, const std::vector<int> &order, const std::vector<int32_t> &doff,
                     const std::vector<int32_t> &deps, std::vector<int32_t> &level, std::string &err);
 void build_pre_order(const Topology &T, std::vector<int32_t> &order);
+// Storage order along a Morton (Z-order) curve of the coordinates, quantised
+// to 21 bits per axis over the cloud's bounding box; points with the same
+// key keep their index order.  perm[logical] = storage index.
+void morton_order(int n, const double *x, const double *y, const double *z, std::vector<int32_t> &perm);
+// Relabel the set-up from logical to storage order: every per-point array
+// is moved to its point's storage index and every point id is mapped, with
+// all orders (levels, index lists, supersonic copies, the residual's wall
+// then interior order) kept as they were.  Results do not change: each
+// point's arithmetic reads the same values in the same order.
+void permute_topology(Topology &T, const std::vector<int32_t> &perm);
 
 // Host threads for the set-up passes, one pool for every set-up running in
 // the process at once (the host's cores less two).  take_setup_threads
@@ -265,6 +280,7 @@ struct DevCloud {
                                   // none of its sweep increments; 0: off
     // chain schedule (per direction: 0 forward, 1 backward)
     int ch_warps, ch_wpb;         // warps and warps per block
+    int ch_spread;                // one chain block per SM (mfcfd_params.chain_spread)
     const int32_t *pre_order;     // all points, forward sweep order first (fused flux)
     const int32_t *ch_ptr[2], *ch_pts[2], *ch_own[2];
     const ChainItem *ch_items[2];
@@ -298,6 +314,10 @@ struct IterStreams {
 cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams &st,
                              double *U_next, double *q_next, cudaEvent_t *ev);
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
+// rows [a, a+rows) of width w: scatter from an index-order buffer to storage
+// order (dst[perm[a+i]] = src[i]), or gather the reverse
+cudaError_t launch_rows(const double *src, double *dst, const int32_t *perm, int a, int rows, int w, bool scatter,
+                        cudaStream_t s);
 // out[0..2] (device) = -sum over wall points of (p - p_inf) A nor
 cudaError_t launch_forces(const DevCloud &d, cudaStream_t s, double area_each, const double *area, double *out);
 int reduction_blocks(int n);
@@ -306,7 +326,7 @@ int device_sms(int device);
 // Launch shape of the chain sweep for about `want` warps: warps per block
 // and blocks (at most SMs - 16 blocks); returns the warps, 0 if the kernel
 // cannot run on the device.
-int chain_shape(int device, int want, int *wpb, int *blocks);
+int chain_shape(int device, int want, int spread, int *wpb, int *blocks);
 // Per-device launch set-up (kernel attributes), done before a stream capture.
 void prepare_launches(int device);
 // Chain-sweep blocks that may run at once, in slots of a sixth of an SM: a
@@ -314,7 +334,7 @@ void prepare_launches(int device);
 // of the mixed-precision sweep (three per SM), 3 for a 4-warp block of the
 // FP64 sweep, 6 for an 8-warp block; see k_sweep_chain.
 int chain_slot_capacity(int device);
-int chain_block_slots(int device, int wpb, bool mixed);
+int chain_block_slots(int device, int wpb, bool mixed, int spread = 0);
 // File formats of the reference program (mfcfd_io.cpp).  Handle-less calls
 // leave their message in g_io_err (mfcfd_last_error(NULL)).
 extern thread_local std::string g_io_err;

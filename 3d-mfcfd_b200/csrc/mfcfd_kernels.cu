@@ -1102,6 +1102,17 @@ static int chain_smem() {
 }
 // three 4-warp blocks per SM: 228 KB of shared memory, 1 KB of it reserved per block
 static_assert(3 * (4 * CHAIN_SMEM_BYTES + 1024) <= 228 * 1024, "three 4-warp chain blocks per SM");
+// A spread chain block asks for this much shared memory, so that no second
+// block fits beside it (2 x (116 + 1) KB > 228 KB) and each of its four
+// warps has one of the SM's four sub-partitions to itself.
+constexpr int CHAIN_SPREAD_SMEM = 116 * 1024;
+static_assert(2 * (CHAIN_SPREAD_SMEM + 1024) > 228 * 1024 && CHAIN_SPREAD_SMEM >= 4 * CHAIN_SMEM_BYTES,
+              "a spread block holds its SM alone");
+
+static int chain_smem_bytes(int wpb, int spread) {
+    if (wpb == 4) return spread ? CHAIN_SPREAD_SMEM : chain_smem<4>();
+    return chain_smem<8>();
+}
 
 // ---------------------------------------------------------------- state update
 
@@ -1348,9 +1359,9 @@ static void set_attributes(int device) {
     // driver, which keeps more L1 for their loads and the flux kernel's
     cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
-    cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
+    cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
     cudaFuncSetAttribute(k_sweep_chain<8, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
-    cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<4>());
+    cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
     cudaFuncSetAttribute(k_sweep_chain<8, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     done[device] = true;
 }
@@ -1363,10 +1374,10 @@ int chain_slot_capacity(int device) {
     return 6 * (sms - CH_FREE_SMS);
 }
 
-int chain_block_slots(int device, int wpb, bool mixed) {
+int chain_block_slots(int device, int wpb, bool mixed, int spread) {
     static std::mutex mu;
     static int cache[256][2][2] = {};
-    if (device < 0 || device >= 256) return 6;
+    if (device < 0 || device >= 256 || spread) return 6;
     const int w8 = wpb == 8 ? 1 : 0, m = mixed ? 1 : 0;
     {
         std::lock_guard<std::mutex> lock(mu);
@@ -1390,12 +1401,23 @@ int chain_block_slots(int device, int wpb, bool mixed) {
     return cache[device][w8][m] = 6 / per_sm;
 }
 
-int chain_shape(int device, int want, int *wpb, int *blocks) {
+int chain_shape(int device, int want, int spread, int *wpb, int *blocks) {
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     set_attributes(device);
     const int max_blocks = sms - CH_FREE_SMS;
     if (max_blocks < 1) return 0;
+    if (spread) {
+        // 4-warp blocks, one per SM
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double>, 4 * 32, CHAIN_SPREAD_SMEM);
+        if (per_sm < 1) return 0;
+        *wpb = 4;
+        int b = (want + 3) / 4;
+        b = b > max_blocks ? max_blocks : (b < 1 ? 1 : b);
+        *blocks = b;
+        return 4 * b;
+    }
     *wpb = want <= 4 * max_blocks ? 4 : 8;
     // with 8-warp blocks, three quarters of the warps: more SMs stay with the
     // concurrent flux kernel, which then keeps ahead of the forward sweep
@@ -1410,7 +1432,35 @@ int chain_shape(int device, int want, int *wpb, int *blocks) {
     if (b > max_blocks) b = max_blocks;
     if (b < 1) b = 1;
     *blocks = b;
-    return b * *wpb;
+    // fewer warps than one block asked for (a single-warp chain measures the
+    // per-point latency floor): the block's other warps exit at once
+    return want < *wpb ? (want < 1 ? 1 : want) : b * *wpb;
+}
+
+// Rows [a, a + rows) of width w between the reference's index order and
+// the storage order: scatter puts row i of src (a transfer buffer in index
+// order) at storage row perm[a + i] of dst; gather does the reverse.
+__global__ void k_rows(const double *src, double *dst, const int32_t *perm, int a, int rows, int w, int scatter) {
+    const size_t total = (size_t)rows * w;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = t / w, c = t - i * w;
+        const size_t s = (size_t)perm[a + i];
+        if (scatter) dst[s * w + c] = src[t];
+        else dst[t] = src[s * w + c];
+    }
+}
+
+cudaError_t launch_rows(const double *src, double *dst, const int32_t *perm, int a, int rows, int w, bool scatter,
+                        cudaStream_t s) {
+    const size_t total = (size_t)rows * w;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    size_t blocks = (total + 255) / 256;
+    const size_t cap = (size_t)device_sms(dev) * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    k_rows<<<(int)blocks, 256, 0, s>>>(src, dst, perm, a, rows, w, scatter ? 1 : 0);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s) {
@@ -1461,13 +1511,14 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     const bool mixed = d.precision == MFCFD_PRECISION_MIXED;   // chain schedule only
     auto sweep = [&](int forward) {
         if (chains) {
-            const int blocks = d.ch_warps / d.ch_wpb;
+            const int blocks = (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb;
+            const int csm = chain_smem_bytes(d.ch_wpb, d.ch_spread);
             if (mixed) {
-                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float>, blocks, 4 * 32, chain_smem<4>(), s, true, d, forward);
-                else launch_prio(k_sweep_chain<8, float>, blocks, 8 * 32, chain_smem<8>(), s, true, d, forward);
+                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float>, blocks, 4 * 32, csm, s, true, d, forward);
+                else launch_prio(k_sweep_chain<8, float>, blocks, 8 * 32, csm, s, true, d, forward);
             } else {
-                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, double>, blocks, 4 * 32, chain_smem<4>(), s, true, d, forward);
-                else launch_prio(k_sweep_chain<8, double>, blocks, 8 * 32, chain_smem<8>(), s, true, d, forward);
+                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, double>, blocks, 4 * 32, csm, s, true, d, forward);
+                else launch_prio(k_sweep_chain<8, double>, blocks, 8 * 32, csm, s, true, d, forward);
             }
         } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);

@@ -878,4 +878,127 @@ void build_pre_order(const Topology &T, std::vector<int32_t> &order) {
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key[a] < key[b]; });
 }
 
+// ---- storage order along a space-filling curve
+
+namespace {
+
+// the bits of v (21 of them) spread to every third bit
+inline uint64_t spread3(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+// per-point rows of width w moved to their storage index
+template <typename V>
+void permute_rows(std::vector<V> &a, const std::vector<int32_t> &perm, size_t w) {
+    if (a.empty()) return;
+    std::vector<V> b(a.size());
+    const int n = (int)perm.size();
+    parallel_for(n, [&](int i) {
+        std::copy(a.begin() + (size_t)i * w, a.begin() + (size_t)(i + 1) * w, b.begin() + (size_t)perm[i] * w);
+    });
+    a.swap(b);
+}
+
+// point ids (0-based; negative: none) mapped in place
+void map_ids(std::vector<int32_t> &a, const std::vector<int32_t> &perm) {
+    parallel_for((int)a.size(), [&](int j) {
+        if (a[j] >= 0) a[j] = perm[a[j]];
+    });
+}
+
+// a point's contiguous sweep entries, re-laid in storage order with mapped ids
+void permute_entries(std::vector<int32_t> &off, std::vector<SweepEntry> &ent, const std::vector<int32_t> &perm,
+                     const std::vector<int32_t> &inv) {
+    const int n = (int)perm.size();
+    std::vector<int32_t> noff(n + 1, 0);
+    for (int q = 0; q < n; ++q) noff[q + 1] = noff[q] + (off[inv[q] + 1] - off[inv[q]]);
+    std::vector<SweepEntry> nent(ent.size());
+    parallel_for(n, [&](int q) {
+        const int p = inv[q];
+        int at = noff[q];
+        for (int e = off[p]; e < off[p + 1]; ++e) {
+            SweepEntry E = ent[e];
+            if (E.k >= 0) E.k = perm[E.k];
+            nent[at++] = E;
+        }
+    });
+    off.swap(noff);
+    ent.swap(nent);
+}
+
+}  // namespace
+
+void morton_order(int n, const double *x, const double *y, const double *z, std::vector<int32_t> &perm) {
+    double lo[3] = {x[0], y[0], z[0]}, hi[3] = {x[0], y[0], z[0]};
+    for (int i = 1; i < n; ++i) {
+        const double v[3] = {x[i], y[i], z[i]};
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], v[a]);
+            hi[a] = std::max(hi[a], v[a]);
+        }
+    }
+    double scale[3];
+    for (int a = 0; a < 3; ++a) scale[a] = hi[a] > lo[a] ? 2097151.0 / (hi[a] - lo[a]) : 0.0;
+    std::vector<std::pair<uint64_t, int32_t>> key(n);
+    parallel_for(n, [&](int i) {
+        const double v[3] = {x[i], y[i], z[i]};
+        uint64_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            double t = (v[a] - lo[a]) * scale[a];
+            t = t < 0.0 ? 0.0 : (t > 2097151.0 ? 2097151.0 : t);
+            q[a] = (uint64_t)t;
+        }
+        key[i] = {spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2), i};
+    });
+    std::sort(key.begin(), key.end());     // (key, index): ties in index order
+    perm.assign(n, 0);
+    for (int s = 0; s < n; ++s) perm[key[s].second] = s;
+}
+
+void permute_topology(Topology &T, const std::vector<int32_t> &perm) {
+    const int n = T.n;
+    T.perm = perm;
+    T.inv.assign(n, 0);
+    for (int i = 0; i < n; ++i) T.inv[perm[i]] = i;
+    // per-point rows
+    permute_rows(T.cls, perm, 1);
+    permute_rows(T.slot_nbr, perm, MAX_SLOTS);
+    map_ids(T.slot_nbr, perm);
+    permute_rows(T.nslot, perm, 1);
+    permute_rows(T.slot_mask, perm, MAX_SLOTS);
+    permute_rows(T.list_cnt, perm, NDIR);
+    permute_rows(T.list_ent, perm, (size_t)NDIR * LIST_STRIDE);
+    permute_rows(T.geo, perm, GEO_STRIDE);
+    permute_rows(T.eps2, perm, 1);
+    permute_rows(T.wq, perm, MAX_CONN);
+    permute_rows(T.wf, perm, MAX_SLOTS);
+    permute_rows(T.fwd_level, perm, 1);
+    permute_rows(T.bwd_level, perm, 1);
+    permute_rows(T.fwd_cnt, perm, NDIR);
+    permute_rows(T.bwd_cnt, perm, NDIR);
+    permute_rows(T.fwd_need, perm, 1);
+    permute_rows(T.bwd_need, perm, 1);
+    permute_rows(T.fwd_old, perm, 1);
+    permute_rows(T.bwd_old, perm, 1);
+    permute_rows(T.sweep_slot_mask, perm, MAX_SLOTS);
+    permute_rows(T.outer_delt, perm, 1);
+    permute_rows(T.swept, perm, 1);
+    permute_rows(T.consumer_shared, perm, 1);
+    permute_rows(T.copy_src, perm, 1);
+    map_ids(T.copy_src, perm);
+    // entries of each sweep, contiguous per point in storage order
+    permute_entries(T.fwd_off, T.fwd_ent, perm, T.inv);
+    permute_entries(T.bwd_off, T.bwd_ent, perm, T.inv);
+    // id lists, their order kept
+    for (std::vector<int32_t> *a : {&T.fwd_lvl_pts, &T.bwd_lvl_pts, &T.wall_idx, &T.outer_idx, &T.interior_idx,
+                                    &T.ss_inlet_idx, &T.ss_outlet_idx, &T.ss_pts, &T.ss_src, &T.g0_pts})
+        map_ids(*a, perm);
+}
+
 }  // namespace mfcfd

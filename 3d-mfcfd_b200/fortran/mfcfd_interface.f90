@@ -17,6 +17,7 @@ module mfcfd_interface
     integer(c_int32_t), parameter :: MFCFD_PRECISION_FP64 = 0, MFCFD_PRECISION_MIXED = 1
     integer(c_int32_t), parameter :: MFCFD_UPDATE_IMPLICIT = 0, MFCFD_UPDATE_EXPLICIT = 1
     integer(c_int32_t), parameter :: MFCFD_SWEEPS_ALIAS = 0, MFCFD_SWEEPS_BACKUP = 1
+    integer(c_int32_t), parameter :: MFCFD_ORDER_INDEX = 0, MFCFD_ORDER_MORTON = 1
 
     ! mirror of struct mfcfd_params
     type, bind(C) :: mfcfd_params
@@ -24,7 +25,7 @@ module mfcfd_interface
         real(c_double) :: rho_inf, u1_inf, u2_inf, u3_inf, pr_inf
         integer(c_int32_t) :: inner_iterations, split_capacity, precision, device, sweep_mode
         integer(c_int32_t) :: update_variant, sweep_variant, chain_warps, gpu_setup, graphs
-        integer(c_int32_t) :: reserved(2)
+        integer(c_int32_t) :: chain_spread, storage_order
     end type mfcfd_params
 
     interface
@@ -105,6 +106,13 @@ module mfcfd_interface
             real(c_double), intent(out) :: res_new
             integer(c_int) :: rc
         end function mfcfd_residual_noalloc
+
+        function mfcfd_set_fault_hook(h, point, wait_limit) result(rc) bind(C, name="mfcfd_set_fault_hook")
+            import :: c_ptr, c_int32_t, c_int
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: point, wait_limit
+            integer(c_int) :: rc
+        end function mfcfd_set_fault_hook
 
         ! the reference program's files (meshfree_solver.f90:20-37)
         function mfcfd_count_input_points(path, n) result(rc) bind(C, name="mfcfd_count_input_points")

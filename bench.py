@@ -12,7 +12,12 @@ cloud is seeded synthetic data from the package generator.  Its state
              copies prim and delU in from pinned host memory (mfcfd_set_state),
              iterates (mfcfd_fpi_step) and copies them back (mfcfd_get_state).
 ``roofline`` the dominant phase's algorithmic bytes (per point, from the
-             byte model of each phase) over its event-timed duration.
+             byte model of each phase) over its event-timed duration; its
+             ``fp64`` part gives the same phase's FP64 operations (counted
+             by the oracle built with counting arithmetic) over that time
+             against the device's FMA rate measured by an in-tree loop
+             kernel, and ``sweep_latency_floor_us`` one warp's time per
+             swept point when it sweeps a small cloud alone.
 Multi-GPU: independent replicas, one per rank (the LU-SGS sweep order is
 global, so one cloud does not shard); value sums the ranks' points.
 
@@ -53,6 +58,21 @@ TOTAL_BYTES = 3368
 # point count, so a launch of n points moves about n times this.
 SWEEP_TRAFFIC_PER_POINT = 160.78e6 / 62400
 
+# FP64 operations per point-iteration of each phase, counted by the oracle
+# built with counting arithmetic (oracle/oracle_flops.cpp: add, multiply,
+# divide and sqrt one each, fma two, exp/log/erf through their own
+# arithmetic in mfmath.h) over the third iteration of each workload:
+#   oracle.flop_counts(cloud.sphere_1m(), 0.8, 2.0, iters=1, skip=2)
+#   oracle.flop_counts(cloud.sphere_62k(), 0.4, 0.0, iters=1, skip=2)
+# divided by the point count.  The reference evaluates D_inv again in the
+# backward sweep; that repeat is left out (the GPU evaluates it once).
+PHASE_FLOPS = {
+    "sphere-1.1M": {"qderiv": 2814.0, "flux": 54246.0, "dinv": 3525.5, "sweep_fwd": 17626.3,
+                    "sweep_bwd": 16805.6, "update": 162.0, "residual": 0.0},
+    "sphere-62k": {"qderiv": 2814.0, "flux": 55989.0, "dinv": 3488.0, "sweep_fwd": 18102.5,
+                   "sweep_bwd": 16082.6, "update": 165.1, "residual": 0.0},
+}
+
 WORKLOADS = {
     "sphere-1.1M": dict(shells=96, per_shell=11500, jitter=0.01, mach=0.8, aoa=2.0, seed=2001),
     "sphere-62k": dict(shells=48, per_shell=1300, jitter=0.02, mach=0.4, aoa=0.0, seed=1001),
@@ -61,6 +81,39 @@ WORKLOADS = {
 # k_flux, two k_sweep_chain, k_update, two reductions, and k_g0 when the
 # cloud has points outside the shared frame; 0/1 add k_dinv_gold)
 KERNELS_PER_ITER = {2: 8, 0: 9, 1: 9}
+
+
+def fp64_peak(device):
+    """FP64 TFLOP/s of the device, measured now by the FMA-loop kernel of
+    mfcfd/libmfcfd_peak.so (best of 5 launches, CUDA events)."""
+    import ctypes
+    L = ctypes.CDLL(os.path.join(PKG, "mfcfd", "libmfcfd_peak.so"))
+    L.mfcfd_fp64_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    tf, ms = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    rc = L.mfcfd_fp64_fma_peak(int(device), 5, ctypes.byref(tf), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"fp64 peak kernel failed: CUDA error {rc}")
+    return tf.value
+
+
+def sweep_latency_floor(device, sweep_mode_kw):
+    """Microseconds per swept point of the backward sweep when one warp
+    sweeps a small cloud (8 shells x 150 points) alone: every hand-off stays
+    in the warp, so this is one point's critical path."""
+    from mfcfd import cloud as cl
+    from mfcfd.solver import Solver
+    c = cl.small_sphere()
+    s = Solver(c, 0.8, 2.0, device=device, chain_warps=1, **sweep_mode_kw)
+    s.initial_conditions()
+    s.q_lskum(3)
+    s.set_profiling(True)
+    s.q_lskum(5, t0=4)
+    ph, it = s.phase_times()
+    n_swept = c.n - int((c.status == cl.STATUS_OUTER).sum()) - 1
+    info = s.info()
+    s.close()
+    return {"us_per_point": ph["sweep_bwd"] * 1e3 / max(it, 1) / max(n_swept, 1),
+            "points": c.n, "warps": info["chain_warps"], "levels_backward": info["n_levels_backward"]}
 
 
 def load_peaks():
@@ -184,6 +237,7 @@ def main():
     ap.add_argument("--batch-clouds", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
+    ap.add_argument("--chain-spread", type=int, default=0, help="1: one 4-warp chain block per SM")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     ap.add_argument("--serve-requests", type=int, default=40)
@@ -235,7 +289,8 @@ def main():
 
     c = cl.shell_cloud(wl["shells"], wl["per_shell"], jitter=wl["jitter"],
                        seed=replicas.replica_seed(wl["seed"], rank))
-    s = Solver(c, wl["mach"], wl["aoa"], device=local_rank, sweep_mode=args.sweep_mode)
+    s = Solver(c, wl["mach"], wl["aoa"], device=local_rank, sweep_mode=args.sweep_mode,
+               chain_spread=args.chain_spread)
     prim0 = cl.initial_state(c, wl["mach"], wl["aoa"])
     s.initial_conditions(prim0)
     info = s.info()
@@ -288,7 +343,28 @@ def main():
                 # the sweeps are bound by their dependency chain, not by HBM:
                 # levels of the schedule and device time per level
                 "sweep_us_per_level": dom_ms * 1e3 / max(1, info["n_levels_forward"]
-                                                        if dom == "sweep_fwd" else info["n_levels_backward"])}
+                                                        if dom == "sweep_fwd" else info["n_levels_backward"]),
+                "sweep_us_per_level_both": {
+                    "forward": phases["sweep_fwd"] / max(piters, 1) * 1e3 / max(1, info["n_levels_forward"]),
+                    "backward": phases["sweep_bwd"] / max(piters, 1) * 1e3 / max(1, info["n_levels_backward"])}}
+    flops = PHASE_FLOPS.get(args.workload)
+    if flops:
+        pk64 = fp64_peak(local_rank)
+        it_flops = sum(flops.values())
+        dom_tf = flops[dom] * c.n / (dom_ms / 1e3) / 1e12
+        it_tf = it_flops * c.n / (ms_max / args.steps / 1e3) / 1e12
+        roofline["fp64"] = {"phase": dom, "flops_per_point": flops[dom], "achieved": dom_tf, "peak": pk64,
+                            "unit": "TFLOP/s", "frac": dom_tf / pk64,
+                            "iteration_flops_per_point": it_flops, "iteration_achieved": it_tf,
+                            "iteration_frac": it_tf / pk64,
+                            "phase_flops_per_point": flops,
+                            "peak_source": "builder-measured: FMA loop kernel (libmfcfd_peak.so), best of 5, "
+                                           "CUDA events, on this GPU in this run",
+                            "counted_by": "oracle built with counting arithmetic (oracle/oracle_flops.cpp)"}
+    if args.sweep_mode == 2:
+        floor = sweep_latency_floor(local_rank, {})
+        roofline["sweep_latency_floor_us"] = floor["us_per_point"]
+        roofline["sweep_latency_floor"] = floor
 
     # end to end through the C ABI with pinned host buffers
     prim_h = torch.empty((c.n, 5), dtype=torch.float64, pin_memory=True).numpy()

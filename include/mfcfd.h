@@ -96,8 +96,20 @@ typedef struct mfcfd_params {
     int32_t graphs;           /* chunks of iterations captured once as CUDA graphs and
                                  replayed: 1 (default) in mfcfd_run_batch, 2 also in
                                  single-handle runs, 0 never (kernels one by one) */
-    int32_t reserved[2];
+    int32_t chain_spread;     /* CHAINS: 1 runs the sweep as 4-warp blocks of which each SM
+                                 holds one, so every warp has an SM sub-partition to
+                                 itself; 0 (default) packs blocks as residency allows */
+    int32_t storage_order;    /* MFCFD_ORDER_MORTON (default) or MFCFD_ORDER_INDEX */
 } mfcfd_params;
+
+/* Order of the points in device memory.  The set-up (split lists, alias
+ * search, sweep order) always works on the reference's point indices, and
+ * every array crossing this interface is in that index order; only the
+ * device layout changes.  MORTON stores the points along a Morton (Z-order)
+ * curve of their coordinates, so a point's neighbours lie near it in memory;
+ * INDEX keeps the caller's order.  Results are the same bits either way. */
+#define MFCFD_ORDER_INDEX     0
+#define MFCFD_ORDER_MORTON    1
 
 /* The reference ships two drivers of its sweep module.  ALIAS:
  * implicit_forward_and_reverse_sweeps.f90 (the active build) sweeps wall and

@@ -37,6 +37,11 @@
 
 #include "../3d-mfcfd_b200/csrc/mfmath.h"
 
+// Phase marks for the counting build (oracle_flops.cpp); nothing otherwise.
+#ifndef ORACLE_PHASE
+#define ORACLE_PHASE(k) ((void)0)
+#endif
+
 namespace {
 
 struct OracleParams {
@@ -861,8 +866,10 @@ void implicit_forward_backward_sweeps(Oracle &o) {
         if (p == 0) continue;   // out of the reference's range; touches no point
         int st = o.status[p];
         if (st == 1 || st == 0) {
+            ORACLE_PHASE(3);
             double D_inv = implicit_D_inv(o, p, st == 1);
             o.dinv[p] = D_inv;
+            ORACLE_PHASE(4);
             sweep_LU(o, p, st == 1, true, LdelU);
             for (int r = 0; r < 5; ++r)
                 o.V5(o.delUp, r + 1, p) = -(D_inv * (o.V5(o.flux_res, r + 1, p) + LdelU[r]));
@@ -876,7 +883,9 @@ void implicit_forward_backward_sweeps(Oracle &o) {
         if (p == 0) continue;
         int st = o.status[p];
         if (st == 1 || st == 0) {
+            ORACLE_PHASE(7);    // the same D_inv again (implicit_forward_and_reverse_sweeps.f90:63)
             double D_inv = implicit_D_inv(o, p, st == 1);
+            ORACLE_PHASE(5);
             sweep_LU(o, p, st == 1, false, LdelU);
             for (int r = 0; r < 5; ++r)
                 o.V5(o.delUn, r + 1, p) = o.V5(o.delUp, r + 1, p) - D_inv * LdelU[r];
@@ -972,15 +981,21 @@ void state_update_explicit(Oracle &o) {
 
 // fpi_solver.f90:20-45
 void fpi_solver(Oracle &o, int t) {
+    ORACLE_PHASE(0);
     compute_conserved_vector(o);
     eval_q_variables(o);
+    ORACLE_PHASE(1);
     eval_q_derivatives(o);
     timestep_delt(o);
+    ORACLE_PHASE(2);
     eval_flux_residual(o);
+    ORACLE_PHASE(4);
     if (o.P.sweep_variant) sweeps_backup(o);
     else implicit_forward_backward_sweeps(o);
+    ORACLE_PHASE(6);
     if (o.P.update_variant) state_update_explicit(o);
     else state_update(o);
+    ORACLE_PHASE(7);
     if (t <= 2) {
         o.res_old = o.res_new;
         o.residue = 0.0;

@@ -140,6 +140,57 @@ class Oracle:
             pass
 
 
+_FLOPS_LIB_PATH = os.path.join(_HERE, "_build", "liboracle_flops.so")
+FLOP_PHASE_NAMES = ("conserved_q", "qderiv_delt", "flux", "dinv", "sweep_fwd", "sweep_bwd", "update",
+                    "other")
+FLOP_KINDS = ("add", "mul", "div", "sqrt", "fma", "exp", "log", "erf", "pow")
+
+
+def flop_counts(cloud, mach, aoa_deg, iters=1, libm=LIBM_MFMATH, prim0=None, skip=0):
+    """FP64 operations of `iters` iterations (after `skip` uncounted ones)
+    of the oracle built with counting arithmetic (oracle_flops.cpp), per
+    phase of fpi_solver: {phase: {kind: count}}, fma counted once per call
+    (two operations).  With libm MFMATH the transcendentals are counted
+    through their own arithmetic; exp/log/erf/pow are also given as calls."""
+    if not os.path.exists(_FLOPS_LIB_PATH):
+        build()
+    from mfcfd.cloud import freestream, initial_state   # noqa: deferred import
+    L = ctypes.CDLL(_FLOPS_LIB_PATH)
+    vp = ctypes.c_void_p
+    L.oracle_create.restype = vp
+    L.oracle_create.argtypes = [ctypes.POINTER(_Params), ctypes.c_int] + [vp] * 10
+    L.oracle_set_prim.argtypes = [vp, vp]
+    L.oracle_set_libm.argtypes = [ctypes.c_int]
+    L.oracle_fpi_step.argtypes = [vp, ctypes.c_int, vp, vp]
+    L.oracle_flops_get.argtypes = [vp]
+    L.oracle_destroy.argtypes = [vp]
+    rho, u1, u2, u3, pr = freestream(mach, aoa_deg)
+    params = _Params(0.0, 2.0, 5.0, rho, u1, u2, u3, pr, 0, 22, 0, 0)
+    keep = [np.ascontiguousarray(a) for a in (
+        cloud.status.astype(np.int32), cloud.x, cloud.y, cloud.z, cloud.tan1, cloud.tan2, cloud.nor,
+        cloud.nbhs.astype(np.int32), cloud.conn.astype(np.int32), cloud.min_dist)]
+    h = L.oracle_create(ctypes.byref(params), cloud.n, *[_ptr(a) for a in keep])
+    p0 = np.ascontiguousarray(initial_state(cloud, mach, aoa_deg) if prim0 is None else prim0,
+                              dtype=np.float64)
+    L.oracle_set_prim(h, _ptr(p0))
+    L.oracle_set_libm(int(libm))
+    r = np.zeros(2)
+    for t in range(1, skip + 1):
+        L.oracle_fpi_step(h, t, _ptr(r[0:1]), _ptr(r[1:2]))
+    L.oracle_flops_reset()
+    for t in range(skip + 1, skip + iters + 1):
+        L.oracle_fpi_step(h, t, _ptr(r[0:1]), _ptr(r[1:2]))
+    out = np.zeros((len(FLOP_PHASE_NAMES), len(FLOP_KINDS)), dtype=np.int64)
+    L.oracle_flops_get(_ptr(out))
+    L.oracle_destroy(h)
+    return {ph: {k: int(out[i, j]) for j, k in enumerate(FLOP_KINDS)} for i, ph in enumerate(FLOP_PHASE_NAMES)}
+
+
+def flops_of(counts: dict) -> int:
+    """Operations of one phase's counts: add, mul, div, sqrt one each, fma two."""
+    return counts["add"] + counts["mul"] + counts["div"] + counts["sqrt"] + 2 * counts["fma"]
+
+
 def forces(cloud, prim, mach, aoa_deg, wall_area=None, ref_area=None):
     """(CL, CD, F) of a state, summed over wall points in index order (the
     project's force definition; the reference computes none):
