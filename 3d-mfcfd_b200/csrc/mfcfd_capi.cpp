@@ -450,12 +450,13 @@ int create_impl(const mfcfd_params *params, int32_t n, const int32_t *status, co
         *out = h;
         return MFCFD_ERR_ARG;
     }
-    if (P.precision != MFCFD_PRECISION_FP64 && P.precision != MFCFD_PRECISION_MIXED) {
+    if (P.precision != MFCFD_PRECISION_FP64 && P.precision != MFCFD_PRECISION_MIXED &&
+        P.precision != MFCFD_PRECISION_MIXED_DC) {
         h->err = "unknown precision";
         *out = h;
         return MFCFD_ERR_UNSUPPORTED;
     }
-    if (P.precision == MFCFD_PRECISION_MIXED && P.sweep_mode != MFCFD_SWEEP_CHAINS) {
+    if (P.precision != MFCFD_PRECISION_FP64 && P.sweep_mode != MFCFD_SWEEP_CHAINS) {
         h->err = "mixed precision requires the chain sweep schedule";
         *out = h;
         return MFCFD_ERR_UNSUPPORTED;
@@ -944,7 +945,7 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
             const int wpb = h->stream ? h->d.ch_wpb : (h->staged ? h->staged->ch_wpb : 0);
             const int w = h->stream ? h->d.ch_warps : (h->staged ? h->staged->ch_w : 0);
             info->chain_slots =
-                wpb > 0 ? (w + wpb - 1) / wpb * chain_block_slots(h->P.device, wpb, h->P.precision == MFCFD_PRECISION_MIXED,
+                wpb > 0 ? (w + wpb - 1) / wpb * chain_block_slots(h->P.device, wpb, h->P.precision != MFCFD_PRECISION_FP64,
                                                       h->P.chain_spread)
                         : 0;
             info->chain_slot_capacity = chain_slot_capacity(h->P.device);
@@ -1047,7 +1048,7 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
             const DevCloud &d = hs[i]->d;
             return d.sweep_mode == MFCFD_SWEEP_CHAINS
                        ? (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb *
-                             chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision == MFCFD_PRECISION_MIXED,
+                             chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision != MFCFD_PRECISION_FP64,
                                                d.ch_spread)
                        : 0;
         };

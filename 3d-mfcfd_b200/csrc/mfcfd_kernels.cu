@@ -386,7 +386,9 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
 //
 // R: the type of the reconstruction, limiter and flux arithmetic (float in
 // mixed precision); the offsets, weights, list sums and 3x3 solves are double.
-template <bool FUSED, typename R>
+// RS: the type of the sweep inputs' fluxes (float whenever the sweeps run in
+// FP32, so that a sweep differences fluxes evaluated the same way).
+template <bool FUSED, typename R, typename RS = R>
 __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -472,7 +474,7 @@ __global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
                 else d.flux_res[5 * (size_t)p + lane] = r;
             }
         }
-        if (FUSED) sweep_inputs_warp<R>(d, p, lane);
+        if (FUSED) sweep_inputs_warp<RS>(d, p, lane);
         __syncwarp();
     }
 }
@@ -1351,6 +1353,8 @@ static void set_attributes(int device) {
                          FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
     cudaFuncSetAttribute(k_flux<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
+    cudaFuncSetAttribute(k_flux<true, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         FLUX_WARPS * FLUX_SMEM_PER_WARP * 8);
     cudaFuncSetAttribute(k_sweep_levels, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SWEEP_WARPS * SWEEP_SMEM_BYTES);
     cudaFuncSetAttribute(k_sweep_df, cudaFuncAttributeMaxDynamicSharedMemorySize, DF_WARPS * SWEEP_SMEM_BYTES);
@@ -1508,7 +1512,8 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     df_warps = df_warps < 64 ? 64 : (df_warps > sms * 8 ? sms * 8 : df_warps);
     const int df_blocks = (df_warps + DF_WARPS - 1) / DF_WARPS;
     const bool chains = d.sweep_mode == MFCFD_SWEEP_CHAINS;
-    const bool mixed = d.precision == MFCFD_PRECISION_MIXED;   // chain schedule only
+    const bool mixed = d.precision != MFCFD_PRECISION_FP64;    // FP32 sweeps; chain schedule only
+    const bool dc = d.precision == MFCFD_PRECISION_MIXED_DC;   // ... with the FP64 flux residual
     auto sweep = [&](int forward) {
         if (chains) {
             const int blocks = (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb;
@@ -1558,7 +1563,8 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         cudaEventRecord(st.fork, s);
         cudaStreamWaitEvent(st.side, st.fork, 0);
         const size_t fsm = FLUX_WARPS * FLUX_SMEM_PER_WARP * 8;
-        if (mixed) launch_prio(k_flux<true, float>, fblocks, FLUX_WARPS * 32, fsm, st.side, false, d);
+        if (dc) launch_prio(k_flux<true, double, float>, fblocks, FLUX_WARPS * 32, fsm, st.side, false, d);
+        else if (mixed) launch_prio(k_flux<true, float>, fblocks, FLUX_WARPS * 32, fsm, st.side, false, d);
         else launch_prio(k_flux<true, double>, fblocks, FLUX_WARPS * 32, fsm, st.side, false, d);
         mark(2, st.side);
         cudaEventRecord(st.join, st.side);

@@ -14,7 +14,8 @@ module mfcfd_interface
         MFCFD_FIELD_DELUP = 7, MFCFD_FIELD_DELUN = 8, MFCFD_FIELD_DINV = 9
     integer(c_int32_t), parameter :: MFCFD_SWEEP_DATAFLOW = 0, MFCFD_SWEEP_LEVELS = 1, &
         MFCFD_SWEEP_CHAINS = 2
-    integer(c_int32_t), parameter :: MFCFD_PRECISION_FP64 = 0, MFCFD_PRECISION_MIXED = 1
+    integer(c_int32_t), parameter :: MFCFD_PRECISION_FP64 = 0, MFCFD_PRECISION_MIXED = 1, &
+        MFCFD_PRECISION_MIXED_DC = 2
     integer(c_int32_t), parameter :: MFCFD_UPDATE_IMPLICIT = 0, MFCFD_UPDATE_EXPLICIT = 1
     integer(c_int32_t), parameter :: MFCFD_SWEEPS_ALIAS = 0, MFCFD_SWEEPS_BACKUP = 1
     integer(c_int32_t), parameter :: MFCFD_ORDER_INDEX = 0, MFCFD_ORDER_MORTON = 1

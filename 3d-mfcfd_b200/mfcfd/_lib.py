@@ -56,6 +56,7 @@ ORDER_MORTON = 1
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_MIXED_DC = 2
 UPDATE_IMPLICIT = 0
 UPDATE_EXPLICIT = 1
 SWEEPS_ALIAS = 0

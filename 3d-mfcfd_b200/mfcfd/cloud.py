@@ -44,6 +44,7 @@ class PointCloud:
     name: str = "cloud"
     wall_area: float = 0.0  # surface area of the body (for force integration)
     ref_area: float = 0.0   # projected reference area for CL/CD
+    wall_areas: np.ndarray | None = None   # (N,) per-point surface areas, or None: wall_area split evenly
 
     @property
     def n(self) -> int:
@@ -135,7 +136,7 @@ def _boundary_frames(nor: np.ndarray):
 def _knn_connectivity(pts: np.ndarray, k: int):
     from scipy.spatial import cKDTree
     tree = cKDTree(pts)
-    dist, idx = tree.query(pts, k=k + 1)
+    dist, idx = tree.query(pts, k=k + 1, workers=-1)
     n = pts.shape[0]
     # Drop the point itself; exact duplicates are not generated.
     self_first = idx[:, 0] == np.arange(n)

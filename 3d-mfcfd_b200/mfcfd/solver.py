@@ -50,6 +50,8 @@ class Solver:
             self.close()
             raise MfcfdError(rc, msg)
         self.history = []
+        if cloud.wall_areas is not None and self.params.device >= 0:
+            self.set_wall_areas(cloud.wall_areas)
 
     # -- reference entry points ------------------------------------------
     def _check(self, rc):
@@ -97,6 +99,16 @@ class Solver:
         self._check(_lib.lib().mfcfd_forces(self.h, float(wa), float(ra), ctypes.byref(cl),
                                             ctypes.byref(cd), ptr(f)))
         return float(cl.value), float(cd.value), f
+
+    def set_wall_areas(self, area=None):
+        """mfcfd_set_wall_areas: per-point areas (N values, index order) for
+        forces(); None returns to the even split of the wall area."""
+        if area is None:
+            self._check(_lib.lib().mfcfd_set_wall_areas(self.h, None))
+            return
+        self._area = np.ascontiguousarray(area, dtype=np.float64)
+        assert self._area.shape == (self.n,)
+        self._check(_lib.lib().mfcfd_set_wall_areas(self.h, ptr(self._area)))
 
     def tune_chain(self, candidates=None, iters: int = 3):
         """mfcfd_tune_chain: time the chain schedule for each candidate warp

@@ -76,6 +76,8 @@ PHASE_FLOPS = {
 WORKLOADS = {
     "sphere-1.1M": dict(shells=96, per_shell=11500, jitter=0.01, mach=0.8, aoa=2.0, seed=2001),
     "sphere-62k": dict(shells=48, per_shell=1300, jitter=0.02, mach=0.4, aoa=0.0, seed=1001),
+    # a mid-size case for profiler captures: its state (~350 MB) exceeds L2
+    "sphere-256k": dict(shells=64, per_shell=4000, jitter=0.015, mach=0.8, aoa=2.0, seed=2501),
 }
 # kernels of one iteration per sweep mode (2 chains: k_qderiv, k_pending,
 # k_flux, two k_sweep_chain, k_update, two reductions, and k_g0 when the
@@ -233,7 +235,12 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mfcfd", choices=["mfcfd", "reference"])
-    ap.add_argument("--workload", default="sphere-1.1M", choices=sorted(WORKLOADS) + ["serve", "batch"])
+    ap.add_argument("--workload", default="sphere-1.1M",
+                    choices=sorted(WORKLOADS) + ["serve", "batch", "wing-4.2M", "wing-250k"])
+    ap.add_argument("--wing-max-iters", type=int, default=3000)
+    ap.add_argument("--wing-target", type=float, default=-6.0, help="residue (log10 drop) to converge to")
+    ap.add_argument("--wing-compare-iters", type=int, default=200,
+                    help="iterations after which mixed CL/CD are compared with an FP64 run")
     ap.add_argument("--batch-clouds", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
@@ -254,6 +261,8 @@ def main():
         return serve_main(args, rank, world, local_rank)
     if args.workload == "batch":
         return batch_main(args, rank, world, local_rank)
+    if args.workload.startswith("wing"):
+        return wing_main(args, rank, world, local_rank)
     wl = WORKLOADS[args.workload]
     metric = "point-iters/s FP64"
 
@@ -455,6 +464,99 @@ def main():
         print(json.dumps(line), flush=True)
     if s is not None:
         s.close()
+    replicas.finalize()
+
+
+def wing_main(args, rank, world, local_rank):
+    """The seeded swept-wing cloud (NACA 0012, semispan 1, taper 0.56, 30 deg
+    sweep, 400 x 120 wall points, ~4.2M points) at M 0.84, alpha 3.06 deg in
+    mixed precision, run until the residue reaches --wing-target (a 1e-6 drop
+    of the density residual) or --wing-max-iters.  Device-timed point-iters/s
+    over the whole run; the mixed CL/CD after --wing-compare-iters iterations
+    against an FP64 run of the same iterations, which also gives the FP64
+    rate."""
+    import torch
+    from mfcfd import _lib, replicas, wing
+    from mfcfd.solver import Solver
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the wing workload runs the GPU forms only; the reference's CPU solver is "
+                              "timed by the point-iteration workloads"}), flush=True)
+        return
+    torch.cuda.set_device(local_rank)
+    rank, world = replicas.init("nccl", timeout_s=3600)
+    big = args.workload == "wing-4.2M"
+    t0 = time.perf_counter()
+    c = (wing.swept_wing(seed=replicas.replica_seed(3001, rank)) if big else
+         wing.swept_wing(points=250_000, nc=160, ns=48, seed=replicas.replica_seed(3001, rank), name="wing-250k"))
+    gen_s = time.perf_counter() - t0
+    mach, aoa = 0.84, 3.06
+
+    def run(precision, max_iters, target, snap):
+        t1 = time.perf_counter()
+        s = Solver(c, mach, aoa, device=local_rank, precision=precision)
+        setup_s = time.perf_counter() - t1
+        s.initial_conditions()
+        st = torch.cuda.ExternalStream(s.stream())
+        ms, t, hist, at_snap = 0.0, 1, [], None
+        chunk = 50
+        while t <= max_iters:
+            k = min(chunk, max_iters - t + 1)
+            if snap and t <= snap < t + k:
+                k = snap - t + 1
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            h = s.q_lskum(k, t0=t)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            hist.extend(h.tolist())
+            t += k
+            if snap and t - 1 == snap:
+                at_snap = s.forces()[:2]
+            if h[-1][1] <= target or not np.isfinite(h[-1][0]):
+                break
+        cl_, cd_, _ = s.forces()
+        info = s.info()
+        s.close()
+        return dict(iters=t - 1, ms=ms, setup_s=setup_s, res=hist, cl=cl_, cd=cd_, at_snap=at_snap, info=info)
+
+    mixed = run(_lib.PRECISION_MIXED, args.wing_max_iters, args.wing_target, args.wing_compare_iters)
+    fp64 = run(_lib.PRECISION_FP64, args.wing_compare_iters, -1e9, None)
+    ms_m = replicas.max_over_ranks(mixed["ms"], device="cuda")
+    ms_f = replicas.max_over_ranks(fp64["ms"], device="cuda")
+    value = c.n * mixed["iters"] * world / (ms_m / 1e3)
+    fvalue = c.n * fp64["iters"] * world / (ms_f / 1e3)
+    if rank == 0:
+        res = np.array(mixed["res"])
+        conv = bool(res[-1, 1] <= args.wing_target)
+        drops = {}
+        for lv in range(1, 7):
+            hit = np.nonzero(res[:, 1] <= -lv)[0]
+            drops[str(-lv)] = int(hit[0]) + 1 if len(hit) else None
+        cm, cf = mixed["at_snap"], (fp64["cl"], fp64["cd"])
+        line = {"metric": "point-iters/s mixed to a 1e-6 residual drop", "value": value, "unit": "point-iters/s",
+                "n_gpus": world, "steps": mixed["iters"], "warmup": 0,
+                "ms_per_step": ms_m / max(1, mixed["iters"]), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "mixed f32/f64", "data": "synthetic (seeded swept-wing cloud)",
+                "config": {"workload": args.workload, "points": c.n, "counts": c.counts(), "mach": mach,
+                           "alpha_deg": aoa, "target_residue": args.wing_target,
+                           "max_iters": args.wing_max_iters, "generate_s": gen_s,
+                           "setup_s": mixed["setup_s"], "levels_forward": mixed["info"]["n_levels_forward"],
+                           "levels_backward": mixed["info"]["n_levels_backward"],
+                           "parallelism": f"replicas x{world}"},
+                "converged": conv, "iterations": mixed["iters"], "first_iteration_at_drop": drops,
+                "final_res_new": res[-1, 0], "final_residue": res[-1, 1], "cl": mixed["cl"], "cd": mixed["cd"],
+                "solve_s": ms_m / 1e3,
+                "fp64": {"value": fvalue, "unit": "point-iters/s", "iterations": fp64["iters"],
+                         "ms_per_step": ms_f / max(1, fp64["iters"])},
+                "mixed_vs_fp64_at_iteration": {"iteration": args.wing_compare_iters,
+                                               "dCL": None if cm is None else cm[0] - cf[0],
+                                               "dCD": None if cm is None else cm[1] - cf[1],
+                                               "cl_fp64": cf[0], "cd_fp64": cf[1]},
+                "residue_history_every_50": [round(float(x), 4) for x in res[49::50, 1]]}
+        print(json.dumps(line), flush=True)
     replicas.finalize()
 
 

@@ -66,7 +66,17 @@ extern "C" {
                                       least-squares moments and 3x3 solves,
                                       D_inv, the increments, the state update,
                                       residual norms and forces in FP64.
-                                      Requires MFCFD_SWEEP_CHAINS. */
+                                      Requires MFCFD_SWEEP_CHAINS.  The FP32
+                                      flux residual leaves a noise floor near a
+                                      1e-5 drop of the density residual. */
+#define MFCFD_PRECISION_MIXED_DC 2 /* defect correction: the flux residual (the
+                                      right-hand side) in FP64 as in the plain
+                                      path, the implicit LU-SGS operator (the
+                                      sweeps' flux evaluations, and the fluxes of
+                                      the state they difference against) in
+                                      FP32.  The iteration's fixed point is the
+                                      FP64 one, so it converges as far as FP64
+                                      does.  Requires MFCFD_SWEEP_CHAINS. */
 
 /*
  * Run-time form of the reference's compile-time constants (parameter.f90:

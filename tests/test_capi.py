@@ -72,11 +72,15 @@ def test_bad_inputs_are_status_codes(mfcfd_lib, small_cloud):
         _create(mfcfd_lib, small_cloud, power=-1.0)
     assert e.value.code == 1
     with pytest.raises(MfcfdError) as e:
-        _create(mfcfd_lib, small_cloud, precision=2)
+        _create(mfcfd_lib, small_cloud, precision=3)
     assert e.value.code == 6
-    with pytest.raises(MfcfdError) as e:          # mixed precision: chain schedule only
-        _create(mfcfd_lib, small_cloud, precision=1, sweep_mode=0)
-    assert e.value.code == 6
+    for prec in (1, 2):                           # mixed precision: chain schedule only
+        with pytest.raises(MfcfdError) as e:
+            _create(mfcfd_lib, small_cloud, precision=prec, sweep_mode=0)
+        assert e.value.code == 6
+    with pytest.raises(MfcfdError) as e:
+        _create(mfcfd_lib, small_cloud, storage_order=2)
+    assert e.value.code == 1
     with pytest.raises(MfcfdError) as e:
         _create(mfcfd_lib, small_cloud, sweep_mode=3)
     assert e.value.code == 1

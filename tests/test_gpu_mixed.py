@@ -21,11 +21,10 @@ PRESSURE_TOL = 1e-4
 RES_TOL = 1e-3
 
 
-def _mixed_vs_oracle(c, mach, aoa, iters, oracle_lib):
-    from mfcfd import _lib
+def _mixed_vs_oracle(c, mach, aoa, iters, oracle_lib, precision=1):
     from mfcfd.cloud import initial_state
     from mfcfd.solver import Solver
-    s = Solver(c, mach, aoa, precision=_lib.PRECISION_MIXED)
+    s = Solver(c, mach, aoa, precision=precision)
     o = oracle_lib.Oracle(c, mach, aoa, libm=oracle_lib.LIBM_MFMATH)
     prim0 = initial_state(c, mach, aoa)
     s.initial_conditions(prim0)
@@ -95,3 +94,44 @@ def test_mixed_precision_is_deterministic_alone_and_in_a_batch(mfcfd_lib):
     assert np.array_equal(solvers[0].get(mfcfd_lib.FIELD_PRIM), alone[0])
     for s in solvers:
         s.close()
+
+
+@pytest.mark.parametrize("mach,aoa,iters", [(0.8, 2.0, 60), (0.4, 0.0, 30)])
+def test_defect_correction_error_against_fp64_oracle(small_cloud, oracle_lib, mfcfd_lib, mach, aoa, iters):
+    """MFCFD_PRECISION_MIXED_DC: the flux residual in FP64, the sweeps in
+    FP32; same bounds as the mixed form."""
+    from mfcfd import _lib
+    from oracle.oracle import forces
+    s, o, hist, ref = _mixed_vs_oracle(small_cloud, mach, aoa, iters, oracle_lib, _lib.PRECISION_MIXED_DC)
+    np.testing.assert_allclose(hist[:, 0], ref[:, 0], rtol=RES_TOL)
+    pm = s.get(mfcfd_lib.FIELD_PRIM)
+    po = o.get(oracle_lib.FIELD_PRIM)
+    assert np.max(np.abs(pm[:, 4] - po[:, 4]) / np.abs(po[:, 4])) <= PRESSURE_TOL
+    clm, cdm, _ = s.forces()
+    clo, cdo, _ = forces(small_cloud, po, mach, aoa)
+    assert abs(clm - clo) <= CL_TOL and abs(cdm - cdo) <= CL_TOL
+
+
+def test_defect_correction_converges_like_fp64(mfcfd_lib):
+    """With the FP64 residual the iteration reaches a 1e-6 drop of the
+    density residual (residue -6) within a few per cent of the iterations
+    FP64 takes, where the all-FP32-flux form stalls near a 1e-5 drop."""
+    from mfcfd import _lib, cloud
+    from mfcfd.solver import Solver
+    c = cloud.small_sphere()
+    first = {}
+    for prec in (_lib.PRECISION_FP64, _lib.PRECISION_MIXED_DC):
+        s = Solver(c, 0.8, 2.0, precision=prec)
+        s.initial_conditions()
+        t, hit = 1, None
+        while t <= 12000 and hit is None:
+            h = s.q_lskum(500, t0=t)
+            below = np.nonzero(h[:, 1] <= -6.0)[0]
+            if len(below):
+                hit = t + int(below[0])
+            t += 500
+        first[prec] = (hit, s.forces()[:2])
+        s.close()
+    it64, itdc = first[_lib.PRECISION_FP64][0], first[_lib.PRECISION_MIXED_DC][0]
+    assert it64 is not None and itdc is not None, first
+    assert itdc <= 1.05 * it64 + 50, first
