@@ -945,7 +945,7 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
             const int wpb = h->stream ? h->d.ch_wpb : (h->staged ? h->staged->ch_wpb : 0);
             const int w = h->stream ? h->d.ch_warps : (h->staged ? h->staged->ch_w : 0);
             info->chain_slots =
-                wpb > 0 ? (w + wpb - 1) / wpb * chain_block_slots(h->P.device, wpb, h->P.precision != MFCFD_PRECISION_FP64,
+                wpb > 0 ? (w + wpb - 1) / wpb * chain_block_slots(h->P.device, wpb, h->P.precision,
                                                       h->P.chain_spread)
                         : 0;
             info->chain_slot_capacity = chain_slot_capacity(h->P.device);
@@ -1002,6 +1002,23 @@ int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new) {
     });
 }
 
+int mfcfd_set_precision(mfcfd_handle *h, int32_t precision) {
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h) return MFCFD_ERR_ARG;
+        if (precision != MFCFD_PRECISION_FP64 && precision != MFCFD_PRECISION_MIXED_DC)
+            return fail(h, MFCFD_ERR_ARG, "only FP64 and MIXED_DC can be switched to");
+        if (h->P.precision == MFCFD_PRECISION_MIXED)
+            return fail(h, MFCFD_ERR_UNSUPPORTED, "a MIXED handle's sweep weights are folded at set-up");
+        if (precision == MFCFD_PRECISION_MIXED_DC && h->P.sweep_mode != MFCFD_SWEEP_CHAINS)
+            return fail(h, MFCFD_ERR_UNSUPPORTED, "mixed precision requires the chain sweep schedule");
+        if (h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "a launch is pending on this handle");
+        h->P.precision = precision;
+        h->d.precision = precision;
+        drop_graphs(h);                    // their launches name the other kernels
+        return MFCFD_OK;
+    });
+}
+
 int mfcfd_set_fault_hook(mfcfd_handle *h, int32_t point, int32_t wait_limit) {
     return host_guard(h ? &h->err : nullptr, [&]() -> int {
         if (!h || point < 0 || wait_limit < 0) return MFCFD_ERR_ARG;
@@ -1048,7 +1065,7 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
             const DevCloud &d = hs[i]->d;
             return d.sweep_mode == MFCFD_SWEEP_CHAINS
                        ? (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb *
-                             chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision != MFCFD_PRECISION_FP64,
+                             chain_block_slots(hs[i]->P.device, d.ch_wpb, d.precision,
                                                d.ch_spread)
                        : 0;
         };

@@ -334,7 +334,9 @@ void prepare_launches(int device);
 // of the mixed-precision sweep (three per SM), 3 for a 4-warp block of the
 // FP64 sweep, 6 for an 8-warp block; see k_sweep_chain.
 int chain_slot_capacity(int device);
-int chain_block_slots(int device, int wpb, bool mixed, int spread = 0);
+// slots (sixths of an SM) of one chain block of the given shape and
+// precision (MFCFD_PRECISION_*)
+int chain_block_slots(int device, int wpb, int precision, int spread = 0);
 // File formats of the reference program (mfcfd_io.cpp).  Handle-less calls
 // leave their message in g_io_err (mfcfd_last_error(NULL)).
 extern thread_local std::string g_io_err;

@@ -756,7 +756,10 @@ __global__ void __launch_bounds__(128) k_g0(DevCloud d) {
 // A CI_G0 point's phase A is a copy of its k_g0 block into T, which the
 // chain kernel issued as a cp.async group before this call (followed by one
 // more group, the next point's stage, when g0_newer); phase B waits for it.
-template <int MODE, typename R>
+// FOLD (mixed precision): each term's weight carries its list's 3x3 solve
+// (set-up folds them), so phase C sums weight x term; otherwise phase C sums
+// the three weighted moments in FP64 and solves, as the reference does.
+template <int MODE, typename R, bool FOLD = false>
 __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepStage *st, bool forward, int lane,
                             double *T, double *ring, int ring_slot, bool g0_newer = false) {
     constexpr bool CHAINS = MODE == MODE_CHAINS;
@@ -919,7 +922,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
 
         // ---- phase C
         double G = 0.0;
-        if constexpr (std::is_same<R, float>::value) {
+        if constexpr (FOLD) {
             // mixed precision: each term's weight already carries the list's
             // 3x3 solve (cofactors / det, FP64, computed at set-up)
             if (lane < 30) {
@@ -1052,13 +1055,16 @@ __global__ void __launch_bounds__(DF_WARPS * 32) k_sweep_df(DevCloud d, int forw
 // released): every poll ends.
 constexpr int CH_FREE_SMS = 16;
 
-template <int WPB, typename R>
+template <int WPB, bool FOLD>
 constexpr int chain_min_blocks() {
-    return (WPB == 4 && std::is_same<R, float>::value) ? 3 : 1;
+    return (WPB == 4 && FOLD) ? 3 : 1;
 }
 
-template <int WPB, typename R>
-__global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, R>()) k_sweep_chain(DevCloud d, int forward) {
+// R: the type of the sweep's flux evaluations; FOLD: folded term weights
+// (MFCFD_PRECISION_MIXED).  FP64 <double, false>; mixed <float, true>;
+// defect correction <float, false>.
+template <int WPB, typename R, bool FOLD>
+__global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, FOLD>()) k_sweep_chain(DevCloud d, int forward) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char *smb = reinterpret_cast<char *>(smem) + warp * CHAIN_SMEM_BYTES;
@@ -1092,7 +1098,8 @@ __global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, R>()) k_sweep_
             cp_async_commit();
         }
         const ChainItem after = idx + 2 < b ? items[idx + 2] : nxt;
-        sweep_point<MODE_CHAINS, R>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING, idx + 1 < b);
+        sweep_point<MODE_CHAINS, R, FOLD>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING,
+                                          idx + 1 < b);
         cur = nxt;
         nxt = after;
     }
@@ -1361,12 +1368,14 @@ static void set_attributes(int device) {
     // three 4-warp blocks of the mixed-precision sweep per SM need the largest
     // shared-memory carveout; the other variants leave the choice to the
     // driver, which keeps more L1 for their loads and the flux kernel's
-    cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    cudaFuncSetAttribute(k_sweep_chain<4, float, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          cudaSharedmemCarveoutMaxShared);
-    cudaFuncSetAttribute(k_sweep_chain<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
-    cudaFuncSetAttribute(k_sweep_chain<8, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
-    cudaFuncSetAttribute(k_sweep_chain<4, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
-    cudaFuncSetAttribute(k_sweep_chain<8, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
+    cudaFuncSetAttribute(k_sweep_chain<4, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
+    cudaFuncSetAttribute(k_sweep_chain<8, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
+    cudaFuncSetAttribute(k_sweep_chain<4, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
+    cudaFuncSetAttribute(k_sweep_chain<8, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
+    cudaFuncSetAttribute(k_sweep_chain<4, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
+    cudaFuncSetAttribute(k_sweep_chain<8, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     done[device] = true;
 }
 
@@ -1378,11 +1387,11 @@ int chain_slot_capacity(int device) {
     return 6 * (sms - CH_FREE_SMS);
 }
 
-int chain_block_slots(int device, int wpb, bool mixed, int spread) {
+int chain_block_slots(int device, int wpb, int precision, int spread) {
     static std::mutex mu;
-    static int cache[256][2][2] = {};
+    static int cache[256][2][3] = {};
     if (device < 0 || device >= 256 || spread) return 6;
-    const int w8 = wpb == 8 ? 1 : 0, m = mixed ? 1 : 0;
+    const int w8 = wpb == 8 ? 1 : 0, m = precision < 0 || precision > 2 ? 0 : precision;
     {
         std::lock_guard<std::mutex> lock(mu);
         if (cache[device][w8][m]) return cache[device][w8][m];
@@ -1391,11 +1400,13 @@ int chain_block_slots(int device, int wpb, bool mixed, int spread) {
     int per_sm = 0;
     cudaError_t e;
     if (w8)
-        e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, float>, 256, chain_smem<8>())
-                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, double>, 256, chain_smem<8>());
+        e = m == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, float, true>, 256, chain_smem<8>())
+          : m == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, float, false>, 256, chain_smem<8>())
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, double, false>, 256, chain_smem<8>());
     else
-        e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, float>, 128, chain_smem<4>())
-                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double>, 128, chain_smem<4>());
+        e = m == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, float, true>, 128, chain_smem<4>())
+          : m == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, float, false>, 128, chain_smem<4>())
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double, false>, 128, chain_smem<4>());
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
         per_sm = 1;
@@ -1414,7 +1425,7 @@ int chain_shape(int device, int want, int spread, int *wpb, int *blocks) {
     if (spread) {
         // 4-warp blocks, one per SM
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double>, 4 * 32, CHAIN_SPREAD_SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double, false>, 4 * 32, CHAIN_SPREAD_SMEM);
         if (per_sm < 1) return 0;
         *wpb = 4;
         int b = (want + 3) / 4;
@@ -1428,9 +1439,9 @@ int chain_shape(int device, int want, int spread, int *wpb, int *blocks) {
     if (*wpb == 8) want = want * 3 / 4;
     int per_sm = 0;
     if (*wpb == 4)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double>, 4 * 32, chain_smem<4>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double, false>, 4 * 32, chain_smem<4>());
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, double>, 8 * 32, chain_smem<8>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, double, false>, 8 * 32, chain_smem<8>());
     if (per_sm < 1) return 0;
     int b = (want + *wpb - 1) / *wpb;
     if (b > max_blocks) b = max_blocks;
@@ -1518,12 +1529,15 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         if (chains) {
             const int blocks = (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb;
             const int csm = chain_smem_bytes(d.ch_wpb, d.ch_spread);
-            if (mixed) {
-                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float>, blocks, 4 * 32, csm, s, true, d, forward);
-                else launch_prio(k_sweep_chain<8, float>, blocks, 8 * 32, csm, s, true, d, forward);
+            if (dc) {
+                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float, false>, blocks, 4 * 32, csm, s, true, d, forward);
+                else launch_prio(k_sweep_chain<8, float, false>, blocks, 8 * 32, csm, s, true, d, forward);
+            } else if (mixed) {
+                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float, true>, blocks, 4 * 32, csm, s, true, d, forward);
+                else launch_prio(k_sweep_chain<8, float, true>, blocks, 8 * 32, csm, s, true, d, forward);
             } else {
-                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, double>, blocks, 4 * 32, csm, s, true, d, forward);
-                else launch_prio(k_sweep_chain<8, double>, blocks, 8 * 32, csm, s, true, d, forward);
+                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, double, false>, blocks, 4 * 32, csm, s, true, d, forward);
+                else launch_prio(k_sweep_chain<8, double, false>, blocks, 8 * 32, csm, s, true, d, forward);
             }
         } else if (d.sweep_mode == MFCFD_SWEEP_LEVELS) {
             k_sweep_levels<<<1, SWEEP_THREADS, SWEEP_WARPS * SWEEP_SMEM_BYTES, s>>>(d, forward);

@@ -43,6 +43,8 @@ struct Request {
     std::vector<double> x, y, z, tan1, tan2, nor, min_dist, prim0;
     int32_t max_iters = 0;
     double target = 0.0, wall_area = 0.0, ref_area = 0.0;
+    double polish = 0.0;              // MIXED_DC: residue at which it switches to FP64 (0: never)
+    bool polished = false;
     mfcfd_handle *h = nullptr;
     int64_t bytes = 0;
     int32_t t = 1;                    // next iteration number
@@ -349,6 +351,21 @@ void mfcfd_server::scheduler_loop() {
                 r->res.converged = rc == MFCFD_OK && r->t - 1 > 2 && r->res.residue <= r->target;
                 if (rc != MFCFD_OK) r->fail = rc;
                 if (rc != MFCFD_OK || r->res.converged || r->res.iters >= r->max_iters) r->retiring = true;
+                if (!r->retiring && !r->polished && r->polish < 0.0 && r->P.precision == MFCFD_PRECISION_MIXED_DC &&
+                    r->t - 1 > 2 && r->res.residue <= r->polish) {
+                    // the last part of the solve in FP64 (its chain blocks may
+                    // take other slots)
+                    r->polished = true;
+                    int prc = mfcfd_set_precision(r->h, MFCFD_PRECISION_FP64);
+                    mfcfd_info info{};
+                    if (prc == MFCFD_OK) prc = mfcfd_get_info(r->h, &info);
+                    if (prc != MFCFD_OK) {
+                        r->fail = prc;
+                        r->retiring = true;
+                    } else {
+                        r->slots = info.chain_slots;
+                    }
+                }
             }
 
             // hand the finished requests to the workers; one that could not be
@@ -482,6 +499,7 @@ int mfcfd_server::submit(const mfcfd_request *q, int64_t *id) {
     const int32_t c = cfg.chunk;
     r->max_iters = (q->max_iters + c - 1) / c * c;
     r->target = q->residue_target;
+    r->polish = q->polish_residue;
     r->wall_area = q->wall_area;
     r->ref_area = q->ref_area;
     r->res.n = q->n;

@@ -657,7 +657,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     // into its terms.  The list's derivative is num(axis, moments, sum w_j t_j)
     // / det, linear in the sums, so every term gets one weight
     // (cofactors . w_j) / det (FP64) and the sweep sums w_j t_j directly.
-    if (P.precision != MFCFD_PRECISION_FP64) {
+    if (P.precision == MFCFD_PRECISION_MIXED) {
         auto fold = [&](const std::vector<int32_t> &off, std::vector<SweepEntry> &ent) {
             parallel_for(n, [&](int p) {
                 for (int e = off[p]; e < off[p + 1]; ++e) {

@@ -108,6 +108,13 @@ module mfcfd_interface
             integer(c_int) :: rc
         end function mfcfd_residual_noalloc
 
+        function mfcfd_set_precision(h, precision) result(rc) bind(C, name="mfcfd_set_precision")
+            import :: c_ptr, c_int32_t, c_int
+            type(c_ptr), value :: h
+            integer(c_int32_t), value :: precision
+            integer(c_int) :: rc
+        end function mfcfd_set_precision
+
         function mfcfd_set_fault_hook(h, point, wait_limit) result(rc) bind(C, name="mfcfd_set_fault_hook")
             import :: c_ptr, c_int32_t, c_int
             type(c_ptr), value :: h

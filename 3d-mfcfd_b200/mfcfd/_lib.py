@@ -24,7 +24,7 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_run", "mfcfd_get", "mfcfd_get_state", "mfcfd_set_state",
            "mfcfd_get_stencils", "mfcfd_get_alias", "mfcfd_get_levels", "mfcfd_get_info",
            "mfcfd_get_stream", "mfcfd_set_profiling", "mfcfd_get_phase_times",
-           "mfcfd_residual_noalloc", "mfcfd_set_fault_hook", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
+           "mfcfd_residual_noalloc", "mfcfd_set_fault_hook", "mfcfd_set_precision", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
            "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch",
            "mfcfd_prepare", "mfcfd_device_bytes", "mfcfd_attach", "mfcfd_tune_chain",
@@ -94,7 +94,8 @@ class Request(ctypes.Structure):
         [(f, ctypes.c_void_p) for f in ("status", "x", "y", "z", "tan1", "tan2", "nor", "nbhs",
                                         "conn", "min_dist", "prim")] + \
         [("max_iters", ctypes.c_int32), ("residue_target", ctypes.c_double),
-         ("wall_area", ctypes.c_double), ("ref_area", ctypes.c_double)]
+         ("wall_area", ctypes.c_double), ("ref_area", ctypes.c_double),
+         ("polish_residue", ctypes.c_double)]
 
 
 class Result(ctypes.Structure):
@@ -151,6 +152,7 @@ def lib():
     L.mfcfd_get_phase_times.argtypes = [vp, vp, vp]
     L.mfcfd_residual_noalloc.argtypes = [vp, vp]
     L.mfcfd_set_fault_hook.argtypes = [vp, i32, i32]
+    L.mfcfd_set_precision.argtypes = [vp, i32]
     cp = ctypes.c_char_p
     L.mfcfd_count_input_points.argtypes = [cp, vp]
     L.mfcfd_read_input_point_data.argtypes = [cp, i32] + [vp] * 10

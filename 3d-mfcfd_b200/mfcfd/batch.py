@@ -74,3 +74,39 @@ def tune_batch(solvers, percents=(75, 100, 125, 150, 200), iters: int = 4):
         s.set_chain_warps(max(4, w * best // 100))
     restore()
     return best, times
+
+
+def solve_batch(solvers, target: float = -6.0, max_iters: int = 12000, chunk: int = 100,
+                polish: float | None = -5.0):
+    """Run every Solver until its residue reaches `target` (or `max_iters`),
+    in batched rounds of `chunk` iterations over the clouds still running.
+    A MIXED_DC solver switches to FP64 once its residue is at or below
+    `polish` (None: never), so it reaches a 1e-6 drop in about FP64's
+    iteration count.  Returns, per solver, a dict with the iterations run,
+    whether it converged, and the seconds from the call to its retirement."""
+    import time
+    t_start = time.perf_counter()
+    live = list(range(len(solvers)))
+    out = [dict(iters=0, converged=False, seconds=None, polished=False) for _ in solvers]
+    while live:
+        hist = run_batch([solvers[i] for i in live], chunk)
+        now = time.perf_counter() - t_start
+        keep = []
+        for j, i in enumerate(live):
+            s = solvers[i]
+            out[i]["iters"] += chunk
+            res = hist[j, -1, 1]
+            t_last = len(s.history)
+            if t_last > 2 and res <= target:
+                out[i].update(converged=True, seconds=now)
+                continue
+            if out[i]["iters"] >= max_iters:
+                out[i]["seconds"] = now
+                continue
+            if (polish is not None and not out[i]["polished"] and s.params.precision == _lib.PRECISION_MIXED_DC
+                    and t_last > 2 and res <= polish):
+                s.set_precision(_lib.PRECISION_FP64)
+                out[i]["polished"] = True
+            keep.append(i)
+        live = keep
+    return out

@@ -39,7 +39,7 @@ class Server:
 
     def submit(self, cloud: PointCloud, mach: float, aoa_deg: float, *, max_iters: int = 1000,
                residue_target: float = -6.0, prim: np.ndarray | None = None, forces: bool = True,
-               **params) -> int:
+               polish_residue: float = 0.0, **params) -> int:
         """Queue one solve; returns its id.  The arrays are copied.  The
         initial state defaults to Solver.initial_conditions' (the impulsive
         start of cloud.initial_state)."""
@@ -56,6 +56,7 @@ class Server:
         q.prim = p0.ctypes.data
         q.max_iters = int(max_iters)
         q.residue_target = float(residue_target)
+        q.polish_residue = float(polish_residue)
         if forces:
             q.wall_area, q.ref_area = float(cloud.wall_area), float(cloud.ref_area)
         rid = ctypes.c_int64()

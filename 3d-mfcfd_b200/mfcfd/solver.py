@@ -212,6 +212,12 @@ class Solver:
         self._check(_lib.lib().mfcfd_residual_noalloc(self.h, ptr(out)))
         return float(out[0])
 
+    def set_precision(self, precision: int):
+        """mfcfd_set_precision: switch between FP64 and MIXED_DC between
+        iterations."""
+        self._check(_lib.lib().mfcfd_set_precision(self.h, int(precision)))
+        self.params.precision = int(precision)
+
     def set_fault_hook(self, point: int, wait_limit: int = 0):
         """Failure-detection test hook (mfcfd_set_fault_hook): point (1-based,
         0 off) publishes none of its sweep increments, and device waits give

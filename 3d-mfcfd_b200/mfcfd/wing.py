@@ -243,12 +243,13 @@ def _list_check(pts, cls, tan1, tan2, nor, nbhs, conn, lo, hi, cap=22):
 def _ghosts(pts: np.ndarray, h: np.ndarray, reach: float):
     """Outer points mirroring every point within reach * h of a face of the
     half box (the symmetry plane z = 0 included) to the other side of that
-    face, with the face's outward normal."""
+    face, with the face's outward normal.  Points within h / 4 of the face
+    are not mirrored: their image would nearly coincide with them."""
     planes = [(0, -BOX, -1.0), (0, BOX, 1.0), (1, -BOX, -1.0), (1, BOX, 1.0), (2, 0.0, -1.0), (2, BOX, 1.0)]
     out, nors = [], []
     for axis, at, sgn in planes:
         dist = (at - pts[:, axis]) * sgn
-        sel = dist < reach * h
+        sel = (dist < reach * h) & (dist > 0.25 * h)
         g = pts[sel].copy()
         g[:, axis] = 2.0 * at - g[:, axis]
         nv = np.zeros((len(g), 3))

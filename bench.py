@@ -236,12 +236,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mfcfd", choices=["mfcfd", "reference"])
     ap.add_argument("--workload", default="sphere-1.1M",
-                    choices=sorted(WORKLOADS) + ["serve", "batch", "wing-4.2M", "wing-250k"])
-    ap.add_argument("--wing-max-iters", type=int, default=3000)
+                    choices=sorted(WORKLOADS) + ["serve", "batch", "batch-converged", "wing-4.2M", "wing-250k"])
+    ap.add_argument("--wing-max-iters", type=int, default=6000)
+    ap.add_argument("--wing-precision", type=int, default=2,
+                    help="2 mixed-dc (FP64 residual, FP32 sweeps; converges), 1 mixed (stalls near a 1e-5 drop)")
     ap.add_argument("--wing-target", type=float, default=-6.0, help="residue (log10 drop) to converge to")
     ap.add_argument("--wing-compare-iters", type=int, default=200,
                     help="iterations after which mixed CL/CD are compared with an FP64 run")
     ap.add_argument("--batch-clouds", type=int, default=24)
+    ap.add_argument("--batch-min-points", type=int, default=10000)
+    ap.add_argument("--batch-max-points", type=int, default=40000)
+    ap.add_argument("--batch-max-iters", type=int, default=12000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
     ap.add_argument("--chain-spread", type=int, default=0, help="1: one 4-warp chain block per SM")
@@ -255,12 +260,18 @@ def main():
     ap.add_argument("--serve-max-iters", type=int, default=600)
     ap.add_argument("--serve-chunk", type=int, default=10)
     ap.add_argument("--serve-setup-threads", type=int, default=8)
+    ap.add_argument("--serve-precision", type=int, default=1, help="1 mixed, 2 mixed-dc (FP64 residual)")
+    ap.add_argument("--serve-conv-requests", type=int, default=6)
+    ap.add_argument("--serve-conv-min-points", type=int, default=5000)
+    ap.add_argument("--serve-conv-max-points", type=int, default=15000)
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.workload == "serve":
         return serve_main(args, rank, world, local_rank)
     if args.workload == "batch":
         return batch_main(args, rank, world, local_rank)
+    if args.workload == "batch-converged":
+        return batch_converged_main(args, rank, world, local_rank)
     if args.workload.startswith("wing"):
         return wing_main(args, rank, world, local_rank)
     wl = WORKLOADS[args.workload]
@@ -429,10 +440,14 @@ def main():
 
     # served solves (a reduced stream: 24 requests of 10k-80k points) beside
     # the point-iteration rate, on one GPU
-    serving = None
+    serving = serving_conv = None
     if world == 1 and not args.no_serving:
         s.close()
         serving = serve_measure(args, rank, world, local_rank, 24, 80000)
+        # converged solves: requests run to a 1e-6 drop of the density residual
+        serving_conv = serve_measure(args, rank, world, local_rank, args.serve_conv_requests,
+                                     args.serve_conv_max_points, min_points=args.serve_conv_min_points,
+                                     target=-6.0, max_iters=12000, precision=2, seed=5500, polish=-5.0)
         s = None
 
     cpu_base = None
@@ -459,7 +474,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "point-iters/s",
                         "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                 "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks, "mixed": mixed,
-                "serving": serving,
+                "serving": serving, "serving_converged": serving_conv,
                 "gpu_launches": (KERNELS_PER_ITER[args.sweep_mode] + (1 if info.get("g0_points") else 0)) * args.steps}
         print(json.dumps(line), flush=True)
     if s is not None:
@@ -499,7 +514,7 @@ def wing_main(args, rank, world, local_rank):
         setup_s = time.perf_counter() - t1
         s.initial_conditions()
         st = torch.cuda.ExternalStream(s.stream())
-        ms, t, hist, at_snap = 0.0, 1, [], None
+        ms, t, hist, at_snap, polished = 0.0, 1, [], None, None
         chunk = 50
         while t <= max_iters:
             k = min(chunk, max_iters - t + 1)
@@ -517,12 +532,16 @@ def wing_main(args, rank, world, local_rank):
                 at_snap = s.forces()[:2]
             if h[-1][1] <= target or not np.isfinite(h[-1][0]):
                 break
+            if precision == _lib.PRECISION_MIXED_DC and polished is None and t > 3 and h[-1][1] <= -5.0:
+                s.set_precision(_lib.PRECISION_FP64)     # the last part of the solve in FP64
+                polished = t - 1
         cl_, cd_, _ = s.forces()
         info = s.info()
         s.close()
-        return dict(iters=t - 1, ms=ms, setup_s=setup_s, res=hist, cl=cl_, cd=cd_, at_snap=at_snap, info=info)
+        return dict(iters=t - 1, ms=ms, setup_s=setup_s, res=hist, cl=cl_, cd=cd_, at_snap=at_snap, info=info,
+                    polished_at=polished)
 
-    mixed = run(_lib.PRECISION_MIXED, args.wing_max_iters, args.wing_target, args.wing_compare_iters)
+    mixed = run(args.wing_precision, args.wing_max_iters, args.wing_target, args.wing_compare_iters)
     fp64 = run(_lib.PRECISION_FP64, args.wing_compare_iters, -1e9, None)
     ms_m = replicas.max_over_ranks(mixed["ms"], device="cuda")
     ms_f = replicas.max_over_ranks(fp64["ms"], device="cuda")
@@ -537,6 +556,7 @@ def wing_main(args, rank, world, local_rank):
             drops[str(-lv)] = int(hit[0]) + 1 if len(hit) else None
         cm, cf = mixed["at_snap"], (fp64["cl"], fp64["cd"])
         line = {"metric": "point-iters/s mixed to a 1e-6 residual drop", "value": value, "unit": "point-iters/s",
+                "precision": {1: "mixed", 2: "mixed-dc (FP64 residual, FP32 sweeps)"}.get(args.wing_precision),
                 "n_gpus": world, "steps": mixed["iters"], "warmup": 0,
                 "ms_per_step": ms_m / max(1, mixed["iters"]), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "mixed f32/f64", "data": "synthetic (seeded swept-wing cloud)",
@@ -547,6 +567,7 @@ def wing_main(args, rank, world, local_rank):
                            "levels_backward": mixed["info"]["n_levels_backward"],
                            "parallelism": f"replicas x{world}"},
                 "converged": conv, "iterations": mixed["iters"], "first_iteration_at_drop": drops,
+                "switched_to_fp64_at_iteration": mixed["polished_at"],
                 "final_res_new": res[-1, 0], "final_residue": res[-1, 1], "cl": mixed["cl"], "cd": mixed["cd"],
                 "solve_s": ms_m / 1e3,
                 "fp64": {"value": fvalue, "unit": "point-iters/s", "iterations": fp64["iters"],
@@ -556,6 +577,85 @@ def wing_main(args, rank, world, local_rank):
                                                "dCD": None if cm is None else cm[1] - cf[1],
                                                "cl_fp64": cf[0], "cd_fp64": cf[1]},
                 "residue_history_every_50": [round(float(x), 4) for x in res[49::50, 1]]}
+        print(json.dumps(line), flush=True)
+    replicas.finalize()
+
+
+def batch_converged_main(args, rank, world, local_rank):
+    """Converged solves of a batch: --batch-clouds seeded sphere and
+    ellipsoid clouds of --batch-min-points to --batch-max-points points
+    (log-uniform, Mach U[0.3, 0.85], alpha U[-5, 5] deg), each run to a 1e-6
+    drop of the density residual (residue -6).  Batched: MIXED_DC (FP64
+    residual, FP32 sweeps) with a switch to FP64 at residue -5, all clouds
+    iterating together in rounds; against the plain FP64 path, one cloud at
+    a time.  Solves/s = clouds / wall time of each; CL/CD of every cloud
+    against its FP64 solve."""
+    import torch
+    from mfcfd import _lib, batch, replicas, serve
+    from mfcfd.solver import Solver
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no batch runner; its CPU solver is timed by the "
+                              "point-iteration workloads"}), flush=True)
+        return
+    torch.cuda.set_device(local_rank)
+    rank, world = replicas.init("nccl", timeout_s=3600)
+    _, clouds, reqs = serve.request_stream(args.batch_clouds, 1.0, replicas.replica_seed(7100, rank),
+                                           args.batch_min_points, args.batch_max_points, pool=args.batch_clouds)
+    flows = [(reqs[i][1], reqs[i][2]) for i in range(len(clouds))]
+    # warm-up: one short batched round (graph capture, first launches)
+    ws = [Solver(clouds[0], *flows[0], device=local_rank, precision=_lib.PRECISION_MIXED_DC)]
+    ws[0].initial_conditions()
+    batch.run_batch(ws, 20)
+    ws[0].close()
+    # plain FP64, one cloud after another
+    t0 = time.perf_counter()
+    fp64 = []
+    for c, (m, a) in zip(clouds, flows):
+        s = Solver(c, m, a, device=local_rank)
+        s.initial_conditions()
+        r = batch.solve_batch([s], max_iters=args.batch_max_iters, polish=None)[0]
+        r["forces"] = s.forces()[:2]
+        fp64.append(r)
+        s.close()
+    torch.cuda.synchronize()
+    seq_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    # batched MIXED_DC with the FP64 polish
+    ss = []
+    for c, (m, a) in zip(clouds, flows):
+        s = Solver(c, m, a, device=local_rank, precision=_lib.PRECISION_MIXED_DC)
+        s.initial_conditions()
+        ss.append(s)
+    replicas.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = batch.solve_batch(ss, max_iters=args.batch_max_iters, polish=-5.0)
+    torch.cuda.synchronize()
+    bat_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    errs = []
+    for s, r, f in zip(ss, out, fp64):
+        cl_, cd_, _ = s.forces()
+        errs.append((abs(cl_ - f["forces"][0]), abs(cd_ - f["forces"][1])))
+        s.close()
+    if rank == 0:
+        n = len(clouds) * world
+        line = {"metric": "converged solves/s (1e-6 residual drop) batched mixed-dc vs FP64 one at a time",
+                "value": n / bat_s, "unit": "solves/s", "n_gpus": world, "steps": len(clouds), "warmup": 1,
+                "ms_per_step": bat_s * 1e3 / len(clouds), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "mixed-dc f32 sweeps / f64 residual, f64 polish from residue -5",
+                "data": "synthetic (seeded sphere/ellipsoid shell clouds)",
+                "config": {"workload": "batch-converged", "clouds": len(clouds),
+                           "points": [c.n for c in clouds], "target_residue": -6.0,
+                           "max_iters": args.batch_max_iters, "polish_residue": -5.0, "round": 100,
+                           "parallelism": f"replicas x{world}"},
+                "converged": sum(1 for r in out if r["converged"]),
+                "iterations": [r["iters"] for r in out],
+                "fp64_one_at_a_time": {"value": n / seq_s, "unit": "solves/s", "seconds": seq_s,
+                                       "converged": sum(1 for r in fp64 if r["converged"]),
+                                       "iterations": [r["iters"] for r in fp64]},
+                "speedup_vs_fp64_one_at_a_time": seq_s / bat_s,
+                "max_abs_dCL": max(e[0] for e in errs), "max_abs_dCD": max(e[1] for e in errs)}
         print(json.dumps(line), flush=True)
     replicas.finalize()
 
@@ -655,7 +755,8 @@ def serve_main(args, rank, world, local_rank):
         return
     torch.cuda.set_device(local_rank)
     rank, world = replicas.init("nccl", timeout_s=1800)
-    line = serve_measure(args, rank, world, local_rank, args.serve_requests, args.serve_max_points)
+    line = serve_measure(args, rank, world, local_rank, args.serve_requests, args.serve_max_points,
+                         precision=args.serve_precision)
     if rank == 0:
         line.update({"metric": "served solves/s", "n_gpus": world, "steps": line["requests"], "warmup": 0,
                      "ms_per_step": 1e3 / line["value"] * world, "higher_is_better": True,
@@ -668,15 +769,24 @@ def serve_main(args, rank, world, local_rank):
     replicas.finalize()
 
 
-def serve_measure(args, rank, world, local_rank, count, max_points):
+def serve_measure(args, rank, world, local_rank, count, max_points, min_points=None, target=None,
+                  max_iters=None, precision=None, seed=5000, polish=0.0):
     """The serving measurement (see serve_main) for `count` requests of
-    clouds up to `max_points` points; returns its summary (rank 0)."""
+    clouds of `min_points` to `max_points` points, each run until its residue
+    is <= `target` (or `max_iters`), served in `precision` with continuous
+    batching against the same stream one request at a time in FP64; returns
+    its summary (rank 0).  Every request's CL/CD is compared with its FP64
+    solve."""
     from mfcfd import _lib, replicas, serve
+    min_points = args.serve_min_points if min_points is None else min_points
+    target = args.serve_target if target is None else target
+    max_iters = args.serve_max_iters if max_iters is None else max_iters
+    precision = _lib.PRECISION_MIXED if precision is None else precision
     arrivals, clouds, reqs = serve.request_stream(count, args.serve_rate,
-                                                  replicas.replica_seed(5000, rank),
-                                                  args.serve_min_points, max_points)
+                                                  replicas.replica_seed(seed, rank),
+                                                  min_points, max_points)
 
-    def run(precision, max_live):
+    def run(prec, max_live):
         # many requests at once: chain schedules of the widest level's width;
         # one at a time: each request's own (twice that)
         with serve.Server(device=local_rank, chunk=args.serve_chunk, setup_threads=args.serve_setup_threads,
@@ -684,7 +794,7 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
             # warm-up request (untimed): first graph capture and launches in the process
             small = min(range(len(clouds)), key=lambda i: clouds[i].n)
             srv.wait(srv.submit(clouds[small], 0.5, 0.0, max_iters=args.serve_chunk, residue_target=-99.0,
-                                precision=precision))
+                                precision=prec))
             replicas.barrier()
             st0 = srv.stats()
             t0 = time.perf_counter()
@@ -693,8 +803,8 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
                 wait = ta - (time.perf_counter() - t0)
                 if wait > 0:
                     time.sleep(wait)
-                ids.append(srv.submit(clouds[ci], m, a, max_iters=args.serve_max_iters,
-                                      residue_target=args.serve_target, precision=precision))
+                ids.append(srv.submit(clouds[ci], m, a, max_iters=max_iters, residue_target=target,
+                                      precision=prec, polish_residue=polish if prec == 2 else 0.0))
             res = [srv.wait(i) for i in ids]
             wall = time.perf_counter() - t0
             st = srv.stats()
@@ -702,20 +812,16 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
                 st[k] -= st0[k]
         return res, replicas.max_over_ranks(wall, device="cuda"), st
 
-    res_m, wall_m, st_m = run(_lib.PRECISION_MIXED, 0)
+    res_m, wall_m, st_m = run(precision, 0)
     res_b, wall_b, _ = run(_lib.PRECISION_FP64, 1)
     total = len(reqs) * world
     lat = serve.latency_summary([r["latency"] for r in res_m])
     lat_b = serve.latency_summary([r["latency"] for r in res_b])
-    # CL/CD of a sample re-solved alone in FP64
-    k = max(2, -(-len(reqs) // 20))
-    errs = []
-    for j in range(k):
-        ci, m, a = reqs[j]
-        ref = serve.solve_alone(clouds[ci], m, a, args.serve_chunk, args.serve_max_iters, args.serve_target,
-                                device=local_rank)
-        errs.append((abs(res_m[j]["cl"] - ref["cl"]), abs(res_m[j]["cd"] - ref["cd"])))
+    # CL/CD of every request against its FP64 solve (the one-at-a-time run)
+    errs = [(abs(a["cl"] - b["cl"]), abs(a["cd"] - b["cd"])) for a, b in zip(res_m, res_b)]
+    k = len(errs)
     conv = sum(1 for r in res_m if r["converged"])
+    conv_b = sum(1 for r in res_b if r["converged"])
 
     def phases(res):
         # host preparation, wait for HBM / SM slots, time on the GPU
@@ -727,11 +833,13 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
     return {"value": total / wall_m, "unit": "solves/s", "requests": len(reqs),
             "config": {"workload": "serve", "requests": len(reqs), "rate_per_s": args.serve_rate,
                        "points_min": min(pts), "points_max": max(pts), "points_total": sum(pts),
-                       "residue_target": args.serve_target, "max_iters": args.serve_max_iters,
-                       "chunk": args.serve_chunk, "precision": "mixed",
+                       "residue_target": target, "max_iters": max_iters, "polish_residue": polish,
+                       "chunk": args.serve_chunk,
+                       "precision": {1: "mixed", 2: "mixed-dc (FP64 residual, FP32 sweeps)"}.get(precision, "fp64"),
                        "parallelism": f"replicas x{world}"},
             "latency_s": lat, "latency_phases_mean_s": phases(res_m), "converged": conv, "failed": sum(1 for r in res_m if r["status"]),
             "iterations_mean": float(np.mean([r["iters"] for r in res_m])),
+            "iterations_mean_fp64": float(np.mean([r["iters"] for r in res_b])), "converged_fp64": conv_b,
             "peak_live": st_m["peak_live"], "peak_bytes_live": st_m["peak_bytes_live"],
             # seconds with a chunk on the GPU, and the chain-sweep slots held,
             # over the stream's wall time (slot_capacity slots in all)
@@ -741,7 +849,8 @@ def serve_measure(args, rank, world, local_rank, count, max_points):
                                    "latency_phases_mean_s": phases(res_b)},
             "speedup_vs_fp64_one_at_a_time": wall_b / wall_m,
             "fp64_resolve_sample": {"requests": k, "max_abs_dCL": max(e[0] for e in errs),
-                                    "max_abs_dCD": max(e[1] for e in errs)},
+                                    "max_abs_dCD": max(e[1] for e in errs),
+                                    "of": "every request against its FP64 solve"},
             # per point: status, xyz, frames, nbhs, conn(27), min_dist, prim in; prim out
             "h2d_bytes_per_request": int(np.mean(pts) * (4 + 24 + 72 + 4 + 108 + 8 + 40)),
             "d2h_bytes_per_request": int(np.mean(pts) * 5 * 8)}

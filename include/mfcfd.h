@@ -321,6 +321,18 @@ int mfcfd_get_phase_times(mfcfd_handle *h, double *ms, int64_t *iters);
 int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new);
 
 /*
+ * Switch a handle between MFCFD_PRECISION_FP64 and MFCFD_PRECISION_MIXED_DC
+ * between iterations (no counterpart in the reference).  The defect-
+ * correction form converges like FP64 down to about a 1e-5 drop of the
+ * density residual and then slows, because its FP32 sweeps resolve
+ * increments only to FP32; switching to FP64 for the last part of a solve
+ * (a "polish") reaches a 1e-6 drop in FP64's iteration count.  The state
+ * and the residual reference carry over.  Handles created MIXED (folded
+ * sweep weights) cannot switch.
+ */
+int mfcfd_set_precision(mfcfd_handle *h, int32_t precision);
+
+/*
  * Failure-detection test hook (no counterpart in the reference, which has no
  * failure detection).  Every device wait of the sweeps is bounded: when one
  * runs out, the kernel sets an error word and returns, and the step reports
@@ -443,6 +455,9 @@ typedef struct mfcfd_request {
     int32_t max_iters;        /* upper bound, rounded up to a multiple of chunk */
     double residue_target;    /* converged when residue <= this after a round */
     double wall_area, ref_area;   /* CL/CD at retirement when both are > 0 */
+    double polish_residue;    /* MIXED_DC requests: switch to FP64 once the residue is at
+                                 or below this after a round (mfcfd_set_precision);
+                                 0: never */
 } mfcfd_request;
 
 typedef struct mfcfd_result {

@@ -112,26 +112,49 @@ def test_defect_correction_error_against_fp64_oracle(small_cloud, oracle_lib, mf
     assert abs(clm - clo) <= CL_TOL and abs(cdm - cdo) <= CL_TOL
 
 
-def test_defect_correction_converges_like_fp64(mfcfd_lib):
-    """With the FP64 residual the iteration reaches a 1e-6 drop of the
-    density residual (residue -6) within a few per cent of the iterations
-    FP64 takes, where the all-FP32-flux form stalls near a 1e-5 drop."""
+def test_defect_correction_with_polish_converges_like_fp64(mfcfd_lib):
+    """MIXED_DC tracks FP64 down to about a 1e-5 drop of the density
+    residual; switched to FP64 there (mfcfd_set_precision), it reaches the
+    1e-6 drop (residue -6) within a few per cent of FP64's iterations, and
+    its forces agree with FP64's converged ones to 1e-4."""
+    from mfcfd import _lib, batch, cloud
+    from mfcfd.solver import Solver
+    c = cloud.small_sphere()
+    res = {}
+    for prec, polish in ((_lib.PRECISION_FP64, None), (_lib.PRECISION_MIXED_DC, -5.0)):
+        s = Solver(c, 0.8, 2.0, precision=prec)
+        s.initial_conditions()
+        r = batch.solve_batch([s], max_iters=12000, chunk=100, polish=polish)[0]
+        res[prec] = (r, s.forces()[:2])
+        s.close()
+    r64, rdc = res[_lib.PRECISION_FP64][0], res[_lib.PRECISION_MIXED_DC][0]
+    assert r64["converged"] and rdc["converged"], res
+    assert rdc["polished"]
+    assert rdc["iters"] <= 1.05 * r64["iters"] + 100, res
+    (cl64, cd64), (cldc, cddc) = res[_lib.PRECISION_FP64][1], res[_lib.PRECISION_MIXED_DC][1]
+    assert abs(cldc - cl64) <= CL_TOL and abs(cddc - cd64) <= CL_TOL
+
+
+def test_precision_switch(mfcfd_lib):
+    """FP64 and MIXED_DC handles switch either way between iterations; a
+    MIXED handle (folded sweep weights) refuses; switching to FP64 before the
+    first iteration gives the plain FP64 bits."""
     from mfcfd import _lib, cloud
     from mfcfd.solver import Solver
     c = cloud.small_sphere()
-    first = {}
-    for prec in (_lib.PRECISION_FP64, _lib.PRECISION_MIXED_DC):
-        s = Solver(c, 0.8, 2.0, precision=prec)
-        s.initial_conditions()
-        t, hit = 1, None
-        while t <= 12000 and hit is None:
-            h = s.q_lskum(500, t0=t)
-            below = np.nonzero(h[:, 1] <= -6.0)[0]
-            if len(below):
-                hit = t + int(below[0])
-            t += 500
-        first[prec] = (hit, s.forces()[:2])
+    a = Solver(c, 0.8, 2.0)
+    a.initial_conditions()
+    ha = a.q_lskum(5)
+    b = Solver(c, 0.8, 2.0, precision=_lib.PRECISION_MIXED_DC)
+    b.initial_conditions()
+    b.set_precision(_lib.PRECISION_FP64)
+    hb = b.q_lskum(5)
+    assert np.array_equal(ha, hb)
+    assert np.array_equal(a.get(mfcfd_lib.FIELD_PRIM), b.get(mfcfd_lib.FIELD_PRIM))
+    b.set_precision(_lib.PRECISION_MIXED_DC)
+    assert np.all(np.isfinite(b.q_lskum(5, t0=6)[:, 0]))
+    m = Solver(c, 0.8, 2.0, precision=_lib.PRECISION_MIXED)
+    with pytest.raises(_lib.MfcfdError):
+        m.set_precision(_lib.PRECISION_FP64)
+    for s in (a, b, m):
         s.close()
-    it64, itdc = first[_lib.PRECISION_FP64][0], first[_lib.PRECISION_MIXED_DC][0]
-    assert it64 is not None and itdc is not None, first
-    assert itdc <= 1.05 * it64 + 50, first

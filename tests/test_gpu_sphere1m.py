@@ -34,5 +34,9 @@ def test_sphere1m_two_iterations_bitexact(oracle_lib, mfcfd_lib):
         bad = np.count_nonzero(got[name].view(np.uint64) != want.view(np.uint64))
         assert bad == 0, f"{name}: {bad} values differ"
     o.close()
+    # res_new sums 1.1M positive terms (the same bits on both sides): the
+    # oracle left to right, the GPU in a fixed tree.  Left-to-right summation
+    # of N positive terms is within N u (1.2e-10 here) relative; the bound
+    # below is a tenth of that
     for (a, _), (b, _) in zip(r_gpu, r_cpu):
-        assert abs(a - b) <= 1e-13 * abs(b)
+        assert abs(a - b) <= 1e-11 * abs(b), (a, b)

@@ -39,17 +39,18 @@ def test_wing_fp64_matches_oracle(small_wing, oracle_lib, mfcfd_lib):
     o.close()
 
 
-def test_wing_mixed_runs_and_tracks_fp64(small_wing, mfcfd_lib):
+def test_wing_defect_correction_runs_and_tracks_fp64(small_wing, mfcfd_lib):
+    """The converging mixed form (FP64 residual, FP32 sweeps) on the wing."""
     from mfcfd.solver import Solver
     c = small_wing
     out = {}
-    for prec in (0, 1):
+    for prec in (0, 2):
         s = Solver(c, 0.84, 3.06, precision=prec)
         s.initial_conditions()
         h = s.q_lskum(60)
         assert np.all(np.isfinite(h[:, 0]))
         out[prec] = (h, s.forces()[:2])
         s.close()
-    np.testing.assert_allclose(out[1][0][:, 0], out[0][0][:, 0], rtol=1e-3)
-    assert abs(out[1][1][0] - out[0][1][0]) <= 1e-4
-    assert abs(out[1][1][1] - out[0][1][1]) <= 1e-4
+    np.testing.assert_allclose(out[2][0][:, 0], out[0][0][:, 0], rtol=1e-3)
+    assert abs(out[2][1][0] - out[0][1][0]) <= 1e-4
+    assert abs(out[2][1][1] - out[0][1][1]) <= 1e-4
