@@ -472,6 +472,11 @@ int create_impl(const mfcfd_params *params, int32_t n, const int32_t *status, co
         *out = h;
         return MFCFD_ERR_ARG;
     }
+    if (P.flux_blocks_per_sm < 0 || P.flux_blocks_per_sm > 64) {
+        h->err = "flux_blocks_per_sm out of range [0, 64]";
+        *out = h;
+        return MFCFD_ERR_ARG;
+    }
     if (P.storage_order != MFCFD_ORDER_INDEX && P.storage_order != MFCFD_ORDER_MORTON) {
         h->err = "unknown storage_order";
         *out = h;
@@ -591,6 +596,7 @@ int attach_device(mfcfd_handle *h) {
         d.ch_warps = st.ch_w;
         d.ch_wpb = st.ch_wpb;
         d.ch_spread = P.chain_spread;
+        d.flux_grid = P.flux_blocks_per_sm > 0 ? P.flux_blocks_per_sm * device_sms(P.device) : 0;
         if ((rc = upload(h, &d.pre_order, st.pre))) return rc;
         for (int dir = 0; dir < 2; ++dir) {
             if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;

@@ -26,7 +26,7 @@ module mfcfd_interface
         real(c_double) :: rho_inf, u1_inf, u2_inf, u3_inf, pr_inf
         integer(c_int32_t) :: inner_iterations, split_capacity, precision, device, sweep_mode
         integer(c_int32_t) :: update_variant, sweep_variant, chain_warps, gpu_setup, graphs
-        integer(c_int32_t) :: chain_spread, storage_order
+        integer(c_int32_t) :: chain_spread, storage_order, flux_blocks_per_sm
     end type mfcfd_params
 
     interface

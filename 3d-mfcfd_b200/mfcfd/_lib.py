@@ -48,7 +48,8 @@ class Params(ctypes.Structure):
                 ("sweep_mode", ctypes.c_int32), ("update_variant", ctypes.c_int32),
                 ("sweep_variant", ctypes.c_int32), ("chain_warps", ctypes.c_int32),
                 ("gpu_setup", ctypes.c_int32), ("graphs", ctypes.c_int32),
-                ("chain_spread", ctypes.c_int32), ("storage_order", ctypes.c_int32)]
+                ("chain_spread", ctypes.c_int32), ("storage_order", ctypes.c_int32),
+                ("flux_blocks_per_sm", ctypes.c_int32)]
 
 
 ORDER_INDEX = 0

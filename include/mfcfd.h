@@ -110,6 +110,9 @@ typedef struct mfcfd_params {
                                  holds one, so every warp has an SM sub-partition to
                                  itself; 0 (default) packs blocks as residency allows */
     int32_t storage_order;    /* MFCFD_ORDER_MORTON (default) or MFCFD_ORDER_INDEX */
+    int32_t flux_blocks_per_sm;   /* CHAINS: the flux residual beside the forward sweep as a
+                                     grid of this many blocks per SM walking the sweep's
+                                     order; 0 (default): one block per four points */
 } mfcfd_params;
 
 /* Order of the points in device memory.  The set-up (split lists, alias
