@@ -3,7 +3,7 @@
 A half wing with a NACA 0012 section (closed trailing edge), semispan 1,
 taper 0.56 and a 30 deg leading-edge sweep, spanwise along +z from the
 symmetry plane z = 0.  Its surface carries 400 chordwise x 120 spanwise wall
-points (status 1).  Volume points fill the half box [-10, 10]^2 x [0, 10]
+points (status 1), and 300 more close the tip (a flat tip face, normal +z).  Volume points fill the half box [-10, 10]^2 x [0, 10]
 with a density proportional to exp(-d / 0.3) in the distance d to the
 wing's surface plus a uniform floor, drawn by rejection sampling over a
 grid of cells refined near the wing.  Points within about one local spacing
@@ -136,6 +136,26 @@ def wall_grid(nc: int = 400, ns: int = 120):
     return p, n, area, cells
 
 
+def tip_cap(nc: int = 400):
+    """Wall points closing the tip: the section face at z = semispan, nc/4
+    chordwise stations (the surface grid's leading-edge clustering) x three
+    rows across the thickness, normal +z; returns points, normals, areas."""
+    m = max(4, nc // 4)
+    pi = 4.0 * math.atan(1.0)
+    xi = np.array([0.5 * (i + 0.5) / m + 0.5 * (1.0 - math.cos(0.5 * pi * (i + 0.5) / m)) for i in range(m)])
+    edges = np.array([0.5 * i / m + 0.5 * (1.0 - math.cos(0.5 * pi * i / m)) for i in range(m + 1)])
+    c = chord(np.array([SEMISPAN]))[0]
+    t = half_thickness(xi) * c
+    rows, areas = [], []
+    for f in (-0.5, 0.0, 0.5):
+        rows.append(np.stack([leading_edge_x(np.full(m, SEMISPAN)) + xi * c, f * t, np.full(m, SEMISPAN)], axis=1))
+        areas.append((edges[1:] - edges[:-1]) * c * (2.0 * t) / 3.0)
+    p = np.concatenate(rows)
+    n = np.zeros_like(p)
+    n[:, 2] = 1.0
+    return p, n, np.concatenate(areas)
+
+
 def _surface_tree(nc: int = 1200, ns: int = 360):
     """k-d tree of a dense sampling of the whole surface (both sides and the
     tip face), for distances from the wing."""
@@ -240,6 +260,68 @@ def _list_check(pts, cls, tan1, tan2, nor, nbhs, conn, lo, hi, cap=22):
     return bad, over
 
 
+def _deep_inside(pts: np.ndarray, frac: float = 0.7) -> np.ndarray:
+    """Inside the wing by more than (1 - frac) of the local half thickness:
+    the chord between two points of one side of the surface dips inside it
+    only by its sag, a segment through the section crosses this core."""
+    x, y, z = pts[:, 0], pts[:, 1], pts[:, 2]
+    inz = (z >= 0.0) & (z < SEMISPAN * (1.0 - 1e-9))   # the tip face itself is not inside
+    zc = np.clip(z, 0.0, SEMISPAN)
+    c = chord(zc)
+    xi = (x - leading_edge_x(zc)) / c
+    return inz & (xi > 0.0) & (xi < 1.0) & (np.abs(y) < frac * c * half_thickness(xi))
+
+
+def _visible_knn(pts: np.ndarray, k: int, tree, extra: int = 16, nwall: int = 0):
+    """The k nearest neighbours of every point that it sees: a candidate is
+    dropped when the segment to it passes through the wing (sampled at seven
+    interior points), so no stencil couples the two sides of the thin
+    trailing edge through the body; the first `nwall` points (walls) take at
+    most k - k//3 wall points.  Points near the wing may keep fewer than k.  Returns nbhs, conn (1-based, zero padded) and min_dist, like
+    cloud._knn_connectivity."""
+    from scipy.spatial import cKDTree
+    n = pts.shape[0]
+    m = k + extra
+    dist, idx = cKDTree(pts).query(pts, k=m + 1, workers=-1)
+    if not np.all(idx[:, 0] == np.arange(n)):
+        raise ValueError("duplicate points in generated cloud")
+    idx, dist = idx[:, 1:], dist[:, 1:]
+    ok = np.ones((n, m), dtype=bool)
+    dw, _ = tree.query(pts, workers=-1)
+    near = np.nonzero(dw < dist[:, -1])[0]      # only these can see through the wing
+    step = 50_000
+    for a in range(0, len(near), step):
+        rows = near[a:a + step]
+        p0 = pts[rows][:, None, :]
+        d = pts[idx[rows]] - p0
+        blocked = np.zeros((len(rows), m), dtype=bool)
+        for f in (0.125, 0.25, 0.375, 0.5, 0.625, 0.75, 0.875):
+            q = (p0 + f * d).reshape(-1, 3)
+            blocked |= _deep_inside(q).reshape(len(rows), m)
+        ok[rows] = ~blocked
+    # the first k visible candidates, in distance order; a wall point takes
+    # at most k - k//3 wall neighbours, so its lists always reach off the
+    # surface (a stencil of surface points alone leaves the derivative along
+    # the normal nearly undetermined)
+    if nwall:
+        is_wall_cand = idx < nwall
+        cap_w = k - k // 3
+        wrank = np.cumsum(ok & is_wall_cand, axis=1)
+        ok[:nwall] &= ~(is_wall_cand[:nwall] & (wrank[:nwall] > cap_w))
+    rank = np.cumsum(ok, axis=1)
+    take = ok & (rank <= k)
+    nbhs = take.sum(axis=1).astype(np.int32)
+    conn = np.zeros((n, MAX_CONN), dtype=np.int32)
+    order = np.argsort(~take, axis=1, kind="stable")[:, :k]
+    sel = np.take_along_axis(idx, order, axis=1) + 1
+    keep = np.arange(k)[None, :] < nbhs[:, None]
+    conn[:, :k] = np.where(keep, sel, 0)
+    kk = conn[:, 0] - 1
+    dx = pts[kk] - pts
+    md = np.sqrt(dx[:, 0] * dx[:, 0] + dx[:, 1] * dx[:, 1] + dx[:, 2] * dx[:, 2])
+    return nbhs, conn, md
+
+
 def _ghosts(pts: np.ndarray, h: np.ndarray, reach: float):
     """Outer points mirroring every point within reach * h of a face of the
     half box (the symmetry plane z = 0 included) to the other side of that
@@ -267,6 +349,8 @@ def swept_wing(points: int = 4_200_000, seed: int = 3001, k: int = 26, nc: int =
     from scipy.spatial import cKDTree
     rng = np.random.Generator(np.random.PCG64(seed))
     pw, nw, aw, _ = wall_grid(nc, ns)
+    pc, ncap, acap = tip_cap(nc)
+    pw, nw, aw = np.concatenate([pw, pc]), np.concatenate([nw, ncap]), np.concatenate([aw, acap])
     tree = _surface_tree(max(nc, 240), max(ns, 72))
     box_vol = (2 * BOX) * (2 * BOX) * BOX
     n_floor = min(floor * box_vol, 0.2 * points)
@@ -315,7 +399,7 @@ def swept_wing(points: int = 4_200_000, seed: int = 3001, k: int = 26, nc: int =
         bidx = np.concatenate([np.arange(nwall), np.arange(len(inner), n)])
         t1b, t2b = _boundary_frames(bnor)
         tan1[bidx], tan2[bidx], nor[bidx] = t1b, t2b, bnor
-        nbhs, conn, md = _knn_connectivity(pts, k)
+        nbhs, conn, md = _visible_knn(pts, k, tree, extra=24, nwall=nwall)
         # no list may exceed the reference's 22 entries of storage (an
         # overflowing list spills into the next point's column): wall and
         # outer points, whose z list is their whole neighbourhood, and
@@ -345,7 +429,8 @@ def swept_wing(points: int = 4_200_000, seed: int = 3001, k: int = 26, nc: int =
         wb = np.nonzero(bad[:nwall])[0]
         if len(wb):
             hw = dist[wb, 6]
-            add = [pw[wb] + 0.5 * hw[:, None] * nw[wb] + sgn * 0.5 * hw[:, None] * tan2[wb] for sgn in (-1.0, 1.0)]
+            add = [pw[wb] + 0.5 * hw[:, None] * nw[wb] + sgn * 0.5 * hw[:, None] * tan2[wb]
+                   + 0.05 * hw[:, None] * rng.uniform(-1.0, 1.0, size=(len(wb), 3)) for sgn in (-1.0, 1.0)]
             vol = np.concatenate([vol[~drop]] + add)
         else:
             vol = vol[~drop]

@@ -515,7 +515,7 @@ def wing_main(args, rank, world, local_rank):
         setup_s = time.perf_counter() - t1
         s.initial_conditions()
         st = torch.cuda.ExternalStream(s.stream())
-        ms, t, hist, at_snap, polished = 0.0, 1, [], None, None
+        ms, t, hist, at_snap, polished, diverged = 0.0, 1, [], None, None, None
         chunk = 50
         while t <= max_iters:
             k = min(chunk, max_iters - t + 1)
@@ -523,7 +523,12 @@ def wing_main(args, rank, world, local_rank):
                 k = snap - t + 1
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
-            h = s.q_lskum(k, t0=t)
+            try:
+                h = s.q_lskum(k, t0=t)
+            except _lib.MfcfdError as err:     # the iteration diverged (non-finite residual)
+                torch.cuda.synchronize()
+                diverged = (t, str(err))
+                break
             e1.record(st)
             torch.cuda.synchronize()
             ms += e0.elapsed_time(e1)
@@ -536,14 +541,23 @@ def wing_main(args, rank, world, local_rank):
             if precision == _lib.PRECISION_MIXED_DC and polished is None and t > 3 and h[-1][1] <= -5.0:
                 s.set_precision(_lib.PRECISION_FP64)     # the last part of the solve in FP64
                 polished = t - 1
-        cl_, cd_, _ = s.forces()
+        cl_, cd_ = s.forces()[:2] if diverged is None else (None, None)
         info = s.info()
         s.close()
-        return dict(iters=t - 1, ms=ms, setup_s=setup_s, res=hist, cl=cl_, cd=cd_, at_snap=at_snap, info=info,
-                    polished_at=polished)
+        return dict(iters=t - 1, ms=ms, setup_s=setup_s, res=hist or [[float("nan"), float("nan")]], cl=cl_,
+                    cd=cd_, at_snap=at_snap, info=info, polished_at=polished, diverged=diverged)
 
     mixed = run(args.wing_precision, args.wing_max_iters, args.wing_target, args.wing_compare_iters)
     fp64 = run(_lib.PRECISION_FP64, args.wing_compare_iters, -1e9, None)
+    if mixed["diverged"] or fp64["diverged"]:
+        if rank == 0:
+            print(json.dumps({"metric": "point-iters/s mixed to a 1e-6 residual drop", "value": None,
+                              "unit": "point-iters/s", "workload": args.workload, "points": c.n,
+                              "diverged": {"mixed": mixed["diverged"], "fp64": fp64["diverged"]},
+                              "note": "the iteration diverged on this cloud; the CPU oracle (the reference's "
+                                      "algorithm) diverges on it as well"}), flush=True)
+        replicas.finalize()
+        return
     ms_m = replicas.max_over_ranks(mixed["ms"], device="cuda")
     ms_f = replicas.max_over_ranks(fp64["ms"], device="cuda")
     value = c.n * mixed["iters"] * world / (ms_m / 1e3)

@@ -71,6 +71,7 @@ struct Oracle {
     std::vector<int> xpos_nbhs, xneg_nbhs, ypos_nbhs, yneg_nbhs, zpos_nbhs, zneg_nbhs;
     std::vector<int> xpos_conn, xneg_conn, ypos_conn, yneg_conn, zpos_conn, zneg_conn;
     std::vector<double> U, delUp, delUn, prim, flux_res, q, qm, dq, temp_dq, delt, dinv;
+    std::vector<double> delUp_fwd;   // delUp as the forward sweep left it (a diagnostic)
     std::vector<int> alias, point_with_alias;
     std::vector<int> interior_idx, wall_idx, outer_idx, ss_inlet_idx, ss_outlet_idx;
     double res_old = 0, res_new = 0, residue = 0, max_res = 0;
@@ -878,6 +879,7 @@ void implicit_forward_backward_sweeps(Oracle &o) {
             for (int r = 1; r <= 5; ++r) o.V5(o.delUp, r, p) = o.V5(o.delUp, r, q);
         }
     }
+    o.delUp_fwd = o.delUp;
     for (int i = o.N; i >= 1; --i) {
         int p = o.point_with_alias[i];
         if (p == 0) continue;
@@ -1105,6 +1107,7 @@ int oracle_get(void *h, int field, double *out) {
     case 7: copyv(o->delUp, 5); return 0;
     case 8: copyv(o->delUn, 5); return 0;
     case 9: copyv(o->dinv, 1); return 0;
+    case 10: if (o->delUp_fwd.empty()) return -1; copyv(o->delUp_fwd, 5); return 0;
     default: return -1;
     }
 }

@@ -16,10 +16,10 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
 FIELD_PRIM, FIELD_U, FIELD_Q, FIELD_QM, FIELD_DQ, FIELD_DELT, FIELD_FLUX_RES, \
-    FIELD_DELUP, FIELD_DELUN, FIELD_DINV = range(10)
+    FIELD_DELUP, FIELD_DELUN, FIELD_DINV, FIELD_DELUP_FORWARD = range(11)
 FIELD_WIDTH = {FIELD_PRIM: 5, FIELD_U: 5, FIELD_Q: 5, FIELD_QM: 10, FIELD_DQ: 15,
                FIELD_DELT: 1, FIELD_FLUX_RES: 5, FIELD_DELUP: 5, FIELD_DELUN: 5,
-               FIELD_DINV: 1}
+               FIELD_DINV: 1, FIELD_DELUP_FORWARD: 5}
 
 LIBM_GLIBC = 0
 LIBM_MFMATH = 1

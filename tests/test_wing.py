@@ -17,7 +17,7 @@ def test_wing_lists_are_usable(small_wing):
     c = small_wing
     assert c.bad_lists == 0 and c.bad_wall_lists == 0
     counts = c.counts()
-    assert counts["wall"] == 80 * 24
+    assert counts["wall"] == 80 * 24 + 3 * 20     # surface grid and tip face
     assert counts["interior"] > 0.7 * c.n and counts["outer"] > 0
     # no list overflows the reference's 22-entry storage, and the library's
     # set-up takes the cloud
@@ -45,7 +45,12 @@ def test_wing_geometry(small_wing):
     w = c.status == STATUS_WALL
     assert not wing.inside_wing(pts[w] + 1e-4 * c.nor[w]).any()
     assert wing.inside_wing(pts[w] - 1e-4 * c.nor[w]).mean() > 0.95
-    # per-point areas add up to the surface area of both sides
+    # no neighbour is seen through the wing
+    for i in np.nonzero(w)[0][::7]:
+        k = c.conn[i, :c.nbhs[i]] - 1
+        mid = 0.5 * (pts[k] + pts[i])
+        assert not wing._deep_inside(mid).any()
+    # per-point areas add up to the surface area of both sides and the tip
     assert c.wall_areas is not None
     s = np.sum(c.wall_areas)
     assert 1.5 < s < 1.7 and abs(s - c.wall_area) < 1e-12
