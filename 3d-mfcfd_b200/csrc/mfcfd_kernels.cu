@@ -759,15 +759,9 @@ __global__ void __launch_bounds__(128) k_g0(DevCloud d) {
 // FOLD (mixed precision): each term's weight carries its list's 3x3 solve
 // (set-up folds them), so phase C sums weight x term; otherwise phase C sums
 // the three weighted moments in FP64 and solves, as the reference does.
-//
-// next_it / next_st (chain schedule, shared-frame points): the next point's
-// stage is issued here, once this lane's first hand-off loads are in
-// flight, so the issue overlaps their round trip; the caller issues it
-// itself otherwise.
 template <int MODE, typename R, bool FOLD = false>
 __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepStage *st, bool forward, int lane,
-                            double *T, double *ring, int ring_slot, bool g0_newer = false,
-                            const ChainItem *next_it = nullptr, SweepStage *next_st = nullptr) {
+                            double *T, double *ring, int ring_slot, bool g0_newer = false) {
     constexpr bool CHAINS = MODE == MODE_CHAINS;
     const int p = it.p;
     const bool wall = (it.info & CI_WALL) != 0;
@@ -856,7 +850,6 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                 }
             }
             int spins = 0;
-            bool issued = next_st == nullptr;
             while (pend) {
                 unsigned long long v[3][5];
 #pragma unroll
@@ -870,10 +863,6 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                     ld_relaxed_v2(gs + 2, v[q][2], v[q][3]);
                     v[q][4] = ld_relaxed_b64(gs + 4);
                 }
-                if (!issued) {   // while the loads above travel
-                    stage_issue(d, *next_it, forward, lane, next_st);
-                    issued = true;
-                }
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
                     if (!((pend >> q) & 1u) || !ready5(v[q])) continue;
@@ -884,8 +873,6 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                 }
                 if (pend && !spin_continue(spins, d)) break;
             }
-            if (!issued) stage_issue(d, *next_it, forward, lane, next_st);
-            if (next_st) cp_async_commit();
         } else {
             FluxPreT<R> Pn;
             AxisTermsT<R> An[3];
@@ -1106,17 +1093,13 @@ __global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, FOLD>()) k_swe
             for (int j = lane; j < G0_DOUBLES / 2; j += 32) cp_async16(dst + 16 * j, src + 16 * j);
             cp_async_commit();
         }
-        // a shared-frame point issues the next stage inside, behind its
-        // hand-off loads; the others (their phase A waits on the g0 group,
-        // which must come first) issue it here
-        const bool defer = idx + 1 < b && (cur.info & CI_SHARED) && !(cur.info & (CI_G0 | CI_COPY));
-        if (idx + 1 < b && !defer) {
+        if (idx + 1 < b) {
             stage_issue(d, nxt, forward != 0, lane, &stg[s ^ 1]);
             cp_async_commit();
         }
         const ChainItem after = idx + 2 < b ? items[idx + 2] : nxt;
         sweep_point<MODE_CHAINS, R, FOLD>(d, cur, &stg[s], forward != 0, lane, T, ring, (idx - a) % CHAIN_RING,
-                                          idx + 1 < b, defer ? &nxt : nullptr, defer ? &stg[s ^ 1] : nullptr);
+                                          idx + 1 < b);
         cur = nxt;
         nxt = after;
     }

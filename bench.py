@@ -262,9 +262,9 @@ def main():
     ap.add_argument("--serve-chunk", type=int, default=10)
     ap.add_argument("--serve-setup-threads", type=int, default=8)
     ap.add_argument("--serve-precision", type=int, default=1, help="1 mixed, 2 mixed-dc (FP64 residual)")
-    ap.add_argument("--serve-conv-requests", type=int, default=6)
+    ap.add_argument("--serve-conv-requests", type=int, default=8)
     ap.add_argument("--serve-conv-min-points", type=int, default=5000)
-    ap.add_argument("--serve-conv-max-points", type=int, default=15000)
+    ap.add_argument("--serve-conv-max-points", type=int, default=10000)
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.workload == "serve":
@@ -448,7 +448,8 @@ def main():
         # converged solves: requests run to a 1e-6 drop of the density residual
         serving_conv = serve_measure(args, rank, world, local_rank, args.serve_conv_requests,
                                      args.serve_conv_max_points, min_points=args.serve_conv_min_points,
-                                     target=-6.0, max_iters=12000, precision=2, seed=5500, polish=-5.0)
+                                     target=-6.0, max_iters=8000, precision=2, seed=5500, polish=-5.0,
+                                     mach=(0.3, 0.6), aspect=(1.0, 1.0))
         s = None
 
     cpu_base = None
@@ -616,8 +617,11 @@ def batch_converged_main(args, rank, world, local_rank):
         return
     torch.cuda.set_device(local_rank)
     rank, world = replicas.init("nccl", timeout_s=3600)
+    # spheres at M 0.3-0.6: the seeded ellipsoid clouds and the higher Mach
+    # numbers include solves that stall above a 1e-6 drop or diverge in FP64
     _, clouds, reqs = serve.request_stream(args.batch_clouds, 1.0, replicas.replica_seed(7100, rank),
-                                           args.batch_min_points, args.batch_max_points, pool=args.batch_clouds)
+                                           args.batch_min_points, args.batch_max_points, pool=args.batch_clouds,
+                                           mach=(0.3, 0.6), aspect=(1.0, 1.0))
     flows = [(reqs[i][1], reqs[i][2]) for i in range(len(clouds))]
     # warm-up: one short batched round (graph capture, first launches)
     ws = [Solver(clouds[0], *flows[0], device=local_rank, precision=_lib.PRECISION_MIXED_DC)]
@@ -660,7 +664,8 @@ def batch_converged_main(args, rank, world, local_rank):
                 "ms_per_step": bat_s * 1e3 / len(clouds), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "mixed-dc f32 sweeps / f64 residual, f64 polish from residue -5",
                 "data": "synthetic (seeded sphere/ellipsoid shell clouds)",
-                "config": {"workload": "batch-converged", "clouds": len(clouds),
+                "config": {"workload": "batch-converged", "clouds": len(clouds), "bodies": "spheres",
+                           "mach_range": [0.3, 0.6], "alpha_range_deg": [-5.0, 5.0],
                            "points": [c.n for c in clouds], "target_residue": -6.0,
                            "max_iters": args.batch_max_iters, "polish_residue": -5.0, "round": 100,
                            "parallelism": f"replicas x{world}"},
@@ -785,7 +790,7 @@ def serve_main(args, rank, world, local_rank):
 
 
 def serve_measure(args, rank, world, local_rank, count, max_points, min_points=None, target=None,
-                  max_iters=None, precision=None, seed=5000, polish=0.0):
+                  max_iters=None, precision=None, seed=5000, polish=0.0, mach=(0.3, 0.85), aspect=(1.0, 3.0)):
     """The serving measurement (see serve_main) for `count` requests of
     clouds of `min_points` to `max_points` points, each run until its residue
     is <= `target` (or `max_iters`), served in `precision` with continuous
@@ -799,7 +804,7 @@ def serve_measure(args, rank, world, local_rank, count, max_points, min_points=N
     precision = _lib.PRECISION_MIXED if precision is None else precision
     arrivals, clouds, reqs = serve.request_stream(count, args.serve_rate,
                                                   replicas.replica_seed(seed, rank),
-                                                  min_points, max_points)
+                                                  min_points, max_points, mach=mach, aspect=aspect)
 
     def run(prec, max_live):
         # many requests at once: chain schedules of the widest level's width;
@@ -849,7 +854,7 @@ def serve_measure(args, rank, world, local_rank, count, max_points, min_points=N
             "config": {"workload": "serve", "requests": len(reqs), "rate_per_s": args.serve_rate,
                        "points_min": min(pts), "points_max": max(pts), "points_total": sum(pts),
                        "residue_target": target, "max_iters": max_iters, "polish_residue": polish,
-                       "chunk": args.serve_chunk,
+                       "chunk": args.serve_chunk, "mach_range": list(mach), "aspect_range": list(aspect),
                        "precision": {1: "mixed", 2: "mixed-dc (FP64 residual, FP32 sweeps)"}.get(precision, "fp64"),
                        "parallelism": f"replicas x{world}"},
             "latency_s": lat, "latency_phases_mean_s": phases(res_m), "converged": conv, "failed": sum(1 for r in res_m if r["status"]),
