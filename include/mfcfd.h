@@ -185,7 +185,9 @@ typedef struct mfcfd_info {
 typedef struct mfcfd_handle mfcfd_handle;
 
 /* Fill *p with parameter.f90's values: power 0, K 2, CFL 5, no inner
- * iterations, rho 1, u = Mach (cos a, sin a, 0), p = 1/1.4, capacity 22. */
+ * iterations, rho 1, u = Mach (cos a, sin a, 0), p = 1/1.4, capacity 22;
+ * and the library's defaults: FP64, device 0, the chain schedule, graphs in
+ * batches, the Morton storage order. */
 void mfcfd_params_init(mfcfd_params *p, double mach, double aoa_deg);
 
 /*
