@@ -53,11 +53,11 @@ PHASE_BYTES = {"qderiv": 372 + 180, "flux": 724, "dinv": 488, "sweep_fwd": 608,
                "sweep_bwd": 608, "update": 196, "residual": 8}
 TOTAL_BYTES = 3368
 # DRAM bytes (read + write) per point of one chain-sweep launch, from the
-# ncu capture of the 256,000-point sphere's forward sweep (630.46 MB read +
-# 73.72 MB written per launch, profiles/ncu_k_sweep_chain_sphere256k.txt);
+# ncu capture of the 256,000-point sphere's forward sweep (630.45 MB read +
+# 75.31 MB written per launch, profiles/ncu_k_sweep_chain_sphere256k.txt);
 # each point stages its own records once, so a launch of n points moves
 # about n times this.
-SWEEP_TRAFFIC_PER_POINT = (630.46e6 + 73.72e6) / 256000
+SWEEP_TRAFFIC_PER_POINT = (630.45e6 + 75.31e6) / 256000
 
 # FP64 operations per point-iteration of each phase, counted by the oracle
 # built with counting arithmetic (oracle/oracle_flops.cpp: add, multiply,
