@@ -163,6 +163,12 @@ struct ChainSchedule {
     int64_t terms_ring = 0, terms_local = 0, terms_cross = 0;   // swept producers
 };
 void build_chain_schedule(Topology &T, int warps, ChainSchedule &S);
+// The warp assignment of one direction: the points of lpts (level-major),
+// their levels, and each point's deepest-level dependencies cand[coff[p] ..
+// coff[p+1]) in entry order; gives every point's owner warp and each warp's
+// points in order.
+void chain_assign(const int32_t *lpts, int nsw, const int32_t *level, const int32_t *coff, const int32_t *cand, int n,
+                  int warps, std::vector<int32_t> &owner, std::vector<std::vector<int32_t>> &lists);
 
 // Set-up passes on the GPU (mfcfd_prep.cu), equal to the host's.  The split
 // pass leaves T untouched and sets *overflow when a list exceeds `cap`
@@ -222,6 +228,23 @@ int host_guard(std::string *err, F &&f) noexcept {
     }
     return code;
 }
+
+// Validation of the inputs, the point classes and the class index lists
+// (T.n, T.cap, T.cls, T.*_idx); the first step of build_topology.
+int classify_points(const mfcfd_params &P, int n, const int32_t *status, const int32_t *nbhs, const int32_t *conn,
+                    Topology &T, std::string &err);
+// One split-list entry written past a list's capacity into the storage that
+// follows it (list d, flat index within the list's array, 1-based id).
+struct SpillWrite {
+    int d;
+    size_t at;
+    int32_t value;
+};
+// The spilled writes of the reference's split storage, in its order, from
+// every point's full list counts cnt[d][i] (T: classes and index lists).
+void split_spill_writes(const Topology &T, const double *x, const double *y, const double *z, const double *tan1,
+                        const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn,
+                        const int32_t *const cnt[NDIR], std::vector<SpillWrite> &out);
 
 // Build everything above.  Returns MFCFD_OK or an error code with a message.
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,

@@ -148,13 +148,46 @@ void give_setup_threads(int k) {
     if (k > 0) setup_pool().fetch_add(k, std::memory_order_relaxed);
 }
 
-int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
-                   const double *y, const double *z, const double *tan1, const double *tan2,
-                   const double *nor, const int32_t *nbhs, const int32_t *conn,
-                   const double *min_dist, Topology &T, std::string &err) {
+namespace {
+
+// A point's neighbours in list order (generate_connectivity.f90:38-246):
+// put(d, k) for each list d that takes neighbour k (1-based id); interior
+// points split all three axes, wall and outer points put every neighbour in
+// their one z list.
+template <class F>
+void split_point(int i, int cls, const double *x, const double *y, const double *z, const double *tan1,
+                 const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn, F &&put) {
+    const double xi = x[i], yi = y[i], zi = z[i];
+    const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
+    for (int r = 0; r < nbhs[i]; ++r) {
+        int k = conn[(size_t)i * MAX_CONN + r];
+        double delx = x[k - 1] - xi, dely = y[k - 1] - yi, delz = z[k - 1] - zi;
+        double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+        double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+        if (cls == CLS_INTERIOR) {
+            double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+            if (dels <= 0.0) put(0, k);
+            if (dels > 0.0) put(1, k);
+            if (delt <= 0.0) put(2, k);
+            if (delt > 0.0) put(3, k);
+            if (deln <= 0.0) put(4, k);
+            if (deln > 0.0) put(5, k);
+        } else {
+            if (dels <= 0.0) put(0, k);
+            if (dels >= 0.0) put(1, k);
+            if (delt <= 0.0) put(2, k);
+            if (delt >= 0.0) put(3, k);
+            put(cls == CLS_WALL ? 5 : 4, k);
+        }
+    }
+}
+
+}  // namespace
+
+int classify_points(const mfcfd_params &P, int n, const int32_t *status, const int32_t *nbhs, const int32_t *conn,
+                    Topology &T, std::string &err) {
     T.n = n;
     T.cap = P.split_capacity > 0 ? P.split_capacity : MAX_CONN;
-    const int cap = T.cap;
     T.cls.assign(n, CLS_SUPERSONIC);
     for (int i = 0; i < n; ++i) {
         if (nbhs[i] < 0 || nbhs[i] > MAX_CONN) {
@@ -179,6 +212,47 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             return MFCFD_ERR_ARG;
         }
     }
+    return MFCFD_OK;
+}
+
+// The reference stores list d of point i at i*cap + j, and an entry past the
+// capacity lands in the following points' storage; it visits the interior,
+// then the wall, then the outer points, each once from zeroed counts, so a
+// cell ends with the value of its last writer in that order.  Each point
+// first fills its own cells; then the spilled entries, in that order,
+// replace an owner's value that came earlier or was never written.  This
+// gives those spilled writes, from every point's full list counts.
+void split_spill_writes(const Topology &T, const double *x, const double *y, const double *z, const double *tan1,
+                        const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn,
+                        const int32_t *const cnt[NDIR], std::vector<SpillWrite> &out) {
+    const int n = T.n, cap = T.cap;
+    out.clear();
+    std::vector<int32_t> visit(n, -1);
+    int at = 0;
+    for (const std::vector<int32_t> *cl : {&T.interior_idx, &T.wall_idx, &T.outer_idx})
+        for (int i : *cl) visit[i] = at++;
+    for (const std::vector<int32_t> *cl : {&T.interior_idx, &T.wall_idx, &T.outer_idx})
+        for (int s : *cl) {
+            bool spills = false;
+            for (int d = 0; d < NDIR; ++d) spills = spills || cnt[d][s] > cap;
+            if (!spills) continue;
+            int c[NDIR] = {0, 0, 0, 0, 0, 0};
+            split_point(s, T.cls[s], x, y, z, tan1, tan2, nor, nbhs, conn, [&](int d, int k) {
+                const int j = c[d]++;
+                if (j < cap) return;
+                const int t = s + j / cap, slot = j % cap;   // the cell's owner and its slot
+                const bool owner_wrote = t < n && visit[t] >= 0 && cnt[d][t] > slot;
+                if (!owner_wrote || visit[t] < visit[s]) out.push_back({d, (size_t)s * cap + j, k});
+            });
+        }
+}
+
+int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
+                   const double *y, const double *z, const double *tan1, const double *tan2,
+                   const double *nor, const int32_t *nbhs, const int32_t *conn,
+                   const double *min_dist, Topology &T, std::string &err) {
+    if (int rc = classify_points(P, n, status, nbhs, conn, T, err)) return rc;
+    const int cap = T.cap;
 
     const bool gpu = P.gpu_setup != 0 && P.device >= 0;
     // ---- split stencils with the reference's storage (generate_connectivity.f90)
@@ -195,70 +269,26 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         T.split_cnt[d].assign(n, 0);
     }
     T.split_overflows = 0;
-    // a point's neighbours in list order: put(d, k) for each list d that
-    // takes neighbour k (1-based id); interior points split all three axes,
-    // wall and outer points put every neighbour in their one z list
-    auto classify = [&](int i, int cls, auto &&put) {
-        const double xi = x[i], yi = y[i], zi = z[i];
-        const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
-        for (int r = 0; r < nbhs[i]; ++r) {
-            int k = conn[(size_t)i * MAX_CONN + r];
-            double delx = x[k - 1] - xi, dely = y[k - 1] - yi, delz = z[k - 1] - zi;
-            double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
-            double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
-            if (cls == CLS_INTERIOR) {
-                double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
-                if (dels <= 0.0) put(0, k);
-                if (dels > 0.0) put(1, k);
-                if (delt <= 0.0) put(2, k);
-                if (delt > 0.0) put(3, k);
-                if (deln <= 0.0) put(4, k);
-                if (deln > 0.0) put(5, k);
-            } else {
-                if (dels <= 0.0) put(0, k);
-                if (dels >= 0.0) put(1, k);
-                if (delt <= 0.0) put(2, k);
-                if (delt >= 0.0) put(3, k);
-                put(cls == CLS_WALL ? 5 : 4, k);
-            }
-        }
-    };
     if (!split_done) {
-        // The reference stores list d of point i at i*cap + j, and an entry
-        // past the capacity lands in the following points' storage; it visits
-        // the interior, then the wall, then the outer points, each once from
-        // zeroed counts, so a cell ends with the value of its last writer in
-        // that order.  Each point first fills its own cells (in parallel);
-        // then the spilled entries, in that order, replace an owner's value
-        // that came earlier or was never written.
-        std::vector<int32_t> visit(n, -1);
-        int at = 0;
-        for (const std::vector<int32_t> *cl : {&T.interior_idx, &T.wall_idx, &T.outer_idx})
-            for (int i : *cl) visit[i] = at++;
-        std::vector<uint8_t> spills(n, 0);
+        // each point fills its own cells (in parallel), then the spilled
+        // entries are written in the reference's visiting order
         parallel_for(n, [&](int i) {
             const int c = T.cls[i];
             if (c != CLS_INTERIOR && c != CLS_WALL && c != CLS_OUTER) return;
-            classify(i, c, [&](int d, int k) {
+            split_point(i, c, x, y, z, tan1, tan2, nor, nbhs, conn, [&](int d, int k) {
                 const int j = T.split_cnt[d][i]++;
                 if (j < cap) T.split[d][(size_t)i * cap + j] = k;
-                else spills[i] = 1;
             });
         });
         for (int d = 0; d < NDIR; ++d)
             for (int i = 0; i < n; ++i) T.split_overflows += std::max(0, T.split_cnt[d][i] - cap);
-        for (const std::vector<int32_t> *cl : {&T.interior_idx, &T.wall_idx, &T.outer_idx})
-            for (int s : *cl) {
-                if (!spills[s]) continue;
-                int cnt[NDIR] = {0, 0, 0, 0, 0, 0};
-                classify(s, T.cls[s], [&](int d, int k) {
-                    const int j = cnt[d]++;
-                    if (j < cap) return;
-                    const int t = s + j / cap, slot = j % cap;   // the cell's owner and its slot
-                    const bool owner_wrote = t < n && visit[t] >= 0 && T.split_cnt[d][t] > slot;
-                    if (!owner_wrote || visit[t] < visit[s]) T.split[d][(size_t)s * cap + j] = k;
-                });
-            }
+        if (T.split_overflows > 0) {
+            const int32_t *cnt[NDIR];
+            for (int d = 0; d < NDIR; ++d) cnt[d] = T.split_cnt[d].data();
+            std::vector<SpillWrite> w;
+            split_spill_writes(T, x, y, z, tan1, tan2, nor, nbhs, conn, cnt, w);
+            for (const SpillWrite &e : w) T.split[e.d][e.at] = e.value;
+        }
     }
 
     // ---- alias breadth-first search (implicit_aliasing.f90:21-42).
@@ -721,6 +751,46 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     return MFCFD_OK;
 }
 
+void chain_assign(const int32_t *lpts, int nsw, const int32_t *level, const int32_t *coff, const int32_t *cand, int n,
+                  int warps, std::vector<int32_t> &owner, std::vector<std::vector<int32_t>> &lists) {
+    owner.assign(n, -1);
+    lists.assign(warps, {});
+    std::vector<int32_t> last_point(warps, -1), last_level(warps, -1);
+    // warps ordered by the level of their last point (lazy min-heap)
+    std::vector<std::pair<int, int>> heap;
+    auto cmp = [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+        return a.first > b.first || (a.first == b.first && a.second > b.second);
+    };
+    for (int w = 0; w < warps; ++w) heap.push_back({-1, w});
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    for (int li = 0; li < nsw; ++li) {   // level-major, a topological order
+        const int p = lpts[li];
+        // continue the warp of the last deepest dependency that is its
+        // warp's latest point; otherwise the warp whose latest point is
+        // shallowest
+        int best = -1;
+        for (int c = coff[p]; c < coff[p + 1]; ++c)
+            if (last_point[owner[cand[c]]] == cand[c]) best = cand[c];
+        int w = -1;
+        if (best >= 0) {
+            w = owner[best];
+        } else {
+            while (true) {     // pop stale heap entries
+                std::pop_heap(heap.begin(), heap.end(), cmp);
+                auto top = heap.back();
+                heap.pop_back();
+                if (top.first == last_level[top.second]) { w = top.second; break; }
+            }
+        }
+        owner[p] = w;
+        lists[w].push_back(p);
+        last_point[w] = p;
+        last_level[w] = level[p];
+        heap.push_back({level[p], w});
+        std::push_heap(heap.begin(), heap.end(), cmp);
+    }
+}
+
 void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
     S.warps = warps;
     const int n = T.n;
@@ -733,16 +803,7 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
         const std::vector<int32_t> &off = fwd ? T.fwd_off : T.bwd_off;
         const std::vector<SweepEntry> &ent = fwd ? T.fwd_ent : T.bwd_ent;
         std::vector<int32_t> &owner = S.owner[dir];
-        owner.assign(n, -1);
-        std::vector<int32_t> last_point(warps, -1), last_level(warps, -1);
-        std::vector<std::vector<int32_t>> lists(warps);
-        // warps ordered by the level of their last point (lazy min-heap)
-        std::vector<std::pair<int, int>> heap;
-        auto cmp = [](const std::pair<int, int> &a, const std::pair<int, int> &b) {
-            return a.first > b.first || (a.first == b.first && a.second > b.second);
-        };
-        for (int w = 0; w < warps; ++w) heap.push_back({-1, w});
-        std::make_heap(heap.begin(), heap.end(), cmp);
+        std::vector<std::vector<int32_t>> lists;
         // each point's dependencies of the deepest level, in entry order
         // (computed in parallel; the assignment below only reads them)
         std::vector<int32_t> coff(n + 1, 0), cand;
@@ -759,39 +820,17 @@ void build_chain_schedule(Topology &T, int warps, ChainSchedule &S) {
         for (int p = 0; p < n; ++p) coff[p + 1] += coff[p];
         cand.resize((size_t)coff[n]);
         parallel_for(n, [&](int p) {
+            // the deepest level first, so only its entries are written and
+            // none lands past the point's own coff range
             int best_level = -1, at = coff[p];
-            for (int e = off[p]; e < off[p + 1]; ++e) {
-                if (!entry_is_dependency(ent[e]) || !T.swept[ent[e].k]) continue;
-                const int lv = level[ent[e].k];
-                if (lv > best_level) { best_level = lv; at = coff[p]; }
-                if (lv == best_level) cand[at++] = ent[e].k;
-            }
+            for (int e = off[p]; e < off[p + 1]; ++e)
+                if (entry_is_dependency(ent[e]) && T.swept[ent[e].k]) best_level = std::max(best_level, level[ent[e].k]);
+            for (int e = off[p]; e < off[p + 1]; ++e)
+                if (entry_is_dependency(ent[e]) && T.swept[ent[e].k] && level[ent[e].k] == best_level)
+                    cand[at++] = ent[e].k;
         });
-        for (int p : lpts) {           // level-major, a topological order
-            // continue the warp of the last deepest dependency that is its
-            // warp's latest point; otherwise the warp whose latest point is
-            // shallowest
-            int best = -1;
-            for (int c = coff[p]; c < coff[p + 1]; ++c)
-                if (last_point[owner[cand[c]]] == cand[c]) best = cand[c];
-            int w = -1;
-            if (best >= 0) {
-                w = owner[best];
-            } else {
-                while (true) {     // pop stale heap entries
-                    std::pop_heap(heap.begin(), heap.end(), cmp);
-                    auto top = heap.back();
-                    heap.pop_back();
-                    if (top.first == last_level[top.second]) { w = top.second; break; }
-                }
-            }
-            owner[p] = w;
-            lists[w].push_back(p);
-            last_point[w] = p;
-            last_level[w] = level[p];
-            heap.push_back({level[p], w});
-            std::push_heap(heap.begin(), heap.end(), cmp);
-        }
+        chain_assign(lpts.data(), (int)lpts.size(), level.data(), coff.data(), cand.data(), n, warps, owner,
+                     lists);
         S.ptr[dir].assign(warps + 1, 0);
         S.pts[dir].clear();
         for (int w = 0; w < warps; ++w) {
