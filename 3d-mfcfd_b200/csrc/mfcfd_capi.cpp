@@ -68,6 +68,11 @@ struct mfcfd_handle {
     int pending_chunk = 0;                 // mfcfd_launch: iterations not yet completed
     int32_t pending_t0 = 0;
     bool graphs_off = false;               // a capture failed: launch one by one
+    // device-resident set-up (mfcfd_params.gpu_setup = 1): the topology was
+    // computed on the device; the host keeps summaries and fetches the
+    // query arrays (stencils, alias, levels) from dt on demand
+    bool dev_setup = false;
+    DevTopology dt;
 };
 
 namespace {
@@ -329,6 +334,31 @@ int apply_chain_schedule(mfcfd_handle *h, int want, int *warps) {
     int wpb = 0, blocks = 0;
     const int w = chain_shape(h->P.device, want, h->P.chain_spread, &wpb, &blocks);
     if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+    if (h->dev_setup) {
+        DevCloud &d = h->d;
+        for (int dir = 0; dir < 2; ++dir) {
+            dfree(h, d.ch_ptr[dir]);
+            dfree(h, d.ch_pts[dir]);
+            dfree(h, d.ch_own[dir]);
+            dfree(h, d.ch_items[dir]);
+        }
+        const DevAlloc alloc = [h](void **ptr, size_t bytes) {
+            uint8_t *p = nullptr;
+            const int r = dalloc(h, &p, bytes);
+            *ptr = p;
+            return r;
+        };
+        std::string err;
+        int64_t terms[3];
+        if (int rc = device_chain_schedule(h->P.device, h->dt, d, w, h->stream, alloc, terms, err))
+            return fail(h, rc, err.empty() ? h->err : err);
+        d.ch_wpb = wpb;
+        d.ch_spread = h->P.chain_spread;
+        drop_graphs(h);
+        for (int k = 0; k < 3; ++k) h->chain_terms[k] = terms[k];
+        *warps = w;
+        return MFCFD_OK;
+    }
     ChainSchedule S;
     build_chain_schedule(h->T, w, S);
     DevCloud &d = h->d;
@@ -384,6 +414,10 @@ namespace {
 int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *z, const double *tan1,
                const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn);
 int attach_device(mfcfd_handle *h);
+int attach_state(mfcfd_handle *h);
+int create_on_device(mfcfd_handle *h, const double *x, const double *y, const double *z, const double *tan1,
+                     const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn,
+                     const double *min_dist);
 
 }  // namespace
 
@@ -484,6 +518,13 @@ int create_impl(const mfcfd_params *params, int32_t n, const int32_t *status, co
     }
     *out = h;   // also on failure: it holds the message
     return host_guard(&h->err, [&]() -> int {
+        if (attach && P.gpu_setup == 1 && P.device >= 0) {
+            int rc = classify_points(P, n, status, nbhs, conn, h->T, h->err);
+            if (rc) return rc;
+            if (device_setup_supported(P, h->T))
+                return create_on_device(h, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist);
+            h->T = Topology();   // the host set-up, with its GPU passes
+        }
         int rc = build_topology(P, n, status, x, y, z, tan1, tan2, nor, nbhs, conn, min_dist, h->T, h->err);
         if (rc) return rc;
         if (P.device < 0) return MFCFD_OK;   // host-only handle: set-up results, no device state
@@ -533,7 +574,7 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
         st->nbhs[s] = nbhs[i];
         for (int r = 0; r < MAX_CONN; ++r) {
             const int32_t k = conn[(size_t)i * MAX_CONN + r];
-            st->conn[s * MAX_CONN + r] = k > 0 ? (int32_t)at(k - 1) : 0;
+            st->conn[s * MAX_CONN + r] = (k > 0 && k <= n) ? (int32_t)at(k - 1) : 0;
         }
     }
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
@@ -551,6 +592,34 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
     return MFCFD_OK;
 }
 
+// The handle's streams: the main stream outranks the side stream, so the
+// chain sweep's blocks are placed before the concurrent flux kernel's.
+int create_streams(mfcfd_handle *h) {
+    if (cudaSetDevice(h->P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CK(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatest));
+    CK(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, least));
+    CK(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming));
+    return MFCFD_OK;
+}
+
+// DevCloud cleared, with the point count and the parameters the kernels read.
+void init_devcloud(mfcfd_handle *h, int n) {
+    const mfcfd_params &P = h->P;
+    DevCloud &d = h->d;
+    std::memset(&d, 0, sizeof d);
+    d.n = n;
+    d.power = P.power;
+    d.inner_iterations = P.inner_iterations;
+    d.update_variant = P.update_variant;
+    d.sweep_variant = P.sweep_variant;
+    d.cfl = P.cfl;
+    d.rho_inf = P.rho_inf; d.u1_inf = P.u1_inf; d.u2_inf = P.u2_inf;
+    d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;
+}
+
 // Streams, device arrays and uploads from the staged copies (with h->dry:
 // only the byte count).
 int attach_device(mfcfd_handle *h) {
@@ -559,30 +628,12 @@ int attach_device(mfcfd_handle *h) {
     const mfcfd_handle::Staged &st = *h->staged;
     const int n = T.n;
     int rc = MFCFD_OK;
-    if (!h->dry) {
-        if (cudaSetDevice(P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
-        // the main stream outranks the side stream, so the chain sweep's
-        // blocks are placed before the concurrent flux kernel's
-        int least = 0, greatest = 0;
-        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        CK(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatest));
-        CK(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, least));
-        CK(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming));
-    }
+    if (!h->dry && (rc = create_streams(h))) return rc;
 
     DevCloud &d = h->d;
-    std::memset(&d, 0, sizeof d);
-    d.n = n;
+    init_devcloud(h, n);
     d.shared_frame = T.shared_frame;
     std::memcpy(d.frame0, T.frame0, sizeof d.frame0);
-    d.power = P.power;
-    d.inner_iterations = P.inner_iterations;
-    d.update_variant = P.update_variant;
-    d.sweep_variant = P.sweep_variant;
-    d.cfl = P.cfl;
-    d.rho_inf = P.rho_inf; d.u1_inf = P.u1_inf; d.u2_inf = P.u2_inf;
-    d.u3_inf = P.u3_inf; d.pr_inf = P.pr_inf;
 
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
         // the schedule marks the entry lists, so it precedes their upload
@@ -645,6 +696,17 @@ int attach_device(mfcfd_handle *h) {
     d.n_wall = (int)T.wall_idx.size();
     d.n_swept = (int)T.fwd_lvl_pts.size();
     d.max_width = T.max_level_width;
+    return attach_state(h);
+}
+
+// The iteration state and the work arrays of a handle whose topology is on
+// the device (with h->dry: only their byte count).
+int attach_state(mfcfd_handle *h) {
+    const mfcfd_params &P = h->P;
+    const Topology &T = h->T;
+    DevCloud &d = h->d;
+    const int n = d.n;
+    int rc = MFCFD_OK;
     d.sweep_mode = P.sweep_mode;
     d.precision = P.precision;
     if ((rc = dalloc(h, &d.sweep_counter, 2))) return rc;
@@ -676,6 +738,114 @@ int attach_device(mfcfd_handle *h) {
     CK(cudaMemsetAsync(d.dinv, 0, (size_t)n * 8, h->stream));
     CK(cudaMemsetAsync(d.res_sqr, 0, (size_t)n * 8, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    return MFCFD_OK;
+}
+
+// mfcfd_create with gpu_setup = 1 where device_setup_supported(): the whole
+// set-up on the device (T holds classify_points' result).
+int create_on_device(mfcfd_handle *h, const double *x, const double *y, const double *z, const double *tan1,
+                     const double *tan2, const double *nor, const int32_t *nbhs, const int32_t *conn,
+                     const double *min_dist) {
+    const mfcfd_params &P = h->P;
+    Topology &T = h->T;
+    const int n = T.n;
+    int rc = MFCFD_OK;
+    if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+        if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
+        if (P.chain_spread < 0 || P.chain_spread > 1) return fail(h, MFCFD_ERR_ARG, "chain_spread must be 0 or 1");
+    }
+    if (P.storage_order == MFCFD_ORDER_MORTON && n > 1) {
+        morton_order(n, x, y, z, T.perm);
+        T.inv.assign(n, 0);
+        for (int i = 0; i < n; ++i) T.inv[T.perm[i]] = i;
+    }
+    std::vector<double> eps2;
+    limiter_eps2(P, n, min_dist, T.perm.empty() ? nullptr : T.perm.data(), eps2);
+    if ((rc = create_streams(h))) return rc;
+    init_devcloud(h, n);
+    h->dev_setup = true;
+    DevCloud &d = h->d;
+    const DevAlloc alloc = [h](void **ptr, size_t bytes) {
+        uint8_t *p = nullptr;
+        const int r = dalloc(h, &p, bytes);
+        *ptr = p;
+        return r;
+    };
+    std::string err;
+    if ((rc = device_setup(P.device, P, T, x, y, z, tan1, tan2, nor, nbhs, conn, eps2, h->stream, alloc, d, h->dt,
+                           err)))
+        return fail(h, rc, err.empty() ? h->err : err);
+    // host summaries, in the host set-up's form
+    T.fwd_lvl_ptr = h->dt.lvl_ptr[0];
+    T.bwd_lvl_ptr = h->dt.lvl_ptr[1];
+    T.max_level_width = h->dt.max_width;
+    T.split_overflows = (int)h->dt.split_overflows;
+    T.shared_frame = d.shared_frame;
+    std::memcpy(T.frame0, d.frame0, sizeof T.frame0);
+    T.g0_pts = h->dt.g0_pts;
+    T.sweep_variant = P.sweep_variant;
+    if (!T.perm.empty()) {
+        std::vector<int8_t> cls(n);
+        for (int i = 0; i < n; ++i) cls[T.perm[i]] = T.cls[i];
+        T.cls.swap(cls);
+        for (std::vector<int32_t> *a : {&T.wall_idx, &T.outer_idx, &T.interior_idx})
+            for (int32_t &v : *a) v = T.perm[v];
+    }
+    if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+        const int want = P.chain_warps > 0 ? P.chain_warps : 2 * T.max_level_width;
+        int wpb = 0, blocks = 0;
+        const int w = chain_shape(P.device, want, P.chain_spread, &wpb, &blocks);
+        if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");
+        int64_t terms[3];
+        if ((rc = device_chain_schedule(P.device, h->dt, d, w, h->stream, alloc, terms, err)))
+            return fail(h, rc, err.empty() ? h->err : err);
+        d.ch_wpb = wpb;
+        d.ch_spread = P.chain_spread;
+        d.flux_grid = P.flux_blocks_per_sm > 0 ? P.flux_blocks_per_sm * device_sms(P.device) : 0;
+        for (int k = 0; k < 3; ++k) h->chain_terms[k] = terms[k];
+        if (d.n_g0 > 0 && (rc = dalloc(h, &d.g0, (size_t)d.n_g0 * G0_DOUBLES))) return rc;
+    }
+    if (!T.perm.empty()) {
+        const int32_t *pd = nullptr;
+        if ((rc = upload(h, &pd, T.perm))) return rc;
+        h->perm_dev = const_cast<int32_t *>(pd);
+        if ((rc = dalloc(h, &h->xfer, (size_t)n * 5))) return rc;
+    }
+    return attach_state(h);
+}
+
+// The topology arrays the queries read, fetched from a device set-up into
+// the host copy the first time they are asked for.
+int fetch_query_arrays(mfcfd_handle *h, bool stencils, bool alias, bool levels) {
+    if (!h->dev_setup) return MFCFD_OK;
+    Topology &T = h->T;
+    const DevTopology &dt = h->dt;
+    const int n = T.n;
+    const size_t flat = (size_t)n * T.cap + 64;
+    if (stencils && T.split[0].empty()) {
+        std::vector<int32_t> cnt((size_t)NDIR * n);
+        CK(cudaMemcpyAsync(cnt.data(), dt.split_cnt, 4 * cnt.size(), cudaMemcpyDeviceToHost, h->stream));
+        for (int k = 0; k < NDIR; ++k) {
+            T.split[k].resize(flat);
+            CK(cudaMemcpyAsync(T.split[k].data(), dt.split[k], 4 * flat, cudaMemcpyDeviceToHost, h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        for (int k = 0; k < NDIR; ++k) T.split_cnt[k].assign(cnt.begin() + (size_t)k * n, cnt.begin() + (size_t)(k + 1) * n);
+    }
+    if (alias && T.alias.empty()) {
+        T.alias.resize(n);
+        T.point_with_alias.resize(n);
+        CK(cudaMemcpyAsync(T.alias.data(), dt.alias, 4 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(T.point_with_alias.data(), dt.pwa, 4 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    if (levels && T.fwd_level.empty()) {
+        T.fwd_level.resize(n);
+        T.bwd_level.resize(n);
+        CK(cudaMemcpyAsync(T.fwd_level.data(), dt.level[0], 4 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(T.bwd_level.data(), dt.level[1], 4 * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
     return MFCFD_OK;
 }
 
@@ -890,6 +1060,7 @@ int mfcfd_get_stencils(mfcfd_handle *h, int32_t *counts, int32_t *lists, int32_t
         if (!h || !counts || !lists || width < 1) return MFCFD_ERR_ARG;
         const Topology &T = h->T;
         if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        if (int rc = fetch_query_arrays(h, true, false, false)) return rc;
         for (int i = 0; i < T.n; ++i)
             for (int dd = 0; dd < NDIR; ++dd) {
                 int c = T.split_cnt[dd][i];
@@ -907,6 +1078,7 @@ int mfcfd_get_alias(mfcfd_handle *h, int32_t *alias, int32_t *point_with_alias) 
         if (!h || !alias || !point_with_alias) return MFCFD_ERR_ARG;
         const Topology &T = h->T;
         if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        if (int rc = fetch_query_arrays(h, false, true, false)) return rc;
         std::memcpy(alias, T.alias.data(), sizeof(int32_t) * T.n);
         std::memcpy(point_with_alias, T.point_with_alias.data(), sizeof(int32_t) * T.n);
         return MFCFD_OK;
@@ -918,11 +1090,63 @@ int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level) {
         if (!h || !level || (dir != 0 && dir != 1)) return MFCFD_ERR_ARG;
         const Topology &T = h->T;
         if (T.n == 0) return fail(h, MFCFD_ERR_ARG, "handle was not created successfully");
+        if (int rc = fetch_query_arrays(h, false, false, true)) return rc;
         const std::vector<int32_t> &src = dir == 0 ? T.fwd_level : T.bwd_level;
         if (T.perm.empty()) std::memcpy(level, src.data(), sizeof(int32_t) * T.n);
         else
             for (int i = 0; i < T.n; ++i) level[i] = src[T.perm[i]];
         return MFCFD_OK;
+    });
+}
+
+int mfcfd_debug_digest(mfcfd_handle *h, const char *name, uint64_t *digest, int64_t *bytes) {
+    return host_guard(h ? &h->err : nullptr, [&]() -> int {
+        if (!h || !name || !digest || !bytes) return MFCFD_ERR_ARG;
+        if (!h->stream) return fail(h, MFCFD_ERR_ARG, "handle has no device state");
+        const DevCloud &d = h->d;
+        const size_t n = (size_t)d.n;
+        int32_t ends[2] = {0, 0};
+        if (d.fwd_off) CK(cudaMemcpy(&ends[0], d.fwd_off + n, 4, cudaMemcpyDeviceToHost));
+        if (d.bwd_off) CK(cudaMemcpy(&ends[1], d.bwd_off + n, 4, cudaMemcpyDeviceToHost));
+        const size_t nsw = (size_t)d.n_swept, w1 = (size_t)d.ch_warps + 1;
+        const bool ch = d.sweep_mode == MFCFD_SWEEP_CHAINS;
+        const struct {
+            const char *name;
+            const void *p;
+            size_t bytes;
+        } arrays[] = {
+            {"x", d.x, 8 * n}, {"y", d.y, 8 * n}, {"z", d.z, 8 * n}, {"frame", d.frame, 72 * n},
+            {"cls", d.cls, n}, {"nbhs", d.nbhs, 4 * n}, {"conn", d.conn, 4 * n * MAX_CONN},
+            {"eps2", d.eps2, 8 * n}, {"slot_nbr", d.slot_nbr, 4 * n * MAX_SLOTS}, {"nslot", d.nslot, n},
+            {"slot_mask", d.slot_mask, n * MAX_SLOTS}, {"list_cnt", d.list_cnt, n * NDIR},
+            {"list_ent", d.list_ent, n * NDIR * LIST_STRIDE}, {"geo", d.geo, 8 * n * GEO_STRIDE},
+            {"swept", d.swept, n}, {"consumer_shared", d.consumer_shared, n},
+            {"fwd_lvl_ptr", d.fwd_lvl_ptr, 4 * ((size_t)d.n_fwd_levels + 1)}, {"fwd_lvl_pts", d.fwd_lvl_pts, 4 * nsw},
+            {"bwd_lvl_ptr", d.bwd_lvl_ptr, 4 * ((size_t)d.n_bwd_levels + 1)}, {"bwd_lvl_pts", d.bwd_lvl_pts, 4 * nsw},
+            {"fwd_off", d.fwd_off, 4 * (n + 1)}, {"bwd_off", d.bwd_off, 4 * (n + 1)},
+            {"fwd_cnt", d.fwd_cnt, n * NDIR}, {"bwd_cnt", d.bwd_cnt, n * NDIR},
+            {"fwd_ent", d.fwd_ent, sizeof(SweepEntry) * (size_t)ends[0]},
+            {"bwd_ent", d.bwd_ent, sizeof(SweepEntry) * (size_t)ends[1]},
+            {"fwd_need", d.fwd_need, 4 * n}, {"bwd_need", d.bwd_need, 4 * n},
+            {"fwd_old", d.fwd_old, 4 * n}, {"bwd_old", d.bwd_old, 4 * n},
+            {"sweep_slot_mask", d.sweep_slot_mask, n * MAX_SLOTS}, {"res_order", d.res_order, 4 * (size_t)d.n_res},
+            {"pre_order", d.pre_order, ch ? 4 * n : 0}, {"g0_pts", d.g0_pts, 4 * (size_t)d.n_g0},
+            {"ch_ptr0", d.ch_ptr[0], ch ? 4 * w1 : 0}, {"ch_pts0", d.ch_pts[0], ch ? 4 * nsw : 0},
+            {"ch_own0", d.ch_own[0], ch ? 4 * n : 0}, {"ch_items0", d.ch_items[0], ch ? sizeof(ChainItem) * nsw : 0},
+            {"ch_ptr1", d.ch_ptr[1], ch ? 4 * w1 : 0}, {"ch_pts1", d.ch_pts[1], ch ? 4 * nsw : 0},
+            {"ch_own1", d.ch_own[1], ch ? 4 * n : 0}, {"ch_items1", d.ch_items[1], ch ? sizeof(ChainItem) * nsw : 0},
+        };
+        for (const auto &a : arrays) {
+            if (std::strcmp(a.name, name) != 0) continue;
+            std::vector<uint8_t> buf(a.bytes);
+            if (a.bytes && a.p) CK(cudaMemcpy(buf.data(), a.p, a.bytes, cudaMemcpyDeviceToHost));
+            uint64_t hsh = 14695981039346656037ull;   // FNV-1a
+            for (uint8_t b : buf) hsh = (hsh ^ b) * 1099511628211ull;
+            *digest = hsh;
+            *bytes = a.p ? (int64_t)a.bytes : -1;
+            return MFCFD_OK;
+        }
+        return fail(h, MFCFD_ERR_ARG, std::string("unknown array ") + name);
     });
 }
 

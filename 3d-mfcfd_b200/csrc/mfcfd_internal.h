@@ -4,6 +4,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <functional>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -183,6 +184,45 @@ int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, 
 int prep_levels_gpu(int device, int n, const std::vector<int> &order, const std::vector<int32_t> &doff,
                     const std::vector<int32_t> &deps, std::vector<int32_t> &level, std::string &err);
 void build_pre_order(const Topology &T, std::vector<int32_t> &order);
+
+// Device-resident set-up (mfcfd_prep.cu; mfcfd_params.gpu_setup = 1 on a
+// handle created with its device).  Every topology array the kernels read
+// is computed on the device, in storage order, from the cloud uploaded once,
+// with the host path's values (the same operations in the same order); the
+// host classifies and orders the points, evaluates the limiter's eps2 (the
+// C library's pow) and assigns the chain schedule's warps from a few arrays
+// per point.  device_setup_supported() names the configurations it covers;
+// the others take the host set-up.
+struct DevCloud;
+using DevAlloc = std::function<int(void **ptr, size_t bytes)>;
+struct DevTopology {
+    // kept on the device for the queries (stencils, alias, levels)
+    int32_t *split[NDIR] = {};     // the reference's storage: cap*n + 64 per list, logical ids and columns
+    int32_t *split_cnt = nullptr;  // NDIR*n, logical
+    int32_t *alias = nullptr;      // n, logical, 1-based values
+    int32_t *pwa = nullptr;        // n, 1-based logical ids, 0: none
+    int32_t *level[2] = {};        // n, storage order, -1: not swept
+    // host copies: level pointers (info), and what the chain schedule's warp
+    // assignment reads (levels, level-major points, deepest dependencies)
+    std::vector<int32_t> lvl_ptr[2];
+    std::vector<int32_t> h_level[2], h_lpts[2], h_coff[2], h_cand[2];
+    std::vector<int32_t> g0_pts;
+    int64_t split_overflows = 0;
+    int max_width = 0;
+};
+bool device_setup_supported(const mfcfd_params &P, const Topology &T);
+// T: classify_points' result with perm/inv set (empty: index order); eps2 in
+// storage order.  Fills d's topology pointers and counts and dt; every
+// allocation goes through `alloc` (owned by the caller, also on failure).
+int device_setup(int device, const mfcfd_params &P, const Topology &T, const double *x, const double *y,
+                 const double *z, const double *tan1, const double *tan2, const double *nor, const int32_t *nbhs,
+                 const int32_t *conn, const std::vector<double> &eps2, cudaStream_t s, const DevAlloc &alloc,
+                 DevCloud &d, DevTopology &dt, std::string &err);
+// The chain schedule of a device set-up for `warps` warps: d.ch_* (allocated
+// through alloc; the caller frees the previous ones), the entries' chain
+// bits re-marked on the device; terms[3] as ChainSchedule::terms_*.
+int device_chain_schedule(int device, DevTopology &dt, DevCloud &d, int warps, cudaStream_t s,
+                          const DevAlloc &alloc, int64_t terms[3], std::string &err);
 // Storage order along a Morton (Z-order) curve of the coordinates, quantised
 // to 21 bits per axis over the cloud's bounding box; points with the same
 // key keep their index order.  perm[logical] = storage index.
@@ -233,6 +273,9 @@ int host_guard(std::string *err, F &&f) noexcept {
 // (T.n, T.cap, T.cls, T.*_idx); the first step of build_topology.
 int classify_points(const mfcfd_params &P, int n, const int32_t *status, const int32_t *nbhs, const int32_t *conn,
                     Topology &T, std::string &err);
+// The limiter's epsilon per point, (vl_const*min_dist)**3 squared
+// (limiters.f90:251-253), at perm[i] (perm null: index order).
+void limiter_eps2(const mfcfd_params &P, int n, const double *min_dist, const int32_t *perm, std::vector<double> &eps2);
 // One split-list entry written past a list's capacity into the storage that
 // follows it (list d, flat index within the list's array, 1-based id).
 struct SpillWrite {

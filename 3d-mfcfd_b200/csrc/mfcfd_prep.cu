@@ -21,8 +21,12 @@
  *    level L), with one kernel per level queued without host round trips.
  */
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -333,14 +337,14 @@ int prep_split_gpu(int device, int n, int cap, const std::vector<int8_t> &cls, c
     return MFCFD_OK;
 }
 
-int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, std::vector<int32_t> &alias,
-                   std::vector<int32_t> &pwa, std::string &err) {
-    PREP_CK(cudaSetDevice(device));
-    Stream st;
-    PREP_CK(cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking));
-    cudaStream_t s = st.s;
+namespace {
+
+// The breadth-first search on device arrays (nbhs, 1-based conn): alias and
+// point_with_alias, both n long, are written on stream s.
+int alias_search(int device, int n, const int32_t *d_nb, const int32_t *d_conn, int32_t *d_alias, int32_t *d_pwa,
+                 cudaStream_t s, std::string &err) {
     DevBufs b;
-    int32_t *d_nb, *d_conn, *d_alias, *d_pwa, *d_fa, *d_fb;
+    int32_t *d_fa, *d_fb;
     unsigned *d_key;
     int *d_flag, *d_pos, *d_sums, *d_total;
     const size_t kspace = (size_t)n * MAX_CONN;
@@ -348,13 +352,9 @@ int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, 
         err = "cloud too large for the GPU alias search";
         return MFCFD_ERR_UNSUPPORTED;
     }
-    PREP_CK(b.alloc(&d_nb, n)); PREP_CK(b.alloc(&d_conn, kspace));
-    PREP_CK(b.alloc(&d_alias, n)); PREP_CK(b.alloc(&d_pwa, n));
     PREP_CK(b.alloc(&d_fa, n)); PREP_CK(b.alloc(&d_fb, n));
     PREP_CK(b.alloc(&d_key, n)); PREP_CK(b.alloc(&d_flag, kspace)); PREP_CK(b.alloc(&d_pos, kspace));
     PREP_CK(b.alloc(&d_sums, (kspace + 1023) / 1024)); PREP_CK(b.alloc(&d_total, 1));
-    PREP_CK(cudaMemcpyAsync(d_nb, nbhs, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
-    PREP_CK(cudaMemcpyAsync(d_conn, conn, 4 * kspace, cudaMemcpyHostToDevice, s));
     PREP_CK(cudaMemsetAsync(d_alias, 0, 4 * (size_t)n, s));
     PREP_CK(cudaMemsetAsync(d_pwa, 0, 4 * (size_t)n, s));
     PREP_CK(cudaMemsetAsync(d_key, 0xff, 4 * (size_t)n, s));
@@ -385,6 +385,25 @@ int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, 
         count += found;
         std::swap(front, next);
     }
+    return MFCFD_OK;
+}
+
+}  // namespace
+
+int prep_alias_gpu(int device, int n, const int32_t *nbhs, const int32_t *conn, std::vector<int32_t> &alias,
+                   std::vector<int32_t> &pwa, std::string &err) {
+    PREP_CK(cudaSetDevice(device));
+    Stream st;
+    PREP_CK(cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking));
+    cudaStream_t s = st.s;
+    DevBufs b;
+    int32_t *d_nb, *d_conn, *d_alias, *d_pwa;
+    const size_t kspace = (size_t)n * MAX_CONN;
+    PREP_CK(b.alloc(&d_nb, n)); PREP_CK(b.alloc(&d_conn, kspace));
+    PREP_CK(b.alloc(&d_alias, n)); PREP_CK(b.alloc(&d_pwa, n));
+    PREP_CK(cudaMemcpyAsync(d_nb, nbhs, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(d_conn, conn, 4 * kspace, cudaMemcpyHostToDevice, s));
+    if (int rc = alias_search(device, n, d_nb, d_conn, d_alias, d_pwa, s, err)) return rc;
     alias.assign(n, 0);
     pwa.assign(n, 0);
     PREP_CK(cudaMemcpyAsync(alias.data(), d_alias, 4 * (size_t)n, cudaMemcpyDeviceToHost, s));
@@ -453,5 +472,970 @@ int prep_levels_gpu(int device, int n, const std::vector<int> &order, const std:
         }
     return MFCFD_OK;
 }
+
+// ================================================================ device-resident set-up
+//
+// The passes of build_topology (mfcfd_setup.cpp) on device arrays, in the
+// storage order of the handle: a point p of storage is the reference's point
+// inv[p], and every point id a kernel writes is a storage index.  Each pass
+// evaluates what the host's does for that point, with the same operations in
+// the same order (this file is compiled without contraction), so the arrays
+// equal those build_topology + permute_topology give.
+
+namespace {
+
+struct SplitPtrs {
+    int32_t *p[NDIR];
+};
+
+__device__ __forceinline__ int map_id(const int32_t *perm, int i) { return perm ? perm[i] : i; }
+
+inline int grid_for(int device, size_t len) {
+    const size_t g = (len + PREP_THREADS - 1) / PREP_THREADS;
+    return (int)std::max<size_t>(1, std::min<size_t>(g, (size_t)device_sms(device) * 16));
+}
+
+#define GRID_STRIDE(t, len) \
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (len); t += (size_t)gridDim.x * blockDim.x)
+
+// storage-order copies of the cloud: coordinates, frames (tan1, tan2, nor per
+// point), classes, neighbour counts and conn with 0-based storage ids (an id
+// past nbhs that is not a point reads 0, like a zero pad)
+__global__ void k_stage_cloud(int n, const int32_t *perm, const double *x, const double *y, const double *z,
+                              const double *t1, const double *t2, const double *nn, const int8_t *cls,
+                              const int32_t *nbhs, const int32_t *conn, double *sx, double *sy, double *sz,
+                              double *frame, int8_t *scls, int32_t *snb, int32_t *sconn) {
+    GRID_STRIDE(t, (size_t)n) {
+        const int i = (int)t, p = map_id(perm, i);
+        sx[p] = x[i];
+        sy[p] = y[i];
+        sz[p] = z[i];
+        for (int r = 0; r < 3; ++r) {
+            frame[9 * (size_t)p + r] = t1[3 * (size_t)i + r];
+            frame[9 * (size_t)p + 3 + r] = t2[3 * (size_t)i + r];
+            frame[9 * (size_t)p + 6 + r] = nn[3 * (size_t)i + r];
+        }
+        scls[p] = cls[i];
+        snb[p] = nbhs[i];
+        for (int r = 0; r < MAX_CONN; ++r) {
+            const int k = conn[(size_t)i * MAX_CONN + r];
+            sconn[(size_t)p * MAX_CONN + r] = (k > 0 && k <= n) ? map_id(perm, k - 1) : 0;
+        }
+    }
+}
+
+// split stencils in the reference's storage (logical): own cells only; the
+// counts are the lists' full lengths
+__global__ void k_split_own(int n, int cap, const int8_t *cls, const double *x, const double *y, const double *z,
+                            const double *tan1, const double *tan2, const double *nor, const int32_t *nbhs,
+                            const int32_t *conn, SplitPtrs split, int32_t *cnt, int *overflow) {
+    GRID_STRIDE(t, (size_t)n) {
+        const int i = (int)t;
+        const int c = cls[i];
+        int cn[NDIR] = {0, 0, 0, 0, 0, 0};
+        if (c == CLS_INTERIOR || c == CLS_WALL || c == CLS_OUTER) {
+            const double xi = x[i], yi = y[i], zi = z[i];
+            const double *t1 = tan1 + 3 * (size_t)i, *t2 = tan2 + 3 * (size_t)i, *nn = nor + 3 * (size_t)i;
+            auto push = [&](int d, int k) {
+                const int j = cn[d]++;
+                if (j < cap) split.p[d][(size_t)i * cap + j] = k;
+            };
+            for (int r = 0; r < nbhs[i]; ++r) {
+                const int k = conn[(size_t)i * MAX_CONN + r];
+                const double delx = x[k - 1] - xi, dely = y[k - 1] - yi, delz = z[k - 1] - zi;
+                const double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+                const double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+                if (c == CLS_INTERIOR) {
+                    const double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                    if (dels <= 0.0) push(0, k);
+                    if (dels > 0.0) push(1, k);
+                    if (delt <= 0.0) push(2, k);
+                    if (delt > 0.0) push(3, k);
+                    if (deln <= 0.0) push(4, k);
+                    if (deln > 0.0) push(5, k);
+                } else {
+                    if (dels <= 0.0) push(0, k);
+                    if (dels >= 0.0) push(1, k);
+                    if (delt <= 0.0) push(2, k);
+                    if (delt >= 0.0) push(3, k);
+                    push(c == CLS_WALL ? 5 : 4, k);
+                }
+            }
+        }
+        bool over = false;
+        for (int d = 0; d < NDIR; ++d) {
+            cnt[(size_t)d * n + i] = cn[d];
+            over = over || cn[d] > cap;
+        }
+        if (over) atomicExch(overflow, 1);
+    }
+}
+
+__global__ void k_spill_apply(int m, const int *d, const long long *at, const int32_t *val, SplitPtrs split) {
+    GRID_STRIDE(t, (size_t)m) split.p[d[t]][at[t]] = val[t];
+}
+
+// alias of every storage point (the sweeps compare aliases)
+__global__ void k_alias_storage(int n, const int32_t *perm, const int32_t *alias, int32_t *salias) {
+    GRID_STRIDE(t, (size_t)n) salias[map_id(perm, (int)t)] = alias[t];
+}
+
+enum { SLOT_OK = 0, SLOT_ZERO, SLOT_LONG, SLOT_WIDE };
+
+// effective lists and neighbour slots (build_topology's "effective lists")
+__global__ void k_slots(int n, int cap, const int32_t *perm, const int32_t *inv, const int8_t *cls,
+                        const int32_t *nbhs, const int32_t *conn, SplitPtrs split, const int32_t *cnt,
+                        int32_t *slot_nbr, uint8_t *nslot, uint8_t *slot_mask, uint8_t *list_cnt, uint8_t *list_ent,
+                        uint8_t *code, int *bad) {
+    GRID_STRIDE(t, (size_t)n) {
+        const int p = (int)t, i = inv ? inv[p] : p;
+        int32_t *slots = slot_nbr + (size_t)p * MAX_SLOTS;
+        uint8_t *mask = slot_mask + (size_t)p * MAX_SLOTS;
+        for (int s = 0; s < MAX_SLOTS; ++s) {
+            slots[s] = -1;
+            mask[s] = 0;
+        }
+        for (int e = 0; e < NDIR * LIST_STRIDE; ++e) list_ent[(size_t)p * NDIR * LIST_STRIDE + e] = 0;
+        for (int d = 0; d < NDIR; ++d) list_cnt[(size_t)p * NDIR + d] = 0;
+        int ns = 0;
+        auto slot_of = [&](int k) -> int {
+            for (int s = 0; s < ns; ++s)
+                if (slots[s] == k) return s;
+            if (ns == MAX_SLOTS) return -1;
+            slots[ns] = k;
+            return ns++;
+        };
+        const int nb = nbhs[i];
+        for (int r = 0; r < nb; ++r) slot_of(map_id(perm, conn[(size_t)i * MAX_CONN + r] - 1));
+        const int c = cls[i];
+        int status = SLOT_OK;
+        for (int d = 0; d < NDIR && status == SLOT_OK; ++d) {
+            const bool unused = (c == CLS_WALL && d == 4) || (c == CLS_OUTER && d == 5) || c == CLS_SUPERSONIC;
+            if (unused) continue;
+            const bool use_conn = c == CLS_WALL && d == 5;
+            const int len = use_conn ? nb : cnt[(size_t)d * n + i];
+            if (!use_conn)
+                for (int j = 0; j < len; ++j) {
+                    const int k = split.p[d][(size_t)i * cap + j];
+                    if (k < 1 || k > n) status = SLOT_ZERO;
+                }
+            if (status != SLOT_OK) break;
+            if (len > MAX_CONN) { status = SLOT_LONG; break; }
+            list_cnt[(size_t)p * NDIR + d] = (uint8_t)len;
+            for (int j = 0; j < len; ++j) {
+                const int k1 = use_conn ? conn[(size_t)i * MAX_CONN + j] : split.p[d][(size_t)i * cap + j];
+                const int s = slot_of(map_id(perm, k1 - 1));
+                if (s < 0) { status = SLOT_WIDE; break; }
+                list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j] = (uint8_t)s;
+                mask[s] |= (uint8_t)(1u << d);
+            }
+        }
+        nslot[p] = (uint8_t)ns;
+        code[i] = (uint8_t)status;
+        if (status != SLOT_OK) atomicMin(bad, i);
+    }
+}
+
+__device__ __forceinline__ double dev_det(double xx, double yy, double zz, double xy, double yz, double zx) {
+    return xx * (yy * zz - yz * yz) - xy * (xy * zz - yz * zx) + zx * (xy * yz - yy * zx);
+}
+
+// Cramer numerators in the reference's operand order (implicit_D_inv_interior
+// .f90:103-105, :225-227, :347-349), as the host set-up's numerator()
+__device__ __forceinline__ double dev_numerator(int axis, double xx, double yy, double zz, double xy, double yz,
+                                                double zx, double fx, double fy, double fz) {
+    if (axis == 0)
+        return fx * (yy * zz - yz * yz) - fy * (xy * zz - zx * yz) + fz * (xy * yz - zx * yy);
+    if (axis == 1)
+        return xx * (fy * zz - yz * fz) - xy * (fx * zz - zx * fz) + zx * (fx * yz - zx * fy);
+    return xx * (yy * fz - fy * yz) - xy * (xy * fz - fx * yz) + zx * (xy * fy - fx * yy);
+}
+
+// least-squares moments, determinant and D_inv numerator per (point, list),
+// weight 1 (power 0)
+__global__ void k_geo(int n, const double *x, const double *y, const double *z, const double *frame,
+                      const uint8_t *list_cnt, const uint8_t *list_ent, const int32_t *slot_nbr, double *geo) {
+    GRID_STRIDE(t, (size_t)n) {
+        const int i = (int)t;
+        const double *t1 = frame + 9 * (size_t)i, *t2 = t1 + 3, *nn = t1 + 6;
+        for (int d = 0; d < NDIR; ++d) {
+            const int c = list_cnt[(size_t)i * NDIR + d];
+            double xx = 0, yy = 0, zz = 0, xy = 0, yz = 0, zx = 0, sdx = 0, sdy = 0, sdz = 0;
+            for (int j = 0; j < c; ++j) {
+                const int s = list_ent[((size_t)i * NDIR + d) * LIST_STRIDE + j];
+                const int k = slot_nbr[(size_t)i * MAX_SLOTS + s];
+                const double delx = x[k] - x[i], dely = y[k] - y[i], delz = z[k] - z[i];
+                const double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+                const double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+                const double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                const double w = 1.0;
+                const double ws = dels * w, wt = delt * w, wn = deln * w;
+                xx = xx + dels * ws;
+                yy = yy + delt * wt;
+                zz = zz + deln * wn;
+                xy = xy + dels * wt;
+                yz = yz + delt * wn;
+                zx = zx + deln * ws;
+                sdx = sdx + ws;
+                sdy = sdy + wt;
+                sdz = sdz + wn;
+            }
+            double *g = geo + (size_t)i * GEO_STRIDE + d * 8;
+            g[G_XX] = xx; g[G_YY] = yy; g[G_ZZ] = zz;
+            g[G_XY] = xy; g[G_YZ] = yz; g[G_ZX] = zx;
+            g[G_DET] = dev_det(xx, yy, zz, xy, yz, zx);
+            g[G_DNUM] = dev_numerator(d / 2, xx, yy, zz, xy, yz, zx, sdx, sdy, sdz);
+        }
+    }
+}
+
+// sweep order: the points point_with_alias names that the sweeps update
+__global__ void k_swept_flags(int n, const int32_t *pwa, const int8_t *cls, int *flag) {
+    GRID_STRIDE(t, (size_t)n) {
+        const int q = pwa[t];
+        const int c = q > 0 ? cls[q - 1] : -1;
+        flag[t] = (c == CLS_WALL || c == CLS_INTERIOR) ? 1 : 0;
+    }
+}
+
+__global__ void k_swept_emit(int n, const int32_t *pwa, const int32_t *perm, const int *flag, const int *pos,
+                             int32_t *order, uint8_t *swept) {
+    GRID_STRIDE(t, (size_t)n) {
+        if (!flag[t]) continue;
+        const int p = map_id(perm, pwa[t] - 1);
+        order[pos[t]] = p;
+        swept[p] = 1;
+    }
+}
+
+__global__ void k_reverse(int m, const int32_t *a, int32_t *b) {
+    GRID_STRIDE(t, (size_t)m) b[t] = a[m - 1 - (int)t];
+}
+
+// sweep terms: count per point (then a scan gives the offsets), fill
+__global__ void k_ent_count(int nsw, bool forward, const int32_t *order, const int32_t *salias,
+                            const uint8_t *list_cnt, const uint8_t *list_ent, const int32_t *slot_nbr, uint8_t *cnt,
+                            int *tot) {
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int p = order[t];
+        int all = 0;
+        for (int d = 0; d < NDIR; ++d) {
+            const int c = list_cnt[(size_t)p * NDIR + d];
+            int taken = 0;
+            for (int j = 0; j < c; ++j) {
+                const int k = slot_nbr[(size_t)p * MAX_SLOTS + list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j]];
+                if (forward ? salias[k] < salias[p] : salias[k] > salias[p]) ++taken;
+            }
+            cnt[(size_t)p * NDIR + d] = (uint8_t)taken;
+            all += taken;
+        }
+        tot[p] = all;
+    }
+}
+
+__global__ void k_ent_fill(int nsw, bool forward, const int32_t *order, const int32_t *salias, const double *x,
+                           const double *y, const double *z, const double *frame, const uint8_t *list_cnt,
+                           const uint8_t *list_ent, const int32_t *slot_nbr, const int32_t *off, SweepEntry *ent,
+                           uint32_t *need, int *too_many) {
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int p = order[t];
+        const double *t1 = frame + 9 * (size_t)p, *t2 = t1 + 3, *nn = t1 + 6;
+        int at = off[p];
+        uint32_t nd = 0;
+        for (int d = 0; d < NDIR; ++d) {
+            const int c = list_cnt[(size_t)p * NDIR + d];
+            for (int j = 0; j < c; ++j) {
+                const int s = list_ent[((size_t)p * NDIR + d) * LIST_STRIDE + j];
+                const int k = slot_nbr[(size_t)p * MAX_SLOTS + s];
+                if (!(forward ? salias[k] < salias[p] : salias[k] > salias[p])) continue;
+                const double delx = x[k] - x[p], dely = y[k] - y[p], delz = z[k] - z[p];
+                const double dels = delx * t1[0] + dely * t1[1] + delz * t1[2];
+                const double delt = delx * t2[0] + dely * t2[1] + delz * t2[2];
+                const double deln = delx * nn[0] + dely * nn[1] + delz * nn[2];
+                const double w = 1.0;
+                SweepEntry &e = ent[at++];
+                e.k = k;
+                e.pad = d | (s << 8);
+                e.w[0] = dels * w;
+                e.w[1] = delt * w;
+                e.w[2] = deln * w;
+                nd |= 1u << s;
+            }
+        }
+        need[p] = nd;
+        if (at - off[p] > SWEEP_MAX_ENTRIES) atomicExch(too_many, 1);
+    }
+}
+
+// levels by Kahn's layering over the sweep terms whose producer is swept
+__global__ void k_dep_count(int nsw, const int32_t *order, const int32_t *off, const SweepEntry *ent,
+                            const uint8_t *swept, int32_t *indeg, int32_t *rcnt) {
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int p = order[t];
+        int c = 0;
+        for (int e = off[p]; e < off[p + 1]; ++e) {
+            const int k = ent[e].k;
+            if (!swept[k]) continue;
+            ++c;
+            atomicAdd(&rcnt[k], 1);
+        }
+        indeg[p] = c;
+    }
+}
+
+__global__ void k_dep_fill(int nsw, const int32_t *order, const int32_t *off, const SweepEntry *ent,
+                           const uint8_t *swept, const int32_t *roff, int32_t *rcur, int32_t *rlist) {
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int p = order[t];
+        for (int e = off[p]; e < off[p + 1]; ++e) {
+            const int k = ent[e].k;
+            if (swept[k]) rlist[roff[k] + atomicAdd(&rcur[k], 1)] = p;
+        }
+    }
+}
+
+__global__ void k_level_keys(int nsw, const int32_t *order, const int32_t *level, uint32_t *key, int32_t *hist,
+                             int *cycle) {
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int lv = level[order[t]];
+        if (lv < 0) {
+            atomicExch(cycle, 1);
+            key[t] = 0;
+            continue;
+        }
+        key[t] = (uint32_t)lv;
+        atomicAdd(&hist[lv], 1);
+    }
+}
+
+// a point's dependencies of the deepest level, in entry order (count, fill)
+__global__ void k_cand(int nsw, const int32_t *order, const int32_t *off, const SweepEntry *ent,
+                       const uint8_t *swept, const int32_t *level, const int32_t *coff, int32_t *cnt_or_cand,
+                       bool fill) {
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int p = order[t];
+        int best = -1;
+        for (int e = off[p]; e < off[p + 1]; ++e)
+            if (swept[ent[e].k]) best = max(best, level[ent[e].k]);
+        int c = 0;
+        for (int e = off[p]; e < off[p + 1]; ++e) {
+            const int k = ent[e].k;
+            if (!swept[k] || level[k] != best) continue;
+            if (fill) cnt_or_cand[coff[p] + c] = k;
+            ++c;
+        }
+        if (!fill) cnt_or_cand[p] = c;
+    }
+}
+
+// where each term's producer increment comes from (chain bits of the
+// entries) and which points publish; terms[0..2] ring, same warp, cross warp
+__global__ void k_chain_mark(int nsw, const int32_t *lpts, const int32_t *off, SweepEntry *ent,
+                             const uint8_t *swept, const uint8_t *shared, const int32_t *owner, const int32_t *pos,
+                             uint8_t *publish, unsigned long long *terms) {
+    unsigned long long ring = 0, local = 0, cross = 0;
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int p = lpts[t];
+        const bool sh = shared[p] != 0;
+        for (int e = off[p]; e < off[p + 1]; ++e) {
+            SweepEntry &E = ent[e];
+            E.pad &= ~ENT_CHAIN_BITS;
+            if (E.pad & (ENT_COPY | ENT_OLD)) continue;
+            const int k = E.k;
+            if (!swept[k]) continue;
+            const bool same = owner[k] == owner[p];
+            if (!sh) continue;
+            if (same && pos[p] - pos[k] <= CHAIN_RING) {
+                E.pad |= ENT_RING | ((pos[k] % CHAIN_RING) << ENT_RING_SHIFT);
+                ++ring;
+            } else {
+                publish[k] = 1;
+                if (same) ++local;
+                else ++cross;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ring += __shfl_down_sync(0xffffffffu, ring, o);
+        local += __shfl_down_sync(0xffffffffu, local, o);
+        cross += __shfl_down_sync(0xffffffffu, cross, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (ring | local | cross)) {
+        atomicAdd(&terms[0], ring);
+        atomicAdd(&terms[1], local);
+        atomicAdd(&terms[2], cross);
+    }
+}
+
+__global__ void k_chain_items(int m, const int32_t *pts, const int32_t *off, const uint8_t *cnt, const int8_t *cls,
+                              const uint8_t *shared, const uint8_t *publish, const int32_t *g0_of, ChainItem *items) {
+    GRID_STRIDE(t, (size_t)m) {
+        const int p = pts[t];
+        ChainItem it;
+        it.p = p;
+        it.off = off[p];
+        it.cnt = 0;
+        for (int e = 0; e < NDIR; ++e) it.cnt |= (uint32_t)cnt[(size_t)p * NDIR + e] << (5 * e);
+        it.info = (cls[p] == CLS_WALL ? CI_WALL : 0u) | (shared[p] ? CI_SHARED : 0u) |
+                  (publish[p] ? CI_PUBLISH : 0u) | (cls[p] == CLS_SUPERSONIC ? CI_COPY : 0u) |
+                  (cls[p] == CLS_OUTER ? CI_OUTER : 0u);
+        if (g0_of[p] >= 0) it.info |= CI_G0 | ((uint32_t)g0_of[p] << CI_G0_SHIFT);
+        items[t] = it;
+    }
+}
+
+__global__ void k_positions(int warps, const int32_t *ptr, const int32_t *pts, int32_t *pos) {
+    GRID_STRIDE(t, (size_t)warps) {
+        for (int i = ptr[t]; i < ptr[t + 1]; ++i) pos[pts[i]] = i - ptr[t];
+    }
+}
+
+// consumers in the shared frame and the phase-A (k_g0) candidates, by
+// logical index
+__global__ void k_shared_g0(int n, const int32_t *perm, const uint8_t *swept, const int8_t *scls, int shared_frame,
+                            uint8_t *shared, int *g0_flag) {
+    GRID_STRIDE(t, (size_t)n) {
+        const int p = map_id(perm, (int)t);
+        const uint8_t sh = (swept[p] && scls[p] == CLS_INTERIOR && shared_frame) ? 1 : 0;
+        shared[p] = sh;
+        g0_flag[t] = (swept[p] && !sh && scls[p] != CLS_SUPERSONIC) ? 1 : 0;
+    }
+}
+
+__global__ void k_g0_emit(int n, const int32_t *perm, const int *flag, const int *pos, int32_t *g0_pts,
+                          int32_t *g0_of) {
+    GRID_STRIDE(t, (size_t)n) {
+        if (!flag[t]) continue;
+        const int p = map_id(perm, (int)t);
+        g0_pts[pos[t]] = p;
+        if (g0_of) g0_of[p] = pos[t];
+    }
+}
+
+// the fused flux kernel's visiting order: keys as build_pre_order's, sorted
+// stably (ties in storage index order)
+__global__ void k_pre_keys(int n, const uint8_t *swept, const int32_t *level, uint32_t *key, int32_t *idx) {
+    GRID_STRIDE(t, (size_t)n) {
+        key[t] = swept[t] ? 2u * (uint32_t)level[t] + 1u : 0xffffffffu;
+        idx[t] = (int32_t)t;
+    }
+}
+
+__global__ void k_pre_min(int nsw, const int32_t *order, const int32_t *off, const SweepEntry *ent,
+                          const uint8_t *swept, const int32_t *level, uint32_t *key) {
+    GRID_STRIDE(t, (size_t)nsw) {
+        const int p = order[t];
+        for (int e = off[p]; e < off[p + 1]; ++e) {
+            if (ent[e].pad & (ENT_COPY | ENT_OLD)) continue;
+            const int k = ent[e].k;
+            if (!swept[k]) atomicMin(&key[k], 2u * (uint32_t)level[p]);
+        }
+    }
+}
+
+__global__ void k_iota(int n, int32_t *a) {
+    GRID_STRIDE(t, (size_t)n) a[t] = (int32_t)t;
+}
+
+}  // namespace
+
+#define DS_TMP(ptr, count)                                                              \
+    do {                                                                                \
+        cudaError_t e_ = tmp.alloc(&(ptr), (count));                                    \
+        if (e_ != cudaSuccess) {                                                        \
+            err = std::string("device set-up scratch: ") + cudaGetErrorString(e_);      \
+            return e_ == cudaErrorMemoryAllocation ? MFCFD_ERR_NOMEM : MFCFD_ERR_CUDA;   \
+        }                                                                               \
+    } while (0)
+
+#define DS_KEEP(ptr, count)                                                             \
+    do {                                                                                \
+        void *v_ = nullptr;                                                             \
+        const size_t c_ = (size_t)(count);                                              \
+        if (int rc_ = alloc(&v_, sizeof(*(ptr)) * (c_ > 0 ? c_ : 1))) {                 \
+            if (err.empty()) err = "device memory allocation failed";                  \
+            return rc_;                                                                 \
+        }                                                                               \
+        (ptr) = static_cast<std::remove_reference_t<decltype(ptr)>>(v_);                \
+    } while (0)
+
+bool device_setup_supported(const mfcfd_params &P, const Topology &T) {
+    return P.device >= 0 && P.sweep_variant == MFCFD_SWEEPS_ALIAS && P.power == 0.0 &&
+           P.precision != MFCFD_PRECISION_MIXED && T.ss_inlet_idx.empty() && T.ss_outlet_idx.empty() && T.n > 0 &&
+           (size_t)T.n * MAX_CONN < 0x7fffffffull;
+}
+
+namespace {
+
+// stable sort of (key, value) pairs by key on the device
+int sort_pairs(const uint32_t *key_in, uint32_t *key_out, const int32_t *val_in, int32_t *val_out, int m,
+               cudaStream_t s, DevBufs &tmp, std::string &err) {
+    if (m <= 0) return MFCFD_OK;
+    size_t bytes = 0;
+    PREP_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key_in, key_out, val_in, val_out, m, 0, 32, s));
+    uint8_t *scratch = nullptr;
+    DS_TMP(scratch, bytes);
+    PREP_CK(cub::DeviceRadixSort::SortPairs(scratch, bytes, key_in, key_out, val_in, val_out, m, 0, 32, s));
+    return MFCFD_OK;
+}
+
+template <typename V>
+int to_host(std::vector<V> &dst, const V *src, size_t count, cudaStream_t s, std::string &err) {
+    dst.resize(count);
+    if (count) PREP_CK(cudaMemcpyAsync(dst.data(), src, sizeof(V) * count, cudaMemcpyDeviceToHost, s));
+    PREP_CK(cudaStreamSynchronize(s));
+    return MFCFD_OK;
+}
+
+__global__ void k_g0_of(int m, const int32_t *g0_pts, int32_t *g0_of) {
+    GRID_STRIDE(t, (size_t)m) g0_of[g0_pts[t]] = (int32_t)t;
+}
+
+}  // namespace
+
+int device_setup(int device, const mfcfd_params &P, const Topology &T, const double *x, const double *y,
+                 const double *z, const double *tan1, const double *tan2, const double *nor, const int32_t *nbhs,
+                 const int32_t *conn, const std::vector<double> &eps2, cudaStream_t s, const DevAlloc &alloc,
+                 DevCloud &d, DevTopology &dt, std::string &err) {
+    const int n = T.n, cap = T.cap;
+    const size_t n3 = 3 * (size_t)n;
+    const bool chains = P.sweep_mode == MFCFD_SWEEP_CHAINS;
+    DevBufs tmp;
+    // ---- the cloud, in the reference's order, and the permutation
+    double *Lx, *Ly, *Lz, *Lt1, *Lt2, *Ln;
+    int32_t *Lnb, *Lconn, *perm = nullptr, *inv = nullptr;
+    int8_t *Lcls;
+    DS_TMP(Lx, n); DS_TMP(Ly, n); DS_TMP(Lz, n);
+    DS_TMP(Lt1, n3); DS_TMP(Lt2, n3); DS_TMP(Ln, n3);
+    DS_TMP(Lnb, n); DS_TMP(Lconn, (size_t)n * MAX_CONN); DS_TMP(Lcls, n);
+    PREP_CK(cudaMemcpyAsync(Lx, x, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Ly, y, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Lz, z, 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Lt1, tan1, 8 * n3, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Lt2, tan2, 8 * n3, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Ln, nor, 8 * n3, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Lnb, nbhs, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Lconn, conn, 4 * (size_t)n * MAX_CONN, cudaMemcpyHostToDevice, s));
+    PREP_CK(cudaMemcpyAsync(Lcls, T.cls.data(), (size_t)n, cudaMemcpyHostToDevice, s));
+    if (!T.perm.empty()) {
+        DS_TMP(perm, n); DS_TMP(inv, n);
+        PREP_CK(cudaMemcpyAsync(perm, T.perm.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+        PREP_CK(cudaMemcpyAsync(inv, T.inv.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+    }
+    const int g = grid_for(device, (size_t)n);
+    int *d_sums, *d_total, *flag, *fpos;
+    DS_TMP(d_sums, ((size_t)n + 1 + 1023) / 1024 + 1); DS_TMP(d_total, 1);
+    DS_TMP(flag, (size_t)n + 1); DS_TMP(fpos, (size_t)n + 1);
+    auto scan = [&](const int *in, int *out, int len, int *total) -> int {
+        if (int rc = exclusive_scan(in, out, len, d_sums, d_total, s, err)) return rc;
+        int v = 0;
+        PREP_CK(cudaMemcpyAsync(&v, d_total, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PREP_CK(cudaStreamSynchronize(s));
+        *total = v;
+        return MFCFD_OK;
+    };
+
+    // ---- storage-order cloud
+    double *sx, *sy, *sz, *frame;
+    int8_t *scls;
+    int32_t *snb, *sconn;
+    DS_KEEP(sx, n); DS_KEEP(sy, n); DS_KEEP(sz, n); DS_KEEP(frame, 9 * (size_t)n);
+    DS_KEEP(scls, n); DS_KEEP(snb, n); DS_KEEP(sconn, (size_t)n * MAX_CONN);
+    k_stage_cloud<<<g, PREP_THREADS, 0, s>>>(n, perm, Lx, Ly, Lz, Lt1, Lt2, Ln, Lcls, Lnb, Lconn, sx, sy, sz, frame,
+                                             scls, snb, sconn);
+    PREP_CK(cudaGetLastError());
+    d.x = sx; d.y = sy; d.z = sz; d.frame = frame; d.cls = scls; d.nbhs = snb; d.conn = sconn;
+
+    // ---- split stencils (generate_connectivity.f90:38-246), the reference's storage
+    SplitPtrs sp;
+    const size_t flat = (size_t)n * cap + 64;
+    for (int k = 0; k < NDIR; ++k) {
+        DS_KEEP(dt.split[k], flat);
+        PREP_CK(cudaMemsetAsync(dt.split[k], 0, 4 * flat, s));
+        sp.p[k] = dt.split[k];
+    }
+    DS_KEEP(dt.split_cnt, (size_t)NDIR * n);
+    int *over;
+    DS_TMP(over, 1);
+    PREP_CK(cudaMemsetAsync(over, 0, sizeof(int), s));
+    k_split_own<<<g, PREP_THREADS, 0, s>>>(n, cap, Lcls, Lx, Ly, Lz, Lt1, Lt2, Ln, Lnb, Lconn, sp, dt.split_cnt, over);
+    PREP_CK(cudaGetLastError());
+    int h_over = 0;
+    PREP_CK(cudaMemcpyAsync(&h_over, over, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PREP_CK(cudaStreamSynchronize(s));
+    dt.split_overflows = 0;
+    if (h_over) {
+        // spilled entries land in the next points' storage in the
+        // reference's visiting order: resolved on the host from the counts
+        std::vector<int32_t> hc;
+        if (int rc = to_host(hc, dt.split_cnt, (size_t)NDIR * n, s, err)) return rc;
+        const int32_t *cnt[NDIR];
+        for (int k = 0; k < NDIR; ++k) {
+            cnt[k] = hc.data() + (size_t)k * n;
+            for (int i = 0; i < n; ++i) dt.split_overflows += std::max(0, cnt[k][i] - cap);
+        }
+        std::vector<SpillWrite> w;
+        split_spill_writes(T, x, y, z, tan1, tan2, nor, nbhs, conn, cnt, w);
+        const int m = (int)w.size();
+        if (m > 0) {
+            std::vector<int> wd(m);
+            std::vector<long long> wat(m);
+            std::vector<int32_t> wv(m);
+            for (int j = 0; j < m; ++j) { wd[j] = w[j].d; wat[j] = (long long)w[j].at; wv[j] = w[j].value; }
+            int *dd; long long *dat; int32_t *dv;
+            DS_TMP(dd, m); DS_TMP(dat, m); DS_TMP(dv, m);
+            PREP_CK(cudaMemcpyAsync(dd, wd.data(), sizeof(int) * m, cudaMemcpyHostToDevice, s));
+            PREP_CK(cudaMemcpyAsync(dat, wat.data(), sizeof(long long) * m, cudaMemcpyHostToDevice, s));
+            PREP_CK(cudaMemcpyAsync(dv, wv.data(), sizeof(int32_t) * m, cudaMemcpyHostToDevice, s));
+            k_spill_apply<<<grid_for(device, m), PREP_THREADS, 0, s>>>(m, dd, dat, dv, sp);
+            PREP_CK(cudaGetLastError());
+            PREP_CK(cudaStreamSynchronize(s));   // the host vectors go out of scope
+        }
+    }
+
+    // ---- alias breadth-first search (implicit_aliasing.f90:21-42)
+    DS_KEEP(dt.alias, n);
+    DS_KEEP(dt.pwa, n);
+    if (int rc = alias_search(device, n, Lnb, Lconn, dt.alias, dt.pwa, s, err)) return rc;
+    int32_t *salias;
+    DS_TMP(salias, n);
+    k_alias_storage<<<g, PREP_THREADS, 0, s>>>(n, perm, dt.alias, salias);
+
+    // ---- effective lists and neighbour slots
+    int32_t *slot_nbr;
+    uint8_t *nslot, *slot_mask, *list_cnt, *list_ent, *code;
+    DS_KEEP(slot_nbr, (size_t)n * MAX_SLOTS); DS_KEEP(nslot, n); DS_KEEP(slot_mask, (size_t)n * MAX_SLOTS);
+    DS_KEEP(list_cnt, (size_t)n * NDIR); DS_KEEP(list_ent, (size_t)n * NDIR * LIST_STRIDE);
+    DS_TMP(code, n);
+    int *bad;
+    DS_TMP(bad, 1);
+    PREP_CK(cudaMemsetAsync(bad, 0x7f, sizeof(int), s));
+    k_slots<<<g, PREP_THREADS, 0, s>>>(n, cap, perm, inv, Lcls, Lnb, Lconn, sp, dt.split_cnt, slot_nbr, nslot,
+                                       slot_mask, list_cnt, list_ent, code, bad);
+    PREP_CK(cudaGetLastError());
+    int h_bad = 0;
+    PREP_CK(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PREP_CK(cudaStreamSynchronize(s));
+    if (h_bad != 0x7f7f7f7f) {
+        uint8_t c = 0;
+        PREP_CK(cudaMemcpyAsync(&c, code + h_bad, 1, cudaMemcpyDeviceToHost, s));
+        PREP_CK(cudaStreamSynchronize(s));
+        const std::string at = std::to_string(h_bad + 1);
+        if (c == SLOT_ZERO) err = "split list of point " + at + " names point 0";
+        else if (c == SLOT_LONG) err = "split list longer than 27 at point " + at;
+        else err = "more than 32 distinct stencil neighbours at point " + at;
+        return MFCFD_ERR_STENCIL;
+    }
+    d.slot_nbr = slot_nbr; d.nslot = nslot; d.slot_mask = slot_mask; d.list_cnt = list_cnt; d.list_ent = list_ent;
+    d.sweep_slot_mask = slot_mask;   // the alias driver's sweep terms use the same lists
+
+    // ---- geometry per (point, list) and the limiter's epsilon
+    double *geo, *e2;
+    DS_KEEP(geo, (size_t)n * GEO_STRIDE);
+    k_geo<<<g, PREP_THREADS, 0, s>>>(n, sx, sy, sz, frame, list_cnt, list_ent, slot_nbr, geo);
+    PREP_CK(cudaGetLastError());
+    DS_KEEP(e2, n);
+    PREP_CK(cudaMemcpyAsync(e2, eps2.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+    d.geo = geo; d.eps2 = e2; d.wq = nullptr; d.wf = nullptr; d.outer_delt = nullptr;
+
+    // ---- sweep orders (implicit_forward_and_reverse_sweeps.f90:26-84)
+    uint8_t *swept;
+    DS_KEEP(swept, n);
+    PREP_CK(cudaMemsetAsync(swept, 0, (size_t)n, s));
+    int nsw = 0;
+    int32_t *order[2];
+    DS_TMP(order[0], n); DS_TMP(order[1], n);
+    k_swept_flags<<<g, PREP_THREADS, 0, s>>>(n, dt.pwa, Lcls, flag);
+    if (int rc = scan(flag, fpos, n, &nsw)) return rc;
+    k_swept_emit<<<g, PREP_THREADS, 0, s>>>(n, dt.pwa, perm, flag, fpos, order[0], swept);
+    if (nsw > 0) k_reverse<<<grid_for(device, nsw), PREP_THREADS, 0, s>>>(nsw, order[0], order[1]);
+    PREP_CK(cudaGetLastError());
+    d.swept = swept;
+    d.n_swept = nsw;
+
+    // ---- per direction: terms, levels, level-major points
+    const int gs = grid_for(device, (size_t)std::max(nsw, 1));
+    dt.max_width = 0;
+    uint8_t *cnt_dir[2];
+    int32_t *off_dir[2], *lpts_dir[2], *lptr_dir[2];
+    uint32_t *need_dir[2], *old_dir[2];
+    SweepEntry *ent_dir[2];
+    int nlev[2] = {0, 0};
+    for (int dir = 0; dir < 2; ++dir) {
+        const bool fwd = dir == 0;
+        DS_KEEP(cnt_dir[dir], (size_t)n * NDIR);
+        PREP_CK(cudaMemsetAsync(cnt_dir[dir], 0, (size_t)n * NDIR, s));
+        DS_KEEP(off_dir[dir], (size_t)n + 1);
+        PREP_CK(cudaMemsetAsync(flag, 0, 4 * ((size_t)n + 1), s));
+        if (nsw > 0)
+            k_ent_count<<<gs, PREP_THREADS, 0, s>>>(nsw, fwd, order[dir], salias, list_cnt, list_ent, slot_nbr,
+                                                    cnt_dir[dir], flag);
+        int ne = 0;
+        if (int rc = scan(flag, off_dir[dir], n + 1, &ne)) return rc;
+        DS_KEEP(ent_dir[dir], ne);
+        DS_KEEP(need_dir[dir], n);
+        DS_KEEP(old_dir[dir], n);
+        PREP_CK(cudaMemsetAsync(need_dir[dir], 0, 4 * (size_t)n, s));
+        PREP_CK(cudaMemsetAsync(old_dir[dir], 0, 4 * (size_t)n, s));
+        int *too_many;
+        DS_TMP(too_many, 1);
+        PREP_CK(cudaMemsetAsync(too_many, 0, sizeof(int), s));
+        if (nsw > 0)
+            k_ent_fill<<<gs, PREP_THREADS, 0, s>>>(nsw, fwd, order[dir], salias, sx, sy, sz, frame, list_cnt,
+                                                   list_ent, slot_nbr, off_dir[dir], ent_dir[dir], need_dir[dir],
+                                                   too_many);
+        PREP_CK(cudaGetLastError());
+        int h_many = 0;
+        PREP_CK(cudaMemcpyAsync(&h_many, too_many, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PREP_CK(cudaStreamSynchronize(s));
+        if (h_many) {
+            err = "a point reads more than " + std::to_string(SWEEP_MAX_ENTRIES) + " sweep terms";
+            return MFCFD_ERR_STENCIL;
+        }
+
+        // levels: the longest path over swept producers (Kahn's layering)
+        DS_KEEP(dt.level[dir], n);
+        PREP_CK(cudaMemsetAsync(dt.level[dir], 0xff, 4 * (size_t)n, s));
+        DS_KEEP(lpts_dir[dir], nsw);
+        std::vector<int32_t> hist;
+        if (nsw > 0) {
+            int32_t *indeg, *rcnt, *roff, *rcur, *rlist, *fa, *fb, *count, *hcnt;
+            uint32_t *key, *key_sorted;
+            int *cycle;
+            DS_TMP(indeg, n); DS_TMP(rcnt, (size_t)n + 1); DS_TMP(roff, (size_t)n + 1); DS_TMP(rcur, n);
+            DS_TMP(rlist, ne); DS_TMP(fa, nsw); DS_TMP(fb, nsw); DS_TMP(count, (size_t)nsw + 2);
+            DS_TMP(hcnt, (size_t)nsw + 1); DS_TMP(key, nsw); DS_TMP(key_sorted, nsw); DS_TMP(cycle, 1);
+            PREP_CK(cudaMemsetAsync(rcnt, 0, 4 * ((size_t)n + 1), s));
+            PREP_CK(cudaMemsetAsync(rcur, 0, 4 * (size_t)n, s));
+            PREP_CK(cudaMemsetAsync(count, 0, 4 * ((size_t)nsw + 2), s));
+            PREP_CK(cudaMemsetAsync(hcnt, 0, 4 * ((size_t)nsw + 1), s));
+            PREP_CK(cudaMemsetAsync(cycle, 0, sizeof(int), s));
+            k_dep_count<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], off_dir[dir], ent_dir[dir], swept, indeg, rcnt);
+            int ndep = 0;
+            if (int rc = scan(rcnt, roff, n + 1, &ndep)) return rc;
+            k_dep_fill<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], off_dir[dir], ent_dir[dir], swept, roff, rcur,
+                                                   rlist);
+            k_lv_roots<<<gs, PREP_THREADS, 0, s>>>(order[dir], nsw, indeg, dt.level[dir], fa, count);
+            PREP_CK(cudaGetLastError());
+            int L = 0;
+            int32_t *front = fa, *next = fb;
+            constexpr int BATCH = 256;
+            while (L < nsw) {
+                const int stop = std::min(nsw, L + BATCH);
+                for (; L < stop; ++L) {
+                    k_lv_step<<<64, PREP_THREADS, 0, s>>>(L, front, count, roff, rlist, indeg, dt.level[dir], next);
+                    std::swap(front, next);
+                }
+                PREP_CK(cudaGetLastError());
+                int last = 0;
+                PREP_CK(cudaMemcpyAsync(&last, count + L, sizeof(int), cudaMemcpyDeviceToHost, s));
+                PREP_CK(cudaStreamSynchronize(s));
+                if (last == 0) break;
+            }
+            k_level_keys<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], dt.level[dir], key, hcnt, cycle);
+            PREP_CK(cudaGetLastError());
+            int h_cycle = 0;
+            PREP_CK(cudaMemcpyAsync(&h_cycle, cycle, sizeof(int), cudaMemcpyDeviceToHost, s));
+            PREP_CK(cudaStreamSynchronize(s));
+            if (h_cycle) {
+                err = "sweep dependencies contain a cycle";
+                return MFCFD_ERR_STENCIL;
+            }
+            // points of each level in the sweep's order
+            if (int rc = sort_pairs(key, key_sorted, order[dir], lpts_dir[dir], nsw, s, tmp, err)) return rc;
+            if (int rc = to_host(hist, hcnt, (size_t)nsw + 1, s, err)) return rc;
+        }
+        int nl = 0;
+        for (int l = 0; l < (int)hist.size(); ++l)
+            if (hist[l] > 0) nl = l + 1;
+        std::vector<int32_t> &lptr = dt.lvl_ptr[dir];
+        lptr.assign(nl + 1, 0);
+        for (int l = 0; l < nl; ++l) {
+            lptr[l + 1] = lptr[l] + hist[l];
+            dt.max_width = std::max(dt.max_width, hist[l]);
+        }
+        DS_KEEP(lptr_dir[dir], nl + 1);
+        PREP_CK(cudaMemcpyAsync(lptr_dir[dir], lptr.data(), 4 * ((size_t)nl + 1), cudaMemcpyHostToDevice, s));
+        PREP_CK(cudaStreamSynchronize(s));
+        nlev[dir] = nl;
+
+        // the chain schedule's inputs on the host: levels, level-major
+        // points, each point's deepest dependencies in entry order
+        if (chains) {
+            if (int rc = to_host(dt.h_level[dir], dt.level[dir], (size_t)n, s, err)) return rc;
+            if (int rc = to_host(dt.h_lpts[dir], lpts_dir[dir], (size_t)nsw, s, err)) return rc;
+            int32_t *ccnt, *coff, *cand;
+            DS_TMP(ccnt, (size_t)n + 1); DS_TMP(coff, (size_t)n + 1);
+            PREP_CK(cudaMemsetAsync(ccnt, 0, 4 * ((size_t)n + 1), s));
+            if (nsw > 0)
+                k_cand<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], off_dir[dir], ent_dir[dir], swept, dt.level[dir],
+                                                   nullptr, ccnt, false);
+            int nc = 0;
+            if (int rc = scan(ccnt, coff, n + 1, &nc)) return rc;
+            DS_TMP(cand, nc);
+            if (nsw > 0)
+                k_cand<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], off_dir[dir], ent_dir[dir], swept, dt.level[dir],
+                                                   coff, cand, true);
+            PREP_CK(cudaGetLastError());
+            if (int rc = to_host(dt.h_coff[dir], coff, (size_t)n + 1, s, err)) return rc;
+            if (int rc = to_host(dt.h_cand[dir], cand, (size_t)nc, s, err)) return rc;
+        }
+    }
+    d.fwd_cnt = cnt_dir[0]; d.bwd_cnt = cnt_dir[1];
+    d.fwd_off = off_dir[0]; d.bwd_off = off_dir[1];
+    d.fwd_ent = ent_dir[0]; d.bwd_ent = ent_dir[1];
+    d.fwd_need = need_dir[0]; d.bwd_need = need_dir[1];
+    d.fwd_old = old_dir[0]; d.bwd_old = old_dir[1];
+    d.fwd_lvl_pts = lpts_dir[0]; d.bwd_lvl_pts = lpts_dir[1];
+    d.fwd_lvl_ptr = lptr_dir[0]; d.bwd_lvl_ptr = lptr_dir[1];
+    d.n_fwd_levels = nlev[0];
+    d.n_bwd_levels = nlev[1];
+    d.max_width = dt.max_width;
+
+    // ---- the shared interior frame (every interior point's frame bit-equal
+    // to the first's), its consumers, and the phase-A (k_g0) points
+    d.shared_frame = 0;
+    if (!T.interior_idx.empty()) {
+        const int i0 = T.interior_idx[0];
+        bool same = true;
+        for (int i : T.interior_idx) {
+            if (std::memcmp(tan1 + 3 * (size_t)i, tan1 + 3 * (size_t)i0, 24) ||
+                std::memcmp(tan2 + 3 * (size_t)i, tan2 + 3 * (size_t)i0, 24) ||
+                std::memcmp(nor + 3 * (size_t)i, nor + 3 * (size_t)i0, 24)) {
+                same = false;
+                break;
+            }
+        }
+        if (same) {
+            d.shared_frame = 1;
+            for (int r = 0; r < 3; ++r) {
+                d.frame0[r] = tan1[3 * (size_t)i0 + r];
+                d.frame0[3 + r] = tan2[3 * (size_t)i0 + r];
+                d.frame0[6 + r] = nor[3 * (size_t)i0 + r];
+            }
+        }
+    }
+    if (!d.shared_frame) std::memset(d.frame0, 0, sizeof d.frame0);
+    uint8_t *shared;
+    DS_KEEP(shared, n);
+    k_shared_g0<<<g, PREP_THREADS, 0, s>>>(n, perm, swept, scls, d.shared_frame, shared, flag);
+    int ng0 = 0;
+    if (int rc = scan(flag, fpos, n, &ng0)) return rc;
+    d.consumer_shared = shared;
+    dt.g0_pts.clear();
+    d.g0_pts = nullptr;
+    d.n_g0 = 0;
+    if (ng0 > std::max(4096, n / 8) || ng0 >= (1 << 24)) ng0 = 0;
+    if (ng0 > 0) {
+        int32_t *g0p;
+        DS_TMP(g0p, ng0);
+        k_g0_emit<<<g, PREP_THREADS, 0, s>>>(n, perm, flag, fpos, g0p, nullptr);
+        PREP_CK(cudaGetLastError());
+        if (int rc = to_host(dt.g0_pts, g0p, (size_t)ng0, s, err)) return rc;
+        if (chains) {
+            int32_t *kept;
+            DS_KEEP(kept, ng0);
+            PREP_CK(cudaMemcpyAsync(kept, g0p, 4 * (size_t)ng0, cudaMemcpyDeviceToDevice, s));
+            d.g0_pts = kept;
+            d.n_g0 = ng0;
+        }
+    }
+
+    // ---- the residual's order: wall, then interior points, each in the
+    // reference's index order (state_update_implicit.f90:28-61)
+    {
+        std::vector<int32_t> ro;
+        ro.reserve(T.wall_idx.size() + T.interior_idx.size());
+        for (int i : T.wall_idx) ro.push_back(T.perm.empty() ? i : T.perm[i]);
+        for (int i : T.interior_idx) ro.push_back(T.perm.empty() ? i : T.perm[i]);
+        int32_t *r;
+        DS_KEEP(r, ro.size());
+        if (!ro.empty()) PREP_CK(cudaMemcpyAsync(r, ro.data(), 4 * ro.size(), cudaMemcpyHostToDevice, s));
+        PREP_CK(cudaStreamSynchronize(s));
+        d.res_order = r;
+        d.n_res = (int)ro.size();
+        d.n_wall = (int)T.wall_idx.size();
+    }
+
+    // ---- the fused flux kernel's visiting order (build_pre_order)
+    d.pre_order = nullptr;
+    if (chains) {
+        uint32_t *key, *key_sorted;
+        int32_t *idx, *pre;
+        DS_TMP(key, n); DS_TMP(key_sorted, n); DS_TMP(idx, n);
+        DS_KEEP(pre, n);
+        k_pre_keys<<<g, PREP_THREADS, 0, s>>>(n, swept, dt.level[0], key, idx);
+        if (nsw > 0)
+            k_pre_min<<<gs, PREP_THREADS, 0, s>>>(nsw, order[0], off_dir[0], ent_dir[0], swept, dt.level[0], key);
+        PREP_CK(cudaGetLastError());
+        if (int rc = sort_pairs(key, key_sorted, idx, pre, n, s, tmp, err)) return rc;
+        d.pre_order = pre;
+    }
+    PREP_CK(cudaStreamSynchronize(s));
+    return MFCFD_OK;
+}
+
+int device_chain_schedule(int device, DevTopology &dt, DevCloud &d, int warps, cudaStream_t s,
+                          const DevAlloc &alloc, int64_t terms[3], std::string &err) {
+    const int n = d.n;
+    DevBufs tmp;
+    terms[0] = terms[1] = terms[2] = 0;
+    int32_t *g0_of, *pos;
+    uint8_t *publish;
+    unsigned long long *dterms;
+    DS_TMP(g0_of, n); DS_TMP(pos, n); DS_TMP(publish, n); DS_TMP(dterms, 3);
+    PREP_CK(cudaMemsetAsync(g0_of, 0xff, 4 * (size_t)n, s));
+    if (d.n_g0 > 0) k_g0_of<<<grid_for(device, d.n_g0), PREP_THREADS, 0, s>>>(d.n_g0, d.g0_pts, g0_of);
+    for (int dir = 0; dir < 2; ++dir) {
+        const int nsw = (int)dt.h_lpts[dir].size();
+        std::vector<int32_t> owner;
+        std::vector<std::vector<int32_t>> lists;
+        chain_assign(dt.h_lpts[dir].data(), nsw, dt.h_level[dir].data(), dt.h_coff[dir].data(),
+                     dt.h_cand[dir].data(), n, warps, owner, lists);
+        std::vector<int32_t> ptr(warps + 1, 0), pts;
+        pts.reserve(nsw);
+        for (int w = 0; w < warps; ++w) {
+            ptr[w] = (int32_t)pts.size();
+            pts.insert(pts.end(), lists[w].begin(), lists[w].end());
+        }
+        ptr[warps] = (int32_t)pts.size();
+        int32_t *dptr, *dpts, *down;
+        ChainItem *items;
+        DS_KEEP(dptr, warps + 1); DS_KEEP(dpts, pts.size()); DS_KEEP(down, n); DS_KEEP(items, pts.size());
+        PREP_CK(cudaMemcpyAsync(dptr, ptr.data(), 4 * ptr.size(), cudaMemcpyHostToDevice, s));
+        if (!pts.empty()) PREP_CK(cudaMemcpyAsync(dpts, pts.data(), 4 * pts.size(), cudaMemcpyHostToDevice, s));
+        PREP_CK(cudaMemcpyAsync(down, owner.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
+        PREP_CK(cudaMemsetAsync(pos, 0xff, 4 * (size_t)n, s));
+        PREP_CK(cudaMemsetAsync(publish, 0, (size_t)n, s));
+        PREP_CK(cudaMemsetAsync(dterms, 0, 3 * sizeof(unsigned long long), s));
+        k_positions<<<grid_for(device, warps), PREP_THREADS, 0, s>>>(warps, dptr, dpts, pos);
+        const int32_t *lpts = dir == 0 ? d.fwd_lvl_pts : d.bwd_lvl_pts;
+        const int32_t *off = dir == 0 ? d.fwd_off : d.bwd_off;
+        SweepEntry *ent = const_cast<SweepEntry *>(dir == 0 ? d.fwd_ent : d.bwd_ent);
+        const uint8_t *cnt = dir == 0 ? d.fwd_cnt : d.bwd_cnt;
+        const int gs = grid_for(device, (size_t)std::max(nsw, 1));
+        if (nsw > 0) {
+            k_chain_mark<<<gs, PREP_THREADS, 0, s>>>(nsw, lpts, off, ent, d.swept, d.consumer_shared, down, pos,
+                                                     publish, dterms);
+            k_chain_items<<<gs, PREP_THREADS, 0, s>>>((int)pts.size(), dpts, off, cnt, d.cls, d.consumer_shared,
+                                                      publish, g0_of, items);
+        }
+        PREP_CK(cudaGetLastError());
+        unsigned long long h[3] = {0, 0, 0};
+        PREP_CK(cudaMemcpyAsync(h, dterms, sizeof h, cudaMemcpyDeviceToHost, s));
+        PREP_CK(cudaStreamSynchronize(s));
+        for (int k = 0; k < 3; ++k) terms[k] += (int64_t)h[k];
+        d.ch_ptr[dir] = dptr;
+        d.ch_pts[dir] = dpts;
+        d.ch_own[dir] = down;
+        d.ch_items[dir] = items;
+    }
+    d.ch_warps = warps;
+    return MFCFD_OK;
+}
+
+#undef DS_TMP
+#undef DS_KEEP
+#undef GRID_STRIDE
 
 }  // namespace mfcfd

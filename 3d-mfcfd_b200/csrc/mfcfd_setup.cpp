@@ -247,6 +247,15 @@ void split_spill_writes(const Topology &T, const double *x, const double *y, con
         }
 }
 
+void limiter_eps2(const mfcfd_params &P, int n, const double *min_dist, const int32_t *perm, std::vector<double> &eps2) {
+    eps2.resize(n);
+    for (int i = 0; i < n; ++i) {
+        double e = P.vl_const * min_dist[i];
+        e = std::pow(e, 3.0);
+        eps2[perm ? perm[i] : i] = e * e;
+    }
+}
+
 int build_topology(const mfcfd_params &P, int n, const int32_t *status, const double *x,
                    const double *y, const double *z, const double *tan1, const double *tan2,
                    const double *nor, const int32_t *nbhs, const int32_t *conn,
@@ -458,12 +467,7 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
     }
 
     // limiter epsilon: (VL_CONST*min_dist)**3 squared (limiters.f90:251-253)
-    T.eps2.resize(n);
-    for (int i = 0; i < n; ++i) {
-        double e = P.vl_const * min_dist[i];
-        e = std::pow(e, 3.0);
-        T.eps2[i] = e * e;
-    }
+    limiter_eps2(P, n, min_dist, nullptr, T.eps2);
 
     // ---- sweep schedules (implicit_forward_and_reverse_sweeps.f90:26-84, or
     // implicit_forward_and_reverse_sweeps_backup.f90:26-141)

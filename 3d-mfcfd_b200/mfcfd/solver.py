@@ -185,6 +185,13 @@ class Solver:
         self._check(_lib.lib().mfcfd_get_levels(self.h, int(direction), ptr(lv)))
         return lv
 
+    def digest(self, name: str):
+        """(FNV-1a digest, bytes) of one device topology array
+        (mfcfd_debug_digest); bytes -1 when the array is not allocated."""
+        dg, nb = ctypes.c_uint64(), ctypes.c_int64()
+        self._check(_lib.lib().mfcfd_debug_digest(self.h, name.encode(), ctypes.byref(dg), ctypes.byref(nb)))
+        return int(dg.value), int(nb.value)
+
     def info(self) -> dict:
         inf = _lib.Info()
         self._check(_lib.lib().mfcfd_get_info(self.h, ctypes.byref(inf)))

@@ -101,8 +101,14 @@ typedef struct mfcfd_params {
     int32_t sweep_variant;    /* MFCFD_SWEEPS_ALIAS (default) or MFCFD_SWEEPS_BACKUP */
     int32_t chain_warps;      /* CHAINS: warps of the schedule; 0 picks about twice the
                                  widest level (fewer warps leave SMs to other clouds) */
-    int32_t gpu_setup;        /* 1: split stencils, alias search and sweep levels of the
-                                 set-up run on params->device (same results as the host) */
+    int32_t gpu_setup;        /* 1: the set-up runs on params->device with the host's
+                                 results.  mfcfd_create computes every topology array on
+                                 the device (the host classifies and orders the points
+                                 and assigns the chain warps) for the alias sweep driver,
+                                 power 0, FP64 or MIXED_DC and no supersonic points;
+                                 otherwise, and in mfcfd_prepare, the split stencils, alias
+                                 search and sweep levels run on the device for the host's
+                                 set-up */
     int32_t graphs;           /* chunks of iterations captured once as CUDA graphs and
                                  replayed: 1 (default) in mfcfd_run_batch, 2 also in
                                  single-handle runs, 0 never (kernels one by one) */
@@ -280,6 +286,13 @@ int mfcfd_get_alias(mfcfd_handle *h, int32_t *alias, int32_t *point_with_alias);
 /* Level of every point in the forward (dir 0) or backward (dir 1) sweep
  * schedule; -1 for points the sweeps skip. */
 int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level);
+
+/* Diagnostics: a 64-bit FNV-1a digest of one device array of the handle's
+ * topology, by its DevCloud name ("geo", "fwd_ent", "ch_items0", ...), and its
+ * size in bytes (-1: not allocated).  Two handles of one cloud and
+ * parameters give equal digests whether their set-up ran on the host or on
+ * the device. */
+int mfcfd_debug_digest(mfcfd_handle *h, const char *name, uint64_t *digest, int64_t *bytes);
 
 int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info);
 
