@@ -754,13 +754,8 @@ int create_on_device(mfcfd_handle *h, const double *x, const double *y, const do
         if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
         if (P.chain_spread < 0 || P.chain_spread > 1) return fail(h, MFCFD_ERR_ARG, "chain_spread must be 0 or 1");
     }
-    if (P.storage_order == MFCFD_ORDER_MORTON && n > 1) {
-        morton_order(n, x, y, z, T.perm);
-        T.inv.assign(n, 0);
-        for (int i = 0; i < n; ++i) T.inv[T.perm[i]] = i;
-    }
     std::vector<double> eps2;
-    limiter_eps2(P, n, min_dist, T.perm.empty() ? nullptr : T.perm.data(), eps2);
+    limiter_eps2(P, n, min_dist, nullptr, eps2);
     if ((rc = create_streams(h))) return rc;
     init_devcloud(h, n);
     h->dev_setup = true;
@@ -1096,6 +1091,15 @@ int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level) {
         else
             for (int i = 0; i < T.n; ++i) level[i] = src[T.perm[i]];
         return MFCFD_OK;
+    });
+}
+
+int mfcfd_knn(int32_t device, int32_t n, const double *x, const double *y, const double *z, int32_t k,
+              int32_t *nbhs, int32_t *conn, double *min_dist) {
+    return host_guard(&g_io_err, [&]() -> int {
+        if (!x || !y || !z || !nbhs || !conn || !min_dist) return MFCFD_ERR_ARG;
+        g_io_err.clear();
+        return knn_connectivity(device, n, x, y, z, k, nbhs, conn, min_dist, g_io_err);
     });
 }
 

@@ -211,10 +211,12 @@ struct DevTopology {
     int max_width = 0;
 };
 bool device_setup_supported(const mfcfd_params &P, const Topology &T);
-// T: classify_points' result with perm/inv set (empty: index order); eps2 in
-// storage order.  Fills d's topology pointers and counts and dt; every
-// allocation goes through `alloc` (owned by the caller, also on failure).
-int device_setup(int device, const mfcfd_params &P, const Topology &T, const double *x, const double *y,
+// T: classify_points' result; T.perm / T.inv receive the storage order
+// (morton_order's, computed on the device; empty for MFCFD_ORDER_INDEX);
+// eps2 in the reference's index order.  Fills d's topology pointers and
+// counts and dt; every allocation goes through `alloc` (owned by the
+// caller, also on failure).
+int device_setup(int device, const mfcfd_params &P, Topology &T, const double *x, const double *y,
                  const double *z, const double *tan1, const double *tan2, const double *nor, const int32_t *nbhs,
                  const int32_t *conn, const std::vector<double> &eps2, cudaStream_t s, const DevAlloc &alloc,
                  DevCloud &d, DevTopology &dt, std::string &err);
@@ -416,6 +418,11 @@ int io_write_primal_output(const std::string &dir, int32_t n, const int32_t *sta
                            const double *y, const double *z, const double *prim, const double *flux_res,
                            const double *dq);
 int io_write_residue(const char *path, int32_t t0, int32_t iters, const double *res_hist, int append);
+
+// k nearest neighbours (mfcfd_knn.cu): on `device` (>= 0) or the host's
+// threads, the same arrays either way.
+int knn_connectivity(int device, int n, const double *x, const double *y, const double *z, int k, int32_t *nbhs,
+                     int32_t *conn, double *min_dist, std::string &err);
 
 // Allocation-free residual (mfcfd_residual_noalloc); the current device must
 // be the handle's.

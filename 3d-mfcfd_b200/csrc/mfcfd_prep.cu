@@ -26,8 +26,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <type_traits>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mfcfd_internal.h"
@@ -808,6 +810,45 @@ __global__ void k_level_keys(int nsw, const int32_t *order, const int32_t *level
     }
 }
 
+// Kahn's layering in one block: the frontier of level L (count0[0] points
+// in front, from k_lv_roots) releases the dependents whose last producer it
+// holds into level L+1; a warp takes a frontier point and its lanes its
+// dependents.  The loop ends when a level releases nothing; it runs at most
+// nsw levels.
+__global__ void __launch_bounds__(1024) k_levels_block(int nsw, int32_t *front, int32_t *next, const int32_t *count0,
+                                                       const int32_t *roff, const int32_t *rlist, int32_t *indeg,
+                                                       int32_t *level) {
+    __shared__ int m, m_next;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    if (threadIdx.x == 0) {
+        m = count0[0];
+        m_next = 0;
+    }
+    __syncthreads();
+    for (int L = 0; L < nsw && m > 0; ++L) {
+        for (int f = warp; f < m; f += warps) {
+            const int p = front[f];
+            const int e1 = roff[p + 1];
+            for (int e = roff[p] + lane; e < e1; e += 32) {
+                const int q = rlist[e];
+                if (atomicSub(&indeg[q], 1) == 1) {
+                    level[q] = L + 1;
+                    next[atomicAdd(&m_next, 1)] = q;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            m = m_next;
+            m_next = 0;
+        }
+        int32_t *t = front;
+        front = next;
+        next = t;
+        __syncthreads();
+    }
+}
+
 // a point's dependencies of the deepest level, in entry order (count, fill)
 __global__ void k_cand(int nsw, const int32_t *order, const int32_t *off, const SweepEntry *ent,
                        const uint8_t *swept, const int32_t *level, const int32_t *coff, int32_t *cnt_or_cand,
@@ -933,10 +974,6 @@ __global__ void k_pre_min(int nsw, const int32_t *order, const int32_t *off, con
     }
 }
 
-__global__ void k_iota(int n, int32_t *a) {
-    GRID_STRIDE(t, (size_t)n) a[t] = (int32_t)t;
-}
-
 }  // namespace
 
 #define DS_TMP(ptr, count)                                                              \
@@ -968,15 +1005,57 @@ bool device_setup_supported(const mfcfd_params &P, const Topology &T) {
 namespace {
 
 // stable sort of (key, value) pairs by key on the device
-int sort_pairs(const uint32_t *key_in, uint32_t *key_out, const int32_t *val_in, int32_t *val_out, int m,
-               cudaStream_t s, DevBufs &tmp, std::string &err) {
+template <typename K>
+int sort_pairs(const K *key_in, K *key_out, const int32_t *val_in, int32_t *val_out, int m, cudaStream_t s,
+               DevBufs &tmp, std::string &err) {
     if (m <= 0) return MFCFD_OK;
     size_t bytes = 0;
-    PREP_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key_in, key_out, val_in, val_out, m, 0, 32, s));
+    const int bits = 8 * (int)sizeof(K);
+    PREP_CK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key_in, key_out, val_in, val_out, m, 0, bits, s));
     uint8_t *scratch = nullptr;
     DS_TMP(scratch, bytes);
-    PREP_CK(cub::DeviceRadixSort::SortPairs(scratch, bytes, key_in, key_out, val_in, val_out, m, 0, 32, s));
+    PREP_CK(cub::DeviceRadixSort::SortPairs(scratch, bytes, key_in, key_out, val_in, val_out, m, 0, bits, s));
     return MFCFD_OK;
+}
+
+// the bits of v (21 of them) spread to every third bit, as morton_order's
+__device__ __forceinline__ uint64_t dev_spread3(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+struct Box {
+    double lo[3], scale[3];
+};
+
+// morton_order's keys (the same quantisation), with the point index as value
+__global__ void k_morton_keys(int n, const double *x, const double *y, const double *z, Box b, uint64_t *key,
+                              int32_t *idx) {
+    GRID_STRIDE(t, (size_t)n) {
+        const double v[3] = {x[t], y[t], z[t]};
+        uint64_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            double u = (v[a] - b.lo[a]) * b.scale[a];
+            u = u < 0.0 ? 0.0 : (u > 2097151.0 ? 2097151.0 : u);
+            q[a] = (uint64_t)u;
+        }
+        key[t] = dev_spread3(q[0]) | (dev_spread3(q[1]) << 1) | (dev_spread3(q[2]) << 2);
+        idx[t] = (int32_t)t;
+    }
+}
+
+__global__ void k_invert(int n, const int32_t *inv, int32_t *perm) {
+    GRID_STRIDE(t, (size_t)n) perm[inv[t]] = (int32_t)t;
+}
+
+template <typename V>
+__global__ void k_scatter(int n, const int32_t *perm, const V *src, V *dst) {
+    GRID_STRIDE(t, (size_t)n) dst[perm ? perm[t] : (int32_t)t] = src[t];
 }
 
 template <typename V>
@@ -993,7 +1072,7 @@ __global__ void k_g0_of(int m, const int32_t *g0_pts, int32_t *g0_of) {
 
 }  // namespace
 
-int device_setup(int device, const mfcfd_params &P, const Topology &T, const double *x, const double *y,
+int device_setup(int device, const mfcfd_params &P, Topology &T, const double *x, const double *y,
                  const double *z, const double *tan1, const double *tan2, const double *nor, const int32_t *nbhs,
                  const int32_t *conn, const std::vector<double> &eps2, cudaStream_t s, const DevAlloc &alloc,
                  DevCloud &d, DevTopology &dt, std::string &err) {
@@ -1017,12 +1096,34 @@ int device_setup(int device, const mfcfd_params &P, const Topology &T, const dou
     PREP_CK(cudaMemcpyAsync(Lnb, nbhs, 4 * (size_t)n, cudaMemcpyHostToDevice, s));
     PREP_CK(cudaMemcpyAsync(Lconn, conn, 4 * (size_t)n * MAX_CONN, cudaMemcpyHostToDevice, s));
     PREP_CK(cudaMemcpyAsync(Lcls, T.cls.data(), (size_t)n, cudaMemcpyHostToDevice, s));
-    if (!T.perm.empty()) {
-        DS_TMP(perm, n); DS_TMP(inv, n);
-        PREP_CK(cudaMemcpyAsync(perm, T.perm.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
-        PREP_CK(cudaMemcpyAsync(inv, T.inv.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, s));
-    }
     const int g = grid_for(device, (size_t)n);
+    T.perm.clear();
+    T.inv.clear();
+    if (P.storage_order == MFCFD_ORDER_MORTON && n > 1) {
+        // morton_order on the device: the bounding box (exact minima and
+        // maxima) on the host, the keys and a stable sort on the device
+        Box b;
+        double hi[3] = {x[0], y[0], z[0]};
+        b.lo[0] = x[0]; b.lo[1] = y[0]; b.lo[2] = z[0];
+        for (int i = 1; i < n; ++i) {
+            const double v[3] = {x[i], y[i], z[i]};
+            for (int a = 0; a < 3; ++a) {
+                b.lo[a] = std::min(b.lo[a], v[a]);
+                hi[a] = std::max(hi[a], v[a]);
+            }
+        }
+        for (int a = 0; a < 3; ++a) b.scale[a] = hi[a] > b.lo[a] ? 2097151.0 / (hi[a] - b.lo[a]) : 0.0;
+        uint64_t *key, *key_sorted;
+        int32_t *idx;
+        DS_TMP(key, n); DS_TMP(key_sorted, n); DS_TMP(idx, n);
+        DS_TMP(perm, n); DS_TMP(inv, n);
+        k_morton_keys<<<g, PREP_THREADS, 0, s>>>(n, Lx, Ly, Lz, b, key, idx);
+        if (int rc = sort_pairs(key, key_sorted, idx, inv, n, s, tmp, err)) return rc;
+        k_invert<<<g, PREP_THREADS, 0, s>>>(n, inv, perm);
+        PREP_CK(cudaGetLastError());
+        if (int rc = to_host(T.perm, perm, (size_t)n, s, err)) return rc;
+        if (int rc = to_host(T.inv, inv, (size_t)n, s, err)) return rc;
+    }
     int *d_sums, *d_total, *flag, *fpos;
     DS_TMP(d_sums, ((size_t)n + 1 + 1023) / 1024 + 1); DS_TMP(d_total, 1);
     DS_TMP(flag, (size_t)n + 1); DS_TMP(fpos, (size_t)n + 1);
@@ -1135,7 +1236,13 @@ int device_setup(int device, const mfcfd_params &P, const Topology &T, const dou
     k_geo<<<g, PREP_THREADS, 0, s>>>(n, sx, sy, sz, frame, list_cnt, list_ent, slot_nbr, geo);
     PREP_CK(cudaGetLastError());
     DS_KEEP(e2, n);
-    PREP_CK(cudaMemcpyAsync(e2, eps2.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+    {
+        double *le2;
+        DS_TMP(le2, n);
+        PREP_CK(cudaMemcpyAsync(le2, eps2.data(), 8 * (size_t)n, cudaMemcpyHostToDevice, s));
+        k_scatter<<<g, PREP_THREADS, 0, s>>>(n, perm, le2, e2);
+        PREP_CK(cudaGetLastError());
+    }
     d.geo = geo; d.eps2 = e2; d.wq = nullptr; d.wf = nullptr; d.outer_delt = nullptr;
 
     // ---- sweep orders (implicit_forward_and_reverse_sweeps.f90:26-84)
@@ -1216,22 +1323,9 @@ int device_setup(int device, const mfcfd_params &P, const Topology &T, const dou
             k_dep_fill<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], off_dir[dir], ent_dir[dir], swept, roff, rcur,
                                                    rlist);
             k_lv_roots<<<gs, PREP_THREADS, 0, s>>>(order[dir], nsw, indeg, dt.level[dir], fa, count);
+            // every level in one block: a barrier per level instead of a launch
+            k_levels_block<<<1, 1024, 0, s>>>(nsw, fa, fb, count, roff, rlist, indeg, dt.level[dir]);
             PREP_CK(cudaGetLastError());
-            int L = 0;
-            int32_t *front = fa, *next = fb;
-            constexpr int BATCH = 256;
-            while (L < nsw) {
-                const int stop = std::min(nsw, L + BATCH);
-                for (; L < stop; ++L) {
-                    k_lv_step<<<64, PREP_THREADS, 0, s>>>(L, front, count, roff, rlist, indeg, dt.level[dir], next);
-                    std::swap(front, next);
-                }
-                PREP_CK(cudaGetLastError());
-                int last = 0;
-                PREP_CK(cudaMemcpyAsync(&last, count + L, sizeof(int), cudaMemcpyDeviceToHost, s));
-                PREP_CK(cudaStreamSynchronize(s));
-                if (last == 0) break;
-            }
             k_level_keys<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], dt.level[dir], key, hcnt, cycle);
             PREP_CK(cudaGetLastError());
             int h_cycle = 0;
@@ -1386,12 +1480,48 @@ int device_chain_schedule(int device, DevTopology &dt, DevCloud &d, int warps, c
     DS_TMP(g0_of, n); DS_TMP(pos, n); DS_TMP(publish, n); DS_TMP(dterms, 3);
     PREP_CK(cudaMemsetAsync(g0_of, 0xff, 4 * (size_t)n, s));
     if (d.n_g0 > 0) k_g0_of<<<grid_for(device, d.n_g0), PREP_THREADS, 0, s>>>(d.n_g0, d.g0_pts, g0_of);
+    // the two directions' warp assignments are independent: the backward
+    // one on a second host thread
+    std::vector<int32_t> owners[2];
+    std::vector<std::vector<int32_t>> lists_of[2];
+    auto assign = [&](int dir) {
+        chain_assign(dt.h_lpts[dir].data(), (int)dt.h_lpts[dir].size(), dt.h_level[dir].data(),
+                     dt.h_coff[dir].data(), dt.h_cand[dir].data(), n, warps, owners[dir], lists_of[dir]);
+    };
+    {
+        std::thread bwd;
+        bool threaded = false;
+        if (take_setup_threads(1) == 1) {
+            try {
+                bwd = std::thread([&] {
+                    try {
+                        assign(1);
+                    } catch (...) {
+                        owners[1].clear();
+                    }
+                });
+                threaded = true;
+            } catch (...) {
+                give_setup_threads(1);
+            }
+        }
+        std::exception_ptr e0;
+        try {
+            assign(0);
+        } catch (...) {
+            e0 = std::current_exception();
+        }
+        if (threaded) {
+            bwd.join();
+            give_setup_threads(1);
+        }
+        if (e0) std::rethrow_exception(e0);
+        if (!threaded || owners[1].size() != (size_t)n) assign(1);
+    }
     for (int dir = 0; dir < 2; ++dir) {
         const int nsw = (int)dt.h_lpts[dir].size();
-        std::vector<int32_t> owner;
-        std::vector<std::vector<int32_t>> lists;
-        chain_assign(dt.h_lpts[dir].data(), nsw, dt.h_level[dir].data(), dt.h_coff[dir].data(),
-                     dt.h_cand[dir].data(), n, warps, owner, lists);
+        const std::vector<int32_t> &owner = owners[dir];
+        const std::vector<std::vector<int32_t>> &lists = lists_of[dir];
         std::vector<int32_t> ptr(warps + 1, 0), pts;
         pts.reserve(nsw);
         for (int w = 0; w < warps; ++w) {

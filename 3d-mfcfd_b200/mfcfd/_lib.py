@@ -22,7 +22,7 @@ FIELD_WIDTH = {FIELD_PRIM: 5, FIELD_U: 5, FIELD_Q: 5, FIELD_QM: 10, FIELD_DQ: 15
 # Every symbol include/mfcfd.h declares.
 EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_step",
            "mfcfd_run", "mfcfd_get", "mfcfd_get_state", "mfcfd_set_state",
-           "mfcfd_get_stencils", "mfcfd_get_alias", "mfcfd_get_levels", "mfcfd_debug_digest", "mfcfd_get_info",
+           "mfcfd_get_stencils", "mfcfd_get_alias", "mfcfd_get_levels", "mfcfd_debug_digest", "mfcfd_knn", "mfcfd_get_info",
            "mfcfd_get_stream", "mfcfd_set_profiling", "mfcfd_get_phase_times",
            "mfcfd_residual_noalloc", "mfcfd_set_fault_hook", "mfcfd_set_precision", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
@@ -147,6 +147,7 @@ def lib():
     L.mfcfd_get_stencils.argtypes = [vp, vp, vp, i32]
     L.mfcfd_get_alias.argtypes = [vp, vp, vp]
     L.mfcfd_get_levels.argtypes = [vp, i32, vp]
+    L.mfcfd_knn.argtypes = [i32, i32, vp, vp, vp, i32, vp, vp, vp]
     L.mfcfd_debug_digest.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64),
                                      ctypes.POINTER(ctypes.c_int64)]
     L.mfcfd_get_info.argtypes = [vp, ctypes.POINTER(Info)]

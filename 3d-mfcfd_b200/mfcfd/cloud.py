@@ -134,26 +134,36 @@ def _boundary_frames(nor: np.ndarray):
 
 
 def _knn_connectivity(pts: np.ndarray, k: int):
-    from scipy.spatial import cKDTree
-    tree = cKDTree(pts)
-    dist, idx = tree.query(pts, k=k + 1, workers=-1)
-    n = pts.shape[0]
-    # Drop the point itself; exact duplicates are not generated.
-    self_first = idx[:, 0] == np.arange(n)
-    if not np.all(self_first):
-        raise ValueError("duplicate points in generated cloud")
-    nb = idx[:, 1:].astype(np.int32)
-    d = dist[:, 1:]
+    """(nbhs, conn, min_dist): the k nearest neighbours of every point, by
+    squared distance then index (the library's mfcfd_knn on the host's
+    threads).  min_dist is the distance to the nearest neighbour, evaluated
+    like the solver evaluates distances (sqrt of the summed squared
+    deltas)."""
+    from ._lib import MfcfdError
+    try:
+        return knn(pts[:, 0], pts[:, 1], pts[:, 2], k, device=-1)
+    except MfcfdError as e:
+        if "coincide" in str(e):
+            raise ValueError("duplicate points in generated cloud") from e
+        raise
+
+
+def knn(x: np.ndarray, y: np.ndarray, z: np.ndarray, k: int = 26, device: int = -1):
+    """(nbhs, conn, min_dist) of the k nearest neighbours of every point
+    through the library (mfcfd_knn): on GPU `device`, or on the host's
+    threads for device < 0; both give the same arrays, ordered by squared
+    distance then index, as _knn_connectivity's."""
+    from . import _lib
+    from ._lib import MfcfdError, ptr
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+    n = x.shape[0]
+    nbhs = np.zeros(n, dtype=np.int32)
     conn = np.zeros((n, MAX_CONN), dtype=np.int32)
-    conn[:, :k] = nb + 1
-    nbhs = np.full(n, k, dtype=np.int32)
-    # min_dist: distance to the nearest neighbour, evaluated like the
-    # solver evaluates distances (sqrt of the summed squared deltas).
-    dx = pts[nb, 0] - pts[:, 0:1]
-    dy = pts[nb, 1] - pts[:, 1:2]
-    dz = pts[nb, 2] - pts[:, 2:3]
-    md = np.sqrt(dx * dx + dy * dy + dz * dz).min(axis=1)
-    del d
+    md = np.zeros(n)
+    L = _lib.lib()
+    rc = L.mfcfd_knn(int(device), n, ptr(x), ptr(y), ptr(z), int(k), ptr(nbhs), ptr(conn), ptr(md))
+    if rc != 0:
+        raise MfcfdError(rc, L.mfcfd_last_error(None).decode())
     return nbhs, conn, md
 
 

@@ -287,6 +287,17 @@ int mfcfd_get_alias(mfcfd_handle *h, int32_t *alias, int32_t *point_with_alias);
  * schedule; -1 for points the sweeps skip. */
 int mfcfd_get_levels(mfcfd_handle *h, int32_t dir, int32_t *level);
 
+/* Connectivity of a cloud that has none: the k (<= 27) nearest neighbours
+ * of every point, as the reference's input file carries them
+ * (point_preprocessor.f90:30-35): conn (27,N) 1-based in increasing order of
+ * (d2, j), d2 = dx*dx + dy*dy + dz*dz with dx = x(j) - x(i), zero padded;
+ * nbhs(i) = k; min_dist(i) = sqrt(d2) of the nearest.  device >= 0 runs on
+ * that GPU, device < 0 on the host's threads; both give the same arrays.
+ * Coinciding points or n <= k give MFCFD_ERR_ARG (message in
+ * mfcfd_last_error(NULL)). */
+int mfcfd_knn(int32_t device, int32_t n, const double *x, const double *y, const double *z, int32_t k,
+              int32_t *nbhs, int32_t *conn, double *min_dist);
+
 /* Diagnostics: a 64-bit FNV-1a digest of one device array of the handle's
  * topology, by its DevCloud name ("geo", "fwd_ent", "ch_items0", ...), and its
  * size in bytes (-1: not allocated).  Two handles of one cloud and
