@@ -115,6 +115,17 @@ module mfcfd_interface
             integer(c_int) :: rc
         end function mfcfd_set_precision
 
+        ! the connectivity of a cloud given only its points: conn(27,N) of
+        ! the k nearest neighbours, on GPU `device` (>= 0) or the host
+        function mfcfd_knn(device, n, x, y, z, k, nbhs, conn, min_dist) result(rc) bind(C, name="mfcfd_knn")
+            import :: c_int32_t, c_double, c_int
+            integer(c_int32_t), value :: device, n, k
+            real(c_double), intent(in) :: x(*), y(*), z(*)
+            integer(c_int32_t), intent(out) :: nbhs(*), conn(27, *)
+            real(c_double), intent(out) :: min_dist(*)
+            integer(c_int) :: rc
+        end function mfcfd_knn
+
         function mfcfd_set_fault_hook(h, point, wait_limit) result(rc) bind(C, name="mfcfd_set_fault_hook")
             import :: c_ptr, c_int32_t, c_int
             type(c_ptr), value :: h

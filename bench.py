@@ -230,6 +230,33 @@ def cpu_reference(procs, warm, steps, mach, aoa):
 
 # ------------------------------------------------------------------ main
 
+def setup_measure(c, wl, args, local_rank, host_s):
+    """Set-up of the workload's cloud: the host set-up (the handle the bench
+    times, already built), the device-resident set-up (gpu_setup = 1; the
+    same arrays, checked by tests/test_gpu_device_setup.py) and the
+    connectivity from raw points (mfcfd_knn) on the GPU and on the host's
+    threads.  Wall-clock seconds of the library calls, inputs on the host."""
+    from mfcfd import cloud as cl
+    from mfcfd.solver import Solver
+    t = time.perf_counter()
+    s2 = Solver(c, wl["mach"], wl["aoa"], device=local_rank, sweep_mode=args.sweep_mode,
+                chain_spread=args.chain_spread, gpu_setup=1)
+    dev_s = time.perf_counter() - t
+    s2.close()
+    cl.knn(c.x[:4096], c.y[:4096], c.z[:4096], 26, device=local_rank)   # module load
+    t = time.perf_counter()
+    _, conn_d, _ = cl.knn(c.x, c.y, c.z, 26, device=local_rank)
+    knn_dev = time.perf_counter() - t
+    t = time.perf_counter()
+    _, conn_h, _ = cl.knn(c.x, c.y, c.z, 26, device=-1)
+    knn_host = time.perf_counter() - t
+    return {"points": c.n, "host_s": host_s, "device_s": dev_s, "speedup": host_s / dev_s,
+            "knn_device_s": knn_dev, "knn_host_s": knn_host, "knn_host_threads": os.cpu_count(),
+            "knn_equal": bool((conn_d == conn_h).all()),
+            "what": "mfcfd_create with the host set-up (gpu_setup 0) and the device-resident set-up "
+                    "(gpu_setup 1), and mfcfd_knn k=26 on the GPU and the host"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -261,6 +288,8 @@ def main():
     ap.add_argument("--serve-max-iters", type=int, default=600)
     ap.add_argument("--serve-chunk", type=int, default=10)
     ap.add_argument("--serve-setup-threads", type=int, default=8)
+    ap.add_argument("--no-setup-timing", action="store_true",
+                    help="skip the set-up and kNN timings of the default line")
     ap.add_argument("--serve-precision", type=int, default=1, help="1 mixed, 2 mixed-dc (FP64 residual)")
     ap.add_argument("--serve-conv-requests", type=int, default=8)
     ap.add_argument("--serve-conv-min-points", type=int, default=5000)
@@ -310,8 +339,13 @@ def main():
 
     c = cl.shell_cloud(wl["shells"], wl["per_shell"], jitter=wl["jitter"],
                        seed=replicas.replica_seed(wl["seed"], rank))
+    t_setup = time.perf_counter()
     s = Solver(c, wl["mach"], wl["aoa"], device=local_rank, sweep_mode=args.sweep_mode,
                chain_spread=args.chain_spread)
+    setup_host_s = time.perf_counter() - t_setup
+    setup = None
+    if world == 1 and not args.no_setup_timing:
+        setup = setup_measure(c, wl, args, local_rank, setup_host_s)
     prim0 = cl.initial_state(c, wl["mach"], wl["aoa"])
     s.initial_conditions(prim0)
     info = s.info()
@@ -476,7 +510,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "point-iters/s",
                         "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                 "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks, "mixed": mixed,
-                "serving": serving, "serving_converged": serving_conv,
+                "serving": serving, "serving_converged": serving_conv, "setup": setup,
                 "gpu_launches": (KERNELS_PER_ITER[args.sweep_mode] + (1 if info.get("g0_points") else 0)) * args.steps}
         print(json.dumps(line), flush=True)
     if s is not None:
