@@ -15,9 +15,12 @@ from . import _lib
 from ._lib import MfcfdError, ptr
 
 
-def run_batch(solvers, iters: int, t0=None):
+def run_batch(solvers, iters: int, t0=None, statuses=None):
     """Run `iters` iterations of every Solver; returns res_hist
-    (len(solvers), iters, 2) and appends to each solver's history."""
+    (len(solvers), iters, 2) and appends to each solver's history.  With a
+    list `statuses`, a cloud's failure (a non-finite residual, say) is
+    recorded there instead of raised, and the other clouds' histories are
+    kept."""
     n = len(solvers)
     hs = (ctypes.c_void_p * n)(*[s.h.value for s in solvers])
     if t0 is None:
@@ -26,12 +29,16 @@ def run_batch(solvers, iters: int, t0=None):
     hist = np.zeros((n, iters, 2))
     status = np.zeros(n, dtype=np.int32)
     rc = _lib.lib().mfcfd_run_batch(hs, n, ptr(t0a), int(iters), ptr(hist), ptr(status))
+    if statuses is not None:
+        statuses[:] = [int(v) for v in status]
     for i, s in enumerate(solvers):
         if status[i] != 0:
+            if statuses is not None:
+                continue
             raise MfcfdError(int(status[i]), _lib.lib().mfcfd_last_error(s.h).decode())
         for j in range(iters):
             s.history.append((int(t0a[i]) + j, float(hist[i, j, 0]), float(hist[i, j, 1])))
-    if rc != 0:
+    if rc != 0 and (statuses is None or not any(statuses)):
         raise MfcfdError(rc, "batch failed")
     return hist
 

@@ -133,15 +133,16 @@ def _boundary_frames(nor: np.ndarray):
     return tan1, tan2
 
 
-def _knn_connectivity(pts: np.ndarray, k: int):
+def _knn_connectivity(pts: np.ndarray, k: int, device: int = -1):
     """(nbhs, conn, min_dist): the k nearest neighbours of every point, by
     squared distance then index (the library's mfcfd_knn on the host's
-    threads).  min_dist is the distance to the nearest neighbour, evaluated
+    threads, or on GPU `device`: the same arrays).  min_dist is the distance
+    to the nearest neighbour, evaluated
     like the solver evaluates distances (sqrt of the summed squared
     deltas)."""
     from ._lib import MfcfdError
     try:
-        return knn(pts[:, 0], pts[:, 1], pts[:, 2], k, device=-1)
+        return knn(pts[:, 0], pts[:, 1], pts[:, 2], k, device=device)
     except MfcfdError as e:
         if "coincide" in str(e):
             raise ValueError("duplicate points in generated cloud") from e
@@ -170,7 +171,7 @@ def knn(x: np.ndarray, y: np.ndarray, z: np.ndarray, k: int = 26, device: int = 
 def shell_cloud(n_shells: int, pts_per_shell: int, r0: float = 0.5,
                 r1: float = 10.0, jitter: float = 0.02, k: int = 26,
                 seed: int = 1001, aspect=(1.0, 1.0, 1.0),
-                name: str = "sphere") -> PointCloud:
+                name: str = "sphere", knn_device: int = -1) -> PointCloud:
     """Concentric shells around a sphere or ellipsoid body.
 
     Shell ``s`` has radius ``r0 * (r1/r0)**(s/(n_shells-1))`` and carries a
@@ -182,7 +183,9 @@ def shell_cloud(n_shells: int, pts_per_shell: int, r0: float = 0.5,
 
     Frames: interior points use the global axes; wall and outer points use
     the outward unit normal as ``nor``, ``tan1 = z x nor`` normalised
-    (x when ``nor`` is along z) and ``tan2 = nor x tan1``.
+    (x when ``nor`` is along z) and ``tan2 = nor x tan1``.  The neighbours
+    are found on GPU ``knn_device`` (>= 0) or the host's threads; the cloud is
+    the same either way.
     """
     if n_shells < 3:
         raise ValueError("need at least 3 shells")
@@ -222,7 +225,7 @@ def shell_cloud(n_shells: int, pts_per_shell: int, r0: float = 0.5,
     b = status != STATUS_INTERIOR
     t1b, t2b = _boundary_frames(nor_b[b])
     tan1[b], tan2[b], nor[b] = t1b, t2b, nor_b[b]
-    nbhs, conn, md = _knn_connectivity(pts, k)
+    nbhs, conn, md = _knn_connectivity(pts, k, knn_device)
     a, bb, c = ax * r0
     # Surface area of the body (Thomsen's approximation for an ellipsoid).
     pp = 1.6075

@@ -167,12 +167,15 @@ def device_bytes(cloud: PointCloud, mach: float, aoa_deg: float, device: int = 0
 
 
 def request_stream(count: int, rate: float, seed: int, n_min: int, n_max: int, pool: int = 8,
-                   mach=(0.3, 0.85), alpha=(-5.0, 5.0), aspect=(1.0, 3.0)):
+                   mach=(0.3, 0.85), alpha=(-5.0, 5.0), aspect=(1.0, 3.0), bodies: str = "mixed",
+                   knn_device: int = -1):
     """A seeded stream of solve requests: Poisson arrival times at `rate`/s,
     each naming one of `pool` shell clouds (sphere or ellipsoid body with
     axis ratios U[aspect], point counts log-uniform in [n_min, n_max], shell
     count proportional to N^(1/3)) and a flow (Mach U[mach], angle of attack
-    U[alpha] degrees).  Returns (arrivals, clouds, [(cloud index, mach, alpha)])."""
+    U[alpha] degrees).  bodies "mixed" alternates spheres and ellipsoids,
+    "ellipsoids" makes every body one.  Returns (arrivals, clouds, [(cloud
+    index, mach, alpha)])."""
     import math
     from . import cloud as cl
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -181,9 +184,11 @@ def request_stream(count: int, rate: float, seed: int, n_min: int, n_max: int, p
         n = math.exp(rng.uniform(math.log(n_min), math.log(n_max)))
         shells = max(8, int(round(1.21 * n ** (1.0 / 3.0))))
         per = max(100, int(round(n / shells)))
-        ax = (1.0, rng.uniform(*aspect), rng.uniform(*aspect)) if j % 2 else (1.0, 1.0, 1.0)
+        ell = bodies == "ellipsoids" or j % 2 == 1
+        ax = (1.0, rng.uniform(*aspect), rng.uniform(*aspect)) if ell else (1.0, 1.0, 1.0)
         clouds.append(cl.shell_cloud(shells, per, jitter=0.02, seed=seed * 100 + j, aspect=ax,
-                                     name=f"{'ellipsoid' if j % 2 else 'sphere'}-{shells}x{per}"))
+                                     name=f"{'ellipsoid' if ell else 'sphere'}-{shells}x{per}",
+                                     knn_device=knn_device))
     arrivals = poisson_arrivals(rate, count, seed + 1)
     reqs = [(int(rng.integers(pool)), float(rng.uniform(*mach)), float(rng.uniform(*alpha)))
             for _ in range(count)]

@@ -272,8 +272,15 @@ def main():
     ap.add_argument("--wing-compare-iters", type=int, default=200,
                     help="iterations after which mixed CL/CD are compared with an FP64 run")
     ap.add_argument("--batch-clouds", type=int, default=24)
-    ap.add_argument("--batch-min-points", type=int, default=10000)
-    ap.add_argument("--batch-max-points", type=int, default=40000)
+    ap.add_argument("--batch-bodies", choices=["mixed", "ellipsoids"], default="mixed")
+    ap.add_argument("--batch-mach", type=float, nargs=2, default=[0.3, 0.85],
+                    help="Mach range of the batch workload's flows")
+    ap.add_argument("--batch-budget-gb", type=float, default=120.0,
+                    help="device memory of one wave of batched handles")
+    ap.add_argument("--batch-min-points", type=int, default=None,
+                    help="smallest cloud (default 20000 for batch, 10000 for batch-converged)")
+    ap.add_argument("--batch-max-points", type=int, default=None,
+                    help="largest cloud (default 100000 for batch, 40000 for batch-converged)")
     ap.add_argument("--batch-max-iters", type=int, default=12000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-mode", type=int, default=2, help="2 chains, 0 dataflow, 1 levels")
@@ -654,8 +661,8 @@ def batch_converged_main(args, rank, world, local_rank):
     # spheres at M 0.3-0.6: the seeded ellipsoid clouds and the higher Mach
     # numbers include solves that stall above a 1e-6 drop or diverge in FP64
     _, clouds, reqs = serve.request_stream(args.batch_clouds, 1.0, replicas.replica_seed(7100, rank),
-                                           args.batch_min_points, args.batch_max_points, pool=args.batch_clouds,
-                                           mach=(0.3, 0.6), aspect=(1.0, 1.0))
+                                           args.batch_min_points or 10000, args.batch_max_points or 40000,
+                                           pool=args.batch_clouds, mach=(0.3, 0.6), aspect=(1.0, 1.0))
     flows = [(reqs[i][1], reqs[i][2]) for i in range(len(clouds))]
     # warm-up: one short batched round (graph capture, first launches)
     ws = [Solver(clouds[0], *flows[0], device=local_rank, precision=_lib.PRECISION_MIXED_DC)]
@@ -716,10 +723,15 @@ def batch_converged_main(args, rank, world, local_rank):
 
 def batch_main(args, rank, world, local_rank):
     """Batched clouds: a seeded set of sphere and ellipsoid clouds of uneven
-    size (log-uniform 20k-100k points) iterated together in mixed precision,
-    each chunk a captured graph and the chain schedules autotuned for the batch,
-    against the same clouds run one after another on the plain FP64 path.
-    Both are device-timed over the same iterations; point-iters/s aggregate."""
+    size (log-uniform --batch-min-points to --batch-max-points) iterated
+    together in mixed precision, each chunk a captured graph and the chain
+    schedules autotuned for the batch, against the same clouds run one after
+    another on the plain FP64 path.  Both are device-timed over the same
+    iterations; point-iters/s aggregate.  A batch larger than
+    --batch-budget-gb of device memory runs in waves of handles that fit;
+    every wave is tuned, warmed and timed the same way and the timed seconds
+    add up.  Set-up and connectivity run on the device (gpu_setup 1,
+    mfcfd_knn), outside the timed regions."""
     import torch
     from mfcfd import _lib, batch, replicas, serve
     from mfcfd.solver import Solver
@@ -730,47 +742,97 @@ def batch_main(args, rank, world, local_rank):
                               "point-iteration workloads"}), flush=True)
         return
     torch.cuda.set_device(local_rank)
-    rank, world = replicas.init("nccl", timeout_s=1800)
+    rank, world = replicas.init("nccl", timeout_s=3600)
+    t_gen = time.perf_counter()
     _, clouds, reqs = serve.request_stream(args.batch_clouds, 1.0, replicas.replica_seed(7000, rank),
-                                           20000, 100000, pool=args.batch_clouds)
+                                           args.batch_min_points or 20000, args.batch_max_points or 100000,
+                                           pool=args.batch_clouds, bodies=args.batch_bodies, knn_device=local_rank,
+                                           mach=tuple(args.batch_mach))
+    t_gen = time.perf_counter() - t_gen
     flows = [(reqs[i][1], reqs[i][2]) for i in range(len(clouds))]
     pts = sum(c.n for c in clouds)
     # plain FP64 path, one cloud after another (device time of `steps` iterations each)
     seq_ms = 0.0
+    seq_restarted = 0
     for c, (m, a) in zip(clouds, flows):
-        s = Solver(c, m, a, device=local_rank)
-        s.initial_conditions()
-        s.q_lskum(args.warmup)
+        s = Solver(c, m, a, device=local_rank, gpu_setup=1)
         st = torch.cuda.ExternalStream(s.stream())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        s.q_lskum(args.steps, t0=1 + args.warmup)
-        e1.record(st)
-        torch.cuda.synchronize()
-        seq_ms += e0.elapsed_time(e1)
+        for attempt in range(2):   # a diverging cloud starts again from the freestream
+            try:
+                s.initial_conditions()
+                s.q_lskum(args.warmup)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                s.q_lskum(args.steps, t0=1 + args.warmup)
+                e1.record(st)
+                torch.cuda.synchronize()
+                seq_ms += e0.elapsed_time(e1)
+                break
+            except _lib.MfcfdError:
+                seq_restarted += 1
+                if attempt == 1:
+                    raise
         s.close()
-    # batched: mixed precision, tuned schedules, graph-captured chunks
-    ss = []
-    for c, (m, a) in zip(clouds, flows):
-        s = Solver(c, m, a, device=local_rank, precision=_lib.PRECISION_MIXED)
-        s.initial_conditions()
-        ss.append(s)
-    t_tune = time.perf_counter()
-    percent, tune_times = batch.tune_batch(ss, iters=4)
-    t_tune = time.perf_counter() - t_tune
-    warps = [s.info()["chain_warps"] for s in ss]
-    # warm-up: the timed chunk length, for both U/q parities (graphs captured)
-    batch.run_batch(ss, args.warmup)
-    for _ in range(1 if args.steps % 2 == 0 else 2):
-        batch.run_batch(ss, args.steps)
-    replicas.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    batch.run_batch(ss, args.steps)
-    torch.cuda.synchronize()
-    bat_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
-    for s in ss:
-        s.close()
+    # batched: mixed precision, tuned schedules, graph-captured chunks, in
+    # waves of handles within the memory budget
+    budget = args.batch_budget_gb * 1e9
+    bat_s, t_setup, t_tune, waves = 0.0, 0.0, 0.0, []
+    percents, warps = [], []
+    j = 0
+    while j < len(clouds):
+        ss, used = [], 0
+        t1 = time.perf_counter()
+        while j < len(clouds):
+            c, (m, a) = clouds[j], flows[j]
+            s = Solver(c, m, a, device=local_rank, precision=_lib.PRECISION_MIXED, gpu_setup=1)
+            s.initial_conditions()
+            ss.append(s)
+            used += s.info()["device_bytes"]
+            j += 1
+            if used > budget:
+                break
+        t_setup += time.perf_counter() - t1
+        t1 = time.perf_counter()
+        percent, _ = batch.tune_batch(ss, iters=4)
+        t_tune += time.perf_counter() - t1
+        percents.append(percent)
+        warps += [s.info()["chain_warps"] for s in ss]
+        def restart_failed(st, ss=ss):
+            # a cloud whose residual went non-finite starts again from the
+            # freestream (the reference scheme diverges on some seeded
+            # ellipsoids); the batch keeps its shape
+            bad = [i for i, v in enumerate(st) if v != 0]
+            for i in bad:
+                ss[i].initial_conditions()
+            return len(bad)
+
+        # warm-up: the timed chunk length, for both U/q parities (graphs captured)
+        st = [0] * len(ss)
+        restarted = 0
+        batch.run_batch(ss, args.warmup, statuses=st)
+        restarted += restart_failed(st)
+        for _ in range(1 if args.steps % 2 == 0 else 2):
+            batch.run_batch(ss, args.steps, statuses=st)
+            restarted += restart_failed(st)
+        for attempt in range(3):
+            replicas.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            batch.run_batch(ss, args.steps, statuses=st)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            k = restart_failed(st)
+            restarted += k
+            if k == 0:
+                break
+        bat_s += dt
+        waves.append({"clouds": len(ss), "points": sum(s.n for s in ss), "device_bytes": used, "timed_s": dt,
+                      "restarted_clouds": restarted})
+        print(f"wave {len(waves)}: {len(ss)} clouds, {waves[-1]['points']} points, {used / 1e9:.1f} GB, "
+              f"{dt:.3f} s, restarted {restarted}", file=sys.stderr, flush=True)
+        for s in ss:
+            s.close()
+    bat_s = replicas.max_over_ranks(bat_s, device="cuda")
     seq_s = replicas.max_over_ranks(seq_ms / 1e3, device="cuda")
     value = pts * args.steps * world / bat_s
     if rank == 0:
@@ -781,13 +843,17 @@ def batch_main(args, rank, world, local_rank):
                 "data": "synthetic (seeded sphere/ellipsoid shell clouds)",
                 "config": {"workload": "batch", "clouds": len(clouds), "points_total": pts,
                            "points_min": min(c.n for c in clouds), "points_max": max(c.n for c in clouds),
-                           "tuned_percent_of_widest_level": percent,
-                           "tune_round_s": {str(k): v for k, v in tune_times.items()},
-                           "tuned_warps": warps, "tune_s": t_tune, "parallelism": f"replicas x{world}",
+                           "bodies": args.batch_bodies, "mach_range": list(args.batch_mach),
+                           "alpha_range_deg": [-5.0, 5.0],
+                           "tuned_percent_of_widest_level": percents, "tuned_warps": warps,
+                           "waves": waves, "budget_gb": args.batch_budget_gb,
+                           "generate_s": t_gen, "setup_s": t_setup, "tune_s": t_tune,
+                           "parallelism": f"replicas x{world}",
                            "timing": "batched: wall clock with device synchronisation around the K "
-                                     "iterations; FP64: device events, clouds one after another"},
+                                     "iterations of each wave, summed; FP64: device events, clouds one "
+                                     "after another"},
                 "fp64_one_at_a_time": {"value": pts * args.steps * world / seq_s, "unit": "point-iters/s",
-                                       "ms_per_step": seq_s * 1e3 / args.steps},
+                                       "ms_per_step": seq_s * 1e3 / args.steps, "restarted": seq_restarted},
                 "speedup_vs_fp64_one_at_a_time": seq_s / bat_s}
         print(json.dumps(line), flush=True)
     replicas.finalize()
