@@ -277,15 +277,20 @@ int level_counts(int n, int count[KNN_MAX_LEVELS], long long span[KNN_MAX_LEVELS
     return levels;
 }
 
+// stream-ordered scratch, so a search beside running solves does not wait
+// for the whole device
 struct KnnBufs {
     std::vector<void *> p;
+    cudaStream_t s;
+    explicit KnnBufs(cudaStream_t st) : s(st) {}
     ~KnnBufs() {
-        for (void *v : p) cudaFree(v);
+        for (void *v : p) cudaFreeAsync(v, s);
+        cudaStreamSynchronize(s);
     }
     template <typename T>
     cudaError_t alloc(T **ptr, size_t count) {
         void *v = nullptr;
-        cudaError_t e = cudaMalloc(&v, sizeof(T) * (count ? count : 1));
+        cudaError_t e = cudaMallocAsync(&v, sizeof(T) * (count ? count : 1), s);
         if (e == cudaSuccess) p.push_back(v);
         *ptr = (T *)v;
         return e;
@@ -310,7 +315,7 @@ int knn_device(int device, int n, const double *x, const double *y, const double
         cudaStream_t s;
         ~StreamGuard() { cudaStreamDestroy(s); }
     } guard{s};
-    KnnBufs b;
+    KnnBufs b(s);
     double *dx, *dy, *dz, *sx, *sy, *sz, *dmd;
     uint64_t *key, *key2;
     int32_t *idx, *id, *dnb, *dconn;

@@ -39,16 +39,25 @@ namespace {
 
 constexpr int PREP_THREADS = 256;
 
-// Device buffers of one pass, freed on every return path.
+// Device buffers of one pass, freed on every return path.  With a stream
+// they are stream-ordered (allocated and freed on it), so a set-up running
+// beside other work never waits for the whole device to drain.
 struct DevBufs {
     std::vector<void *> ptrs;
+    cudaStream_t stream = nullptr;
+    DevBufs() = default;
+    explicit DevBufs(cudaStream_t s) : stream(s) {}
     ~DevBufs() {
-        for (void *p : ptrs) cudaFree(p);
+        for (void *p : ptrs) {
+            if (stream) cudaFreeAsync(p, stream);
+            else cudaFree(p);
+        }
     }
     template <typename T>
     cudaError_t alloc(T **p, size_t count) {
         void *v = nullptr;
-        cudaError_t e = cudaMalloc(&v, sizeof(T) * (count > 0 ? count : 1));
+        const size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+        cudaError_t e = stream ? cudaMallocAsync(&v, bytes, stream) : cudaMalloc(&v, bytes);
         if (e == cudaSuccess) ptrs.push_back(v);
         *p = (T *)v;
         return e;
@@ -345,7 +354,7 @@ namespace {
 // point_with_alias, both n long, are written on stream s.
 int alias_search(int device, int n, const int32_t *d_nb, const int32_t *d_conn, int32_t *d_alias, int32_t *d_pwa,
                  cudaStream_t s, std::string &err) {
-    DevBufs b;
+    DevBufs b(s);
     int32_t *d_fa, *d_fb;
     unsigned *d_key;
     int *d_flag, *d_pos, *d_sums, *d_total;
@@ -1103,7 +1112,7 @@ int device_setup(int device, const mfcfd_params &P, Topology &T, const double *x
     const int n = T.n, cap = T.cap;
     const size_t n3 = 3 * (size_t)n;
     const bool chains = P.sweep_mode == MFCFD_SWEEP_CHAINS;
-    DevBufs tmp;
+    DevBufs tmp(s);
     // ---- the cloud, in the reference's order, and the permutation
     double *Lx, *Ly, *Lz, *Lt1, *Lt2, *Ln;
     int32_t *Lnb, *Lconn, *perm = nullptr, *inv = nullptr;
@@ -1500,7 +1509,7 @@ int device_setup(int device, const mfcfd_params &P, Topology &T, const double *x
 int device_chain_schedule(int device, DevTopology &dt, DevCloud &d, int warps, cudaStream_t s,
                           const DevAlloc &alloc, int64_t terms[3], std::string &err) {
     const int n = d.n;
-    DevBufs tmp;
+    DevBufs tmp(s);
     terms[0] = terms[1] = terms[2] = 0;
     int32_t *g0_of, *pos;
     uint8_t *publish;

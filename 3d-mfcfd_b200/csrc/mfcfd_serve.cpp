@@ -108,9 +108,46 @@ struct mfcfd_server {
 
     void worker_loop();
     void scheduler_loop();
+    int create_on_device(const RequestPtr &r);
     void retire(const RequestPtr &r, int status);
     int submit(const mfcfd_request *q, int64_t *id);
 };
+
+// device_setup: the request's handle made on the device when it is admitted
+// (its inputs were kept); the reservation becomes the handle's own bytes.
+int mfcfd_server::create_on_device(const RequestPtr &r) {
+    mfcfd_params P = r->P;
+    P.device = cfg.device;
+    P.gpu_setup = 1;
+    mfcfd_handle *h = nullptr;
+    int rc = mfcfd_create(&P, r->n, r->status.data(), r->x.data(), r->y.data(), r->z.data(), r->tan1.data(),
+                          r->tan2.data(), r->nor.data(), r->nbhs.data(), r->conn.data(), r->min_dist.data(), &h);
+    if (!rc && cfg.chain_percent > 0 && P.sweep_mode == MFCFD_SWEEP_CHAINS) {
+        mfcfd_info info;
+        rc = mfcfd_get_info(h, &info);
+        if (!rc)
+            rc = mfcfd_set_chain_warps(h, std::max(4, (int)((int64_t)info.max_level_width * cfg.chain_percent / 100)),
+                                       nullptr);
+    }
+    int64_t bytes = 0;
+    if (!rc) rc = mfcfd_device_bytes(h, &bytes);
+    if (rc && h) set_message(r->err, mfcfd_last_error(h));
+    std::vector<int32_t>().swap(r->status);
+    std::vector<int32_t>().swap(r->nbhs);
+    std::vector<int32_t>().swap(r->conn);
+    for (auto *v : {&r->x, &r->y, &r->z, &r->tan1, &r->tan2, &r->nor, &r->min_dist}) std::vector<double>().swap(*v);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!rc) {
+            st.bytes_live += bytes - r->bytes;
+            st.peak_bytes_live = std::max(st.peak_bytes_live, st.bytes_live);
+            r->bytes = bytes;
+            r->res.device_bytes = bytes;
+        }
+    }
+    r->h = h;   // destroyed with the request on failure too
+    return rc;
+}
 
 void mfcfd_server::worker_loop() {
     for (;;) {
@@ -134,7 +171,12 @@ void mfcfd_server::worker_loop() {
             continue;
         }
         if (job == ATTACH) {
-            int rc = mfcfd_attach(r->h);
+            int rc = MFCFD_OK;
+            if (cfg.device_setup) {
+                rc = create_on_device(r);
+            } else {
+                rc = mfcfd_attach(r->h);
+            }
             if (!rc) rc = mfcfd_set_prim(r->h, r->prim0.data());
             std::vector<double>().swap(r->prim0);
             mfcfd_info info;
@@ -157,6 +199,33 @@ void mfcfd_server::worker_loop() {
                 cv_sched.notify_one();
             }
             if (!queued) retire(r, MFCFD_ERR_NOMEM);
+            continue;
+        }
+        if (cfg.device_setup) {
+            // set up at admission: reserve an estimate of its device bytes
+            const int64_t bytes = (int64_t)r->n * MFCFD_DEVICE_SETUP_BYTES_PER_POINT;
+            std::lock_guard<std::mutex> lk(mu);
+            --preparing;
+            r->res.t_ready = now();
+            r->res.device_bytes = bytes;
+            int rc = MFCFD_OK;
+            if (bytes > cfg.hbm_budget) {
+                rc = MFCFD_ERR_NOMEM;
+                set_message(r->err, "the request needs more device memory than the server's budget");
+            } else {
+                try {
+                    ready.push_back(r);
+                } catch (...) {
+                    rc = MFCFD_ERR_NOMEM;
+                }
+            }
+            if (rc) {
+                finish_locked(r, rc);
+            } else {
+                r->bytes = bytes;
+                ++events;
+                cv_sched.notify_one();
+            }
             continue;
         }
         mfcfd_params P = r->P;
@@ -418,7 +487,7 @@ int mfcfd_server_create(const mfcfd_server_config *cfg, mfcfd_server **out) {
     *out = nullptr;
     if (!cfg || cfg->device < 0 || cfg->max_live < 0 || cfg->setup_threads < 1 || cfg->setup_threads > 64 ||
         cfg->chunk < 1 || cfg->chunk > 1024 || cfg->hbm_budget < 0 || cfg->chain_percent < 0 ||
-        cfg->chain_percent > 1000)
+        cfg->chain_percent > 1000 || cfg->device_setup < 0 || cfg->device_setup > 1)
         return MFCFD_ERR_ARG;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return MFCFD_ERR_CUDA;
     auto *s = new (std::nothrow) mfcfd_server();

@@ -86,7 +86,7 @@ class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("max_live", ctypes.c_int32),
                 ("setup_threads", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("hbm_budget", ctypes.c_int64), ("chain_percent", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 7)]
+                ("device_setup", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
 
 
 class Request(ctypes.Structure):

@@ -27,9 +27,10 @@ def _cloud_arrays(cloud: PointCloud):
 
 class Server:
     def __init__(self, device: int = 0, max_live: int = 0, setup_threads: int = 2, chunk: int = 20,
-                 hbm_budget: int = 0, chain_percent: int = 100):
+                 hbm_budget: int = 0, chain_percent: int = 100, device_setup: bool = False):
         cfg = _lib.ServerConfig(device=device, max_live=max_live, setup_threads=setup_threads,
-                                chunk=chunk, hbm_budget=hbm_budget, chain_percent=chain_percent)
+                                chunk=chunk, hbm_budget=hbm_budget, chain_percent=chain_percent,
+                                device_setup=1 if device_setup else 0)
         self.chunk = chunk
         self.h = ctypes.c_void_p()
         rc = _lib.lib().mfcfd_server_create(ctypes.byref(cfg), ctypes.byref(self.h))

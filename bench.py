@@ -295,6 +295,8 @@ def main():
     ap.add_argument("--serve-max-iters", type=int, default=600)
     ap.add_argument("--serve-chunk", type=int, default=10)
     ap.add_argument("--serve-setup-threads", type=int, default=8)
+    ap.add_argument("--serve-device-setup", action="store_true",
+                    help="the server sets each request up on the device at admission")
     ap.add_argument("--no-setup-timing", action="store_true",
                     help="skip the set-up and kNN timings of the default line")
     ap.add_argument("--serve-precision", type=int, default=1, help="1 mixed, 2 mixed-dc (FP64 residual)")
@@ -904,13 +906,15 @@ def serve_measure(args, rank, world, local_rank, count, max_points, min_points=N
     precision = _lib.PRECISION_MIXED if precision is None else precision
     arrivals, clouds, reqs = serve.request_stream(count, args.serve_rate,
                                                   replicas.replica_seed(seed, rank),
-                                                  min_points, max_points, mach=mach, aspect=aspect)
+                                                  min_points, max_points, mach=mach, aspect=aspect,
+                                                  knn_device=local_rank)
 
     def run(prec, max_live):
         # many requests at once: chain schedules of the widest level's width;
         # one at a time: each request's own (twice that)
         with serve.Server(device=local_rank, chunk=args.serve_chunk, setup_threads=args.serve_setup_threads,
-                          max_live=max_live, chain_percent=100 if max_live == 0 else 0) as srv:
+                          max_live=max_live, chain_percent=100 if max_live == 0 else 0,
+                          device_setup=args.serve_device_setup) as srv:
             # warm-up request (untimed): first graph capture and launches in the process
             small = min(range(len(clouds)), key=lambda i: clouds[i].n)
             srv.wait(srv.submit(clouds[small], 0.5, 0.0, max_iters=args.serve_chunk, residue_target=-99.0,
@@ -955,6 +959,7 @@ def serve_measure(args, rank, world, local_rank, count, max_points, min_points=N
                        "points_min": min(pts), "points_max": max(pts), "points_total": sum(pts),
                        "residue_target": target, "max_iters": max_iters, "polish_residue": polish,
                        "chunk": args.serve_chunk, "mach_range": list(mach), "aspect_range": list(aspect),
+                       "setup": "device, at admission" if args.serve_device_setup else "host, at arrival",
                        "precision": {1: "mixed", 2: "mixed-dc (FP64 residual, FP32 sweeps)"}.get(precision, "fp64"),
                        "parallelism": f"replicas x{world}"},
             "latency_s": lat, "latency_phases_mean_s": phases(res_m), "converged": conv, "failed": sum(1 for r in res_m if r["status"]),

@@ -105,7 +105,7 @@ typedef struct mfcfd_params {
                                  results.  mfcfd_create computes every topology array on
                                  the device (the host classifies and orders the points
                                  and assigns the chain warps) for the alias sweep driver,
-                                 power 0, FP64 or MIXED_DC and no supersonic points;
+                                 power 0 and no supersonic points;
                                  otherwise, and in mfcfd_prepare, the split stencils, alias
                                  search and sweep levels run on the device for the host's
                                  set-up */
@@ -469,8 +469,15 @@ typedef struct mfcfd_server_config {
     int32_t chain_percent;    /* chain schedule of each request: this percentage of its widest
                                  sweep level in warps (100 suits many requests at once);
                                  0: the request's own setting */
-    int32_t reserved[7];
+    int32_t device_setup;     /* 1: each request is set up on the device when it is admitted
+                                 (mfcfd_create with gpu_setup = 1) instead of on the host
+                                 when it arrives; admission reserves
+                                 MFCFD_DEVICE_SETUP_BYTES_PER_POINT bytes per point and
+                                 then holds the handle's own count (mfcfd_device_bytes) */
+    int32_t reserved[6];
 } mfcfd_server_config;
+
+#define MFCFD_DEVICE_SETUP_BYTES_PER_POINT 6144
 
 typedef struct mfcfd_request {
     mfcfd_params params;      /* flow, precision, schedule; device is the server's */

@@ -10,7 +10,7 @@ uploads, for clouds with and without spilled split lists, wall frames that
 vary from point to point, phase-A (k_g0) points, either storage order and
 every sweep schedule.  Iterations then give the same bits by construction;
 that is checked too.  Configurations the device path does not cover (the
-backup driver, supersonic points, power != 0, MIXED) take the host path and
+backup driver, supersonic points, power != 0) take the host path and
 must still match.
 """
 import numpy as np
@@ -50,6 +50,7 @@ CASES = {
     "chains-index-order": dict(storage_order=0),
     "chains-capacity-12": dict(split_capacity=12),
     "chains-dc": dict(precision=2),
+    "chains-mixed": dict(precision=1),
     "levels": dict(sweep_mode=1),
     "dataflow": dict(sweep_mode=0),
 }
@@ -116,7 +117,7 @@ def test_device_setup_iterations_and_tuning(mfcfd_lib):
         dev.close()
 
 
-@pytest.mark.parametrize("kw", [dict(sweep_variant=1), dict(precision=1), dict(power=1.0)])
+@pytest.mark.parametrize("kw", [dict(sweep_variant=1), dict(power=1.0)])
 def test_device_setup_fallbacks_match(mfcfd_lib, kw):
     """Configurations the device path does not cover take the host set-up."""
     from mfcfd import cloud

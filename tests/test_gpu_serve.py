@@ -145,3 +145,30 @@ def test_malformed_request_fails_alone(mfcfd_lib):
     assert st["failed"] == 1 and st["completed"] == 2
     alone = serve.solve_alone(good, 0.6, 1.0, 10, 20, -9.0)
     assert np.array_equal(res[0]["prim"], alone["prim"])
+
+
+def test_device_setup_server_equals_host_setup(mfcfd_lib):
+    """device_setup = 1: requests set up on the device at admission give the
+    same results as the host-prepared server's (the set-up arrays are the
+    same bytes); the supersonic request falls back to the host set-up inside
+    mfcfd_create.  The reservation becomes the handle's own bytes, and every
+    byte is released at the end."""
+    from mfcfd import serve
+    chunk = 10
+    cases = _cases()
+    out = []
+    for dev in (False, True):
+        with serve.Server(chunk=chunk, setup_threads=2, device_setup=dev) as srv:
+            ids = [srv.submit(c, m, a, max_iters=60, residue_target=-1.0, **kw) for c, m, a, kw in cases]
+            res = [srv.wait(i, timeout=300) for i in ids]
+            st = srv.stats()
+        assert st["completed"] == len(cases) and st["failed"] == 0 and st["live"] == 0
+        assert st["bytes_live"] == 0
+        out.append(res)
+    for a, b in zip(*out):
+        assert a["status"] == b["status"] == 0
+        assert a["iters"] == b["iters"]
+        assert np.array_equal(a["prim"], b["prim"])
+        assert a["cl"] == b["cl"] and a["cd"] == b["cd"]
+    for (c, _, _, _), b in zip(cases, out[1]):
+        assert b["device_bytes"] > 0
