@@ -614,6 +614,7 @@ constexpr int SW_RING_DOUBLES = CHAIN_RING * 30;                    // chain: la
 constexpr int SWEEP_SMEM_BYTES = SW_T_DOUBLES * 8 + (int)sizeof(SweepStage);   // one stage
 constexpr int CHAIN_SMEM_BYTES = (SW_T_DOUBLES + SW_RING_DOUBLES) * 8 + 2 * (int)sizeof(SweepStage);
 static_assert(SW_T_DOUBLES >= SWEEP_MAX_ENTRIES * 5, "T buffer too small");
+static_assert(SW_T_DOUBLES * 8 >= SWEEP_MAX_ENTRIES * 5 * 8 + SWEEP_MAX_ENTRIES, "no room for the terms' flags");
 static_assert(SW_T_DOUBLES == G0_DOUBLES && G0_DOUBLES % 2 == 0, "a g0 block is one T buffer of 16-byte pairs");
 static_assert(SWEEP_MAX_ENTRIES <= 96, "entries are polled in three passes of 32");
 static_assert(sizeof(SweepStage) % 16 == 0 && SWEEP_SMEM_BYTES % 16 == 0 && CHAIN_SMEM_BYTES % 16 == 0,
@@ -820,6 +821,7 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
             if (!hold) st_relaxed_f64(dst, dnew);
         }
     } else {
+        double sx = 0.0, sy = 0.0, sz = 0.0, G0acc = 0.0;   // phase C's list sums
         const uint32_t need = shared ? 0u : st->need;
         const bool mine = !shared && (need >> lane) & 1u;
         const bool g0 = CHAINS && (it.info & CI_G0) != 0;   // warp-uniform
@@ -831,10 +833,18 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         }
 
         // ---- phase B
+        // The list sums of phase C run in list order from `pos`; in the shared
+        // frame they advance over the terms that have landed while later
+        // ones are still awaited, so only the terms after the last arrival
+        // remain once it lands (the additions keep their order).
+        int pos = lo;
         if (shared) {
             // lane owns entries lane, lane+32, lane+64; all their loads are in
-            // flight together, re-polling only the ones still pending
+            // flight together, re-polling only the ones still pending; a
+            // landed term's flag (past the 96 terms' values in T) tells the
+            // summing lanes it is there
             const double *src = forward ? d.dgf : d.dgb;
+            uint8_t *rdy = reinterpret_cast<uint8_t *>(T + 5 * SWEEP_MAX_ENTRIES);
             uint32_t pend = 0;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
@@ -845,33 +855,60 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
                     const double *rs = ring + 30 * ((pad >> ENT_RING_SHIFT) & 15) + 5 * (pad & 255);
 #pragma unroll
                     for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = rs[cc];
+                    rdy[j] = 1;
                 } else {
                     pend |= 1u << q;
+                    rdy[j] = 0;
                 }
             }
             int spins = 0;
-            while (pend) {
-                unsigned long long v[3][5];
+            for (;;) {
+                if (pend) {
+                    unsigned long long v[3][5];
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    if (!((pend >> q) & 1u)) continue;
-                    const int j = lane + 32 * q;
-                    // backup driver: a term from before the sweep reads dg_old
-                    const double *base = (E[j].pad & ENT_OLD) ? d.dg_old : src;
-                    const double *gs = base + DG_STRIDE * (size_t)E[j].k + DG_LIST * (E[j].pad & 255);
-                    ld_relaxed_v2(gs, v[q][0], v[q][1]);
-                    ld_relaxed_v2(gs + 2, v[q][2], v[q][3]);
-                    v[q][4] = ld_relaxed_b64(gs + 4);
+                    for (int q = 0; q < 3; ++q) {
+                        if (!((pend >> q) & 1u)) continue;
+                        const int j = lane + 32 * q;
+                        // backup driver: a term from before the sweep reads dg_old
+                        const double *base = (E[j].pad & ENT_OLD) ? d.dg_old : src;
+                        const double *gs = base + DG_STRIDE * (size_t)E[j].k + DG_LIST * (E[j].pad & 255);
+                        ld_relaxed_v2(gs, v[q][0], v[q][1]);
+                        ld_relaxed_v2(gs + 2, v[q][2], v[q][3]);
+                        v[q][4] = ld_relaxed_b64(gs + 4);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        if (!((pend >> q) & 1u) || !ready5(v[q])) continue;
+                        const int j = lane + 32 * q;
+#pragma unroll
+                        for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __longlong_as_double(v[q][cc]);
+                        rdy[j] = 1;
+                        pend &= ~(1u << q);
+                    }
+                    if (pend && !spin_continue(spins, d)) {
+                        // the wait ran out (d.err is set): the terms stay unset
+#pragma unroll
+                        for (int q = 0; q < 3; ++q)
+                            if ((pend >> q) & 1u) rdy[lane + 32 * q] = 1;
+                        pend = 0;
+                    }
                 }
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    if (!((pend >> q) & 1u) || !ready5(v[q])) continue;
-                    const int j = lane + 32 * q;
-#pragma unroll
-                    for (int cc = 0; cc < 5; ++cc) T[j * 5 + cc] = __longlong_as_double(v[q][cc]);
-                    pend &= ~(1u << q);
+                __syncwarp();
+                if (__all_sync(FULL, pend == 0)) break;
+                if (lane < 30) {
+                    while (pos < hi && rdy[pos]) {
+                        const double t = T[pos * 5 + c];
+                        if constexpr (FOLD) {
+                            G0acc = G0acc + t * E[pos].w[0];
+                        } else {
+                            sx = sx + t * E[pos].w[0];
+                            sy = sy + t * E[pos].w[1];
+                            sz = sz + t * E[pos].w[2];
+                        }
+                        ++pos;
+                    }
                 }
-                if (pend && !spin_continue(spins, d)) break;
+                __syncwarp();
             }
         } else {
             FluxPreT<R> Pn;
@@ -920,25 +957,25 @@ __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepS
         }
         __syncwarp();
 
-        // ---- phase C
+        // ---- phase C (from pos: the terms not yet summed)
         double G = 0.0;
         if constexpr (FOLD) {
             // mixed precision: each term's weight already carries the list's
             // 3x3 solve (cofactors / det, FP64, computed at set-up)
+            G = G0acc;
             if (lane < 30) {
 #pragma unroll 4
-                for (int jj = lo; jj < hi; ++jj) {
+                for (int jj = pos; jj < hi; ++jj) {
                     const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
                     G = G + t * E[jj].w[0];
                 }
             }
         } else {
-            double sx = 0.0, sy = 0.0, sz = 0.0;
             if (lane < 30) {
                 // unrolled so the next terms' shared-memory loads overlap; the
                 // additions keep their order
 #pragma unroll 4
-                for (int jj = lo; jj < hi; ++jj) {
+                for (int jj = pos; jj < hi; ++jj) {
                     const double t = shared ? T[jj * 5 + c] : T[(dd * MAX_SLOTS + ((E[jj].pad >> 8) & 255)) * 5 + c];
                     sx = sx + t * E[jj].w[0];
                     sy = sy + t * E[jj].w[1];
