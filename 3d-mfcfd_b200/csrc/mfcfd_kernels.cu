@@ -389,12 +389,13 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
 // RS: the type of the sweep inputs' fluxes (float whenever the sweeps run in
 // FP32, so that a sweep differences fluxes evaluated the same way).
 template <bool FUSED, typename R, typename RS = R>
-__global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d) {
+__global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d, int i0, int i1) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *T = smem + warp * FLUX_SMEM_PER_WARP;     // T[(dir*32 + slot)*5 + c]
     double *W = T + NDIR * MAX_SLOTS * 5;             // W[slot*3 + axis]
-    for (int i = blockIdx.x * FLUX_WARPS + warp; i < d.n; i += gridDim.x * FLUX_WARPS) {
+    // positions [i0, i1) of the visiting order (pre_order when FUSED)
+    for (int i = i0 + blockIdx.x * FLUX_WARPS + warp; i < i1; i += gridDim.x * FLUX_WARPS) {
         const int p = FUSED ? d.pre_order[i] : i;
         const int cls = d.cls[p];
         if (cls <= 2) {
@@ -1611,21 +1612,31 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         // both run.
         k_pending<<<sms * 8, 256, 0, s>>>(d, 1);
         mark(3, s);
+        const size_t fsm = FLUX_WARPS * FLUX_SMEM_PER_WARP * 8;
+        auto flux = [&](int i0, int i1, int grid, cudaStream_t on, bool high) {
+            if (dc) launch_prio(k_flux<true, double, float>, grid, FLUX_WARPS * 32, fsm, on, high, d, i0, i1);
+            else if (mixed) launch_prio(k_flux<true, float>, grid, FLUX_WARPS * 32, fsm, on, high, d, i0, i1);
+            else launch_prio(k_flux<true, double>, grid, FLUX_WARPS * 32, fsm, on, high, d, i0, i1);
+        };
+        // the first flux_lead points of the order on the whole device before
+        // the sweep starts: the sweep consumes its inputs about as fast as the
+        // flux kernel, beside it, produces them, and without this lead it
+        // polls for inputs not yet written
+        const int lead = std::min(d.flux_lead, n);
+        if (lead > 0) flux(0, lead, (lead + FLUX_WARPS - 1) / FLUX_WARPS, s, true);
         cudaEventRecord(st.fork, s);
         cudaStreamWaitEvent(st.side, st.fork, 0);
-        const size_t fsm = FLUX_WARPS * FLUX_SMEM_PER_WARP * 8;
         // a smaller grid walks the same order with its warps striding through it
-        const int fgrid = d.flux_grid > 0 && d.flux_grid < fblocks ? d.flux_grid : fblocks;
-        if (dc) launch_prio(k_flux<true, double, float>, fgrid, FLUX_WARPS * 32, fsm, st.side, false, d);
-        else if (mixed) launch_prio(k_flux<true, float>, fgrid, FLUX_WARPS * 32, fsm, st.side, false, d);
-        else launch_prio(k_flux<true, double>, fgrid, FLUX_WARPS * 32, fsm, st.side, false, d);
+        const int rblocks = (n - lead + FLUX_WARPS - 1) / FLUX_WARPS;
+        const int fgrid = d.flux_grid > 0 && d.flux_grid < rblocks ? d.flux_grid : rblocks;
+        if (lead < n) flux(lead, n, fgrid, st.side, false);
         mark(2, st.side);
         cudaEventRecord(st.join, st.side);
         sweep(1);
         mark(4, s);
         cudaStreamWaitEvent(s, st.join, 0);
     } else {
-        k_flux<false, double><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d);
+        k_flux<false, double><<<fblocks, FLUX_WARPS * 32, FLUX_WARPS * FLUX_SMEM_PER_WARP * 8, s>>>(d, 0, n);
         mark(2, s);
         k_pending<<<sms * 8, 256, 0, s>>>(d, 0);
         k_dinv_gold<<<(n + 127) / 128, 128, 0, s>>>(d);
