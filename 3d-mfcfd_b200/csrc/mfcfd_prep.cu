@@ -1359,7 +1359,9 @@ int device_setup(int device, const mfcfd_params &P, Topology &T, const double *x
             if (int rc = scan(rcnt, roff, n + 1, &ndep)) return rc;
             k_dep_fill<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], off_dir[dir], ent_dir[dir], swept, roff, rcur,
                                                    rlist);
-            k_lv_roots<<<gs, PREP_THREADS, 0, s>>>(order[dir], nsw, indeg, dt.level[dir], fa, count);
+            // one thread per point of the order (k_lv_roots has no grid-stride loop)
+            k_lv_roots<<<(nsw + PREP_THREADS - 1) / PREP_THREADS, PREP_THREADS, 0, s>>>(order[dir], nsw, indeg,
+                                                                                     dt.level[dir], fa, count);
             // every level in one block: a barrier per level instead of a launch
             k_levels_block<<<1, 1024, 0, s>>>(nsw, fa, fb, count, roff, rlist, indeg, dt.level[dir]);
             PREP_CK(cudaGetLastError());

@@ -159,3 +159,29 @@ def test_device_setup_sphere1m_equals_host(mfcfd_lib):
     finally:
         host.close()
         dev.close()
+
+
+def test_device_setup_roots_late_in_a_large_order(mfcfd_lib):
+    """Points without swept lower-alias neighbours (level 0) far into a long
+    sweep order: the 1.1M sphere with shell 60 made outer (not swept), so the
+    first points of shell 61 reached past it are roots at about 64% of the
+    order, beyond one launch-grid's worth of threads.  (A capped root launch
+    once missed them on an 830k-point wing.)"""
+    from mfcfd import cloud
+    from mfcfd.cloud import STATUS_OUTER
+    c = cloud.sphere_1m()
+    st = c.status.copy()
+    st[60 * 11500:61 * 11500] = STATUS_OUTER
+    c.status = st
+    host, dev = _pair(c)
+    try:
+        a, b = _digests(host), _digests(dev)
+        for k in ARRAYS:
+            assert a[k] == b[k], k
+        lv = dev.levels(0)
+        order_pos = np.argsort(np.argsort(dev.alias()[0]))
+        roots = np.nonzero(lv == 0)[0]
+        assert (order_pos[roots] > 650_000).any()
+    finally:
+        host.close()
+        dev.close()
