@@ -117,6 +117,14 @@ def test_prepare_needs_a_device_and_serving_helpers(mfcfd_lib, small_cloud):
     cfg = _lib.ServerConfig(device=0, max_live=0, setup_threads=0, chunk=10)
     srv = ctypes.c_void_p()
     assert L.mfcfd_server_create(ctypes.byref(cfg), ctypes.byref(srv)) == 1
+    cfg = _lib.ServerConfig(device=0, max_live=0, setup_threads=2, chunk=10, device_setup=2)
+    assert L.mfcfd_server_create(ctypes.byref(cfg), ctypes.byref(srv)) == 1
+    # the connectivity search checks its arguments before touching a device
+    x = np.zeros(4)
+    nb, cn, md = np.zeros(4, np.int32), np.zeros((4, 27), np.int32), np.zeros(4)
+    assert L.mfcfd_knn(0, 4, _lib.ptr(x), _lib.ptr(x), _lib.ptr(x), 28, _lib.ptr(nb), _lib.ptr(cn),
+                       _lib.ptr(md)) == 1
+    assert L.mfcfd_knn(0, 4, _lib.ptr(x), _lib.ptr(x), _lib.ptr(x), 3, None, _lib.ptr(cn), _lib.ptr(md)) == 1
 
 
 def test_host_memory_exhaustion_is_a_status_not_a_crash():

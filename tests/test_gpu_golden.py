@@ -22,13 +22,15 @@ def golden():
         return {k: z[k] for k in z.files}
 
 
+@pytest.mark.parametrize("gpu_setup", [0, 1])
 @pytest.mark.parametrize("sweep_mode", [0, 1, 2])
 @pytest.mark.parametrize("case", [0, 1])
-def test_gpu_matches_reference_bitwise(golden, mfcfd_lib, case, sweep_mode):
+def test_gpu_matches_reference_bitwise(golden, mfcfd_lib, case, sweep_mode, gpu_setup):
+    """gpu_setup 1: the set-up computed on the device gives the same bits."""
     from mfcfd.solver import Solver
     meta = json.loads(str(golden["meta"]))
     mach, aoa = meta["cases"][case]
-    s = Solver(golden_cloud(golden), mach, aoa, sweep_mode=sweep_mode)
+    s = Solver(golden_cloud(golden), mach, aoa, sweep_mode=sweep_mode, gpu_setup=gpu_setup)
     s.initial_conditions(golden[f"case{case}_prim0"])
     pre = f"case{case}_mfmath_"
     res = golden[pre + "res"]
