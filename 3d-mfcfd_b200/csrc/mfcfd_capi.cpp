@@ -592,16 +592,6 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
     return MFCFD_OK;
 }
 
-// Points of the flux kernel's order computed on the whole device before the
-// forward chain sweep starts.  Beside the sweep the FP64 flux kernel produces
-// the sweep's inputs about as fast as the sweep consumes them; a lead of 16%
-// keeps it ahead (1.1M sphere, FP64: 54.9 against 56.6 ms per iteration; 8%
-// 55.7, 24% 56.1).  The FP32 flux kernel of MIXED is ahead anyway, and any
-// lead only adds to the iteration (42.5 ms at 0, 43.5 at 16%).
-int flux_lead_points(int n, int precision) {
-    return precision == MFCFD_PRECISION_MIXED ? 0 : (int)((int64_t)n * 16 / 100);
-}
-
 // The handle's streams: the main stream outranks the side stream, so the
 // chain sweep's blocks are placed before the concurrent flux kernel's.
 int create_streams(mfcfd_handle *h) {
@@ -658,7 +648,6 @@ int attach_device(mfcfd_handle *h) {
         d.ch_wpb = st.ch_wpb;
         d.ch_spread = P.chain_spread;
         d.flux_grid = P.flux_blocks_per_sm > 0 ? P.flux_blocks_per_sm * device_sms(P.device) : 0;
-        d.flux_lead = flux_lead_points(n, P.precision);
         if ((rc = upload(h, &d.pre_order, st.pre))) return rc;
         for (int dir = 0; dir < 2; ++dir) {
             if ((rc = upload(h, &d.ch_ptr[dir], S.ptr[dir]))) return rc;
@@ -808,7 +797,6 @@ int create_on_device(mfcfd_handle *h, const double *x, const double *y, const do
         d.ch_wpb = wpb;
         d.ch_spread = P.chain_spread;
         d.flux_grid = P.flux_blocks_per_sm > 0 ? P.flux_blocks_per_sm * device_sms(P.device) : 0;
-        d.flux_lead = flux_lead_points(n, P.precision);
         for (int k = 0; k < 3; ++k) h->chain_terms[k] = terms[k];
         if (d.n_g0 > 0 && (rc = dalloc(h, &d.g0, (size_t)d.n_g0 * G0_DOUBLES))) return rc;
     }

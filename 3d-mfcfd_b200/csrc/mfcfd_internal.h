@@ -350,8 +350,6 @@ struct DevCloud {
     int ch_warps, ch_wpb;         // warps and warps per block
     int ch_spread;                // one chain block per SM (mfcfd_params.chain_spread)
     int flux_grid;                // blocks of the fused flux kernel; 0: one per FLUX_WARPS points
-    int flux_lead;                // points of the flux kernel's order computed before the forward
-                                  // chain sweep starts (the rest runs beside it)
     const int32_t *pre_order;     // all points, forward sweep order first (fused flux)
     const int32_t *ch_ptr[2], *ch_pts[2], *ch_own[2];
     const ChainItem *ch_items[2];

@@ -388,8 +388,17 @@ __device__ __forceinline__ void sweep_inputs_warp(const DevCloud &d, int i, int 
 // mixed precision); the offsets, weights, list sums and 3x3 solves are double.
 // RS: the type of the sweep inputs' fluxes (float whenever the sweeps run in
 // FP32, so that a sweep differences fluxes evaluated the same way).
+// Blocks of the flux kernel per SM the compiler must fit: four for the FP64
+// evaluation (128 registers, 16 warps per SM).  Beside the forward sweep it
+// then keeps ahead of the sweep, which otherwise polled for inputs not yet
+// written (1.1M points: flux 22.1 against 26.5 ms, iteration 53.0 against
+// 55.1 ms with the earlier remedy, a lead launch of the order's first 16%).
+// FP32 keeps the default: it is well ahead anyway.
+template <typename R>
+constexpr int flux_min_blocks() { return sizeof(R) == 8 ? 4 : 1; }
+
 template <bool FUSED, typename R, typename RS = R>
-__global__ void __launch_bounds__(FLUX_WARPS * 32) k_flux(DevCloud d, int i0, int i1) {
+__global__ void __launch_bounds__(FLUX_WARPS * 32, flux_min_blocks<R>()) k_flux(DevCloud d, int i0, int i1) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *T = smem + warp * FLUX_SMEM_PER_WARP;     // T[(dir*32 + slot)*5 + c]
@@ -1618,18 +1627,11 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
             else if (mixed) launch_prio(k_flux<true, float>, grid, FLUX_WARPS * 32, fsm, on, high, d, i0, i1);
             else launch_prio(k_flux<true, double>, grid, FLUX_WARPS * 32, fsm, on, high, d, i0, i1);
         };
-        // the first flux_lead points of the order on the whole device before
-        // the sweep starts: the sweep consumes its inputs about as fast as the
-        // flux kernel, beside it, produces them, and without this lead it
-        // polls for inputs not yet written
-        const int lead = std::min(d.flux_lead, n);
-        if (lead > 0) flux(0, lead, (lead + FLUX_WARPS - 1) / FLUX_WARPS, s, true);
         cudaEventRecord(st.fork, s);
         cudaStreamWaitEvent(st.side, st.fork, 0);
         // a smaller grid walks the same order with its warps striding through it
-        const int rblocks = (n - lead + FLUX_WARPS - 1) / FLUX_WARPS;
-        const int fgrid = d.flux_grid > 0 && d.flux_grid < rblocks ? d.flux_grid : rblocks;
-        if (lead < n) flux(lead, n, fgrid, st.side, false);
+        const int fgrid = d.flux_grid > 0 && d.flux_grid < fblocks ? d.flux_grid : fblocks;
+        flux(0, n, fgrid, st.side, false);
         mark(2, st.side);
         cudaEventRecord(st.join, st.side);
         sweep(1);

@@ -520,10 +520,9 @@ def main():
                         "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                 "roofline": roofline, "cpu_baseline": cpu_base, "clocks": clocks, "mixed": mixed,
                 "serving": serving, "serving_converged": serving_conv, "setup": setup,
-                # + k_g0 when the cloud has points outside the shared frame, + the flux
-                # kernel's lead launch (FP64 chain schedule)
-                "gpu_launches": (KERNELS_PER_ITER[args.sweep_mode] + (1 if info.get("g0_points") else 0)
-                                 + (1 if args.sweep_mode == 2 else 0)) * args.steps}
+                # + k_g0 when the cloud has points outside the shared frame
+                "gpu_launches": (KERNELS_PER_ITER[args.sweep_mode] + (1 if info.get("g0_points") else 0))
+                                * args.steps}
         print(json.dumps(line), flush=True)
     if s is not None:
         s.close()
