@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -592,10 +593,29 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
     return MFCFD_OK;
 }
 
+// The device's default memory pool (every handle's stream-ordered memory)
+// keeps what handles free for the next ones instead of unmapping it at the
+// next synchronisation: a new handle's set-up then finds its memory mapped
+// (1.1M points: 0.46 s, against up to 1.2 s when it had to be mapped again).
+// cudaMemPoolTrimTo on the pool returns it.  Set once per device.
+void keep_pool_memory(int device) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (std::find(done.begin(), done.end(), device) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done.push_back(device);
+}
+
 // The handle's streams: the main stream outranks the side stream, so the
 // chain sweep's blocks are placed before the concurrent flux kernel's.
 int create_streams(mfcfd_handle *h) {
     if (cudaSetDevice(h->P.device) != cudaSuccess) return fail(h, MFCFD_ERR_CUDA, "cudaSetDevice failed");
+    keep_pool_memory(h->P.device);
     int least = 0, greatest = 0;
     CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     CK(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatest));
