@@ -583,7 +583,7 @@ int stage_host(mfcfd_handle *h, const double *x, const double *y, const double *
         // schedule itself is built when first needed (attach_device), so a
         // warp count set before then costs one build
         if (P.chain_warps < 0) return fail(h, MFCFD_ERR_ARG, "chain_warps must not be negative");
-        const int want = P.chain_warps > 0 ? P.chain_warps : 2 * h->T.max_level_width;
+        const int want = P.chain_warps > 0 ? P.chain_warps : std::max(1, 2 * h->T.max_level_width);
         int blocks = 0;
         if (P.chain_spread < 0 || P.chain_spread > 1) return fail(h, MFCFD_ERR_ARG, "chain_spread must be 0 or 1");
         st->ch_w = chain_shape(P.device, want, P.chain_spread, &st->ch_wpb, &blocks);
@@ -807,7 +807,7 @@ int create_on_device(mfcfd_handle *h, const double *x, const double *y, const do
             for (int32_t &v : *a) v = T.perm[v];
     }
     if (P.sweep_mode == MFCFD_SWEEP_CHAINS) {
-        const int want = P.chain_warps > 0 ? P.chain_warps : 2 * T.max_level_width;
+        const int want = P.chain_warps > 0 ? P.chain_warps : std::max(1, 2 * T.max_level_width);
         int wpb = 0, blocks = 0;
         const int w = chain_shape(P.device, want, P.chain_spread, &wpb, &blocks);
         if (w < 1) return fail(h, MFCFD_ERR_CUDA, "chain sweep kernel cannot be resident");

@@ -182,3 +182,57 @@ def test_device_setup_roots_late_in_a_large_order(mfcfd_lib):
     finally:
         host.close()
         dev.close()
+
+
+def _ragged_cloud(outer_all=False, seed=11):
+    """A small random cloud with ragged neighbour lists (0 to 26 entries), a
+    few wall points and an outer layer; with outer_all every point is outer,
+    so nothing is swept."""
+    from mfcfd import cloud
+    from mfcfd.cloud import STATUS_INTERIOR, STATUS_OUTER, STATUS_WALL, PointCloud
+    rng = np.random.default_rng(seed)
+    n = 400
+    pts = rng.uniform(-1.0, 1.0, size=(n, 3))
+    nbhs, conn, md = cloud.knn(pts[:, 0], pts[:, 1], pts[:, 2], 26, device=-1)
+    nbhs = rng.integers(0, 27, size=n).astype(np.int32)
+    nbhs[0] = 26                                   # the search starts at point 1
+    conn[np.arange(conn.shape[1])[None, :] >= nbhs[:, None]] = 0
+    r = np.sqrt((pts * pts).sum(axis=1))
+    status = np.full(n, STATUS_INTERIOR, dtype=np.int32)
+    status[r > 0.95] = STATUS_OUTER
+    status[:20] = STATUS_WALL
+    if outer_all:
+        status[:] = STATUS_OUTER
+    tan1 = np.tile([1.0, 0.0, 0.0], (n, 1))
+    tan2 = np.tile([0.0, 1.0, 0.0], (n, 1))
+    nor = np.tile([0.0, 0.0, 1.0], (n, 1))
+    return PointCloud(status=status, x=pts[:, 0].copy(), y=pts[:, 1].copy(), z=pts[:, 2].copy(), tan1=tan1,
+                      tan2=tan2, nor=nor, nbhs=nbhs, conn=conn, min_dist=md, name="ragged")
+
+
+@pytest.mark.parametrize("outer_all", [False, True])
+@pytest.mark.parametrize("sweep_mode", [0, 2])
+def test_device_setup_ragged_and_empty(mfcfd_lib, outer_all, sweep_mode):
+    """Ragged neighbour counts (some points with none) and a cloud whose
+    sweeps visit no point: the same arrays, or the same error, either way."""
+    from mfcfd._lib import MfcfdError
+    from mfcfd.solver import Solver
+    c = _ragged_cloud(outer_all)
+    try:
+        host = Solver(c, 0.5, 1.0, gpu_setup=0, sweep_mode=sweep_mode)
+    except MfcfdError as e:
+        with pytest.raises(MfcfdError) as g:
+            Solver(c, 0.5, 1.0, gpu_setup=1, sweep_mode=sweep_mode)
+        assert str(g.value) == str(e)
+        return
+    dev = Solver(c, 0.5, 1.0, gpu_setup=1, sweep_mode=sweep_mode)
+    try:
+        a, b = _digests(host), _digests(dev)
+        for k in ARRAYS:
+            assert a[k] == b[k], k
+        for d in (0, 1):
+            assert np.array_equal(host.levels(d), dev.levels(d))
+        assert host.info()["n_levels_forward"] == dev.info()["n_levels_forward"]
+    finally:
+        host.close()
+        dev.close()
