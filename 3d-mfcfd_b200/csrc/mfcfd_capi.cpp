@@ -74,6 +74,10 @@ struct mfcfd_handle {
     // query arrays (stencils, alias, levels) from dt on demand
     bool dev_setup = false;
     DevTopology dt;
+    // mixed precision: sweep terms per direction, and (MIXED_DC) their
+    // unfolded weights, which the switch to FP64 puts back
+    int64_t n_ent[2] = {0, 0};
+    double *w_saved[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -381,6 +385,8 @@ int apply_chain_schedule(mfcfd_handle *h, int want, int *warps) {
                                             cudaMemcpyHostToDevice, h->stream);
             if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpyAsync");
         }
+    // the host's terms carry the unfolded weights
+    if (d.precision != MFCFD_PRECISION_FP64) CK(launch_fold_terms(d, h->w_saved, true, h->stream));
     d.ch_warps = w;
     d.ch_wpb = wpb;
     d.ch_spread = h->P.chain_spread;
@@ -716,6 +722,8 @@ int attach_device(mfcfd_handle *h) {
     d.n_wall = (int)T.wall_idx.size();
     d.n_swept = (int)T.fwd_lvl_pts.size();
     d.max_width = T.max_level_width;
+    h->n_ent[0] = (int64_t)T.fwd_ent.size();
+    h->n_ent[1] = (int64_t)T.bwd_ent.size();
     return attach_state(h);
 }
 
@@ -746,6 +754,10 @@ int attach_state(mfcfd_handle *h) {
         if ((rc = upload(h, &d.ss_pts, T.ss_pts))) return rc;
         if ((rc = upload(h, &d.ss_src, T.ss_src))) return rc;
     }
+    if (P.precision == MFCFD_PRECISION_MIXED_DC) {
+        AL(h->w_saved[0], 3 * (size_t)std::max<int64_t>(h->n_ent[0], 1));
+        AL(h->w_saved[1], 3 * (size_t)std::max<int64_t>(h->n_ent[1], 1));
+    }
 #undef AL
     d.U = h->U_buf[0];
     d.q = h->q_buf[0];
@@ -757,6 +769,8 @@ int attach_state(mfcfd_handle *h) {
     CK(cudaMemsetAsync(d.flux_res, 0, n5 * 8, h->stream));
     CK(cudaMemsetAsync(d.dinv, 0, (size_t)n * 8, h->stream));
     CK(cudaMemsetAsync(d.res_sqr, 0, (size_t)n * 8, h->stream));
+    if (P.precision != MFCFD_PRECISION_FP64 && P.sweep_mode == MFCFD_SWEEP_CHAINS)
+        CK(launch_fold_terms(d, h->w_saved, true, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return MFCFD_OK;
 }
@@ -826,6 +840,8 @@ int create_on_device(mfcfd_handle *h, const double *x, const double *y, const do
         h->perm_dev = const_cast<int32_t *>(pd);
         if ((rc = dalloc(h, &h->xfer, (size_t)n * 5))) return rc;
     }
+    h->n_ent[0] = h->dt.n_ent[0];
+    h->n_ent[1] = h->dt.n_ent[1];
     return attach_state(h);
 }
 
@@ -1262,10 +1278,23 @@ int mfcfd_set_precision(mfcfd_handle *h, int32_t precision) {
         if (precision != MFCFD_PRECISION_FP64 && precision != MFCFD_PRECISION_MIXED_DC)
             return fail(h, MFCFD_ERR_ARG, "only FP64 and MIXED_DC can be switched to");
         if (h->P.precision == MFCFD_PRECISION_MIXED)
-            return fail(h, MFCFD_ERR_UNSUPPORTED, "a MIXED handle's sweep weights are folded at set-up");
+            return fail(h, MFCFD_ERR_UNSUPPORTED, "a MIXED handle keeps only its folded sweep weights");
         if (precision == MFCFD_PRECISION_MIXED_DC && h->P.sweep_mode != MFCFD_SWEEP_CHAINS)
             return fail(h, MFCFD_ERR_UNSUPPORTED, "mixed precision requires the chain sweep schedule");
         if (h->pending_chunk) return fail(h, MFCFD_ERR_ARG, "a launch is pending on this handle");
+        if (precision == h->P.precision) return MFCFD_OK;
+        if (h->stream) {
+            // MIXED_DC sweeps read folded weights, FP64 ones the three
+            // weighted offsets: put back the saved ones, or save and fold
+            if (precision == MFCFD_PRECISION_MIXED_DC)
+                for (int dir = 0; dir < 2; ++dir)
+                    if (!h->w_saved[dir]) {
+                        int rc = dalloc(h, &h->w_saved[dir], 3 * (size_t)std::max<int64_t>(h->n_ent[dir], 1));
+                        if (rc) return rc;
+                    }
+            CK(launch_fold_terms(h->d, h->w_saved, precision == MFCFD_PRECISION_MIXED_DC, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
         h->P.precision = precision;
         h->d.precision = precision;
         drop_graphs(h);                    // their launches name the other kernels

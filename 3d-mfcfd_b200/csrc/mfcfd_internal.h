@@ -208,6 +208,7 @@ struct DevTopology {
     std::vector<int32_t> h_level[2], h_lpts[2], h_coff[2], h_cand[2];
     std::vector<int32_t> g0_pts;
     int64_t split_overflows = 0;
+    int64_t n_ent[2] = {0, 0};    // sweep terms per direction
     int max_width = 0;
 };
 bool device_setup_supported(const mfcfd_params &P, const Topology &T);
@@ -423,6 +424,11 @@ int io_write_residue(const char *path, int32_t t0, int32_t iters, const double *
 // threads, the same arrays either way.
 int knn_connectivity(int device, int n, const double *x, const double *y, const double *z, int k, int32_t *nbhs,
                      int32_t *conn, double *min_dist, std::string &err);
+
+// Mixed precision: fold each sweep term's 3x3 solve into its weight (saving
+// the three weights first into saved[dir], 3 per term, when non-null), or
+// put the saved weights back (fold false).
+cudaError_t launch_fold_terms(const DevCloud &d, double *const saved[2], bool fold, cudaStream_t s);
 
 // Allocation-free residual (mfcfd_residual_noalloc); the current device must
 // be the handle's.

@@ -768,7 +768,8 @@ __global__ void __launch_bounds__(128) k_g0(DevCloud d) {
 // chain kernel issued as a cp.async group before this call (followed by one
 // more group, the next point's stage, when g0_newer); phase B waits for it.
 // FOLD (mixed precision): each term's weight carries its list's 3x3 solve
-// (set-up folds them), so phase C sums weight x term; otherwise phase C sums
+// (folded when the handle is attached), so phase C sums weight x term;
+// otherwise phase C sums
 // the three weighted moments in FP64 and solves, as the reference does.
 template <int MODE, typename R, bool FOLD = false>
 __device__ void sweep_point(const DevCloud &d, const ChainItem &it, const SweepStage *st, bool forward, int lane,
@@ -1108,8 +1109,8 @@ constexpr int chain_min_blocks() {
 }
 
 // R: the type of the sweep's flux evaluations; FOLD: folded term weights
-// (MFCFD_PRECISION_MIXED).  FP64 <double, false>; mixed <float, true>;
-// defect correction <float, false>.
+// (MFCFD_PRECISION_MIXED and MIXED_DC).  FP64 <double, false>; mixed and
+// defect correction <float, true>.
 template <int WPB, typename R, bool FOLD>
 __global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, FOLD>()) k_sweep_chain(DevCloud d, int forward) {
     extern __shared__ double smem[];
@@ -1329,6 +1330,52 @@ int device_sms(int device) {
     return cache[device];
 }
 
+// Mixed precision (MIXED, MIXED_DC): each sweep term's weight with its list's
+// 3x3 least-squares solve folded in.  The list's derivative is num(axis,
+// moments, sum w_j t_j) / det, linear in the sums, so every term gets one
+// weight (cofactors . w_j) / det, in FP64, and the sweep sums w_j t_j
+// directly.  fold: the three weights are saved first when `saved` is given
+// (3 per term), then replaced; !fold: put back from `saved`.
+__global__ void k_fold_terms(DevCloud d, int dir, double *saved, int fold) {
+    const int *off = dir == 0 ? d.fwd_off : d.bwd_off;
+    SweepEntry *ent = const_cast<SweepEntry *>(dir == 0 ? d.fwd_ent : d.bwd_ent);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.n; p += gridDim.x * blockDim.x) {
+        for (int e = off[p]; e < off[p + 1]; ++e) {
+            SweepEntry &E = ent[e];
+            if (E.pad & ENT_COPY) continue;
+            if (!fold) {
+                E.w[0] = saved[3 * (size_t)e];
+                E.w[1] = saved[3 * (size_t)e + 1];
+                E.w[2] = saved[3 * (size_t)e + 2];
+                continue;
+            }
+            if (saved) {
+                saved[3 * (size_t)e] = E.w[0];
+                saved[3 * (size_t)e + 1] = E.w[1];
+                saved[3 * (size_t)e + 2] = E.w[2];
+            }
+            const int dd = E.pad & 255;
+            const bool outer_zp = d.sweep_variant == MFCFD_SWEEPS_BACKUP && d.cls[p] == CLS_OUTER && dd == 4;
+            const double *g = d.geo + (size_t)p * GEO_STRIDE + (outer_zp ? 5 : dd) * 8;
+            const double xx = g[G_XX], yy = g[G_YY], zz = g[G_ZZ], xy = g[G_XY], yz = g[G_YZ], zx = g[G_ZX];
+            double a, b, c;
+            if (dd / 2 == 0) { a = yy * zz - yz * yz; b = -(xy * zz - zx * yz); c = xy * yz - zx * yy; }
+            else if (dd / 2 == 1) { a = -(xy * zz - zx * yz); b = xx * zz - zx * zx; c = -(xx * yz - xy * zx); }
+            else { a = xy * yz - zx * yy; b = -(xx * yz - zx * xy); c = xx * yy - xy * xy; }
+            const double w = (a * E.w[0] + b * E.w[1] + c * E.w[2]) / g[G_DET];
+            E.w[0] = w;
+            E.w[1] = 0.0;
+            E.w[2] = 0.0;
+        }
+    }
+}
+
+cudaError_t launch_fold_terms(const DevCloud &d, double *const saved[2], bool fold, cudaStream_t s) {
+    const int grid = (d.n + 255) / 256;
+    for (int dir = 0; dir < 2; ++dir) k_fold_terms<<<grid, 256, 0, s>>>(d, dir, saved[dir], fold ? 1 : 0);
+    return cudaGetLastError();
+}
+
 int reduction_blocks(int n) {
     int b = (n + 4095) / 4096;
     return b < 1 ? 1 : (b > 1024 ? 1024 : b);
@@ -1421,8 +1468,6 @@ static void set_attributes(int device) {
     cudaFuncSetAttribute(k_sweep_chain<8, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     cudaFuncSetAttribute(k_sweep_chain<4, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
     cudaFuncSetAttribute(k_sweep_chain<8, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
-    cudaFuncSetAttribute(k_sweep_chain<4, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
-    cudaFuncSetAttribute(k_sweep_chain<8, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     done[device] = true;
 }
 
@@ -1447,12 +1492,10 @@ int chain_block_slots(int device, int wpb, int precision, int spread) {
     int per_sm = 0;
     cudaError_t e;
     if (w8)
-        e = m == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, float, true>, 256, chain_smem<8>())
-          : m == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, float, false>, 256, chain_smem<8>())
+        e = m != 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, float, true>, 256, chain_smem<8>())
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<8, double, false>, 256, chain_smem<8>());
     else
-        e = m == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, float, true>, 128, chain_smem<4>())
-          : m == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, float, false>, 128, chain_smem<4>())
+        e = m != 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, float, true>, 128, chain_smem<4>())
                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chain<4, double, false>, 128, chain_smem<4>());
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
@@ -1576,10 +1619,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         if (chains) {
             const int blocks = (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb;
             const int csm = chain_smem_bytes(d.ch_wpb, d.ch_spread);
-            if (dc) {
-                if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float, false>, blocks, 4 * 32, csm, s, true, d, forward);
-                else launch_prio(k_sweep_chain<8, float, false>, blocks, 8 * 32, csm, s, true, d, forward);
-            } else if (mixed) {
+            if (mixed) {   // MIXED and MIXED_DC: folded weights
                 if (d.ch_wpb == 4) launch_prio(k_sweep_chain<4, float, true>, blocks, 4 * 32, csm, s, true, d, forward);
                 else launch_prio(k_sweep_chain<8, float, true>, blocks, 8 * 32, csm, s, true, d, forward);
             } else {

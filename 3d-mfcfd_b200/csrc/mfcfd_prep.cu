@@ -778,30 +778,6 @@ __global__ void k_ent_fill(int nsw, bool forward, const int32_t *order, const in
     }
 }
 
-// mixed precision: each sweep term's weight with its list's 3x3
-// least-squares solve folded in, (cofactors . w) / det, as build_topology's
-// fold (alias driver: the term's own list row)
-__global__ void k_fold(int nsw, const int32_t *order, const int32_t *off, const double *geo, SweepEntry *ent) {
-    GRID_STRIDE(t, (size_t)nsw) {
-        const int p = order[t];
-        for (int e = off[p]; e < off[p + 1]; ++e) {
-            SweepEntry &E = ent[e];
-            if (E.pad & ENT_COPY) continue;
-            const int d = E.pad & 255;
-            const double *g = geo + (size_t)p * GEO_STRIDE + d * 8;
-            const double xx = g[G_XX], yy = g[G_YY], zz = g[G_ZZ], xy = g[G_XY], yz = g[G_YZ], zx = g[G_ZX];
-            double a, b, c;
-            if (d / 2 == 0) { a = yy * zz - yz * yz; b = -(xy * zz - zx * yz); c = xy * yz - zx * yy; }
-            else if (d / 2 == 1) { a = -(xy * zz - zx * yz); b = xx * zz - zx * zx; c = -(xx * yz - xy * zx); }
-            else { a = xy * yz - zx * yy; b = -(xx * yz - zx * xy); c = xx * yy - xy * xy; }
-            const double w = (a * E.w[0] + b * E.w[1] + c * E.w[2]) / g[G_DET];
-            E.w[0] = w;
-            E.w[1] = 0.0;
-            E.w[2] = 0.0;
-        }
-    }
-}
-
 // levels by Kahn's layering over the sweep terms whose producer is swept
 __global__ void k_dep_count(int nsw, const int32_t *order, const int32_t *off, const SweepEntry *ent,
                             const uint8_t *swept, int32_t *indeg, int32_t *rcnt) {
@@ -1332,10 +1308,7 @@ int device_setup(int device, const mfcfd_params &P, Topology &T, const double *x
             err = "a point reads more than " + std::to_string(SWEEP_MAX_ENTRIES) + " sweep terms";
             return MFCFD_ERR_STENCIL;
         }
-        if (P.precision == MFCFD_PRECISION_MIXED && nsw > 0) {
-            k_fold<<<gs, PREP_THREADS, 0, s>>>(nsw, order[dir], off_dir[dir], geo, ent_dir[dir]);
-            PREP_CK(cudaGetLastError());
-        }
+        dt.n_ent[dir] = ne;
 
         // levels: the longest path over swept producers (Kahn's layering)
         DS_KEEP(dt.level[dir], n);

@@ -687,36 +687,6 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
         return MFCFD_ERR_STENCIL;
     }
 
-    // ---- mixed precision: fold each sweep list's 3x3 least-squares solve
-    // into its terms.  The list's derivative is num(axis, moments, sum w_j t_j)
-    // / det, linear in the sums, so every term gets one weight
-    // (cofactors . w_j) / det (FP64) and the sweep sums w_j t_j directly.
-    if (P.precision == MFCFD_PRECISION_MIXED) {
-        auto fold = [&](const std::vector<int32_t> &off, std::vector<SweepEntry> &ent) {
-            parallel_for(n, [&](int p) {
-                for (int e = off[p]; e < off[p + 1]; ++e) {
-                    SweepEntry &E = ent[e];
-                    if (E.pad & ENT_COPY) continue;
-                    const int d = E.pad & 255;
-                    const int row = (backup && T.cls[p] == CLS_OUTER && d == 4) ? 5 : d;
-                    const double *g = &T.geo[(size_t)p * GEO_STRIDE + row * 8];
-                    const double xx = g[G_XX], yy = g[G_YY], zz = g[G_ZZ], xy = g[G_XY], yz = g[G_YZ],
-                                 zx = g[G_ZX];
-                    double a, b, c;
-                    if (d / 2 == 0) { a = yy * zz - yz * yz; b = -(xy * zz - zx * yz); c = xy * yz - zx * yy; }
-                    else if (d / 2 == 1) { a = -(xy * zz - zx * yz); b = xx * zz - zx * zx; c = -(xx * yz - xy * zx); }
-                    else { a = xy * yz - zx * yy; b = -(xx * yz - zx * xy); c = xx * yy - xy * xy; }
-                    const double w = (a * E.w[0] + b * E.w[1] + c * E.w[2]) / g[G_DET];
-                    E.w[0] = w;
-                    E.w[1] = 0.0;
-                    E.w[2] = 0.0;
-                }
-            });
-        };
-        fold(T.fwd_off, T.fwd_ent);
-        fold(T.bwd_off, T.bwd_ent);
-    }
-
     // ---- shared interior frame: lets producers publish flux increments
     T.shared_frame = 0;
     if (!T.interior_idx.empty()) {

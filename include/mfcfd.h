@@ -356,8 +356,11 @@ int mfcfd_residual_noalloc(mfcfd_handle *h, double *res_new);
  * density residual and then slows, because its FP32 sweeps resolve
  * increments only to FP32; switching to FP64 for the last part of a solve
  * (a "polish") reaches a 1e-6 drop in FP64's iteration count.  The state
- * and the residual reference carry over.  Handles created MIXED (folded
- * sweep weights) cannot switch.
+ * and the residual reference carry over.  A MIXED_DC handle sweeps with
+ * each list's 3x3 solve folded into its terms' weights and keeps the
+ * unfolded weights (24 bytes per sweep term), which the switch to FP64 puts
+ * back bit for bit.  Handles created MIXED (folded weights only) cannot
+ * switch.
  */
 int mfcfd_set_precision(mfcfd_handle *h, int32_t precision);
 

@@ -136,9 +136,11 @@ def test_defect_correction_with_polish_converges_like_fp64(mfcfd_lib):
 
 
 def test_precision_switch(mfcfd_lib):
-    """FP64 and MIXED_DC handles switch either way between iterations; a
-    MIXED handle (folded sweep weights) refuses; switching to FP64 before the
-    first iteration gives the plain FP64 bits."""
+    """FP64 and MIXED_DC handles switch either way between iterations: a
+    MIXED_DC handle sweeps with folded weights and keeps the unfolded ones,
+    which the switch to FP64 puts back bit for bit.  A MIXED handle (folded
+    weights only) refuses; switching to FP64 before the first iteration gives
+    the plain FP64 bits."""
     from mfcfd import _lib, cloud
     from mfcfd.solver import Solver
     c = cloud.small_sphere()
@@ -147,11 +149,16 @@ def test_precision_switch(mfcfd_lib):
     ha = a.q_lskum(5)
     b = Solver(c, 0.8, 2.0, precision=_lib.PRECISION_MIXED_DC)
     b.initial_conditions()
+    assert b.digest("fwd_ent") != a.digest("fwd_ent")          # folded weights
     b.set_precision(_lib.PRECISION_FP64)
+    assert b.digest("fwd_ent") == a.digest("fwd_ent") and b.digest("bwd_ent") == a.digest("bwd_ent")
     hb = b.q_lskum(5)
     assert np.array_equal(ha, hb)
     assert np.array_equal(a.get(mfcfd_lib.FIELD_PRIM), b.get(mfcfd_lib.FIELD_PRIM))
     b.set_precision(_lib.PRECISION_MIXED_DC)
+    d = Solver(c, 0.8, 2.0, precision=_lib.PRECISION_MIXED_DC)
+    assert b.digest("fwd_ent") == d.digest("fwd_ent") and b.digest("bwd_ent") == d.digest("bwd_ent")
+    d.close()
     assert np.all(np.isfinite(b.q_lskum(5, t0=6)[:, 0]))
     m = Solver(c, 0.8, 2.0, precision=_lib.PRECISION_MIXED)
     with pytest.raises(_lib.MfcfdError):
