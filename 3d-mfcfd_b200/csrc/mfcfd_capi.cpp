@@ -1219,6 +1219,7 @@ int mfcfd_get_info(mfcfd_handle *h, mfcfd_info *info) {
                                                       h->P.chain_spread)
                         : 0;
             info->chain_slot_capacity = chain_slot_capacity(h->P.device);
+            info->chain_warps_per_block = wpb;
             if (!info->chain_warps) info->chain_warps = w;
             info->g0_points = (int32_t)h->T.g0_pts.size();
         }
@@ -1390,6 +1391,180 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
             if (rc && first_err == MFCFD_OK) first_err = rc;
             done[i] += chunk_of[i];
             if (done[i] < iters) ready.push_back(i);
+        }
+        return first_err;
+    });
+}
+
+namespace {
+
+// Streams and events of one mfcfd_run_group call, released on every path.
+struct GroupRun {
+    cudaStream_t s = nullptr;
+    cudaEvent_t start = nullptr, bwd = nullptr;
+    struct Graph {
+        int chunk;
+        std::vector<int> cur;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    ~GroupRun() {
+        if (s) cudaStreamSynchronize(s);
+        for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+        if (start) cudaEventDestroy(start);
+        if (bwd) cudaEventDestroy(bwd);
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+// The launches of `chunk` lockstep iterations of a group on gr.s: per
+// iteration every handle's ITER_PRE on its own streams, the group's forward
+// sweep once all of them may start, its backward sweep once every flux
+// residual has ended, then every handle's ITER_POST.  All the handles'
+// streams join gr.s at the end.
+cudaError_t launch_group_chunk(mfcfd_handle *const *hs, int count, int chunk, GroupRun &gr, ChainGroup &G) {
+    const DevCloud &d0 = hs[0]->d;
+    cudaError_t e = cudaEventRecord(gr.start, gr.s);
+    for (int i = 0; i < count && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(hs[i]->stream, gr.start, 0);
+    for (int j = 0; j < chunk && e == cudaSuccess; ++j) {
+        for (int i = 0; i < count && e == cudaSuccess; ++i) {
+            mfcfd_handle *h = hs[i];
+            DevCloud &dc = G.cloud[i];
+            dc = h->d;
+            dc.U = h->U_buf[h->cur];
+            dc.q = h->q_buf[h->cur];
+            const IterStreams st{h->stream, h->side, h->fork, h->join};
+            e = launch_iteration(dc, j, st, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], nullptr, ITER_PRE);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(gr.s, h->fork, 0);
+        }
+        if (e == cudaSuccess) e = launch_chain_group(G, d0.ch_wpb, d0.precision, d0.ch_spread, 1, gr.s);
+        for (int i = 0; i < count && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(gr.s, hs[i]->join, 0);
+        if (e == cudaSuccess) e = launch_chain_group(G, d0.ch_wpb, d0.precision, d0.ch_spread, 0, gr.s);
+        if (e == cudaSuccess) e = cudaEventRecord(gr.bwd, gr.s);
+        for (int i = 0; i < count && e == cudaSuccess; ++i) {
+            mfcfd_handle *h = hs[i];
+            const IterStreams st{h->stream, h->side, h->fork, h->join};
+            e = cudaStreamWaitEvent(h->stream, gr.bwd, 0);
+            if (e == cudaSuccess)
+                e = launch_iteration(G.cloud[i], j, st, h->U_buf[1 - h->cur], h->q_buf[1 - h->cur], nullptr,
+                                     ITER_POST);
+            h->last = h->cur;
+            h->cur = 1 - h->cur;
+        }
+    }
+    for (int i = 0; i < count && e == cudaSuccess; ++i) {
+        e = cudaEventRecord(hs[i]->batch_ev, hs[i]->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(gr.s, hs[i]->batch_ev, 0);
+    }
+    return e;
+}
+
+}  // namespace
+
+int mfcfd_run_group(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, int32_t iters, double *res_hist,
+                    int32_t *status) {
+    return host_guard(hs && count > 0 && hs[0] ? &hs[0]->err : nullptr, [&]() -> int {
+        if (!hs || count < 1 || count > MFCFD_GROUP_MAX_CLOUDS || !t0 || iters < 0) return MFCFD_ERR_ARG;
+        const int dev = hs[0] ? hs[0]->P.device : -1;
+        for (int32_t i = 0; i < count; ++i) {
+            mfcfd_handle *h = hs[i];
+            if (!h || !h->stream || !h->have_state || h->P.device != dev || h->pending_chunk) return MFCFD_ERR_ARG;
+            for (int32_t j = 0; j < i; ++j)
+                if (hs[j] == h) return MFCFD_ERR_ARG;   // each handle once
+            if (status) status[i] = MFCFD_OK;
+        }
+        mfcfd_handle *h0 = hs[0];
+        const DevCloud &d0 = h0->d;
+        int slots = 0;
+        for (int32_t i = 0; i < count; ++i) {
+            const mfcfd_handle *h = hs[i];
+            const DevCloud &d = h->d;
+            if (d.sweep_mode != MFCFD_SWEEP_CHAINS)
+                return fail(h0, MFCFD_ERR_UNSUPPORTED, "a group runs chain-schedule handles only");
+            if (d.ch_wpb != d0.ch_wpb || d.ch_spread != d0.ch_spread ||
+                (d.precision == MFCFD_PRECISION_FP64) != (d0.precision == MFCFD_PRECISION_FP64))
+                return fail(h0, MFCFD_ERR_UNSUPPORTED,
+                            "a group's handles share one chain block shape, chain_spread and precision class");
+            if (h->profiling) return fail(h0, MFCFD_ERR_UNSUPPORTED, "phase timing is per handle, not in a group");
+            slots += (d.ch_warps + d.ch_wpb - 1) / d.ch_wpb * chain_block_slots(dev, d.ch_wpb, d.precision, d.ch_spread);
+        }
+        mfcfd_handle *const h = h0;        // errors of the group's own calls
+        if (cudaSetDevice(dev) != cudaSuccess) return MFCFD_ERR_CUDA;
+        if (slots > chain_slot_capacity(dev))
+            return fail(h0, MFCFD_ERR_UNSUPPORTED,
+                        "the group's chain sweeps (" + std::to_string(slots) + " slots) do not fit the device (" +
+                            std::to_string(chain_slot_capacity(dev)) + ")");
+        if (!chain_group_fits(dev, d0.ch_wpb, d0.precision, d0.ch_spread))
+            return fail(h, MFCFD_ERR_UNSUPPORTED, "the group sweep kernel holds fewer blocks per SM than a handle's");
+        for (int32_t i = 0; i < count; ++i)
+            if (!hs[i]->batch_ev && cudaEventCreateWithFlags(&hs[i]->batch_ev, cudaEventDisableTiming) != cudaSuccess)
+                return cuda_fail(hs[i], cudaGetLastError(), "cudaEventCreateWithFlags");
+        prepare_launches(dev);
+        auto G = std::make_unique<ChainGroup>();
+        G->count = count;
+        G->block_start[0] = 0;
+        for (int32_t i = 0; i < count; ++i)
+            G->block_start[i + 1] = G->block_start[i] + (hs[i]->d.ch_warps + d0.ch_wpb - 1) / d0.ch_wpb;
+        GroupRun gr;
+        int lo = 0, hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        CK(cudaStreamCreateWithPriority(&gr.s, cudaStreamNonBlocking, hi));
+        CK(cudaEventCreateWithFlags(&gr.start, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&gr.bwd, cudaEventDisableTiming));
+        int res_cap = 1 << 30;
+        bool graphs = true;
+        for (int32_t i = 0; i < count; ++i) {
+            res_cap = std::min(res_cap, std::max(hs[i]->res_cap, 1));
+            graphs = graphs && hs[i]->P.graphs >= 1 && !hs[i]->graphs_off;
+        }
+        int first_err = MFCFD_OK;
+        for (int32_t done = 0; done < iters;) {
+            const int chunk = std::min<int32_t>(iters - done, res_cap);
+            for (int32_t i = 0; i < count; ++i) hs[i]->res_valid = false;
+            std::vector<int> cur(count), last(count);
+            for (int32_t i = 0; i < count; ++i) cur[i] = hs[i]->cur, last[i] = hs[i]->last;
+            GroupRun::Graph *g = nullptr;
+            for (auto &x : gr.graphs)
+                if (x.chunk == chunk && x.cur == cur) g = &x;
+            if (!g && graphs) {
+                cudaGraph_t graph = nullptr;
+                cudaGraphExec_t exec = nullptr;
+                cudaError_t e = cudaStreamBeginCapture(gr.s, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    const cudaError_t el = launch_group_chunk(hs, count, chunk, gr, *G);
+                    e = cudaStreamEndCapture(gr.s, &graph);
+                    if (e == cudaSuccess) e = el;
+                }
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                for (int32_t i = 0; i < count; ++i) hs[i]->cur = cur[i], hs[i]->last = last[i];
+                if (e == cudaSuccess && exec) {
+                    gr.graphs.push_back({chunk, cur, exec});
+                    g = &gr.graphs.back();
+                } else {
+                    (void)cudaGetLastError();   // launch one by one from here on
+                    graphs = false;
+                }
+            }
+            if (g) {
+                CK(cudaGraphLaunch(g->exec, gr.s));
+                for (int32_t i = 0; i < count; ++i) {
+                    hs[i]->last = (chunk & 1) ? cur[i] : 1 - cur[i];
+                    hs[i]->cur = (chunk & 1) ? 1 - cur[i] : cur[i];
+                }
+            } else {
+                CK(launch_group_chunk(hs, count, chunk, gr, *G));
+            }
+            CK(cudaStreamSynchronize(gr.s));
+            for (int32_t i = 0; i < count; ++i) {
+                int st = MFCFD_OK;
+                double *rh = res_hist ? res_hist + 2 * ((size_t)i * iters + done) : nullptr;
+                int rc = finish_chunk(hs[i], t0[i] + done, chunk, rh, &st);
+                if (!rc) rc = st;
+                if (status && rc && status[i] == MFCFD_OK) status[i] = rc;
+                if (rc && first_err == MFCFD_OK) first_err = rc;
+            }
+            done += chunk;
         }
         return first_err;
     });

@@ -370,6 +370,16 @@ struct DevCloud {
     double *res_dev;              // per-iteration res_new history
 };
 
+// The clouds of one group chain-sweep launch (mfcfd_run_group), passed as
+// the kernel's parameters: MFCFD_GROUP_MAX_CLOUDS views and the first block
+// of each cloud (block_start[count] = the grid).
+struct ChainGroup {
+    int count;
+    int block_start[MFCFD_GROUP_MAX_CLOUDS + 1];
+    DevCloud cloud[MFCFD_GROUP_MAX_CLOUDS];
+};
+static_assert(sizeof(ChainGroup) <= 32000, "a group launch's parameters must stay within 32 KB");
+
 // Streams of one handle: the main stream (high priority) and a side stream
 // that runs the flux residual beside the chain schedule's forward sweep,
 // with the events that fork and join them.
@@ -381,8 +391,20 @@ struct IterStreams {
 // kernel launchers (mfcfd_kernels.cu)
 // ev: null, or MFCFD_NPHASE+1 events recorded around the phases (ev[2] on
 // the side stream under the chain schedule).
+// part: ITER_ALL, or (chain schedule only) ITER_PRE -- every launch before
+// the sweeps, the flux residual on the side stream ending in st.join, with
+// st.fork recorded on the main stream where the forward sweep may start --
+// and ITER_POST, the state update and residual after the backward sweep.
+enum IterPart { ITER_ALL = 0, ITER_PRE = 1, ITER_POST = 2 };
 cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams &st,
-                             double *U_next, double *q_next, cudaEvent_t *ev);
+                             double *U_next, double *q_next, cudaEvent_t *ev, IterPart part = ITER_ALL);
+// One chain sweep (forward or backward) of every cloud of g in one launch;
+// all the group's clouds have chain blocks of wpb warps and one precision.
+cudaError_t launch_chain_group(const ChainGroup &g, int wpb, int precision, int spread, int forward,
+                               cudaStream_t s);
+// Whether the group kernel of this shape keeps the single-cloud kernel's
+// blocks per SM (so chain_block_slots holds for it too).
+bool chain_group_fits(int device, int wpb, int precision, int spread);
 cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s);
 // rows [a, a+rows) of width w: scatter from an index-order buffer to storage
 // order (dst[perm[a+i]] = src[i]), or gather the reverse

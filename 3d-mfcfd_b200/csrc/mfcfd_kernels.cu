@@ -1108,18 +1108,19 @@ constexpr int chain_min_blocks() {
     return (WPB == 4 && FOLD) ? 3 : 1;
 }
 
-// R: the type of the sweep's flux evaluations; FOLD: folded term weights
-// (MFCFD_PRECISION_MIXED and MIXED_DC).  FP64 <double, false>; mixed and
-// defect correction <float, true>.
+// One block of a cloud's chain sweep: block `block` of the cloud's
+// (ch_warps + WPB - 1) / WPB.  R: the type of the sweep's flux evaluations;
+// FOLD: folded term weights (MFCFD_PRECISION_MIXED and MIXED_DC).  FP64
+// <double, false>; mixed and defect correction <float, true>.
 template <int WPB, typename R, bool FOLD>
-__global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, FOLD>()) k_sweep_chain(DevCloud d, int forward) {
+__device__ __forceinline__ void chain_sweep(const DevCloud &d, int forward, int block) {
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char *smb = reinterpret_cast<char *>(smem) + warp * CHAIN_SMEM_BYTES;
     double *T = reinterpret_cast<double *>(smb);
     double *ring = T + SW_T_DOUBLES;
     SweepStage *stg = reinterpret_cast<SweepStage *>(ring + SW_RING_DOUBLES);
-    const int me = blockIdx.x * WPB + warp;
+    const int me = block * WPB + warp;
     if (me >= d.ch_warps) return;
     const int dir = forward ? 0 : 1;
     const int a = d.ch_ptr[dir][me], b = d.ch_ptr[dir][me + 1];
@@ -1151,6 +1152,24 @@ __global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, FOLD>()) k_swe
         cur = nxt;
         nxt = after;
     }
+}
+
+template <int WPB, typename R, bool FOLD>
+__global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, FOLD>()) k_sweep_chain(DevCloud d, int forward) {
+    chain_sweep<WPB, R, FOLD>(d, forward, blockIdx.x);
+}
+
+// The chain sweeps of a group of clouds in one launch: blocks
+// [block_start[c], block_start[c + 1]) are cloud c's.  The clouds share
+// nothing; a block finds its cloud and runs that cloud's schedule as the
+// single-cloud kernel would.  The group lives in the launch's parameters, so
+// every block reads its cloud's pointers from the constant bank.
+template <int WPB, typename R, bool FOLD>
+__global__ void __launch_bounds__(WPB * 32, chain_min_blocks<WPB, FOLD>())
+    k_sweep_chain_group(const __grid_constant__ ChainGroup g, int forward) {
+    int c = 0;
+    while (c + 1 < g.count && (int)blockIdx.x >= g.block_start[c + 1]) ++c;
+    chain_sweep<WPB, R, FOLD>(g.cloud[c], forward, (int)blockIdx.x - g.block_start[c]);
 }
 
 template <int WPB>
@@ -1468,6 +1487,16 @@ static void set_attributes(int device) {
     cudaFuncSetAttribute(k_sweep_chain<8, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
     cudaFuncSetAttribute(k_sweep_chain<4, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CHAIN_SPREAD_SMEM);
     cudaFuncSetAttribute(k_sweep_chain<8, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, chain_smem<8>());
+    cudaFuncSetAttribute(k_sweep_chain_group<4, float, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(k_sweep_chain_group<4, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         CHAIN_SPREAD_SMEM);
+    cudaFuncSetAttribute(k_sweep_chain_group<8, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         chain_smem<8>());
+    cudaFuncSetAttribute(k_sweep_chain_group<4, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         CHAIN_SPREAD_SMEM);
+    cudaFuncSetAttribute(k_sweep_chain_group<8, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         chain_smem<8>());
     done[device] = true;
 }
 
@@ -1504,6 +1533,32 @@ int chain_block_slots(int device, int wpb, int precision, int spread) {
     per_sm = per_sm < 1 ? 1 : (per_sm > 3 ? 3 : per_sm);
     std::lock_guard<std::mutex> lock(mu);
     return cache[device][w8][m] = 6 / per_sm;
+}
+
+bool chain_group_fits(int device, int wpb, int precision, int spread) {
+    set_attributes(device);
+    const bool mixed = precision != MFCFD_PRECISION_FP64;
+    const int smem = chain_smem_bytes(wpb, spread);
+    int one = 0, group = 0;
+    cudaError_t e1, e2;
+    if (wpb == 8) {
+        e1 = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&one, k_sweep_chain<8, float, true>, 256, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&one, k_sweep_chain<8, double, false>, 256, smem);
+        e2 = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group, k_sweep_chain_group<8, float, true>, 256, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group, k_sweep_chain_group<8, double, false>, 256,
+                                                                   smem);
+    } else {
+        e1 = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&one, k_sweep_chain<4, float, true>, 128, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&one, k_sweep_chain<4, double, false>, 128, smem);
+        e2 = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group, k_sweep_chain_group<4, float, true>, 128, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group, k_sweep_chain_group<4, double, false>, 128,
+                                                                   smem);
+    }
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return group >= 1 && group >= one;
 }
 
 int chain_shape(int device, int want, int spread, int *wpb, int *blocks) {
@@ -1599,8 +1654,20 @@ static cudaError_t launch_prio(void (*kern)(Args...), int grid, int block, size_
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);
 }
 
+cudaError_t launch_chain_group(const ChainGroup &g, int wpb, int precision, int spread, int forward,
+                               cudaStream_t s) {
+    const int blocks = g.block_start[g.count];
+    const int csm = chain_smem_bytes(wpb, spread);
+    if (precision != MFCFD_PRECISION_FP64) {
+        if (wpb == 4) return launch_prio(k_sweep_chain_group<4, float, true>, blocks, 4 * 32, csm, s, true, g, forward);
+        return launch_prio(k_sweep_chain_group<8, float, true>, blocks, 8 * 32, csm, s, true, g, forward);
+    }
+    if (wpb == 4) return launch_prio(k_sweep_chain_group<4, double, false>, blocks, 4 * 32, csm, s, true, g, forward);
+    return launch_prio(k_sweep_chain_group<8, double, false>, blocks, 8 * 32, csm, s, true, g, forward);
+}
+
 cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams &st, double *U_next,
-                             double *q_next, cudaEvent_t *ev) {
+                             double *q_next, cudaEvent_t *ev, IterPart part) {
     const int n = d.n;
     cudaStream_t s = st.main;
     int dev = 0;
@@ -1635,6 +1702,8 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     };
     auto mark = [&](int i, cudaStream_t on) { if (ev) cudaEventRecord(ev[i], on); };
     const int fblocks = (n + FLUX_WARPS - 1) / FLUX_WARPS;
+    if (part != ITER_ALL && !chains) return cudaErrorInvalidValue;
+    if (part == ITER_POST) goto post;
     mark(0, s);
     // supersonic copies may read a neighbour's increment from before the
     // sweeps, which k_pending is about to mark
@@ -1674,6 +1743,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
         flux(0, n, fgrid, st.side, false);
         mark(2, st.side);
         cudaEventRecord(st.join, st.side);
+        if (part == ITER_PRE) return cudaGetLastError();
         sweep(1);
         mark(4, s);
         cudaStreamWaitEvent(s, st.join, 0);
@@ -1688,6 +1758,7 @@ cudaError_t launch_iteration(const DevCloud &d, int iter_slot, const IterStreams
     }
     sweep(0);
     mark(5, s);
+post:
     k_update<<<(n + 127) / 128, 128, 0, s>>>(d, U_next, q_next);
     if (d.n_ss > 0) k_update_ss<<<1, 32, 0, s>>>(d, U_next, q_next);
     mark(6, s);

@@ -26,13 +26,14 @@ EXPORTS = ("mfcfd_params_init", "mfcfd_create", "mfcfd_set_prim", "mfcfd_fpi_ste
            "mfcfd_get_stream", "mfcfd_set_profiling", "mfcfd_get_phase_times",
            "mfcfd_residual_noalloc", "mfcfd_set_fault_hook", "mfcfd_set_precision", "mfcfd_count_input_points", "mfcfd_read_input_point_data",
            "mfcfd_read_stored_solution", "mfcfd_print_primal_output", "mfcfd_write_residue",
-           "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch",
+           "mfcfd_forces", "mfcfd_set_wall_areas", "mfcfd_run_batch", "mfcfd_run_group",
            "mfcfd_prepare", "mfcfd_device_bytes", "mfcfd_attach", "mfcfd_tune_chain",
            "mfcfd_set_chain_warps", "mfcfd_launch", "mfcfd_complete",
            "mfcfd_server_create", "mfcfd_server_submit", "mfcfd_server_wait",
            "mfcfd_server_get_stats", "mfcfd_server_destroy",
            "mfcfd_destroy", "mfcfd_last_error", "mfcfd_strerror")
 NOALLOC_MAX_TERMS = 1024 * 4096
+GROUP_MAX_CLOUDS = 32
 NPHASE = 7
 PHASES = ("qderiv", "flux", "dinv", "sweep_fwd", "sweep_bwd", "update", "residual")
 
@@ -78,7 +79,7 @@ class Info(ctypes.Structure):
                 ("chain_warps", ctypes.c_int32), ("chain_terms_ring", ctypes.c_int64),
                 ("chain_terms_local", ctypes.c_int64), ("chain_terms_cross", ctypes.c_int64),
                 ("chain_slots", ctypes.c_int32), ("chain_slot_capacity", ctypes.c_int32),
-                ("g0_points", ctypes.c_int32)]
+                ("g0_points", ctypes.c_int32), ("chain_warps_per_block", ctypes.c_int32)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -166,6 +167,7 @@ def lib():
     L.mfcfd_forces.argtypes = [vp, dbl, dbl, vp, vp, vp]
     L.mfcfd_set_wall_areas.argtypes = [vp, vp]
     L.mfcfd_run_batch.argtypes = [vp, i32, vp, i32, vp, vp]
+    L.mfcfd_run_group.argtypes = [vp, i32, vp, i32, vp, vp]
     L.mfcfd_prepare.argtypes = [ctypes.POINTER(Params), i32] + [vp] * 10 + [ctypes.POINTER(vp)]
     L.mfcfd_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_int64)]
     L.mfcfd_attach.argtypes = [vp]

@@ -1,9 +1,13 @@
-"""Concurrent iteration of several clouds on one GPU (mfcfd_run_batch).
+"""Concurrent iteration of several clouds on one GPU.
 
-Each cloud keeps its own handle (state resident, own streams); a batch call
-launches every cloud's iterations in turn so that one cloud's latency-bound
-LU-SGS sweeps run beside another's.  Clouds whose chain-schedule sweeps
-would not all fit on the device together are run in successive waves.
+Each cloud keeps its own handle (state resident, own streams).  A batch call
+(mfcfd_run_batch) launches every cloud's iterations in turn so that one
+cloud's latency-bound LU-SGS sweeps run beside another's; clouds whose
+chain-schedule sweeps would not all fit on the device together run as they
+fit, each starting its next chunk as soon as there is room.  A group call
+(mfcfd_run_group) runs up to 32 clouds in lockstep with each sweep
+direction of all of them in one kernel launch; plan_groups packs a batch
+into such groups and run_grouped runs them one after another.
 """
 from __future__ import annotations
 
@@ -21,6 +25,64 @@ def run_batch(solvers, iters: int, t0=None, statuses=None):
     list `statuses`, a cloud's failure (a non-finite residual, say) is
     recorded there instead of raised, and the other clouds' histories are
     kept."""
+    return _run("mfcfd_run_batch", solvers, iters, t0, statuses)
+
+
+def run_group(solvers, iters: int, t0=None, statuses=None):
+    """As run_batch, in lockstep with one chain-sweep launch per direction
+    for all the solvers (mfcfd_run_group): at most GROUP_MAX_CLOUDS chain-
+    schedule solvers of one block shape and precision class whose sweeps
+    fit the device together (plan_groups makes such groups)."""
+    return _run("mfcfd_run_group", solvers, iters, t0, statuses)
+
+
+def plan_groups(solvers):
+    """Pack solvers into groups that mfcfd_run_group accepts: by block shape
+    and precision class, largest clouds first, each group filled while its
+    chain slots fit the device and it has fewer than GROUP_MAX_CLOUDS
+    solvers.  Clouds of similar size then share a group, so a lockstep
+    iteration waits little for its slowest sweep.  Returns lists of indices
+    into `solvers`."""
+    infos = [s.info() for s in solvers]
+    keys = {}
+    for i, (s, inf) in enumerate(zip(solvers, infos)):
+        k = (inf["chain_warps_per_block"], int(s.params.chain_spread), int(s.params.precision) != 0)
+        keys.setdefault(k, []).append(i)
+    groups = []
+    for k in sorted(keys):
+        idx = sorted(keys[k], key=lambda i: -solvers[i].n)
+        cur, used = [], 0
+        for i in idx:
+            sl, cap = infos[i]["chain_slots"], infos[i]["chain_slot_capacity"]
+            if cur and (used + sl > cap or len(cur) >= _lib.GROUP_MAX_CLOUDS):
+                groups.append(cur)
+                cur, used = [], 0
+            cur.append(i)
+            used += sl
+        if cur:
+            groups.append(cur)
+    return groups
+
+
+def run_grouped(solvers, iters: int, groups=None, statuses=None):
+    """run_group over plan_groups(solvers) (or the given groups), one group
+    after another; returns res_hist (len(solvers), iters, 2) in the solvers'
+    order."""
+    groups = plan_groups(solvers) if groups is None else groups
+    hist = np.zeros((len(solvers), iters, 2))
+    st = [0] * len(solvers)
+    for g in groups:
+        part = [] if statuses is not None else None
+        hist[g] = run_group([solvers[i] for i in g], iters, statuses=part)
+        if part is not None:
+            for i, v in zip(g, part):
+                st[i] = v
+    if statuses is not None:
+        statuses[:] = st
+    return hist
+
+
+def _run(fn: str, solvers, iters: int, t0, statuses):
     n = len(solvers)
     hs = (ctypes.c_void_p * n)(*[s.h.value for s in solvers])
     if t0 is None:
@@ -28,7 +90,10 @@ def run_batch(solvers, iters: int, t0=None, statuses=None):
     t0a = np.ascontiguousarray(t0, dtype=np.int32)
     hist = np.zeros((n, iters, 2))
     status = np.zeros(n, dtype=np.int32)
-    rc = _lib.lib().mfcfd_run_batch(hs, n, ptr(t0a), int(iters), ptr(hist), ptr(status))
+    rc = getattr(_lib.lib(), fn)(hs, n, ptr(t0a), int(iters), ptr(hist), ptr(status))
+    if rc != 0 and not status.any():   # refused as a whole: nothing ran
+        msg = _lib.lib().mfcfd_last_error(solvers[0].h).decode() if n else ""
+        raise MfcfdError(rc, msg or "batch failed")
     if statuses is not None:
         statuses[:] = [int(v) for v in status]
     for i, s in enumerate(solvers):
@@ -38,8 +103,6 @@ def run_batch(solvers, iters: int, t0=None, statuses=None):
             raise MfcfdError(int(status[i]), _lib.lib().mfcfd_last_error(s.h).decode())
         for j in range(iters):
             s.history.append((int(t0a[i]) + j, float(hist[i, j, 0]), float(hist[i, j, 1])))
-    if rc != 0 and (statuses is None or not any(statuses)):
-        raise MfcfdError(rc, "batch failed")
     return hist
 
 

@@ -283,6 +283,8 @@ def main():
                     help="Mach range of the batch workload's flows")
     ap.add_argument("--batch-budget-gb", type=float, default=120.0,
                     help="device memory of one wave of batched handles")
+    ap.add_argument("--no-batch-grouped", dest="batch_grouped", action="store_false",
+                    help="batch workload: skip the lockstep group form (mfcfd_run_group)")
     ap.add_argument("--batch-min-points", type=int, default=None,
                     help="smallest cloud (default 20000 for batch, 10000 for batch-converged)")
     ap.add_argument("--batch-max-points", type=int, default=None,
@@ -786,7 +788,7 @@ def batch_main(args, rank, world, local_rank):
     # batched: mixed precision, tuned schedules, graph-captured chunks, in
     # waves of handles within the memory budget
     budget = args.batch_budget_gb * 1e9
-    bat_s, t_setup, t_tune, waves = 0.0, 0.0, 0.0, []
+    bat_s, grp_s, t_setup, t_tune, waves = 0.0, 0.0, 0.0, 0.0, []
     percents, warps = [], []
     j = 0
     while j < len(clouds):
@@ -838,6 +840,24 @@ def batch_main(args, rank, world, local_rank):
         bat_s += dt
         waves.append({"clouds": len(ss), "points": sum(s.n for s in ss), "device_bytes": used, "timed_s": dt,
                       "restarted_clouds": restarted})
+        if args.batch_grouped:
+            # the same handles in lockstep groups, each sweep direction of a
+            # group in one launch (mfcfd_run_group); warmed the same way
+            groups = batch.plan_groups(ss)
+            for _ in range(1 if args.steps % 2 == 0 else 2):
+                batch.run_grouped(ss, args.steps, groups, statuses=st)
+                restart_failed(st)
+            for attempt in range(3):
+                replicas.barrier()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                batch.run_grouped(ss, args.steps, groups, statuses=st)
+                torch.cuda.synchronize()
+                gdt = time.perf_counter() - t0
+                if restart_failed(st) == 0:
+                    break
+            grp_s += gdt
+            waves[-1].update({"grouped_timed_s": gdt, "groups": [len(g) for g in groups]})
         print(f"wave {len(waves)}: {len(ss)} clouds, {waves[-1]['points']} points, {used / 1e9:.1f} GB, "
               f"{dt:.3f} s, restarted {restarted}", file=sys.stderr, flush=True)
         for s in ss:
@@ -865,6 +885,13 @@ def batch_main(args, rank, world, local_rank):
                 "fp64_one_at_a_time": {"value": pts * args.steps * world / seq_s, "unit": "point-iters/s",
                                        "ms_per_step": seq_s * 1e3 / args.steps, "restarted": seq_restarted},
                 "speedup_vs_fp64_one_at_a_time": seq_s / bat_s}
+        if args.batch_grouped:
+            line["grouped"] = {"value": pts * args.steps * world / grp_s, "unit": "point-iters/s",
+                               "ms_per_step": grp_s * 1e3 / args.steps,
+                               "speedup_vs_fp64_one_at_a_time": seq_s / grp_s,
+                               "form": "mfcfd_run_group: lockstep groups of up to 32 clouds of similar size, "
+                                       "one chain-sweep launch per direction per group iteration, groups "
+                                       "one after another"}
         print(json.dumps(line), flush=True)
     replicas.finalize()
 

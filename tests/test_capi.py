@@ -97,6 +97,15 @@ def test_host_only_handle_refuses_device_calls(mfcfd_lib, small_cloud):
     with pytest.raises(MfcfdError):
         s.residual_noalloc()
     assert s.info()["n_points"] == small_cloud.n
+    # a group needs handles with device state, at most MFCFD_GROUP_MAX_CLOUDS
+    import ctypes
+    import numpy as np
+    from mfcfd import _lib
+    t0 = np.ones(40, dtype=np.int32)
+    for count in (0, 1, _lib.GROUP_MAX_CLOUDS + 1):
+        hs = (ctypes.c_void_p * 40)(*([s.h.value] * 40))
+        assert _lib.lib().mfcfd_run_group(hs, count, _lib.ptr(t0), 1, None, None) == 1
+    assert _lib.lib().mfcfd_run_group(None, 1, _lib.ptr(t0), 1, None, None) == 1
 
 
 def test_prepare_needs_a_device_and_serving_helpers(mfcfd_lib, small_cloud):
