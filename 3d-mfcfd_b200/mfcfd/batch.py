@@ -147,19 +147,22 @@ def tune_batch(solvers, percents=(75, 100, 125, 150, 200), iters: int = 4):
 
 
 def solve_batch(solvers, target: float = -6.0, max_iters: int = 12000, chunk: int = 100,
-                polish: float | None = -5.0):
+                polish: float | None = -5.0, grouped: bool = False):
     """Run every Solver until its residue reaches `target` (or `max_iters`),
     in batched rounds of `chunk` iterations over the clouds still running.
     A MIXED_DC solver switches to FP64 once its residue is at or below
     `polish` (None: never), so it reaches a 1e-6 drop in about FP64's
-    iteration count.  Returns, per solver, a dict with the iterations run,
-    whether it converged, and the seconds from the call to its retirement."""
+    iteration count.  With `grouped`, each round runs as lockstep groups
+    (run_grouped, planned again every round, since clouds retire and switch
+    precision class); otherwise as one run_batch.  Returns, per solver, a
+    dict with the iterations run, whether it converged, and the seconds
+    from the call to its retirement."""
     import time
     t_start = time.perf_counter()
     live = list(range(len(solvers)))
     out = [dict(iters=0, converged=False, seconds=None, polished=False) for _ in solvers]
     while live:
-        hist = run_batch([solvers[i] for i in live], chunk)
+        hist = (run_grouped if grouped else run_batch)([solvers[i] for i in live], chunk)
         now = time.perf_counter() - t_start
         keep = []
         for j, i in enumerate(live):

@@ -283,8 +283,12 @@ def main():
                     help="Mach range of the batch workload's flows")
     ap.add_argument("--batch-budget-gb", type=float, default=120.0,
                     help="device memory of one wave of batched handles")
+    ap.add_argument("--batch-graphs", type=int, choices=[0, 1], default=1,
+                    help="batch workload: capture chunks as CUDA graphs (1) or launch kernel by kernel (0, "
+                         "the form for profiling: launches run in the order issued)")
     ap.add_argument("--no-batch-grouped", dest="batch_grouped", action="store_false",
-                    help="batch workload: skip the lockstep group form (mfcfd_run_group)")
+                    help="batch and batch-converged workloads: skip the lockstep group form "
+                         "(mfcfd_run_group)")
     ap.add_argument("--batch-min-points", type=int, default=None,
                     help="smallest cloud (default 20000 for batch, 10000 for batch-converged)")
     ap.add_argument("--batch-max-points", type=int, default=None,
@@ -710,6 +714,31 @@ def batch_converged_main(args, rank, world, local_rank):
         cl_, cd_, _ = s.forces()
         errs.append((abs(cl_ - f["forces"][0]), abs(cd_ - f["forces"][1])))
         s.close()
+    grouped = None
+    if args.batch_grouped:
+        # the same solves as lockstep groups (mfcfd_run_group), fresh handles
+        ss = []
+        for c, (m, a) in zip(clouds, flows):
+            s = Solver(c, m, a, device=local_rank, precision=_lib.PRECISION_MIXED_DC)
+            s.initial_conditions()
+            ss.append(s)
+        replicas.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gout = batch.solve_batch(ss, max_iters=args.batch_max_iters, polish=-5.0, grouped=True)
+        torch.cuda.synchronize()
+        grp_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
+        gerr = []
+        for s, f in zip(ss, fp64):
+            cl_, cd_, _ = s.forces()
+            gerr.append((abs(cl_ - f["forces"][0]), abs(cd_ - f["forces"][1])))
+            s.close()
+        grouped = {"value": len(clouds) * world / grp_s, "unit": "solves/s", "seconds": grp_s,
+                   "converged": sum(1 for r in gout if r["converged"]),
+                   "iterations": [r["iters"] for r in gout],
+                   "speedup_vs_fp64_one_at_a_time": seq_s / grp_s,
+                   "max_abs_dCL": max(e[0] for e in gerr), "max_abs_dCD": max(e[1] for e in gerr),
+                   "form": "mfcfd_run_group: each 100-iteration round as lockstep groups"}
     if rank == 0:
         n = len(clouds) * world
         line = {"metric": "converged solves/s (1e-6 residual drop) batched mixed-dc vs FP64 one at a time",
@@ -729,6 +758,8 @@ def batch_converged_main(args, rank, world, local_rank):
                                        "iterations": [r["iters"] for r in fp64]},
                 "speedup_vs_fp64_one_at_a_time": seq_s / bat_s,
                 "max_abs_dCL": max(e[0] for e in errs), "max_abs_dCD": max(e[1] for e in errs)}
+        if grouped:
+            line["grouped"] = grouped
         print(json.dumps(line), flush=True)
     replicas.finalize()
 
@@ -796,7 +827,8 @@ def batch_main(args, rank, world, local_rank):
         t1 = time.perf_counter()
         while j < len(clouds):
             c, (m, a) = clouds[j], flows[j]
-            s = Solver(c, m, a, device=local_rank, precision=_lib.PRECISION_MIXED, gpu_setup=1)
+            s = Solver(c, m, a, device=local_rank, precision=_lib.PRECISION_MIXED, gpu_setup=1,
+                       graphs=args.batch_graphs)
             s.initial_conditions()
             ss.append(s)
             used += s.info()["device_bytes"]
