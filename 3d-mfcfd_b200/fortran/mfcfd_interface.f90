@@ -194,6 +194,17 @@ module mfcfd_interface
             integer(c_int) :: rc
         end function mfcfd_run_batch
 
+        ! the same in lockstep, each sweep of all count (<= 32) handles in one launch
+        function mfcfd_run_group(hs, count, t0, iters, res_hist, status) result(rc) bind(C, name="mfcfd_run_group")
+            import :: c_ptr, c_int32_t, c_double, c_int
+            type(c_ptr), intent(in) :: hs(*)
+            integer(c_int32_t), value :: count, iters
+            integer(c_int32_t), intent(in) :: t0(*)
+            real(c_double), intent(out) :: res_hist(*)
+            integer(c_int32_t), intent(out) :: status(*)
+            integer(c_int) :: rc
+        end function mfcfd_run_group
+
         function mfcfd_tune_chain(h, candidates, count, iters, chosen, ms) result(rc) bind(C, name="mfcfd_tune_chain")
             import :: c_ptr, c_int32_t, c_int
             type(c_ptr), value :: h, candidates, ms

@@ -270,18 +270,19 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
                     double *res_hist, int32_t *status);
 
 /*
- * Groups: iterations t0[i] .. t0[i]+iters-1 of up to MFCFD_GROUP_MAX_CLOUDS
- * handles of one device in lockstep, each sweep direction of every handle
- * in ONE kernel launch (the persistent multi-cloud chain sweep); the other
- * kernels of an iteration run per handle, on the handles' own streams,
- * between the group's sweeps.  The handles use the chain schedule with the
- * same block shape (mfcfd_info.chain_warps_per_block), chain_spread and
- * precision class (FP64, or MIXED / MIXED_DC), and their
+ * Groups (the q_lskum loop, q_lskum.f90:28-32, of several clouds at once; no
+ * counterpart in the reference): iterations t0[i] .. t0[i]+iters-1 of up to
+ * MFCFD_GROUP_MAX_CLOUDS handles of one device in lockstep, each sweep
+ * direction of every handle in ONE kernel launch (the persistent multi-cloud
+ * chain sweep); the other kernels of an iteration run per handle, on the
+ * handles' own streams, between the group's sweeps.  The handles use the
+ * chain schedule with the same block shape (mfcfd_info.chain_warps_per_block),
+ * chain_spread and precision class (FP64, or MIXED / MIXED_DC), and their
  * mfcfd_info.chain_slots add up to chain_slot_capacity at most; otherwise
- * MFCFD_ERR_UNSUPPORTED.  Every
- * handle gets the bits mfcfd_run gives it.  A group waits each iteration for
- * its slowest sweep, so handles of similar size group best.  res_hist and
- * status as in mfcfd_run_batch.
+ * MFCFD_ERR_UNSUPPORTED, before anything runs.  Every handle gets the bits
+ * mfcfd_run gives it.  A group waits each iteration for its slowest sweep,
+ * so handles of similar size group best.  res_hist and status as in
+ * mfcfd_run_batch.
  */
 #define MFCFD_GROUP_MAX_CLOUDS 32
 int mfcfd_run_group(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, int32_t iters,
