@@ -1635,12 +1635,13 @@ cudaError_t launch_conserved_q(const DevCloud &d, cudaStream_t s) {
 template <typename... Args, typename... Act>
 static cudaError_t launch_prio(void (*kern)(Args...), int grid, int block, size_t smem, cudaStream_t s, bool high,
                                Act &&...args) {
-    static int prio[2] = {0, 0};
-    static bool have = false;
-    if (!have) {
-        cudaDeviceGetStreamPriorityRange(&prio[0], &prio[1]);   // least, greatest
-        have = true;
-    }
+    // least and greatest priority, looked up once (thread-safe initialisation:
+    // group runs may launch from several host threads)
+    static const std::pair<int, int> prio = [] {
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        return std::make_pair(lo, hi);
+    }();
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
@@ -1648,7 +1649,7 @@ static cudaError_t launch_prio(void (*kern)(Args...), int grid, int block, size_
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributePriority;
-    attr[0].val.priority = high ? prio[1] : prio[0];
+    attr[0].val.priority = high ? prio.second : prio.first;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);

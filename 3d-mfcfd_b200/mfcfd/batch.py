@@ -7,7 +7,8 @@ chain-schedule sweeps would not all fit on the device together run as they
 fit, each starting its next chunk as soon as there is room.  A group call
 (mfcfd_run_group) runs up to 32 clouds in lockstep with each sweep
 direction of all of them in one kernel launch; plan_groups packs a batch
-into such groups and run_grouped runs them one after another.
+into such groups and run_grouped runs them, side by side where their
+sweeps fit the device together.
 """
 from __future__ import annotations
 
@@ -64,19 +65,57 @@ def plan_groups(solvers):
     return groups
 
 
+def plan_waves(solvers, groups):
+    """Consecutive groups whose chain slots fit the device together, as
+    lists of group indices: the groups of a wave may run side by side."""
+    waves, cur, used = [], [], 0
+    for gi, g in enumerate(groups):
+        infos = [solvers[i].info() for i in g]
+        sl, cap = sum(x["chain_slots"] for x in infos), infos[0]["chain_slot_capacity"]
+        if cur and used + sl > cap:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(gi)
+        used += sl
+    if cur:
+        waves.append(cur)
+    return waves
+
+
 def run_grouped(solvers, iters: int, groups=None, statuses=None):
-    """run_group over plan_groups(solvers) (or the given groups), one group
-    after another; returns res_hist (len(solvers), iters, 2) in the solvers'
-    order."""
+    """run_group over plan_groups(solvers) (or the given groups); returns
+    res_hist (len(solvers), iters, 2) in the solvers' order.  Groups whose
+    chain sweeps fit the device together (plan_waves) run side by side, one
+    host thread each (the library call releases the interpreter), so all
+    their sweeps stay resident; the waves run one after another."""
+    import threading
     groups = plan_groups(solvers) if groups is None else groups
     hist = np.zeros((len(solvers), iters, 2))
     st = [0] * len(solvers)
-    for g in groups:
-        part = [] if statuses is not None else None
-        hist[g] = run_group([solvers[i] for i in g], iters, statuses=part)
-        if part is not None:
-            for i, v in zip(g, part):
-                st[i] = v
+    for wave in plan_waves(solvers, groups):
+        errors = []
+
+        def one(g):
+            part = [] if statuses is not None else None
+            try:
+                hist[g] = run_group([solvers[i] for i in g], iters, statuses=part)
+            except Exception as e:          # re-raised below, after the wave
+                errors.append(e)
+                return
+            if part is not None:
+                for i, v in zip(g, part):
+                    st[i] = v
+
+        if len(wave) == 1:
+            one(groups[wave[0]])
+        else:
+            threads = [threading.Thread(target=one, args=(groups[gi],)) for gi in wave]
+            for t in threads:
+                t.start()
+            for t in threads:
+                t.join()
+        if errors:
+            raise errors[0]
     if statuses is not None:
         statuses[:] = st
     return hist

@@ -283,6 +283,9 @@ def main():
                     help="Mach range of the batch workload's flows")
     ap.add_argument("--batch-budget-gb", type=float, default=120.0,
                     help="device memory of one wave of batched handles")
+    ap.add_argument("--no-batch-fp64", dest="batch_fp64", action="store_false",
+                    help="batch-converged: skip the FP64 one-at-a-time solves (no speed-up or CL/CD "
+                         "error in the line; for comparing the batched forms alone)")
     ap.add_argument("--batch-graphs", type=int, choices=[0, 1], default=1,
                     help="batch workload: capture chunks as CUDA graphs (1) or launch kernel by kernel (0, "
                          "the form for profiling: launches run in the order issued)")
@@ -689,6 +692,9 @@ def batch_converged_main(args, rank, world, local_rank):
     t0 = time.perf_counter()
     fp64 = []
     for c, (m, a) in zip(clouds, flows):
+        if not args.batch_fp64:
+            fp64.append({"forces": (float("nan"), float("nan")), "iters": None, "converged": None})
+            continue
         s = Solver(c, m, a, device=local_rank)
         s.initial_conditions()
         r = batch.solve_batch([s], max_iters=args.batch_max_iters, polish=None)[0]
@@ -696,7 +702,7 @@ def batch_converged_main(args, rank, world, local_rank):
         fp64.append(r)
         s.close()
     torch.cuda.synchronize()
-    seq_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda")
+    seq_s = replicas.max_over_ranks(time.perf_counter() - t0, device="cuda") if args.batch_fp64 else float("nan")
     # batched MIXED_DC with the FP64 polish
     ss = []
     for c, (m, a) in zip(clouds, flows):
