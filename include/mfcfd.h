@@ -282,7 +282,11 @@ int mfcfd_run_batch(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, i
  * MFCFD_ERR_UNSUPPORTED, before anything runs.  Every handle gets the bits
  * mfcfd_run gives it.  A group waits each iteration for its slowest sweep,
  * so handles of similar size group best.  res_hist and status as in
- * mfcfd_run_batch.
+ * mfcfd_run_batch.  Calls on disjoint handles may run from separate host
+ * threads at once; as with mfcfd_launch, the chain sweeps running at the
+ * same time must then fit the device together (their chain_slots add up to
+ * chain_slot_capacity at most), or their bounded waits may run out
+ * (MFCFD_ERR_TIMEOUT).
  */
 #define MFCFD_GROUP_MAX_CLOUDS 32
 int mfcfd_run_group(mfcfd_handle *const *hs, int32_t count, const int32_t *t0, int32_t iters,
