@@ -74,9 +74,13 @@ extern "C" {
                                       path, the implicit LU-SGS operator (the
                                       sweeps' flux evaluations, and the fluxes of
                                       the state they difference against) in
-                                      FP32.  The iteration's fixed point is the
-                                      FP64 one, so it converges as far as FP64
-                                      does.  Requires MFCFD_SWEEP_CHAINS. */
+                                      FP32, each sweep list's 3x3 solve folded
+                                      into its terms' weights.  The iteration's
+                                      fixed point is the FP64 one; below about a
+                                      1e-5 drop it slows, since FP32 increments
+                                      resolve the state only to FP32 (finish in
+                                      FP64: mfcfd_set_precision).  Requires
+                                      MFCFD_SWEEP_CHAINS. */
 
 /*
  * Run-time form of the reference's compile-time constants (parameter.f90:
