@@ -654,17 +654,34 @@ int build_topology(const mfcfd_params &P, int n, const int32_t *status, const do
             if ((gpu_rc = prep_levels_gpu(P.device, n, order, doff, deps, level, err))) return false;
             for (int p : order) maxl = std::max(maxl, (int)level[p]);
         } else {
-            auto visit = [&](int p) {
+            // the producers each point depends on, gathered in parallel and
+            // laid out in the sweep order, so that the sequential
+            // longest-path pass reads them front to back
+            const int m = (int)order.size();
+            std::vector<int32_t> doff((size_t)m + 1, 0), deps;
+            parallel_for(m, [&](int oi) {
+                const int p = order[oi];
+                int c = 0;
+                for (int e = off[p]; e < off[p + 1]; ++e) c += is_dep(ent[e]) ? 1 : 0;
+                doff[(size_t)oi + 1] = c;
+            });
+            for (int oi = 0; oi < m; ++oi) doff[(size_t)oi + 1] += doff[oi];
+            deps.resize((size_t)doff[m]);
+            parallel_for(m, [&](int oi) {
+                const int p = order[oi];
+                int at = doff[oi];
+                for (int e = off[p]; e < off[p + 1]; ++e)
+                    if (is_dep(ent[e])) deps[at++] = ent[e].k;
+            });
+            for (int oi = 0; oi < m; ++oi) {
                 int lv = 0;
-                for (int e = off[p]; e < off[p + 1]; ++e) {
-                    if (!is_dep(ent[e])) continue;
-                    const int k = ent[e].k;
+                for (int j = doff[oi]; j < doff[(size_t)oi + 1]; ++j) {
+                    const int k = deps[j];
                     if (level[k] + 1 > lv) lv = level[k] + 1;
                 }
-                level[p] = lv;
+                level[order[oi]] = lv;
                 maxl = std::max(maxl, lv);
-            };
-            for (int p : order) visit(p);
+            }
         }
         int nl = maxl + 1;
         lptr.assign(nl + 1, 0);
